@@ -1,0 +1,197 @@
+/* latec_b200.h -- C ABI of the B200 (sm_100a) LATEC hot path.
+ *
+ * The reference LATEC is a Python package whose hot path sits behind a
+ * duck-typed plugin boundary: the codec driver calls
+ * predictor.predict(recon, known, pos) and then quantize / pack_stage on the
+ * result (reference latec/codec.py:384-510). This library replaces the work
+ * behind that boundary with CUDA kernels; each entry point below names the
+ * reference function(s) it replaces. Plain pointers and sizes only: device
+ * pointers are raw CUDA device addresses, `stream` is a cudaStream_t (NULL =
+ * legacy default stream). Every function returns LATEC_OK (0) or a negative
+ * LATEC_ERR_* code; kernels that detect malformed input set bits in a
+ * caller-provided device error word instead of faulting.
+ */
+#ifndef LATEC_B200_H
+#define LATEC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LATEC_MAX_NDIM 6
+
+#define LATEC_OK 0
+#define LATEC_ERR_ARG (-1)         /* invalid argument (ValueError in the reference) */
+#define LATEC_ERR_CUDA (-2)        /* CUDA launch / runtime failure */
+#define LATEC_ERR_UNSUPPORTED (-3) /* valid in the reference, not supported here */
+#define LATEC_ERR_STREAM (-4)      /* malformed stream */
+#define LATEC_ERR_WORKSPACE (-5)   /* workspace too small */
+#define LATEC_ERR_INTERNAL (-6)
+
+#define LATEC_F32 1
+#define LATEC_F64 2
+
+#define LATEC_RANS_LANES 0  /* native 32-lane interleaved coder */
+#define LATEC_RANS_COMPAT 1 /* single-stack coder, reference byte stream */
+
+typedef struct latec_plan latec_plan;
+
+/* Quantizer / predictor parameters shared by all stages of one pass. */
+typedef struct latec_quant_params {
+    int32_t dtype;        /* LATEC_F32 or LATEC_F64 (value/reconstruction type) */
+    int32_t channels;     /* C of the (C, *spatial) field */
+    int32_t radius;       /* quantizer radius, <= 32768 */
+    int32_t order;        /* 0 linear, 1 cubic */
+    int32_t center;       /* 0 average odd axes, 1 first odd axis, 2 last odd axis */
+    int32_t end_mode;     /* bit 0 quadratic ends, bit 1 extrapolation */
+    int32_t round_output; /* verify against the rounded reconstruction (integer sources) */
+    int32_t reserved;
+} latec_quant_params;
+
+/* Per-stage results written on the device. */
+typedef struct latec_stage_stats {
+    uint32_t n_out;    /* outliers of the stage */
+    uint32_t maxq;     /* max |q| over in-range codes */
+    uint32_t pad0, pad1;
+    double stats[5];   /* pred SAE, pred SSE, recon SAE, recon SSE, recon max */
+} latec_stage_stats;
+
+/* One stage of the entropy stage (host array; copied to the device). */
+typedef struct latec_rans_stage {
+    uint64_t codes_off;   /* first code of the stage in the codes buffer */
+    uint64_t out_off;     /* first outlier of the stage in the outlier buffer */
+    uint64_t enc;         /* device address: encoder symbol table (24 B/entry) */
+    uint64_t cdf;         /* device address: CDF rows (alphabet + 1 u32 each) */
+    uint64_t bucket;      /* device address: decoder bucket rows (4096 u16 each) */
+    uint64_t scratch_off; /* filled by the library */
+    uint64_t blob_off;    /* decode: word offset of the stage blob */
+    uint64_t rec_off;     /* filled by the library */
+    uint64_t framed_hi;   /* stage frame word without its 45-bit length */
+    uint32_t n;           /* symbols */
+    uint32_t K;           /* lane coder: symbols per lane per chunk */
+    uint32_t n_chunks;    /* filled by the library (encode) / given (decode) */
+    uint32_t chunk0;      /* filled by the library */
+    uint32_t alphabet;    /* 2^(kexp+1) */
+    int32_t kexp;
+    int32_t radius;
+    int32_t mode;         /* LATEC_RANS_LANES or LATEC_RANS_COMPAT */
+    int32_t per_point;    /* 1: per-symbol table row from the levels array */
+    uint32_t blob_words;  /* decode: blob length in words */
+    uint32_t n_out;
+    uint32_t pad;
+} latec_rans_stage;
+
+/* ---- schedule: replaces latec/levels.py:100-147 (iter_stage_plan),
+ *      221-282 (stage_counts), 297-326 (stage_strides), 469-574
+ *      (stage_layouts). anchor_block must be 1. */
+int latec_plan_create(const uint32_t* shape, int32_t ndim, int32_t levels,
+                      int32_t anchor_stride, int32_t anchor_block, latec_plan** out);
+int latec_plan_destroy(latec_plan* plan);
+int latec_plan_num_stages(const latec_plan* plan);
+int latec_plan_stage_info(const latec_plan* plan, int32_t stage, uint64_t* n_points,
+                          int32_t* stride, int32_t* weight, int32_t* axis);
+
+/* Host-side (no GPU) decode of stage ranks [first, first + count) into flat
+ * grid indices, the exact mapping the kernels use; equals the reference's
+ * np.flatnonzero(stage mask) order (latec/levels.py:184-208 mask_tiles). */
+int latec_plan_stage_flat(const latec_plan* plan, int32_t stage, uint64_t first, uint64_t count,
+                          int64_t* out_flat);
+
+/* Bytes of device workspace latec_encode_stages / latec_decode_stages /
+ * latec_quantize need for this plan. */
+uint64_t latec_stage_workspace_bytes(const latec_plan* plan, int32_t channels, int32_t dtype);
+uint64_t latec_flat_workspace_bytes(uint64_t items, int32_t dtype);
+
+/* ---- fused predict + quantize + reconstruct over every stage of the plan:
+ *      replaces latec/codec.py:384-459 (_compress_region) with
+ *      latec/predictor.py:255-317 (InterpPredictor.predict) and
+ *      latec/quantizer.py:28-120 (quantize / dequantize).
+ * x, recon: (C, *spatial) device arrays of dtype; recon must be zeroed.
+ * stage_eb: host array, one absolute bound per stage.
+ * codes: u16, C*n_t per stage, stage t at offset C*sum(n_<t).
+ * outliers: dtype elements, stage t's compacted outliers at the same offset.
+ * stats: device array of num_stages latec_stage_stats (zeroed by the call).
+ * hist_seg: device, per stage and per 2^22-code segment, 512 u32 bins
+ *   (bin 0 outliers, bin q+256 for |q| < 256), stage t at offset
+ *   512*sum(segments_<t); zeroed by the call.
+ * hist_total: device, num_stages * 65536 u32 code bins for |q| >= 256,
+ *   zeroed by the call. */
+int latec_encode_stages(const latec_plan* plan, const latec_quant_params* prm,
+                        const double* stage_eb, const void* x, void* recon, uint16_t* codes,
+                        void* outliers, latec_stage_stats* stats, uint32_t* hist_seg,
+                        uint32_t* hist_total, void* workspace, uint64_t workspace_bytes,
+                        void* stream);
+
+/* ---- predict one stage from recon (InterpPredictor.predict,
+ *      latec/predictor.py:255-317): pred gets C*n_t values, channel-major. */
+int latec_interp_predict_stage(const latec_plan* plan, int32_t stage,
+                               const latec_quant_params* prm, const void* recon, void* pred,
+                               void* stream);
+
+/* ---- quantize a compact array against a given prediction
+ *      (latec/quantizer.py:28-87 + dequantize 90-111): the GNN path.
+ *      recon_out gets the decoder's reconstruction; hist_seg/hist_total as
+ *      above for one stage; stats one element. */
+int latec_quantize(const latec_quant_params* prm, double eb, uint64_t items, const void* x,
+                   const void* pred, uint16_t* codes, void* recon_out, void* outliers,
+                   latec_stage_stats* stats, uint32_t* hist_seg, uint32_t* hist_total,
+                   void* workspace, uint64_t workspace_bytes, void* stream);
+
+/* ---- decode: predict + dequantize over every stage
+ *      (latec/codec.py:462-510 _decompress_region). codes as produced by
+ *      latec_rans_decode; outliers: device byte array holding every stage's
+ *      outliers (dtype elements, no alignment required), stage t starting at
+ *      byte out_off[t] with n_out[t] entries (host arrays). err: device word,
+ *      bit 1 = outlier count mismatch. recon must be zeroed. */
+int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
+                        const double* stage_eb, const uint16_t* codes, const void* outliers,
+                        const uint64_t* out_off, const uint32_t* n_out, void* recon,
+                        uint32_t* err, void* workspace, uint64_t workspace_bytes, void* stream);
+
+/* ---- rANS tables: encoder symbols and decoder buckets for `rows` CDF rows
+ *      of alphabet + 1 entries (latec/rans.py:304-329 tables, compiled the
+ *      way latec/rans.py:629-657 compiles constriction models). */
+int latec_rans_build_tables(const uint32_t* cdf_rows, int32_t alphabet, int32_t rows, void* enc,
+                            uint16_t* bucket, void* stream);
+
+/* Bytes of device workspace latec_rans_encode needs for these stages
+ * (fills scratch_off / n_chunks / chunk0 of the host array). */
+uint64_t latec_rans_encode_workspace_bytes(latec_rans_stage* stages, int32_t n_stages);
+
+/* ---- entropy-code every stage and assemble the stage records
+ *      (latec/bitstream.py:178-243 pack_stage with latec/rans.py:466-498
+ *      rans_encode_const / 546-578 rans_encode) into `payload` on the
+ *      device: per stage u32 n | u64 frame | blob | u32 n_out | outliers.
+ *      payload_len: device u64; err: device u32 (bit 2: symbol outside the
+ *      alphabet, bit 32: payload capacity exceeded). */
+int latec_rans_encode(latec_rans_stage* stages, int32_t n_stages, const uint16_t* codes,
+                      const uint8_t* levels, const latec_stage_stats* stats,
+                      const void* outliers, int32_t elem, uint8_t* payload, uint64_t payload_cap,
+                      uint64_t* payload_len, uint32_t* err, void* workspace,
+                      uint64_t workspace_bytes, void* stream);
+
+/* ---- decode every stage's rANS blob (latec/bitstream.py:288-344
+ *      unpack_stage with latec/rans.py:501-535 / 581-616) into codes.
+ *      words: device u32 array holding the blobs (stage t at blob_off);
+ *      chunk_range: device u64 pairs (start, end) of every lane-coder chunk
+ *      stream, as absolute word offsets in `words`, global chunk order.
+ *      err bits: 4 read past a chunk, 8 bad final state, 16 compat stream. */
+uint64_t latec_rans_decode_workspace_bytes(int32_t n_stages);
+int latec_rans_decode(const latec_rans_stage* stages, int32_t n_stages, uint32_t total_chunks,
+                      const uint32_t* words, const uint64_t* chunk_range, const uint8_t* levels,
+                      uint16_t* codes, uint32_t* err, void* workspace, uint64_t workspace_bytes,
+                      void* stream);
+
+/* Library version string. */
+const char* latec_version(void);
+
+/* Number of CUDA kernel launches this library has issued in this process. */
+uint64_t latec_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LATEC_B200_H */

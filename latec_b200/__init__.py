@@ -1,0 +1,13 @@
+"""LATEC on NVIDIA B200: error-bounded progressive compression with CUDA kernels.
+
+Drop-in for the reference package's public API (``latec/__init__.py``):
+``compress``, ``decompress``, ``InterpPredictor`` and the learned
+``GNNCodec``. The compute runs in ``liblatec_b200.so`` (sm_100a); there is no
+CPU fallback.
+"""
+
+from .codec import compress, decompress
+from .predictor import InterpPredictor
+
+__all__ = ["compress", "decompress", "InterpPredictor"]
+__version__ = "0.1.0"

@@ -1,0 +1,118 @@
+"""ctypes binding of ``liblatec_b200.so`` (the C ABI in ``include/latec_b200.h``).
+
+There is no CPU fallback: importing the compute entry points on a machine
+without the built library or without a CUDA device raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblatec_b200.so")
+
+LATEC_OK = 0
+ERRORS = {
+    -1: (ValueError, "invalid argument"),
+    -2: (RuntimeError, "CUDA error"),
+    -3: (NotImplementedError, "unsupported configuration"),
+    -4: (ValueError, "malformed stream"),
+    -5: (RuntimeError, "workspace too small"),
+    -6: (RuntimeError, "internal error"),
+}
+F32, F64 = 1, 2
+RANS_LANES, RANS_COMPAT = 0, 1
+
+U32, U64, I32, P, D = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_double
+
+
+class QuantParams(ctypes.Structure):
+    _fields_ = [("dtype", I32), ("channels", I32), ("radius", I32), ("order", I32),
+                ("center", I32), ("end_mode", I32), ("round_output", I32), ("reserved", I32)]
+
+
+class StageStats(ctypes.Structure):
+    _fields_ = [("n_out", U32), ("maxq", U32), ("pad0", U32), ("pad1", U32),
+                ("stats", D * 5)]
+
+
+class RansStage(ctypes.Structure):
+    _fields_ = [("codes_off", U64), ("out_off", U64), ("enc", U64), ("cdf", U64), ("bucket", U64),
+                ("scratch_off", U64), ("blob_off", U64), ("rec_off", U64), ("framed_hi", U64),
+                ("n", U32), ("K", U32), ("n_chunks", U32), ("chunk0", U32), ("alphabet", U32),
+                ("kexp", I32), ("radius", I32), ("mode", I32), ("per_point", I32),
+                ("blob_words", U32), ("n_out", U32), ("pad", U32)]
+
+
+# Every symbol the header declares, with (restype, argtypes).
+SIGNATURES = {
+    "latec_version": (ctypes.c_char_p, []),
+    "latec_launch_count": (U64, []),
+    "latec_plan_create": (ctypes.c_int, [P, I32, I32, I32, I32, ctypes.POINTER(P)]),
+    "latec_plan_destroy": (ctypes.c_int, [P]),
+    "latec_plan_num_stages": (ctypes.c_int, [P]),
+    "latec_plan_stage_info": (ctypes.c_int, [P, I32, ctypes.POINTER(U64), ctypes.POINTER(I32),
+                                             ctypes.POINTER(I32), ctypes.POINTER(I32)]),
+    "latec_plan_stage_flat": (ctypes.c_int, [P, I32, U64, U64, P]),
+    "latec_stage_workspace_bytes": (U64, [P, I32, I32]),
+    "latec_flat_workspace_bytes": (U64, [U64, I32]),
+    "latec_encode_stages": (ctypes.c_int, [P, ctypes.POINTER(QuantParams), P, P, P, P, P, P, P,
+                                           P, P, U64, P]),
+    "latec_interp_predict_stage": (ctypes.c_int, [P, I32, ctypes.POINTER(QuantParams), P, P, P]),
+    "latec_quantize": (ctypes.c_int, [ctypes.POINTER(QuantParams), D, U64, P, P, P, P, P, P, P,
+                                      P, P, U64, P]),
+    "latec_decode_stages": (ctypes.c_int, [P, ctypes.POINTER(QuantParams), P, P, P, P, P, P, P,
+                                           P, U64, P]),
+    "latec_rans_build_tables": (ctypes.c_int, [P, I32, I32, P, P, P]),
+    "latec_rans_encode_workspace_bytes": (U64, [P, I32]),
+    "latec_rans_encode": (ctypes.c_int, [P, I32, P, P, P, P, I32, P, U64, P, P, P, U64, P]),
+    "latec_rans_decode_workspace_bytes": (U64, [I32]),
+    "latec_rans_decode": (ctypes.c_int, [P, I32, U32, P, P, P, P, P, P, U64, P]),
+}
+
+_lib = None
+
+
+def load(require_gpu: bool = True):
+    """Load the CUDA library; raise if it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `make -C latec_b200/csrc` "
+                "(the LATEC B200 codec has no CPU fallback)")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    if require_gpu:
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("the LATEC B200 codec needs a CUDA device (no CPU fallback)")
+    return _lib
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != LATEC_OK:
+        exc, msg = ERRORS.get(rc, (RuntimeError, f"error {rc}"))
+        raise exc(f"{what}: {msg} (code {rc})" if what else f"{msg} (code {rc})")
+
+
+def ptr(t) -> int:
+    """Device (or host) address of a tensor / array, 0 for None."""
+    if t is None:
+        return 0
+    if hasattr(t, "data_ptr"):
+        return t.data_ptr()
+    return t.ctypes.data
+
+
+def stream_ptr(stream=None) -> int:
+    import torch
+
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream

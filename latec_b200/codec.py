@@ -1,0 +1,644 @@
+"""Closed-loop LATEC codec on the GPU: ``compress`` / ``decompress``.
+
+Same public signatures, stream container, per-stage statistics and error
+behaviour as the reference driver (``latec/codec.py:45-322``); the stage loop
+(``latec/codec.py:384-510``) runs as CUDA kernels through the C ABI:
+
+* encode: one fused predict + quantize + reconstruct kernel per stage writes
+  codes, the reconstruction, outliers (compacted in scan order) and the
+  stage's symbol histogram; the host fits the stage-constant rANS model from
+  the histogram (the reference's float32 fit), then one launch entropy-codes
+  every stage and assembles the stage records on the device;
+* decode: one launch rANS-decodes every stage's codes, then one predict +
+  dequantize kernel per stage rebuilds the field.
+
+Entropy back ends: ``entropy="native"`` (default) writes the 32-lane
+interleaved rANS blobs and a raw-block zstd frame (flag ``FLAG_LANES``);
+``entropy="compat"`` writes the reference's own single-stack rANS stream,
+literal-zstd stages and a level-``zstd_level`` zstd frame, which the
+reference's ``decompress`` reads.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import struct
+import time
+
+import numpy as np
+
+from . import _lib, bitstream, levels, rans_model
+from .bitstream import (DTYPE_CODES, DTYPE_IDS, END_MODE_SHIFT, FLAG_CUBIC, FLAG_INTERP,
+                        FLAG_LANES, FLAG_RANS, Header)
+
+END_MODE_MAX = 3
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _is_tensor(x):
+    try:
+        import torch
+
+        return isinstance(x, torch.Tensor)
+    except Exception:  # pragma: no cover
+        return False
+
+
+def _np_dtype(x):
+    if _is_tensor(x):
+        torch = _torch()
+        m = {torch.uint8: np.uint8, torch.float32: np.float32, torch.float64: np.float64,
+             torch.float16: np.float16, torch.int16: np.int16, torch.int32: np.int32,
+             torch.int64: np.int64, torch.bfloat16: None}
+        dt = m.get(x.dtype)
+        return np.dtype(dt) if dt is not None else None
+    return np.dtype(x.dtype)
+
+
+def _prepare(img, device):
+    """Shape normalisation of ``latec/codec.py:72-91`` plus float64; returns the
+    channel-first device field and its description."""
+    torch = _torch()
+    if not _is_tensor(img):
+        img = np.asarray(img)
+    ndim = img.ndim
+    shape = tuple(int(n) for n in img.shape)
+    is_image = ndim <= 2 or (ndim == 3 and shape[-1] in (1, 3))
+    dt = _np_dtype(img)
+    if dt is None or dt not in DTYPE_IDS:
+        raise KeyError(dt)
+    src = DTYPE_IDS[dt]
+    if not is_image:
+        spatial, c = shape, 1
+    elif ndim == 2:
+        spatial, c = shape, 1
+    elif ndim == 3:
+        spatial, c = shape[:-1], shape[-1]
+    else:  # 0-D / 1-D input: the reference's image branch leaves no spatial axis
+        spatial, c = shape[:-1], 1
+    if len(spatial) < 1:
+        raise ValueError("shape must have at least one axis")
+    ft = torch.float64 if src == 2 else torch.float32
+    t = img if _is_tensor(img) else torch.from_numpy(np.ascontiguousarray(img))
+    t = t.to(device=device, non_blocking=True)
+    t = t.to(ft)
+    if is_image and ndim == 3:
+        t = t.movedim(-1, 0)
+    else:
+        t = t.reshape((1,) + tuple(spatial))
+    return t.contiguous(), tuple(spatial), c, src
+
+
+class _Buffers:
+    """Device buffers of one compress/decompress call, reused across tune candidates."""
+
+    def __init__(self, plan, c, dtype_id, device):
+        torch = _torch()
+        self.torch = torch
+        self.plan = plan
+        self.c = c
+        self.elem = 8 if dtype_id == 2 else 4
+        self.ldtype = _lib.F64 if dtype_id == 2 else _lib.F32
+        self.device = device
+        self.items = [n * c for n in plan.counts]
+        self.offsets = np.concatenate([[0], np.cumsum(self.items)]).astype(np.int64)
+        self.total = int(self.offsets[-1])
+        self.segs = [-(-n // rans_model.SEG) for n in self.items]
+        self.seg_off = np.concatenate([[0], np.cumsum(self.segs)]).astype(np.int64)
+        ns = len(plan)
+        self.codes = torch.empty(max(self.total, 1), dtype=torch.int16, device=device)
+        self.outliers = torch.empty(max(self.total, 1) * self.elem, dtype=torch.uint8, device=device)
+        self.stats = torch.empty(ns * ctypes.sizeof(_lib.StageStats), dtype=torch.uint8, device=device)
+        self.hist_seg = torch.empty(max(int(self.seg_off[-1]), 1) * 2 * rans_model.HWIN,
+                                    dtype=torch.int32, device=device)
+        self.hist_total = torch.empty(ns * 65536, dtype=torch.int32, device=device)
+        lib = _lib.load()
+        wsb = lib.latec_stage_workspace_bytes(plan.handle, c, self.ldtype)
+        self.ws = torch.empty(max(int(wsb), 1), dtype=torch.uint8, device=device)
+        self.err = torch.zeros(2, dtype=torch.int64, device=device)
+
+
+def _qparams(dtype_id, c, radius, order, center, end_mode, round_output):
+    return _lib.QuantParams(dtype=_lib.F64 if dtype_id == 2 else _lib.F32, channels=c,
+                            radius=int(radius), order=1 if order == "cubic" else 0,
+                            center=int(center), end_mode=int(end_mode),
+                            round_output=int(bool(round_output)), reserved=0)
+
+
+def _stats_from_device(buf, ns):
+    raw = buf.stats.cpu().numpy().tobytes()
+    arr = (_lib.StageStats * ns).from_buffer_copy(raw)
+    return arr
+
+
+def _check_radius(radius):
+    if not 1 <= int(radius) <= 1 << 15:
+        raise NotImplementedError(
+            f"the CUDA quantizer supports radius in [1, 32768] (16-bit codes); got {radius}")
+
+
+class _Encoder:
+    """One compress call's GPU state: the field, the plan and the buffers."""
+
+    def __init__(self, field, spatial, c, src, levels_, anchor_stride, anchor_block, radius,
+                 order, entropy, zstd_level, device):
+        self.field, self.spatial, self.c, self.src = field, spatial, c, src
+        self.plan = levels.plan_for(spatial, levels_, anchor_stride, anchor_block)
+        self.radius, self.order, self.entropy, self.zstd_level = radius, order, entropy, zstd_level
+        self.device = device
+        self.buf = _Buffers(self.plan, c, src, device)
+        self.mode = _lib.RANS_LANES if entropy == "native" else _lib.RANS_COMPAT
+        self.lib = _lib.load()
+
+    def encode(self, ebs, center, end_mode, recon):
+        """Run every stage; return (payload uint8 array, per-stage stats dict)."""
+        torch = _torch()
+        lib, b, plan = self.lib, self.buf, self.plan
+        ns = len(plan)
+        prm = _qparams(self.src, self.c, self.radius, self.order, center, end_mode,
+                       self.src == 0)
+        eb_arr = (ctypes.c_double * ns)(*[float(e) for e in ebs])
+        stream = _lib.stream_ptr()
+        t0 = time.perf_counter()
+        recon.zero_()
+        _lib.check(lib.latec_encode_stages(
+            plan.handle, ctypes.byref(prm), eb_arr, self.field.data_ptr(), recon.data_ptr(),
+            b.codes.data_ptr(), b.outliers.data_ptr(), b.stats.data_ptr(), b.hist_seg.data_ptr(),
+            b.hist_total.data_ptr(), b.ws.data_ptr(), b.ws.numel(), stream), "latec_encode_stages")
+        st = _stats_from_device(b, ns)
+        hist_seg = b.hist_seg.cpu().numpy().view(np.uint32).reshape(-1, 2 * rans_model.HWIN)
+        t1 = time.perf_counter()
+        # ---- host model fit per stage (the reference's float32 histogram fit)
+        fits = []
+        need_total = [t for t in range(ns) if st[t].maxq >= rans_model.HWIN]
+        totals = {}
+        if need_total:
+            idx = torch.tensor(need_total, device=self.device)
+            rows = b.hist_total.view(ns, 65536)[idx].cpu().numpy().view(np.uint32)
+            totals = {t: rows[i] for i, t in enumerate(need_total)}
+        for t in range(ns):
+            n = b.items[t]
+            if n == 0:
+                fits.append((1, 0, 0, 0, 0.0))
+                continue
+            kexp = rans_model.kexp_from_maxq(st[t].maxq)
+            if kexp > 15:
+                raise ValueError("rANS coder window does not fit the stage frame")
+            seg = hist_seg[b.seg_off[t]:b.seg_off[t + 1]]
+            hist = rans_model.stage_hist_f32(n, kexp, self.radius, seg, totals.get(t))
+            level, shape, owx, bits = rans_model.fit_const_level(hist, n, kexp)
+            fits.append((kexp, level, shape, owx, bits))
+        # ---- entropy stage on the device
+        stages = (_lib.RansStage * ns)()
+        keep = []
+        for t in range(ns):
+            kexp, level, shape, owx, bits = fits[t]
+            d = stages[t]
+            d.codes_off = int(b.offsets[t])
+            d.out_off = int(b.offsets[t])
+            d.n = b.items[t]
+            d.kexp = kexp
+            d.radius = int(self.radius)
+            d.mode = self.mode
+            d.per_point = 0
+            d.framed_hi = bitstream.pack_frame(0, kexp, shape, level, owx, False)
+            d.alphabet = 1 << (kexp + 1)
+            if d.n:
+                cdf, enc, bucket, alphabet = rans_model.device_tables.get(
+                    self.mode, kexp, shape, owx, level, self.device)
+                keep.append((cdf, enc, bucket))
+                d.cdf, d.enc, d.bucket = cdf.data_ptr(), enc.data_ptr(), bucket.data_ptr()
+                d.K = rans_model.lanes_K(d.n, bits) if self.mode == _lib.RANS_LANES else 0
+        wsb = lib.latec_rans_encode_workspace_bytes(stages, ns)
+        ws = torch.empty(max(int(wsb), 1), dtype=torch.uint8, device=self.device)
+        cap = 0
+        for t in range(ns):
+            d = stages[t]
+            cap += 16 + 4 * (1 + 65 * d.n_chunks + d.n + 2) + b.elem * b.items[t]
+        cap = (cap + 15) // 16 * 16
+        payload = torch.empty(cap, dtype=torch.uint8, device=self.device)
+        plen = torch.zeros(1, dtype=torch.int64, device=self.device)
+        err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        _lib.check(lib.latec_rans_encode(
+            stages, ns, b.codes.data_ptr(), None, b.stats.data_ptr(), b.outliers.data_ptr(),
+            b.elem, payload.data_ptr(), cap, plen.data_ptr(), err.data_ptr(), ws.data_ptr(),
+            ws.numel(), stream), "latec_rans_encode")
+        n_bytes = int(plen.item())
+        e = int(err.item())
+        if e:
+            raise RuntimeError(f"entropy coder reported error bits {e:#x}")
+        host = payload[:n_bytes].cpu().numpy()
+        t2 = time.perf_counter()
+        if self.mode == _lib.RANS_COMPAT:
+            host = self._compat_literals(host, fits, st)
+        del keep
+        rec_bytes = self._record_sizes(host, ns)
+        stage = dict(
+            stage_codes=[int(v) for v in b.items],
+            stage_outliers=[int(st[t].n_out) for t in range(ns)],
+            stage_payload_bytes=rec_bytes,
+            stage_model_bits=[0.0] * ns,
+            stage_pred_sae=[float(st[t].stats[0]) for t in range(ns)],
+            stage_pred_sse=[float(st[t].stats[1]) for t in range(ns)],
+            stage_recon_sae=[float(st[t].stats[2]) for t in range(ns)],
+            stage_recon_sse=[float(st[t].stats[3]) for t in range(ns)],
+            stage_recon_max=[float(st[t].stats[4]) for t in range(ns)],
+            predict_s=t1 - t0, quantize_s=0.0, entropy_s=t2 - t1,
+            outliers=int(sum(int(st[t].n_out) for t in range(ns))),
+            stage_fit=fits,
+        )
+        return host, stage
+
+    def _record_sizes(self, payload, ns):
+        out, off = [], 0
+        for _ in range(ns):
+            n, word = struct.unpack_from("<IQ", payload, off)
+            hlen = word & ((1 << 45) - 1)
+            (n_out,) = struct.unpack_from("<I", payload, off + 12 + hlen)
+            size = 16 + hlen + self.buf.elem * n_out
+            out.append(size)
+            off += size
+        return out
+
+    def _compat_literals(self, payload, fits, st):
+        """Reference back-end choice for large stages (``latec/bitstream.py:203-219``):
+        the narrowed symbols deflated by zstd replace the rANS blob when a
+        level-1 scout and then the full-level pass beat the model's bits."""
+        b = self.buf
+        parts, off = [], 0
+        for t in range(len(self.plan)):
+            n, word = struct.unpack_from("<IQ", payload, off)
+            hlen = word & ((1 << 45) - 1)
+            (n_out,) = struct.unpack_from("<I", payload, off + 12 + hlen)
+            size = 16 + hlen + b.elem * n_out
+            rec = payload[off:off + size]
+            kexp, level, shape, owx, bits = fits[t]
+            if n >= rans_model.LITERAL_MIN:
+                codes = b.codes[b.offsets[t]:b.offsets[t + 1]].cpu().numpy().view(np.uint16)
+                syms = rans_model.narrow(codes, self.radius, kexp).astype(
+                    rans_model.literal_dtype(kexp)).tobytes()
+                z = bitstream.zstd()
+                scout = z.compress(syms, 1)
+                if len(scout) * rans_model.LITERAL_SCOUT_SLACK < bits / 8.0:
+                    blob = z.compress(syms, self.zstd_level)
+                    if len(blob) * 8.0 < bits:
+                        head = struct.pack("<IQ", n, bitstream.pack_frame(
+                            len(blob), kexp, shape, level, owx, True))
+                        tail = rec[12 + hlen:].tobytes()
+                        rec = np.frombuffer(head + blob + tail, np.uint8)
+            parts.append(np.asarray(rec, np.uint8))
+            off += size
+        return np.concatenate(parts) if parts else np.zeros(0, np.uint8)
+
+
+def _finalize(canvas, src_dtype, channels, as_numpy=True):
+    """``latec/codec.py:513-524``: (C, *S) -> (*S, C) in the source dtype."""
+    torch = _torch()
+    out = canvas.movedim(0, -1)
+    dt = DTYPE_CODES[src_dtype]
+    if np.issubdtype(dt, np.integer):
+        info = np.iinfo(dt)
+        out = torch.clamp(torch.round(out), info.min, info.max).to(torch.uint8)
+    elif dt == np.float64:
+        out = out.to(torch.float64)
+    else:
+        out = out.to(torch.float32)
+    if channels == 1:
+        out = out[..., 0]
+    if as_numpy:
+        return out.contiguous().cpu().numpy()
+    return out.contiguous()
+
+
+def _is_gpu_interp(predictor):
+    return getattr(predictor, "_latec_gpu_interp", False)
+
+
+def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, radius=1 << 15,
+             zstd_level=9, eb_ratio=None, tune="fast", tune_size_slack=1.05, verbose=False, *,
+             entropy="native", device=None, recon="auto"):
+    """Compress an image or an arbitrary-rank scalar field; returns ``(stream, stats)``.
+
+    Mirrors ``latec/codec.py:45-285``. ``img`` may be a NumPy array or a torch
+    tensor (host or CUDA). Extra keyword-only options: ``entropy`` ("native" or
+    "compat"), ``device`` (CUDA device; default the current one) and ``recon``
+    ("auto": ``stats["recon"]`` in the input's kind -- NumPy for NumPy input,
+    a device tensor for a CUDA tensor -- or "numpy", "device", "none").
+    """
+    torch = _torch()
+    _lib.load()
+    if entropy not in ("native", "compat"):
+        raise ValueError("entropy must be 'native' or 'compat'")
+    if not eb > 0:
+        raise ValueError(f"error bound must be > 0, got {eb}")
+    _check_radius(radius)
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    input_is_cuda = _is_tensor(img) and img.is_cuda
+    field, spatial, c, src = _prepare(img, dev)
+    if len(spatial) > 6:
+        raise NotImplementedError("the CUDA codec supports up to 6 spatial axes")
+    mm = torch.aminmax(field) if field.numel() else None
+    vmin, vmax = (float(mm.min.item()), float(mm.max.item())) if mm is not None else (0.0, 0.0)
+    if not (vmax > vmin):
+        if not (np.isnan(vmin) or np.isnan(vmax)):
+            vmax = vmin + 1.0
+    for name, val in (("levels", levels), ("anchor_stride", anchor_stride),
+                      ("anchor_block", anchor_block)):
+        got = getattr(predictor, name, val)
+        if got != val:
+            raise ValueError(f"predictor {name}={got} != compress {name}={val}")
+    if not _is_gpu_interp(predictor):
+        raise NotImplementedError(
+            "the CUDA codec runs InterpPredictor stages on the device; use GNNCodec for the "
+            "learned predictor")
+    from . import levels as _levels
+
+    _levels.check_plan(spatial, levels, anchor_stride, anchor_block)
+    order = predictor.order
+    enc = _Encoder(field, spatial, c, src, levels, anchor_stride, anchor_block, radius, order,
+                   entropy, zstd_level, dev)
+    flags = getattr(predictor, "stream_flag", 0)
+    if entropy == "native":
+        flags |= FLAG_LANES
+
+    def ebs_for(ratio):
+        return _levels.stage_ebs(spatial, levels, anchor_stride, anchor_block, eb, ratio)
+
+    def make_header(center, ratio, end_mode):
+        return Header(channels=c, src_dtype=src, spatial=tuple(spatial), eb=float(eb),
+                      levels=levels, anchor_stride=anchor_stride, anchor_block=anchor_block,
+                      radius=radius, max_radius=getattr(predictor, "max_radius", 0),
+                      agg_level=-1 if getattr(predictor, "agg_level", None) is None
+                      else int(predictor.agg_level),
+                      vmin=vmin, vmax=vmax,
+                      ckpt_hash=getattr(predictor, "checkpoint_hash", b"\0" * 16),
+                      flags=flags | (int(end_mode) << END_MODE_SHIFT), interp_center=center,
+                      eb_ratio=ratio)
+
+    if tune not in ("fast", "size", "rd"):
+        raise ValueError("tune must be 'fast', 'size', or 'rd'")
+    tunable = getattr(predictor, "tunable", False)
+    nd = len(spatial)
+    if getattr(predictor, "center", None) is None:
+        predictor.center = 1 if nd >= 4 else 0
+    if getattr(predictor, "end_mode", None) is None:
+        predictor.end_mode = 1
+    if eb_ratio is not None:
+        ratio_cands = [eb_ratio]
+    elif tunable and tune != "fast":
+        ratio_cands = [1.0, 0.9, 0.8, 0.7]
+    else:
+        ratio_cands = [getattr(predictor, "fast_eb_ratio", 1.0)]
+    sweep = tunable and tune != "fast" and eb_ratio is None
+    base_center = predictor.center
+    center_cands = [base_center] + ([x for x in (0, 1, 2) if x != base_center] if sweep else [])
+    base_end = predictor.end_mode
+    candidates = []
+    seen = set()
+
+    def run(ratio, center, end_mode):
+        rc = torch.empty_like(field)
+        payload, st = enc.encode(ebs_for(ratio), center, end_mode, rc)
+        header = make_header(center, ratio, end_mode)
+        t0 = time.perf_counter()
+        if entropy == "native":
+            body = bitstream.raw_zstd_frame(payload)
+        else:
+            body = np.frombuffer(bitstream.zstd().compress(payload, zstd_level), np.uint8)
+        stream = header.pack() + body.tobytes()
+        st["entropy_s"] += time.perf_counter() - t0
+        st["raw_payload_bytes"] = len(payload)
+        st["compressed_bytes"] = len(stream)
+        st["recon_sse"] = float(sum(st["stage_recon_sse"]))
+        candidates.append((len(stream), st["recon_sse"], ratio, center, end_mode, stream, rc, st))
+
+    def run_once(ratio, center, end_mode):
+        if (ratio, center, end_mode) not in seen:
+            seen.add((ratio, center, end_mode))
+            run(ratio, center, end_mode)
+
+    run_once(ratio_cands[0], base_center, base_end)
+    chosen_end = base_end
+    if sweep:
+        for em in range(END_MODE_MAX + 1):
+            run_once(ratio_cands[0], base_center, em)
+        chosen_end = min(candidates, key=lambda x: (x[0], x[1]))[4]
+    for ratio in ratio_cands:
+        for center in center_cands:
+            run_once(ratio, center, chosen_end)
+    if tune == "rd" and eb_ratio is None and tunable and len(candidates) > 1:
+        limit = min(x[0] for x in candidates) * tune_size_slack
+        best = min((x for x in candidates if x[0] <= limit),
+                   key=lambda x: (x[1], x[0], x[2], x[3], x[4]))
+    else:
+        best = min(candidates, key=lambda x: (x[0], x[1], x[2], x[3], x[4]))
+    _, _, ratio, center, end_mode, stream, canvas, stats = best
+    stats["tune_candidates"] = len(candidates)
+    stats["search_predict_s"] = sum(x[7]["predict_s"] for x in candidates)
+    stats["search_quantize_s"] = sum(x[7]["quantize_s"] for x in candidates)
+    stats["search_entropy_s"] = sum(x[7]["entropy_s"] for x in candidates)
+    predictor.center = center
+    predictor.end_mode = end_mode
+    stats["eb_ratio"] = ratio
+    stats["interp_center"] = center
+    stats["interp_end_mode"] = end_mode
+    stats["tune"] = tune
+    stats["tune_size_slack"] = tune_size_slack if (tune == "rd" and eb_ratio is None and tunable) else 1.0
+    stats["entropy"] = entropy
+    if verbose:
+        print(f"tuned: eb_ratio={ratio} center={center} end_mode={end_mode} "
+              f"compressed={len(stream)} bytes raw={stats['raw_payload_bytes']} bytes "
+              f"sse={stats['recon_sse']:.6g}")
+    mode = recon if recon != "auto" else ("device" if input_is_cuda else "numpy")
+    if mode == "none":
+        stats["recon"] = None
+    else:
+        stats["recon"] = _finalize(canvas, src, c, as_numpy=(mode == "numpy"))
+    nbytes = img.nbytes if not _is_tensor(img) else img.numel() * img.element_size()
+    stats["original_bytes"] = int(nbytes)
+    stats["ratio"] = nbytes / len(stream)
+    return stream, stats
+
+
+def _parse_records(payload, ns, elem):
+    recs, off = [], 0
+    for t in range(ns):
+        if off + 12 > len(payload):
+            raise ValueError("truncated stage record")
+        n, word = struct.unpack_from("<IQ", payload, off)
+        f = bitstream.unpack_frame(word)
+        blob = off + 12
+        if blob + f["hlen"] + 4 > len(payload):
+            raise ValueError("truncated stage record")
+        (n_out,) = struct.unpack_from("<I", payload, blob + f["hlen"])
+        out_at = blob + f["hlen"] + 4
+        end = out_at + elem * n_out
+        if end > len(payload):
+            raise ValueError("truncated stage record")
+        recs.append(dict(f, n=n, blob=blob, n_out=n_out, out_at=out_at))
+        off = end
+    if off != len(payload):
+        raise ValueError("trailing data after the last stage record")
+    return recs
+
+
+def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
+    """Decompress a LATEC stream (``latec/codec.py:288-322``). ``out="device"``
+    returns a CUDA tensor instead of a NumPy array."""
+    torch = _torch()
+    lib = _lib.load()
+    from . import levels as _levels
+    from .predictor import InterpPredictor
+
+    header = Header.unpack(stream)
+    payload = bitstream.read_body(memoryview(stream)[header.size:])
+    if header.flags & FLAG_RANS:
+        raise NotImplementedError("per-point scale streams are decoded by GNNCodec.uncompress")
+    if predictor_factory is None:
+        if header.flags & FLAG_INTERP:
+            predictor_factory = lambda hdr: InterpPredictor(  # noqa: E731
+                "cubic" if hdr.flags & FLAG_CUBIC else "linear", hdr.levels, hdr.anchor_stride,
+                hdr.anchor_block)
+        else:
+            raise ValueError("stream needs a predictor_factory")
+    predictor = predictor_factory(header)
+    if hasattr(predictor, "center"):
+        predictor.center = header.interp_center
+    if hasattr(predictor, "end_mode"):
+        predictor.end_mode = (header.flags >> END_MODE_SHIFT) & END_MODE_MAX
+    if not _is_gpu_interp(predictor):
+        raise NotImplementedError("the CUDA codec decodes InterpPredictor streams")
+    if header.src_dtype not in DTYPE_CODES:
+        raise KeyError(header.src_dtype)
+    _check_radius(header.radius)
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    spatial, c = tuple(header.spatial), int(header.channels)
+    if c < 1:
+        raise ValueError("stream has no channels")
+    plan = _levels.plan_for(spatial, header.levels, header.anchor_stride, header.anchor_block)
+    ns = len(plan)
+    ebs = _levels.stage_ebs(spatial, header.levels, header.anchor_stride, header.anchor_block,
+                            header.eb, header.eb_ratio)
+    elem = 8 if header.src_dtype == 2 else 4
+    recs = _parse_records(payload, ns, elem)
+    mode = _lib.RANS_LANES if header.flags & FLAG_LANES else _lib.RANS_COMPAT
+    items = [n * c for n in plan.counts]
+    offsets = np.concatenate([[0], np.cumsum(items)]).astype(np.int64)
+    for t in range(ns):
+        if recs[t]["n"] != items[t]:
+            raise ValueError("stage code count mismatch")
+        if not recs[t]["kexp"]:
+            raise ValueError("rANS stage record has no coder window")
+    aligned = all(r["blob"] % 4 == 0 for r in recs if not r["literal"])
+    pad = (-len(payload)) % 4
+    pbuf = np.concatenate([payload, np.zeros(pad, np.uint8)]) if pad else payload
+    if len(pbuf) == 0:
+        pbuf = np.zeros(4, np.uint8)
+    pay_dev = torch.from_numpy(np.ascontiguousarray(pbuf)).to(dev)
+    if aligned:
+        words_host = pbuf.view(np.uint32)
+        words_dev = pay_dev
+        blob_word = [r["blob"] // 4 for r in recs]
+    else:  # literal stages broke the word alignment: gather the rANS blobs
+        pieces, blob_word, at = [], [], 0
+        for r in recs:
+            nw = 0 if r["literal"] else -(-r["hlen"] // 4)
+            pieces.append(payload[r["blob"]:r["blob"] + 4 * nw])
+            blob_word.append(at)
+            at += nw
+        words_host = np.concatenate(pieces + [np.zeros(4, np.uint8)]).view(np.uint32)
+        words_dev = torch.from_numpy(words_host.view(np.uint8).copy()).to(dev)
+    stages = (_lib.RansStage * ns)()
+    keep, ranges, literal_codes = [], [], {}
+    chunk = 0
+    for t in range(ns):
+        r, d = recs[t], stages[t]
+        d.codes_off = int(offsets[t])
+        d.n = r["n"]
+        d.kexp, d.radius, d.mode = r["kexp"], int(header.radius), mode
+        d.alphabet = 1 << (r["kexp"] + 1)
+        d.chunk0 = chunk
+        if r["n"] == 0:
+            if r["hlen"]:
+                raise ValueError("non-empty rANS blob for an empty stage")
+            continue
+        if r["literal"]:
+            syms = np.frombuffer(bitstream.zstd().decompress_into(
+                payload[r["blob"]:r["blob"] + r["hlen"]]).tobytes(),
+                rans_model.literal_dtype(r["kexp"]), count=r["n"])
+            literal_codes[t] = rans_model.widen(syms, header.radius, r["kexp"]).astype(np.uint16)
+            d.mode = mode
+            d.n = 0
+            continue
+        if r["hlen"] % 4:
+            raise ValueError("rANS payload is not aligned to 32-bit words")
+        cdf, enc, bucket, _ = rans_model.device_tables.get(mode, r["kexp"], r["shape"], r["owx"],
+                                                           r["level"], dev)
+        keep.append((cdf, enc, bucket))
+        d.cdf, d.enc, d.bucket = cdf.data_ptr(), enc.data_ptr(), bucket.data_ptr()
+        d.blob_off = blob_word[t]
+        d.blob_words = r["hlen"] // 4
+        if mode == _lib.RANS_LANES:
+            w0 = blob_word[t]
+            wh = words_host
+            if d.blob_words < 1:
+                raise ValueError("truncated lane-coder blob")
+            K = int(wh[w0])
+            if K < 1:
+                raise ValueError("lane coder blob has K = 0")
+            nc = -(-r["n"] // (32 * K))
+            if 1 + nc > d.blob_words:
+                raise ValueError("truncated lane-coder chunk table")
+            cw = wh[w0 + 1:w0 + 1 + nc].astype(np.uint64)
+            starts = w0 + 1 + nc + np.concatenate([[0], np.cumsum(cw)[:-1]]).astype(np.uint64)
+            ends = starts + cw
+            if int(ends[-1]) != w0 + d.blob_words:
+                raise ValueError("lane-coder chunk table does not match the blob length")
+            ranges.append(np.stack([starts, ends], 1).reshape(-1))
+            d.K, d.n_chunks = K, nc
+            chunk += nc
+    total_chunks = chunk
+    rng_dev = torch.from_numpy(np.concatenate(ranges).astype(np.uint64).view(np.int64)).to(dev) \
+        if ranges else None
+    codes = torch.empty(max(int(offsets[-1]), 1), dtype=torch.int16, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    wsb = lib.latec_rans_decode_workspace_bytes(ns)
+    ws = torch.empty(int(wsb), dtype=torch.uint8, device=dev)
+    stream_p = _lib.stream_ptr()
+    _lib.check(lib.latec_rans_decode(stages, ns, total_chunks, words_dev.data_ptr(),
+                                     rng_dev.data_ptr() if rng_dev is not None else None, None,
+                                     codes.data_ptr(), err.data_ptr(), ws.data_ptr(), ws.numel(),
+                                     stream_p), "latec_rans_decode")
+    for t, lc in literal_codes.items():
+        codes[int(offsets[t]):int(offsets[t + 1])].copy_(torch.from_numpy(lc.view(np.int16)).to(dev))
+    del keep
+    ldt = _lib.F64 if header.src_dtype == 2 else _lib.F32
+    prm = _qparams(header.src_dtype, c, header.radius,
+                   "cubic" if predictor.order == "cubic" else "linear", predictor.center,
+                   predictor.end_mode, header.src_dtype == 0)
+    ft = torch.float64 if header.src_dtype == 2 else torch.float32
+    recon = torch.zeros((c,) + spatial, dtype=ft, device=dev)
+    eb_arr = (ctypes.c_double * ns)(*[float(e) for e in ebs])
+    out_off = (ctypes.c_uint64 * ns)(*[r["out_at"] for r in recs])
+    n_out = (ctypes.c_uint32 * ns)(*[r["n_out"] for r in recs])
+    wsb2 = lib.latec_stage_workspace_bytes(plan.handle, c, ldt)
+    ws2 = torch.empty(max(int(wsb2), 1), dtype=torch.uint8, device=dev)
+    _lib.check(lib.latec_decode_stages(plan.handle, ctypes.byref(prm), eb_arr, codes.data_ptr(),
+                                       pay_dev.data_ptr(), out_off, n_out, recon.data_ptr(),
+                                       err.data_ptr(), ws2.data_ptr(), ws2.numel(), stream_p),
+               "latec_decode_stages")
+    e = int(err.item())
+    if e & 1:
+        raise ValueError("outlier count mismatch")
+    if e & (4 | 8):
+        raise ValueError("trailing data in rANS payload")
+    if e & 16:
+        raise ValueError("malformed rANS payload")
+    if e:
+        raise ValueError(f"malformed stream (error bits {e:#x})")
+    return _finalize(recon, header.src_dtype, c, as_numpy=(out == "numpy"))

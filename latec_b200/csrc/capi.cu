@@ -1,0 +1,404 @@
+// extern "C" entry points of liblatec_b200 (declared in include/latec_b200.h).
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "interp_kernels.cuh"
+#include "plan.h"
+#include "rans_kernels.cuh"
+
+#include <atomic>
+
+using namespace latec;
+
+static std::atomic<unsigned long long> g_launches{0};
+namespace latec {
+void count_launches(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+}  // namespace latec
+
+static_assert(sizeof(latec_stage_stats) == sizeof(StageAcc), "stats layout");
+static_assert(sizeof(latec_rans_stage) == sizeof(RansStageDesc), "rans stage layout");
+static_assert(sizeof(EncSym) == 24, "encoder symbol layout");
+
+namespace {
+
+constexpr uint64_t ALIGN = 256;
+inline uint64_t align_up(uint64_t v) { return (v + ALIGN - 1) & ~(ALIGN - 1); }
+
+struct Carve {
+    uint8_t* base;
+    uint64_t off = 0;
+    template <typename T>
+    T* take(uint64_t count) {
+        T* p = base ? (T*)(base + off) : nullptr;
+        off = align_up(off + count * sizeof(T));
+        return p;
+    }
+};
+
+inline int elem_of(int dtype) { return dtype == LATEC_F64 ? 8 : 4; }
+
+bool valid_params(const latec_quant_params* p) {
+    if (!p) return false;
+    if (p->dtype != LATEC_F32 && p->dtype != LATEC_F64) return false;
+    if (p->channels < 1 || p->radius < 1 || p->radius > 32768) return false;
+    if (p->order < 0 || p->order > 1 || p->center < 0 || p->center > 2) return false;
+    if (p->end_mode < 0 || p->end_mode > 3) return false;
+    return true;
+}
+
+bool make_q(const latec_quant_params* p, double eb, uint64_t points, QParams& q) {
+    if (!(eb > 0.0)) return false;
+    q.w = 2.0 * eb;
+    const double inv = 1.0 / q.w;
+    q.inv_w = (std::isfinite(inv) && q.w > 0x1p-1000 && std::isfinite(q.w)) ? inv : 0.0;
+    q.eb = eb;
+    q.eb_f = (float)eb;
+    q.radius = p->radius;
+    q.order = p->order;
+    q.center = p->center;
+    q.end_mode = p->end_mode;
+    q.round_output = p->round_output;
+    q.channels = p->channels;
+    q.points = points;
+    return true;
+}
+
+struct StageWs {
+    void* staging;
+    uint32_t* tile_cnt;
+    uint32_t* tile_off;
+    uint32_t* total;
+    double* partials;
+};
+
+uint64_t stage_ws(const latec_plan* plan, uint64_t max_items_override, int elem, StageWs* out,
+                  void* base) {
+    uint64_t max_items = max_items_override;
+    if (plan)
+        for (auto& d : plan->stages) max_items = d.n > max_items ? d.n : max_items;
+    Carve c{(uint8_t*)base};
+    StageWs w;
+    w.staging = c.take<uint8_t>(max_items * elem);
+    w.tile_cnt = c.take<uint32_t>(n_tiles(max_items) + 1);
+    w.tile_off = c.take<uint32_t>(n_tiles(max_items) + 1);
+    w.total = c.take<uint32_t>(4);
+    w.partials = c.take<double>((uint64_t)n_blocks(max_items) * 5 + 5);
+    if (out) *out = w;
+    return c.off;
+}
+
+__global__ void k_check_count(const uint32_t* total, uint32_t expected, uint32_t* err) {
+    if (threadIdx.x == 0 && *total != expected) atomicOr(err, 1u);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* latec_version(void) { return "latec_b200 0.1 (sm_100a)"; }
+
+uint64_t latec_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int latec_plan_create(const uint32_t* shape, int32_t ndim, int32_t levels, int32_t anchor_stride,
+                      int32_t anchor_block, latec_plan** out) {
+    if (!shape || !out) return LATEC_ERR_ARG;
+    latec_plan* p = new (std::nothrow) latec_plan();
+    if (!p) return LATEC_ERR_INTERNAL;
+    const int rc = build_plan(*p, shape, ndim, levels, anchor_stride, anchor_block);
+    if (rc) {
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return LATEC_OK;
+}
+
+int latec_plan_destroy(latec_plan* plan) {
+    delete plan;
+    return LATEC_OK;
+}
+
+int latec_plan_num_stages(const latec_plan* plan) {
+    return plan ? (int)plan->stages.size() : LATEC_ERR_ARG;
+}
+
+int latec_plan_stage_info(const latec_plan* plan, int32_t stage, uint64_t* n_points,
+                          int32_t* stride, int32_t* weight, int32_t* axis) {
+    if (!plan || stage < 0 || stage >= (int)plan->stages.size()) return LATEC_ERR_ARG;
+    const StageDesc& d = plan->stages[stage];
+    if (n_points) *n_points = d.n;
+    if (stride) *stride = d.s;
+    if (weight) *weight = d.weight;
+    if (axis) *axis = d.axis;
+    return LATEC_OK;
+}
+
+int latec_plan_stage_flat(const latec_plan* plan, int32_t stage, uint64_t first, uint64_t count,
+                          int64_t* out_flat) {
+    if (!plan || stage < 0 || stage >= (int)plan->stages.size() || (count && !out_flat))
+        return LATEC_ERR_ARG;
+    const StageDesc& d = plan->stages[stage];
+    if (first + count > d.n) return LATEC_ERR_ARG;
+    int32_t coord[MAXD];
+    for (uint64_t i = 0; i < count; i++) out_flat[i] = stage_coords(d, (uint32_t)(first + i), coord);
+    return LATEC_OK;
+}
+
+uint64_t latec_stage_workspace_bytes(const latec_plan* plan, int32_t channels, int32_t dtype) {
+    if (!plan || channels < 1) return 0;
+    uint64_t m = 0;
+    for (auto& d : plan->stages) m = (uint64_t)d.n * channels > m ? (uint64_t)d.n * channels : m;
+    return stage_ws(nullptr, m, elem_of(dtype), nullptr, nullptr);
+}
+
+uint64_t latec_flat_workspace_bytes(uint64_t items, int32_t dtype) {
+    return stage_ws(nullptr, items, elem_of(dtype), nullptr, nullptr);
+}
+
+int latec_encode_stages(const latec_plan* plan, const latec_quant_params* prm,
+                        const double* stage_eb, const void* x, void* recon, uint16_t* codes,
+                        void* outliers, latec_stage_stats* stats, uint32_t* hist_seg,
+                        uint32_t* hist_total, void* workspace, uint64_t workspace_bytes,
+                        void* stream) {
+    if (!plan || !valid_params(prm) || !stage_eb || !x || !recon || !codes || !outliers ||
+        !stats || !hist_seg || !hist_total)
+        return LATEC_ERR_ARG;
+    const int C = prm->channels, elem = elem_of(prm->dtype);
+    const uint64_t need = latec_stage_workspace_bytes(plan, C, prm->dtype);
+    if (!workspace || workspace_bytes < need) return LATEC_ERR_WORKSPACE;
+    uint64_t m = 0;
+    for (auto& d : plan->stages) m = (uint64_t)d.n * C > m ? (uint64_t)d.n * C : m;
+    StageWs w;
+    stage_ws(nullptr, m, elem, &w, workspace);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int ns = (int)plan->stages.size();
+    uint64_t total_segs = 0;
+    for (auto& d : plan->stages) total_segs += n_segments((uint64_t)d.n * C);
+    if (cudaMemsetAsync(stats, 0, sizeof(latec_stage_stats) * ns, st) != cudaSuccess ||
+        cudaMemsetAsync(hist_seg, 0, sizeof(uint32_t) * HBINS * total_segs, st) != cudaSuccess ||
+        cudaMemsetAsync(hist_total, 0, sizeof(uint32_t) * 65536ull * ns, st) != cudaSuccess)
+        return LATEC_ERR_CUDA;
+    uint64_t off = 0, seg = 0;
+    for (int t = 0; t < ns; t++) {
+        const StageDesc& d = plan->stages[t];
+        const uint64_t items = (uint64_t)d.n * C;
+        QParams q;
+        if (!make_q(prm, stage_eb[t], plan->points, q)) return LATEC_ERR_ARG;
+        StageAcc* acc = (StageAcc*)(stats + t);
+        int rc = launch_interp_quant(d, q, prm->dtype, t == 0, x, recon, codes + off, w.staging,
+                                     w.tile_cnt, hist_total + 65536ull * t,
+                                     hist_seg + (uint64_t)HBINS * seg, acc, w.partials, st);
+        if (!rc) rc = launch_tile_scan(w.tile_cnt, n_tiles(items), w.tile_off, &acc->n_out, st);
+        if (!rc)
+            rc = launch_compact(codes + off, items, w.staging, elem, w.tile_cnt, w.tile_off,
+                                (uint8_t*)outliers + off * elem, st);
+        if (!rc) rc = launch_stats_reduce(w.partials, n_blocks(items), acc, st);
+        if (rc) return rc;
+        off += items;
+        seg += n_segments(items);
+    }
+    return LATEC_OK;
+}
+
+int latec_interp_predict_stage(const latec_plan* plan, int32_t stage,
+                               const latec_quant_params* prm, const void* recon, void* pred,
+                               void* stream) {
+    if (!plan || !valid_params(prm) || stage < 1 || stage >= (int)plan->stages.size() || !recon ||
+        !pred)
+        return LATEC_ERR_ARG;
+    QParams q;
+    make_q(prm, 1.0, plan->points, q);
+    return launch_interp_predict(plan->stages[stage], q, prm->dtype, recon, pred,
+                                 (cudaStream_t)stream);
+}
+
+int latec_quantize(const latec_quant_params* prm, double eb, uint64_t items, const void* x,
+                   const void* pred, uint16_t* codes, void* recon_out, void* outliers,
+                   latec_stage_stats* stats, uint32_t* hist_seg, uint32_t* hist_total,
+                   void* workspace, uint64_t workspace_bytes, void* stream) {
+    if (!valid_params(prm) || (items && (!x || !pred || !codes || !recon_out || !outliers)) ||
+        !stats || !hist_seg || !hist_total)
+        return LATEC_ERR_ARG;
+    const int elem = elem_of(prm->dtype);
+    if (!workspace || workspace_bytes < latec_flat_workspace_bytes(items, prm->dtype))
+        return LATEC_ERR_WORKSPACE;
+    StageWs w;
+    stage_ws(nullptr, items, elem, &w, workspace);
+    QParams q;
+    if (!make_q(prm, eb, items, q)) return LATEC_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemsetAsync(stats, 0, sizeof(latec_stage_stats), st) != cudaSuccess ||
+        cudaMemsetAsync(hist_seg, 0, sizeof(uint32_t) * HBINS * n_segments(items), st) !=
+            cudaSuccess ||
+        cudaMemsetAsync(hist_total, 0, sizeof(uint32_t) * 65536ull, st) != cudaSuccess)
+        return LATEC_ERR_CUDA;
+    StageAcc* acc = (StageAcc*)stats;
+    int rc = launch_quantize_flat(q, prm->dtype, items, x, pred, codes, w.staging, w.tile_cnt,
+                                  hist_total, hist_seg, acc, w.partials, recon_out, st);
+    if (!rc) rc = launch_tile_scan(w.tile_cnt, n_tiles(items), w.tile_off, &acc->n_out, st);
+    if (!rc)
+        rc = launch_compact(codes, items, w.staging, elem, w.tile_cnt, w.tile_off, outliers, st);
+    if (!rc) rc = launch_stats_reduce(w.partials, n_blocks(items), acc, st);
+    return rc;
+}
+
+int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
+                        const double* stage_eb, const uint16_t* codes, const void* outliers,
+                        const uint64_t* out_off, const uint32_t* n_out, void* recon,
+                        uint32_t* err, void* workspace, uint64_t workspace_bytes, void* stream) {
+    if (!plan || !valid_params(prm) || !stage_eb || !codes || !out_off || !n_out || !recon || !err)
+        return LATEC_ERR_ARG;
+    const int C = prm->channels, elem = elem_of(prm->dtype);
+    if (!workspace || workspace_bytes < latec_stage_workspace_bytes(plan, C, prm->dtype))
+        return LATEC_ERR_WORKSPACE;
+    uint64_t m = 0;
+    for (auto& d : plan->stages) m = (uint64_t)d.n * C > m ? (uint64_t)d.n * C : m;
+    StageWs w;
+    stage_ws(nullptr, m, elem, &w, workspace);
+    cudaStream_t st = (cudaStream_t)stream;
+    uint64_t off = 0;
+    for (int t = 0; t < (int)plan->stages.size(); t++) {
+        const StageDesc& d = plan->stages[t];
+        const uint64_t items = (uint64_t)d.n * C;
+        if (!items) continue;
+        QParams q;
+        if (!make_q(prm, stage_eb[t], plan->points, q)) return LATEC_ERR_ARG;
+        int rc = launch_count_zeros(codes + off, items, w.tile_cnt, st);
+        if (!rc) rc = launch_tile_scan(w.tile_cnt, n_tiles(items), w.tile_off, w.total, st);
+        if (!rc) {
+            k_check_count<<<1, 32, 0, st>>>(w.total, n_out[t], err);
+            count_launches(1);
+            rc = cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
+        }
+        if (!rc)
+            rc = launch_interp_dequant(d, q, prm->dtype, t == 0, codes + off,
+                                       outliers ? (const uint8_t*)outliers + out_off[t] : nullptr,
+                                       w.tile_off, n_out[t], recon, err, st);
+        if (rc) return rc;
+        off += items;
+    }
+    return LATEC_OK;
+}
+
+int latec_rans_build_tables(const uint32_t* cdf_rows, int32_t alphabet, int32_t rows, void* enc,
+                            uint16_t* bucket, void* stream) {
+    if (!cdf_rows || alphabet < 2 || alphabet > 65536 || rows < 1) return LATEC_ERR_ARG;
+    return launch_build_tables(cdf_rows, alphabet, rows, (EncSym*)enc, bucket,
+                               (cudaStream_t)stream);
+}
+
+static uint64_t rans_layout(latec_rans_stage* s, int n, uint64_t* scratch_words,
+                            uint32_t* total_chunks) {
+    uint64_t sw = 0;
+    uint32_t chunks = 0;
+    for (int t = 0; t < n; t++) {
+        latec_rans_stage& d = s[t];
+        d.scratch_off = sw;
+        d.chunk0 = chunks;
+        if (d.mode == LATEC_RANS_LANES) {
+            const uint64_t per = 32ull * (d.K ? d.K : 1);
+            d.n_chunks = d.n ? (uint32_t)((d.n + per - 1) / per) : 0;
+            chunks += d.n_chunks;
+            sw += (uint64_t)d.n_chunks * (64 + per);
+        } else {
+            d.n_chunks = 0;
+            sw += (uint64_t)d.n + 2;
+        }
+        sw = (sw + 63) & ~63ull;
+    }
+    *scratch_words = sw;
+    *total_chunks = chunks;
+    Carve c{nullptr};
+    c.take<RansStageDesc>(n);
+    c.take<uint32_t>(sw);
+    c.take<uint32_t>(chunks + 1);
+    c.take<uint32_t>(chunks + 1);
+    c.take<uint32_t>(n + 1);
+    return c.off;
+}
+
+uint64_t latec_rans_encode_workspace_bytes(latec_rans_stage* stages, int32_t n_stages) {
+    if (!stages || n_stages < 1) return 0;
+    uint64_t sw;
+    uint32_t tc;
+    return rans_layout(stages, n_stages, &sw, &tc);
+}
+
+int latec_rans_encode(latec_rans_stage* stages, int32_t n_stages, const uint16_t* codes,
+                      const uint8_t* levels, const latec_stage_stats* stats,
+                      const void* outliers, int32_t elem, uint8_t* payload, uint64_t payload_cap,
+                      uint64_t* payload_len, uint32_t* err, void* workspace,
+                      uint64_t workspace_bytes, void* stream) {
+    if (!stages || n_stages < 1 || !codes || !stats || !payload || !payload_len || !err ||
+        (elem != 4 && elem != 8))
+        return LATEC_ERR_ARG;
+    for (int t = 0; t < n_stages; t++) {
+        const latec_rans_stage& d = stages[t];
+        if (d.n && (!d.cdf || d.alphabet < 2 || d.alphabet > 65536 || d.kexp < 1 || d.kexp > 15))
+            return LATEC_ERR_ARG;
+        if (d.n && d.mode == LATEC_RANS_LANES && (!d.enc || d.K < 1)) return LATEC_ERR_ARG;
+        if (d.per_point && !levels) return LATEC_ERR_ARG;
+    }
+    uint64_t sw;
+    uint32_t tc;
+    const uint64_t need = rans_layout(stages, n_stages, &sw, &tc);
+    if (!workspace || workspace_bytes < need) return LATEC_ERR_WORKSPACE;
+    Carve c{(uint8_t*)workspace};
+    RansStageDesc* dst = c.take<RansStageDesc>(n_stages);
+    uint32_t* scratch = c.take<uint32_t>(sw);
+    uint32_t* chunk_words = c.take<uint32_t>(tc + 1);
+    uint32_t* chunk_off = c.take<uint32_t>(tc + 1);
+    uint32_t* stage_words = c.take<uint32_t>(n_stages + 1);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemcpyAsync(dst, stages, sizeof(RansStageDesc) * n_stages, cudaMemcpyHostToDevice, st) !=
+        cudaSuccess)
+        return LATEC_ERR_CUDA;
+    if (cudaMemsetAsync(stage_words, 0, sizeof(uint32_t) * (n_stages + 1), st) != cudaSuccess)
+        return LATEC_ERR_CUDA;
+    bool any_compat = false;
+    for (int t = 0; t < n_stages; t++) any_compat |= stages[t].mode == LATEC_RANS_COMPAT;
+    int rc = launch_lanes_encode(dst, n_stages, tc, codes, levels, scratch, chunk_words, err, st);
+    if (!rc && any_compat)
+        rc = launch_stack_encode(dst, n_stages, codes, levels, scratch, stage_words, err, st);
+    if (!rc)
+        rc = launch_assemble(dst, n_stages, tc, scratch, chunk_words, chunk_off, scratch,
+                             stage_words, (const StageAcc*)stats, (const uint8_t*)outliers, elem,
+                             payload, payload_cap, payload_len, err, st);
+    return rc;
+}
+
+uint64_t latec_rans_decode_workspace_bytes(int32_t n_stages) {
+    Carve c{nullptr};
+    c.take<RansStageDesc>(n_stages > 0 ? n_stages : 1);
+    return c.off;
+}
+
+int latec_rans_decode(const latec_rans_stage* stages, int32_t n_stages, uint32_t total_chunks,
+                      const uint32_t* words, const uint64_t* chunk_range, const uint8_t* levels,
+                      uint16_t* codes, uint32_t* err, void* workspace, uint64_t workspace_bytes,
+                      void* stream) {
+    if (!stages || n_stages < 1 || !codes || !err) return LATEC_ERR_ARG;
+    if (!workspace || workspace_bytes < latec_rans_decode_workspace_bytes(n_stages))
+        return LATEC_ERR_WORKSPACE;
+    bool any_compat = false;
+    for (int t = 0; t < n_stages; t++) {
+        const latec_rans_stage& d = stages[t];
+        if (d.n && (!d.cdf || !d.bucket || d.alphabet < 2 || d.alphabet > 65536)) return LATEC_ERR_ARG;
+        if (d.per_point && !levels) return LATEC_ERR_ARG;
+        any_compat |= d.mode == LATEC_RANS_COMPAT && d.n;
+    }
+    if (total_chunks && (!words || !chunk_range)) return LATEC_ERR_ARG;
+    Carve c{(uint8_t*)workspace};
+    RansStageDesc* dst = c.take<RansStageDesc>(n_stages);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemcpyAsync(dst, stages, sizeof(RansStageDesc) * n_stages, cudaMemcpyHostToDevice, st) !=
+        cudaSuccess)
+        return LATEC_ERR_CUDA;
+    int rc = launch_lanes_decode(dst, n_stages, total_chunks, words, chunk_range, levels, codes,
+                                 err, st);
+    if (!rc && any_compat) rc = launch_stack_decode(dst, n_stages, words, levels, codes, err, st);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,633 @@
+// Fused dyadic interpolation + error-bounded quantizer (encode) and
+// interpolation + dequantizer (decode) for one sub-stage of the schedule.
+//
+// Bit-exactness contract with the reference (latec/predictor.py:97-156,
+// 255-317; latec/quantizer.py:28-120): every prediction is evaluated in
+// float64 on the float32 (or float64) reconstruction, in the reference's
+// operation order, with explicitly rounded intrinsics so that nothing is
+// contracted into an FMA; the quotient (x - p) / 2eb is the correctly rounded
+// float64 division (a reciprocal product is used only when it provably rounds
+// to the same integer); the reconstruction is f32(p + 2eb * q) and the bound is
+// verified in float32 exactly as the reference decoder computes it.
+#include <cuda_runtime.h>
+
+#include "interp_kernels.cuh"
+
+namespace latec {
+
+template <typename T>
+__device__ __forceinline__ double ldv(const T* p) {
+    return (double)__ldg(p);
+}
+
+// 1-D line rule along one odd axis (c >= s always holds there, so the -s tap
+// is valid): cubic / quadratic ends / linear, else the one-sided rule.
+// latec/predictor.py:121-156.
+template <typename T>
+__device__ __forceinline__ double axis_interp(const T* __restrict__ rc, int64_t flat, int c,
+                                              int n, int64_t gs, int s, int cubic, int em) {
+    const int64_t o1 = (int64_t)s * gs;
+    const double Lm1 = ldv(rc + flat - o1);
+    const bool vp1 = c + s < n;
+    const bool vm3 = c - 3 * s >= 0;
+    if (vp1) {
+        const double Lp1 = ldv(rc + flat + o1);
+        const double lin = 0.5 * __dadd_rn(Lm1, Lp1);
+        if (!cubic) return lin;
+        const bool vp3 = c + 3 * s < n;
+        if (vm3 && vp3) {
+            const double Lm3 = ldv(rc + flat - 3 * o1);
+            const double Lp3 = ldv(rc + flat + 3 * o1);
+            double t = __dadd_rn(-Lm3, __dmul_rn(9.0, Lm1));
+            t = __dadd_rn(t, __dmul_rn(9.0, Lp1));
+            t = __dsub_rn(t, Lp3);
+            return t * 0.0625;
+        }
+        if (em & 1) {
+            if (vp3) {  // interp_quad_1: leading end
+                const double Lp3 = ldv(rc + flat + 3 * o1);
+                double t = __dadd_rn(__dmul_rn(3.0, Lm1), __dmul_rn(6.0, Lp1));
+                t = __dsub_rn(t, Lp3);
+                return t * 0.125;
+            }
+            if (vm3) {  // interp_quad_2: trailing end
+                const double Lm3 = ldv(rc + flat - 3 * o1);
+                double t = __dadd_rn(-Lm3, __dmul_rn(6.0, Lm1));
+                t = __dadd_rn(t, __dmul_rn(3.0, Lp1));
+                return t * 0.125;
+            }
+        }
+        return lin;
+    }
+    if ((em & 2) && vm3) {  // interp_linear1 extrapolation past the line end
+        const double Lm3 = ldv(rc + flat - 3 * o1);
+        return __dsub_rn(__dmul_rn(1.5, Lm1), __dmul_rn(0.5, Lm3));
+    }
+    return Lm1;
+}
+
+// Prediction of one stage point from its own odd axes (center combine of
+// latec/predictor.py:286-314; terms of even axes are exact zeros there).
+template <typename T>
+__device__ __forceinline__ double predict_point(const StageDesc& d, const QParams& q,
+                                                const T* __restrict__ rc, int64_t flat,
+                                                const int32_t* coord) {
+    if (d.kind == 0) {
+        const int a = d.axis;
+        return axis_interp(rc, flat, coord[a], d.shape[a], d.gstride[a], d.s, q.order, q.end_mode);
+    }
+    if (q.center == 0) {
+        double total = 0.0;
+        int cnt = 0;
+#pragma unroll
+        for (int j = 0; j < MAXD; j++) {
+            if (j < d.ndim && (coord[j] & d.s)) {
+                double v = axis_interp(rc, flat, coord[j], d.shape[j], d.gstride[j], d.s, q.order,
+                                       q.end_mode);
+                total = cnt ? __dadd_rn(total, v) : v;
+                cnt++;
+            }
+        }
+        if (cnt == 1) return total;
+        if (cnt == 2) return total * 0.5;
+        if (cnt == 4) return total * 0.25;
+        return __ddiv_rn(total, (double)cnt);
+    }
+    int pick = -1;
+#pragma unroll
+    for (int j = 0; j < MAXD; j++) {
+        if (j < d.ndim && (coord[j] & d.s)) {
+            if (q.center == 2 || pick < 0) pick = j;
+        }
+    }
+    return axis_interp(rc, flat, coord[pick], d.shape[pick], d.gstride[pick], d.s, q.order,
+                       q.end_mode);
+}
+
+// rint((x - p) / w) with the division's exact rounding: the reciprocal
+// product is used unless it lies within a few ulps of a half-integer.
+__device__ __forceinline__ double quotient_rint(double diff, const QParams& q) {
+    if (q.inv_w != 0.0) {
+        const double a = __dmul_rn(diff, q.inv_w);
+        const double r = rint(a);
+        const double frac = fabs(__dsub_rn(a, r));
+        const double tol = fabs(a) * 0x1p-48 + 0x1p-1000;
+        if (!(fabs(frac - 0.5) <= tol)) return r;  // NaN/inf fall through unchanged
+    }
+    return rint(__ddiv_rn(diff, q.w));
+}
+
+struct QOut {
+    uint32_t code;  // 0 = outlier
+    int32_t qv;     // bin index when in range
+};
+
+// Quantize one value (float32 source). Returns the code and writes the
+// reconstruction the decoder will produce.
+__device__ __forceinline__ QOut quant_f32(float x, double pd, const QParams& q, float& rv) {
+    const double qd = quotient_rint(__dsub_rn((double)x, pd), q);
+    QOut o{0u, 0};
+    rv = x;
+    if (fabs(qd) < (double)q.radius) {
+        const int qi = (int)qd;
+        const float rf = __double2float_rn(__dadd_rn(pd, __dmul_rn(q.w, (double)qi)));
+        const float chk = q.round_output ? rintf(rf) : rf;
+        if (fabsf(__fsub_rn(x, chk)) <= q.eb_f) {
+            o.code = (uint32_t)(qi + q.radius);
+            o.qv = qi;
+            rv = rf;
+        }
+    }
+    return o;
+}
+
+// float64 source: prediction, reconstruction and bound check stay float64.
+__device__ __forceinline__ QOut quant_f64(double x, double pd, const QParams& q, double& rv) {
+    const double qd = quotient_rint(__dsub_rn(x, pd), q);
+    QOut o{0u, 0};
+    rv = x;
+    if (fabs(qd) < (double)q.radius) {
+        const int qi = (int)qd;
+        double rd = __dadd_rn(pd, __dmul_rn(q.w, (double)qi));
+        const double chk = q.round_output ? rint(rd) : rd;
+        if (fabs(__dsub_rn(x, chk)) <= q.eb) {
+            o.code = (uint32_t)(qi + q.radius);
+            o.qv = qi;
+            rv = rd;
+        }
+    }
+    return o;
+}
+
+template <typename T>
+struct Quant;
+template <>
+struct Quant<float> {
+    __device__ static QOut run(float x, double pd, const QParams& q, float& rv) {
+        return quant_f32(x, (double)__double2float_rn(pd), q, rv);
+    }
+    __device__ static double err(float x, double pd) {  // f32 residual, like the reference stats
+        return (double)__fsub_rn(x, __double2float_rn(pd));
+    }
+    __device__ static double rerr(float x, float rv) { return (double)fabsf(__fsub_rn(x, rv)); }
+};
+template <>
+struct Quant<double> {
+    __device__ static QOut run(double x, double pd, const QParams& q, double& rv) {
+        return quant_f64(x, pd, q, rv);
+    }
+    __device__ static double err(double x, double pd) { return __dsub_rn(x, pd); }
+    __device__ static double rerr(double x, double rv) { return fabs(__dsub_rn(x, rv)); }
+};
+
+// Block-wide reduction helpers -------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ uint32_t warp_umax(uint32_t v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+struct BlockAcc {
+    double s[5];
+    uint32_t maxq;
+};
+
+// Flush the per-block histogram window and statistics.
+__device__ __forceinline__ void block_finish(BlockAcc& a, uint32_t* sh_hist, uint32_t* hist_seg,
+                                             uint64_t block_base, StageAcc* acc,
+                                             double* partials) {
+    __shared__ double sh_red[5][THREADS / 32];
+    __shared__ uint32_t sh_mq[THREADS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 4; k++) a.s[k] = warp_sum(a.s[k]);
+    a.s[4] = warp_max(a.s[4]);
+    a.maxq = warp_umax(a.maxq);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 5; k++) sh_red[k][wid] = a.s[k];
+        sh_mq[wid] = a.maxq;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s[5] = {0, 0, 0, 0, 0};
+        uint32_t mq = 0;
+        for (int w = 0; w < THREADS / 32; w++) {
+            for (int k = 0; k < 4; k++) s[k] += sh_red[k][w];
+            s[4] = fmax(s[4], sh_red[4][w]);
+            mq = max(mq, sh_mq[w]);
+        }
+        for (int k = 0; k < 5; k++) partials[(size_t)blockIdx.x * 5 + k] = s[k];
+        if (mq) atomicMax(&acc->maxq, mq);
+    }
+    const uint32_t seg = (uint32_t)(block_base >> SEG_SHIFT);
+    for (int b = threadIdx.x; b < HBINS; b += THREADS) {
+        const uint32_t v = sh_hist[b];
+        if (v) atomicAdd(&hist_seg[(size_t)seg * HBINS + b], v);
+    }
+}
+
+__device__ __forceinline__ void hist_add(uint32_t* sh_hist, uint32_t* hist_total, QOut o,
+                                         int radius, uint32_t& maxq) {
+    if (!o.code) {
+        atomicAdd(&sh_hist[0], 1u);
+        return;
+    }
+    const uint32_t aq = (uint32_t)abs(o.qv);
+    maxq = max(maxq, aq);
+    if (aq < HWIN)
+        atomicAdd(&sh_hist[o.qv + HWIN], 1u);
+    else
+        atomicAdd(&hist_total[o.code], 1u);
+}
+
+// ---------------------------------------------------------------- encode
+template <typename T>
+__global__ void __launch_bounds__(THREADS)
+    k_interp_quant(const StageDesc d, const QParams q, const int is_anchor,
+                   const T* __restrict__ x, T* __restrict__ recon, uint16_t* __restrict__ codes,
+                   T* __restrict__ staging, uint32_t* __restrict__ tile_cnt,
+                   uint32_t* __restrict__ hist_total, uint32_t* __restrict__ hist_seg,
+                   StageAcc* __restrict__ acc, double* __restrict__ partials) {
+    __shared__ uint32_t sh_hist[HBINS];
+    for (int b = threadIdx.x; b < HBINS; b += THREADS) sh_hist[b] = 0;
+    __syncthreads();
+    const uint64_t items = (uint64_t)q.channels * d.n;
+    const uint64_t block_base = (uint64_t)blockIdx.x * BLOCK_PTS;
+    BlockAcc a{{0, 0, 0, 0, 0}, 0};
+    for (int t = 0; t < TILES_PER_BLOCK; t++) {
+        const uint64_t tile_base = block_base + (uint64_t)t * TILE;
+        if (tile_base >= items) break;
+        int outl = 0;
+#pragma unroll 1
+        for (int k = 0; k < TILE / THREADS; k++) {
+            const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
+            bool is_out = false;
+            if (i < items) {
+                uint32_t c = 0, rank = (uint32_t)i;
+                if (q.channels > 1) {
+                    c = (uint32_t)(i / d.n);
+                    rank = (uint32_t)(i - (uint64_t)c * d.n);
+                }
+                int32_t coord[MAXD];
+                const int64_t flat = stage_coords(d, rank, coord);
+                T* rc = recon + (uint64_t)c * q.points;
+                const double pd = is_anchor ? 0.0 : predict_point<T>(d, q, rc, flat, coord);
+                const T xv = x[(uint64_t)c * q.points + flat];
+                T rv;
+                const QOut o = Quant<T>::run(xv, pd, q, rv);
+                rc[flat] = rv;
+                codes[i] = (uint16_t)o.code;
+                is_out = o.code == 0;
+                if (is_out) staging[i] = xv;
+                hist_add(sh_hist, hist_total, o, q.radius, a.maxq);
+                const double e = Quant<T>::err(xv, pd);
+                a.s[0] += fabs(e);
+                a.s[1] += e * e;
+                const double re = Quant<T>::rerr(xv, rv);
+                a.s[2] += re;
+                a.s[3] += re * re;
+                a.s[4] = fmax(a.s[4], re);
+            }
+            outl += __syncthreads_count(is_out);
+        }
+        if (threadIdx.x == 0) tile_cnt[tile_base / TILE] = (uint32_t)outl;
+    }
+    __syncthreads();
+    block_finish(a, sh_hist, hist_seg, block_base, acc, partials);
+}
+
+// Quantize a compact array against a given prediction (predictor-agnostic
+// path: GNN and caller-supplied predictors). recon_out gets the decoder's
+// reconstruction in the same compact order.
+template <typename T>
+__global__ void __launch_bounds__(THREADS)
+    k_quantize_flat(const QParams q, const uint64_t items, const T* __restrict__ x,
+                    const T* __restrict__ pred, uint16_t* __restrict__ codes,
+                    T* __restrict__ staging, uint32_t* __restrict__ tile_cnt,
+                    uint32_t* __restrict__ hist_total, uint32_t* __restrict__ hist_seg,
+                    StageAcc* __restrict__ acc, double* __restrict__ partials,
+                    T* __restrict__ recon_out) {
+    __shared__ uint32_t sh_hist[HBINS];
+    for (int b = threadIdx.x; b < HBINS; b += THREADS) sh_hist[b] = 0;
+    __syncthreads();
+    const uint64_t block_base = (uint64_t)blockIdx.x * BLOCK_PTS;
+    BlockAcc a{{0, 0, 0, 0, 0}, 0};
+    for (int t = 0; t < TILES_PER_BLOCK; t++) {
+        const uint64_t tile_base = block_base + (uint64_t)t * TILE;
+        if (tile_base >= items) break;
+        int outl = 0;
+        for (int k = 0; k < TILE / THREADS; k++) {
+            const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
+            bool is_out = false;
+            if (i < items) {
+                const T xv = x[i];
+                const double pd = (double)pred[i];
+                T rv;
+                const QOut o = Quant<T>::run(xv, pd, q, rv);
+                recon_out[i] = rv;
+                codes[i] = (uint16_t)o.code;
+                is_out = o.code == 0;
+                if (is_out) staging[i] = xv;
+                hist_add(sh_hist, hist_total, o, q.radius, a.maxq);
+                const double e = Quant<T>::err(xv, pd);
+                a.s[0] += fabs(e);
+                a.s[1] += e * e;
+                const double re = Quant<T>::rerr(xv, rv);
+                a.s[2] += re;
+                a.s[3] += re * re;
+                a.s[4] = fmax(a.s[4], re);
+            }
+            outl += __syncthreads_count(is_out);
+        }
+        if (threadIdx.x == 0) tile_cnt[tile_base / TILE] = (uint32_t)outl;
+    }
+    __syncthreads();
+    block_finish(a, sh_hist, hist_seg, block_base, acc, partials);
+}
+
+// Prediction only (the predictor plugin's ``predict``): compact output.
+template <typename T>
+__global__ void __launch_bounds__(THREADS)
+    k_interp_predict(const StageDesc d, const QParams q, const T* __restrict__ recon,
+                     T* __restrict__ pred) {
+    const uint64_t items = (uint64_t)q.channels * d.n;
+    const uint64_t i = (uint64_t)blockIdx.x * THREADS + threadIdx.x;
+    if (i >= items) return;
+    uint32_t c = 0, rank = (uint32_t)i;
+    if (q.channels > 1) {
+        c = (uint32_t)(i / d.n);
+        rank = (uint32_t)(i - (uint64_t)c * d.n);
+    }
+    int32_t coord[MAXD];
+    const int64_t flat = stage_coords(d, rank, coord);
+    const double pd = predict_point<T>(d, q, recon + (uint64_t)c * q.points, flat, coord);
+    pred[i] = (T)pd;
+}
+
+// ---------------------------------------------------------------- scans
+__global__ void __launch_bounds__(THREADS)
+    k_count_zeros(const uint16_t* __restrict__ codes, const uint64_t items,
+                  uint32_t* __restrict__ tile_cnt) {
+    const uint64_t tile_base = (uint64_t)blockIdx.x * TILE;
+    int cnt = 0;
+    for (int k = 0; k < TILE / THREADS; k++) {
+        const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
+        cnt += (i < items && codes[i] == 0) ? 1 : 0;
+    }
+    __shared__ int sh[THREADS / 32];
+    int v = cnt;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int w = 0; w < THREADS / 32; w++) s += sh[w];
+        tile_cnt[blockIdx.x] = (uint32_t)s;
+    }
+}
+
+// Exclusive scan of per-tile counts by one CTA; total written to *total.
+__global__ void __launch_bounds__(1024)
+    k_tile_scan(const uint32_t* __restrict__ cnt, const uint32_t tiles,
+                uint32_t* __restrict__ off, uint32_t* __restrict__ total) {
+    __shared__ uint32_t sh[1024];
+    const uint32_t per = (tiles + 1023) / 1024;
+    const uint32_t a = threadIdx.x * per, b = min(tiles, a + per);
+    uint32_t s = 0;
+    for (uint32_t i = a; i < b; i++) s += cnt[i];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+        uint32_t v = threadIdx.x >= (unsigned)o ? sh[threadIdx.x - o] : 0u;
+        __syncthreads();
+        sh[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t run = sh[threadIdx.x] - s;
+    for (uint32_t i = a; i < b; i++) {
+        off[i] = run;
+        run += cnt[i];
+    }
+    if (threadIdx.x == 1023) *total = sh[1023];
+}
+
+// Block-local exclusive scan of a per-thread flag in item order (k-major).
+__device__ __forceinline__ uint32_t block_excl_flag(bool f, uint32_t& block_total) {
+    __shared__ uint32_t sh_w[THREADS / 32];
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh_w[wid] = __popc(bal);
+    __syncthreads();
+    uint32_t before = 0, tot = 0;
+    for (int w = 0; w < THREADS / 32; w++) {
+        if (w < wid) before += sh_w[w];
+        tot += sh_w[w];
+    }
+    __syncthreads();
+    block_total = tot;
+    return before + __popc(bal & ((1u << lane) - 1u));
+}
+
+__global__ void __launch_bounds__(THREADS)
+    k_compact(const uint16_t* __restrict__ codes, const uint64_t items,
+              const uint8_t* __restrict__ staging, const int elem,
+              const uint32_t* __restrict__ tile_cnt, const uint32_t* __restrict__ tile_off,
+              uint8_t* __restrict__ out) {
+    const uint32_t tile = blockIdx.x;
+    if (tile_cnt[tile] == 0) return;
+    const uint64_t tile_base = (uint64_t)tile * TILE;
+    uint32_t run = tile_off[tile];
+    for (int k = 0; k < TILE / THREADS; k++) {
+        const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
+        const bool z = i < items && codes[i] == 0;
+        uint32_t tot;
+        const uint32_t pos = run + block_excl_flag(z, tot);
+        if (z) {
+            for (int b = 0; b < elem; b++) out[(uint64_t)pos * elem + b] = staging[i * elem + b];
+        }
+        run += tot;
+    }
+}
+
+__global__ void k_stats_reduce(const double* __restrict__ partials, const uint32_t blocks,
+                               StageAcc* __restrict__ acc) {
+    // one thread, fixed order: deterministic
+    if (threadIdx.x) return;
+    double s[5] = {0, 0, 0, 0, 0};
+    for (uint32_t b = 0; b < blocks; b++) {
+        for (int k = 0; k < 4; k++) s[k] += partials[(size_t)b * 5 + k];
+        s[4] = fmax(s[4], partials[(size_t)b * 5 + 4]);
+    }
+    for (int k = 0; k < 5; k++) acc->stats[k] = s[k];
+}
+
+// ---------------------------------------------------------------- decode
+template <typename T>
+__device__ __forceinline__ T load_unaligned(const uint8_t* p) {
+    uint8_t b[sizeof(T)];
+#pragma unroll
+    for (int k = 0; k < (int)sizeof(T); k++) b[k] = p[k];
+    T v;
+    memcpy(&v, b, sizeof(T));
+    return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(THREADS)
+    k_interp_dequant(const StageDesc d, const QParams q, const int is_anchor,
+                     const uint16_t* __restrict__ codes, const uint8_t* __restrict__ outliers,
+                     const uint32_t* __restrict__ tile_off, const uint32_t n_out,
+                     T* __restrict__ recon, uint32_t* __restrict__ err) {
+    const uint64_t items = (uint64_t)q.channels * d.n;
+    const uint64_t tile_base = (uint64_t)blockIdx.x * TILE;
+    uint32_t run = tile_off[blockIdx.x];
+    for (int k = 0; k < TILE / THREADS; k++) {
+        const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
+        const bool valid = i < items;
+        const uint32_t code = valid ? codes[i] : 1u;
+        uint32_t tot;
+        const uint32_t pos = run + block_excl_flag(code == 0, tot);
+        run += tot;
+        if (!valid) continue;
+        uint32_t c = 0, rank = (uint32_t)i;
+        if (q.channels > 1) {
+            c = (uint32_t)(i / d.n);
+            rank = (uint32_t)(i - (uint64_t)c * d.n);
+        }
+        int32_t coord[MAXD];
+        const int64_t flat = stage_coords(d, rank, coord);
+        T* rc = recon + (uint64_t)c * q.points;
+        T rv;
+        if (code == 0) {
+            if (pos < n_out) {
+                rv = load_unaligned<T>(outliers + (uint64_t)pos * sizeof(T));
+            } else {
+                rv = (T)0;
+                atomicOr(err, 1u);
+            }
+        } else {
+            const double pd0 = is_anchor ? 0.0 : predict_point<T>(d, q, rc, flat, coord);
+            const double qv = (double)((int)code - q.radius);
+            if (sizeof(T) == 4) {
+                const double pd = (double)__double2float_rn(pd0);
+                rv = (T)__double2float_rn(__dadd_rn(pd, __dmul_rn(q.w, qv)));
+            } else {
+                rv = (T)__dadd_rn(pd0, __dmul_rn(q.w, qv));
+            }
+        }
+        rc[flat] = rv;
+    }
+}
+
+// ---------------------------------------------------------------- launchers
+static int last_err() {
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
+}
+
+int launch_interp_quant(const StageDesc& d, const QParams& q, int dtype, int is_anchor,
+                        const void* x, void* recon, uint16_t* codes, void* staging,
+                        uint32_t* tile_cnt, uint32_t* hist_total, uint32_t* hist_seg,
+                        StageAcc* acc, double* partials, cudaStream_t st) {
+    const uint64_t items = (uint64_t)q.channels * d.n;
+    if (!items) return LATEC_OK;
+    const uint32_t blocks = n_blocks(items);
+    if (dtype == LATEC_F64)
+        k_interp_quant<double><<<blocks, THREADS, 0, st>>>(
+            d, q, is_anchor, (const double*)x, (double*)recon, codes, (double*)staging, tile_cnt,
+            hist_total, hist_seg, acc, partials);
+    else
+        k_interp_quant<float><<<blocks, THREADS, 0, st>>>(
+            d, q, is_anchor, (const float*)x, (float*)recon, codes, (float*)staging, tile_cnt,
+            hist_total, hist_seg, acc, partials);
+    return last_err();
+}
+
+int launch_quantize_flat(const QParams& q, int dtype, uint64_t items, const void* x,
+                         const void* pred, uint16_t* codes, void* staging, uint32_t* tile_cnt,
+                         uint32_t* hist_total, uint32_t* hist_seg, StageAcc* acc,
+                         double* partials, void* recon_out, cudaStream_t st) {
+    if (!items) return LATEC_OK;
+    const uint32_t blocks = n_blocks(items);
+    if (dtype == LATEC_F64)
+        k_quantize_flat<double><<<blocks, THREADS, 0, st>>>(
+            q, items, (const double*)x, (const double*)pred, codes, (double*)staging, tile_cnt,
+            hist_total, hist_seg, acc, partials, (double*)recon_out);
+    else
+        k_quantize_flat<float><<<blocks, THREADS, 0, st>>>(
+            q, items, (const float*)x, (const float*)pred, codes, (float*)staging, tile_cnt,
+            hist_total, hist_seg, acc, partials, (float*)recon_out);
+    return last_err();
+}
+
+int launch_interp_predict(const StageDesc& d, const QParams& q, int dtype, const void* recon,
+                          void* pred, cudaStream_t st) {
+    const uint64_t items = (uint64_t)q.channels * d.n;
+    if (!items) return LATEC_OK;
+    const uint32_t blocks = (uint32_t)((items + THREADS - 1) / THREADS);
+    if (dtype == LATEC_F64)
+        k_interp_predict<double><<<blocks, THREADS, 0, st>>>(d, q, (const double*)recon,
+                                                              (double*)pred);
+    else
+        k_interp_predict<float><<<blocks, THREADS, 0, st>>>(d, q, (const float*)recon,
+                                                            (float*)pred);
+    return last_err();
+}
+
+int launch_count_zeros(const uint16_t* codes, uint64_t items, uint32_t* tile_cnt,
+                       cudaStream_t st) {
+    if (!items) return LATEC_OK;
+    k_count_zeros<<<n_tiles(items), THREADS, 0, st>>>(codes, items, tile_cnt);
+    return last_err();
+}
+
+int launch_tile_scan(const uint32_t* tile_cnt, uint32_t tiles, uint32_t* tile_off,
+                     uint32_t* total, cudaStream_t st) {
+    if (!tiles) return LATEC_OK;
+    k_tile_scan<<<1, 1024, 0, st>>>(tile_cnt, tiles, tile_off, total);
+    return last_err();
+}
+
+int launch_compact(const uint16_t* codes, uint64_t items, const void* staging, int elem,
+                   const uint32_t* tile_cnt, const uint32_t* tile_off, void* out,
+                   cudaStream_t st) {
+    if (!items) return LATEC_OK;
+    k_compact<<<n_tiles(items), THREADS, 0, st>>>(codes, items, (const uint8_t*)staging, elem,
+                                                   tile_cnt, tile_off, (uint8_t*)out);
+    return last_err();
+}
+
+int launch_stats_reduce(const double* partials, uint32_t blocks, StageAcc* acc,
+                        cudaStream_t st) {
+    if (!blocks) return LATEC_OK;
+    k_stats_reduce<<<1, 32, 0, st>>>(partials, blocks, acc);
+    return last_err();
+}
+
+int launch_interp_dequant(const StageDesc& d, const QParams& q, int dtype, int is_anchor,
+                          const uint16_t* codes, const void* outliers, const uint32_t* tile_off,
+                          uint32_t n_out, void* recon, uint32_t* err, cudaStream_t st) {
+    const uint64_t items = (uint64_t)q.channels * d.n;
+    if (!items) return LATEC_OK;
+    if (dtype == LATEC_F64)
+        k_interp_dequant<double><<<n_tiles(items), THREADS, 0, st>>>(
+            d, q, is_anchor, codes, (const uint8_t*)outliers, tile_off, n_out, (double*)recon, err);
+    else
+        k_interp_dequant<float><<<n_tiles(items), THREADS, 0, st>>>(
+            d, q, is_anchor, codes, (const uint8_t*)outliers, tile_off, n_out, (float*)recon, err);
+    return last_err();
+}
+
+}  // namespace latec

@@ -1,0 +1,70 @@
+// Kernel launch helpers of the fused interpolation / quantizer stage.
+#pragma once
+
+#include "latec_common.cuh"
+
+namespace latec {
+
+constexpr int TILE = 2048;            // outlier-count granularity (points)
+constexpr int TILES_PER_BLOCK = 4;    // one CTA walks 4 consecutive tiles
+constexpr int BLOCK_PTS = TILE * TILES_PER_BLOCK;
+constexpr int THREADS = 256;
+constexpr int HWIN = 256;             // histogram window |q| < HWIN kept in SMEM
+constexpr int HBINS = 2 * HWIN;       // bin 0: outliers, q + HWIN otherwise
+constexpr int SEG_SHIFT = 22;         // float32 histogram accumulation segment
+
+struct QParams {
+    double w;        // 2 * eb, float64
+    double inv_w;    // 1 / w, or 0 when the reciprocal is not finite
+    double eb;       // float64 bound (float64 path)
+    float eb_f;      // float32(eb) (float32 path)
+    int radius;
+    int order;       // 0 linear, 1 cubic
+    int center;      // 0 average, 1 first odd axis, 2 last odd axis
+    int end_mode;    // bit 0 quadratic ends, bit 1 extrapolation
+    int round_output;
+    int channels;
+    uint64_t points;  // grid points per channel
+};
+
+// Per-stage device accumulators (one struct per stage).
+struct StageAcc {
+    uint32_t n_out;
+    uint32_t maxq;
+    uint32_t pad0, pad1;
+    double stats[5];  // pred_sae, pred_sse, recon_sae, recon_sse, recon_max
+};
+
+inline uint32_t n_tiles(uint64_t items) { return (uint32_t)((items + TILE - 1) / TILE); }
+inline uint32_t n_blocks(uint64_t items) {
+    return (uint32_t)((items + BLOCK_PTS - 1) / BLOCK_PTS);
+}
+inline uint32_t n_segments(uint64_t items) {
+    return (uint32_t)((items + (1ull << SEG_SHIFT) - 1) >> SEG_SHIFT);
+}
+
+// Launchers (interp_kernels.cu). items = channels * stage points.
+int launch_interp_quant(const StageDesc& d, const QParams& q, int dtype, int is_anchor,
+                        const void* x, void* recon, uint16_t* codes, void* staging,
+                        uint32_t* tile_cnt, uint32_t* hist_total, uint32_t* hist_seg,
+                        StageAcc* acc, double* partials, cudaStream_t st);
+int launch_interp_predict(const StageDesc& d, const QParams& q, int dtype, const void* recon,
+                          void* pred, cudaStream_t st);
+int launch_count_zeros(const uint16_t* codes, uint64_t items, uint32_t* tile_cnt,
+                       cudaStream_t st);
+int launch_tile_scan(const uint32_t* tile_cnt, uint32_t tiles, uint32_t* tile_off,
+                     uint32_t* total, cudaStream_t st);
+int launch_compact(const uint16_t* codes, uint64_t items, const void* staging, int elem,
+                   const uint32_t* tile_cnt, const uint32_t* tile_off, void* out,
+                   cudaStream_t st);
+int launch_stats_reduce(const double* partials, uint32_t blocks, StageAcc* acc,
+                        cudaStream_t st);
+int launch_interp_dequant(const StageDesc& d, const QParams& q, int dtype, int is_anchor,
+                          const uint16_t* codes, const void* outliers, const uint32_t* tile_off,
+                          uint32_t n_out, void* recon, uint32_t* err, cudaStream_t st);
+int launch_quantize_flat(const QParams& q, int dtype, uint64_t items, const void* x,
+                         const void* pred, uint16_t* codes, void* staging, uint32_t* tile_cnt,
+                         uint32_t* hist_total, uint32_t* hist_seg, StageAcc* acc,
+                         double* partials, void* recon_out, cudaStream_t st);
+
+}  // namespace latec

@@ -27,13 +27,14 @@
  *      stage blob = u32 K | u32 chunk_words[n_chunks] | chunk streams
  *      n_chunks = ceil(n / (32 K)); chunk c holds symbols [32Kc, 32K(c+1)),
  *      lane l of the chunk codes symbols 32Kc + 32k + l, k = 0..K-1.
- *      Each lane is a 64-bit rANS state in [2^32, 2^64), initial 2^32,
- *      24-bit precision, 32-bit renormalisation words:
- *        encode (reverse k order): if x >= p << 40 emit low word, x >>= 32;
+ *      Each lane is a 64-bit rANS state in [2^31, 2^63), initial 2^31,
+ *      24-bit precision, 32-bit renormalisation words (the range keeps every
+ *      state below 2^63, where a 64-bit reciprocal division is exact):
+ *        encode (reverse k order): if x >= p << 39 emit low word, x >>= 32;
  *                                  x = (x / p) << 24 | (x % p + left)
  *        decode (forward k order): s = x & (2^24-1) -> symbol;
  *                                  x = p * (x >> 24) + s - left;
- *                                  if x < 2^32: x = x << 32 | next word
+ *                                  if x < 2^31: x = x << 32 | next word
  *      Chunk stream, in decoder read order: for every active lane ascending,
  *      the final encoder state as (high word, low word); then the refill words
  *      by decode step k ascending, lanes ascending within a step.
@@ -159,7 +160,7 @@ long oracle_lanes_encode(const int32_t* syms, const uint8_t* levels, long n, int
         uint64_t x[32];
         int active[32];
         for (int l = 0; l < 32; l++) {
-            x[l] = 1ull << 32;
+            x[l] = 1ull << 31;
             active[l] = base + l < n;
         }
         long tail = 0; /* refill words, filled from the end of scratch */
@@ -174,7 +175,7 @@ long oracle_lanes_encode(const int32_t* syms, const uint8_t* levels, long n, int
                 const uint32_t* cdf = cdfs + (size_t)(levels ? levels[i] : 0) * (alphabet + 1);
                 uint32_t left = cdf[s], p = cdf[s + 1] - cdf[s];
                 if (p == 0) { free(scratch); return -2; }
-                if (x[l] >= ((uint64_t)p << 40)) {
+                if (x[l] >= ((uint64_t)p << 39)) {
                     emit[ne++] = (uint32_t)x[l];
                     x[l] >>= 32;
                 }
@@ -232,7 +233,7 @@ int oracle_lanes_decode(const uint32_t* words, long n_words, const uint8_t* leve
                 int s = find_sym(cdf, alphabet, q);
                 uint32_t left = cdf[s], p = cdf[s + 1] - cdf[s];
                 x[l] = (uint64_t)p * (x[l] >> PREC) + (q - left);
-                if (x[l] < (1ull << 32)) {
+                if (x[l] < (1ull << 31)) {
                     if (pos >= end) return -5;
                     x[l] = (x[l] << 32) | words[pos++];
                 }
@@ -240,7 +241,7 @@ int oracle_lanes_decode(const uint32_t* words, long n_words, const uint8_t* leve
             }
         }
         for (int l = 0; l < 32; l++)
-            if (base + l < n && x[l] != (1ull << 32)) return -5;
+            if (base + l < n && x[l] != (1ull << 31)) return -5;
         if (pos != end) return -5;
     }
     return pos == n_words ? 0 : -5;

@@ -1,0 +1,188 @@
+"""Host-side logic and the C ABI library, without a GPU."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import ans as oans
+from oracle import codec as ocodec
+from oracle import levels as olevels
+from oracle import rans_model as orm
+from tests.golden_io import load_npz
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _lib():
+    from latec_b200 import _lib
+
+    return _lib
+
+
+def test_library_exports_every_header_symbol():
+    _l = _lib()
+    lib = _l.load(require_gpu=False)
+    header = open(os.path.join(ROOT, "include", "latec_b200.h")).read()
+    names = set(re.findall(r"^\s*(?:const\s+)?(?:int|uint64_t|char\s*\*|const char\*)\s*\*?\s*(latec_\w+)\(",
+                           header, re.M))
+    names |= set(re.findall(r"\b(latec_\w+)\(", header))
+    names = {n for n in names if not n.endswith("_t")}
+    assert names, "no declarations found"
+    for n in sorted(names):
+        assert hasattr(lib, n), f"missing export {n}"
+    assert set(names) == set(_l.SIGNATURES), "binding and header disagree"
+    assert lib.latec_version().startswith(b"latec_b200")
+
+
+def test_compute_entry_points_refuse_without_gpu():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    with pytest.raises(RuntimeError):
+        _lib().load(require_gpu=True)
+
+
+SCHEDULES = [((64, 64), 3, 8), ((33, 65), 4, 16), ((19, 23, 17), 3, 8), ((16, 16, 16, 16), 4, 16),
+             ((17, 16, 16, 16, 16), 4, 16), ((64, 64), 5, 16), ((1, 7), 3, 8), ((5, 1, 7), 2, 4),
+             ((9, 10, 11, 12), 2, 4), ((7, 5, 6, 3, 4, 5), 2, 4), ((2, 2), 4, 16), ((1, 1000), 5, 32)]
+
+
+@pytest.mark.parametrize("shape,lv,stride", SCHEDULES)
+def test_plan_counts_and_rank_decode_match_masks(shape, lv, stride):
+    """The kernels' rank -> grid-index decode (run here on the host) visits
+    every stage's points in the reference's flatnonzero(mask) order."""
+    from latec_b200 import levels
+
+    _l = _lib()
+    lib = _l.load(require_gpu=False)
+    p = levels.Plan(shape, lv, stride)
+    assert p.counts == olevels.stage_counts(shape, lv, stride, 1)
+    for t, m in enumerate(olevels.stage_masks(shape, lv, stride, 1)):
+        want = np.flatnonzero(m)
+        got = np.empty(len(want), np.int64)
+        _l.check(lib.latec_plan_stage_flat(p.handle, t, 0, len(want), got.ctypes.data))
+        assert np.array_equal(got, want), t
+
+
+def test_plan_rejects_bad_parameters():
+    from latec_b200 import levels
+
+    with pytest.raises(ValueError):
+        levels.Plan((64, 64), 3, 7)
+    with pytest.raises(ValueError):
+        levels.Plan((64, 64), 2, 16)
+    with pytest.raises(ValueError):
+        levels.Plan((), 2, 4)
+    with pytest.raises(NotImplementedError):
+        levels.Plan((64, 64), 3, 8, 4)
+
+
+def test_stage_ebs_match_reference_schedule():
+    from latec_b200 import levels
+    from tests.golden_io import schedule_cases
+
+    for c in schedule_cases():
+        got = levels.stage_ebs(tuple(c["shape"]), c["levels"], c["stride"], c["block"], 1e-3, 0.9)
+        assert [float(v) for v in got] == c["ebs"]
+
+
+def test_tables_match_reference_golden():
+    from latec_b200 import rans_model as rm
+    from tests.golden_io import sha
+
+    z = load_npz("rans.npz")
+    for t in z["meta"]["tables"]:
+        assert sha(rm.cdfs(t["kexp"], t["shape"], t["owx"]).astype("<u4")) == t["sha"]
+    for i, c in enumerate(z["meta"]["const_level"]):
+        codes = z[f"cl_codes_{i}"]
+        hist = orm.const_hist(codes, 1 << 15, c["kexp"])
+        assert rm.fit_const_level(hist, len(codes), c["kexp"]) == (
+            c["level"], c["shape"], c["owx"], c["bits"])
+
+
+@pytest.mark.parametrize("n,kexp", [(5000, 3), (3 * (1 << 22) + 1234, 2), (9 * (1 << 22), 1),
+                                    ((1 << 22) * 5 + 77, 9)])
+def test_histogram_reconstruction_replays_float32_accumulation(n, kexp):
+    """Per-segment window counts reproduce the reference's float32 histogram
+    exactly, including bins whose count passes 2^24."""
+    from latec_b200 import rans_model as rm
+
+    rs = np.random.RandomState(n % 1000)
+    span = (1 << kexp) - 1
+    q = np.clip(np.round(rs.laplace(0, 0.05 if n > 1 << 24 else 2, n)), -span, span).astype(np.int64)
+    codes = (q + (1 << 15)).astype(np.uint32)
+    codes[rs.rand(n) < 1e-4] = 0
+    want = orm.const_hist(codes, 1 << 15, kexp)
+    nseg = -(-n // (1 << 22))
+    seg = np.zeros((nseg, 2 * rm.HWIN), np.uint32)
+    total = np.zeros(65536, np.uint32)
+    for s in range(nseg):
+        c = codes[s << 22:(s + 1) << 22]
+        qq = c.astype(np.int64) - (1 << 15)
+        inw = (c != 0) & (np.abs(qq) < rm.HWIN)
+        seg[s] += np.bincount(np.where(c == 0, 0, np.where(inw, qq + rm.HWIN, 0)),
+                              minlength=2 * rm.HWIN).astype(np.uint32) * 0
+        seg[s, 0] = np.count_nonzero(c == 0)
+        seg[s] += np.bincount(qq[inw] + rm.HWIN, minlength=2 * rm.HWIN).astype(np.uint32)
+        big = (c != 0) & ~inw
+        total += np.bincount(c[big], minlength=65536).astype(np.uint32)
+    got = rm.stage_hist_f32(n, kexp, 1 << 15, seg, total)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_fast_quantisation_matches_oracle_c():
+    from latec_b200 import rans_model as rm
+
+    for kexp, shape, owx in [(1, 0, 0), (3, 5, 2), (8, 12, 7), (11, 20, 1)]:
+        rows = rm.cdfs(kexp, shape, owx)
+        got = rm.fast_quantize_rows(rows[::9])
+        want = oans.wire_cdfs(rows[::9])
+        assert np.array_equal(got, want)
+
+
+def test_lanes_chunking_rule_matches_oracle():
+    from latec_b200 import rans_model as rm
+
+    for n, bits in [(1, 0.0), (100, 5.0), (65536, 3e3), (65536, 9e5), (50_000_000, 1e6),
+                    (50_000_000, 2e8), (117_000_000, 5e9)]:
+        assert rm.lanes_K(n, bits) == ocodec.lanes_K(n, bits)
+
+
+def test_header_and_frame_layout_match_reference_format():
+    from latec_b200 import bitstream as bs
+
+    h = bs.Header(channels=1, src_dtype=1, spatial=(512, 512), eb=1e-3, levels=4,
+                  anchor_stride=16, anchor_block=1, radius=1 << 15, max_radius=0, agg_level=-1,
+                  vmin=-3.5, vmax=4.25, flags=bs.FLAG_INTERP | bs.FLAG_CUBIC | (1 << 9),
+                  interp_center=0, eb_ratio=0.9)
+    raw = h.pack()
+    oh = ocodec.pack_header(dict(flags=h.flags, channels=1, src_dtype=1, levels=4,
+                                 anchor_stride=16, anchor_block=1, interp_center=0,
+                                 radius=1 << 15, eb=1e-3, vmin=-3.5, vmax=4.25, eb_ratio=0.9,
+                                 spatial=(512, 512)))
+    assert raw == oh and len(raw) == 80 + 1 + 8
+    assert bs.Header.unpack(raw) == h
+    with pytest.raises(ValueError):
+        bs.Header.unpack(b"XXXXXXXX" + raw[8:])
+    w = bs.pack_frame(12345, 7, 20, 63, 7, True)
+    assert w == ocodec.framed(12345, 7, 20, 63, 7, True)
+    assert bs.unpack_frame(w) == dict(hlen=12345, kexp=7, shape=20, level=63, owx=7, literal=True)
+    with pytest.raises(ValueError):
+        bs.pack_frame(1 << 45, 1, 0)
+
+
+@pytest.mark.parametrize("n", [0, 1, 1000, 1 << 17, (1 << 17) + 1, 3 * (1 << 17), 700_001])
+def test_raw_zstd_frame_is_a_valid_zstd_frame(n):
+    from latec_b200 import bitstream as bs
+
+    payload = np.random.RandomState(n % 97).randint(0, 256, n).astype(np.uint8)
+    frame = bs.raw_zstd_frame(payload)
+    assert bs.zstd().decompress_into(frame).tobytes() == payload.tobytes()
+    assert bs.read_body(frame).tobytes() == payload.tobytes()
+    assert frame.tobytes() == ocodec.raw_zstd_frame(payload.tobytes())
+    z = bs.zstd().compress(payload.tobytes(), 3)
+    assert bs.read_body(np.frombuffer(z, np.uint8)).tobytes() == payload.tobytes()
