@@ -40,6 +40,10 @@ def _gpu_compress(x, m, entropy="native"):
                        eb_ratio=ck.get("eb_ratio"), entropy=entropy)
 
 
+def _bytes(a):
+    return np.ascontiguousarray(np.asarray(a)).view(np.uint8)
+
+
 def _oracle_stages(stream):
     """Stage codes / outliers of a stream, parsed and entropy-decoded by the oracle."""
     h = ocodec.unpack_header(stream)
@@ -73,7 +77,7 @@ def test_stage_codes_outliers_recon_bit_exact(name):
     assert st["stage_outliers"] == m["stage_outliers"]
     assert sha(np.asarray(st["recon"], np.float32).astype("<f4")) == m["recon_sha"]
     back = _lb().decompress(stream)
-    assert np.array_equal(np.asarray(back).view(np.uint8), np.asarray(st["recon"]).view(np.uint8))
+    assert np.array_equal(_bytes(back), _bytes(st["recon"]))
 
 
 @pytest.mark.parametrize("name", ["grf2d_128", "odd3d_c0_e1", "odd3d_c2_e3", "grf4d_default_center",
@@ -102,9 +106,9 @@ def test_stream_bytes_match_oracle(name, entropy):
         assert stream == ostream
     # cross decode: the oracle reads the GPU stream and the GPU reads the oracle's
     back_o = ocodec.decompress(stream)
-    assert np.array_equal(np.asarray(back_o).view(np.uint8), np.asarray(st["recon"]).view(np.uint8))
+    assert np.array_equal(_bytes(back_o), _bytes(st["recon"]))
     back_g = _lb().decompress(ostream)
-    assert np.array_equal(np.asarray(back_g).view(np.uint8), np.asarray(ost["recon"]).view(np.uint8))
+    assert np.array_equal(_bytes(back_g), _bytes(ost["recon"]))
 
 
 def test_float64_path_matches_oracle_and_bound():
