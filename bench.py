@@ -164,6 +164,39 @@ def run_reference(args, rank):
     }), flush=True)
 
 
+def run_profile(args, dev):
+    """Warm-up plus timed device-resident round trips at --shape, with the
+    per-phase wall times the codec records; used under ncu for launch lists."""
+    import torch
+
+    import latec_b200 as lb
+    from latec_b200 import fields
+
+    shape = tuple(args.shape) if args.shape else SHAPE
+    x = fields.turbulence_jumps(shape, seed=0, device=dev)
+    mm = torch.aminmax(x)
+    eb = REL_EB * (float(mm.max.item()) - float(mm.min.item()))
+    rows = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        stream, st = lb.compress(x, eb, lb.InterpPredictor("cubic", LEVELS, STRIDE, 1),
+                                 levels=LEVELS, anchor_stride=STRIDE, recon="none")
+        b = time.perf_counter()
+        out = lb.decompress(stream, out="device")
+        torch.cuda.synchronize()
+        c = time.perf_counter()
+        if i >= args.warmup:
+            rows.append({"compress_ms": (b - a) * 1e3, "decompress_ms": (c - b) * 1e3,
+                         "stages_ms": st["predict_s"] * 1e3, "entropy_ms": st["entropy_s"] * 1e3,
+                         "fit_ms": st["fit_s"] * 1e3, "rans_ms": st["rans_s"] * 1e3,
+                         "download_ms": st["download_s"] * 1e3,
+                         "bytes": len(stream)})
+        del out
+    print(json.dumps({"profile": list(shape), "eb": eb, "ratio": x.numel() * 4 / len(stream),
+                      "rows": rows}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -171,6 +204,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="latec_b200", choices=["latec_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="only warm-up + timed device round trips (for ncu launch lists)")
+    ap.add_argument("--shape", type=int, nargs="+", default=None,
+                    help="field shape for --profile (default 512 512 512)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -194,6 +231,8 @@ def main():
     from latec_b200 import _lib
 
     lib = _lib.load()
+    if args.profile:
+        return run_profile(args, dev)
     x, eb = make_field(dev)
     nbytes = x.numel() * x.element_size()
 
@@ -270,7 +309,7 @@ def main():
         if i:
             times.append(e0.elapsed_time(e1))
     pass_ms = statistics.median(times)
-    alg_bytes = plan.points * (4 + 4 + 2)
+    alg_bytes = sum(plan.counts) * (4 + 4 + 2)
     peak, peak_kind = _peaks()
     achieved = alg_bytes / (pass_ms / 1e3) / 1e9
     del rc, enc

@@ -193,6 +193,7 @@ class _Encoder:
             hist = rans_model.stage_hist_f32(n, kexp, self.radius, seg, totals.get(t))
             level, shape, owx, bits = rans_model.fit_const_level(hist, n, kexp)
             fits.append((kexp, level, shape, owx, bits))
+        t_fit = time.perf_counter()
         # ---- entropy stage on the device
         stages = (_lib.RansStage * ns)()
         keep = []
@@ -229,6 +230,7 @@ class _Encoder:
             b.elem, payload.data_ptr(), cap, plen.data_ptr(), err.data_ptr(), ws.data_ptr(),
             ws.numel(), stream), "latec_rans_encode")
         n_bytes = int(plen.item())
+        t_rans = time.perf_counter()
         e = int(err.item())
         if e:
             raise RuntimeError(f"entropy coder reported error bits {e:#x}")
@@ -249,6 +251,7 @@ class _Encoder:
             stage_recon_sse=[float(st[t].stats[3]) for t in range(ns)],
             stage_recon_max=[float(st[t].stats[4]) for t in range(ns)],
             predict_s=t1 - t0, quantize_s=0.0, entropy_s=t2 - t1,
+            fit_s=t_fit - t1, rans_s=t_rans - t_fit, download_s=t2 - t_rans,
             outliers=int(sum(int(st[t].n_out) for t in range(ns))),
             stage_fit=fits,
         )

@@ -461,16 +461,28 @@ __global__ void __launch_bounds__(THREADS)
     }
 }
 
-__global__ void k_stats_reduce(const double* __restrict__ partials, const uint32_t blocks,
-                               StageAcc* __restrict__ acc) {
-    // one thread, fixed order: deterministic
-    if (threadIdx.x) return;
+// Deterministic block reduction of the per-block statistics: a fixed
+// thread -> block assignment and a fixed tree, independent of timing.
+__global__ void __launch_bounds__(256)
+    k_stats_reduce(const double* __restrict__ partials, const uint32_t blocks,
+                   StageAcc* __restrict__ acc) {
+    __shared__ double sh[5][256];
     double s[5] = {0, 0, 0, 0, 0};
-    for (uint32_t b = 0; b < blocks; b++) {
+    for (uint32_t b = threadIdx.x; b < blocks; b += 256) {
         for (int k = 0; k < 4; k++) s[k] += partials[(size_t)b * 5 + k];
         s[4] = fmax(s[4], partials[(size_t)b * 5 + 4]);
     }
-    for (int k = 0; k < 5; k++) acc->stats[k] = s[k];
+    for (int k = 0; k < 5; k++) sh[k][threadIdx.x] = s[k];
+    __syncthreads();
+    for (int o = 128; o; o >>= 1) {
+        if (threadIdx.x < (unsigned)o) {
+            for (int k = 0; k < 4; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + o];
+            sh[4][threadIdx.x] = fmax(sh[4][threadIdx.x], sh[4][threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 5; k++) acc->stats[k] = sh[k][0];
 }
 
 // ---------------------------------------------------------------- decode
@@ -612,7 +624,7 @@ int launch_compact(const uint16_t* codes, uint64_t items, const void* staging, i
 int launch_stats_reduce(const double* partials, uint32_t blocks, StageAcc* acc,
                         cudaStream_t st) {
     if (!blocks) return LATEC_OK;
-    k_stats_reduce<<<1, 32, 0, st>>>(partials, blocks, acc);
+    k_stats_reduce<<<1, 256, 0, st>>>(partials, blocks, acc);
     return last_err();
 }
 

@@ -67,7 +67,7 @@ def level_weights(kexp, n_levels=N_LEVELS):
     return w
 
 
-@lru_cache(maxsize=32)
+@lru_cache(maxsize=512)
 def shaped_weights(kexp, shape, n_levels=N_LEVELS):
     """Mixture entry ``shape``: (1-w) p[level] + w p[level+d] (``latec/rans.py:376-384``)."""
     weights = level_weights(kexp, n_levels)
@@ -121,7 +121,7 @@ def quantize_pmf_rows(weights, total):
     return pmf.astype(np.uint32)
 
 
-@lru_cache(maxsize=16)
+@lru_cache(maxsize=256)
 def cdfs(kexp, shape=0, owx=0, n_levels=N_LEVELS, precision=PRECISION):
     """``(n_levels, alphabet + 1)`` uint32 CDF rows (``latec/rans.py:304-329``)."""
     alphabet = 2 * ((1 << kexp) - 1) + 2
@@ -134,7 +134,7 @@ def cdfs(kexp, shape=0, owx=0, n_levels=N_LEVELS, precision=PRECISION):
     return out
 
 
-@lru_cache(maxsize=16)
+@lru_cache(maxsize=512)
 def neg_log2_weights(kexp, shape, owx, n_levels=N_LEVELS, precision=PRECISION):
     """``latec/rans.py:387-392``."""
     weights = with_outlier_weight(shaped_weights(kexp, shape, n_levels), owx)
