@@ -80,7 +80,7 @@ typedef struct latec_rans_stage {
     int32_t per_point;    /* 1: per-symbol table row from the levels array */
     uint32_t blob_words;  /* decode: blob length in words */
     uint32_t n_out;
-    uint32_t pad;
+    uint32_t block0;      /* filled by the library (decode) */
 } latec_rans_stage;
 
 /* ---- schedule: replaces latec/levels.py:100-147 (iter_stage_plan),
@@ -160,7 +160,9 @@ int latec_rans_build_tables(const uint32_t* cdf_rows, int32_t alphabet, int32_t 
  * (fills scratch_off / n_chunks / chunk0 of the host array). */
 uint64_t latec_rans_encode_workspace_bytes(latec_rans_stage* stages, int32_t n_stages);
 
-/* ---- entropy-code every stage and assemble the stage records
+/* ---- entropy-code every stage and assemble the stage records.
+ *      On return the workspace starts with the n_stages stage descriptors
+ *      (device copy) with blob_words, n_out and rec_off filled in
  *      (latec/bitstream.py:178-243 pack_stage with latec/rans.py:466-498
  *      rans_encode_const / 546-578 rans_encode) into `payload` on the
  *      device: per stage u32 n | u64 frame | blob | u32 n_out | outliers.
@@ -179,10 +181,19 @@ int latec_rans_encode(latec_rans_stage* stages, int32_t n_stages, const uint16_t
  *      stream, as absolute word offsets in `words`, global chunk order.
  *      err bits: 4 read past a chunk, 8 bad final state, 16 compat stream. */
 uint64_t latec_rans_decode_workspace_bytes(int32_t n_stages);
-int latec_rans_decode(const latec_rans_stage* stages, int32_t n_stages, uint32_t total_chunks,
+int latec_rans_decode(latec_rans_stage* stages, int32_t n_stages, uint32_t total_chunks,
                       const uint32_t* words, const uint64_t* chunk_range, const uint8_t* levels,
                       uint16_t* codes, uint32_t* err, void* workspace, uint64_t workspace_bytes,
                       void* stream);
+
+/* ---- container framing on the device (latec/bitstream.py:155-164
+ *      write_stream / read_stream): out = header[hlen] followed by a zstd
+ *      frame of raw blocks holding the n payload bytes, and the inverse
+ *      (frame = the zstd frame after the header). */
+uint64_t latec_raw_frame_bytes(uint64_t payload_bytes);
+int latec_frame_raw(const uint8_t* payload, uint64_t n, const uint8_t* header, uint32_t hlen,
+                    uint8_t* out, uint64_t out_cap, void* stream);
+int latec_unframe_raw(const uint8_t* frame, uint64_t n, uint8_t* payload, void* stream);
 
 /* Library version string. */
 const char* latec_version(void);

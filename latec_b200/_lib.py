@@ -42,7 +42,7 @@ class RansStage(ctypes.Structure):
                 ("scratch_off", U64), ("blob_off", U64), ("rec_off", U64), ("framed_hi", U64),
                 ("n", U32), ("K", U32), ("n_chunks", U32), ("chunk0", U32), ("alphabet", U32),
                 ("kexp", I32), ("radius", I32), ("mode", I32), ("per_point", I32),
-                ("blob_words", U32), ("n_out", U32), ("pad", U32)]
+                ("blob_words", U32), ("n_out", U32), ("block0", U32)]
 
 
 # Every symbol the header declares, with (restype, argtypes).
@@ -69,6 +69,9 @@ SIGNATURES = {
     "latec_rans_encode": (ctypes.c_int, [P, I32, P, P, P, P, I32, P, U64, P, P, P, U64, P]),
     "latec_rans_decode_workspace_bytes": (U64, [I32]),
     "latec_rans_decode": (ctypes.c_int, [P, I32, U32, P, P, P, P, P, P, U64, P]),
+    "latec_raw_frame_bytes": (U64, [U64]),
+    "latec_frame_raw": (ctypes.c_int, [P, U64, P, ctypes.c_uint32, P, U64, P]),
+    "latec_unframe_raw": (ctypes.c_int, [P, U64, P, P]),
 }
 
 _lib = None
@@ -109,6 +112,22 @@ def ptr(t) -> int:
     if hasattr(t, "data_ptr"):
         return t.data_ptr()
     return t.ctypes.data
+
+
+_pinned: dict = {}
+
+
+def pinned(nbytes: int, slot: str = "io"):
+    """A cached page-locked host buffer of at least ``nbytes`` (per slot)."""
+    import torch
+
+    buf = _pinned.get(slot)
+    if buf is None or buf.numel() < nbytes:
+        size = max(int(nbytes), 1 << 20)
+        size = 1 << (size - 1).bit_length()
+        buf = torch.empty(size, dtype=torch.uint8, pin_memory=True)
+        _pinned[slot] = buf
+    return buf
 
 
 def stream_ptr(stream=None) -> int:

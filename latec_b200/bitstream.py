@@ -212,6 +212,56 @@ def raw_zstd_frame(payload: np.ndarray) -> np.ndarray:
     return out
 
 
+class PayloadReader:
+    """Random access to the stage payload, either a plain host array or the
+    payload inside a zstd frame of raw blocks (payload byte ``p`` sits at frame
+    offset ``13 + 3 * (p // 128 KiB + 1) + p``), without unframing it on the host."""
+
+    def __init__(self, data: np.ndarray, n: int, framed: bool):
+        self.data, self.n, self.framed = data, int(n), framed
+
+    def __len__(self):
+        return self.n
+
+    def _idx(self, p, k):
+        idx = np.arange(p, p + k, dtype=np.int64)
+        if self.framed:
+            idx = 13 + 3 * (idx // _RAW_BLOCK + 1) + idx
+        return idx
+
+    def take(self, p: int, k: int) -> np.ndarray:
+        if p < 0 or p + k > self.n:
+            raise ValueError("truncated stage record")
+        if not self.framed:
+            return self.data[p:p + k]
+        return self.data[self._idx(p, k)]
+
+    def u32s(self, p: int, count: int) -> np.ndarray:
+        return np.ascontiguousarray(self.take(p, 4 * count)).view("<u4")
+
+    def unpack(self, fmt: str, p: int):
+        return struct.unpack(fmt, self.take(p, struct.calcsize(fmt)).tobytes())
+
+
+def raw_frame_size(body: np.ndarray):
+    """Payload size if ``body`` is exactly a single-segment zstd frame of raw
+    blocks in the layout ``raw_zstd_frame`` writes, else None."""
+    if len(body) < 13 or bytes(body[:5]) != struct.pack("<IB", 0xFD2FB528, 0xE0):
+        return None
+    (n,) = struct.unpack_from("<Q", body, 5)
+    nblk = max(1, -(-n // _RAW_BLOCK))
+    if len(body) != 13 + 3 * nblk + n:
+        return None
+    starts = 13 + np.arange(nblk, dtype=np.int64) * (_RAW_BLOCK + 3)
+    hdr = (body[starts].astype(np.uint32) | (body[starts + 1].astype(np.uint32) << 8)
+           | (body[starts + 2].astype(np.uint32) << 16))
+    sizes = np.full(nblk, _RAW_BLOCK, np.uint32)
+    sizes[-1] = n - (nblk - 1) * _RAW_BLOCK
+    want = sizes << 3
+    want[-1] |= 1
+    return int(n) if np.array_equal(hdr, want) else None
+
+
 def read_body(data) -> np.ndarray:
     """Decode the zstd frame after the header into the payload bytes. Frames of
     raw blocks (the native writer's) are unpacked with a strided copy; any

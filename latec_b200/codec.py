@@ -234,12 +234,11 @@ class _Encoder:
         e = int(err.item())
         if e:
             raise RuntimeError(f"entropy coder reported error bits {e:#x}")
-        host = payload[:n_bytes].cpu().numpy()
-        t2 = time.perf_counter()
-        if self.mode == _lib.RANS_COMPAT:
-            host = self._compat_literals(host, fits, st)
+        desc = (_lib.RansStage * ns).from_buffer_copy(
+            ws[:ctypes.sizeof(_lib.RansStage) * ns].cpu().numpy().tobytes())
+        rec_bytes = [16 + 4 * int(desc[t].blob_words) + b.elem * int(desc[t].n_out)
+                     for t in range(ns)]
         del keep
-        rec_bytes = self._record_sizes(host, ns)
         stage = dict(
             stage_codes=[int(v) for v in b.items],
             stage_outliers=[int(st[t].n_out) for t in range(ns)],
@@ -250,12 +249,41 @@ class _Encoder:
             stage_recon_sae=[float(st[t].stats[2]) for t in range(ns)],
             stage_recon_sse=[float(st[t].stats[3]) for t in range(ns)],
             stage_recon_max=[float(st[t].stats[4]) for t in range(ns)],
-            predict_s=t1 - t0, quantize_s=0.0, entropy_s=t2 - t1,
-            fit_s=t_fit - t1, rans_s=t_rans - t_fit, download_s=t2 - t_rans,
+            predict_s=t1 - t0, quantize_s=0.0, entropy_s=t_rans - t1,
+            fit_s=t_fit - t1, rans_s=t_rans - t_fit,
             outliers=int(sum(int(st[t].n_out) for t in range(ns))),
             stage_fit=fits,
         )
-        return host, stage
+        return payload, n_bytes, stage
+
+    def to_stream(self, payload, n_bytes, header: bytes, stage):
+        """Container bytes: native streams are framed on the device and copied
+        once through pinned memory; compat streams take the reference's
+        literal-zstd decisions and a level-``zstd_level`` zstd frame on the host."""
+        torch = _torch()
+        t0 = time.perf_counter()
+        if self.mode == _lib.RANS_LANES:
+            total = len(header) + int(self.lib.latec_raw_frame_bytes(n_bytes))
+            hdr = torch.frombuffer(bytearray(header), dtype=torch.uint8).to(self.device)
+            out = torch.empty(total, dtype=torch.uint8, device=self.device)
+            _lib.check(self.lib.latec_frame_raw(payload.data_ptr(), n_bytes, hdr.data_ptr(),
+                                                len(header), out.data_ptr(), total,
+                                                _lib.stream_ptr()), "latec_frame_raw")
+            pin = _lib.pinned(total, "stream_out")
+            pin[:total].copy_(out, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+            stream = bytes(pin[:total].numpy())
+        else:
+            host = payload[:n_bytes].cpu().numpy()
+            host = self._compat_literals(host, stage["stage_fit"])
+            stage["stage_payload_bytes"] = self._record_sizes(host, len(self.plan))
+            body = bitstream.zstd().compress(host, self.zstd_level)
+            stream = header + body
+            n_bytes = len(host)
+        stage["entropy_s"] += time.perf_counter() - t0
+        stage["download_s"] = time.perf_counter() - t0
+        stage["raw_payload_bytes"] = int(n_bytes)
+        return stream
 
     def _record_sizes(self, payload, ns):
         out, off = [], 0
@@ -268,7 +296,7 @@ class _Encoder:
             off += size
         return out
 
-    def _compat_literals(self, payload, fits, st):
+    def _compat_literals(self, payload, fits):
         """Reference back-end choice for large stages (``latec/bitstream.py:203-219``):
         the narrowed symbols deflated by zstd replace the rANS blob when a
         level-1 scout and then the full-level pass beat the model's bits."""
@@ -313,9 +341,13 @@ def _finalize(canvas, src_dtype, channels, as_numpy=True):
         out = out.to(torch.float32)
     if channels == 1:
         out = out[..., 0]
+    out = out.contiguous()
     if as_numpy:
-        return out.contiguous().cpu().numpy()
-    return out.contiguous()
+        host = torch.empty(out.shape, dtype=out.dtype, pin_memory=True)
+        host.copy_(out, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return host.numpy()
+    return out
 
 
 def _is_gpu_interp(predictor):
@@ -406,16 +438,9 @@ def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, rad
 
     def run(ratio, center, end_mode):
         rc = torch.empty_like(field)
-        payload, st = enc.encode(ebs_for(ratio), center, end_mode, rc)
-        header = make_header(center, ratio, end_mode)
-        t0 = time.perf_counter()
-        if entropy == "native":
-            body = bitstream.raw_zstd_frame(payload)
-        else:
-            body = np.frombuffer(bitstream.zstd().compress(payload, zstd_level), np.uint8)
-        stream = header.pack() + body.tobytes()
-        st["entropy_s"] += time.perf_counter() - t0
-        st["raw_payload_bytes"] = len(payload)
+        payload, n_bytes, st = enc.encode(ebs_for(ratio), center, end_mode, rc)
+        stream = enc.to_stream(payload, n_bytes, make_header(center, ratio, end_mode).pack(), st)
+        del payload
         st["compressed_bytes"] = len(stream)
         st["recon_sse"] = float(sum(st["stage_recon_sse"]))
         candidates.append((len(stream), st["recon_sse"], ratio, center, end_mode, stream, rc, st))
@@ -468,26 +493,35 @@ def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, rad
     return stream, stats
 
 
-def _parse_records(payload, ns, elem):
+def _parse_records(reader, ns, elem):
+    """Walk the stage records (``latec/bitstream.py:288-344`` framing)."""
     recs, off = [], 0
-    for t in range(ns):
-        if off + 12 > len(payload):
-            raise ValueError("truncated stage record")
-        n, word = struct.unpack_from("<IQ", payload, off)
+    for _ in range(ns):
+        n, word = reader.unpack("<IQ", off)
         f = bitstream.unpack_frame(word)
         blob = off + 12
-        if blob + f["hlen"] + 4 > len(payload):
-            raise ValueError("truncated stage record")
-        (n_out,) = struct.unpack_from("<I", payload, blob + f["hlen"])
+        (n_out,) = reader.unpack("<I", blob + f["hlen"])
         out_at = blob + f["hlen"] + 4
         end = out_at + elem * n_out
-        if end > len(payload):
+        if end > len(reader):
             raise ValueError("truncated stage record")
         recs.append(dict(f, n=n, blob=blob, n_out=n_out, out_at=out_at))
         off = end
-    if off != len(payload):
+    if off != len(reader):
         raise ValueError("trailing data after the last stage record")
     return recs
+
+
+def _upload_stream(body, dev):
+    """Host bytes -> device through a pinned staging buffer."""
+    torch = _torch()
+    n = len(body)
+    pin = _lib.pinned(n + 4, "stream_in")
+    pin.numpy()[:n] = body
+    d = torch.empty(n + 4, dtype=torch.uint8, device=dev)
+    d[:n].copy_(pin[:n], non_blocking=True)
+    d[n:].zero_()
+    return d
 
 
 def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
@@ -499,7 +533,7 @@ def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
     from .predictor import InterpPredictor
 
     header = Header.unpack(stream)
-    payload = bitstream.read_body(memoryview(stream)[header.size:])
+    body = np.frombuffer(memoryview(stream)[header.size:], np.uint8)
     if header.flags & FLAG_RANS:
         raise NotImplementedError("per-point scale streams are decoded by GNNCodec.uncompress")
     if predictor_factory is None:
@@ -528,7 +562,20 @@ def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
     ebs = _levels.stage_ebs(spatial, header.levels, header.anchor_stride, header.anchor_block,
                             header.eb, header.eb_ratio)
     elem = 8 if header.src_dtype == 2 else 4
-    recs = _parse_records(payload, ns, elem)
+    n_raw = bitstream.raw_frame_size(body)
+    if n_raw is not None:  # native frames: unframe on the device, read headers in place
+        reader = bitstream.PayloadReader(body, n_raw, framed=True)
+        frame_dev = _upload_stream(body, dev)
+        pay_dev = torch.empty(n_raw + 4 + (-n_raw) % 4, dtype=torch.uint8, device=dev)
+        pay_dev.zero_()
+        _lib.check(lib.latec_unframe_raw(frame_dev.data_ptr(), n_raw, pay_dev.data_ptr(),
+                                         _lib.stream_ptr()), "latec_unframe_raw")
+        del frame_dev
+    else:
+        payload = bitstream.zstd().decompress_into(body)
+        reader = bitstream.PayloadReader(payload, len(payload), framed=False)
+        pay_dev = _upload_stream(payload, dev)
+    recs = _parse_records(reader, ns, elem)
     mode = _lib.RANS_LANES if header.flags & FLAG_LANES else _lib.RANS_COMPAT
     items = [n * c for n in plan.counts]
     offsets = np.concatenate([[0], np.cumsum(items)]).astype(np.int64)
@@ -538,24 +585,18 @@ def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
         if not recs[t]["kexp"]:
             raise ValueError("rANS stage record has no coder window")
     aligned = all(r["blob"] % 4 == 0 for r in recs if not r["literal"])
-    pad = (-len(payload)) % 4
-    pbuf = np.concatenate([payload, np.zeros(pad, np.uint8)]) if pad else payload
-    if len(pbuf) == 0:
-        pbuf = np.zeros(4, np.uint8)
-    pay_dev = torch.from_numpy(np.ascontiguousarray(pbuf)).to(dev)
     if aligned:
-        words_host = pbuf.view(np.uint32)
         words_dev = pay_dev
         blob_word = [r["blob"] // 4 for r in recs]
     else:  # literal stages broke the word alignment: gather the rANS blobs
         pieces, blob_word, at = [], [], 0
         for r in recs:
             nw = 0 if r["literal"] else -(-r["hlen"] // 4)
-            pieces.append(payload[r["blob"]:r["blob"] + 4 * nw])
+            pieces.append(np.asarray(reader.take(r["blob"], 4 * nw)))
             blob_word.append(at)
             at += nw
-        words_host = np.concatenate(pieces + [np.zeros(4, np.uint8)]).view(np.uint32)
-        words_dev = torch.from_numpy(words_host.view(np.uint8).copy()).to(dev)
+        words_host = np.concatenate(pieces + [np.zeros(4, np.uint8)])
+        words_dev = torch.from_numpy(words_host).to(dev)
     stages = (_lib.RansStage * ns)()
     keep, ranges, literal_codes = [], [], {}
     chunk = 0
@@ -572,7 +613,7 @@ def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
             continue
         if r["literal"]:
             syms = np.frombuffer(bitstream.zstd().decompress_into(
-                payload[r["blob"]:r["blob"] + r["hlen"]]).tobytes(),
+                reader.take(r["blob"], r["hlen"])).tobytes(),
                 rans_model.literal_dtype(r["kexp"]), count=r["n"])
             literal_codes[t] = rans_model.widen(syms, header.radius, r["kexp"]).astype(np.uint16)
             d.mode = mode
@@ -588,16 +629,15 @@ def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
         d.blob_words = r["hlen"] // 4
         if mode == _lib.RANS_LANES:
             w0 = blob_word[t]
-            wh = words_host
             if d.blob_words < 1:
                 raise ValueError("truncated lane-coder blob")
-            K = int(wh[w0])
+            K = int(reader.u32s(r["blob"], 1)[0])
             if K < 1:
                 raise ValueError("lane coder blob has K = 0")
             nc = -(-r["n"] // (32 * K))
             if 1 + nc > d.blob_words:
                 raise ValueError("truncated lane-coder chunk table")
-            cw = wh[w0 + 1:w0 + 1 + nc].astype(np.uint64)
+            cw = reader.u32s(r["blob"] + 4, nc).astype(np.uint64)
             starts = w0 + 1 + nc + np.concatenate([[0], np.cumsum(cw)[:-1]]).astype(np.uint64)
             ends = starts + cw
             if int(ends[-1]) != w0 + d.blob_words:

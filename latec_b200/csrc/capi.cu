@@ -374,7 +374,7 @@ uint64_t latec_rans_decode_workspace_bytes(int32_t n_stages) {
     return c.off;
 }
 
-int latec_rans_decode(const latec_rans_stage* stages, int32_t n_stages, uint32_t total_chunks,
+int latec_rans_decode(latec_rans_stage* stages, int32_t n_stages, uint32_t total_chunks,
                       const uint32_t* words, const uint64_t* chunk_range, const uint8_t* levels,
                       uint16_t* codes, uint32_t* err, void* workspace, uint64_t workspace_bytes,
                       void* stream) {
@@ -389,14 +389,27 @@ int latec_rans_decode(const latec_rans_stage* stages, int32_t n_stages, uint32_t
         any_compat |= d.mode == LATEC_RANS_COMPAT && d.n;
     }
     if (total_chunks && (!words || !chunk_range)) return LATEC_ERR_ARG;
+    // One decoder CTA covers DEC_WARPS chunks of one stage: number the CTAs.
+    RansStageDesc* host = (RansStageDesc*)stages;  // only block0 is written
+    uint32_t blocks = 0, max_alpha = 0;
+    for (int t = 0; t < n_stages; t++) {
+        host[t].block0 = blocks;
+        if (host[t].mode == LATEC_RANS_LANES && host[t].n) {
+            blocks += (host[t].n_chunks + DEC_WARPS - 1) / DEC_WARPS;
+            // only alphabets the kernel stages in shared memory size the allocation
+            if (!host[t].per_point && host[t].alphabet <= (uint32_t)SMEM_ALPHA &&
+                host[t].alphabet > max_alpha)
+                max_alpha = host[t].alphabet;
+        }
+    }
     Carve c{(uint8_t*)workspace};
     RansStageDesc* dst = c.take<RansStageDesc>(n_stages);
     cudaStream_t st = (cudaStream_t)stream;
     if (cudaMemcpyAsync(dst, stages, sizeof(RansStageDesc) * n_stages, cudaMemcpyHostToDevice, st) !=
         cudaSuccess)
         return LATEC_ERR_CUDA;
-    int rc = launch_lanes_decode(dst, n_stages, total_chunks, words, chunk_range, levels, codes,
-                                 err, st);
+    int rc = launch_lanes_decode(dst, n_stages, total_chunks ? blocks : 0, (int)max_alpha, words,
+                                 chunk_range, levels, codes, err, st);
     if (!rc && any_compat) rc = launch_stack_decode(dst, n_stages, words, levels, codes, err, st);
     return rc;
 }

@@ -273,6 +273,8 @@ __global__ void __launch_bounds__(THREADS)
         for (int k = 0; k < TILE / THREADS; k++) {
             const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
             bool is_out = false;
+            int key = -1;  // histogram bin of this lane's code (-1 none, -2 outside window)
+            uint32_t code = 0;
             if (i < items) {
                 uint32_t c = 0, rank = (uint32_t)i;
                 if (q.channels > 1) {
@@ -287,10 +289,17 @@ __global__ void __launch_bounds__(THREADS)
                 T rv;
                 const QOut o = Quant<T>::run(xv, pd, q, rv);
                 rc[flat] = rv;
+                code = o.code;
                 codes[i] = (uint16_t)o.code;
                 is_out = o.code == 0;
                 if (is_out) staging[i] = xv;
-                hist_add(sh_hist, hist_total, o, q.radius, a.maxq);
+                if (is_out) {
+                    key = 0;
+                } else {
+                    const uint32_t aq = (uint32_t)abs(o.qv);
+                    a.maxq = max(a.maxq, aq);
+                    key = aq < HWIN ? o.qv + HWIN : -2;
+                }
                 const double e = Quant<T>::err(xv, pd);
                 a.s[0] += fabs(e);
                 a.s[1] += e * e;
@@ -299,6 +308,11 @@ __global__ void __launch_bounds__(THREADS)
                 a.s[3] += re * re;
                 a.s[4] = fmax(a.s[4], re);
             }
+            // warp-aggregated histogram: one shared atomic per distinct bin
+            const unsigned same = __match_any_sync(0xffffffffu, key);
+            if (key >= 0 && (threadIdx.x & 31) == __ffs(same) - 1)
+                atomicAdd(&sh_hist[key], (uint32_t)__popc(same));
+            if (key == -2) atomicAdd(&hist_total[code], 1u);
             outl += __syncthreads_count(is_out);
         }
         if (threadIdx.x == 0) tile_cnt[tile_base / TILE] = (uint32_t)outl;

@@ -137,28 +137,59 @@ __global__ void __launch_bounds__(128)
     if (lane == 0) chunk_words[chunk] = 2u * __popc(abal) + tail;
 }
 
-__device__ __forceinline__ uint32_t lookup_sym(const uint32_t* __restrict__ cdf,
-                                               const uint16_t* __restrict__ bucket, uint32_t slot,
-                                               uint32_t alphabet) {
-    uint32_t s = __ldg(bucket + (slot >> (PREC - BUCKET_BITS)));
-    while (s + 1 < alphabet && __ldg(cdf + s + 1) <= slot) s++;
-    return s;
+// Symbol whose CDF interval holds `slot`: the bucket of the slot's top bits
+// brackets it between bucket[b] and bucket[b + 1]; a binary search finishes.
+__device__ __forceinline__ uint32_t lookup_sym(const uint32_t* cdf, const uint16_t* bucket,
+                                               uint32_t slot, uint32_t alphabet) {
+    const uint32_t b = slot >> (PREC - BUCKET_BITS);
+    uint32_t lo = bucket[b];
+    uint32_t hi = (b + 1 < (uint32_t)NBUCKET) ? bucket[b + 1] : alphabet - 1;
+    while (lo < hi) {  // largest s in [lo, hi] with cdf[s] <= slot
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (cdf[mid] <= slot) lo = mid; else hi = mid - 1;
+    }
+    return lo;
 }
 
-__global__ void __launch_bounds__(128)
-    k_lanes_decode(const RansStageDesc* __restrict__ st, int n_stages, uint32_t total_chunks,
+__device__ __forceinline__ int find_block_stage(const RansStageDesc* st, int n_stages,
+                                                uint32_t block) {
+    int lo = 0, hi = n_stages;  // last stage with block0 <= block
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (st[mid].block0 <= block) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// One CTA per DEC_WARPS chunks of a single stage; stage-constant tables are
+// staged in shared memory.
+__global__ void __launch_bounds__(32 * DEC_WARPS)
+    k_lanes_decode(const RansStageDesc* __restrict__ st, int n_stages, const uint32_t smem_alpha,
                    const uint32_t* __restrict__ words, const uint64_t* __restrict__ chunk_range,
                    const uint8_t* __restrict__ levels, uint16_t* __restrict__ codes,
                    uint32_t* __restrict__ err) {
-    const uint32_t chunk = blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (chunk >= total_chunks) return;
-    const int lane = threadIdx.x & 31;
-    const RansStageDesc& d = st[find_stage(st, n_stages, chunk)];
-    const uint32_t K = d.K;
-    const uint64_t base = (uint64_t)(chunk - d.chunk0) * 32u * K;
+    extern __shared__ uint32_t smem[];
+    const RansStageDesc& d = st[find_block_stage(st, n_stages, blockIdx.x)];
+    const uint32_t local = (blockIdx.x - d.block0) * DEC_WARPS + (threadIdx.x >> 5);
+    // smem_alpha: the largest alphabet the dynamic shared memory was sized for
+    const bool smem_tables = !d.per_point && d.alphabet <= smem_alpha;
     const uint32_t alpha1 = d.alphabet + 1;
     const uint32_t* cdfs = (const uint32_t*)d.cdf;
     const uint16_t* buckets = (const uint16_t*)d.bucket;
+    if (smem_tables) {
+        uint32_t* sc = smem;
+        uint16_t* sb = (uint16_t*)(smem + alpha1);
+        for (uint32_t i = threadIdx.x; i < alpha1; i += blockDim.x) sc[i] = cdfs[i];
+        for (uint32_t i = threadIdx.x; i < (uint32_t)NBUCKET; i += blockDim.x) sb[i] = buckets[i];
+        __syncthreads();
+        cdfs = sc;
+        buckets = sb;
+    }
+    if (local >= d.n_chunks) return;
+    const uint32_t chunk = d.chunk0 + local;
+    const int lane = threadIdx.x & 31;
+    const uint32_t K = d.K;
+    const uint64_t base = (uint64_t)local * 32u * K;
     const uint8_t* lv = d.per_point ? levels + d.codes_off : nullptr;
     uint16_t* out = codes + d.codes_off;
     uint64_t pos = chunk_range[2 * (uint64_t)chunk];
@@ -182,7 +213,7 @@ __global__ void __launch_bounds__(128)
             const uint32_t* cdf = cdfs + (uint64_t)row * alpha1;
             const uint32_t slot = (uint32_t)(x & PMASK);
             const uint32_t s = lookup_sym(cdf, buckets + (uint64_t)row * NBUCKET, slot, d.alphabet);
-            const uint32_t left = __ldg(cdf + s), f = __ldg(cdf + s + 1) - left;
+            const uint32_t left = cdf[s], f = cdf[s + 1] - left;
             x = (uint64_t)f * (x >> PREC) + (slot - left);
             out[i] = (uint16_t)widen(s, d.radius, d.kexp);
             need = x < LANE_L;
@@ -405,12 +436,18 @@ int launch_lanes_encode(const RansStageDesc* st, int n_stages, uint32_t total_ch
     return last_err();
 }
 
-int launch_lanes_decode(const RansStageDesc* st, int n_stages, uint32_t total_chunks,
-                        const uint32_t* words, const uint64_t* chunk_range, const uint8_t* levels,
-                        uint16_t* codes, uint32_t* err, cudaStream_t s) {
-    if (!total_chunks) return LATEC_OK;
-    k_lanes_decode<<<(total_chunks + 3) / 4, 128, 0, s>>>(st, n_stages, total_chunks, words,
-                                                          chunk_range, levels, codes, err);
+int launch_lanes_decode(const RansStageDesc* st, int n_stages, uint32_t total_blocks,
+                        int max_alphabet, const uint32_t* words, const uint64_t* chunk_range,
+                        const uint8_t* levels, uint16_t* codes, uint32_t* err, cudaStream_t s) {
+    if (!total_blocks) return LATEC_OK;
+    const int a = max_alphabet <= SMEM_ALPHA ? max_alphabet : 0;
+    const size_t smem = a ? (size_t)(a + 1) * 4 + NBUCKET * 2 : 0;
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(k_lanes_decode, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+        return LATEC_ERR_CUDA;
+    k_lanes_decode<<<total_blocks, 32 * DEC_WARPS, smem, s>>>(st, n_stages, (uint32_t)a, words,
+                                                               chunk_range, levels, codes, err);
     return last_err();
 }
 

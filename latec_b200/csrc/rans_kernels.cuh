@@ -42,15 +42,19 @@ struct RansStageDesc {
     int32_t per_point;    // 1: per-symbol table row from the levels array
     uint32_t blob_words;  // encode: computed; decode: given
     uint32_t n_out;
-    uint32_t pad;
+    uint32_t block0;      // decode: first CTA of the stage (filled by the library)
 };
+
+constexpr int DEC_WARPS = 4;             // warps (chunks) per decoder CTA
+constexpr int SMEM_ALPHA = 16384;        // largest alphabet decoded from shared memory
 
 int launch_build_tables(const uint32_t* cdf, int alphabet, int rows, EncSym* enc, uint16_t* bucket,
                         cudaStream_t st);
 int launch_lanes_encode(const RansStageDesc* st, int n_stages, uint32_t total_chunks,
                         const uint16_t* codes, const uint8_t* levels, uint32_t* scratch,
                         uint32_t* chunk_words, uint32_t* err, cudaStream_t s);
-int launch_lanes_decode(const RansStageDesc* st, int n_stages, uint32_t total_chunks,
+int launch_lanes_decode(const RansStageDesc* st, int n_stages, uint32_t total_blocks,
+                        int max_alphabet,
                         const uint32_t* words, const uint64_t* chunk_range, const uint8_t* levels,
                         uint16_t* codes, uint32_t* err, cudaStream_t s);
 int launch_stack_encode(const RansStageDesc* st, int n_stages, const uint16_t* codes,
