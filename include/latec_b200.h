@@ -186,6 +186,18 @@ int latec_rans_decode(latec_rans_stage* stages, int32_t n_stages, uint32_t total
                       uint16_t* codes, uint32_t* err, void* workspace, uint64_t workspace_bytes,
                       void* stream);
 
+/* ---- native-mode stage model fit on the device: the reference's
+ *      (level, shape) argmin (latec/rans.py:395-430) with float64 pairwise
+ *      sums. stages_host: n latec_fit_stage_size()-byte descriptors (see
+ *      fit_kernels.cu); hist_seg / hist_total as written by
+ *      latec_encode_stages; counts: device u32 scratch (sum of alphabets);
+ *      costs: device f64 scratch (n * 24 * 64); out: device f64 (3 per
+ *      stage: cost in bits, level, shape id). */
+uint64_t latec_fit_stage_size(void);
+int latec_fit_const(const void* stages_host, int32_t n, const uint32_t* hist_seg,
+                    const uint32_t* hist_total, uint32_t* counts, double* costs, double* out,
+                    void* workspace, uint64_t workspace_bytes, void* stream);
+
 /* ---- container framing on the device (latec/bitstream.py:155-164
  *      write_stream / read_stream): out = header[hlen] followed by a zstd
  *      frame of raw blocks holding the n payload bytes, and the inverse
@@ -193,7 +205,23 @@ int latec_rans_decode(latec_rans_stage* stages, int32_t n_stages, uint32_t total
 uint64_t latec_raw_frame_bytes(uint64_t payload_bytes);
 int latec_frame_raw(const uint8_t* payload, uint64_t n, const uint8_t* header, uint32_t hlen,
                     uint8_t* out, uint64_t out_cap, void* stream);
-int latec_unframe_raw(const uint8_t* frame, uint64_t n, uint8_t* payload, void* stream);
+/* err (device, may be NULL): bit 64 = a raw block header differs from the
+ * layout latec_frame_raw writes. */
+int latec_unframe_raw(const uint8_t* frame, uint64_t n, uint8_t* payload, uint32_t* err,
+                      void* stream);
+
+/* ---- stage-record walk on the device (latec/bitstream.py:288-344):
+ *      records gets n_stages entries of latec_record_size() bytes
+ *      {u64 blob, u64 out_at, u64 frame, u32 n, u32 n_out, u32 K,
+ *       u32 n_chunks, u32 chunk0, u32 status}; total_chunks (device u64) the
+ *      lane-coder chunk count. latec_chunk_ranges then writes each chunk's
+ *      (start, end) word offsets for latec_rans_decode (err bit 128: a chunk
+ *      table that does not fill its blob). */
+uint64_t latec_record_size(void);
+int latec_parse_records(const uint8_t* payload, uint64_t n_bytes, int32_t n_stages, int32_t elem,
+                        int32_t lanes, void* records, uint64_t* total_chunks, void* stream);
+int latec_chunk_ranges(const uint32_t* words, const void* records, int32_t n_stages,
+                       uint64_t* ranges, uint32_t* err, void* stream);
 
 /* Library version string. */
 const char* latec_version(void);

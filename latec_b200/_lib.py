@@ -45,6 +45,17 @@ class RansStage(ctypes.Structure):
                 ("blob_words", U32), ("n_out", U32), ("block0", U32)]
 
 
+class Record(ctypes.Structure):
+    _fields_ = [("blob", U64), ("out_at", U64), ("frame", U64), ("n", U32), ("n_out", U32),
+                ("K", U32), ("n_chunks", U32), ("chunk0", U32), ("status", U32)]
+
+
+class FitStage(ctypes.Structure):
+    _fields_ = [("counts_off", U64), ("w_table", U64), ("seg_off", U64), ("n_segs", U32),
+                ("alphabet", U32), ("kexp", I32), ("radius", I32), ("n_shapes", U32),
+                ("stage", U32), ("shape_ids", U32 * 24)]
+
+
 # Every symbol the header declares, with (restype, argtypes).
 SIGNATURES = {
     "latec_version": (ctypes.c_char_p, []),
@@ -69,9 +80,14 @@ SIGNATURES = {
     "latec_rans_encode": (ctypes.c_int, [P, I32, P, P, P, P, I32, P, U64, P, P, P, U64, P]),
     "latec_rans_decode_workspace_bytes": (U64, [I32]),
     "latec_rans_decode": (ctypes.c_int, [P, I32, U32, P, P, P, P, P, P, U64, P]),
+    "latec_fit_stage_size": (U64, []),
+    "latec_fit_const": (ctypes.c_int, [P, I32, P, P, P, P, P, P, U64, P]),
     "latec_raw_frame_bytes": (U64, [U64]),
     "latec_frame_raw": (ctypes.c_int, [P, U64, P, ctypes.c_uint32, P, U64, P]),
-    "latec_unframe_raw": (ctypes.c_int, [P, U64, P, P]),
+    "latec_unframe_raw": (ctypes.c_int, [P, U64, P, P, P]),
+    "latec_record_size": (U64, []),
+    "latec_parse_records": (ctypes.c_int, [P, U64, I32, I32, I32, P, P, P]),
+    "latec_chunk_ranges": (ctypes.c_int, [P, P, I32, P, P, P]),
 }
 
 _lib = None

@@ -171,28 +171,11 @@ class _Encoder:
             b.codes.data_ptr(), b.outliers.data_ptr(), b.stats.data_ptr(), b.hist_seg.data_ptr(),
             b.hist_total.data_ptr(), b.ws.data_ptr(), b.ws.numel(), stream), "latec_encode_stages")
         st = _stats_from_device(b, ns)
-        hist_seg = b.hist_seg.cpu().numpy().view(np.uint32).reshape(-1, 2 * rans_model.HWIN)
         t1 = time.perf_counter()
-        # ---- host model fit per stage (the reference's float32 histogram fit)
-        fits = []
-        need_total = [t for t in range(ns) if st[t].maxq >= rans_model.HWIN]
-        totals = {}
-        if need_total:
-            idx = torch.tensor(need_total, device=self.device)
-            rows = b.hist_total.view(ns, 65536)[idx].cpu().numpy().view(np.uint32)
-            totals = {t: rows[i] for i, t in enumerate(need_total)}
-        for t in range(ns):
-            n = b.items[t]
-            if n == 0:
-                fits.append((1, 0, 0, 0, 0.0))
-                continue
-            kexp = rans_model.kexp_from_maxq(st[t].maxq)
-            if kexp > 15:
-                raise ValueError("rANS coder window does not fit the stage frame")
-            seg = hist_seg[b.seg_off[t]:b.seg_off[t + 1]]
-            hist = rans_model.stage_hist_f32(n, kexp, self.radius, seg, totals.get(t))
-            level, shape, owx, bits = rans_model.fit_const_level(hist, n, kexp)
-            fits.append((kexp, level, shape, owx, bits))
+        if self.mode == _lib.RANS_LANES:
+            fits = self._fit_native(st)
+        else:
+            fits = self._fit_reference(st)
         t_fit = time.perf_counter()
         # ---- entropy stage on the device
         stages = (_lib.RansStage * ns)()
@@ -256,6 +239,73 @@ class _Encoder:
         )
         return payload, n_bytes, stage
 
+    def _fit_native(self, st):
+        """Native-mode stage model fit on the device (fit_kernels.cu)."""
+        torch = _torch()
+        b, ns = self.buf, len(self.plan)
+        idx = [t for t in range(ns) if b.items[t]]
+        fits = [(1, 0, 0, 0, 0.0)] * ns
+        if not idx:
+            return fits
+        fs = (_lib.FitStage * len(idx))()
+        meta, keep, off = [], [], 0
+        for j, t in enumerate(idx):
+            kexp = rans_model.kexp_from_maxq(st[t].maxq)
+            if kexp > 15:
+                raise ValueError("rANS coder window does not fit the stage frame")
+            owx = rans_model.choose_outlier_weight(int(st[t].n_out), b.items[t])
+            w, ids = rans_model.device_weights.get(kexp, owx, self.device)
+            keep.append(w)
+            f = fs[j]
+            f.counts_off, f.w_table = off, w.data_ptr()
+            f.seg_off, f.n_segs = int(b.seg_off[t]), int(b.segs[t])
+            f.alphabet, f.kexp, f.radius = 2 << kexp, kexp, int(self.radius)
+            f.n_shapes, f.stage = len(ids), t
+            for k, sid in enumerate(ids):
+                f.shape_ids[k] = sid
+            off += 2 << kexp
+            meta.append((kexp, owx))
+        n = len(idx)
+        counts = torch.empty(off, dtype=torch.int32, device=self.device)
+        costs = torch.empty(n * 24 * 64, dtype=torch.float64, device=self.device)
+        out = torch.empty(n * 3, dtype=torch.float64, device=self.device)
+        ws = torch.empty(n * ctypes.sizeof(_lib.FitStage) + 256, dtype=torch.uint8, device=self.device)
+        _lib.check(self.lib.latec_fit_const(fs, n, b.hist_seg.data_ptr(), b.hist_total.data_ptr(),
+                                            counts.data_ptr(), costs.data_ptr(), out.data_ptr(),
+                                            ws.data_ptr(), ws.numel(), _lib.stream_ptr()),
+                   "latec_fit_const")
+        res = out.cpu().numpy().reshape(n, 3)
+        for j, t in enumerate(idx):
+            kexp, owx = meta[j]
+            fits[t] = (kexp, int(res[j, 1]), int(res[j, 2]), owx, float(res[j, 0]))
+        return fits
+
+    def _fit_reference(self, st):
+        """The reference's float32 fit on the host (compat streams)."""
+        torch = _torch()
+        b, ns = self.buf, len(self.plan)
+        hist_seg = b.hist_seg.cpu().numpy().view(np.uint32).reshape(-1, 2 * rans_model.HWIN)
+        need_total = [t for t in range(ns) if st[t].maxq >= rans_model.HWIN]
+        totals = {}
+        if need_total:
+            rows = b.hist_total.view(ns, 65536)[torch.tensor(need_total, device=self.device)]
+            rows = rows.cpu().numpy().view(np.uint32)
+            totals = {t: rows[i] for i, t in enumerate(need_total)}
+        fits = []
+        for t in range(ns):
+            n = b.items[t]
+            if n == 0:
+                fits.append((1, 0, 0, 0, 0.0))
+                continue
+            kexp = rans_model.kexp_from_maxq(st[t].maxq)
+            if kexp > 15:
+                raise ValueError("rANS coder window does not fit the stage frame")
+            seg = hist_seg[b.seg_off[t]:b.seg_off[t + 1]]
+            hist = rans_model.stage_hist_f32(n, kexp, self.radius, seg, totals.get(t))
+            level, shape, owx, bits = rans_model.fit_const_level(hist, n, kexp)
+            fits.append((kexp, level, shape, owx, bits))
+        return fits
+
     def to_stream(self, payload, n_bytes, header: bytes, stage):
         """Container bytes: native streams are framed on the device and copied
         once through pinned memory; compat streams take the reference's
@@ -269,10 +319,13 @@ class _Encoder:
             _lib.check(self.lib.latec_frame_raw(payload.data_ptr(), n_bytes, hdr.data_ptr(),
                                                 len(header), out.data_ptr(), total,
                                                 _lib.stream_ptr()), "latec_frame_raw")
-            pin = _lib.pinned(total, "stream_out")
-            pin[:total].copy_(out, non_blocking=True)
-            torch.cuda.current_stream().synchronize()
-            stream = bytes(pin[:total].numpy())
+            if getattr(self, "stream_out", "bytes") == "device":
+                stream = out
+            else:
+                pin = _lib.pinned(total, "stream_out")
+                pin[:total].copy_(out, non_blocking=True)
+                torch.cuda.current_stream().synchronize()
+                stream = bytes(pin[:total].numpy())
         else:
             host = payload[:n_bytes].cpu().numpy()
             host = self._compat_literals(host, stage["stage_fit"])
@@ -356,7 +409,7 @@ def _is_gpu_interp(predictor):
 
 def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, radius=1 << 15,
              zstd_level=9, eb_ratio=None, tune="fast", tune_size_slack=1.05, verbose=False, *,
-             entropy="native", device=None, recon="auto"):
+             entropy="native", device=None, recon="auto", stream_out="bytes"):
     """Compress an image or an arbitrary-rank scalar field; returns ``(stream, stats)``.
 
     Mirrors ``latec/codec.py:45-285``. ``img`` may be a NumPy array or a torch
@@ -369,6 +422,10 @@ def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, rad
     _lib.load()
     if entropy not in ("native", "compat"):
         raise ValueError("entropy must be 'native' or 'compat'")
+    if stream_out not in ("bytes", "device"):
+        raise ValueError("stream_out must be 'bytes' or 'device'")
+    if stream_out == "device" and entropy != "native":
+        raise ValueError("device streams use the native entropy mode")
     if not eb > 0:
         raise ValueError(f"error bound must be > 0, got {eb}")
     _check_radius(radius)
@@ -397,6 +454,7 @@ def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, rad
     order = predictor.order
     enc = _Encoder(field, spatial, c, src, levels, anchor_stride, anchor_block, radius, order,
                    entropy, zstd_level, dev)
+    enc.stream_out = stream_out
     flags = getattr(predictor, "stream_flag", 0)
     if entropy == "native":
         flags |= FLAG_LANES
@@ -489,27 +547,8 @@ def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, rad
         stats["recon"] = _finalize(canvas, src, c, as_numpy=(mode == "numpy"))
     nbytes = img.nbytes if not _is_tensor(img) else img.numel() * img.element_size()
     stats["original_bytes"] = int(nbytes)
-    stats["ratio"] = nbytes / len(stream)
+    stats["ratio"] = nbytes / (stream.numel() if _is_tensor(stream) else len(stream))
     return stream, stats
-
-
-def _parse_records(reader, ns, elem):
-    """Walk the stage records (``latec/bitstream.py:288-344`` framing)."""
-    recs, off = [], 0
-    for _ in range(ns):
-        n, word = reader.unpack("<IQ", off)
-        f = bitstream.unpack_frame(word)
-        blob = off + 12
-        (n_out,) = reader.unpack("<I", blob + f["hlen"])
-        out_at = blob + f["hlen"] + 4
-        end = out_at + elem * n_out
-        if end > len(reader):
-            raise ValueError("truncated stage record")
-        recs.append(dict(f, n=n, blob=blob, n_out=n_out, out_at=out_at))
-        off = end
-    if off != len(reader):
-        raise ValueError("trailing data after the last stage record")
-    return recs
 
 
 def _upload_stream(body, dev):
@@ -524,16 +563,45 @@ def _upload_stream(body, dev):
     return d
 
 
+def _raw_frame_size(head13: bytes, n_body: int):
+    """Payload size when the body is a raw-block frame of the native layout."""
+    if len(head13) < 13 or head13[:5] != struct.pack("<IB", 0xFD2FB528, 0xE0):
+        return None
+    (n,) = struct.unpack_from("<Q", head13, 5)
+    nblk = max(1, -(-n // (1 << 17)))
+    return int(n) if n_body == 13 + 3 * nblk + n else None
+
+
+_STATUS = {1: "truncated stage record", 2: "truncated stage record", 3: "truncated stage record",
+           4: "rANS payload is not aligned to 32-bit words", 5: "lane coder blob has K = 0",
+           6: "truncated lane-coder chunk table", 7: "trailing data after the last stage record"}
+
+
 def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
-    """Decompress a LATEC stream (``latec/codec.py:288-322``). ``out="device"``
-    returns a CUDA tensor instead of a NumPy array."""
+    """Decompress a LATEC stream (``latec/codec.py:288-322``).
+
+    ``stream`` is ``bytes`` (or any buffer) or a CUDA ``uint8`` tensor; the
+    stage records are parsed, entropy-decoded and dequantized on the device.
+    ``out="device"`` returns a CUDA tensor instead of a NumPy array."""
     torch = _torch()
     lib = _lib.load()
     from . import levels as _levels
     from .predictor import InterpPredictor
 
-    header = Header.unpack(stream)
-    body = np.frombuffer(memoryview(stream)[header.size:], np.uint8)
+    is_dev = _is_tensor(stream) and stream.is_cuda
+    if is_dev:
+        if stream.dtype != torch.uint8 or stream.dim() != 1:
+            raise ValueError("a device stream must be a 1-D uint8 tensor")
+        n_total = stream.numel()
+        prefix = stream[:min(n_total, 4096)].cpu().numpy().tobytes()
+        dev = stream.device
+    else:
+        mv = memoryview(stream).cast("B")
+        n_total = len(mv)
+        prefix = mv[:min(n_total, 4096)].tobytes()
+        dev = torch.device(device) if device is not None else torch.device(
+            "cuda", torch.cuda.current_device())
+    header = Header.unpack(prefix)
     if header.flags & FLAG_RANS:
         raise NotImplementedError("per-point scale streams are decoded by GNNCodec.uncompress")
     if predictor_factory is None:
@@ -553,7 +621,6 @@ def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
     if header.src_dtype not in DTYPE_CODES:
         raise KeyError(header.src_dtype)
     _check_radius(header.radius)
-    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     spatial, c = tuple(header.spatial), int(header.channels)
     if c < 1:
         raise ValueError("stream has no channels")
@@ -562,123 +629,122 @@ def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
     ebs = _levels.stage_ebs(spatial, header.levels, header.anchor_stride, header.anchor_block,
                             header.eb, header.eb_ratio)
     elem = 8 if header.src_dtype == 2 else 4
-    n_raw = bitstream.raw_frame_size(body)
-    if n_raw is not None:  # native frames: unframe on the device, read headers in place
-        reader = bitstream.PayloadReader(body, n_raw, framed=True)
-        frame_dev = _upload_stream(body, dev)
-        pay_dev = torch.empty(n_raw + 4 + (-n_raw) % 4, dtype=torch.uint8, device=dev)
-        pay_dev.zero_()
-        _lib.check(lib.latec_unframe_raw(frame_dev.data_ptr(), n_raw, pay_dev.data_ptr(),
-                                         _lib.stream_ptr()), "latec_unframe_raw")
+    mode = _lib.RANS_LANES if header.flags & FLAG_LANES else _lib.RANS_COMPAT
+    sp = _lib.stream_ptr()
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    # ---- payload on the device
+    n_body = n_total - header.size
+    n_raw = _raw_frame_size(prefix[header.size:header.size + 13], n_body)
+    if n_raw is not None:
+        if is_dev:
+            frame_dev = stream[header.size:]
+        else:
+            frame_dev = _upload_stream(np.frombuffer(mv[header.size:], np.uint8), dev)
+        n_pay = n_raw
+        pay_dev = torch.zeros(n_pay + 8 + (-n_pay) % 4, dtype=torch.uint8, device=dev)
+        _lib.check(lib.latec_unframe_raw(frame_dev.data_ptr(), n_pay, pay_dev.data_ptr(),
+                                         err.data_ptr(), sp), "latec_unframe_raw")
         del frame_dev
     else:
+        body = (stream[header.size:].cpu().numpy() if is_dev
+                else np.frombuffer(mv[header.size:], np.uint8))
         payload = bitstream.zstd().decompress_into(body)
-        reader = bitstream.PayloadReader(payload, len(payload), framed=False)
+        n_pay = len(payload)
         pay_dev = _upload_stream(payload, dev)
-    recs = _parse_records(reader, ns, elem)
-    mode = _lib.RANS_LANES if header.flags & FLAG_LANES else _lib.RANS_COMPAT
+    # ---- stage records, parsed on the device
+    rec_dev = torch.empty(ns * ctypes.sizeof(_lib.Record), dtype=torch.uint8, device=dev)
+    tc_dev = torch.zeros(1, dtype=torch.int64, device=dev)
+    _lib.check(lib.latec_parse_records(pay_dev.data_ptr(), n_pay, ns, elem,
+                                       int(mode == _lib.RANS_LANES), rec_dev.data_ptr(),
+                                       tc_dev.data_ptr(), sp), "latec_parse_records")
+    recs = (_lib.Record * ns).from_buffer_copy(rec_dev.cpu().numpy().tobytes())
+    total_chunks = int(tc_dev.item())
+    if int(err.item()) & 64:
+        raise ValueError("zstd frame is corrupt")
     items = [n * c for n in plan.counts]
     offsets = np.concatenate([[0], np.cumsum(items)]).astype(np.int64)
+    frames = []
     for t in range(ns):
-        if recs[t]["n"] != items[t]:
+        if recs[t].status:
+            raise ValueError(_STATUS.get(recs[t].status, "malformed stage record"))
+        f = bitstream.unpack_frame(int(recs[t].frame))
+        if recs[t].n != items[t]:
             raise ValueError("stage code count mismatch")
-        if not recs[t]["kexp"]:
+        if not f["kexp"]:
             raise ValueError("rANS stage record has no coder window")
-    aligned = all(r["blob"] % 4 == 0 for r in recs if not r["literal"])
-    if aligned:
-        words_dev = pay_dev
-        blob_word = [r["blob"] // 4 for r in recs]
-    else:  # literal stages broke the word alignment: gather the rANS blobs
-        pieces, blob_word, at = [], [], 0
-        for r in recs:
-            nw = 0 if r["literal"] else -(-r["hlen"] // 4)
-            pieces.append(np.asarray(reader.take(r["blob"], 4 * nw)))
-            blob_word.append(at)
+        if recs[t].n == 0 and f["hlen"]:
+            raise ValueError("non-empty rANS blob for an empty stage")
+        frames.append(f)
+    aligned = all(recs[t].blob % 4 == 0 for t in range(ns) if not frames[t]["literal"])
+    blob_word = [recs[t].blob // 4 for t in range(ns)]
+    words_dev = pay_dev
+    if not aligned:  # literal stages broke the word alignment: gather the rANS blobs
+        pieces, at = [], 0
+        for t in range(ns):
+            nw = 0 if frames[t]["literal"] else -(-frames[t]["hlen"] // 4)
+            pieces.append(pay_dev[recs[t].blob:recs[t].blob + 4 * nw])
+            blob_word[t] = at
             at += nw
-        words_host = np.concatenate(pieces + [np.zeros(4, np.uint8)])
-        words_dev = torch.from_numpy(words_host).to(dev)
+        words_dev = torch.cat(pieces + [torch.zeros(8, dtype=torch.uint8, device=dev)])
+    ranges = None
+    if mode == _lib.RANS_LANES and total_chunks:
+        ranges = torch.empty(2 * total_chunks, dtype=torch.int64, device=dev)
+        _lib.check(lib.latec_chunk_ranges(words_dev.data_ptr(), rec_dev.data_ptr(), ns,
+                                          ranges.data_ptr(), err.data_ptr(), sp),
+                   "latec_chunk_ranges")
     stages = (_lib.RansStage * ns)()
-    keep, ranges, literal_codes = [], [], {}
-    chunk = 0
+    keep, literal_codes = [], {}
     for t in range(ns):
-        r, d = recs[t], stages[t]
+        r, f, d = recs[t], frames[t], stages[t]
         d.codes_off = int(offsets[t])
-        d.n = r["n"]
-        d.kexp, d.radius, d.mode = r["kexp"], int(header.radius), mode
-        d.alphabet = 1 << (r["kexp"] + 1)
-        d.chunk0 = chunk
-        if r["n"] == 0:
-            if r["hlen"]:
-                raise ValueError("non-empty rANS blob for an empty stage")
+        d.n = r.n
+        d.kexp, d.radius, d.mode = f["kexp"], int(header.radius), mode
+        d.alphabet = 1 << (f["kexp"] + 1)
+        d.chunk0, d.n_chunks, d.K = r.chunk0, r.n_chunks, r.K
+        if r.n == 0:
             continue
-        if r["literal"]:
-            syms = np.frombuffer(bitstream.zstd().decompress_into(
-                reader.take(r["blob"], r["hlen"])).tobytes(),
-                rans_model.literal_dtype(r["kexp"]), count=r["n"])
-            literal_codes[t] = rans_model.widen(syms, header.radius, r["kexp"]).astype(np.uint16)
-            d.mode = mode
+        if f["literal"]:
+            blob = pay_dev[r.blob:r.blob + f["hlen"]].cpu().numpy()
+            syms = np.frombuffer(bitstream.zstd().decompress_into(blob).tobytes(),
+                                 rans_model.literal_dtype(f["kexp"]), count=r.n)
+            literal_codes[t] = rans_model.widen(syms, header.radius, f["kexp"]).astype(np.uint16)
             d.n = 0
             continue
-        if r["hlen"] % 4:
+        if f["hlen"] % 4:
             raise ValueError("rANS payload is not aligned to 32-bit words")
-        cdf, enc, bucket, _ = rans_model.device_tables.get(mode, r["kexp"], r["shape"], r["owx"],
-                                                           r["level"], dev)
+        cdf, enc, bucket, _ = rans_model.device_tables.get(mode, f["kexp"], f["shape"], f["owx"],
+                                                           f["level"], dev)
         keep.append((cdf, enc, bucket))
         d.cdf, d.enc, d.bucket = cdf.data_ptr(), enc.data_ptr(), bucket.data_ptr()
         d.blob_off = blob_word[t]
-        d.blob_words = r["hlen"] // 4
-        if mode == _lib.RANS_LANES:
-            w0 = blob_word[t]
-            if d.blob_words < 1:
-                raise ValueError("truncated lane-coder blob")
-            K = int(reader.u32s(r["blob"], 1)[0])
-            if K < 1:
-                raise ValueError("lane coder blob has K = 0")
-            nc = -(-r["n"] // (32 * K))
-            if 1 + nc > d.blob_words:
-                raise ValueError("truncated lane-coder chunk table")
-            cw = reader.u32s(r["blob"] + 4, nc).astype(np.uint64)
-            starts = w0 + 1 + nc + np.concatenate([[0], np.cumsum(cw)[:-1]]).astype(np.uint64)
-            ends = starts + cw
-            if int(ends[-1]) != w0 + d.blob_words:
-                raise ValueError("lane-coder chunk table does not match the blob length")
-            ranges.append(np.stack([starts, ends], 1).reshape(-1))
-            d.K, d.n_chunks = K, nc
-            chunk += nc
-    total_chunks = chunk
-    rng_dev = torch.from_numpy(np.concatenate(ranges).astype(np.uint64).view(np.int64)).to(dev) \
-        if ranges else None
+        d.blob_words = f["hlen"] // 4
     codes = torch.empty(max(int(offsets[-1]), 1), dtype=torch.int16, device=dev)
-    err = torch.zeros(1, dtype=torch.int32, device=dev)
-    wsb = lib.latec_rans_decode_workspace_bytes(ns)
-    ws = torch.empty(int(wsb), dtype=torch.uint8, device=dev)
-    stream_p = _lib.stream_ptr()
+    ws = torch.empty(int(lib.latec_rans_decode_workspace_bytes(ns)), dtype=torch.uint8, device=dev)
     _lib.check(lib.latec_rans_decode(stages, ns, total_chunks, words_dev.data_ptr(),
-                                     rng_dev.data_ptr() if rng_dev is not None else None, None,
+                                     ranges.data_ptr() if ranges is not None else None, None,
                                      codes.data_ptr(), err.data_ptr(), ws.data_ptr(), ws.numel(),
-                                     stream_p), "latec_rans_decode")
+                                     sp), "latec_rans_decode")
     for t, lc in literal_codes.items():
         codes[int(offsets[t]):int(offsets[t + 1])].copy_(torch.from_numpy(lc.view(np.int16)).to(dev))
-    del keep
     ldt = _lib.F64 if header.src_dtype == 2 else _lib.F32
-    prm = _qparams(header.src_dtype, c, header.radius,
-                   "cubic" if predictor.order == "cubic" else "linear", predictor.center,
+    prm = _qparams(header.src_dtype, c, header.radius, predictor.order, predictor.center,
                    predictor.end_mode, header.src_dtype == 0)
     ft = torch.float64 if header.src_dtype == 2 else torch.float32
     recon = torch.zeros((c,) + spatial, dtype=ft, device=dev)
     eb_arr = (ctypes.c_double * ns)(*[float(e) for e in ebs])
-    out_off = (ctypes.c_uint64 * ns)(*[r["out_at"] for r in recs])
-    n_out = (ctypes.c_uint32 * ns)(*[r["n_out"] for r in recs])
-    wsb2 = lib.latec_stage_workspace_bytes(plan.handle, c, ldt)
-    ws2 = torch.empty(max(int(wsb2), 1), dtype=torch.uint8, device=dev)
+    out_off = (ctypes.c_uint64 * ns)(*[recs[t].out_at for t in range(ns)])
+    n_out = (ctypes.c_uint32 * ns)(*[recs[t].n_out for t in range(ns)])
+    ws2 = torch.empty(max(int(lib.latec_stage_workspace_bytes(plan.handle, c, ldt)), 1),
+                      dtype=torch.uint8, device=dev)
     _lib.check(lib.latec_decode_stages(plan.handle, ctypes.byref(prm), eb_arr, codes.data_ptr(),
                                        pay_dev.data_ptr(), out_off, n_out, recon.data_ptr(),
-                                       err.data_ptr(), ws2.data_ptr(), ws2.numel(), stream_p),
+                                       err.data_ptr(), ws2.data_ptr(), ws2.numel(), sp),
                "latec_decode_stages")
     e = int(err.item())
+    del keep
     if e & 1:
         raise ValueError("outlier count mismatch")
-    if e & (4 | 8):
+    if e & (4 | 8 | 128):
         raise ValueError("trailing data in rANS payload")
     if e & 16:
         raise ValueError("malformed rANS payload")

@@ -292,3 +292,34 @@ class DeviceTables:
 
 
 device_tables = DeviceTables()
+
+
+class DeviceWeights:
+    """Device copies of the stacked -log2 weight tables of every dictionary
+    entry the encoder considers, ``(n_shapes, 64, alphabet)`` float32, keyed by
+    ``(kexp, owx)`` (the native-mode fit's operand)."""
+
+    def __init__(self, budget_bytes=1 << 30):
+        self.budget, self.used = budget_bytes, 0
+        self.cache: "OrderedDict[tuple, tuple]" = OrderedDict()
+
+    def get(self, kexp, owx, device):
+        import torch
+
+        key = (kexp, owx, str(device))
+        hit = self.cache.get(key)
+        if hit is not None:
+            self.cache.move_to_end(key)
+            return hit
+        ids = shape_ids(kexp)
+        w = np.stack([neg_log2_weights(kexp, sid, owx) for sid in ids])
+        t = torch.from_numpy(np.ascontiguousarray(w)).to(device)
+        self.cache[key] = (t, ids)
+        self.used += t.numel() * 4
+        while len(self.cache) > 1 and self.used > self.budget:
+            _, old = self.cache.popitem(last=False)
+            self.used -= old[0].numel() * 4
+        return t, ids
+
+
+device_weights = DeviceWeights()

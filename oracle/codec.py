@@ -11,8 +11,9 @@ Two entropy modes, selected by the container flag ``FLAG_LANES``:
   around the payload.
 * ``"native"`` -- the CUDA library's stream: the same stage records, but each
   rANS blob is the 32-lane interleaved coder of ``oracle/ans.c`` with the
-  reference's own 24-bit tables, no literal stages, and the payload stored in
-  a zstd frame of raw blocks (decodable by any zstd decoder).
+  reference's own 24-bit tables, the stage model fitted with float64 pairwise
+  sums (``rans_model.fit_const_native``), no literal stages, and the payload
+  stored in a zstd frame of raw blocks (decodable by any zstd decoder).
 
 float64 input (new; the reference raises on it) uses dtype id 2, keeps the
 reconstruction, the predictions and the outliers in float64 and checks the
@@ -174,7 +175,11 @@ def pack_stage(codes, outliers, radius, mode, zstd_level=9):
     """Stage record; ``latec/bitstream.py:178-243`` (stage-constant path)."""
     codes = np.asarray(codes, np.uint32)
     kexp = rans_model.choose_kexp(codes, radius)
-    level, shape, owx, bits = rans_model.choose_const_level(codes, radius, kexp)
+    if mode == "native" and len(codes):
+        counts = np.bincount(rans_model.narrow(codes, radius, kexp), minlength=2 << kexp)
+        level, shape, owx, bits = rans_model.fit_const_native(counts, len(codes), kexp)
+    else:
+        level, shape, owx, bits = rans_model.choose_const_level(codes, radius, kexp)
     literal = False
     blob = None
     syms = rans_model.narrow(codes, radius, kexp) if len(codes) else np.zeros(0, np.int64)

@@ -87,7 +87,7 @@ def level_weights(kexp, n_levels=N_LEVELS):
     return w
 
 
-@lru_cache(maxsize=32)
+@lru_cache(maxsize=256)
 def shaped_weights(kexp, shape, n_levels=N_LEVELS):
     """``latec/rans.py:376-384``."""
     weights = level_weights(kexp, n_levels)
@@ -143,7 +143,7 @@ def quantize_pmf_rows(weights, total):
     return pmf.astype(np.uint32)
 
 
-@lru_cache(maxsize=16)
+@lru_cache(maxsize=256)
 def build_cdfs(kexp, shape=0, n_levels=N_LEVELS, precision=PRECISION, owx=0):
     """``(n_levels, alphabet + 1)`` uint32 CDFs; ``latec/rans.py:304-329``."""
     span = (1 << kexp) - 1
@@ -156,7 +156,7 @@ def build_cdfs(kexp, shape=0, n_levels=N_LEVELS, precision=PRECISION, owx=0):
     return cdfs
 
 
-@lru_cache(maxsize=16)
+@lru_cache(maxsize=256)
 def neg_log2_weights(kexp, shape, n_levels=N_LEVELS, precision=PRECISION, owx=0):
     """``latec/rans.py:387-392``."""
     weights = with_outlier_weight(shaped_weights(kexp, shape, n_levels), owx)
@@ -262,3 +262,23 @@ def model_bits(codes, levels64, radius, kexp, shape=0):
             cdf = cdfs[level]
             probs[idx] = cdf[s + 1].astype(np.int64) - cdf[s].astype(np.int64)
     return float((-np.log2(probs / (1 << PRECISION))).sum())
+
+
+def fit_const_native(counts, n_codes, kexp, n_levels=N_LEVELS, precision=PRECISION):
+    """Stage-constant fit of the native entropy mode: the reference's model
+    space and selection rule (``latec/rans.py:421-430``) with every cost a
+    float64 pairwise tree sum of correctly rounded products
+    ``f64(W[level, sym]) * f64(count[sym])`` over the power-of-two alphabet."""
+    counts = np.asarray(counts, np.float64)
+    owx = choose_outlier_weight(int(counts[0]), n_codes)
+    best = (np.inf, 0, 0)
+    for sid in shape_ids(int(kexp)):
+        p = neg_log2_weights(int(kexp), int(sid), n_levels, precision, owx).astype(np.float64)
+        p = p * counts[None, :]
+        while p.shape[1] > 1:
+            p = p[:, 0::2] + p[:, 1::2]
+        cost = p[:, 0]
+        level = int(cost.argmin())
+        if cost[level] < best[0]:
+            best = (float(cost[level]), level, int(sid))
+    return best[1], best[2], owx, best[0]

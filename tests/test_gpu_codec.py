@@ -255,3 +255,23 @@ def test_empty_stages_and_tiny_grids():
         ostream, _ = ocodec.compress(x, 1e-3, levels_=lv, anchor_stride=stride, mode="native")
         assert stream == ostream
         assert np.abs(lb.decompress(stream) - x).max() <= 1e-3
+
+
+def test_device_stream_roundtrip_equals_host_stream():
+    """stream_out="device" keeps the container in HBM: same bytes as the host
+    stream, decodable from the tensor without host copies of the payload."""
+    import torch
+
+    from latec_b200 import fields
+
+    x = fields.turbulence_jumps((70, 64, 50), seed=12)
+    lb = _lb()
+    s_host, st = lb.compress(x, 1e-3, lb.InterpPredictor("cubic", 4, 16, 1), levels=4,
+                             anchor_stride=16)
+    xd = torch.from_numpy(x).cuda()
+    s_dev, st2 = lb.compress(xd, 1e-3, lb.InterpPredictor("cubic", 4, 16, 1), levels=4,
+                             anchor_stride=16, stream_out="device")
+    assert s_dev.is_cuda and bytes(s_dev.cpu().numpy()) == s_host
+    back = lb.decompress(s_dev, out="device")
+    assert torch.equal(back, st2["recon"])
+    assert np.array_equal(lb.decompress(s_host), st["recon"])

@@ -112,7 +112,7 @@ def test_codec_stages_match_reference(name):
         x, m["eb"], order=m["order"], levels_=ck["levels"], anchor_stride=ck["anchor_stride"],
         anchor_block=ck["anchor_block"], radius=ck.get("radius", 1 << 15),
         eb_ratio=ck.get("eb_ratio"), center=pk.get("center"), end_mode=pk.get("end_mode"),
-        mode="native")
+        mode="compat")
     assert (st["center"], st["end_mode"], st["eb_ratio"]) == (m["center"], m["end_mode"], m["eb_ratio"])
     assert len(st["stages"]) == len(m["stages"])
     for t, (got, want) in enumerate(zip(st["stages"], m["stages"])):
