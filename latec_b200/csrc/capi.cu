@@ -274,7 +274,7 @@ int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
         if (!rc)
             rc = launch_interp_dequant(d, q, prm->dtype, t == 0, codes + off,
                                        outliers ? (const uint8_t*)outliers + out_off[t] : nullptr,
-                                       w.tile_off, n_out[t], recon, err, st);
+                                       w.tile_cnt, w.tile_off, n_out[t], recon, err, st);
         if (rc) return rc;
         off += items;
     }

@@ -68,22 +68,34 @@ __device__ __forceinline__ double axis_interp(const T* __restrict__ rc, int64_t 
 
 // Prediction of one stage point from its own odd axes (center combine of
 // latec/predictor.py:286-314; terms of even axes are exact zeros there).
-template <typename T>
+// ND/KIND/CUBIC specialise the rank, the stage layout and the interpolation
+// order at compile time (ND == 0: runtime rank).
+template <typename T, int ND, int KIND, int CUBIC>
 __device__ __forceinline__ double predict_point(const StageDesc& d, const QParams& q,
                                                 const T* __restrict__ rc, int64_t flat,
                                                 const int32_t* coord) {
-    if (d.kind == 0) {
-        const int a = d.axis;
-        return axis_interp(rc, flat, coord[a], d.shape[a], d.gstride[a], d.s, q.order, q.end_mode);
+    constexpr int NDV = ND > 0 ? ND : MAXD;
+    if (KIND == 0) {
+        int ca = 0, na = 1;
+        int64_t gs = 0;
+#pragma unroll
+        for (int j = 0; j < NDV; j++) {
+            if (j == d.axis) {
+                ca = coord[j];
+                na = d.shape[j];
+                gs = d.gstride[j];
+            }
+        }
+        return axis_interp(rc, flat, ca, na, gs, d.s, CUBIC, q.end_mode);
     }
     if (q.center == 0) {
         double total = 0.0;
         int cnt = 0;
 #pragma unroll
-        for (int j = 0; j < MAXD; j++) {
-            if (j < d.ndim && (coord[j] & d.s)) {
-                double v = axis_interp(rc, flat, coord[j], d.shape[j], d.gstride[j], d.s, q.order,
-                                       q.end_mode);
+        for (int j = 0; j < NDV; j++) {
+            if ((ND > 0 || j < d.ndim) && (coord[j] & d.s)) {
+                const double v = axis_interp(rc, flat, coord[j], d.shape[j], d.gstride[j], d.s,
+                                             CUBIC, q.end_mode);
                 total = cnt ? __dadd_rn(total, v) : v;
                 cnt++;
             }
@@ -93,15 +105,19 @@ __device__ __forceinline__ double predict_point(const StageDesc& d, const QParam
         if (cnt == 4) return total * 0.25;
         return __ddiv_rn(total, (double)cnt);
     }
-    int pick = -1;
+    int ca = 0, na = 1;
+    int64_t gs = 0;
+    bool found = false;
 #pragma unroll
-    for (int j = 0; j < MAXD; j++) {
-        if (j < d.ndim && (coord[j] & d.s)) {
-            if (q.center == 2 || pick < 0) pick = j;
+    for (int j = 0; j < NDV; j++) {
+        if ((ND > 0 || j < d.ndim) && (coord[j] & d.s) && (q.center == 2 || !found)) {
+            ca = coord[j];
+            na = d.shape[j];
+            gs = d.gstride[j];
+            found = true;
         }
     }
-    return axis_interp(rc, flat, coord[pick], d.shape[pick], d.gstride[pick], d.s, q.order,
-                       q.end_mode);
+    return axis_interp(rc, flat, ca, na, gs, d.s, CUBIC, q.end_mode);
 }
 
 // rint((x - p) / w) with the division's exact rounding: the reciprocal
@@ -252,7 +268,10 @@ __device__ __forceinline__ void hist_add(uint32_t* sh_hist, uint32_t* hist_total
 }
 
 // ---------------------------------------------------------------- encode
-template <typename T>
+// One CTA walks TILES_PER_BLOCK consecutive tiles of the stage's ranks; each
+// thread handles ranks tile + k * THREADS + tid (coalesced codes). The inner
+// loop has no block barrier: outlier counts go to per-tile shared counters.
+template <typename T, int ND, int KIND, int CUBIC>
 __global__ void __launch_bounds__(THREADS)
     k_interp_quant(const StageDesc d, const QParams q, const int is_anchor,
                    const T* __restrict__ x, T* __restrict__ recon, uint16_t* __restrict__ codes,
@@ -260,20 +279,22 @@ __global__ void __launch_bounds__(THREADS)
                    uint32_t* __restrict__ hist_total, uint32_t* __restrict__ hist_seg,
                    StageAcc* __restrict__ acc, double* __restrict__ partials) {
     __shared__ uint32_t sh_hist[HBINS];
+    __shared__ uint32_t sh_tile[TILES_PER_BLOCK];
     for (int b = threadIdx.x; b < HBINS; b += THREADS) sh_hist[b] = 0;
+    if (threadIdx.x < TILES_PER_BLOCK) sh_tile[threadIdx.x] = 0;
     __syncthreads();
     const uint64_t items = (uint64_t)q.channels * d.n;
     const uint64_t block_base = (uint64_t)blockIdx.x * BLOCK_PTS;
+    const int lane = threadIdx.x & 31;
     BlockAcc a{{0, 0, 0, 0, 0}, 0};
     for (int t = 0; t < TILES_PER_BLOCK; t++) {
         const uint64_t tile_base = block_base + (uint64_t)t * TILE;
         if (tile_base >= items) break;
-        int outl = 0;
-#pragma unroll 1
+        uint32_t outl = 0;
+#pragma unroll 2
         for (int k = 0; k < TILE / THREADS; k++) {
             const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
-            bool is_out = false;
-            int key = -1;  // histogram bin of this lane's code (-1 none, -2 outside window)
+            int key = -1;  // histogram bin (-1 none, -2 outside the window)
             uint32_t code = 0;
             if (i < items) {
                 uint32_t c = 0, rank = (uint32_t)i;
@@ -281,19 +302,20 @@ __global__ void __launch_bounds__(THREADS)
                     c = (uint32_t)(i / d.n);
                     rank = (uint32_t)(i - (uint64_t)c * d.n);
                 }
-                int32_t coord[MAXD];
-                const int64_t flat = stage_coords(d, rank, coord);
+                int32_t coord[ND > 0 ? ND : MAXD];
+                const int64_t flat = stage_coords_t<ND, KIND>(d, rank, coord);
                 T* rc = recon + (uint64_t)c * q.points;
-                const double pd = is_anchor ? 0.0 : predict_point<T>(d, q, rc, flat, coord);
+                const double pd =
+                    is_anchor ? 0.0 : predict_point<T, ND, KIND, CUBIC>(d, q, rc, flat, coord);
                 const T xv = x[(uint64_t)c * q.points + flat];
                 T rv;
                 const QOut o = Quant<T>::run(xv, pd, q, rv);
                 rc[flat] = rv;
                 code = o.code;
                 codes[i] = (uint16_t)o.code;
-                is_out = o.code == 0;
-                if (is_out) staging[i] = xv;
-                if (is_out) {
+                if (!o.code) {
+                    staging[i] = xv;
+                    outl++;
                     key = 0;
                 } else {
                     const uint32_t aq = (uint32_t)abs(o.qv);
@@ -310,14 +332,18 @@ __global__ void __launch_bounds__(THREADS)
             }
             // warp-aggregated histogram: one shared atomic per distinct bin
             const unsigned same = __match_any_sync(0xffffffffu, key);
-            if (key >= 0 && (threadIdx.x & 31) == __ffs(same) - 1)
-                atomicAdd(&sh_hist[key], (uint32_t)__popc(same));
+            if (key >= 0 && lane == __ffs(same) - 1) atomicAdd(&sh_hist[key], (uint32_t)__popc(same));
             if (key == -2) atomicAdd(&hist_total[code], 1u);
-            outl += __syncthreads_count(is_out);
         }
-        if (threadIdx.x == 0) tile_cnt[tile_base / TILE] = (uint32_t)outl;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) outl += __shfl_xor_sync(0xffffffffu, outl, o);
+        if (lane == 0 && outl) atomicAdd(&sh_tile[t], outl);
     }
     __syncthreads();
+    if (threadIdx.x < TILES_PER_BLOCK) {
+        const uint64_t tb = block_base + (uint64_t)threadIdx.x * TILE;
+        if (tb < items) tile_cnt[tb / TILE] = sh_tile[threadIdx.x];
+    }
     block_finish(a, sh_hist, hist_seg, block_base, acc, partials);
 }
 
@@ -371,7 +397,7 @@ __global__ void __launch_bounds__(THREADS)
 }
 
 // Prediction only (the predictor plugin's ``predict``): compact output.
-template <typename T>
+template <typename T, int ND, int KIND, int CUBIC>
 __global__ void __launch_bounds__(THREADS)
     k_interp_predict(const StageDesc d, const QParams q, const T* __restrict__ recon,
                      T* __restrict__ pred) {
@@ -383,10 +409,10 @@ __global__ void __launch_bounds__(THREADS)
         c = (uint32_t)(i / d.n);
         rank = (uint32_t)(i - (uint64_t)c * d.n);
     }
-    int32_t coord[MAXD];
-    const int64_t flat = stage_coords(d, rank, coord);
-    const double pd = predict_point<T>(d, q, recon + (uint64_t)c * q.points, flat, coord);
-    pred[i] = (T)pd;
+    int32_t coord[ND > 0 ? ND : MAXD];
+    const int64_t flat = stage_coords_t<ND, KIND>(d, rank, coord);
+    pred[i] = (T)predict_point<T, ND, KIND, CUBIC>(d, q, recon + (uint64_t)c * q.points, flat,
+                                                    coord);
 }
 
 // ---------------------------------------------------------------- scans
@@ -510,14 +536,61 @@ __device__ __forceinline__ T load_unaligned(const uint8_t* p) {
     return v;
 }
 
-template <typename T>
+template <typename T, int ND, int KIND, int CUBIC>
+__device__ __forceinline__ void dequant_point(const StageDesc& d, const QParams& q,
+                                              const int is_anchor, uint64_t i, uint32_t code,
+                                              const uint8_t* __restrict__ outliers, uint32_t pos,
+                                              uint32_t n_out, T* __restrict__ recon,
+                                              uint32_t* __restrict__ err) {
+    uint32_t c = 0, rank = (uint32_t)i;
+    if (q.channels > 1) {
+        c = (uint32_t)(i / d.n);
+        rank = (uint32_t)(i - (uint64_t)c * d.n);
+    }
+    int32_t coord[ND > 0 ? ND : MAXD];
+    const int64_t flat = stage_coords_t<ND, KIND>(d, rank, coord);
+    T* rc = recon + (uint64_t)c * q.points;
+    T rv;
+    if (code == 0) {
+        if (pos < n_out) {
+            rv = load_unaligned<T>(outliers + (uint64_t)pos * sizeof(T));
+        } else {
+            rv = (T)0;
+            atomicOr(err, 1u);
+        }
+    } else {
+        const double pd0 = is_anchor ? 0.0 : predict_point<T, ND, KIND, CUBIC>(d, q, rc, flat, coord);
+        const double qv = (double)((int)code - q.radius);
+        if (sizeof(T) == 4) {
+            const double pd = (double)__double2float_rn(pd0);
+            rv = (T)__double2float_rn(__dadd_rn(pd, __dmul_rn(q.w, qv)));
+        } else {
+            rv = (T)__dadd_rn(pd0, __dmul_rn(q.w, qv));
+        }
+    }
+    rc[flat] = rv;
+}
+
+// Tiles without outliers (the common case) take a barrier-free path; others
+// rank their outliers with a block scan in item order.
+template <typename T, int ND, int KIND, int CUBIC>
 __global__ void __launch_bounds__(THREADS)
     k_interp_dequant(const StageDesc d, const QParams q, const int is_anchor,
                      const uint16_t* __restrict__ codes, const uint8_t* __restrict__ outliers,
-                     const uint32_t* __restrict__ tile_off, const uint32_t n_out,
-                     T* __restrict__ recon, uint32_t* __restrict__ err) {
+                     const uint32_t* __restrict__ tile_cnt, const uint32_t* __restrict__ tile_off,
+                     const uint32_t n_out, T* __restrict__ recon, uint32_t* __restrict__ err) {
     const uint64_t items = (uint64_t)q.channels * d.n;
     const uint64_t tile_base = (uint64_t)blockIdx.x * TILE;
+    if (tile_cnt[blockIdx.x] == 0) {
+#pragma unroll 2
+        for (int k = 0; k < TILE / THREADS; k++) {
+            const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
+            if (i < items)
+                dequant_point<T, ND, KIND, CUBIC>(d, q, is_anchor, i, codes[i], outliers, 0, n_out,
+                                                  recon, err);
+        }
+        return;
+    }
     uint32_t run = tile_off[blockIdx.x];
     for (int k = 0; k < TILE / THREADS; k++) {
         const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
@@ -526,34 +599,9 @@ __global__ void __launch_bounds__(THREADS)
         uint32_t tot;
         const uint32_t pos = run + block_excl_flag(code == 0, tot);
         run += tot;
-        if (!valid) continue;
-        uint32_t c = 0, rank = (uint32_t)i;
-        if (q.channels > 1) {
-            c = (uint32_t)(i / d.n);
-            rank = (uint32_t)(i - (uint64_t)c * d.n);
-        }
-        int32_t coord[MAXD];
-        const int64_t flat = stage_coords(d, rank, coord);
-        T* rc = recon + (uint64_t)c * q.points;
-        T rv;
-        if (code == 0) {
-            if (pos < n_out) {
-                rv = load_unaligned<T>(outliers + (uint64_t)pos * sizeof(T));
-            } else {
-                rv = (T)0;
-                atomicOr(err, 1u);
-            }
-        } else {
-            const double pd0 = is_anchor ? 0.0 : predict_point<T>(d, q, rc, flat, coord);
-            const double qv = (double)((int)code - q.radius);
-            if (sizeof(T) == 4) {
-                const double pd = (double)__double2float_rn(pd0);
-                rv = (T)__double2float_rn(__dadd_rn(pd, __dmul_rn(q.w, qv)));
-            } else {
-                rv = (T)__dadd_rn(pd0, __dmul_rn(q.w, qv));
-            }
-        }
-        rc[flat] = rv;
+        if (valid)
+            dequant_point<T, ND, KIND, CUBIC>(d, q, is_anchor, i, code, outliers, pos, n_out, recon,
+                                              err);
     }
 }
 
@@ -563,6 +611,37 @@ static int last_err() {
     return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
 }
 
+// Compile-time dispatch over (dtype, rank 2/3/4 or runtime, layout, order).
+#define LATEC_DISPATCH(KERNEL_CALL)                                                      \
+    do {                                                                                 \
+        const int nd_ = (d.ndim >= 2 && d.ndim <= 4) ? d.ndim : 0;                      \
+        const int kd_ = d.kind ? 1 : 0, cu_ = q.order ? 1 : 0;                           \
+        if (dtype == LATEC_F64) {                                                        \
+            using T = double;                                                            \
+            DISPATCH_ND(KERNEL_CALL);                                                    \
+        } else {                                                                         \
+            using T = float;                                                             \
+            DISPATCH_ND(KERNEL_CALL);                                                    \
+        }                                                                                \
+    } while (0)
+#define DISPATCH_ND(KERNEL_CALL)                                                         \
+    switch (nd_) {                                                                       \
+        case 2: DISPATCH_KC(2, KERNEL_CALL); break;                                      \
+        case 3: DISPATCH_KC(3, KERNEL_CALL); break;                                      \
+        case 4: DISPATCH_KC(4, KERNEL_CALL); break;                                      \
+        default: DISPATCH_KC(0, KERNEL_CALL); break;                                     \
+    }
+#define DISPATCH_KC(NDC, KERNEL_CALL)                                                    \
+    do {                                                                                 \
+        if (kd_) {                                                                       \
+            if (cu_) { constexpr int ND = NDC, KIND = 1, CUBIC = 1; KERNEL_CALL; }       \
+            else { constexpr int ND = NDC, KIND = 1, CUBIC = 0; KERNEL_CALL; }           \
+        } else {                                                                         \
+            if (cu_) { constexpr int ND = NDC, KIND = 0, CUBIC = 1; KERNEL_CALL; }       \
+            else { constexpr int ND = NDC, KIND = 0, CUBIC = 0; KERNEL_CALL; }           \
+        }                                                                                \
+    } while (0)
+
 int launch_interp_quant(const StageDesc& d, const QParams& q, int dtype, int is_anchor,
                         const void* x, void* recon, uint16_t* codes, void* staging,
                         uint32_t* tile_cnt, uint32_t* hist_total, uint32_t* hist_seg,
@@ -570,14 +649,9 @@ int launch_interp_quant(const StageDesc& d, const QParams& q, int dtype, int is_
     const uint64_t items = (uint64_t)q.channels * d.n;
     if (!items) return LATEC_OK;
     const uint32_t blocks = n_blocks(items);
-    if (dtype == LATEC_F64)
-        k_interp_quant<double><<<blocks, THREADS, 0, st>>>(
-            d, q, is_anchor, (const double*)x, (double*)recon, codes, (double*)staging, tile_cnt,
-            hist_total, hist_seg, acc, partials);
-    else
-        k_interp_quant<float><<<blocks, THREADS, 0, st>>>(
-            d, q, is_anchor, (const float*)x, (float*)recon, codes, (float*)staging, tile_cnt,
-            hist_total, hist_seg, acc, partials);
+    LATEC_DISPATCH((k_interp_quant<T, ND, KIND, CUBIC><<<blocks, THREADS, 0, st>>>(
+        d, q, is_anchor, (const T*)x, (T*)recon, codes, (T*)staging, tile_cnt, hist_total,
+        hist_seg, acc, partials)));
     return last_err();
 }
 
@@ -603,12 +677,8 @@ int launch_interp_predict(const StageDesc& d, const QParams& q, int dtype, const
     const uint64_t items = (uint64_t)q.channels * d.n;
     if (!items) return LATEC_OK;
     const uint32_t blocks = (uint32_t)((items + THREADS - 1) / THREADS);
-    if (dtype == LATEC_F64)
-        k_interp_predict<double><<<blocks, THREADS, 0, st>>>(d, q, (const double*)recon,
-                                                              (double*)pred);
-    else
-        k_interp_predict<float><<<blocks, THREADS, 0, st>>>(d, q, (const float*)recon,
-                                                            (float*)pred);
+    LATEC_DISPATCH((k_interp_predict<T, ND, KIND, CUBIC><<<blocks, THREADS, 0, st>>>(
+        d, q, (const T*)recon, (T*)pred)));
     return last_err();
 }
 
@@ -643,16 +713,14 @@ int launch_stats_reduce(const double* partials, uint32_t blocks, StageAcc* acc,
 }
 
 int launch_interp_dequant(const StageDesc& d, const QParams& q, int dtype, int is_anchor,
-                          const uint16_t* codes, const void* outliers, const uint32_t* tile_off,
-                          uint32_t n_out, void* recon, uint32_t* err, cudaStream_t st) {
+                          const uint16_t* codes, const void* outliers, const uint32_t* tile_cnt,
+                          const uint32_t* tile_off, uint32_t n_out, void* recon, uint32_t* err,
+                          cudaStream_t st) {
     const uint64_t items = (uint64_t)q.channels * d.n;
     if (!items) return LATEC_OK;
-    if (dtype == LATEC_F64)
-        k_interp_dequant<double><<<n_tiles(items), THREADS, 0, st>>>(
-            d, q, is_anchor, codes, (const uint8_t*)outliers, tile_off, n_out, (double*)recon, err);
-    else
-        k_interp_dequant<float><<<n_tiles(items), THREADS, 0, st>>>(
-            d, q, is_anchor, codes, (const uint8_t*)outliers, tile_off, n_out, (float*)recon, err);
+    LATEC_DISPATCH((k_interp_dequant<T, ND, KIND, CUBIC><<<n_tiles(items), THREADS, 0, st>>>(
+        d, q, is_anchor, codes, (const uint8_t*)outliers, tile_cnt, tile_off, n_out, (T*)recon,
+        err)));
     return last_err();
 }
 

@@ -60,8 +60,9 @@ int launch_compact(const uint16_t* codes, uint64_t items, const void* staging, i
 int launch_stats_reduce(const double* partials, uint32_t blocks, StageAcc* acc,
                         cudaStream_t st);
 int launch_interp_dequant(const StageDesc& d, const QParams& q, int dtype, int is_anchor,
-                          const uint16_t* codes, const void* outliers, const uint32_t* tile_off,
-                          uint32_t n_out, void* recon, uint32_t* err, cudaStream_t st);
+                          const uint16_t* codes, const void* outliers, const uint32_t* tile_cnt,
+                          const uint32_t* tile_off, uint32_t n_out, void* recon, uint32_t* err,
+                          cudaStream_t st);
 int launch_quantize_flat(const QParams& q, int dtype, uint64_t items, const void* x,
                          const void* pred, uint16_t* codes, void* staging, uint32_t* tile_cnt,
                          uint32_t* hist_total, uint32_t* hist_seg, StageAcc* acc,

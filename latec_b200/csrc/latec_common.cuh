@@ -110,4 +110,47 @@ __host__ __device__ __forceinline__ int64_t stage_coords(const StageDesc& d, uin
     return flat;
 }
 
+// Compile-time specialised decode: ND > 0 fixes the rank (loops unroll, the
+// coordinates stay in registers), KIND fixes the stage layout; ND == 0 falls
+// back to the runtime rank.
+template <int ND, int KIND>
+__host__ __device__ __forceinline__ int64_t stage_coords_t(const StageDesc& d, uint32_t rank,
+                                                           int32_t* coord) {
+    constexpr int NDV = ND > 0 ? ND : MAXD;
+    int64_t flat = 0;
+    uint32_t rem = rank;
+    if (KIND == 0) {
+#pragma unroll
+        for (int j = NDV - 1; j >= 0; j--) {
+            if (ND > 0 || j < d.ndim) {
+                const uint32_t q = fdiv(rem, d.size_div[j]);
+                const uint32_t m = rem - q * d.size_div[j].d;
+                rem = q;
+                coord[j] = d.start[j] + d.step * (int32_t)m;
+                flat += (int64_t)coord[j] * d.gstride[j];
+            }
+        }
+    } else {
+        int r = d.weight;
+        const int32_t s2 = 2 * d.s;
+#pragma unroll
+        for (int j = 0; j < NDV; j++) {
+            if (ND > 0 || j < d.ndim) {
+                const FastDiv& g = d.g_div[j][r];
+                const uint32_t m = fdiv(rem, g);
+                rem -= m * g.d;
+                const uint32_t f0 = d.f_even[j][r];
+                const int p = rem >= f0;
+                if (p) {
+                    rem -= f0;
+                    r -= 1;
+                }
+                coord[j] = s2 * (int32_t)m + (p ? d.s : 0);
+                flat += (int64_t)coord[j] * d.gstride[j];
+            }
+        }
+    }
+    return flat;
+}
+
 }  // namespace latec
