@@ -64,7 +64,7 @@ typedef struct latec_rans_stage {
     uint64_t out_off;     /* first outlier of the stage in the outlier buffer */
     uint64_t enc;         /* device address: encoder symbol table (24 B/entry) */
     uint64_t cdf;         /* device address: CDF rows (alphabet + 1 u32 each) */
-    uint64_t bucket;      /* device address: decoder bucket rows (4096 u16 each) */
+    uint64_t bucket;      /* device address: decoder bucket rows (1024 u16 each) */
     uint64_t scratch_off; /* filled by the library */
     uint64_t blob_off;    /* decode: word offset of the stage blob */
     uint64_t rec_off;     /* filled by the library */

@@ -321,6 +321,11 @@ class _Encoder:
                                                 _lib.stream_ptr()), "latec_frame_raw")
             if getattr(self, "stream_out", "bytes") == "device":
                 stream = out
+            elif getattr(self, "stream_out", "bytes") == "numpy":
+                host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+                host.copy_(out, non_blocking=True)
+                torch.cuda.current_stream().synchronize()
+                stream = host.numpy()
             else:
                 pin = _lib.pinned(total, "stream_out")
                 pin[:total].copy_(out, non_blocking=True)
@@ -422,10 +427,10 @@ def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, rad
     _lib.load()
     if entropy not in ("native", "compat"):
         raise ValueError("entropy must be 'native' or 'compat'")
-    if stream_out not in ("bytes", "device"):
-        raise ValueError("stream_out must be 'bytes' or 'device'")
-    if stream_out == "device" and entropy != "native":
-        raise ValueError("device streams use the native entropy mode")
+    if stream_out not in ("bytes", "device", "numpy"):
+        raise ValueError("stream_out must be 'bytes', 'numpy' or 'device'")
+    if stream_out != "bytes" and entropy != "native":
+        raise ValueError("numpy and device streams use the native entropy mode")
     if not eb > 0:
         raise ValueError(f"error bound must be > 0, got {eb}")
     _check_radius(radius)
@@ -552,9 +557,17 @@ def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, rad
 
 
 def _upload_stream(body, dev):
-    """Host bytes -> device through a pinned staging buffer."""
+    """Host bytes -> device: one DMA from page-locked memory, else through a
+    pinned staging buffer."""
     torch = _torch()
     n = len(body)
+    if isinstance(body, np.ndarray) and body.flags.writeable and n:
+        t = torch.from_numpy(body)
+        if t.is_pinned():
+            d = torch.empty(n + 4, dtype=torch.uint8, device=dev)
+            d[:n].copy_(t, non_blocking=True)
+            d[n:].zero_()
+            return d
     pin = _lib.pinned(n + 4, "stream_in")
     pin.numpy()[:n] = body
     d = torch.empty(n + 4, dtype=torch.uint8, device=dev)
@@ -598,6 +611,7 @@ def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
     else:
         mv = memoryview(stream).cast("B")
         n_total = len(mv)
+        np_stream = stream if isinstance(stream, np.ndarray) else None
         prefix = mv[:min(n_total, 4096)].tobytes()
         dev = torch.device(device) if device is not None else torch.device(
             "cuda", torch.cuda.current_device())
@@ -639,7 +653,9 @@ def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
         if is_dev:
             frame_dev = stream[header.size:]
         else:
-            frame_dev = _upload_stream(np.frombuffer(mv[header.size:], np.uint8), dev)
+            body_np = (np_stream.reshape(-1)[header.size:] if np_stream is not None
+                       else np.frombuffer(mv[header.size:], np.uint8))
+            frame_dev = _upload_stream(body_np, dev)
         n_pay = n_raw
         pay_dev = torch.zeros(n_pay + 8 + (-n_pay) % 4, dtype=torch.uint8, device=dev)
         _lib.check(lib.latec_unframe_raw(frame_dev.data_ptr(), n_pay, pay_dev.data_ptr(),

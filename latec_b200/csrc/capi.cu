@@ -83,7 +83,7 @@ uint64_t stage_ws(const latec_plan* plan, uint64_t max_items_override, int elem,
     w.tile_cnt = c.take<uint32_t>(n_tiles(max_items) + 1);
     w.tile_off = c.take<uint32_t>(n_tiles(max_items) + 1);
     w.total = c.take<uint32_t>(4);
-    w.partials = c.take<double>((uint64_t)n_blocks(max_items) * 5 + 5);
+    w.partials = c.take<double>((uint64_t)MAX_BLOCKS * 5 + 5);
     if (out) *out = w;
     return c.off;
 }

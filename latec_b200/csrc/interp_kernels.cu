@@ -218,10 +218,8 @@ struct BlockAcc {
     uint32_t maxq;
 };
 
-// Flush the per-block histogram window and statistics.
-__device__ __forceinline__ void block_finish(BlockAcc& a, uint32_t* sh_hist, uint32_t* hist_seg,
-                                             uint64_t block_base, StageAcc* acc,
-                                             double* partials) {
+// Per-block statistics: warp shuffles, then one partial row per CTA.
+__device__ __forceinline__ void block_finish(BlockAcc& a, double* partials, StageAcc* acc) {
     __shared__ double sh_red[5][THREADS / 32];
     __shared__ uint32_t sh_mq[THREADS / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -246,105 +244,133 @@ __device__ __forceinline__ void block_finish(BlockAcc& a, uint32_t* sh_hist, uin
         for (int k = 0; k < 5; k++) partials[(size_t)blockIdx.x * 5 + k] = s[k];
         if (mq) atomicMax(&acc->maxq, mq);
     }
-    const uint32_t seg = (uint32_t)(block_base >> SEG_SHIFT);
-    for (int b = threadIdx.x; b < HBINS; b += THREADS) {
-        const uint32_t v = sh_hist[b];
-        if (v) atomicAdd(&hist_seg[(size_t)seg * HBINS + b], v);
-    }
-}
-
-__device__ __forceinline__ void hist_add(uint32_t* sh_hist, uint32_t* hist_total, QOut o,
-                                         int radius, uint32_t& maxq) {
-    if (!o.code) {
-        atomicAdd(&sh_hist[0], 1u);
-        return;
-    }
-    const uint32_t aq = (uint32_t)abs(o.qv);
-    maxq = max(maxq, aq);
-    if (aq < HWIN)
-        atomicAdd(&sh_hist[o.qv + HWIN], 1u);
-    else
-        atomicAdd(&hist_total[o.code], 1u);
 }
 
 // ---------------------------------------------------------------- encode
-// One CTA walks TILES_PER_BLOCK consecutive tiles of the stage's ranks; each
-// thread handles ranks tile + k * THREADS + tid (coalesced codes). The inner
-// loop has no block barrier: outlier counts go to per-tile shared counters.
+// A CTA owns a contiguous run of 512-point groups of the stage's ranks; each
+// thread takes two points of a group (ranks g + tid and g + 256 + tid, so
+// codes are written coalesced) and keeps both in flight: both predictions
+// are issued before either result is stored. Outliers are counted into their
+// 2048-point tile with global atomics (tile_cnt is zeroed by the caller); the
+// shared histogram is flushed whenever the run crosses a 2^22-code segment.
+template <typename T, int ND, int KIND, int CUBIC>
+__device__ __forceinline__ double locate_predict(const StageDesc& d, const QParams& q,
+                                                 const int is_anchor, uint64_t i,
+                                                 const T* __restrict__ recon, int64_t& flat,
+                                                 uint32_t& c) {
+    c = 0;
+    uint32_t rank = (uint32_t)i;
+    if (q.channels > 1) {
+        c = (uint32_t)(i / d.n);
+        rank = (uint32_t)(i - (uint64_t)c * d.n);
+    }
+    int32_t coord[ND > 0 ? ND : MAXD];
+    flat = stage_coords_t<ND, KIND>(d, rank, coord);
+    return is_anchor ? 0.0
+                     : predict_point<T, ND, KIND, CUBIC>(d, q, recon + (uint64_t)c * q.points, flat,
+                                                         coord);
+}
+
+template <typename T>
+__device__ __forceinline__ void encode_value(const QParams& q, uint64_t i, T xv, double pd,
+                                             T* __restrict__ dst, T* __restrict__ staging,
+                                             uint32_t* __restrict__ tile_cnt,
+                                             uint16_t* __restrict__ codes, BlockAcc& a, int& key,
+                                             uint32_t& code) {
+    T rv;
+    const QOut o = Quant<T>::run(xv, pd, q, rv);
+    *dst = rv;
+    code = o.code;
+    codes[i] = (uint16_t)o.code;
+    if (!o.code) {
+        staging[i] = xv;
+        atomicAdd(&tile_cnt[i / TILE], 1u);
+        key = 0;
+    } else {
+        const uint32_t aq = (uint32_t)abs(o.qv);
+        a.maxq = max(a.maxq, aq);
+        key = aq < HWIN ? o.qv + HWIN : -2;
+    }
+    const double e = Quant<T>::err(xv, pd);
+    a.s[0] += fabs(e);
+    a.s[1] += e * e;
+    const double re = Quant<T>::rerr(xv, rv);
+    a.s[2] += re;
+    a.s[3] += re * re;
+    a.s[4] = fmax(a.s[4], re);
+}
+
+__device__ __forceinline__ void hist_warp(uint32_t* sh_hist, uint32_t* hist_total, int key,
+                                          uint32_t code, int lane) {
+    const unsigned same = __match_any_sync(0xffffffffu, key);
+    if (key >= 0 && lane == __ffs(same) - 1) atomicAdd(&sh_hist[key], (uint32_t)__popc(same));
+    if (key == -2) atomicAdd(&hist_total[code], 1u);
+}
+
+__device__ __forceinline__ void flush_hist(uint32_t* sh_hist, uint32_t* hist_seg, uint32_t seg) {
+    for (int b = threadIdx.x; b < HBINS; b += THREADS) {
+        const uint32_t v = sh_hist[b];
+        if (v) {
+            atomicAdd(&hist_seg[(size_t)seg * HBINS + b], v);
+            sh_hist[b] = 0;
+        }
+    }
+}
+
 template <typename T, int ND, int KIND, int CUBIC>
 __global__ void __launch_bounds__(THREADS)
-    k_interp_quant(const StageDesc d, const QParams q, const int is_anchor,
+    k_interp_quant(const StageDesc d, const QParams q, const int is_anchor, const uint32_t gpb,
                    const T* __restrict__ x, T* __restrict__ recon, uint16_t* __restrict__ codes,
                    T* __restrict__ staging, uint32_t* __restrict__ tile_cnt,
                    uint32_t* __restrict__ hist_total, uint32_t* __restrict__ hist_seg,
                    StageAcc* __restrict__ acc, double* __restrict__ partials) {
     __shared__ uint32_t sh_hist[HBINS];
-    __shared__ uint32_t sh_tile[TILES_PER_BLOCK];
     for (int b = threadIdx.x; b < HBINS; b += THREADS) sh_hist[b] = 0;
-    if (threadIdx.x < TILES_PER_BLOCK) sh_tile[threadIdx.x] = 0;
     __syncthreads();
     const uint64_t items = (uint64_t)q.channels * d.n;
-    const uint64_t block_base = (uint64_t)blockIdx.x * BLOCK_PTS;
+    const uint64_t groups = (items + GROUP - 1) / GROUP;
+    const uint64_t g0 = (uint64_t)blockIdx.x * gpb;
+    const uint64_t g1 = g0 + gpb < groups ? g0 + gpb : groups;
     const int lane = threadIdx.x & 31;
     BlockAcc a{{0, 0, 0, 0, 0}, 0};
-    for (int t = 0; t < TILES_PER_BLOCK; t++) {
-        const uint64_t tile_base = block_base + (uint64_t)t * TILE;
-        if (tile_base >= items) break;
-        uint32_t outl = 0;
-#pragma unroll 2
-        for (int k = 0; k < TILE / THREADS; k++) {
-            const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
-            int key = -1;  // histogram bin (-1 none, -2 outside the window)
-            uint32_t code = 0;
-            if (i < items) {
-                uint32_t c = 0, rank = (uint32_t)i;
-                if (q.channels > 1) {
-                    c = (uint32_t)(i / d.n);
-                    rank = (uint32_t)(i - (uint64_t)c * d.n);
-                }
-                int32_t coord[ND > 0 ? ND : MAXD];
-                const int64_t flat = stage_coords_t<ND, KIND>(d, rank, coord);
-                T* rc = recon + (uint64_t)c * q.points;
-                const double pd =
-                    is_anchor ? 0.0 : predict_point<T, ND, KIND, CUBIC>(d, q, rc, flat, coord);
-                const T xv = x[(uint64_t)c * q.points + flat];
-                T rv;
-                const QOut o = Quant<T>::run(xv, pd, q, rv);
-                rc[flat] = rv;
-                code = o.code;
-                codes[i] = (uint16_t)o.code;
-                if (!o.code) {
-                    staging[i] = xv;
-                    outl++;
-                    key = 0;
-                } else {
-                    const uint32_t aq = (uint32_t)abs(o.qv);
-                    a.maxq = max(a.maxq, aq);
-                    key = aq < HWIN ? o.qv + HWIN : -2;
-                }
-                const double e = Quant<T>::err(xv, pd);
-                a.s[0] += fabs(e);
-                a.s[1] += e * e;
-                const double re = Quant<T>::rerr(xv, rv);
-                a.s[2] += re;
-                a.s[3] += re * re;
-                a.s[4] = fmax(a.s[4], re);
-            }
-            // warp-aggregated histogram: one shared atomic per distinct bin
-            const unsigned same = __match_any_sync(0xffffffffu, key);
-            if (key >= 0 && lane == __ffs(same) - 1) atomicAdd(&sh_hist[key], (uint32_t)__popc(same));
-            if (key == -2) atomicAdd(&hist_total[code], 1u);
+    uint32_t cur_seg = (uint32_t)((g0 * GROUP) >> SEG_SHIFT);
+    for (uint64_t g = g0; g < g1; g++) {
+        const uint64_t base = g * GROUP;
+        const uint32_t seg = (uint32_t)(base >> SEG_SHIFT);
+        if (seg != cur_seg) {  // uniform across the CTA
+            __syncthreads();
+            flush_hist(sh_hist, hist_seg, cur_seg);
+            __syncthreads();
+            cur_seg = seg;
         }
-#pragma unroll
-        for (int o = 16; o; o >>= 1) outl += __shfl_xor_sync(0xffffffffu, outl, o);
-        if (lane == 0 && outl) atomicAdd(&sh_tile[t], outl);
+        const uint64_t i0 = base + threadIdx.x, i1 = i0 + THREADS;
+        const bool v0 = i0 < items, v1 = i1 < items;
+        int64_t f0 = 0, f1 = 0;
+        uint32_t c0 = 0, c1 = 0;
+        double p0 = 0.0, p1 = 0.0;
+        T x0 = (T)0, x1 = (T)0;
+        if (v0) {
+            p0 = locate_predict<T, ND, KIND, CUBIC>(d, q, is_anchor, i0, recon, f0, c0);
+            x0 = x[(uint64_t)c0 * q.points + f0];
+        }
+        if (v1) {
+            p1 = locate_predict<T, ND, KIND, CUBIC>(d, q, is_anchor, i1, recon, f1, c1);
+            x1 = x[(uint64_t)c1 * q.points + f1];
+        }
+        int k0 = -1, k1 = -1;
+        uint32_t cd0 = 0, cd1 = 0;
+        if (v0)
+            encode_value<T>(q, i0, x0, p0, recon + (uint64_t)c0 * q.points + f0, staging, tile_cnt,
+                            codes, a, k0, cd0);
+        if (v1)
+            encode_value<T>(q, i1, x1, p1, recon + (uint64_t)c1 * q.points + f1, staging, tile_cnt,
+                            codes, a, k1, cd1);
+        hist_warp(sh_hist, hist_total, k0, cd0, lane);
+        hist_warp(sh_hist, hist_total, k1, cd1, lane);
     }
     __syncthreads();
-    if (threadIdx.x < TILES_PER_BLOCK) {
-        const uint64_t tb = block_base + (uint64_t)threadIdx.x * TILE;
-        if (tb < items) tile_cnt[tb / TILE] = sh_tile[threadIdx.x];
-    }
-    block_finish(a, sh_hist, hist_seg, block_base, acc, partials);
+    flush_hist(sh_hist, hist_seg, cur_seg);
+    block_finish(a, partials, acc);
 }
 
 // Quantize a compact array against a given prediction (predictor-agnostic
@@ -352,48 +378,43 @@ __global__ void __launch_bounds__(THREADS)
 // reconstruction in the same compact order.
 template <typename T>
 __global__ void __launch_bounds__(THREADS)
-    k_quantize_flat(const QParams q, const uint64_t items, const T* __restrict__ x,
-                    const T* __restrict__ pred, uint16_t* __restrict__ codes,
-                    T* __restrict__ staging, uint32_t* __restrict__ tile_cnt,
-                    uint32_t* __restrict__ hist_total, uint32_t* __restrict__ hist_seg,
-                    StageAcc* __restrict__ acc, double* __restrict__ partials,
-                    T* __restrict__ recon_out) {
+    k_quantize_flat(const QParams q, const uint64_t items, const uint32_t gpb,
+                    const T* __restrict__ x, const T* __restrict__ pred,
+                    uint16_t* __restrict__ codes, T* __restrict__ staging,
+                    uint32_t* __restrict__ tile_cnt, uint32_t* __restrict__ hist_total,
+                    uint32_t* __restrict__ hist_seg, StageAcc* __restrict__ acc,
+                    double* __restrict__ partials, T* __restrict__ recon_out) {
     __shared__ uint32_t sh_hist[HBINS];
     for (int b = threadIdx.x; b < HBINS; b += THREADS) sh_hist[b] = 0;
     __syncthreads();
-    const uint64_t block_base = (uint64_t)blockIdx.x * BLOCK_PTS;
+    const uint64_t groups = (items + GROUP - 1) / GROUP;
+    const uint64_t g0 = (uint64_t)blockIdx.x * gpb;
+    const uint64_t g1 = g0 + gpb < groups ? g0 + gpb : groups;
+    const int lane = threadIdx.x & 31;
     BlockAcc a{{0, 0, 0, 0, 0}, 0};
-    for (int t = 0; t < TILES_PER_BLOCK; t++) {
-        const uint64_t tile_base = block_base + (uint64_t)t * TILE;
-        if (tile_base >= items) break;
-        int outl = 0;
-        for (int k = 0; k < TILE / THREADS; k++) {
-            const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
-            bool is_out = false;
-            if (i < items) {
-                const T xv = x[i];
-                const double pd = (double)pred[i];
-                T rv;
-                const QOut o = Quant<T>::run(xv, pd, q, rv);
-                recon_out[i] = rv;
-                codes[i] = (uint16_t)o.code;
-                is_out = o.code == 0;
-                if (is_out) staging[i] = xv;
-                hist_add(sh_hist, hist_total, o, q.radius, a.maxq);
-                const double e = Quant<T>::err(xv, pd);
-                a.s[0] += fabs(e);
-                a.s[1] += e * e;
-                const double re = Quant<T>::rerr(xv, rv);
-                a.s[2] += re;
-                a.s[3] += re * re;
-                a.s[4] = fmax(a.s[4], re);
-            }
-            outl += __syncthreads_count(is_out);
+    uint32_t cur_seg = (uint32_t)((g0 * GROUP) >> SEG_SHIFT);
+    for (uint64_t g = g0; g < g1; g++) {
+        const uint64_t base = g * GROUP;
+        const uint32_t seg = (uint32_t)(base >> SEG_SHIFT);
+        if (seg != cur_seg) {
+            __syncthreads();
+            flush_hist(sh_hist, hist_seg, cur_seg);
+            __syncthreads();
+            cur_seg = seg;
         }
-        if (threadIdx.x == 0) tile_cnt[tile_base / TILE] = (uint32_t)outl;
+        for (int h = 0; h < GROUP / THREADS; h++) {
+            const uint64_t i = base + (uint64_t)h * THREADS + threadIdx.x;
+            int key = -1;
+            uint32_t code = 0;
+            if (i < items)
+                encode_value<T>(q, i, x[i], (double)pred[i], recon_out + i, staging, tile_cnt,
+                                codes, a, key, code);
+            hist_warp(sh_hist, hist_total, key, code, lane);
+        }
     }
     __syncthreads();
-    block_finish(a, sh_hist, hist_seg, block_base, acc, partials);
+    flush_hist(sh_hist, hist_seg, cur_seg);
+    block_finish(a, partials, acc);
 }
 
 // Prediction only (the predictor plugin's ``predict``): compact output.
@@ -536,6 +557,16 @@ __device__ __forceinline__ T load_unaligned(const uint8_t* p) {
     return v;
 }
 
+template <typename T>
+__device__ __forceinline__ T dequant_value(const QParams& q, double pd0, uint32_t code) {
+    const double qv = (double)((int)code - q.radius);
+    if (sizeof(T) == 4) {
+        const double pd = (double)__double2float_rn(pd0);
+        return (T)__double2float_rn(__dadd_rn(pd, __dmul_rn(q.w, qv)));
+    }
+    return (T)__dadd_rn(pd0, __dmul_rn(q.w, qv));
+}
+
 template <typename T, int ND, int KIND, int CUBIC>
 __device__ __forceinline__ void dequant_point(const StageDesc& d, const QParams& q,
                                               const int is_anchor, uint64_t i, uint32_t code,
@@ -581,13 +612,24 @@ __global__ void __launch_bounds__(THREADS)
                      const uint32_t n_out, T* __restrict__ recon, uint32_t* __restrict__ err) {
     const uint64_t items = (uint64_t)q.channels * d.n;
     const uint64_t tile_base = (uint64_t)blockIdx.x * TILE;
-    if (tile_cnt[blockIdx.x] == 0) {
-#pragma unroll 2
-        for (int k = 0; k < TILE / THREADS; k++) {
-            const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
-            if (i < items)
-                dequant_point<T, ND, KIND, CUBIC>(d, q, is_anchor, i, codes[i], outliers, 0, n_out,
-                                                  recon, err);
+    if (tile_cnt[blockIdx.x] == 0) {  // no outliers: two points in flight per thread
+        for (int k = 0; k < TILE / THREADS; k += 2) {
+            const uint64_t i0 = tile_base + (uint64_t)k * THREADS + threadIdx.x;
+            const uint64_t i1 = i0 + THREADS;
+            int64_t f0 = 0, f1 = 0;
+            uint32_t c0 = 0, c1 = 0;
+            double p0 = 0.0, p1 = 0.0;
+            uint32_t q0 = 1, q1 = 1;
+            if (i0 < items) {
+                q0 = codes[i0];
+                p0 = locate_predict<T, ND, KIND, CUBIC>(d, q, is_anchor, i0, recon, f0, c0);
+            }
+            if (i1 < items) {
+                q1 = codes[i1];
+                p1 = locate_predict<T, ND, KIND, CUBIC>(d, q, is_anchor, i1, recon, f1, c1);
+            }
+            if (i0 < items) recon[(uint64_t)c0 * q.points + f0] = dequant_value<T>(q, p0, q0);
+            if (i1 < items) recon[(uint64_t)c1 * q.points + f1] = dequant_value<T>(q, p1, q1);
         }
         return;
     }
@@ -642,15 +684,33 @@ static int last_err() {
         }                                                                                \
     } while (0)
 
+static uint32_t groups_per_block(uint64_t items, uint32_t* blocks) {
+    const uint64_t groups = (items + GROUP - 1) / GROUP;
+    uint64_t b = groups < (uint64_t)MAX_BLOCKS ? groups : (uint64_t)MAX_BLOCKS;
+    if (b < 1) b = 1;
+    const uint64_t gpb = (groups + b - 1) / b;
+    *blocks = (uint32_t)((groups + gpb - 1) / gpb);
+    return (uint32_t)gpb;
+}
+
+uint32_t encode_blocks(uint64_t items) {
+    uint32_t b;
+    groups_per_block(items, &b);
+    return b;
+}
+
 int launch_interp_quant(const StageDesc& d, const QParams& q, int dtype, int is_anchor,
                         const void* x, void* recon, uint16_t* codes, void* staging,
                         uint32_t* tile_cnt, uint32_t* hist_total, uint32_t* hist_seg,
                         StageAcc* acc, double* partials, cudaStream_t st) {
     const uint64_t items = (uint64_t)q.channels * d.n;
     if (!items) return LATEC_OK;
-    const uint32_t blocks = n_blocks(items);
+    uint32_t blocks;
+    const uint32_t gpb = groups_per_block(items, &blocks);
+    if (cudaMemsetAsync(tile_cnt, 0, sizeof(uint32_t) * n_tiles(items), st) != cudaSuccess)
+        return LATEC_ERR_CUDA;
     LATEC_DISPATCH((k_interp_quant<T, ND, KIND, CUBIC><<<blocks, THREADS, 0, st>>>(
-        d, q, is_anchor, (const T*)x, (T*)recon, codes, (T*)staging, tile_cnt, hist_total,
+        d, q, is_anchor, gpb, (const T*)x, (T*)recon, codes, (T*)staging, tile_cnt, hist_total,
         hist_seg, acc, partials)));
     return last_err();
 }
@@ -660,14 +720,17 @@ int launch_quantize_flat(const QParams& q, int dtype, uint64_t items, const void
                          uint32_t* hist_total, uint32_t* hist_seg, StageAcc* acc,
                          double* partials, void* recon_out, cudaStream_t st) {
     if (!items) return LATEC_OK;
-    const uint32_t blocks = n_blocks(items);
+    uint32_t blocks;
+    const uint32_t gpb = groups_per_block(items, &blocks);
+    if (cudaMemsetAsync(tile_cnt, 0, sizeof(uint32_t) * n_tiles(items), st) != cudaSuccess)
+        return LATEC_ERR_CUDA;
     if (dtype == LATEC_F64)
         k_quantize_flat<double><<<blocks, THREADS, 0, st>>>(
-            q, items, (const double*)x, (const double*)pred, codes, (double*)staging, tile_cnt,
-            hist_total, hist_seg, acc, partials, (double*)recon_out);
+            q, items, gpb, (const double*)x, (const double*)pred, codes, (double*)staging,
+            tile_cnt, hist_total, hist_seg, acc, partials, (double*)recon_out);
     else
         k_quantize_flat<float><<<blocks, THREADS, 0, st>>>(
-            q, items, (const float*)x, (const float*)pred, codes, (float*)staging, tile_cnt,
+            q, items, gpb, (const float*)x, (const float*)pred, codes, (float*)staging, tile_cnt,
             hist_total, hist_seg, acc, partials, (float*)recon_out);
     return last_err();
 }

@@ -6,9 +6,9 @@
 namespace latec {
 
 constexpr int TILE = 2048;            // outlier-count granularity (points)
-constexpr int TILES_PER_BLOCK = 4;    // one CTA walks 4 consecutive tiles
-constexpr int BLOCK_PTS = TILE * TILES_PER_BLOCK;
 constexpr int THREADS = 256;
+constexpr int GROUP = 2 * THREADS;    // encode: points per CTA iteration (two per thread)
+constexpr int MAX_BLOCKS = 148 * 8;   // encode grid cap (8 CTAs per SM)
 constexpr int HWIN = 256;             // histogram window |q| < HWIN kept in SMEM
 constexpr int HBINS = 2 * HWIN;       // bin 0: outliers, q + HWIN otherwise
 constexpr int SEG_SHIFT = 22;         // float32 histogram accumulation segment
@@ -36,9 +36,9 @@ struct StageAcc {
 };
 
 inline uint32_t n_tiles(uint64_t items) { return (uint32_t)((items + TILE - 1) / TILE); }
-inline uint32_t n_blocks(uint64_t items) {
-    return (uint32_t)((items + BLOCK_PTS - 1) / BLOCK_PTS);
-}
+// CTAs of the encode kernels for a stage of `items` points (partials rows).
+uint32_t encode_blocks(uint64_t items);
+inline uint32_t n_blocks(uint64_t items) { return encode_blocks(items); }
 inline uint32_t n_segments(uint64_t items) {
     return (uint32_t)((items + (1ull << SEG_SHIFT) - 1) >> SEG_SHIFT);
 }

@@ -6,7 +6,7 @@
 
 namespace latec {
 
-constexpr int BUCKET_BITS = 12;
+constexpr int BUCKET_BITS = 10;
 constexpr int NBUCKET = 1 << BUCKET_BITS;
 constexpr int MODE_LANES = 0;
 constexpr int MODE_COMPAT = 1;
@@ -45,8 +45,8 @@ struct RansStageDesc {
     uint32_t block0;      // decode: first CTA of the stage (filled by the library)
 };
 
-constexpr int DEC_WARPS = 4;             // warps (chunks) per decoder CTA
-constexpr int SMEM_ALPHA = 16384;        // largest alphabet decoded from shared memory
+constexpr int DEC_WARPS = 16;            // warps (chunks) per decoder CTA
+constexpr int SMEM_ALPHA = 8192;         // largest alphabet decoded from shared memory
 
 int launch_build_tables(const uint32_t* cdf, int alphabet, int rows, EncSym* enc, uint16_t* bucket,
                         cudaStream_t st);
