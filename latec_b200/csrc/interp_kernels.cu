@@ -686,6 +686,10 @@ static int last_err() {
 
 static uint32_t groups_per_block(uint64_t items, uint32_t* blocks) {
     const uint64_t groups = (items + GROUP - 1) / GROUP;
+    if (groups == 0) {  // empty stage: no CTAs
+        *blocks = 0;
+        return 1;
+    }
     uint64_t b = groups < (uint64_t)MAX_BLOCKS ? groups : (uint64_t)MAX_BLOCKS;
     if (b < 1) b = 1;
     const uint64_t gpb = (groups + b - 1) / b;
