@@ -325,13 +325,14 @@ def main():
     xh_np = xh
     del x
     torch.cuda.empty_cache()
-    for _ in range(2):
+    for _ in range(max(3, args.warmup)):  # first calls pay the page-locked allocations
         s_e, _ = lb.compress(xh_np, eb, pred(), levels=LEVELS, anchor_stride=STRIDE, recon="none",
                              stream_out="numpy")
-        lb.decompress(s_e)
+        back = lb.decompress(s_e)
+    del back
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    e_steps = max(1, min(args.steps, 3))
+    e_steps = max(1, args.steps)
     for _ in range(e_steps):
         s_e, _ = lb.compress(xh_np, eb, pred(), levels=LEVELS, anchor_stride=STRIDE, recon="none",
                              stream_out="numpy")
