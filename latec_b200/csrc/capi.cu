@@ -2,6 +2,7 @@
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "interp_kernels.cuh"
 #include "plan.h"
@@ -66,31 +67,41 @@ bool make_q(const latec_quant_params* p, double eb, uint64_t points, QParams& q)
 
 struct StageWs {
     void* staging;
-    uint32_t* tile_cnt;
+    uint32_t* tile_cnt;   // per tile of the largest stage (encode) / of all stages (decode)
     uint32_t* tile_off;
     uint32_t* total;
     double* partials;
+    DecStage* dec;        // decode: per-stage descriptors of the all-stage tile passes
 };
 
-uint64_t stage_ws(const latec_plan* plan, uint64_t max_items_override, int elem, StageWs* out,
+// Workspace carve-up: `max_items` sizes the per-stage encode scratch;
+// `all_tiles` / `n_stages` the decode's all-stage tile arrays.
+uint64_t stage_ws(uint64_t max_items, uint64_t all_tiles, int n_stages, int elem, StageWs* out,
                   void* base) {
-    uint64_t max_items = max_items_override;
-    if (plan)
-        for (auto& d : plan->stages) max_items = d.n > max_items ? d.n : max_items;
     Carve c{(uint8_t*)base};
     StageWs w;
+    const uint64_t tiles = (n_tiles(max_items) > all_tiles ? n_tiles(max_items) : all_tiles) + 1;
     w.staging = c.take<uint8_t>(max_items * elem);
-    w.tile_cnt = c.take<uint32_t>(n_tiles(max_items) + 1);
-    w.tile_off = c.take<uint32_t>(n_tiles(max_items) + 1);
+    w.tile_cnt = c.take<uint32_t>(tiles);
+    w.tile_off = c.take<uint32_t>(tiles);
     w.total = c.take<uint32_t>(4);
     w.partials = c.take<double>((uint64_t)MAX_BLOCKS * 5 + 5);
+    w.dec = c.take<DecStage>(n_stages > 0 ? n_stages : 1);
     if (out) *out = w;
     return c.off;
 }
 
-__global__ void k_check_count(const uint32_t* total, uint32_t expected, uint32_t* err) {
-    if (threadIdx.x == 0 && *total != expected) atomicOr(err, 1u);
+void plan_sizes(const latec_plan* plan, int C, uint64_t* max_items, uint64_t* all_tiles) {
+    uint64_t m = 0, t = 0;
+    for (auto& d : plan->stages) {
+        const uint64_t items = (uint64_t)d.n * C;
+        m = items > m ? items : m;
+        t += n_tiles(items);
+    }
+    *max_items = m;
+    *all_tiles = t;
 }
+
 
 }  // namespace
 
@@ -147,13 +158,13 @@ int latec_plan_stage_flat(const latec_plan* plan, int32_t stage, uint64_t first,
 
 uint64_t latec_stage_workspace_bytes(const latec_plan* plan, int32_t channels, int32_t dtype) {
     if (!plan || channels < 1) return 0;
-    uint64_t m = 0;
-    for (auto& d : plan->stages) m = (uint64_t)d.n * channels > m ? (uint64_t)d.n * channels : m;
-    return stage_ws(nullptr, m, elem_of(dtype), nullptr, nullptr);
+    uint64_t m, t;
+    plan_sizes(plan, channels, &m, &t);
+    return stage_ws(m, t, (int)plan->stages.size(), elem_of(dtype), nullptr, nullptr);
 }
 
 uint64_t latec_flat_workspace_bytes(uint64_t items, int32_t dtype) {
-    return stage_ws(nullptr, items, elem_of(dtype), nullptr, nullptr);
+    return stage_ws(items, 0, 1, elem_of(dtype), nullptr, nullptr);
 }
 
 int latec_encode_stages(const latec_plan* plan, const latec_quant_params* prm,
@@ -167,10 +178,10 @@ int latec_encode_stages(const latec_plan* plan, const latec_quant_params* prm,
     const int C = prm->channels, elem = elem_of(prm->dtype);
     const uint64_t need = latec_stage_workspace_bytes(plan, C, prm->dtype);
     if (!workspace || workspace_bytes < need) return LATEC_ERR_WORKSPACE;
-    uint64_t m = 0;
-    for (auto& d : plan->stages) m = (uint64_t)d.n * C > m ? (uint64_t)d.n * C : m;
+    uint64_t m, tiles_all;
+    plan_sizes(plan, C, &m, &tiles_all);
     StageWs w;
-    stage_ws(nullptr, m, elem, &w, workspace);
+    stage_ws(m, tiles_all, (int)plan->stages.size(), elem, &w, workspace);
     cudaStream_t st = (cudaStream_t)stream;
     const int ns = (int)plan->stages.size();
     uint64_t total_segs = 0;
@@ -186,14 +197,13 @@ int latec_encode_stages(const latec_plan* plan, const latec_quant_params* prm,
         QParams q;
         if (!make_q(prm, stage_eb[t], plan->points, q)) return LATEC_ERR_ARG;
         StageAcc* acc = (StageAcc*)(stats + t);
+        // the pass's last CTA reduces the statistics and scans the tile counts
         int rc = launch_interp_quant(d, q, prm->dtype, t == 0, x, recon, codes + off, w.staging,
-                                     w.tile_cnt, hist_total + 65536ull * t,
+                                     w.tile_cnt, w.tile_off, hist_total + 65536ull * t,
                                      hist_seg + (uint64_t)HBINS * seg, acc, w.partials, st);
-        if (!rc) rc = launch_tile_scan(w.tile_cnt, n_tiles(items), w.tile_off, &acc->n_out, st);
         if (!rc)
             rc = launch_compact(codes + off, items, w.staging, elem, w.tile_cnt, w.tile_off,
                                 (uint8_t*)outliers + off * elem, st);
-        if (!rc) rc = launch_stats_reduce(w.partials, n_blocks(items), acc, st);
         if (rc) return rc;
         off += items;
         seg += n_segments(items);
@@ -224,7 +234,7 @@ int latec_quantize(const latec_quant_params* prm, double eb, uint64_t items, con
     if (!workspace || workspace_bytes < latec_flat_workspace_bytes(items, prm->dtype))
         return LATEC_ERR_WORKSPACE;
     StageWs w;
-    stage_ws(nullptr, items, elem, &w, workspace);
+    stage_ws(items, 0, 1, elem, &w, workspace);
     QParams q;
     if (!make_q(prm, eb, items, q)) return LATEC_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
@@ -235,11 +245,9 @@ int latec_quantize(const latec_quant_params* prm, double eb, uint64_t items, con
         return LATEC_ERR_CUDA;
     StageAcc* acc = (StageAcc*)stats;
     int rc = launch_quantize_flat(q, prm->dtype, items, x, pred, codes, w.staging, w.tile_cnt,
-                                  hist_total, hist_seg, acc, w.partials, recon_out, st);
-    if (!rc) rc = launch_tile_scan(w.tile_cnt, n_tiles(items), w.tile_off, &acc->n_out, st);
+                                  w.tile_off, hist_total, hist_seg, acc, w.partials, recon_out, st);
     if (!rc)
         rc = launch_compact(codes, items, w.staging, elem, w.tile_cnt, w.tile_off, outliers, st);
-    if (!rc) rc = launch_stats_reduce(w.partials, n_blocks(items), acc, st);
     return rc;
 }
 
@@ -249,34 +257,41 @@ int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
                         uint32_t* err, void* workspace, uint64_t workspace_bytes, void* stream) {
     if (!plan || !valid_params(prm) || !stage_eb || !codes || !out_off || !n_out || !recon || !err)
         return LATEC_ERR_ARG;
-    const int C = prm->channels, elem = elem_of(prm->dtype);
+    const int C = prm->channels;
     if (!workspace || workspace_bytes < latec_stage_workspace_bytes(plan, C, prm->dtype))
         return LATEC_ERR_WORKSPACE;
-    uint64_t m = 0;
-    for (auto& d : plan->stages) m = (uint64_t)d.n * C > m ? (uint64_t)d.n * C : m;
+    uint64_t m, tiles_all;
+    plan_sizes(plan, C, &m, &tiles_all);
+    const int ns = (int)plan->stages.size();
     StageWs w;
-    stage_ws(nullptr, m, elem, &w, workspace);
+    stage_ws(m, tiles_all, ns, elem_of(prm->dtype), &w, workspace);
     cudaStream_t st = (cudaStream_t)stream;
+    // all stages' outlier tiles in two launches
+    std::vector<DecStage> ds(ns);
     uint64_t off = 0;
-    for (int t = 0; t < (int)plan->stages.size(); t++) {
+    uint32_t tile0 = 0;
+    for (int t = 0; t < ns; t++) {
+        const uint64_t items = (uint64_t)plan->stages[t].n * C;
+        ds[t] = DecStage{off, items, tile0, n_out[t]};
+        off += items;
+        tile0 += n_tiles(items);
+    }
+    if (cudaMemcpyAsync(w.dec, ds.data(), sizeof(DecStage) * ns, cudaMemcpyHostToDevice, st) !=
+        cudaSuccess)
+        return LATEC_ERR_CUDA;
+    int rc = launch_count_zeros_all(w.dec, ns, tile0, codes, w.tile_cnt, st);
+    if (!rc) rc = launch_tile_offsets_all(w.dec, ns, w.tile_cnt, w.tile_off, err, st);
+    if (rc) return rc;
+    for (int t = 0; t < ns; t++) {
         const StageDesc& d = plan->stages[t];
-        const uint64_t items = (uint64_t)d.n * C;
-        if (!items) continue;
+        if (!ds[t].items) continue;
         QParams q;
         if (!make_q(prm, stage_eb[t], plan->points, q)) return LATEC_ERR_ARG;
-        int rc = launch_count_zeros(codes + off, items, w.tile_cnt, st);
-        if (!rc) rc = launch_tile_scan(w.tile_cnt, n_tiles(items), w.tile_off, w.total, st);
-        if (!rc) {
-            k_check_count<<<1, 32, 0, st>>>(w.total, n_out[t], err);
-            count_launches(1);
-            rc = cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
-        }
-        if (!rc)
-            rc = launch_interp_dequant(d, q, prm->dtype, t == 0, codes + off,
-                                       outliers ? (const uint8_t*)outliers + out_off[t] : nullptr,
-                                       w.tile_cnt, w.tile_off, n_out[t], recon, err, st);
+        rc = launch_interp_dequant(d, q, prm->dtype, t == 0, codes + ds[t].codes_off,
+                                   outliers ? (const uint8_t*)outliers + out_off[t] : nullptr,
+                                   w.tile_cnt + ds[t].tile0, w.tile_off + ds[t].tile0, n_out[t],
+                                   recon, err, st);
         if (rc) return rc;
-        off += items;
     }
     return LATEC_OK;
 }

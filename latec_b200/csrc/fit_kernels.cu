@@ -54,74 +54,89 @@ __global__ void k_fit_counts(const FitStage* __restrict__ fs, const uint32_t* __
     counts[f.counts_off + sym] = v;
 }
 
-// One CTA per (stage, shape, level): the pairwise tree sum of the products.
-// Each thread folds a power-of-two run of adjacent terms with a binary-counter
-// stack (exactly the perfect tree over its run); the CTA then combines runs by
-// adjacent pairs with doubling strides.
+// One CTA per (stage, shape); each warp computes the cost of levels
+// warp, warp + 8, ...: lane l folds the power-of-two run of adjacent terms
+// [l*m, (l+1)*m) with a binary-counter stack (exactly the perfect tree over its
+// run), then the warp combines runs by adjacent pairs with doubling strides,
+// which is the perfect binary tree over the whole alphabet.
 __global__ void __launch_bounds__(256)
     k_fit_costs(const FitStage* __restrict__ fs, const uint32_t* __restrict__ counts,
                 double* __restrict__ costs) {
-    const uint32_t level = blockIdx.x;  // 0..63
-    const uint32_t sh = blockIdx.y;
-    const FitStage& f = fs[blockIdx.z];
+    const uint32_t sh = blockIdx.x;
+    const FitStage& f = fs[blockIdx.y];
     if (sh >= f.n_shapes) return;
     const uint32_t A = f.alphabet;
-    const uint32_t T = A < 256 ? A : 256;  // power of two
-    const uint32_t m = A / T;               // power of two
-    __shared__ double red[256];
-    const float* W = (const float*)f.w_table + ((uint64_t)sh * 64 + level) * A;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t m = A >= 32 ? A / 32 : 1;  // terms per lane (power of two)
     const uint32_t* cnt = counts + f.counts_off;
-    double acc = 0.0;
-    if (threadIdx.x < T) {
-        double stack[17];
-        int depth[17];
-        int top = 0;
-        const uint32_t a = threadIdx.x * m;
-        for (uint32_t i = 0; i < m; i++) {
-            double v = __dmul_rn((double)W[a + i], (double)cnt[a + i]);
-            int d = 0;
-            while (top > 0 && depth[top - 1] == d) {
-                v = __dadd_rn(stack[--top], v);
-                d++;
+    for (uint32_t level = warp; level < 64; level += 8) {
+        const float* W = (const float*)f.w_table + ((uint64_t)sh * 64 + level) * A;
+        double v = 0.0;
+        const uint32_t a = lane * m;
+        if (a < A) {
+            double stack[12];
+            int depth[12];
+            int top = 0;
+            for (uint32_t i = 0; i < m; i++) {
+                double t = __dmul_rn((double)W[a + i], (double)cnt[a + i]);
+                int dd = 0;
+                while (top > 0 && depth[top - 1] == dd) {
+                    t = __dadd_rn(stack[--top], t);
+                    dd++;
+                }
+                stack[top] = t;
+                depth[top] = dd;
+                top++;
             }
-            stack[top] = v;
-            depth[top] = d;
-            top++;
+            v = stack[0];
         }
-        acc = stack[0];  // m is a power of two: one full tree remains
+        const uint32_t runs = A >= 32 ? 32 : A;
+        for (uint32_t st = 1; st < runs; st <<= 1) {
+            const double o = __shfl_down_sync(0xffffffffu, v, st);
+            if ((lane & (2 * st - 1)) == 0) v = __dadd_rn(v, o);
+        }
+        if (lane == 0) costs[((uint64_t)blockIdx.y * 24 + sh) * 64 + level] = v;
     }
-    red[threadIdx.x] = acc;
-    __syncthreads();
-    for (uint32_t s = 1; s < T; s <<= 1) {
-        if (threadIdx.x < T && (threadIdx.x & (2 * s - 1)) == 0)
-            red[threadIdx.x] = __dadd_rn(red[threadIdx.x], red[threadIdx.x + s]);
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) costs[((uint64_t)blockIdx.z * 24 + sh) * 64 + level] = red[0];
 }
 
-// Per stage: first argmin over levels, first strictly smaller over shapes.
+// One warp per stage: first argmin over levels (lower level wins ties), then
+// the first strictly smaller cost over shapes in dictionary order.
 __global__ void k_fit_pick(const FitStage* __restrict__ fs, int n, const double* __restrict__ costs,
                            double* __restrict__ out) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x;
     if (t >= n) return;
+    const int lane = threadIdx.x;
     const FitStage& f = fs[t];
     double best = __longlong_as_double(0x7ff0000000000000ll);  // +inf
     int bl = 0, bs = 0;
     for (uint32_t sh = 0; sh < f.n_shapes; sh++) {
         const double* c = costs + ((uint64_t)t * 24 + sh) * 64;
-        int l = 0;
-        for (int k = 1; k < 64; k++)
-            if (c[k] < c[l]) l = k;
-        if (c[l] < best) {
-            best = c[l];
+        double v = c[lane];
+        int l = lane;
+        const double v2 = c[lane + 32];
+        if (v2 < v) {
+            v = v2;
+            l = lane + 32;
+        }
+        for (int o = 16; o; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+            const int ol = __shfl_xor_sync(0xffffffffu, l, o);
+            if (ov < v || (ov == v && ol < l)) {
+                v = ov;
+                l = ol;
+            }
+        }
+        if (v < best) {
+            best = v;
             bl = l;
             bs = (int)f.shape_ids[sh];
         }
     }
-    out[3 * t] = best;
-    out[3 * t + 1] = (double)bl;
-    out[3 * t + 2] = (double)bs;
+    if (lane == 0) {
+        out[3 * t] = best;
+        out[3 * t + 1] = (double)bl;
+        out[3 * t + 2] = (double)bs;
+    }
 }
 
 }  // namespace latec
@@ -152,8 +167,8 @@ int latec_fit_const(const void* stages_host, int32_t n, const uint32_t* hist_seg
     if (cudaMemcpyAsync(d, h, sizeof(FitStage) * n, cudaMemcpyHostToDevice, st) != cudaSuccess)
         return LATEC_ERR_CUDA;
     k_fit_counts<<<dim3((max_a + 255) / 256, n), 256, 0, st>>>(d, hist_seg, hist_total, counts);
-    k_fit_costs<<<dim3(64, max_s, n), 256, 0, st>>>(d, counts, costs);
-    k_fit_pick<<<(n + 63) / 64, 64, 0, st>>>(d, n, costs, out);
+    k_fit_costs<<<dim3(max_s, n), 256, 0, st>>>(d, counts, costs);
+    k_fit_pick<<<n, 32, 0, st>>>(d, n, costs, out);
     count_launches(3);
     return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
 }

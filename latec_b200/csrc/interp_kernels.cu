@@ -246,6 +246,63 @@ __device__ __forceinline__ void block_finish(BlockAcc& a, double* partials, Stag
     }
 }
 
+// ---------------------------------------------------------------- stage tail
+// Run by the last CTA of a stage pass (the one whose arrival completes the
+// per-stage counter): the fixed-order reduction of the per-CTA statistics and
+// the exclusive scan of the per-tile outlier counts. Both are deterministic:
+// neither depends on which CTA happens to arrive last.
+__device__ void stage_tail(const double* __restrict__ partials, uint32_t blocks,
+                           const uint32_t* __restrict__ tile_cnt, uint32_t tiles,
+                           uint32_t* __restrict__ tile_off, StageAcc* __restrict__ acc) {
+    __shared__ double red[5][THREADS];
+    __shared__ uint32_t sc[THREADS];
+    double s[5] = {0, 0, 0, 0, 0};
+    for (uint32_t b = threadIdx.x; b < blocks; b += THREADS) {
+        for (int k = 0; k < 4; k++) s[k] += partials[(size_t)b * 5 + k];
+        s[4] = fmax(s[4], partials[(size_t)b * 5 + 4]);
+    }
+    for (int k = 0; k < 5; k++) red[k][threadIdx.x] = s[k];
+    // tile scan: thread t sums a contiguous run, then a block scan of the runs
+    const uint32_t per = (tiles + THREADS - 1) / THREADS;
+    const uint32_t a = threadIdx.x * per, e = min(tiles, a + per);
+    uint32_t run = 0;
+    for (uint32_t i = a; i < e; i++) run += tile_cnt[i];
+    sc[threadIdx.x] = run;
+    __syncthreads();
+    for (int o = THREADS / 2; o; o >>= 1) {
+        if (threadIdx.x < (unsigned)o) {
+            for (int k = 0; k < 4; k++) red[k][threadIdx.x] += red[k][threadIdx.x + o];
+            red[4][threadIdx.x] = fmax(red[4][threadIdx.x], red[4][threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    for (int o = 1; o < THREADS; o <<= 1) {
+        const uint32_t v = threadIdx.x >= (unsigned)o ? sc[threadIdx.x - o] : 0u;
+        __syncthreads();
+        sc[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t off = sc[threadIdx.x] - run;
+    for (uint32_t i = a; i < e; i++) {
+        tile_off[i] = off;
+        off += tile_cnt[i];
+    }
+    if (threadIdx.x == THREADS - 1) acc->n_out = sc[THREADS - 1];
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 5; k++) acc->stats[k] = red[k][0];
+}
+
+// Arrival counter: true in the CTA that finishes the stage.
+__device__ __forceinline__ bool last_block(StageAcc* acc) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(&acc->done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last;
+}
+
 // ---------------------------------------------------------------- encode
 // A CTA owns a contiguous run of 512-point groups of the stage's ranks; each
 // thread takes two points of a group (ranks g + tid and g + 256 + tid, so
@@ -318,12 +375,13 @@ __device__ __forceinline__ void flush_hist(uint32_t* sh_hist, uint32_t* hist_seg
 }
 
 template <typename T, int ND, int KIND, int CUBIC>
-__global__ void __launch_bounds__(THREADS)
+__global__ void __launch_bounds__(THREADS, 5)
     k_interp_quant(const StageDesc d, const QParams q, const int is_anchor, const uint32_t gpb,
                    const T* __restrict__ x, T* __restrict__ recon, uint16_t* __restrict__ codes,
                    T* __restrict__ staging, uint32_t* __restrict__ tile_cnt,
-                   uint32_t* __restrict__ hist_total, uint32_t* __restrict__ hist_seg,
-                   StageAcc* __restrict__ acc, double* __restrict__ partials) {
+                   uint32_t* __restrict__ tile_off, uint32_t* __restrict__ hist_total,
+                   uint32_t* __restrict__ hist_seg, StageAcc* __restrict__ acc,
+                   double* __restrict__ partials) {
     __shared__ uint32_t sh_hist[HBINS];
     for (int b = threadIdx.x; b < HBINS; b += THREADS) sh_hist[b] = 0;
     __syncthreads();
@@ -371,6 +429,7 @@ __global__ void __launch_bounds__(THREADS)
     __syncthreads();
     flush_hist(sh_hist, hist_seg, cur_seg);
     block_finish(a, partials, acc);
+    if (last_block(acc)) stage_tail(partials, gridDim.x, tile_cnt, n_tiles_of(items), tile_off, acc);
 }
 
 // Quantize a compact array against a given prediction (predictor-agnostic
@@ -381,9 +440,10 @@ __global__ void __launch_bounds__(THREADS)
     k_quantize_flat(const QParams q, const uint64_t items, const uint32_t gpb,
                     const T* __restrict__ x, const T* __restrict__ pred,
                     uint16_t* __restrict__ codes, T* __restrict__ staging,
-                    uint32_t* __restrict__ tile_cnt, uint32_t* __restrict__ hist_total,
-                    uint32_t* __restrict__ hist_seg, StageAcc* __restrict__ acc,
-                    double* __restrict__ partials, T* __restrict__ recon_out) {
+                    uint32_t* __restrict__ tile_cnt, uint32_t* __restrict__ tile_off,
+                    uint32_t* __restrict__ hist_total, uint32_t* __restrict__ hist_seg,
+                    StageAcc* __restrict__ acc, double* __restrict__ partials,
+                    T* __restrict__ recon_out) {
     __shared__ uint32_t sh_hist[HBINS];
     for (int b = threadIdx.x; b < HBINS; b += THREADS) sh_hist[b] = 0;
     __syncthreads();
@@ -415,6 +475,7 @@ __global__ void __launch_bounds__(THREADS)
     __syncthreads();
     flush_hist(sh_hist, hist_seg, cur_seg);
     block_finish(a, partials, acc);
+    if (last_block(acc)) stage_tail(partials, gridDim.x, tile_cnt, n_tiles_of(items), tile_off, acc);
 }
 
 // Prediction only (the predictor plugin's ``predict``): compact output.
@@ -437,14 +498,22 @@ __global__ void __launch_bounds__(THREADS)
 }
 
 // ---------------------------------------------------------------- scans
+// Decode: zero codes (outliers) per 2048-code tile of every stage in one pass.
 __global__ void __launch_bounds__(THREADS)
-    k_count_zeros(const uint16_t* __restrict__ codes, const uint64_t items,
-                  uint32_t* __restrict__ tile_cnt) {
-    const uint64_t tile_base = (uint64_t)blockIdx.x * TILE;
+    k_count_zeros_all(const DecStage* __restrict__ ds, int n_stages, const uint16_t* __restrict__ codes,
+                      uint32_t* __restrict__ tile_cnt) {
+    const uint32_t gt = blockIdx.x;
+    int lo = 0, hi = n_stages;  // last stage with tile0 <= gt
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (ds[mid].tile0 <= gt) lo = mid; else hi = mid;
+    }
+    const DecStage& d = ds[lo];
+    const uint64_t base = (uint64_t)(gt - d.tile0) * TILE;
     int cnt = 0;
     for (int k = 0; k < TILE / THREADS; k++) {
-        const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
-        cnt += (i < items && codes[i] == 0) ? 1 : 0;
+        const uint64_t i = base + (uint64_t)k * THREADS + threadIdx.x;
+        cnt += (i < d.items && codes[d.codes_off + i] == 0) ? 1 : 0;
     }
     __shared__ int sh[THREADS / 32];
     int v = cnt;
@@ -453,35 +522,40 @@ __global__ void __launch_bounds__(THREADS)
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
     __syncthreads();
     if (threadIdx.x == 0) {
-        int s = 0;
-        for (int w = 0; w < THREADS / 32; w++) s += sh[w];
-        tile_cnt[blockIdx.x] = (uint32_t)s;
+        int t = 0;
+        for (int w = 0; w < THREADS / 32; w++) t += sh[w];
+        tile_cnt[gt] = (uint32_t)t;
     }
 }
 
-// Exclusive scan of per-tile counts by one CTA; total written to *total.
-__global__ void __launch_bounds__(1024)
-    k_tile_scan(const uint32_t* __restrict__ cnt, const uint32_t tiles,
-                uint32_t* __restrict__ off, uint32_t* __restrict__ total) {
-    __shared__ uint32_t sh[1024];
-    const uint32_t per = (tiles + 1023) / 1024;
-    const uint32_t a = threadIdx.x * per, b = min(tiles, a + per);
-    uint32_t s = 0;
-    for (uint32_t i = a; i < b; i++) s += cnt[i];
-    sh[threadIdx.x] = s;
+// Decode: per stage (one CTA each) the exclusive tile offsets and the check
+// that the stage's zero codes match its stored outlier count.
+__global__ void __launch_bounds__(THREADS)
+    k_tile_offsets_all(const DecStage* __restrict__ ds, const uint32_t* __restrict__ tile_cnt,
+                       uint32_t* __restrict__ tile_off, uint32_t* __restrict__ err) {
+    const DecStage& d = ds[blockIdx.x];
+    const uint32_t tiles = n_tiles_of(d.items);
+    if (!tiles) return;
+    __shared__ uint32_t sc[THREADS];
+    const uint32_t* cnt = tile_cnt + d.tile0;
+    const uint32_t per = (tiles + THREADS - 1) / THREADS;
+    const uint32_t a = threadIdx.x * per, e = min(tiles, a + per);
+    uint32_t run = 0;
+    for (uint32_t i = a; i < e; i++) run += cnt[i];
+    sc[threadIdx.x] = run;
     __syncthreads();
-    for (int o = 1; o < 1024; o <<= 1) {
-        uint32_t v = threadIdx.x >= (unsigned)o ? sh[threadIdx.x - o] : 0u;
+    for (int o = 1; o < THREADS; o <<= 1) {
+        const uint32_t v = threadIdx.x >= (unsigned)o ? sc[threadIdx.x - o] : 0u;
         __syncthreads();
-        sh[threadIdx.x] += v;
+        sc[threadIdx.x] += v;
         __syncthreads();
     }
-    uint32_t run = sh[threadIdx.x] - s;
-    for (uint32_t i = a; i < b; i++) {
-        off[i] = run;
-        run += cnt[i];
+    uint32_t off = sc[threadIdx.x] - run;
+    for (uint32_t i = a; i < e; i++) {
+        tile_off[d.tile0 + i] = off;
+        off += cnt[i];
     }
-    if (threadIdx.x == 1023) *total = sh[1023];
+    if (threadIdx.x == THREADS - 1 && sc[THREADS - 1] != d.n_out) atomicOr(err, 1u);
 }
 
 // Block-local exclusive scan of a per-thread flag in item order (k-major).
@@ -506,44 +580,21 @@ __global__ void __launch_bounds__(THREADS)
               const uint8_t* __restrict__ staging, const int elem,
               const uint32_t* __restrict__ tile_cnt, const uint32_t* __restrict__ tile_off,
               uint8_t* __restrict__ out) {
-    const uint32_t tile = blockIdx.x;
-    if (tile_cnt[tile] == 0) return;
-    const uint64_t tile_base = (uint64_t)tile * TILE;
-    uint32_t run = tile_off[tile];
-    for (int k = 0; k < TILE / THREADS; k++) {
-        const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
-        const bool z = i < items && codes[i] == 0;
-        uint32_t tot;
-        const uint32_t pos = run + block_excl_flag(z, tot);
-        if (z) {
-            for (int b = 0; b < elem; b++) out[(uint64_t)pos * elem + b] = staging[i * elem + b];
+    const uint32_t tiles = n_tiles_of(items);
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        if (tile_cnt[tile] == 0) continue;  // uniform across the CTA
+        const uint64_t tile_base = (uint64_t)tile * TILE;
+        uint32_t run = tile_off[tile];
+        for (int k = 0; k < TILE / THREADS; k++) {
+            const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
+            const bool z = i < items && codes[i] == 0;
+            uint32_t tot;
+            const uint32_t pos = run + block_excl_flag(z, tot);
+            if (z)
+                for (int b = 0; b < elem; b++) out[(uint64_t)pos * elem + b] = staging[i * elem + b];
+            run += tot;
         }
-        run += tot;
     }
-}
-
-// Deterministic block reduction of the per-block statistics: a fixed
-// thread -> block assignment and a fixed tree, independent of timing.
-__global__ void __launch_bounds__(256)
-    k_stats_reduce(const double* __restrict__ partials, const uint32_t blocks,
-                   StageAcc* __restrict__ acc) {
-    __shared__ double sh[5][256];
-    double s[5] = {0, 0, 0, 0, 0};
-    for (uint32_t b = threadIdx.x; b < blocks; b += 256) {
-        for (int k = 0; k < 4; k++) s[k] += partials[(size_t)b * 5 + k];
-        s[4] = fmax(s[4], partials[(size_t)b * 5 + 4]);
-    }
-    for (int k = 0; k < 5; k++) sh[k][threadIdx.x] = s[k];
-    __syncthreads();
-    for (int o = 128; o; o >>= 1) {
-        if (threadIdx.x < (unsigned)o) {
-            for (int k = 0; k < 4; k++) sh[k][threadIdx.x] += sh[k][threadIdx.x + o];
-            sh[4][threadIdx.x] = fmax(sh[4][threadIdx.x], sh[4][threadIdx.x + o]);
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0)
-        for (int k = 0; k < 5; k++) acc->stats[k] = sh[k][0];
 }
 
 // ---------------------------------------------------------------- decode
@@ -605,7 +656,7 @@ __device__ __forceinline__ void dequant_point(const StageDesc& d, const QParams&
 // Tiles without outliers (the common case) take a barrier-free path; others
 // rank their outliers with a block scan in item order.
 template <typename T, int ND, int KIND, int CUBIC>
-__global__ void __launch_bounds__(THREADS)
+__global__ void __launch_bounds__(THREADS, 5)
     k_interp_dequant(const StageDesc d, const QParams q, const int is_anchor,
                      const uint16_t* __restrict__ codes, const uint8_t* __restrict__ outliers,
                      const uint32_t* __restrict__ tile_cnt, const uint32_t* __restrict__ tile_off,
@@ -705,8 +756,8 @@ uint32_t encode_blocks(uint64_t items) {
 
 int launch_interp_quant(const StageDesc& d, const QParams& q, int dtype, int is_anchor,
                         const void* x, void* recon, uint16_t* codes, void* staging,
-                        uint32_t* tile_cnt, uint32_t* hist_total, uint32_t* hist_seg,
-                        StageAcc* acc, double* partials, cudaStream_t st) {
+                        uint32_t* tile_cnt, uint32_t* tile_off, uint32_t* hist_total,
+                        uint32_t* hist_seg, StageAcc* acc, double* partials, cudaStream_t st) {
     const uint64_t items = (uint64_t)q.channels * d.n;
     if (!items) return LATEC_OK;
     uint32_t blocks;
@@ -714,15 +765,15 @@ int launch_interp_quant(const StageDesc& d, const QParams& q, int dtype, int is_
     if (cudaMemsetAsync(tile_cnt, 0, sizeof(uint32_t) * n_tiles(items), st) != cudaSuccess)
         return LATEC_ERR_CUDA;
     LATEC_DISPATCH((k_interp_quant<T, ND, KIND, CUBIC><<<blocks, THREADS, 0, st>>>(
-        d, q, is_anchor, gpb, (const T*)x, (T*)recon, codes, (T*)staging, tile_cnt, hist_total,
-        hist_seg, acc, partials)));
+        d, q, is_anchor, gpb, (const T*)x, (T*)recon, codes, (T*)staging, tile_cnt, tile_off,
+        hist_total, hist_seg, acc, partials)));
     return last_err();
 }
 
 int launch_quantize_flat(const QParams& q, int dtype, uint64_t items, const void* x,
                          const void* pred, uint16_t* codes, void* staging, uint32_t* tile_cnt,
-                         uint32_t* hist_total, uint32_t* hist_seg, StageAcc* acc,
-                         double* partials, void* recon_out, cudaStream_t st) {
+                         uint32_t* tile_off, uint32_t* hist_total, uint32_t* hist_seg,
+                         StageAcc* acc, double* partials, void* recon_out, cudaStream_t st) {
     if (!items) return LATEC_OK;
     uint32_t blocks;
     const uint32_t gpb = groups_per_block(items, &blocks);
@@ -731,11 +782,11 @@ int launch_quantize_flat(const QParams& q, int dtype, uint64_t items, const void
     if (dtype == LATEC_F64)
         k_quantize_flat<double><<<blocks, THREADS, 0, st>>>(
             q, items, gpb, (const double*)x, (const double*)pred, codes, (double*)staging,
-            tile_cnt, hist_total, hist_seg, acc, partials, (double*)recon_out);
+            tile_cnt, tile_off, hist_total, hist_seg, acc, partials, (double*)recon_out);
     else
         k_quantize_flat<float><<<blocks, THREADS, 0, st>>>(
             q, items, gpb, (const float*)x, (const float*)pred, codes, (float*)staging, tile_cnt,
-            hist_total, hist_seg, acc, partials, (float*)recon_out);
+            tile_off, hist_total, hist_seg, acc, partials, (float*)recon_out);
     return last_err();
 }
 
@@ -749,17 +800,17 @@ int launch_interp_predict(const StageDesc& d, const QParams& q, int dtype, const
     return last_err();
 }
 
-int launch_count_zeros(const uint16_t* codes, uint64_t items, uint32_t* tile_cnt,
-                       cudaStream_t st) {
-    if (!items) return LATEC_OK;
-    k_count_zeros<<<n_tiles(items), THREADS, 0, st>>>(codes, items, tile_cnt);
+int launch_count_zeros_all(const DecStage* ds, int n_stages, uint32_t total_tiles,
+                           const uint16_t* codes, uint32_t* tile_cnt, cudaStream_t st) {
+    if (!total_tiles) return LATEC_OK;
+    k_count_zeros_all<<<total_tiles, THREADS, 0, st>>>(ds, n_stages, codes, tile_cnt);
     return last_err();
 }
 
-int launch_tile_scan(const uint32_t* tile_cnt, uint32_t tiles, uint32_t* tile_off,
-                     uint32_t* total, cudaStream_t st) {
-    if (!tiles) return LATEC_OK;
-    k_tile_scan<<<1, 1024, 0, st>>>(tile_cnt, tiles, tile_off, total);
+int launch_tile_offsets_all(const DecStage* ds, int n_stages, const uint32_t* tile_cnt,
+                            uint32_t* tile_off, uint32_t* err, cudaStream_t st) {
+    if (!n_stages) return LATEC_OK;
+    k_tile_offsets_all<<<n_stages, THREADS, 0, st>>>(ds, tile_cnt, tile_off, err);
     return last_err();
 }
 
@@ -767,15 +818,9 @@ int launch_compact(const uint16_t* codes, uint64_t items, const void* staging, i
                    const uint32_t* tile_cnt, const uint32_t* tile_off, void* out,
                    cudaStream_t st) {
     if (!items) return LATEC_OK;
-    k_compact<<<n_tiles(items), THREADS, 0, st>>>(codes, items, (const uint8_t*)staging, elem,
-                                                   tile_cnt, tile_off, (uint8_t*)out);
-    return last_err();
-}
-
-int launch_stats_reduce(const double* partials, uint32_t blocks, StageAcc* acc,
-                        cudaStream_t st) {
-    if (!blocks) return LATEC_OK;
-    k_stats_reduce<<<1, 256, 0, st>>>(partials, blocks, acc);
+    const uint32_t tiles = n_tiles(items);
+    k_compact<<<tiles < 592u ? tiles : 592u, THREADS, 0, st>>>(
+        codes, items, (const uint8_t*)staging, elem, tile_cnt, tile_off, (uint8_t*)out);
     return last_err();
 }
 

@@ -31,11 +31,23 @@ struct QParams {
 struct StageAcc {
     uint32_t n_out;
     uint32_t maxq;
-    uint32_t pad0, pad1;
+    uint32_t done;   // CTAs of the stage pass that have finished
+    uint32_t pad1;
     double stats[5];  // pred_sae, pred_sse, recon_sae, recon_sse, recon_max
 };
 
 inline uint32_t n_tiles(uint64_t items) { return (uint32_t)((items + TILE - 1) / TILE); }
+__host__ __device__ inline uint32_t n_tiles_of(uint64_t items) {
+    return (uint32_t)((items + TILE - 1) / TILE);
+}
+
+// Decode: one stage of the all-stage tile passes.
+struct DecStage {
+    uint64_t codes_off;  // first code of the stage
+    uint64_t items;      // codes of the stage
+    uint32_t tile0;      // first global tile of the stage
+    uint32_t n_out;      // outliers stored for the stage
+};
 // CTAs of the encode kernels for a stage of `items` points (partials rows).
 uint32_t encode_blocks(uint64_t items);
 inline uint32_t n_blocks(uint64_t items) { return encode_blocks(items); }
@@ -46,26 +58,24 @@ inline uint32_t n_segments(uint64_t items) {
 // Launchers (interp_kernels.cu). items = channels * stage points.
 int launch_interp_quant(const StageDesc& d, const QParams& q, int dtype, int is_anchor,
                         const void* x, void* recon, uint16_t* codes, void* staging,
-                        uint32_t* tile_cnt, uint32_t* hist_total, uint32_t* hist_seg,
-                        StageAcc* acc, double* partials, cudaStream_t st);
+                        uint32_t* tile_cnt, uint32_t* tile_off, uint32_t* hist_total,
+                        uint32_t* hist_seg, StageAcc* acc, double* partials, cudaStream_t st);
 int launch_interp_predict(const StageDesc& d, const QParams& q, int dtype, const void* recon,
                           void* pred, cudaStream_t st);
-int launch_count_zeros(const uint16_t* codes, uint64_t items, uint32_t* tile_cnt,
-                       cudaStream_t st);
-int launch_tile_scan(const uint32_t* tile_cnt, uint32_t tiles, uint32_t* tile_off,
-                     uint32_t* total, cudaStream_t st);
+int launch_count_zeros_all(const DecStage* ds, int n_stages, uint32_t total_tiles,
+                           const uint16_t* codes, uint32_t* tile_cnt, cudaStream_t st);
+int launch_tile_offsets_all(const DecStage* ds, int n_stages, const uint32_t* tile_cnt,
+                            uint32_t* tile_off, uint32_t* err, cudaStream_t st);
 int launch_compact(const uint16_t* codes, uint64_t items, const void* staging, int elem,
                    const uint32_t* tile_cnt, const uint32_t* tile_off, void* out,
                    cudaStream_t st);
-int launch_stats_reduce(const double* partials, uint32_t blocks, StageAcc* acc,
-                        cudaStream_t st);
 int launch_interp_dequant(const StageDesc& d, const QParams& q, int dtype, int is_anchor,
                           const uint16_t* codes, const void* outliers, const uint32_t* tile_cnt,
                           const uint32_t* tile_off, uint32_t n_out, void* recon, uint32_t* err,
                           cudaStream_t st);
 int launch_quantize_flat(const QParams& q, int dtype, uint64_t items, const void* x,
                          const void* pred, uint16_t* codes, void* staging, uint32_t* tile_cnt,
-                         uint32_t* hist_total, uint32_t* hist_seg, StageAcc* acc,
-                         double* partials, void* recon_out, cudaStream_t st);
+                         uint32_t* tile_off, uint32_t* hist_total, uint32_t* hist_seg,
+                         StageAcc* acc, double* partials, void* recon_out, cudaStream_t st);
 
 }  // namespace latec
