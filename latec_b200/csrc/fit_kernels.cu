@@ -54,11 +54,12 @@ __global__ void k_fit_counts(const FitStage* __restrict__ fs, const uint32_t* __
     counts[f.counts_off + sym] = v;
 }
 
-// One CTA per (stage, shape); each warp computes the cost of levels
-// warp, warp + 8, ...: lane l folds the power-of-two run of adjacent terms
-// [l*m, (l+1)*m) with a binary-counter stack (exactly the perfect tree over its
-// run), then the warp combines runs by adjacent pairs with doubling strides,
-// which is the perfect binary tree over the whole alphabet.
+// One CTA per (stage, shape); warp w computes the cost of levels w, w + 8, ...
+// For each level the warp walks the alphabet 32 adjacent terms at a time
+// (coalesced loads): a shuffle tree over adjacent lanes sums the 32 products
+// (the perfect binary tree over those terms) and lane 0 folds the successive
+// 32-term subtree sums with a binary-counter stack, which completes the
+// perfect binary tree over the whole power-of-two alphabet.
 __global__ void __launch_bounds__(256)
     k_fit_costs(const FitStage* __restrict__ fs, const uint32_t* __restrict__ counts,
                 double* __restrict__ costs) {
@@ -67,35 +68,32 @@ __global__ void __launch_bounds__(256)
     if (sh >= f.n_shapes) return;
     const uint32_t A = f.alphabet;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t m = A >= 32 ? A / 32 : 1;  // terms per lane (power of two)
+    const uint32_t width = A < 32 ? A : 32;  // terms per shuffle tree (power of two)
     const uint32_t* cnt = counts + f.counts_off;
     for (uint32_t level = warp; level < 64; level += 8) {
         const float* W = (const float*)f.w_table + ((uint64_t)sh * 64 + level) * A;
-        double v = 0.0;
-        const uint32_t a = lane * m;
-        if (a < A) {
-            double stack[12];
-            int depth[12];
-            int top = 0;
-            for (uint32_t i = 0; i < m; i++) {
-                double t = __dmul_rn((double)W[a + i], (double)cnt[a + i]);
+        double stack[12];
+        int depth[12];
+        int top = 0;
+        for (uint32_t base = 0; base < A; base += 32) {
+            const uint32_t i = base + lane;
+            double v = (lane < (int)width) ? __dmul_rn((double)W[i], (double)cnt[i]) : 0.0;
+            for (uint32_t st = 1; st < width; st <<= 1) {
+                const double o = __shfl_down_sync(0xffffffffu, v, st);
+                if ((lane & (2 * st - 1)) == 0) v = __dadd_rn(v, o);
+            }
+            if (lane == 0) {
                 int dd = 0;
                 while (top > 0 && depth[top - 1] == dd) {
-                    t = __dadd_rn(stack[--top], t);
+                    v = __dadd_rn(stack[--top], v);
                     dd++;
                 }
-                stack[top] = t;
+                stack[top] = v;
                 depth[top] = dd;
                 top++;
             }
-            v = stack[0];
         }
-        const uint32_t runs = A >= 32 ? 32 : A;
-        for (uint32_t st = 1; st < runs; st <<= 1) {
-            const double o = __shfl_down_sync(0xffffffffu, v, st);
-            if ((lane & (2 * st - 1)) == 0) v = __dadd_rn(v, o);
-        }
-        if (lane == 0) costs[((uint64_t)blockIdx.y * 24 + sh) * 64 + level] = v;
+        if (lane == 0) costs[((uint64_t)blockIdx.y * 24 + sh) * 64 + level] = stack[0];
     }
 }
 

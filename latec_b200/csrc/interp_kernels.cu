@@ -216,6 +216,7 @@ __device__ __forceinline__ uint32_t warp_umax(uint32_t v) {
 struct BlockAcc {
     double s[5];
     uint32_t maxq;
+    uint32_t nout;
 };
 
 // Per-block statistics: warp shuffles, then one partial row per CTA.
@@ -227,22 +228,29 @@ __device__ __forceinline__ void block_finish(BlockAcc& a, double* partials, Stag
     for (int k = 0; k < 4; k++) a.s[k] = warp_sum(a.s[k]);
     a.s[4] = warp_max(a.s[4]);
     a.maxq = warp_umax(a.maxq);
+    uint32_t no = a.nout;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) no += __shfl_xor_sync(0xffffffffu, no, o);
+    __shared__ uint32_t sh_no[THREADS / 32];
     if (lane == 0) {
 #pragma unroll
         for (int k = 0; k < 5; k++) sh_red[k][wid] = a.s[k];
         sh_mq[wid] = a.maxq;
+        sh_no[wid] = no;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         double s[5] = {0, 0, 0, 0, 0};
-        uint32_t mq = 0;
+        uint32_t mq = 0, nt = 0;
         for (int w = 0; w < THREADS / 32; w++) {
             for (int k = 0; k < 4; k++) s[k] += sh_red[k][w];
             s[4] = fmax(s[4], sh_red[4][w]);
             mq = max(mq, sh_mq[w]);
+            nt += sh_no[w];
         }
         for (int k = 0; k < 5; k++) partials[(size_t)blockIdx.x * 5 + k] = s[k];
         if (mq) atomicMax(&acc->maxq, mq);
+        if (nt) atomicAdd(&acc->nout, nt);
     }
 }
 
@@ -262,8 +270,10 @@ __device__ void stage_tail(const double* __restrict__ partials, uint32_t blocks,
         s[4] = fmax(s[4], partials[(size_t)b * 5 + 4]);
     }
     for (int k = 0; k < 5; k++) red[k][threadIdx.x] = s[k];
-    // tile scan: thread t sums a contiguous run, then a block scan of the runs
-    const uint32_t per = (tiles + THREADS - 1) / THREADS;
+    // tile scan (only when the stage has outliers): thread t sums a contiguous
+    // run of tiles, then a block scan of the runs
+    const bool any = *(volatile uint32_t*)&acc->nout != 0;
+    const uint32_t per = any ? (tiles + THREADS - 1) / THREADS : 0;
     const uint32_t a = threadIdx.x * per, e = min(tiles, a + per);
     uint32_t run = 0;
     for (uint32_t i = a; i < e; i++) run += tile_cnt[i];
@@ -287,7 +297,7 @@ __device__ void stage_tail(const double* __restrict__ partials, uint32_t blocks,
         tile_off[i] = off;
         off += tile_cnt[i];
     }
-    if (threadIdx.x == THREADS - 1) acc->n_out = sc[THREADS - 1];
+    if (threadIdx.x == THREADS - 1) acc->n_out = any ? sc[THREADS - 1] : 0u;
     if (threadIdx.x == 0)
         for (int k = 0; k < 5; k++) acc->stats[k] = red[k][0];
 }
@@ -342,6 +352,7 @@ __device__ __forceinline__ void encode_value(const QParams& q, uint64_t i, T xv,
     if (!o.code) {
         staging[i] = xv;
         atomicAdd(&tile_cnt[i / TILE], 1u);
+        a.nout++;
         key = 0;
     } else {
         const uint32_t aq = (uint32_t)abs(o.qv);
@@ -375,7 +386,7 @@ __device__ __forceinline__ void flush_hist(uint32_t* sh_hist, uint32_t* hist_seg
 }
 
 template <typename T, int ND, int KIND, int CUBIC>
-__global__ void __launch_bounds__(THREADS, 5)
+__global__ void __launch_bounds__(THREADS, 4)
     k_interp_quant(const StageDesc d, const QParams q, const int is_anchor, const uint32_t gpb,
                    const T* __restrict__ x, T* __restrict__ recon, uint16_t* __restrict__ codes,
                    T* __restrict__ staging, uint32_t* __restrict__ tile_cnt,
@@ -390,7 +401,7 @@ __global__ void __launch_bounds__(THREADS, 5)
     const uint64_t g0 = (uint64_t)blockIdx.x * gpb;
     const uint64_t g1 = g0 + gpb < groups ? g0 + gpb : groups;
     const int lane = threadIdx.x & 31;
-    BlockAcc a{{0, 0, 0, 0, 0}, 0};
+    BlockAcc a{{0, 0, 0, 0, 0}, 0, 0};
     uint32_t cur_seg = (uint32_t)((g0 * GROUP) >> SEG_SHIFT);
     for (uint64_t g = g0; g < g1; g++) {
         const uint64_t base = g * GROUP;
@@ -451,7 +462,7 @@ __global__ void __launch_bounds__(THREADS)
     const uint64_t g0 = (uint64_t)blockIdx.x * gpb;
     const uint64_t g1 = g0 + gpb < groups ? g0 + gpb : groups;
     const int lane = threadIdx.x & 31;
-    BlockAcc a{{0, 0, 0, 0, 0}, 0};
+    BlockAcc a{{0, 0, 0, 0, 0}, 0, 0};
     uint32_t cur_seg = (uint32_t)((g0 * GROUP) >> SEG_SHIFT);
     for (uint64_t g = g0; g < g1; g++) {
         const uint64_t base = g * GROUP;

@@ -32,7 +32,7 @@ struct StageAcc {
     uint32_t n_out;
     uint32_t maxq;
     uint32_t done;   // CTAs of the stage pass that have finished
-    uint32_t pad1;
+    uint32_t nout;   // running outlier total (CTA atomics)
     double stats[5];  // pred_sae, pred_sse, recon_sae, recon_sse, recon_max
 };
 
