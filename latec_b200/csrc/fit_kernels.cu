@@ -54,28 +54,32 @@ __global__ void k_fit_counts(const FitStage* __restrict__ fs, const uint32_t* __
     counts[f.counts_off + sym] = v;
 }
 
-// One CTA per (stage, shape); warp w computes the cost of levels w, w + 8, ...
-// For each level the warp walks the alphabet 32 adjacent terms at a time
-// (coalesced loads): a shuffle tree over adjacent lanes sums the 32 products
-// (the perfect binary tree over those terms) and lane 0 folds the successive
-// 32-term subtree sums with a binary-counter stack, which completes the
-// perfect binary tree over the whole power-of-two alphabet.
+// One CTA per (stage, shape, level). The alphabet is split into 8 (or fewer)
+// power-of-two spans of adjacent terms, one per warp; a warp walks its span 32
+// terms at a time (coalesced loads), sums each 32 with a shuffle tree over
+// adjacent lanes and folds the 32-term subtree sums in lane 0 with a
+// binary-counter stack; the warp totals are then paired adjacently. Every
+// partial sum is a node of the perfect binary tree over the alphabet.
 __global__ void __launch_bounds__(256)
     k_fit_costs(const FitStage* __restrict__ fs, const uint32_t* __restrict__ counts,
                 double* __restrict__ costs) {
-    const uint32_t sh = blockIdx.x;
-    const FitStage& f = fs[blockIdx.y];
+    const uint32_t level = blockIdx.x, sh = blockIdx.y;
+    const FitStage& f = fs[blockIdx.z];
     if (sh >= f.n_shapes) return;
     const uint32_t A = f.alphabet;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t width = A < 32 ? A : 32;  // terms per shuffle tree (power of two)
-    const uint32_t* cnt = counts + f.counts_off;
-    for (uint32_t level = warp; level < 64; level += 8) {
+    const uint32_t span = A >= 256 ? A / 8 : (A >= 32 ? 32 : A);  // terms per warp
+    const uint32_t n_warps = A / span;
+    const uint32_t width = span < 32 ? span : 32;
+    __shared__ double wsum[8];
+    if (warp < (int)n_warps) {
         const float* W = (const float*)f.w_table + ((uint64_t)sh * 64 + level) * A;
+        const uint32_t* cnt = counts + f.counts_off;
         double stack[12];
         int depth[12];
         int top = 0;
-        for (uint32_t base = 0; base < A; base += 32) {
+        const uint32_t a0 = warp * span;
+        for (uint32_t base = a0; base < a0 + span; base += 32) {
             const uint32_t i = base + lane;
             double v = (lane < (int)width) ? __dmul_rn((double)W[i], (double)cnt[i]) : 0.0;
             for (uint32_t st = 1; st < width; st <<= 1) {
@@ -93,7 +97,13 @@ __global__ void __launch_bounds__(256)
                 top++;
             }
         }
-        if (lane == 0) costs[((uint64_t)blockIdx.y * 24 + sh) * 64 + level] = stack[0];
+        if (lane == 0) wsum[warp] = stack[0];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (uint32_t st = 1; st < n_warps; st <<= 1)
+            for (uint32_t w = 0; w + st < n_warps; w += 2 * st) wsum[w] = __dadd_rn(wsum[w], wsum[w + st]);
+        costs[((uint64_t)blockIdx.z * 24 + sh) * 64 + level] = wsum[0];
     }
 }
 
@@ -165,7 +175,7 @@ int latec_fit_const(const void* stages_host, int32_t n, const uint32_t* hist_seg
     if (cudaMemcpyAsync(d, h, sizeof(FitStage) * n, cudaMemcpyHostToDevice, st) != cudaSuccess)
         return LATEC_ERR_CUDA;
     k_fit_counts<<<dim3((max_a + 255) / 256, n), 256, 0, st>>>(d, hist_seg, hist_total, counts);
-    k_fit_costs<<<dim3(max_s, n), 256, 0, st>>>(d, counts, costs);
+    k_fit_costs<<<dim3(64, max_s, n), 256, 0, st>>>(d, counts, costs);
     k_fit_pick<<<n, 32, 0, st>>>(d, n, costs, out);
     count_launches(3);
     return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;

@@ -79,6 +79,9 @@ __device__ __forceinline__ uint32_t widen(uint32_t sym, int radius, int kexp) {
 }
 
 // --------------------------------------------------------------- lanes
+// Encoder: one warp per chunk, steps k = K-1 .. 0. Codes are fetched 32 steps
+// at a time (32 independent coalesced loads per lane), so the per-step
+// dependency chain is only the state update and the renormalisation ballot.
 __global__ void __launch_bounds__(128)
     k_lanes_encode(const RansStageDesc* __restrict__ st, int n_stages, uint32_t total_chunks,
                    const uint16_t* __restrict__ codes, const uint8_t* __restrict__ levels,
@@ -96,38 +99,51 @@ __global__ void __launch_bounds__(128)
     uint32_t* refill_end = region + 64 + 32u * K;
     const uint16_t* c = codes + d.codes_off;
     const uint8_t* lv = d.per_point ? levels + d.codes_off : nullptr;
+    const uint64_t n = d.n;
     uint64_t x = LANE_L;
     uint32_t tail = 0;
     const unsigned lt = (1u << lane) - 1u;
-    for (int k = (int)K - 1; k >= 0; k--) {
-        const uint64_t i = base + (uint64_t)k * 32u + lane;
-        const bool valid = i < d.n;
-        EncSym e;
-        bool flush = false;
-        if (valid) {
-            const uint32_t sym = narrow(c[i], d.radius, d.kexp);
-            const uint32_t row = lv ? lv[i] : 0u;
-            if (sym >= d.alphabet) {
-                atomicOr(err, 2u);
-                e = enc[row * alpha1];
-            } else {
-                e = enc[row * alpha1 + sym];
+    for (int hb = (int)K; hb > 0; hb -= 32) {
+        const int lb = hb > 32 ? hb - 32 : 0;
+        uint32_t cb[32];
+        uint8_t rb[32];
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            const uint64_t i = base + (uint64_t)(lb + j) * 32u + lane;
+            const bool ok = lb + j < hb && i < n;
+            cb[j] = ok ? (uint32_t)c[i] : 0xFFFFFFFFu;
+            rb[j] = (ok && lv) ? lv[i] : 0;
+        }
+#pragma unroll
+        for (int j = 31; j >= 0; j--) {
+            if (lb + j >= hb) continue;  // uniform across the warp
+            const bool valid = cb[j] != 0xFFFFFFFFu;
+            EncSym e;
+            bool flush = false;
+            if (valid) {
+                const uint32_t sym = narrow(cb[j], d.radius, d.kexp);
+                if (sym >= d.alphabet) {
+                    atomicOr(err, 2u);
+                    e = enc[rb[j] * alpha1];
+                } else {
+                    e = enc[rb[j] * alpha1 + sym];
+                }
+                flush = x >= ((uint64_t)e.freq << 39);
             }
-            flush = x >= ((uint64_t)e.freq << 39);
-        }
-        const unsigned bal = __ballot_sync(0xffffffffu, flush);
-        const uint32_t ne = __popc(bal);
-        if (flush) {
-            refill_end[-(int64_t)tail - (int64_t)ne + __popc(bal & lt)] = (uint32_t)x;
-            x >>= 32;
-        }
-        tail += ne;
-        if (valid) {
-            const uint64_t q = __umul64hi(x, e.rcp) >> e.shift;
-            x = x + e.bias + q * e.cmpl;
+            const unsigned bal = __ballot_sync(0xffffffffu, flush);
+            const uint32_t ne = __popc(bal);
+            if (flush) {
+                refill_end[-(int64_t)tail - (int64_t)ne + __popc(bal & lt)] = (uint32_t)x;
+                x >>= 32;
+            }
+            tail += ne;
+            if (valid) {
+                const uint64_t q = __umul64hi(x, e.rcp) >> e.shift;
+                x = x + e.bias + q * e.cmpl;
+            }
         }
     }
-    const bool active = base + lane < d.n;
+    const bool active = base + lane < n;
     const unsigned abal = __ballot_sync(0xffffffffu, active);
     if (active) {
         const uint32_t p = 2u * __popc(abal & lt);
@@ -169,8 +185,10 @@ __global__ void __launch_bounds__(32 * DEC_WARPS)
                    const uint8_t* __restrict__ levels, uint16_t* __restrict__ codes,
                    uint32_t* __restrict__ err) {
     extern __shared__ uint32_t smem[];
+    __shared__ uint32_t ring_all[DEC_WARPS][RING];
     const RansStageDesc& d = st[find_block_stage(st, n_stages, blockIdx.x)];
     const uint32_t local = (blockIdx.x - d.block0) * DEC_WARPS + (threadIdx.x >> 5);
+    uint32_t* ring = ring_all[threadIdx.x >> 5];
     // smem_alpha: the largest alphabet the dynamic shared memory was sized for
     const bool smem_tables = !d.per_point && d.alphabet <= smem_alpha;
     const uint32_t alpha1 = d.alphabet + 1;
@@ -204,7 +222,16 @@ __global__ void __launch_bounds__(32 * DEC_WARPS)
         else atomicOr(err, 4u);
     }
     pos += 2u * __popc(abal);
+    // refill words are consumed in order: keep [pos, hi) in a per-warp ring,
+    // topped up RING/2 words at a time with coalesced loads
+    uint64_t hi = pos;
     for (uint32_t k = 0; k < K; k++) {
+        if (hi < pos + 32 && hi < end) {  // uniform across the warp
+            const uint64_t top = hi + RING / 2 < end ? hi + RING / 2 : end;
+            for (uint64_t w = hi + lane; w < top; w += 32) ring[w & (RING - 1)] = words[w];
+            hi = top;
+            __syncwarp();
+        }
         const uint64_t i = base + (uint64_t)k * 32u + lane;
         const bool valid = i < d.n;
         bool need = false;
@@ -221,10 +248,11 @@ __global__ void __launch_bounds__(32 * DEC_WARPS)
         const unsigned bal = __ballot_sync(0xffffffffu, need);
         if (need) {
             const uint64_t p = pos + __popc(bal & lt);
-            if (p < end) x = (x << 32) | words[p];
+            if (p < hi) x = (x << 32) | ring[p & (RING - 1)];
             else atomicOr(err, 4u);
         }
         pos += __popc(bal);
+        __syncwarp();
     }
     if ((active && x != LANE_L) || (lane == 0 && pos != end)) atomicOr(err, 8u);
 }

@@ -47,6 +47,7 @@ struct RansStageDesc {
 
 constexpr int DEC_WARPS = 16;            // warps (chunks) per decoder CTA
 constexpr int SMEM_ALPHA = 8192;         // largest alphabet decoded from shared memory
+constexpr int RING = 256;                // decoder word window per warp (power of two)
 
 int launch_build_tables(const uint32_t* cdf, int alphabet, int rows, EncSym* enc, uint16_t* bucket,
                         cudaStream_t st);
