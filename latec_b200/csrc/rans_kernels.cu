@@ -470,7 +470,8 @@ int launch_lanes_decode(const RansStageDesc* st, int n_stages, uint32_t total_bl
     if (!total_blocks) return LATEC_OK;
     const int a = max_alphabet <= SMEM_ALPHA ? max_alphabet : 0;
     const size_t smem = a ? (size_t)(a + 1) * 4 + NBUCKET * 2 : 0;
-    if (smem > 48 * 1024 &&
+    // the static word rings plus the dynamic tables may pass the 48 KB default
+    if (smem + sizeof(uint32_t) * DEC_WARPS * RING > 48 * 1024 &&
         cudaFuncSetAttribute(k_lanes_decode, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess)
         return LATEC_ERR_CUDA;
