@@ -79,9 +79,6 @@ __device__ __forceinline__ uint32_t widen(uint32_t sym, int radius, int kexp) {
 }
 
 // --------------------------------------------------------------- lanes
-// Encoder: one warp per chunk, steps k = K-1 .. 0. Codes are fetched 32 steps
-// at a time (32 independent coalesced loads per lane), so the per-step
-// dependency chain is only the state update and the renormalisation ballot.
 __global__ void __launch_bounds__(128)
     k_lanes_encode(const RansStageDesc* __restrict__ st, int n_stages, uint32_t total_chunks,
                    const uint16_t* __restrict__ codes, const uint8_t* __restrict__ levels,
@@ -99,51 +96,38 @@ __global__ void __launch_bounds__(128)
     uint32_t* refill_end = region + 64 + 32u * K;
     const uint16_t* c = codes + d.codes_off;
     const uint8_t* lv = d.per_point ? levels + d.codes_off : nullptr;
-    const uint64_t n = d.n;
     uint64_t x = LANE_L;
     uint32_t tail = 0;
     const unsigned lt = (1u << lane) - 1u;
-    for (int hb = (int)K; hb > 0; hb -= 32) {
-        const int lb = hb > 32 ? hb - 32 : 0;
-        uint32_t cb[32];
-        uint8_t rb[32];
-#pragma unroll
-        for (int j = 0; j < 32; j++) {
-            const uint64_t i = base + (uint64_t)(lb + j) * 32u + lane;
-            const bool ok = lb + j < hb && i < n;
-            cb[j] = ok ? (uint32_t)c[i] : 0xFFFFFFFFu;
-            rb[j] = (ok && lv) ? lv[i] : 0;
+    for (int k = (int)K - 1; k >= 0; k--) {
+        const uint64_t i = base + (uint64_t)k * 32u + lane;
+        const bool valid = i < d.n;
+        EncSym e;
+        bool flush = false;
+        if (valid) {
+            const uint32_t sym = narrow(c[i], d.radius, d.kexp);
+            const uint32_t row = lv ? lv[i] : 0u;
+            if (sym >= d.alphabet) {
+                atomicOr(err, 2u);
+                e = enc[row * alpha1];
+            } else {
+                e = enc[row * alpha1 + sym];
+            }
+            flush = x >= ((uint64_t)e.freq << 39);
         }
-#pragma unroll
-        for (int j = 31; j >= 0; j--) {
-            if (lb + j >= hb) continue;  // uniform across the warp
-            const bool valid = cb[j] != 0xFFFFFFFFu;
-            EncSym e;
-            bool flush = false;
-            if (valid) {
-                const uint32_t sym = narrow(cb[j], d.radius, d.kexp);
-                if (sym >= d.alphabet) {
-                    atomicOr(err, 2u);
-                    e = enc[rb[j] * alpha1];
-                } else {
-                    e = enc[rb[j] * alpha1 + sym];
-                }
-                flush = x >= ((uint64_t)e.freq << 39);
-            }
-            const unsigned bal = __ballot_sync(0xffffffffu, flush);
-            const uint32_t ne = __popc(bal);
-            if (flush) {
-                refill_end[-(int64_t)tail - (int64_t)ne + __popc(bal & lt)] = (uint32_t)x;
-                x >>= 32;
-            }
-            tail += ne;
-            if (valid) {
-                const uint64_t q = __umul64hi(x, e.rcp) >> e.shift;
-                x = x + e.bias + q * e.cmpl;
-            }
+        const unsigned bal = __ballot_sync(0xffffffffu, flush);
+        const uint32_t ne = __popc(bal);
+        if (flush) {
+            refill_end[-(int64_t)tail - (int64_t)ne + __popc(bal & lt)] = (uint32_t)x;
+            x >>= 32;
+        }
+        tail += ne;
+        if (valid) {
+            const uint64_t q = __umul64hi(x, e.rcp) >> e.shift;
+            x = x + e.bias + q * e.cmpl;
         }
     }
-    const bool active = base + lane < n;
+    const bool active = base + lane < d.n;
     const unsigned abal = __ballot_sync(0xffffffffu, active);
     if (active) {
         const uint32_t p = 2u * __popc(abal & lt);
