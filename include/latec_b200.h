@@ -223,6 +223,25 @@ int latec_parse_records(const uint8_t* payload, uint64_t n_bytes, int32_t n_stag
 int latec_chunk_ranges(const uint32_t* words, const void* records, int32_t n_stages,
                        uint64_t* ranges, uint32_t* err, void* stream);
 
+/* ---- flat quantizer without any device allocation (no counterpart in the
+ *      reference). For callers that cannot call cudaMalloc -- e.g. an
+ *      application whose GPU memory is owned by another allocator, or a
+ *      latency-critical loop where cudaMalloc/cudaFree would synchronise the
+ *      device. Same inputs, outputs and results as latec_quantize, but its
+ *      scratch is a file-scope device array (about 4 MiB, held by every GPU
+ *      that loads the library until exit) instead of a caller workspace.
+ *      items must not exceed LATEC_STATIC_MAX_ITEMS (else
+ *      LATEC_ERR_TOO_LARGE). All calls on a device share that array: calls
+ *      whose GPU work overlaps race and must not be issued. The first call on
+ *      each device looks the array up (cudaGetSymbolAddress); make it before
+ *      any stream capture. */
+#define LATEC_ERR_TOO_LARGE (-7)
+#define LATEC_STATIC_MAX_ITEMS (1u << 19)
+int latec_quantize_static(const latec_quant_params* prm, double eb, uint64_t items, const void* x,
+                          const void* pred, uint16_t* codes, void* recon_out, void* outliers,
+                          latec_stage_stats* stats, uint32_t* hist_seg, uint32_t* hist_total,
+                          void* stream);
+
 /* Library version string. */
 const char* latec_version(void);
 

@@ -20,6 +20,7 @@ ERRORS = {
     -4: (ValueError, "malformed stream"),
     -5: (RuntimeError, "workspace too small"),
     -6: (RuntimeError, "internal error"),
+    -7: (ValueError, "input larger than the entry point's fixed limit"),
 }
 F32, F64 = 1, 2
 RANS_LANES, RANS_COMPAT = 0, 1
@@ -82,6 +83,8 @@ SIGNATURES = {
     "latec_rans_decode": (ctypes.c_int, [P, I32, U32, P, P, P, P, P, P, U64, P]),
     "latec_fit_stage_size": (U64, []),
     "latec_fit_const": (ctypes.c_int, [P, I32, P, P, P, P, P, P, U64, P]),
+    "latec_quantize_static": (ctypes.c_int, [ctypes.POINTER(QuantParams), D, U64, P, P, P, P, P,
+                                             P, P, P, P]),
     "latec_raw_frame_bytes": (U64, [U64]),
     "latec_frame_raw": (ctypes.c_int, [P, U64, P, ctypes.c_uint32, P, U64, P]),
     "latec_unframe_raw": (ctypes.c_int, [P, U64, P, P, P]),
