@@ -120,6 +120,140 @@ __device__ __forceinline__ double predict_point(const StageDesc& d, const QParam
     return axis_interp(rc, flat, ca, na, gs, d.s, CUBIC, q.end_mode);
 }
 
+// ---- gather / combine form of predict_point, used by the stage kernels ----
+// All taps a point needs are loaded first, without branches (a tap outside
+// the line reads the -s tap, which always exists, and is then ignored), so a
+// thread has every load of its points in flight before any arithmetic; the
+// combine step is axis_interp's arithmetic, operation for operation.
+template <typename T>
+struct AxisTaps {
+    T m1, p1, m3, p3;
+    uint32_t ok;  // bit 0: +s valid, bit 1: -3s valid, bit 2: +3s valid
+};
+
+template <typename T, int CUBIC>
+__device__ __forceinline__ void load_axis(const T* __restrict__ rc, int64_t flat, int c, int n,
+                                          int64_t gs, int s, AxisTaps<T>& t) {
+    const int64_t o1 = (int64_t)s * gs;
+    const bool vp1 = c + s < n, vm3 = c - 3 * s >= 0, vp3 = c + 3 * s < n;
+    const T* b = rc + flat;
+    t.m1 = __ldg(b - o1);
+    t.p1 = __ldg(b + (vp1 ? o1 : -o1));
+    t.m3 = __ldg(b + (vm3 ? -3 * o1 : -o1));
+    t.p3 = CUBIC ? __ldg(b + (vp3 ? 3 * o1 : -o1)) : (T)0;
+    t.ok = (vp1 ? 1u : 0u) | (vm3 ? 2u : 0u) | (vp3 ? 4u : 0u);
+}
+
+template <typename T, int CUBIC>
+__device__ __forceinline__ double axis_combine(const AxisTaps<T>& t, int em) {
+    const double Lm1 = (double)t.m1;
+    const bool vp1 = t.ok & 1u, vm3 = t.ok & 2u, vp3 = t.ok & 4u;
+    if (vp1) {
+        const double Lp1 = (double)t.p1;
+        const double lin = 0.5 * __dadd_rn(Lm1, Lp1);
+        if (!CUBIC) return lin;
+        if (vm3 && vp3) {
+            const double Lm3 = (double)t.m3, Lp3 = (double)t.p3;
+            double u = __dadd_rn(-Lm3, __dmul_rn(9.0, Lm1));
+            u = __dadd_rn(u, __dmul_rn(9.0, Lp1));
+            u = __dsub_rn(u, Lp3);
+            return u * 0.0625;
+        }
+        if (em & 1) {
+            if (vp3) {
+                const double Lp3 = (double)t.p3;
+                double u = __dadd_rn(__dmul_rn(3.0, Lm1), __dmul_rn(6.0, Lp1));
+                u = __dsub_rn(u, Lp3);
+                return u * 0.125;
+            }
+            if (vm3) {
+                const double Lm3 = (double)t.m3;
+                double u = __dadd_rn(-Lm3, __dmul_rn(6.0, Lm1));
+                u = __dadd_rn(u, __dmul_rn(3.0, Lp1));
+                return u * 0.125;
+            }
+        }
+        return lin;
+    }
+    if ((em & 2) && vm3) return __dsub_rn(__dmul_rn(1.5, Lm1), __dmul_rn(0.5, (double)t.m3));
+    return Lm1;
+}
+
+// Taps of one point: one axis for KIND 0 and for centers 1/2, every odd axis
+// for KIND 1 with center 0 (in axis order).
+template <typename T, int ND, int KIND>
+struct PointTaps {
+    static constexpr int NA = KIND ? (ND > 0 ? ND : MAXD) : 1;
+    AxisTaps<T> ax[NA];
+    uint32_t odd;  // center 0, KIND 1: mask of the odd axes
+};
+
+template <typename T, int ND, int KIND, int CUBIC>
+__device__ __forceinline__ void gather_point(const StageDesc& d, const QParams& q,
+                                             const T* __restrict__ rc, int64_t flat,
+                                             const int32_t* coord, PointTaps<T, ND, KIND>& pt) {
+    constexpr int NDV = ND > 0 ? ND : MAXD;
+    pt.odd = 0;
+    if (KIND == 0) {
+        int ca = 0, na = 1;
+        int64_t gs = 0;
+#pragma unroll
+        for (int j = 0; j < NDV; j++) {
+            if (j == d.axis) {
+                ca = coord[j];
+                na = d.shape[j];
+                gs = d.gstride[j];
+            }
+        }
+        load_axis<T, CUBIC>(rc, flat, ca, na, gs, d.s, pt.ax[0]);
+        return;
+    }
+    if (q.center == 0) {
+#pragma unroll
+        for (int j = 0; j < NDV; j++) {
+            if ((ND > 0 || j < d.ndim) && (coord[j] & d.s)) {
+                pt.odd |= 1u << j;
+                load_axis<T, CUBIC>(rc, flat, coord[j], d.shape[j], d.gstride[j], d.s,
+                                    pt.ax[KIND ? j : 0]);
+            }
+        }
+        return;
+    }
+    int ca = 0, na = 1;
+    int64_t gs = 0;
+    bool found = false;
+#pragma unroll
+    for (int j = 0; j < NDV; j++) {
+        if ((ND > 0 || j < d.ndim) && (coord[j] & d.s) && (q.center == 2 || !found)) {
+            ca = coord[j];
+            na = d.shape[j];
+            gs = d.gstride[j];
+            found = true;
+        }
+    }
+    load_axis<T, CUBIC>(rc, flat, ca, na, gs, d.s, pt.ax[0]);
+}
+
+template <typename T, int ND, int KIND, int CUBIC>
+__device__ __forceinline__ double combine_point(const QParams& q, const PointTaps<T, ND, KIND>& pt) {
+    constexpr int NDV = ND > 0 ? ND : MAXD;
+    if (KIND == 0 || q.center != 0) return axis_combine<T, CUBIC>(pt.ax[0], q.end_mode);
+    double total = 0.0;
+    int cnt = 0;
+#pragma unroll
+    for (int j = 0; j < NDV; j++) {
+        if (pt.odd & (1u << j)) {
+            const double v = axis_combine<T, CUBIC>(pt.ax[KIND ? j : 0], q.end_mode);
+            total = cnt ? __dadd_rn(total, v) : v;
+            cnt++;
+        }
+    }
+    if (cnt == 1) return total;
+    if (cnt == 2) return total * 0.5;
+    if (cnt == 4) return total * 0.25;
+    return __ddiv_rn(total, (double)cnt);
+}
+
 // rint((x - p) / w) with the division's exact rounding: the reciprocal
 // product is used unless it lies within a few ulps of a half-integer.
 __device__ __forceinline__ double quotient_rint(double diff, const QParams& q) {
@@ -338,6 +472,24 @@ __device__ __forceinline__ double locate_predict(const StageDesc& d, const QPara
                                                          coord);
 }
 
+// Locate one stage point and load its taps (prediction deferred to combine).
+template <typename T, int ND, int KIND, int CUBIC>
+__device__ __forceinline__ void locate_gather(const StageDesc& d, const QParams& q,
+                                              const int is_anchor, uint64_t i,
+                                              const T* __restrict__ recon, int64_t& flat,
+                                              uint32_t& c, PointTaps<T, ND, KIND>& pt) {
+    c = 0;
+    uint32_t rank = (uint32_t)i;
+    if (q.channels > 1) {
+        c = (uint32_t)(i / d.n);
+        rank = (uint32_t)(i - (uint64_t)c * d.n);
+    }
+    int32_t coord[ND > 0 ? ND : MAXD];
+    flat = stage_coords_t<ND, KIND>(d, rank, coord);
+    if (!is_anchor)
+        gather_point<T, ND, KIND, CUBIC>(d, q, recon + (uint64_t)c * q.points, flat, coord, pt);
+}
+
 template <typename T>
 __device__ __forceinline__ void encode_value(const QParams& q, uint64_t i, T xv, double pd,
                                              T* __restrict__ dst, T* __restrict__ staging,
@@ -386,7 +538,7 @@ __device__ __forceinline__ void flush_hist(uint32_t* sh_hist, uint32_t* hist_seg
 }
 
 template <typename T, int ND, int KIND, int CUBIC>
-__global__ void __launch_bounds__(THREADS, 4)
+__global__ void __launch_bounds__(THREADS, KIND ? 3 : 4)
     k_interp_quant(const StageDesc d, const QParams q, const int is_anchor, const uint32_t gpb,
                    const T* __restrict__ x, T* __restrict__ recon, uint16_t* __restrict__ codes,
                    T* __restrict__ staging, uint32_t* __restrict__ tile_cnt,
@@ -416,16 +568,18 @@ __global__ void __launch_bounds__(THREADS, 4)
         const bool v0 = i0 < items, v1 = i1 < items;
         int64_t f0 = 0, f1 = 0;
         uint32_t c0 = 0, c1 = 0;
-        double p0 = 0.0, p1 = 0.0;
         T x0 = (T)0, x1 = (T)0;
+        PointTaps<T, ND, KIND> t0, t1;
         if (v0) {
-            p0 = locate_predict<T, ND, KIND, CUBIC>(d, q, is_anchor, i0, recon, f0, c0);
+            locate_gather<T, ND, KIND, CUBIC>(d, q, is_anchor, i0, recon, f0, c0, t0);
             x0 = x[(uint64_t)c0 * q.points + f0];
         }
         if (v1) {
-            p1 = locate_predict<T, ND, KIND, CUBIC>(d, q, is_anchor, i1, recon, f1, c1);
+            locate_gather<T, ND, KIND, CUBIC>(d, q, is_anchor, i1, recon, f1, c1, t1);
             x1 = x[(uint64_t)c1 * q.points + f1];
         }
+        const double p0 = (v0 && !is_anchor) ? combine_point<T, ND, KIND, CUBIC>(q, t0) : 0.0;
+        const double p1 = (v1 && !is_anchor) ? combine_point<T, ND, KIND, CUBIC>(q, t1) : 0.0;
         int k0 = -1, k1 = -1;
         uint32_t cd0 = 0, cd1 = 0;
         if (v0)
@@ -667,7 +821,7 @@ __device__ __forceinline__ void dequant_point(const StageDesc& d, const QParams&
 // Tiles without outliers (the common case) take a barrier-free path; others
 // rank their outliers with a block scan in item order.
 template <typename T, int ND, int KIND, int CUBIC>
-__global__ void __launch_bounds__(THREADS, 5)
+__global__ void __launch_bounds__(THREADS, KIND ? 4 : 5)
     k_interp_dequant(const StageDesc d, const QParams q, const int is_anchor,
                      const uint16_t* __restrict__ codes, const uint8_t* __restrict__ outliers,
                      const uint32_t* __restrict__ tile_cnt, const uint32_t* __restrict__ tile_off,
@@ -680,16 +834,20 @@ __global__ void __launch_bounds__(THREADS, 5)
             const uint64_t i1 = i0 + THREADS;
             int64_t f0 = 0, f1 = 0;
             uint32_t c0 = 0, c1 = 0;
-            double p0 = 0.0, p1 = 0.0;
             uint32_t q0 = 1, q1 = 1;
+            PointTaps<T, ND, KIND> t0, t1;
             if (i0 < items) {
                 q0 = codes[i0];
-                p0 = locate_predict<T, ND, KIND, CUBIC>(d, q, is_anchor, i0, recon, f0, c0);
+                locate_gather<T, ND, KIND, CUBIC>(d, q, is_anchor, i0, recon, f0, c0, t0);
             }
             if (i1 < items) {
                 q1 = codes[i1];
-                p1 = locate_predict<T, ND, KIND, CUBIC>(d, q, is_anchor, i1, recon, f1, c1);
+                locate_gather<T, ND, KIND, CUBIC>(d, q, is_anchor, i1, recon, f1, c1, t1);
             }
+            const double p0 =
+                (i0 < items && !is_anchor) ? combine_point<T, ND, KIND, CUBIC>(q, t0) : 0.0;
+            const double p1 =
+                (i1 < items && !is_anchor) ? combine_point<T, ND, KIND, CUBIC>(q, t1) : 0.0;
             if (i0 < items) recon[(uint64_t)c0 * q.points + f0] = dequant_value<T>(q, p0, q0);
             if (i1 < items) recon[(uint64_t)c1 * q.points + f1] = dequant_value<T>(q, p1, q1);
         }
