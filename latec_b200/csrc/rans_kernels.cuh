@@ -45,7 +45,7 @@ struct RansStageDesc {
     uint32_t block0;      // decode: first CTA of the stage (filled by the library)
 };
 
-constexpr int DEC_WARPS = 16;            // warps (chunks) per decoder CTA
+constexpr int DEC_WARPS = 4;             // warps (chunks) per decoder CTA
 constexpr int SMEM_ALPHA = 8192;         // largest alphabet decoded from shared memory
 constexpr int RING = 256;                // decoder word window per warp (power of two)
 
