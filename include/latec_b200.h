@@ -223,6 +223,35 @@ int latec_parse_records(const uint8_t* payload, uint64_t n_bytes, int32_t n_stag
 int latec_chunk_ranges(const uint32_t* words, const void* records, int32_t n_stages,
                        uint64_t* ranges, uint32_t* err, void* stream);
 
+/* ---- per-point rANS support (the learned path's entropy stage).
+ *      latec_scale_levels: latec/rans.py:270-278 scale_to_level -- level of
+ *      each float32 scale = number of the n_levels - 1 ascending float32
+ *      thresholds (host array) not above it; NaN gives level 0.
+ *      latec_level_order: the symbol order of latec/rans.py:546-578 (level 0
+ *      first, each level in index order) as a permutation order[j] = index of
+ *      the j-th coded symbol (stable counting sort; n < 2^32).
+ *      latec_permute: dst[j] = src[order[j]] (inverse = 0) or
+ *      dst[order[j]] = src[j] (inverse = 1), elem 1, 2 or 4 bytes.
+ *      latec_point_bits: latec/rans.py:332-357 model_bits, n_partial float64
+ *      partial sums (one per CTA, summed by the caller); err bit 1 = a code
+ *      outside the window.
+ *      latec_shape_costs: latec/rans.py:204-243 choose_shape costs over every
+ *      step-th symbol, n_partial partials per shape (shape-major). */
+int latec_scale_levels(const float* scale, uint64_t n, const float* thresholds, int32_t n_levels,
+                       uint8_t* levels, void* stream);
+uint64_t latec_level_order_workspace_bytes(uint64_t n);
+int latec_level_order(const uint8_t* levels, uint64_t n, uint32_t* order, void* workspace,
+                      uint64_t workspace_bytes, void* stream);
+int latec_permute(const void* src, int32_t elem, const uint32_t* order, uint64_t n, void* dst,
+                  int32_t inverse, void* stream);
+int latec_point_bits(const uint16_t* codes, const uint8_t* levels, uint64_t n, const uint32_t* cdf,
+                     uint32_t alphabet, int32_t radius, int32_t kexp, double* partial,
+                     int32_t n_partial, uint32_t* err, void* stream);
+int latec_shape_costs(const uint16_t* codes, const uint8_t* levels, uint64_t n, uint64_t step,
+                      const double* weights, uint32_t alphabet, int32_t n_levels, int32_t radius,
+                      int32_t kexp, double floor_p, const int32_t* shape_d, const double* shape_w,
+                      int32_t n_shapes, double* partial, int32_t n_partial, void* stream);
+
 /* ---- flat quantizer without any device allocation (no counterpart in the
  *      reference). For callers that cannot call cudaMalloc -- e.g. an
  *      application whose GPU memory is owned by another allocator, or a

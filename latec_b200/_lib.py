@@ -85,6 +85,13 @@ SIGNATURES = {
     "latec_fit_const": (ctypes.c_int, [P, I32, P, P, P, P, P, P, U64, P]),
     "latec_quantize_static": (ctypes.c_int, [ctypes.POINTER(QuantParams), D, U64, P, P, P, P, P,
                                              P, P, P, P]),
+    "latec_scale_levels": (ctypes.c_int, [P, U64, P, I32, P, P]),
+    "latec_level_order_workspace_bytes": (U64, [U64]),
+    "latec_level_order": (ctypes.c_int, [P, U64, P, P, U64, P]),
+    "latec_permute": (ctypes.c_int, [P, I32, P, U64, P, I32, P]),
+    "latec_point_bits": (ctypes.c_int, [P, P, U64, P, U32, I32, I32, P, I32, P, P]),
+    "latec_shape_costs": (ctypes.c_int, [P, P, U64, U64, P, U32, I32, I32, I32, D, P, P, I32, P,
+                                         I32, P]),
     "latec_raw_frame_bytes": (U64, [U64]),
     "latec_frame_raw": (ctypes.c_int, [P, U64, P, ctypes.c_uint32, P, U64, P]),
     "latec_unframe_raw": (ctypes.c_int, [P, U64, P, P, P]),

@@ -3,7 +3,8 @@
 This package restates, on the CPU, the algorithm of the reference LATEC code for
 the path the CUDA library implements: the dyadic stage schedule, the
 cubic/linear interpolation predictor, the error-bounded quantizer, the
-Laplace-mixture rANS model tables and the LATEC001 container. Each function
+Laplace-mixture rANS model tables, the per-point rANS coder (``point.py``)
+and the LATEC001 container. Each function
 cites the reference file and line it follows (paths relative to the reference
 project root).
 

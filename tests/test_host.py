@@ -186,3 +186,17 @@ def test_raw_zstd_frame_is_a_valid_zstd_frame(n):
     assert frame.tobytes() == ocodec.raw_zstd_frame(payload.tobytes())
     z = bs.zstd().compress(payload.tobytes(), 3)
     assert bs.read_body(np.frombuffer(z, np.uint8)).tobytes() == payload.tobytes()
+
+
+def test_level_thresholds_bracket_the_reference_levels():
+    """The float32 level boundaries the device compares against reproduce
+    latec/rans.py:270-278 exactly on both sides of every boundary."""
+    from latec_b200.rans import level_thresholds
+    from oracle import rans_model as orm
+
+    for eb in (1e-6, 1e-3, 0.25, 3.0):
+        th = level_thresholds(eb)
+        assert th.dtype == np.float32 and np.all(np.diff(th) > 0)
+        assert np.array_equal(orm.scale_to_level(th, eb), np.arange(1, 64))
+        below = np.nextafter(th, np.float32(-np.inf))
+        assert np.array_equal(orm.scale_to_level(below, eb), np.arange(0, 63))
