@@ -252,6 +252,55 @@ int latec_shape_costs(const uint16_t* codes, const uint8_t* levels, uint64_t n, 
                       int32_t kexp, double floor_p, const int32_t* shape_d, const double* shape_w,
                       int32_t n_shapes, double* partial, int32_t n_partial, void* stream);
 
+/* ---- the axial GNN predictor of the learned path (latec/gnn_predictor.py).
+ *      Parameters: one packed float32 device buffer of
+ *      latec_gnn_param_count(d, agg_level) floats, the reference state_dict
+ *      tensors (build_model, :593-933) concatenated in this order: init.net.0,
+ *      init.net.2, dir_state.table, dir.net.0, dir.net.2, bidir.net.0,
+ *      bidir.net.2, line_pool {wk.0, wk.2, wv, null_k, null_v}, axis_pool
+ *      {same}, head.net.0, head.net.2, mix.net.0, mix.net.2 (weight before
+ *      bias). E: the (B, N, K, d) float32 embedding field; contexts
+ *      (B, M, K, d). Geometry: one stage's queries and, per line, the nearest
+ *      known neighbour on each side (:245-443 _StageGeom), with the live pairs
+ *      listed per query tile (two-sided first, then one-sided).
+ *      float32 arithmetic in a fixed order: identical on every run. */
+typedef struct {
+    int32_t d, agg_level;
+    const float* params;
+} latec_gnn_model;
+
+typedef struct {
+    int32_t M, L, K, m_tile, n_tiles;
+    const int32_t* query;   /* device (M) flat indices */
+    const int32_t* nbr_p;   /* device (L, M), -1 = no neighbour */
+    const int32_t* nbr_n;
+    const float* logd_p;    /* device (L, M) log2 distance + line term */
+    const float* logd_n;
+    const int32_t* two;     /* device: two-sided pair ids l * M + m, per tile */
+    const int32_t* one;     /* device: one-sided pair ids, per tile */
+    const int32_t* row_of;  /* device (L, M): tile-local live row, -1 = dead */
+    const int64_t* two_off; /* host (n_tiles + 1) */
+    const int64_t* one_off; /* host (n_tiles + 1) */
+    const int32_t* sidx_p;  /* device (L, K) direction-state rows */
+    const int32_t* sidx_n;
+} latec_gnn_geom;
+
+uint64_t latec_gnn_param_count(int32_t d, int32_t agg_level);
+uint64_t latec_gnn_workspace_bytes(int32_t d, int32_t B, int32_t M, int32_t L, int32_t K,
+                                   int32_t m_tile);
+/* GNN.embed (:843-871): per-axis contexts of the stage's queries. */
+int latec_gnn_embed(const latec_gnn_model* model, int32_t B, int64_t N, const float* E,
+                    const latec_gnn_geom* geom, float* ctx, void* workspace,
+                    uint64_t workspace_bytes, void* stream);
+/* GNN.head_of + PredHead (:760-790, 922-931): mu, log2 b per query. */
+int latec_gnn_head(const latec_gnn_model* model, int32_t B, int32_t M, int32_t K, const float* ctx,
+                   float eb, float* mu, float* log_b, void* workspace, uint64_t workspace_bytes,
+                   void* stream);
+/* GNN.finalize (:901-920): E[b, query[m], k] = Mix(ctx, Init(vals[b, m])). */
+int latec_gnn_finalize(const latec_gnn_model* model, int32_t B, int64_t N, int32_t M, int32_t K,
+                       const int32_t* query, const float* ctx, const float* vals, float* E,
+                       void* workspace, uint64_t workspace_bytes, void* stream);
+
 /* ---- flat quantizer without any device allocation (no counterpart in the
  *      reference). For callers that cannot call cudaMalloc -- e.g. an
  *      application whose GPU memory is owned by another allocator, or a

@@ -57,6 +57,17 @@ class FitStage(ctypes.Structure):
                 ("stage", U32), ("shape_ids", U32 * 24)]
 
 
+class GnnModel(ctypes.Structure):
+    _fields_ = [("d", I32), ("agg_level", I32), ("params", P)]
+
+
+class GnnGeom(ctypes.Structure):
+    _fields_ = [("M", I32), ("L", I32), ("K", I32), ("m_tile", I32), ("n_tiles", I32),
+                ("query", P), ("nbr_p", P), ("nbr_n", P), ("logd_p", P), ("logd_n", P),
+                ("two", P), ("one", P), ("row_of", P), ("two_off", P), ("one_off", P),
+                ("sidx_p", P), ("sidx_n", P)]
+
+
 # Every symbol the header declares, with (restype, argtypes).
 SIGNATURES = {
     "latec_version": (ctypes.c_char_p, []),
@@ -92,6 +103,14 @@ SIGNATURES = {
     "latec_point_bits": (ctypes.c_int, [P, P, U64, P, U32, I32, I32, P, I32, P, P]),
     "latec_shape_costs": (ctypes.c_int, [P, P, U64, U64, P, U32, I32, I32, I32, D, P, P, I32, P,
                                          I32, P]),
+    "latec_gnn_param_count": (U64, [I32, I32]),
+    "latec_gnn_workspace_bytes": (U64, [I32, I32, I32, I32, I32, I32]),
+    "latec_gnn_embed": (ctypes.c_int, [ctypes.POINTER(GnnModel), I32, ctypes.c_int64, P,
+                                       ctypes.POINTER(GnnGeom), P, P, U64, P]),
+    "latec_gnn_head": (ctypes.c_int, [ctypes.POINTER(GnnModel), I32, I32, I32, P,
+                                      ctypes.c_float, P, P, P, U64, P]),
+    "latec_gnn_finalize": (ctypes.c_int, [ctypes.POINTER(GnnModel), I32, ctypes.c_int64, I32,
+                                          I32, P, P, P, P, P, U64, P]),
     "latec_raw_frame_bytes": (U64, [U64]),
     "latec_frame_raw": (ctypes.c_int, [P, U64, P, ctypes.c_uint32, P, U64, P]),
     "latec_unframe_raw": (ctypes.c_int, [P, U64, P, P, P]),
