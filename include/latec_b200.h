@@ -139,6 +139,16 @@ int latec_quantize(const latec_quant_params* prm, double eb, uint64_t items, con
                    latec_stage_stats* stats, uint32_t* hist_seg, uint32_t* hist_total,
                    void* workspace, uint64_t workspace_bytes, void* stream);
 
+/* ---- predictor-agnostic dequantize (latec/quantizer.py:82-120, and the
+ *      learned codec's device twin latec/gnn_codec.py:1038-1044): recon_out[i]
+ *      = the next outlier (scan order) where codes[i] == 0, else the
+ *      quantizer's reconstruction of pred[i]; bit-identical to the recon_out
+ *      of latec_quantize. err bit 1: the zero codes do not match n_out. */
+uint64_t latec_dequantize_workspace_bytes(uint64_t items);
+int latec_dequantize(const latec_quant_params* prm, double eb, uint64_t items, const void* pred,
+                     const uint16_t* codes, const void* outliers, uint32_t n_out, void* recon_out,
+                     uint32_t* err, void* workspace, uint64_t workspace_bytes, void* stream);
+
 /* ---- decode: predict + dequantize over every stage
  *      (latec/codec.py:462-510 _decompress_region). codes as produced by
  *      latec_rans_decode; outliers: device byte array holding every stage's

@@ -7,7 +7,8 @@ CPU fallback.
 """
 
 from .codec import compress, decompress
+from .gnn_codec import GNNCodec, GNNCompressorCodec
 from .predictor import InterpPredictor
 
-__all__ = ["compress", "decompress", "InterpPredictor"]
+__all__ = ["compress", "decompress", "InterpPredictor", "GNNCodec", "GNNCompressorCodec"]
 __version__ = "0.1.0"

@@ -251,6 +251,43 @@ int latec_quantize(const latec_quant_params* prm, double eb, uint64_t items, con
     return rc;
 }
 
+uint64_t latec_dequantize_workspace_bytes(uint64_t items) {
+    Carve c{nullptr};  // the layout latec_dequantize carves
+    c.take<DecStage>(1);
+    c.take<uint32_t>((uint64_t)n_tiles(items) + 1);
+    c.take<uint32_t>((uint64_t)n_tiles(items) + 1);
+    return c.off;
+}
+
+int latec_dequantize(const latec_quant_params* prm, double eb, uint64_t items, const void* pred,
+                     const uint16_t* codes, const void* outliers, uint32_t n_out, void* recon_out,
+                     uint32_t* err, void* workspace, uint64_t workspace_bytes, void* stream) {
+    if (!valid_params(prm) || !err || (items && (!pred || !codes || !recon_out)) ||
+        (n_out && !outliers))
+        return LATEC_ERR_ARG;
+    if (!items) return LATEC_OK;
+    if (!workspace || workspace_bytes < latec_dequantize_workspace_bytes(items))
+        return LATEC_ERR_WORKSPACE;
+    QParams q;
+    if (!make_q(prm, eb, items, q)) return LATEC_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    Carve c{(uint8_t*)workspace};
+    DecStage* ds = c.take<DecStage>(1);
+    const uint32_t tiles = n_tiles(items);
+    uint32_t* tile_cnt = c.take<uint32_t>(tiles + 1);
+    uint32_t* tile_off = c.take<uint32_t>(tiles + 1);
+    DecStage h{0, items, 0, n_out};
+    if (cudaMemcpyAsync(ds, &h, sizeof(h), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemsetAsync(tile_cnt, 0, sizeof(uint32_t) * tiles, st) != cudaSuccess)
+        return LATEC_ERR_CUDA;
+    int rc = launch_count_zeros_all(ds, 1, tiles, codes, tile_cnt, st);
+    if (!rc) rc = launch_tile_offsets_all(ds, 1, tile_cnt, tile_off, err, st);
+    if (!rc)
+        rc = launch_dequant_flat(q, prm->dtype, items, pred, codes, outliers, tile_cnt, tile_off,
+                                 n_out, recon_out, err, st);
+    return rc;
+}
+
 int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
                         const double* stage_eb, const uint16_t* codes, const void* outliers,
                         const uint64_t* out_off, const uint32_t* n_out, void* recon,

@@ -867,6 +867,42 @@ __global__ void __launch_bounds__(THREADS, KIND ? 4 : 5)
     }
 }
 
+// Predictor-agnostic decode of a compact array (the decode twin of
+// k_quantize_flat): recon = outlier (scan order) where code == 0, else the
+// quantizer's reconstruction of pred. One CTA per 2048-code tile.
+template <typename T>
+__global__ void __launch_bounds__(THREADS)
+    k_dequant_flat(const QParams q, const uint64_t items, const T* __restrict__ pred,
+                   const uint16_t* __restrict__ codes, const uint8_t* __restrict__ outliers,
+                   const uint32_t* __restrict__ tile_cnt, const uint32_t* __restrict__ tile_off,
+                   const uint32_t n_out, T* __restrict__ recon, uint32_t* __restrict__ err) {
+    const uint64_t tile_base = (uint64_t)blockIdx.x * TILE;
+    const bool any = tile_cnt[blockIdx.x] != 0;  // uniform across the CTA
+    uint32_t run = any ? tile_off[blockIdx.x] : 0u;
+    for (int k = 0; k < TILE / THREADS; k++) {
+        const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
+        const bool valid = i < items;
+        const uint32_t code = valid ? codes[i] : 1u;
+        uint32_t pos = 0;
+        if (any) {
+            uint32_t tot;
+            pos = run + block_excl_flag(code == 0, tot);
+            run += tot;
+        }
+        if (!valid) continue;
+        if (code == 0) {
+            if (pos < n_out) {
+                recon[i] = load_unaligned<T>(outliers + (uint64_t)pos * sizeof(T));
+            } else {
+                recon[i] = (T)0;
+                atomicOr(err, 1u);
+            }
+        } else {
+            recon[i] = dequant_value<T>(q, (double)pred[i], code);
+        }
+    }
+}
+
 // ---------------------------------------------------------------- launchers
 static int last_err() {
     count_launches(1);
@@ -980,6 +1016,22 @@ int launch_tile_offsets_all(const DecStage* ds, int n_stages, const uint32_t* ti
                             uint32_t* tile_off, uint32_t* err, cudaStream_t st) {
     if (!n_stages) return LATEC_OK;
     k_tile_offsets_all<<<n_stages, THREADS, 0, st>>>(ds, tile_cnt, tile_off, err);
+    return last_err();
+}
+
+int launch_dequant_flat(const QParams& q, int dtype, uint64_t items, const void* pred,
+                        const uint16_t* codes, const void* outliers, const uint32_t* tile_cnt,
+                        const uint32_t* tile_off, uint32_t n_out, void* recon, uint32_t* err,
+                        cudaStream_t st) {
+    if (!items) return LATEC_OK;
+    if (dtype == LATEC_F64)
+        k_dequant_flat<double><<<n_tiles(items), THREADS, 0, st>>>(
+            q, items, (const double*)pred, codes, (const uint8_t*)outliers, tile_cnt, tile_off,
+            n_out, (double*)recon, err);
+    else
+        k_dequant_flat<float><<<n_tiles(items), THREADS, 0, st>>>(
+            q, items, (const float*)pred, codes, (const uint8_t*)outliers, tile_cnt, tile_off,
+            n_out, (float*)recon, err);
     return last_err();
 }
 

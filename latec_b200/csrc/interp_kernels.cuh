@@ -73,6 +73,10 @@ int launch_interp_dequant(const StageDesc& d, const QParams& q, int dtype, int i
                           const uint16_t* codes, const void* outliers, const uint32_t* tile_cnt,
                           const uint32_t* tile_off, uint32_t n_out, void* recon, uint32_t* err,
                           cudaStream_t st);
+int launch_dequant_flat(const QParams& q, int dtype, uint64_t items, const void* pred,
+                        const uint16_t* codes, const void* outliers, const uint32_t* tile_cnt,
+                        const uint32_t* tile_off, uint32_t n_out, void* recon, uint32_t* err,
+                        cudaStream_t st);
 int launch_quantize_flat(const QParams& q, int dtype, uint64_t items, const void* x,
                          const void* pred, uint16_t* codes, void* staging, uint32_t* tile_cnt,
                          uint32_t* tile_off, uint32_t* hist_total, uint32_t* hist_seg,

@@ -1,0 +1,377 @@
+"""``GNNCodec``: the learned LATEC codec on the device (``latec/gnn_codec.py``).
+
+Same API as the reference codec: ``GNNCodec(checkpoint_path, device=None, *,
+strict_checkpoint=True)``, ``compress(x, error_bound, ...) -> bytes`` and
+``uncompress(stream) -> torch.Tensor`` (alias ``decompress``), and the same
+stream container: ``<8sII`` prefix (magic ``LATECGNN``, version, header
+length), a JSON metadata header, then a zstd frame of the stage payload
+(``latec/gnn_codec.py:229-246``).
+
+The tensor is min-max normalised to [0, 1] in float32 and ``error_bound`` is
+applied to the normalised values, so it is relative to the data range, as in
+the reference (``:1509-1522``). Each stage of the dyadic schedule is coded as
+follows.
+
+1. The GNN predicts (mu, log2 b) at the stage's points (``gnn.stage_forward``,
+   CUDA kernels).
+2. The device quantizer codes x against mu, with the reference's exact
+   rounding and bound check.
+3. log2 b becomes per-point scale levels (``rans.scale_to_level``).
+4. The codes are entropy-coded by the native per-point lane coder with the
+   dictionary shape of least cost (``rans.choose_shape``).
+5. The reconstruction finalises the stage's embeddings before the next stage.
+
+The decoder repeats the same float path and dequantizes on the device.
+
+Scope of this version:
+
+* The whole tensor is one region: no chunk grid and no halos.
+* There is no interpolation gate: every stage uses the GNN.
+* Float inputs only.
+* The network runs in float32. The ``fp16`` and ``compile`` flags are accepted
+  and recorded as float32 / not compiled.
+
+Streams carry ``"float_path": "latec_b200-f32-1"``. As the reference's own
+encoder/decoder contract requires, they decode only with this float path.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import json
+import struct
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib, bitstream, gnn, rans
+from .levels import stage_ebs
+
+MAGIC = b"LATECGNN"
+VERSION = 14
+PREFIX = "<8sII"
+PREFIX_SIZE = struct.calcsize(PREFIX)
+FLOAT_PATH = "latec_b200-f32-1"
+AUTO_CHUNK_THRESHOLD = 1 << 21
+RANK_LEVELS = {2: 8, 4: 5, 5: 4}
+EB_COARSE_FACTOR = 0.9
+EB_COARSE_SWEEP = (1.0, 0.9, 0.65, 0.41)
+INTERP_KINDS = {"interp-cubic": 1, "interp-linear-first": 2, "interp-linear-last": 3}
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def auto_levels(shape, agg_level=2):
+    """``latec/gnn_codec.py:69-95``: schedule depth from the input rank,
+    capped so the anchor stride stays <= half the largest axis."""
+    ndim = len(shape)
+    if ndim == 3:
+        rank_levels = 7 if agg_level == 1 else 6
+    elif ndim in RANK_LEVELS:
+        rank_levels = RANK_LEVELS[ndim]
+    else:
+        rank_levels = (AUTO_CHUNK_THRESHOLD.bit_length() - 1) // ndim
+    size_cap = max(1, (int(max(shape)).bit_length() - 1) - 1)
+    return max(1, min(rank_levels, size_cap))
+
+
+def per_step_eb_ratio(coarse_factor, levels):
+    """``latec/gnn_codec.py:111-122``."""
+    if levels <= 1:
+        return 1.0
+    return float(coarse_factor) ** (1.0 / (levels - 1))
+
+
+def write_stream(meta, payload: bytes, zstd_level: int) -> bytes:
+    header = json.dumps(meta, sort_keys=True, separators=(",", ":")).encode("utf-8")
+    body = bitstream.zstd().compress(np.frombuffer(payload, np.uint8), int(zstd_level))
+    return struct.pack(PREFIX, MAGIC, VERSION, len(header)) + header + body
+
+
+def read_stream(stream: bytes):
+    if len(stream) < PREFIX_SIZE:
+        raise ValueError("not a LATEC GNN stream")
+    magic, version, hlen = struct.unpack_from(PREFIX, stream, 0)
+    if magic != MAGIC:
+        raise ValueError(f"not a LATEC GNN stream (bad magic {magic!r})")
+    if version != VERSION:
+        raise ValueError(f"unsupported LATEC GNN stream version {version}")
+    if PREFIX_SIZE + hlen > len(stream):
+        raise ValueError("truncated LATEC GNN stream header")
+    meta = json.loads(stream[PREFIX_SIZE:PREFIX_SIZE + hlen].decode("utf-8"))
+    payload = bitstream.zstd().decompress_into(
+        np.frombuffer(stream[PREFIX_SIZE + hlen:], np.uint8)).tobytes()
+    return meta, payload
+
+
+def _qparams(radius):
+    return _lib.QuantParams(dtype=_lib.F32, channels=1, radius=int(radius), order=1, center=0,
+                            end_mode=1, round_output=0, reserved=0)
+
+
+class GNNCodec:
+    """The learned codec (``latec/gnn_codec.py:1509-1922``)."""
+
+    def __init__(self, checkpoint_path=None, device=None, *, strict_checkpoint=True,
+                 weights=None, d=64, agg_level=1):
+        """``checkpoint_path``: a v7 axial-GNN checkpoint (as the reference).
+        Alternatively ``weights`` (a dict with the reference parameter names,
+        e.g. ``gnn.random_weights``) with ``d`` / ``agg_level``."""
+        torch = _torch()
+        _lib.load()
+        if weights is None:
+            if checkpoint_path is None:
+                raise ValueError("a checkpoint path or a weights dict is required")
+            path = Path(checkpoint_path)
+            if not path.exists():
+                raise FileNotFoundError(f"GNN checkpoint not found: {path}")
+            weights, d, agg_level = gnn.load_checkpoint(path)
+            h = hashlib.sha256()
+            with open(path, "rb") as f:
+                for block in iter(lambda: f.read(1 << 20), b""):
+                    h.update(block)
+            self.checkpoint_hash = h.digest()[:16]
+        else:
+            h = hashlib.sha256()
+            for k in gnn.param_shapes(d, agg_level):
+                h.update(np.ascontiguousarray(weights[k], np.float32).tobytes())
+            self.checkpoint_hash = h.digest()[:16]
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        self.strict_checkpoint = bool(strict_checkpoint)
+        self.d, self.agg_level = int(d), int(agg_level)
+        self.model = gnn.GNNModel(weights, self.d, self.agg_level, self.device)
+        self._geoms = {}
+
+    # ---------------------------------------------------------------- helpers
+    def _geometry(self, shape, levels):
+        key = (tuple(shape), int(levels))
+        g = self._geoms.get(key)
+        if g is None:
+            stride = 1 << int(levels)
+            g = gnn.build_stage_geoms(shape, levels, stride, 1, stride, self.agg_level,
+                                      device=self.device)[0]
+            self._geoms = {key: g}  # one shape at a time
+        return g
+
+    def _stage_ebs(self, shape, levels, eb, ratio):
+        """Per non-empty stage eb, in the geometry's stage order."""
+        from .levels import plan_for
+
+        stride = 1 << int(levels)
+        ebs = stage_ebs(shape, levels, stride, 1, eb, ratio)
+        counts = plan_for(shape, levels, stride, 1).counts
+        return [float(e) for e, n in zip(ebs, counts) if n]
+
+    # ---------------------------------------------------------------- encode
+    def compress(self, x, error_bound: float = 1e-2, *, levels="auto", radius: int = 1 << 15,
+                 zstd_level: int = 9, eb_ratio=None, tune: str = "fast", chunk_size=None,
+                 fp16: bool = True, compile="auto", gate: bool = True, gate_fine: bool = False,
+                 predictor: str = "gnn") -> bytes:
+        """Compress a NumPy array or torch tensor (``latec/gnn_codec.py:1576-1775``)."""
+        torch = _torch()
+        if tune not in ("fast", "size"):
+            raise ValueError("tune must be 'fast' or 'size'")
+        if isinstance(levels, str) and levels != "auto":
+            raise ValueError("levels must be a positive int or 'auto'")
+        if isinstance(compile, str) and compile != "auto":
+            raise ValueError("compile must be a bool or 'auto'")
+        if not isinstance(levels, str) and int(levels) < 1:
+            raise ValueError("levels must be >= 1")
+        if predictor != "gnn" and predictor not in INTERP_KINDS:
+            raise ValueError(f"predictor must be 'gnn' or one of {sorted(INTERP_KINDS)}")
+        if predictor != "gnn":
+            raise NotImplementedError("the interpolation ablation of the GNN codec is not built")
+        radius = int(radius)
+        if not 1 <= radius <= 32768:
+            raise ValueError("radius must be in [1, 32768]")
+        is_t = isinstance(x, torch.Tensor)
+        arr = x.detach() if is_t else np.asarray(x)
+        if (arr.numel() if is_t else arr.size) == 0:
+            raise ValueError("cannot compress an empty tensor")
+        np_dtype = np.dtype(str(arr.dtype).replace("torch.", "")) if is_t else np.dtype(arr.dtype)
+        if np_dtype.kind not in "biuf":
+            raise TypeError(f"unsupported dtype {np_dtype}; expected numeric data")
+        if np_dtype.kind != "f":
+            raise NotImplementedError("the GNN codec here codes floating-point tensors")
+        eb = float(error_bound)
+        if eb <= 0:
+            raise ValueError("error_bound must be > 0")
+        original_shape = tuple(int(n) for n in arr.shape)
+        shape = original_shape if original_shape else (1,)
+        lv = auto_levels(shape, self.agg_level) if isinstance(levels, str) else int(levels)
+        stride = 1 << lv
+        if chunk_size is not None:
+            edges = ((int(chunk_size),) * len(shape) if np.isscalar(chunk_size)
+                     else tuple(int(e) for e in chunk_size))
+            if len(edges) != len(shape):
+                raise ValueError("chunk_size must be scalar or one entry per axis")
+            for e in edges:
+                if e < stride or e % stride:
+                    raise ValueError("chunk_size must be a positive multiple of anchor_stride")
+            if any(e < n for e, n in zip(edges, shape)):
+                raise NotImplementedError("the GNN codec here codes the tensor as one region")
+        edges = tuple(-(-n // stride) * stride for n in shape)
+        t = arr if is_t else torch.from_numpy(np.ascontiguousarray(arr))
+        t = t.reshape(shape).to(self.device)
+        mm = torch.aminmax(t)
+        vmin = float(np.float32(float(mm.min.item())))
+        vmax = float(np.float32(float(mm.max.item())))
+        if vmax <= vmin:
+            vmax = vmin + 1.0
+        span = vmax - vmin
+        xn = ((t.to(torch.float32) - np.float32(vmin)) / np.float32(span)).reshape(-1).contiguous()
+        coarse = ([float(eb_ratio)] if eb_ratio is not None
+                  else (list(EB_COARSE_SWEEP) if tune == "size" else [EB_COARSE_FACTOR]))
+        ratios = sorted({per_step_eb_ratio(c, lv) for c in coarse})
+        best = None
+        for ratio in ratios:
+            payload = self._encode(xn, shape, lv, eb, ratio, radius)
+            meta = {"shape": list(original_shape), "dtype": np_dtype.str, "error_bound": eb,
+                    "levels": lv, "radius": radius, "vmin": vmin, "vmax": vmax,
+                    "eb_ratio": ratio, "checkpoint_hash": self.checkpoint_hash.hex(),
+                    "chunks": list(edges), "m_tile": 1 << 16, "fp16": False, "compiled": False,
+                    "predictor": "gnn", "float_path": FLOAT_PATH, "d": self.d,
+                    "agg_level": self.agg_level}
+            stream = write_stream(meta, payload, zstd_level)
+            if best is None or len(stream) < len(best):
+                best = stream
+        return best
+
+    def _encode(self, xn, shape, levels, eb, ratio, radius):
+        torch = _torch()
+        lib = _lib.load()
+        geoms = self._geometry(shape, levels)
+        ebs = self._stage_ebs(shape, levels, eb, ratio)
+        prm = _qparams(radius)
+        dev = self.device
+        E = torch.zeros((1, xn.numel(), len(shape), self.d), dtype=torch.float32, device=dev)
+        records, prev, ctx, vals = [], None, None, None
+        for g, seb in zip(geoms, ebs):
+            (mu, lb), E, ctx = gnn.stage_forward(self.model, E, prev, g, vals, finalize_ctx=ctx,
+                                                 eb=seb)
+            mu = mu.reshape(-1).contiguous()
+            xs = xn[g.query_idx].contiguous()
+            n = g.M
+            codes = torch.empty(n, dtype=torch.int16, device=dev)
+            recon = torch.empty(n, dtype=torch.float32, device=dev)
+            outl = torch.empty(n, dtype=torch.float32, device=dev)
+            stats = torch.zeros(ctypes_sizeof_stats(), dtype=torch.uint8, device=dev)
+            hseg = torch.empty(max(1, -(-n // (1 << 22))) * 512, dtype=torch.int32, device=dev)
+            htot = torch.empty(65536, dtype=torch.int32, device=dev)
+            ws = torch.empty(int(lib.latec_flat_workspace_bytes(n, _lib.F32)), dtype=torch.uint8,
+                             device=dev)
+            _lib.check(lib.latec_quantize(_byref(prm), seb, n, xs.data_ptr(), mu.data_ptr(),
+                                          codes.data_ptr(), recon.data_ptr(), outl.data_ptr(),
+                                          stats.data_ptr(), hseg.data_ptr(), htot.data_ptr(),
+                                          ws.data_ptr(), ws.numel(), _lib.stream_ptr()),
+                       "latec_quantize")
+            st = _lib.StageStats.from_buffer_copy(stats.cpu().numpy().tobytes())
+            kexp = max(1, int(st.maxq).bit_length())
+            scale = torch.exp2(lb.reshape(-1))
+            lv64 = rans.scale_to_level(scale, seb)
+            tables = rans.build_laplace_tables(seb, radius)
+            codes_u = codes.view(torch.int16)
+            shape_id = rans.choose_shape(_u16_as_i64(codes_u), lv64, tables, kexp) if n else 0
+            blob = rans.rans_encode(_u16_as_i64(codes_u), lv64, tables, kexp=kexp,
+                                    shape=shape_id, mode="native")
+            n_out = int(st.n_out)
+            frame = bitstream.pack_frame(len(blob), kexp, shape_id, 0, 0, False)
+            records.append(struct.pack("<IQ", n, frame) + blob + struct.pack("<I", n_out)
+                           + outl[:n_out].cpu().numpy().astype("<f4").tobytes())
+            prev, vals = g, recon.reshape(1, -1)
+        return b"".join(records)
+
+    # ---------------------------------------------------------------- decode
+    def uncompress(self, stream):
+        """Decompress a stream from ``compress`` into a torch tensor of the
+        original shape and dtype (``latec/gnn_codec.py:1777-1830``)."""
+        torch = _torch()
+        lib = _lib.load()
+        meta, payload = read_stream(bytes(stream))
+        if meta.get("float_path") != FLOAT_PATH:
+            raise ValueError("stream was not written by this codec's float path")
+        if self.strict_checkpoint and meta["checkpoint_hash"] != self.checkpoint_hash.hex():
+            raise ValueError("checkpoint hash differs from the stream metadata")
+        original_shape = tuple(int(n) for n in meta["shape"])
+        shape = original_shape or (1,)
+        dtype = np.dtype(meta["dtype"])
+        vmin, vmax = float(meta["vmin"]), float(meta["vmax"])
+        if vmax <= vmin:
+            vmax = vmin + 1.0
+        levels, radius = int(meta["levels"]), int(meta["radius"])
+        geoms = self._geometry(shape, levels)
+        ebs = self._stage_ebs(shape, levels, float(meta["error_bound"]), float(meta["eb_ratio"]))
+        prm = _qparams(radius)
+        dev = self.device
+        N = int(np.prod(shape))
+        recon_all = torch.zeros(N, dtype=torch.float32, device=dev)
+        E = torch.zeros((1, N, len(shape), self.d), dtype=torch.float32, device=dev)
+        off, prev, ctx, vals = 0, None, None, None
+        err = torch.zeros(1, dtype=torch.int32, device=dev)
+        for g, seb in zip(geoms, ebs):
+            (mu, lb), E, ctx = gnn.stage_forward(self.model, E, prev, g, vals, finalize_ctx=ctx,
+                                                 eb=seb)
+            mu = mu.reshape(-1).contiguous()
+            if off + 12 > len(payload):
+                raise ValueError("truncated GNN stage payload")
+            n, frame = struct.unpack_from("<IQ", payload, off)
+            f = bitstream.unpack_frame(frame)
+            if n != g.M:
+                raise ValueError("stage size differs from the schedule")
+            blob = payload[off + 12:off + 12 + f["hlen"]]
+            off += 12 + f["hlen"]
+            if off + 4 > len(payload):
+                raise ValueError("truncated GNN stage payload")
+            (n_out,) = struct.unpack_from("<I", payload, off)
+            off += 4
+            outl = np.frombuffer(payload, "<f4", count=n_out, offset=off) if n_out else \
+                np.zeros(1, np.float32)
+            off += 4 * n_out
+            lv64 = rans.scale_to_level(torch.exp2(lb.reshape(-1)), seb)
+            tables = rans.build_laplace_tables(seb, radius)
+            codes = rans.rans_decode(blob, lv64, tables, kexp=f["kexp"], shape=f["shape"],
+                                     mode="native")
+            codes_d = torch.from_numpy(codes.astype(np.uint16).view(np.int16)).to(dev)
+            outl_d = torch.from_numpy(np.ascontiguousarray(outl, np.float32)).to(dev)
+            recon = torch.empty(n, dtype=torch.float32, device=dev)
+            ws = torch.empty(max(int(lib.latec_dequantize_workspace_bytes(n)), 1),
+                             dtype=torch.uint8, device=dev)
+            _lib.check(lib.latec_dequantize(_byref(prm), seb, n, mu.data_ptr(), codes_d.data_ptr(),
+                                            outl_d.data_ptr(), n_out, recon.data_ptr(),
+                                            err.data_ptr(), ws.data_ptr(), ws.numel(),
+                                            _lib.stream_ptr()), "latec_dequantize")
+            recon_all[g.query_idx] = recon
+            prev, vals = g, recon.reshape(1, -1)
+        if off != len(payload):
+            raise ValueError("trailing data in GNN stage payload")
+        if int(err.item()):
+            raise ValueError("outlier count mismatch")
+        out = recon_all * np.float32(vmax - vmin) + np.float32(vmin)
+        out = out.reshape(original_shape).cpu()
+        return out.to(getattr(torch, dtype.name)) if dtype != np.float32 else out
+
+    decompress = uncompress
+
+
+GNNCompressorCodec = GNNCodec
+
+
+def ctypes_sizeof_stats():
+    import ctypes
+
+    return ctypes.sizeof(_lib.StageStats)
+
+
+def _byref(prm):
+    import ctypes
+
+    return ctypes.byref(prm)
+
+
+def _u16_as_i64(codes_i16):
+    """int16 storage of u16 codes -> int64 code values."""
+    return codes_i16.to(_torch().int64) & 0xFFFF

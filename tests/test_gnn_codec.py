@@ -1,0 +1,145 @@
+"""The learned codec (latec/gnn_codec.py) on the device: the flat
+dequantizer against the quantizer, and GNNCodec round trips with the bound
+held on every value, deterministic streams and the reference container."""
+
+import struct
+
+import numpy as np
+import pytest
+
+RADIUS = 1 << 15
+
+
+def test_auto_levels_follow_the_reference_table():
+    from latec_b200.gnn_codec import auto_levels, per_step_eb_ratio
+
+    assert auto_levels((512, 512), 1) == 8
+    assert auto_levels((128, 128, 64, 64), 1) == 5
+    assert auto_levels((256, 256, 256), 1) == 7
+    assert auto_levels((256, 256, 256), 2) == 6
+    assert auto_levels((20, 20), 1) == 3  # stride <= half the largest axis
+    assert per_step_eb_ratio(0.9, 1) == 1.0
+    assert per_step_eb_ratio(0.9, 5) ** 4 == pytest.approx(0.9)
+
+
+def _field(shape, seed):
+    rs = np.random.RandomState(seed)
+    g = np.meshgrid(*[np.linspace(0, 1, n) for n in shape], indexing="ij")
+    f = sum(np.sin((3 + k) * 2.7 * a + rs.rand() * 6) for k, a in enumerate(g))
+    return (f + 0.02 * rs.randn(*shape)).astype(np.float32) * 7.0 - 3.0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+def test_flat_dequantize_matches_quantizer(dtype):
+    import ctypes
+
+    import torch
+
+    from latec_b200 import _lib
+
+    lib = _lib.load()
+    ft = torch.float32 if dtype == "f32" else torch.float64
+    rs = np.random.RandomState(4)
+    n = 300_001
+    x = torch.from_numpy(rs.randn(n) * 5).to(ft).cuda()
+    pred = (x + torch.from_numpy(rs.randn(n) * 0.01).to(ft).cuda()).contiguous()
+    x[::101] = 1e6
+    prm = _lib.QuantParams(dtype=_lib.F32 if dtype == "f32" else _lib.F64, channels=1,
+                           radius=RADIUS, order=1, center=0, end_mode=1, round_output=0,
+                           reserved=0)
+    codes = torch.empty(n, dtype=torch.int16, device="cuda")
+    recon = torch.empty(n, dtype=ft, device="cuda")
+    outl = torch.empty(n, dtype=ft, device="cuda")
+    stats = torch.zeros(ctypes.sizeof(_lib.StageStats), dtype=torch.uint8, device="cuda")
+    hseg = torch.empty(512, dtype=torch.int32, device="cuda")
+    htot = torch.empty(65536, dtype=torch.int32, device="cuda")
+    ws = torch.empty(int(lib.latec_flat_workspace_bytes(n, prm.dtype)), dtype=torch.uint8,
+                     device="cuda")
+    sp = torch.cuda.current_stream().cuda_stream
+    _lib.check(lib.latec_quantize(ctypes.byref(prm), 0.01, n, x.data_ptr(), pred.data_ptr(),
+                                  codes.data_ptr(), recon.data_ptr(), outl.data_ptr(),
+                                  stats.data_ptr(), hseg.data_ptr(), htot.data_ptr(),
+                                  ws.data_ptr(), ws.numel(), sp))
+    st = _lib.StageStats.from_buffer_copy(stats.cpu().numpy().tobytes())
+    assert st.n_out > n // 101 - 2
+    back = torch.full((n,), 7.0, dtype=ft, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    ws2 = torch.empty(int(lib.latec_dequantize_workspace_bytes(n)), dtype=torch.uint8,
+                      device="cuda")
+    _lib.check(lib.latec_dequantize(ctypes.byref(prm), 0.01, n, pred.data_ptr(), codes.data_ptr(),
+                                    outl.data_ptr(), st.n_out, back.data_ptr(), err.data_ptr(),
+                                    ws2.data_ptr(), ws2.numel(), sp))
+    assert int(err.item()) == 0
+    assert torch.equal(back.view(torch.uint8), recon.view(torch.uint8))
+    _lib.check(lib.latec_dequantize(ctypes.byref(prm), 0.01, n, pred.data_ptr(), codes.data_ptr(),
+                                    outl.data_ptr(), st.n_out - 1, back.data_ptr(),
+                                    err.data_ptr(), ws2.data_ptr(), ws2.numel(), sp))
+    assert int(err.item()) & 1
+
+
+def _codec(seed=7, agg=1):
+    from latec_b200 import gnn
+    from latec_b200.gnn_codec import GNNCodec
+
+    return GNNCodec(weights=gnn.random_weights(seed, 64, agg), d=64, agg_level=agg)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,levels,eb,tune", [((40, 36), 3, 1e-3, "fast"),
+                                                   ((24, 20, 18), 2, 1e-2, "size"),
+                                                   ((70, 9), "auto", 3e-3, "fast")])
+def test_gnn_codec_round_trip_holds_the_bound(shape, levels, eb, tune):
+    import torch
+
+    from latec_b200.gnn_codec import MAGIC, VERSION, read_stream
+
+    codec = _codec()
+    x = _field(shape, 3)
+    s1 = codec.compress(x, eb, levels=levels, tune=tune)
+    s2 = codec.compress(torch.from_numpy(x).cuda(), eb, levels=levels, tune=tune)
+    assert s1 == s2  # deterministic, host or device input
+    magic, version, hlen = struct.unpack_from("<8sII", s1, 0)
+    assert magic == MAGIC and version == VERSION
+    meta, _ = read_stream(s1)
+    assert meta["shape"] == list(shape) and meta["dtype"] == np.dtype(np.float32).str
+    out = codec.uncompress(s1)
+    assert isinstance(out, torch.Tensor) and out.dtype == torch.float32
+    assert tuple(out.shape) == shape
+    vmin, vmax = float(np.float32(x.min())), float(np.float32(x.max()))
+    xn = (x.astype(np.float32) - np.float32(vmin)) / np.float32(vmax - vmin)
+    on = (out.numpy() - np.float32(vmin)) / np.float32(vmax - vmin)
+    slack = 4 * np.finfo(np.float32).eps
+    assert np.abs(on.astype(np.float64) - xn).max() <= eb + slack
+    assert np.array_equal(codec.uncompress(s1).numpy(), out.numpy())
+    assert len(s1) < x.nbytes
+
+
+@pytest.mark.gpu
+def test_gnn_codec_float64_and_errors():
+    import torch
+
+    from latec_b200.gnn_codec import GNNCodec
+
+    codec = _codec()
+    x = _field((33, 31), 5).astype(np.float64)
+    s = codec.compress(x, 1e-3, levels=3)
+    out = codec.uncompress(s)
+    assert out.dtype == torch.float64
+    span = x.max() - x.min()
+    assert np.abs(out.numpy() - x).max() <= 1e-3 * span * (1 + 1e-5) + 1e-6 * span
+    with pytest.raises(ValueError):
+        codec.uncompress(b"NOTLATEC" + s[8:])
+    with pytest.raises(ValueError):
+        _codec(seed=8).uncompress(s)  # foreign weights: checkpoint hash differs
+    assert _codec(seed=8).__class__ is GNNCodec
+    with pytest.raises(ValueError):
+        codec.compress(np.zeros((0, 4), np.float32), 1e-3)
+    with pytest.raises(ValueError):
+        codec.compress(x, 0.0)
+    with pytest.raises(NotImplementedError):
+        codec.compress(x.astype(np.int32), 1e-3)
+    with pytest.raises(NotImplementedError):
+        codec.compress(x, 1e-3, levels=3, chunk_size=8)
+    with pytest.raises(FileNotFoundError):
+        GNNCodec("/nonexistent/checkpoint.pt")
