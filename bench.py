@@ -54,14 +54,51 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi sampler during the timed region."""
+    """SM clock and clock-event reasons during the timed region, read (never
+    set) through NVML every 5 ms; nvidia-smi at 200 ms when NVML is missing."""
+
+    # NVML clock-event reason bits
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap"}
 
     def __init__(self, gpu_index):
         self.idx = gpu_index
-        self.rows = []
+        self.rows = []  # (sm_mhz, max_mhz, reasons bitmask)
         self.proc = None
+        self.stop = threading.Event()
+        self.t = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:
+            p = torch.cuda.get_device_properties(self.idx)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.idx)
+
+    def _nvml_loop(self, nv, h):
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                self.rows.append((float(sm), float(mx), int(rs)))
+            except Exception:
+                pass
+            self.stop.wait(0.005)
 
     def __enter__(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.t = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            pass
         q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
@@ -69,39 +106,40 @@ class ClockSampler:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200",
                  "-i", str(self.idx)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t = threading.Thread(target=self._smi_read, daemon=True)
             self.t.start()
         except Exception:
             self.proc = None
         return self
 
-    def _read(self):
+    def _smi_read(self):
+        bits = [0x8, 0x40, 0x20, 0x4]
         for line in self.proc.stdout:
-            self.rows.append([v.strip() for v in line.split(",")])
+            r = [v.strip() for v in line.split(",")]
+            try:
+                mask = sum(b for b, v in zip(bits, r[2:6]) if v.lower() == "active")
+                self.rows.append((float(r[0]), float(r[1]), mask))
+            except (ValueError, IndexError):
+                continue
 
     def __exit__(self, *a):
+        self.stop.set()
         if self.proc is not None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.t is not None:
+            self.t.join(timeout=5)
 
     def summary(self):
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        sm, mx, reasons = [], [], set()
-        for r in self.rows:
-            try:
-                sm.append(float(r[0]))
-                mx.append(float(r[1]))
-                for n, v in zip(names, r[2:6]):
-                    if v.lower() == "active":
-                        reasons.add(n)
-            except (ValueError, IndexError):
-                continue
-        if not sm:
+        if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons)}
+        reasons = sorted({n for _, _, m in self.rows for b, n in self.REASONS.items() if m & b})
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows),
+                "sm_max_mhz": max(r[1] for r in self.rows), "reasons": reasons,
+                "samples": len(self.rows)}
 
 
 def make_field(device):
@@ -132,6 +170,58 @@ def cpu_baseline(steps=1):
         dt = time.perf_counter() - t0
         best = dt if best is None else min(best, dt)
     return x.nbytes / best / 1e9, x.nbytes / len(stream)
+
+
+# DRAM bytes (read + write) of one fused encode pass over the 512^3 workload:
+# the ncu capture of the same pass at 384^3 scaled by the point count.
+TRAFFIC_PER_PASS = 4.155e9
+
+GNN_SHAPE = (32, 32, 32, 32)
+GNN_EB, GNN_LEVELS = 1e-3, 4
+
+
+def gnn_leg(dev, steps=2):
+    """Learned codec beside the plain one on one 32^4 chunk of the 4-D mixed
+    field (0.5 anisotropic GRF + 0.5 turbulence+jumps; the reference's auto
+    chunk of a 128x128x64x64 tensor), absolute eb 1e-3, levels 4, seeded
+    random GNN weights (no trained checkpoint is available on the box).
+    Wall time of compress + decompress through the public API with the field
+    on the device."""
+    import torch
+
+    import latec_b200 as lb
+    from latec_b200 import fields, gnn
+
+    x = fields.mixed_4d(GNN_SHAPE, seed=3, device=dev)
+    span = float(x.max().item()) - float(x.min().item())
+    codec = lb.GNNCodec(weights=gnn.random_weights(0, 64, 1), d=64, agg_level=1, device=dev)
+    rel = GNN_EB / span
+    s = codec.compress(x, rel, levels=GNN_LEVELS)  # warm-up (geometry, tables)
+    codec.uncompress(s)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s = codec.compress(x, rel, levels=GNN_LEVELS)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(steps):
+        out = codec.uncompress(s)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    err = float((out.to(dev) - x).abs().max().item())
+    # float32 normalise / denormalise slack of the reference
+    # (latec/gnn_codec.py:188-226): the bound is exact on the [0, 1] values
+    vmin, vmax = float(x.min().item()), float(x.max().item())
+    slack = 2.0 ** -24 * (3.0 * span + max(abs(vmin), abs(vmax)))
+    si, _ = lb.compress(x, GNN_EB, lb.InterpPredictor("cubic", GNN_LEVELS, 16, 1),
+                        levels=GNN_LEVELS, anchor_stride=16, recon="none")
+    nbytes = x.numel() * 4
+    return {"workload": "one 32^4 chunk of the 4-D mixed field, abs eb 1e-3, levels 4",
+            "weights": "seeded random initialisation (untrained)",
+            "ratio_gnn": nbytes / len(s), "ratio_interp": nbytes / len(si),
+            "compress_gbs": nbytes * steps / (t1 - t0) / 1e9,
+            "decompress_gbs": nbytes * steps / (t2 - t1) / 1e9,
+            "max_abs_err": err, "bound": GNN_EB, "roundtrip_slack": slack, "dtype": "f32"}
 
 
 def run_reference(args, rank):
@@ -206,6 +296,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="latec_b200", choices=["latec_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-gnn", action="store_true", help="skip the learned-codec leg")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + timed device round trips (for ncu launch lists)")
     ap.add_argument("--shape", type=int, nargs="+", default=None,
@@ -352,6 +443,7 @@ def main():
         cpu = {"value": v, "unit": "GB/s", "cores": 1, "kind": "port",
                "sample": f"{SAMPLE[0]}^3 float32 field of the same generator, one compress + "
                          "decompress round trip with the CPU oracle (NumPy + C rANS, compat mode)"}
+    gnn_line = None if args.no_gnn else gnn_leg(dev)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -369,13 +461,16 @@ def main():
                    "shape": list(SHAPE), "eb": eb, "parallelism": f"replicas x{world}",
                    "l2": "input 512 MiB > 126 MB L2, no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": TRAFFIC_PER_PASS,
+                     "traffic_source": "ncu dram bytes of the pass at 384^3 scaled by points "
+                                       "(profiles/k_interp_quant_turb384.md)",
                      "kernel": "k_interp_quant pass (31 stages incl. scan/compaction)",
                      "alg_bytes": alg_bytes, "pass_ms": pass_ms, "peak_kind": peak_kind},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": "GB/s", "h2d_bytes_per_step": nbytes + len(s_e),
                 "d2h_bytes_per_step": nbytes + len(s_e)},
         "gpu_launches": int(launches),
+        "gnn": gnn_line,
         "clocks": sampler.summary(),
     }), flush=True)
 

@@ -311,6 +311,18 @@ int latec_gnn_finalize(const latec_gnn_model* model, int32_t B, int64_t N, int32
                        const int32_t* query, const float* ctx, const float* vals, float* E,
                        void* workspace, uint64_t workspace_bytes, void* stream);
 
+/* ---- tensor-core MLP of the GNN message pass (BiDirEmbed / DirEmbed /
+ *      MixEmbed, latec/gnn_predictor.py:624-661,792-806): Y = W2 * gelu(W1 * X
+ *      + b1) + b2 with hidden width 128 and output width 64, BF16 operands
+ *      and FP32 accumulation on tcgen05. Weights are packed on the host into
+ *      the tensor cores' BF16 layout by latec_gnn_pack_bf16 (n x k float32,
+ *      k zero-padded to kp, a multiple of 16; out: n * kp uint16). err bit 1:
+ *      a tensor-core completion wait ran out (the output is invalid). */
+int latec_gnn_pack_bf16(const float* w, int32_t n, int32_t k, int32_t kp, uint16_t* out);
+int latec_gnn_mlp2_bf16(const float* X, int32_t ldx, int64_t rows, int32_t k1, int32_t k1p,
+                        const void* w1p, const float* b1, const void* w2p, const float* b2,
+                        float* Y, int32_t ldy, uint32_t* err, void* stream);
+
 /* ---- flat quantizer without any device allocation (no counterpart in the
  *      reference). For callers that cannot call cudaMalloc -- e.g. an
  *      application whose GPU memory is owned by another allocator, or a

@@ -114,6 +114,9 @@ SIGNATURES = {
                                       ctypes.c_float, P, P, P, U64, P]),
     "latec_gnn_finalize": (ctypes.c_int, [ctypes.POINTER(GnnModel), I32, ctypes.c_int64, I32,
                                           I32, P, P, P, P, P, U64, P]),
+    "latec_gnn_pack_bf16": (ctypes.c_int, [P, I32, I32, I32, P]),
+    "latec_gnn_mlp2_bf16": (ctypes.c_int, [P, I32, ctypes.c_int64, I32, I32, P, P, P, P, P, I32,
+                                           P, P]),
     "latec_raw_frame_bytes": (U64, [U64]),
     "latec_frame_raw": (ctypes.c_int, [P, U64, P, ctypes.c_uint32, P, U64, P]),
     "latec_unframe_raw": (ctypes.c_int, [P, U64, P, P, P]),

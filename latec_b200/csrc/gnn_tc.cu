@@ -1,0 +1,301 @@
+// Fused two-layer MLP of the GNN message pass on the 5th-generation tensor
+// cores: Y = W2 * gelu(W1 * X + b1) + b2 for rows of X, with BF16 operands in
+// shared memory and FP32 accumulators in tensor memory (tcgen05).
+//
+// One persistent CTA of 4 warps per SM. W1 (N1 x K1) and W2 (N2 x N1) are
+// staged once per CTA in shared memory; then for every 128-row tile:
+//   1. the 128 rows of X (float32, any row stride) are rounded to BF16 into
+//      shared memory (zero-padded to K1p, a multiple of 16);
+//   2. one elected thread issues K1p / 16 tcgen05.mma (M 128, N N1, K 16)
+//      into TMEM columns [0, N1) and commits them to an mbarrier;
+//   3. each warp reads its 32 TMEM lanes (rows) back with tcgen05.ld, adds b1,
+//      applies GELU and writes the BF16 hidden row to shared memory: the A
+//      operand of layer 2;
+//   4. N1 / 16 tcgen05.mma into TMEM columns [N1, N1 + N2), commit, wait;
+//   5. the epilogue adds b2 and stores the float32 row of Y.
+// Operands use the no-swizzle K-major canonical layout: 8 x 16-byte core
+// matrices, row groups 128 bytes apart (SBO) and 8-element K chunks R * 16
+// bytes apart (LBO), R the operand's rows. Weights arrive pre-packed in that
+// layout (latec_gnn_pack_bf16). Every mbarrier wait has an iteration limit;
+// on expiry the kernel records an error, stops issuing and frees its TMEM.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "latec_common.cuh"
+
+namespace latec {
+namespace {
+
+constexpr int TC_THREADS = 128;
+constexpr int TC_M = 128;
+constexpr uint32_t TC_WAIT_LIMIT = 1u << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Canonical K-major element offset of (row r, column k) in an R-row operand.
+__host__ __device__ __forceinline__ uint32_t canon(uint32_t r, uint32_t k, uint32_t R) {
+    return ((k >> 3) * (R >> 3) + (r >> 3)) * 64u + (r & 7u) * 8u + (k & 7u);
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);  // version 1, no swizzle
+}
+
+// kind::f16 instruction descriptor: BF16 A and B (K-major), FP32 D, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(uint32_t M, uint32_t N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+        mbar));
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, P;\n\t}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(parity));
+    return ok != 0;
+}
+
+// Bounded wait: false if the phase did not complete within the limit.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    for (uint32_t i = 0; i < TC_WAIT_LIMIT; i++)
+        if (mbar_try_wait(mbar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%"
+        "14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float gelu_tc(float x) {
+    return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f));
+}
+
+// N1 = hidden width (128), N2 = output width (64); K1P = padded input width.
+template <int N1, int N2>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_mlp2_tc(const float* __restrict__ X, int ldx, int rows, int k1, int k1p,
+              const __nv_bfloat16* __restrict__ w1p, const float* __restrict__ b1,
+              const __nv_bfloat16* __restrict__ w2p, const float* __restrict__ b2,
+              float* __restrict__ Y, int ldy, uint32_t* __restrict__ err) {
+    extern __shared__ __align__(128) uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    __nv_bfloat16* sw1 = (__nv_bfloat16*)smem_raw;             // N1 x k1p
+    __nv_bfloat16* sw2 = sw1 + (size_t)N1 * k1p;                // N2 x N1
+    __nv_bfloat16* sa = sw2 + (size_t)N2 * N1;                  // 128 x k1p
+    __nv_bfloat16* sh = sa + (size_t)TC_M * k1p;                // 128 x N1
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    // stage the packed weights (16-byte copies)
+    {
+        const int4* s1 = (const int4*)w1p;
+        int4* d1 = (int4*)sw1;
+        for (int i = tid; i < N1 * k1p / 8; i += TC_THREADS) d1[i] = s1[i];
+        const int4* s2 = (const int4*)w2p;
+        int4* d2 = (int4*)sw2;
+        for (int i = tid; i < N2 * N1 / 8; i += TC_THREADS) d2[i] = s2[i];
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    constexpr uint32_t TMEM_COLS = (N1 + N2) <= 128 ? 128 : ((N1 + N2) <= 256 ? 256 : 512);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_base)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base;
+    const uint32_t mb = smem_u32(&mbar);
+    uint32_t phase = 0;
+    bool ok = true;
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    const int row_in_tile = warp * 32 + lane;  // TMEM lane of this thread
+    const int n_tiles = (rows + TC_M - 1) / TC_M;
+
+    for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+        const int r0 = t * TC_M;
+        // 1. X rows -> BF16 A operand (each warp fills 32 rows, lanes along k)
+        for (int rr = 0; rr < 32; rr++) {
+            const int r = warp * 32 + rr;
+            const int gr = r0 + r;
+            for (int k = lane; k < k1p; k += 32) {
+                const float v = (gr < rows && k < k1) ? X[(int64_t)gr * ldx + k] : 0.0f;
+                sa[canon(r, k, TC_M)] = __float2bfloat16_rn(v);
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        // 2. layer 1
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sw1);
+            for (int kk = 0; kk < k1p / 16; kk++) {
+                const uint64_t ad = smem_desc(a0 + kk * 2 * TC_M * 16, TC_M * 16, 128);
+                const uint64_t bd = smem_desc(b0 + kk * 2 * N1 * 16, N1 * 16, 128);
+                mma_bf16(tmem, ad, bd, idesc_bf16(TC_M, N1), kk > 0);
+            }
+            mma_commit(mb);
+        }
+        ok = __syncthreads_and(mbar_wait(mb, phase)) != 0;  // one decision for the CTA
+        if (!ok) {
+            if (tid == 0) atomicOr(err, 1u);
+            break;
+        }
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        // 3. epilogue 1: bias + GELU -> BF16 hidden (A operand of layer 2)
+        for (int c = 0; c < N1; c += 16) {
+            float v[16];
+            tmem_ld16(tmem + lane_base + c, v);
+#pragma unroll
+            for (int i = 0; i < 16; i++)
+                sh[canon(row_in_tile, c + i, TC_M)] =
+                    __float2bfloat16_rn(gelu_tc(__fadd_rn(v[i], b1[c + i])));
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        // 4. layer 2
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t a0 = smem_u32(sh), b0 = smem_u32(sw2);
+            for (int kk = 0; kk < N1 / 16; kk++) {
+                const uint64_t ad = smem_desc(a0 + kk * 2 * TC_M * 16, TC_M * 16, 128);
+                const uint64_t bd = smem_desc(b0 + kk * 2 * N2 * 16, N2 * 16, 128);
+                mma_bf16(tmem + N1, ad, bd, idesc_bf16(TC_M, N2), kk > 0);
+            }
+            mma_commit(mb);
+        }
+        ok = __syncthreads_and(mbar_wait(mb, phase)) != 0;  // one decision for the CTA
+        if (!ok) {
+            if (tid == 0) atomicOr(err, 1u);
+            break;
+        }
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        // 5. epilogue 2: bias -> float32 rows of Y
+        const int gr = r0 + row_in_tile;
+        for (int c = 0; c < N2; c += 16) {
+            float v[16];
+            tmem_ld16(tmem + lane_base + N1 + c, v);
+            if (gr < rows) {
+#pragma unroll
+                for (int i = 0; i < 16; i++) Y[(int64_t)gr * ldy + c + i] = __fadd_rn(v[i], b2[c + i]);
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+    }
+    if (!ok) {
+        // an MMA may still be in flight: wait for it (bounded) before freeing
+        // the tensor memory it writes
+        mbar_wait(mb, phase);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(TMEM_COLS));
+    }
+}
+
+}  // namespace
+
+// Shared memory of the fused kernel for an input width padded to k1p.
+uint64_t mlp2_tc_smem(int k1p, int n1, int n2) {
+    return 2ull * ((uint64_t)n1 * k1p + (uint64_t)n2 * n1 + (uint64_t)TC_M * k1p +
+                   (uint64_t)TC_M * n1);
+}
+
+int mlp2_tc(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* w1p,
+            const float* b1, const void* w2p, const float* b2, int n1, int n2, float* Y, int ldy,
+            uint32_t* err, int n_sm, cudaStream_t st) {
+    if (rows <= 0) return LATEC_OK;
+    if (n1 != 128 || n2 != 64 || k1p % 16 || k1p < k1 || rows > 0x7fffffffLL)
+        return LATEC_ERR_UNSUPPORTED;
+    const uint64_t smem = mlp2_tc_smem(k1p, n1, n2);
+    if (smem > 220 * 1024) return LATEC_ERR_UNSUPPORTED;
+    auto kern = k_mlp2_tc<128, 64>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return LATEC_ERR_CUDA;
+    const int64_t tiles = (rows + TC_M - 1) / TC_M;
+    const int grid = (int)(tiles < n_sm ? tiles : n_sm);
+    kern<<<grid, TC_THREADS, smem, st>>>(X, ldx, (int)rows, k1, k1p, (const __nv_bfloat16*)w1p, b1,
+                                         (const __nv_bfloat16*)w2p, b2, Y, ldy, err);
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
+}
+
+}  // namespace latec
+
+using namespace latec;
+
+extern "C" {
+
+// Pack a float32 (n x k) weight matrix, row-major, into the BF16 no-swizzle
+// K-major canonical layout the tensor-core MLP reads (k zero-padded to kp,
+// a multiple of 16; n a multiple of 8). Host arrays; out has n * kp entries.
+int latec_gnn_pack_bf16(const float* w, int32_t n, int32_t k, int32_t kp, uint16_t* out) {
+    if (!w || !out || n < 8 || n % 8 || k < 1 || kp < k || kp % 16) return LATEC_ERR_ARG;
+    for (int r = 0; r < n; r++)
+        for (int c = 0; c < kp; c++) {
+            const float v = c < k ? w[(int64_t)r * k + c] : 0.0f;
+            const __nv_bfloat16 b = __float2bfloat16_rn(v);
+            out[canon((uint32_t)r, (uint32_t)c, (uint32_t)n)] = *(const uint16_t*)&b;
+        }
+    return LATEC_OK;
+}
+
+// Y = W2 * gelu(W1 * X + b1) + b2 on the tensor cores (hidden 128, output 64).
+// w1p / w2p: device, packed by latec_gnn_pack_bf16 (w1: 128 x k1p,
+// w2: 64 x 128). err bit 1: a tensor-core wait ran out (results invalid).
+int latec_gnn_mlp2_bf16(const float* X, int32_t ldx, int64_t rows, int32_t k1, int32_t k1p,
+                        const void* w1p, const float* b1, const void* w2p, const float* b2,
+                        float* Y, int32_t ldy, uint32_t* err, void* stream) {
+    if ((rows && (!X || !Y)) || !w1p || !b1 || !w2p || !b2 || !err || ldx < k1 || ldy < 64)
+        return LATEC_ERR_ARG;
+    int dev = 0, n_sm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    return mlp2_tc(X, ldx, rows, k1, k1p, w1p, b1, w2p, b2, 128, 64, Y, ldy, err, n_sm,
+                   (cudaStream_t)stream);
+}
+
+}  // extern "C"
