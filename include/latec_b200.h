@@ -277,6 +277,11 @@ int latec_shape_costs(const uint16_t* codes, const uint8_t* levels, uint64_t n, 
 typedef struct {
     int32_t d, agg_level;
     const float* params;
+    /* optional: BiDirEmbed, DirEmbed and MixEmbed weights packed by
+     * latec_gnn_pack_bf16 (in that order, first then second layer each), to run
+     * those MLPs in BF16 on the tensor cores (d = 64 only); NULL = float32 */
+    const void* packed_bf16;
+    uint32_t* tc_err;  /* device word, bit 1: a tensor-core wait ran out */
 } latec_gnn_model;
 
 typedef struct {

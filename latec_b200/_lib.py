@@ -58,7 +58,7 @@ class FitStage(ctypes.Structure):
 
 
 class GnnModel(ctypes.Structure):
-    _fields_ = [("d", I32), ("agg_level", I32), ("params", P)]
+    _fields_ = [("d", I32), ("agg_level", I32), ("params", P), ("packed_bf16", P), ("tc_err", P)]
 
 
 class GnnGeom(ctypes.Structure):

@@ -19,6 +19,11 @@
 
 
 namespace latec {
+
+int mlp2_tc(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* w1p,
+            const float* b1, const void* w2p, const float* b2, int n1, int n2, float* Y, int ldy,
+            uint32_t* err, int n_sm, cudaStream_t st);
+
 namespace {
 
 constexpr int LT = 256;  // threads of every kernel here
@@ -286,6 +291,49 @@ Params carve(const float* p0, int d, int agg) {
     return q;
 }
 
+// BF16 tensor-core copies of the BiDir / Dir / Mix MLP weights (d = 64):
+// each layer in the layout of latec_gnn_pack_bf16, input width padded to 16.
+struct Packed {
+    const uint16_t *bi1, *bi2, *dir1, *dir2, *mix1, *mix2;
+    int bi_k1p, dir_k1p, mix_k1p;
+};
+
+inline int pad16(int k) { return (k + 15) / 16 * 16; }
+
+Packed packed_of(const void* base, const Params& P) {
+    Packed k;
+    const uint16_t* p = (const uint16_t*)base;
+    k.bi_k1p = pad16(2 * P.de + 2);
+    k.dir_k1p = pad16(P.de + 2);
+    k.mix_k1p = pad16(2 * P.d);
+    k.bi1 = p; p += (size_t)P.h * k.bi_k1p;
+    k.bi2 = p; p += (size_t)P.d * P.h;
+    k.dir1 = p; p += (size_t)P.h * k.dir_k1p;
+    k.dir2 = p; p += (size_t)P.d * P.h;
+    k.mix1 = p; p += (size_t)P.h * k.mix_k1p;
+    k.mix2 = p;
+    return k;
+}
+
+int n_sms() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0, v = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess &&
+            cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
+            n = v;
+        else
+            n = 148;
+    }
+    return n;
+}
+
+// Two-layer MLP over rows of X: on the tensor cores when the model carries
+// packed BF16 weights, else the float32 path.
+int mlp2(const latec_gnn_model* m, const float* X, int ldx, int64_t rows, int k1, const float* w1,
+         const float* b1, const uint16_t* w1p, int k1p, const float* w2, const float* b2,
+         const uint16_t* w2p, int h, int d, float* H, float* Y, int ldy, cudaStream_t st);
+
 int linear(const float* X, int ldx, int64_t rows, int in, const float* W, const float* b, int out,
            float* Y, int ldy, int act, cudaStream_t st) {
     if (rows <= 0) return LATEC_OK;
@@ -297,6 +345,17 @@ int linear(const float* X, int ldx, int64_t rows, int in, const float* W, const 
     return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
 }
 
+int mlp2(const latec_gnn_model* m, const float* X, int ldx, int64_t rows, int k1, const float* w1,
+         const float* b1, const uint16_t* w1p, int k1p, const float* w2, const float* b2,
+         const uint16_t* w2p, int h, int d, float* H, float* Y, int ldy, cudaStream_t st) {
+    if (m->packed_bf16)
+        return mlp2_tc(X, ldx, rows, k1, k1p, w1p, b1, w2p, b2, h, d, Y, ldy, m->tc_err, n_sms(),
+                       st);
+    int rc = linear(X, ldx, rows, k1, w1, b1, h, H, h, 1, st);
+    if (!rc) rc = linear(H, h, rows, h, w2, b2, d, Y, ldy, 0, st);
+    return rc;
+}
+
 unsigned blocks_for(int64_t threads) { return (unsigned)((threads + LT - 1) / LT); }
 
 int launched(int n) {
@@ -306,7 +365,7 @@ int launched(int n) {
 
 bool valid_model(const latec_gnn_model* m) {
     return m && m->params && m->d >= 4 && m->d <= 128 && m->d % 2 == 0 && m->agg_level >= 1 &&
-           m->agg_level <= 8;
+           m->agg_level <= 8 && (!m->packed_bf16 || (m->d == 64 && m->tc_err));
 }
 
 }  // namespace
@@ -317,7 +376,7 @@ using namespace latec;
 extern "C" {
 
 uint64_t latec_gnn_param_count(int32_t d, int32_t agg_level) {
-    latec_gnn_model m{d, agg_level, (const float*)16};
+    latec_gnn_model m{d, agg_level, (const float*)16, nullptr, nullptr};
     if (!valid_model(&m)) return 0;
     return carve(nullptr, d, agg_level).count;
 }
@@ -355,6 +414,7 @@ int latec_gnn_embed(const latec_gnn_model* model, int32_t B, int64_t N, const fl
         return LATEC_ERR_WORKSPACE;
     cudaStream_t st = (cudaStream_t)stream;
     const Params P = carve(model->params, d, model->agg_level);
+    const Packed pk = packed_of(model->packed_bf16, P);
     const float scale = 1.0f / sqrtf((float)d);
     const int64_t w2 = 2 * P.de + 2, w1 = P.de + 2;
     int rc = LATEC_OK;
@@ -378,15 +438,18 @@ int latec_gnn_embed(const latec_gnn_model* model, int32_t B, int64_t N, const fl
                 k_rows_two<<<blocks_for(n2 * K * 32), LT, 0, st>>>(E, N, K, d, P.ds, P.table, g, b,
                                                                   g.two + g.two_off[t], n2, X);
                 rc = launched(1);
-                if (!rc) rc = linear(X, (int)w2, n2 * K, (int)w2, P.bi0w, P.bi0b, P.h, H, P.h, 1, st);
-                if (!rc) rc = linear(H, P.h, n2 * K, P.h, P.bi2w, P.bi2b, d, msb, d, 0, st);
+                if (!rc)
+                    rc = mlp2(model, X, (int)w2, n2 * K, (int)w2, P.bi0w, P.bi0b, pk.bi1, pk.bi_k1p,
+                              P.bi2w, P.bi2b, pk.bi2, P.h, d, H, msb, d, st);
             }
             if (n1 && !rc) {
                 k_rows_one<<<blocks_for(n1 * K * 32), LT, 0, st>>>(E, N, K, d, P.ds, P.table, g, b,
                                                                   g.one + g.one_off[t], n1, X);
                 rc = launched(1);
-                if (!rc) rc = linear(X, (int)w1, n1 * K, (int)w1, P.dir0w, P.dir0b, P.h, H, P.h, 1, st);
-                if (!rc) rc = linear(H, P.h, n1 * K, P.h, P.dir2w, P.dir2b, d, msb + n2 * K * d, d, 0, st);
+                if (!rc)
+                    rc = mlp2(model, X, (int)w1, n1 * K, (int)w1, P.dir0w, P.dir0b, pk.dir1,
+                              pk.dir_k1p, P.dir2w, P.dir2b, pk.dir2, P.h, d, H, msb + n2 * K * d, d,
+                              st);
             }
         }
         // line pool keys and values of every live row
@@ -466,8 +529,10 @@ int latec_gnn_finalize(const latec_gnn_model* model, int32_t B, int64_t N, int32
     if (rc) return rc;
     k_mix_rows<<<blocks_for(bmk * 2 * d), LT, 0, st>>>(ctx, VE, bmk, K, d, X);
     rc = launched(1);
-    if (!rc) rc = linear(X, 2 * d, bmk, 2 * d, P.mx0w, P.mx0b, P.h, H, P.h, 1, st);
-    if (!rc) rc = linear(H, P.h, bmk, P.h, P.mx2w, P.mx2b, d, Y, d, 0, st);
+    const Packed pk = packed_of(model->packed_bf16, P);
+    if (!rc)
+        rc = mlp2(model, X, 2 * d, bmk, 2 * d, P.mx0w, P.mx0b, pk.mix1, pk.mix_k1p, P.mx2w, P.mx2b,
+                  pk.mix2, P.h, d, H, Y, d, st);
     if (rc) return rc;
     k_scatter_e<<<blocks_for(bmk * d), LT, 0, st>>>(Y, query, B, M, K, d, N, E);
     return launched(1);

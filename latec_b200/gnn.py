@@ -301,13 +301,22 @@ class GNNModel:
     """The axial GNN with its parameters packed on the device in the
     reference state_dict order; every method runs the CUDA kernels."""
 
-    def __init__(self, weights: dict, d: int = 64, agg_level: int = 1, device=None):
+    def __init__(self, weights: dict, d: int = 64, agg_level: int = 1, device=None,
+                 precision: str = "f32"):
+        """``precision``: "f32" (every layer in float32) or "bf16" (the
+        BiDirEmbed, DirEmbed and MixEmbed MLPs in BF16 on the tensor cores with
+        float32 accumulation; pools and readout stay float32; d = 64)."""
         import ctypes
 
         torch = _torch()
         from . import _lib
 
         lib = _lib.load()
+        if precision not in ("f32", "bf16"):
+            raise ValueError("precision must be 'f32' or 'bf16'")
+        if precision == "bf16" and int(d) != 64:
+            raise NotImplementedError("the tensor-core message pass is built for d = 64")
+        self.precision = precision
         self.d, self.agg_level = int(d), int(agg_level)
         shapes = param_shapes(self.d, self.agg_level)
         flat = np.concatenate([np.asarray(weights[k], np.float32).reshape(-1) for k in shapes])
@@ -318,6 +327,21 @@ class GNNModel:
         self.params = torch.from_numpy(flat).to(self.device)
         m = _lib.GnnModel()
         m.d, m.agg_level, m.params = self.d, self.agg_level, self.params.data_ptr()
+        self.tc_err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        if precision == "bf16":
+            parts = []
+            for name in ("bidir.net.0", "bidir.net.2", "dir.net.0", "dir.net.2", "mix.net.0",
+                         "mix.net.2"):
+                w = np.ascontiguousarray(weights[name + ".weight"], np.float32)
+                n, k = w.shape
+                kp = -(-k // 16) * 16
+                out = np.empty(n * kp, np.uint16)
+                _lib.check(lib.latec_gnn_pack_bf16(w.ctypes.data, n, k, kp, out.ctypes.data),
+                           "latec_gnn_pack_bf16")
+                parts.append(out)
+            self.packed = torch.from_numpy(np.concatenate(parts).view(np.int16)).to(self.device)
+            m.packed_bf16 = self.packed.data_ptr()
+            m.tc_err = self.tc_err.data_ptr()
         self.struct = m
         self._ws = None
         self._lib = lib

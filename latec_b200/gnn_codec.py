@@ -28,11 +28,14 @@ Scope of this version:
 * The whole tensor is one region: no chunk grid and no halos.
 * There is no interpolation gate: every stage uses the GNN.
 * Float inputs only.
-* The network runs in float32. The ``fp16`` and ``compile`` flags are accepted
-  and recorded as float32 / not compiled.
+* ``fp16=True`` (the default, as in the reference) runs the message and
+  finalisation MLPs in BF16 on the tensor cores (tcgen05) with float32
+  accumulation; pools and the readout stay float32. ``fp16=False`` is float32
+  throughout. ``compile`` is accepted and recorded as not compiled.
 
-Streams carry ``"float_path": "latec_b200-f32-1"``. As the reference's own
-encoder/decoder contract requires, they decode only with this float path.
+Streams carry their ``"float_path"`` (``latec_b200-bf16-1`` or
+``latec_b200-f32-1``). As the reference's own encoder/decoder contract
+requires, they decode only with that float path.
 """
 
 from __future__ import annotations
@@ -51,7 +54,7 @@ MAGIC = b"LATECGNN"
 VERSION = 14
 PREFIX = "<8sII"
 PREFIX_SIZE = struct.calcsize(PREFIX)
-FLOAT_PATH = "latec_b200-f32-1"
+FLOAT_PATHS = {False: "latec_b200-f32-1", True: "latec_b200-bf16-1"}
 AUTO_CHUNK_THRESHOLD = 1 << 21
 RANK_LEVELS = {2: 8, 4: 5, 5: 4}
 EB_COARSE_FACTOR = 0.9
@@ -143,8 +146,20 @@ class GNNCodec:
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         self.strict_checkpoint = bool(strict_checkpoint)
         self.d, self.agg_level = int(d), int(agg_level)
-        self.model = gnn.GNNModel(weights, self.d, self.agg_level, self.device)
+        self._weights = weights
+        self._models = {}
         self._geoms = {}
+
+    def _model(self, reduced: bool):
+        """float32 model, or BF16 tensor-core message pass (the counterpart of
+        the reference's fp16 message pass) when ``reduced``."""
+        reduced = bool(reduced) and self.d == 64
+        m = self._models.get(reduced)
+        if m is None:
+            m = gnn.GNNModel(self._weights, self.d, self.agg_level, self.device,
+                             precision="bf16" if reduced else "f32")
+            self._models[reduced] = m
+        return m
 
     # ---------------------------------------------------------------- helpers
     def _geometry(self, shape, levels):
@@ -228,20 +243,24 @@ class GNNCodec:
                   else (list(EB_COARSE_SWEEP) if tune == "size" else [EB_COARSE_FACTOR]))
         ratios = sorted({per_step_eb_ratio(c, lv) for c in coarse})
         best = None
+        reduced = bool(fp16) and self.d == 64
+        model = self._model(reduced)
         for ratio in ratios:
-            payload = self._encode(xn, shape, lv, eb, ratio, radius)
+            payload = self._encode(model, xn, shape, lv, eb, ratio, radius)
             meta = {"shape": list(original_shape), "dtype": np_dtype.str, "error_bound": eb,
                     "levels": lv, "radius": radius, "vmin": vmin, "vmax": vmax,
                     "eb_ratio": ratio, "checkpoint_hash": self.checkpoint_hash.hex(),
-                    "chunks": list(edges), "m_tile": 1 << 16, "fp16": False, "compiled": False,
-                    "predictor": "gnn", "float_path": FLOAT_PATH, "d": self.d,
+                    "chunks": list(edges), "m_tile": 1 << 16, "fp16": reduced, "compiled": False,
+                    "predictor": "gnn", "float_path": FLOAT_PATHS[reduced], "d": self.d,
                     "agg_level": self.agg_level}
+            if int(model.tc_err.item()):
+                raise RuntimeError("a tensor-core wait ran out during the GNN forward")
             stream = write_stream(meta, payload, zstd_level)
             if best is None or len(stream) < len(best):
                 best = stream
         return best
 
-    def _encode(self, xn, shape, levels, eb, ratio, radius):
+    def _encode(self, model, xn, shape, levels, eb, ratio, radius):
         torch = _torch()
         lib = _lib.load()
         geoms = self._geometry(shape, levels)
@@ -251,7 +270,7 @@ class GNNCodec:
         E = torch.zeros((1, xn.numel(), len(shape), self.d), dtype=torch.float32, device=dev)
         records, prev, ctx, vals = [], None, None, None
         for g, seb in zip(geoms, ebs):
-            (mu, lb), E, ctx = gnn.stage_forward(self.model, E, prev, g, vals, finalize_ctx=ctx,
+            (mu, lb), E, ctx = gnn.stage_forward(model, E, prev, g, vals, finalize_ctx=ctx,
                                                  eb=seb)
             mu = mu.reshape(-1).contiguous()
             xs = xn[g.query_idx].contiguous()
@@ -292,8 +311,9 @@ class GNNCodec:
         torch = _torch()
         lib = _lib.load()
         meta, payload = read_stream(bytes(stream))
-        if meta.get("float_path") != FLOAT_PATH:
+        if meta.get("float_path") not in FLOAT_PATHS.values():
             raise ValueError("stream was not written by this codec's float path")
+        model = self._model(meta["float_path"] == FLOAT_PATHS[True])
         if self.strict_checkpoint and meta["checkpoint_hash"] != self.checkpoint_hash.hex():
             raise ValueError("checkpoint hash differs from the stream metadata")
         original_shape = tuple(int(n) for n in meta["shape"])
@@ -313,7 +333,7 @@ class GNNCodec:
         off, prev, ctx, vals = 0, None, None, None
         err = torch.zeros(1, dtype=torch.int32, device=dev)
         for g, seb in zip(geoms, ebs):
-            (mu, lb), E, ctx = gnn.stage_forward(self.model, E, prev, g, vals, finalize_ctx=ctx,
+            (mu, lb), E, ctx = gnn.stage_forward(model, E, prev, g, vals, finalize_ctx=ctx,
                                                  eb=seb)
             mu = mu.reshape(-1).contiguous()
             if off + 12 > len(payload):
@@ -350,6 +370,8 @@ class GNNCodec:
             raise ValueError("trailing data in GNN stage payload")
         if int(err.item()):
             raise ValueError("outlier count mismatch")
+        if int(model.tc_err.item()):
+            raise RuntimeError("a tensor-core wait ran out during the GNN forward")
         out = recon_all * np.float32(vmax - vmin) + np.float32(vmin)
         out = out.reshape(original_shape).cpu()
         return out.to(getattr(torch, dtype.name)) if dtype != np.float32 else out

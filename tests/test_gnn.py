@@ -91,3 +91,34 @@ def test_device_forward_is_deterministic_and_tiles():
         assert np.array_equal(m1.cpu().numpy().view(np.uint32), m3.cpu().numpy().view(np.uint32))
     assert np.array_equal(Ea.cpu().numpy(), Eb.cpu().numpy())
     assert np.array_equal(Ea.cpu().numpy(), Et.cpu().numpy())
+
+
+# BF16 operands (8-bit mantissa) in the message and finalisation MLPs: the
+# predictions move by the rounding of those operands, well under these bounds
+# (the codec's bound never depends on them: quantization enforces it).
+BF16_MU_ATOL = 1e-2
+BF16_LB_ATOL = 1e-1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["g2d", "g3d", "g2d_agg2"])
+def test_bf16_tensor_core_forward_close_to_oracle(name):
+    from latec_b200 import gnn
+    from oracle import gnn as ognn
+
+    c = CASES[name]
+    w = gnn.random_weights(c["seed"], 64, c["agg_level"])
+    model = gnn.GNNModel(w, 64, c["agg_level"], precision="bf16")
+    out, E = gnn.run_stages(model, Z[f"{name}_x"], _geoms(c, None), eb=c["eb"])
+    again, E2 = gnn.run_stages(model, Z[f"{name}_x"], _geoms(c, None), eb=c["eb"])
+    ogeoms = ognn.stage_geoms(tuple(c["shape"]), c["levels"], c["stride"], c["block"],
+                              c["max_radius"], c["agg_level"])
+    want, _ = ognn.run_stages(w, Z[f"{name}_x"], ogeoms, c["agg_level"], eb=c["eb"])
+    assert int(model.tc_err.item()) == 0
+    dmu = max(float(np.abs(m.cpu().numpy() - m64).max()) for (m, _), (m64, _) in zip(out, want))
+    dlb = max(float(np.abs(l.cpu().numpy() - l64).max()) for (_, l), (_, l64) in zip(out, want))
+    print(f"{name}: bf16 vs float64 oracle: max |d mu| {dmu:.3g}, max |d log2 b| {dlb:.3g}")
+    assert dmu < BF16_MU_ATOL and dlb < BF16_LB_ATOL
+    for (m1, l1), (m2, l2) in zip(out, again):  # deterministic
+        assert np.array_equal(m1.cpu().numpy().view(np.uint32), m2.cpu().numpy().view(np.uint32))
+    assert np.array_equal(E.cpu().numpy(), E2.cpu().numpy())

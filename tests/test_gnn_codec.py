@@ -86,23 +86,25 @@ def _codec(seed=7, agg=1):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("shape,levels,eb,tune", [((40, 36), 3, 1e-3, "fast"),
-                                                   ((24, 20, 18), 2, 1e-2, "size"),
-                                                   ((70, 9), "auto", 3e-3, "fast")])
-def test_gnn_codec_round_trip_holds_the_bound(shape, levels, eb, tune):
+@pytest.mark.parametrize("shape,levels,eb,tune,fp16", [((40, 36), 3, 1e-3, "fast", True),
+                                                        ((40, 36), 3, 1e-3, "fast", False),
+                                                        ((24, 20, 18), 2, 1e-2, "size", True),
+                                                        ((70, 9), "auto", 3e-3, "fast", True)])
+def test_gnn_codec_round_trip_holds_the_bound(shape, levels, eb, tune, fp16):
     import torch
 
     from latec_b200.gnn_codec import MAGIC, VERSION, read_stream
 
     codec = _codec()
     x = _field(shape, 3)
-    s1 = codec.compress(x, eb, levels=levels, tune=tune)
-    s2 = codec.compress(torch.from_numpy(x).cuda(), eb, levels=levels, tune=tune)
+    s1 = codec.compress(x, eb, levels=levels, tune=tune, fp16=fp16)
+    s2 = codec.compress(torch.from_numpy(x).cuda(), eb, levels=levels, tune=tune, fp16=fp16)
     assert s1 == s2  # deterministic, host or device input
     magic, version, hlen = struct.unpack_from("<8sII", s1, 0)
     assert magic == MAGIC and version == VERSION
     meta, _ = read_stream(s1)
     assert meta["shape"] == list(shape) and meta["dtype"] == np.dtype(np.float32).str
+    assert meta["fp16"] == fp16 and meta["float_path"].startswith("latec_b200-")
     out = codec.uncompress(s1)
     assert isinstance(out, torch.Tensor) and out.dtype == torch.float32
     assert tuple(out.shape) == shape
