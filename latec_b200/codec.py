@@ -130,6 +130,22 @@ def _qparams(dtype_id, c, radius, order, center, end_mode, round_output):
                             round_output=int(bool(round_output)), reserved=0)
 
 
+# numpy twin of the FitStage descriptor (fit_kernels.cu), field for field
+# numpy twin of latec_rans_stage (include/latec_b200.h), field for field
+_RANS_DTYPE = np.dtype([(n, np.uint64) for n in ("codes_off", "out_off", "enc", "cdf", "bucket",
+                                                 "scratch_off", "blob_off", "rec_off",
+                                                 "framed_hi")]
+                       + [("n", np.uint32), ("K", np.uint32), ("n_chunks", np.uint32),
+                          ("chunk0", np.uint32), ("alphabet", np.uint32), ("kexp", np.int32),
+                          ("radius", np.int32), ("mode", np.int32), ("per_point", np.int32),
+                          ("blob_words", np.uint32), ("n_out", np.uint32), ("block0", np.uint32)],
+                       align=True)
+_FIT_DTYPE = np.dtype([("counts_off", np.uint64), ("w_table", np.uint64), ("seg_off", np.uint64),
+                       ("n_segs", np.uint32), ("alphabet", np.uint32), ("kexp", np.int32),
+                       ("radius", np.int32), ("n_shapes", np.uint32), ("stage", np.uint32),
+                       ("shape_ids", np.uint32, (24,))], align=True)
+
+
 def _stats_from_device(buf, ns):
     raw = buf.stats.cpu().numpy().tobytes()
     arr = (_lib.StageStats * ns).from_buffer_copy(raw)
@@ -178,32 +194,31 @@ class _Encoder:
             fits = self._fit_reference(st)
         t_fit = time.perf_counter()
         # ---- entropy stage on the device
-        stages = (_lib.RansStage * ns)()
+        rs = np.zeros(ns, _RANS_DTYPE)
         keep = []
+        kx = np.asarray([f[0] for f in fits], np.int64)
+        rs["codes_off"] = rs["out_off"] = np.asarray(b.offsets[:ns], np.uint64)
+        rs["n"] = np.asarray(b.items[:ns], np.uint32)
+        rs["kexp"], rs["radius"], rs["mode"] = kx, int(self.radius), self.mode
+        rs["alphabet"] = (1 << (kx + 1)).astype(np.uint32)
         for t in range(ns):
             kexp, level, shape, owx, bits = fits[t]
-            d = stages[t]
-            d.codes_off = int(b.offsets[t])
-            d.out_off = int(b.offsets[t])
-            d.n = b.items[t]
-            d.kexp = kexp
-            d.radius = int(self.radius)
-            d.mode = self.mode
-            d.per_point = 0
-            d.framed_hi = bitstream.pack_frame(0, kexp, shape, level, owx, False)
-            d.alphabet = 1 << (kexp + 1)
-            if d.n:
+            rs["framed_hi"][t] = bitstream.pack_frame(0, kexp, shape, level, owx, False)
+            n = int(b.items[t])
+            if n:
                 cdf, enc, bucket, alphabet = rans_model.device_tables.get(
                     self.mode, kexp, shape, owx, level, self.device)
                 keep.append((cdf, enc, bucket))
-                d.cdf, d.enc, d.bucket = cdf.data_ptr(), enc.data_ptr(), bucket.data_ptr()
-                d.K = rans_model.lanes_K(d.n, bits) if self.mode == _lib.RANS_LANES else 0
+                rs["cdf"][t], rs["enc"][t], rs["bucket"][t] = (cdf.data_ptr(), enc.data_ptr(),
+                                                               bucket.data_ptr())
+                if self.mode == _lib.RANS_LANES:
+                    rs["K"][t] = rans_model.lanes_K(n, bits)
+        stages = rs.ctypes.data
         wsb = lib.latec_rans_encode_workspace_bytes(stages, ns)
         ws = torch.empty(max(int(wsb), 1), dtype=torch.uint8, device=self.device)
-        cap = 0
-        for t in range(ns):
-            d = stages[t]
-            cap += 16 + 4 * (1 + 65 * d.n_chunks + d.n + 2) + b.elem * b.items[t]
+        items = np.asarray(b.items[:ns], np.int64)
+        cap = int(np.sum(16 + 4 * (1 + 65 * rs["n_chunks"].astype(np.int64) + items + 2)
+                         + b.elem * items))
         cap = (cap + 15) // 16 * 16
         payload = torch.empty(cap, dtype=torch.uint8, device=self.device)
         plen = torch.zeros(1, dtype=torch.int64, device=self.device)
@@ -247,30 +262,39 @@ class _Encoder:
         fits = [(1, 0, 0, 0, 0.0)] * ns
         if not idx:
             return fits
-        fs = (_lib.FitStage * len(idx))()
-        meta, keep, off = [], [], 0
-        for j, t in enumerate(idx):
-            kexp = rans_model.kexp_from_maxq(st[t].maxq)
-            if kexp > 15:
-                raise ValueError("rANS coder window does not fit the stage frame")
-            owx = rans_model.choose_outlier_weight(int(st[t].n_out), b.items[t])
-            w, ids = rans_model.device_weights.get(kexp, owx, self.device)
+        n = len(idx)
+        items = np.asarray([b.items[t] for t in idx], np.int64)
+        maxq = np.asarray([int(st[t].maxq) for t in idx], np.int64)
+        nout = np.asarray([int(st[t].n_out) for t in idx], np.int64)
+        kexps = np.asarray([rans_model.kexp_from_maxq(q) for q in maxq.tolist()], np.int64)
+        if np.any(kexps > 15):
+            raise ValueError("rANS coder window does not fit the stage frame")
+        owxs = rans_model.choose_outlier_weights(nout, items)
+        fs = np.zeros(n, _FIT_DTYPE)
+        alph = (2 << kexps).astype(np.int64)
+        fs["counts_off"] = np.concatenate([[0], np.cumsum(alph)[:-1]])
+        fs["seg_off"] = np.asarray([int(b.seg_off[t]) for t in idx], np.uint64)
+        fs["n_segs"] = np.asarray([int(b.segs[t]) for t in idx], np.uint32)
+        fs["alphabet"], fs["kexp"], fs["radius"] = alph, kexps, int(self.radius)
+        fs["stage"] = np.asarray(idx, np.uint32)
+        keep, tabs = [], {}
+        for key in set(zip(kexps.tolist(), owxs.tolist())):
+            w, ids = rans_model.device_weights.get(key[0], key[1], self.device)
             keep.append(w)
-            f = fs[j]
-            f.counts_off, f.w_table = off, w.data_ptr()
-            f.seg_off, f.n_segs = int(b.seg_off[t]), int(b.segs[t])
-            f.alphabet, f.kexp, f.radius = 2 << kexp, kexp, int(self.radius)
-            f.n_shapes, f.stage = len(ids), t
-            for k, sid in enumerate(ids):
-                f.shape_ids[k] = sid
-            off += 2 << kexp
-            meta.append((kexp, owx))
+            row = np.zeros(24, np.uint32)
+            row[:len(ids)] = ids
+            tabs[key] = (w.data_ptr(), len(ids), row)
+        for j, key in enumerate(zip(kexps.tolist(), owxs.tolist())):
+            ptr, nsh, row = tabs[key]
+            fs["w_table"][j], fs["n_shapes"][j], fs["shape_ids"][j] = ptr, nsh, row
+        meta = list(zip(kexps.tolist(), owxs.tolist()))
+        off = int(alph.sum())
         n = len(idx)
         counts = torch.empty(off, dtype=torch.int32, device=self.device)
         costs = torch.empty(n * 24 * 64, dtype=torch.float64, device=self.device)
         out = torch.empty(n * 3, dtype=torch.float64, device=self.device)
         ws = torch.empty(n * ctypes.sizeof(_lib.FitStage) + 256, dtype=torch.uint8, device=self.device)
-        _lib.check(self.lib.latec_fit_const(fs, n, b.hist_seg.data_ptr(), b.hist_total.data_ptr(),
+        _lib.check(self.lib.latec_fit_const(fs.ctypes.data, n, b.hist_seg.data_ptr(), b.hist_total.data_ptr(),
                                             counts.data_ptr(), costs.data_ptr(), out.data_ptr(),
                                             ws.data_ptr(), ws.numel(), _lib.stream_ptr()),
                    "latec_fit_const")

@@ -142,12 +142,26 @@ def neg_log2_weights(kexp, shape, owx, n_levels=N_LEVELS, precision=PRECISION):
     return -np.log2(np.maximum(weights, 1.0 / (1 << precision))).astype(np.float32)
 
 
+_LOG_OW = np.log(np.maximum(np.asarray(OUTLIER_WEIGHTS, np.float64), 1e-12))
+
+
 def choose_outlier_weight(n_outliers, n_codes):
     """``latec/rans.py:162-169``."""
     if n_codes <= 0 or n_outliers <= 0:
         return 0
     rate = n_outliers / n_codes
-    return int(np.argmin([abs(np.log(max(w, 1e-12)) - np.log(rate)) for w in OUTLIER_WEIGHTS]))
+    return int(np.argmin(np.abs(_LOG_OW - np.log(rate))))
+
+
+def choose_outlier_weights(n_outliers, n_codes):
+    """Vector form of ``choose_outlier_weight`` (same float64 operations)."""
+    n_out = np.asarray(n_outliers, np.float64)
+    n = np.asarray(n_codes, np.float64)
+    ok = (n > 0) & (n_out > 0)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rate = np.where(ok, n_out / np.where(n > 0, n, 1.0), 1.0)
+        idx = np.argmin(np.abs(_LOG_OW[None, :] - np.log(rate)[:, None]), axis=1)
+    return np.where(ok, idx, 0).astype(np.int64)
 
 
 def kexp_from_maxq(maxq):
