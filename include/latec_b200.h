@@ -149,6 +149,14 @@ int latec_dequantize(const latec_quant_params* prm, double eb, uint64_t items, c
                      const uint16_t* codes, const void* outliers, uint32_t n_out, void* recon_out,
                      uint32_t* err, void* workspace, uint64_t workspace_bytes, void* stream);
 
+/* ---- scheduling of the decode stage kernels (no counterpart in the
+ *      reference): 0 (default) = one launch per stage; 1 = levels of >= 4 Mi
+ *      points run as one level kernel (work items per sub-stage and slab along
+ *      axis 0, claimed in an order where every item's dependencies come
+ *      first, so that slabs stay in L2); 2 = every level that qualifies.
+ *      Results are bit-identical in all modes. Process-wide. */
+int latec_set_level_mode(int32_t mode);
+
 /* ---- decode: predict + dequantize over every stage
  *      (latec/codec.py:462-510 _decompress_region). codes as produced by
  *      latec_rans_decode; outliers: device byte array holding every stage's

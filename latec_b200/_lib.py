@@ -88,6 +88,7 @@ SIGNATURES = {
     "latec_dequantize_workspace_bytes": (U64, [U64]),
     "latec_dequantize": (ctypes.c_int, [ctypes.POINTER(QuantParams), D, U64, P, P, P, U32, P, P,
                                         P, U64, P]),
+    "latec_set_level_mode": (ctypes.c_int, [I32]),
     "latec_decode_stages": (ctypes.c_int, [P, ctypes.POINTER(QuantParams), P, P, P, P, P, P, P,
                                            P, U64, P]),
     "latec_rans_build_tables": (ctypes.c_int, [P, I32, I32, P, P, P]),

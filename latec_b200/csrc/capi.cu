@@ -1,4 +1,5 @@
 // extern "C" entry points of liblatec_b200 (declared in include/latec_b200.h).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -65,6 +66,15 @@ bool make_q(const latec_quant_params* p, double eb, uint64_t points, QParams& q)
     return true;
 }
 
+// Level-kernel bounds (per level): bands per sub-stage, sub-stages per level.
+constexpr uint32_t LVL_MAX_BANDS = 1024;
+constexpr uint32_t LVL_MAX_STAGES = 2 * MAXD - 1;
+constexpr uint32_t LVL_MAX_DEPS = LVL_MAX_STAGES * LVL_MAX_BANDS * LVL_MAX_STAGES * 4;
+constexpr uint32_t LVL_CHUNK_TILES = 4;  // tiles per decode work item
+// slabs between a sub-stage and the next weight in the claim order: a whole
+// slab step separates an item from the items it depends on
+constexpr int LVL_LAG = 2;
+
 struct StageWs {
     void* staging;
     uint32_t* tile_cnt;   // per tile of the largest stage (encode) / of all stages (decode)
@@ -72,6 +82,12 @@ struct StageWs {
     uint32_t* total;
     double* partials;
     DecStage* dec;        // decode: per-stage descriptors of the all-stage tile passes
+    LvlStage* lvl_stages; // level kernels: descriptors, bands, dependencies, items, counters
+    LvlBand* lvl_bands;
+    LvlDep* lvl_deps;
+    LvlItem* lvl_items;
+    uint32_t* lvl_ctr;
+    uint64_t lvl_items_cap;
 };
 
 // Workspace carve-up: `max_items` sizes the per-stage encode scratch;
@@ -87,6 +103,12 @@ uint64_t stage_ws(uint64_t max_items, uint64_t all_tiles, int n_stages, int elem
     w.total = c.take<uint32_t>(4);
     w.partials = c.take<double>((uint64_t)MAX_BLOCKS * 5 + 5);
     w.dec = c.take<DecStage>(n_stages > 0 ? n_stages : 1);
+    w.lvl_items_cap = all_tiles + (uint64_t)LVL_MAX_STAGES * LVL_MAX_BANDS;
+    w.lvl_stages = c.take<LvlStage>(LVL_MAX_STAGES);
+    w.lvl_bands = c.take<LvlBand>((uint64_t)LVL_MAX_STAGES * LVL_MAX_BANDS);
+    w.lvl_deps = c.take<LvlDep>(LVL_MAX_DEPS);
+    w.lvl_items = c.take<LvlItem>(w.lvl_items_cap);
+    w.lvl_ctr = c.take<uint32_t>((uint64_t)LVL_MAX_STAGES * LVL_MAX_BANDS + 1);
     if (out) *out = w;
     return c.off;
 }
@@ -103,9 +125,147 @@ void plan_sizes(const latec_plan* plan, int C, uint64_t* max_items, uint64_t* al
 }
 
 
+// 0 per-stage launches (default: measured faster on B200, see the design
+// notes), 1 level kernels for levels of >= 4 Mi points, 2 every level that
+// qualifies
+std::atomic<int> g_level_mode{0};
+
+// First rank of stage d whose axis-0 coordinate is >= z (ranks follow the flat
+// grid order, so the axis-0 coordinate never decreases with the rank).
+uint64_t rank_at_z(const StageDesc& d, int32_t z) {
+    uint64_t lo = 0, hi = d.n;
+    int32_t coord[MAXD];
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) / 2;
+        stage_coords(d, (uint32_t)mid, coord);
+        if (coord[0] < z) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+int32_t z_of(const StageDesc& d, uint64_t r) {
+    int32_t coord[MAXD];
+    stage_coords(d, (uint32_t)r, coord);
+    return coord[0];
+}
+
+struct LevelBuild {
+    std::vector<LvlStage> st;
+    std::vector<LvlBand> bands;
+    std::vector<LvlDep> deps;
+    std::vector<LvlItem> items;
+};
+
+// Work items of one level [t0, t1) for the level decode kernel, or false when
+// the level does not qualify (one channel, 2+ axes, enough bands) or when some
+// dependency would not precede the item that needs it in the claim order.
+// Bands are slabs of T planes along axis 0, T >= 5 s (taps reach 3 s; one
+// slab of slack covers the rounding of band starts down to a tile).
+bool build_level(const latec_plan* plan, int t0, int t1, int C, int elem, int mode,
+                 uint64_t items_cap, LevelBuild& L, uint32_t* tiles_per_stage) {
+    if (mode == 0 || C != 1 || plan->ndim < 2 || t0 < 1 || t1 - t0 < 2 ||
+        t1 - t0 > (int)LVL_MAX_STAGES)
+        return false;
+    const int s = plan->stages[t0].s;
+    const int32_t nz = (int32_t)plan->shape[0];
+    uint64_t level_points = 0;
+    for (int t = t0; t < t1; t++) level_points += plan->stages[t].n;
+    if (mode == 1 && level_points < (4ull << 20)) return false;
+    const uint64_t plane_bytes = plan->points / (uint64_t)nz * (uint64_t)(elem + 2);
+    const int32_t unit = 2 * s;
+    // ~12 MB slabs keep a few of them in L2; mode 2 takes the thinnest legal
+    // slab so that small grids get several bands too
+    int32_t T = mode == 2 ? 5 * s : (int32_t)((12ull << 20) / (plane_bytes ? plane_bytes : 1));
+    if (T < 5 * s) T = 5 * s;
+    // at least two tiles of every sub-stage per slab, so that rounding slab
+    // starts down to a tile moves them by less than half a slab
+    for (int t = t0; t < t1; t++) {
+        const uint64_t per_plane = plan->stages[t].n / (uint64_t)nz + 1;
+        const uint64_t need = (2ull * TILE + per_plane - 1) / per_plane;
+        if ((uint64_t)T < need) T = (int32_t)std::min<uint64_t>(need, (uint64_t)nz);
+    }
+    T = (T + unit - 1) / unit * unit;
+    int32_t B = (nz + T - 1) / T;
+    if (B > (int32_t)LVL_MAX_BANDS) {
+        T = (nz + LVL_MAX_BANDS - 1) / LVL_MAX_BANDS;
+        T = (T + unit - 1) / unit * unit;
+        B = (nz + T - 1) / T;
+    }
+    if (B < 2) return false;
+    const int ns = t1 - t0;
+    std::vector<std::vector<uint64_t>> R(ns, std::vector<uint64_t>(B + 1));
+    std::vector<std::vector<int32_t>> zs(ns, std::vector<int32_t>(B)), ze(ns, std::vector<int32_t>(B));
+    int maxlag = 0;
+    for (int j = 0; j < ns; j++) {
+        const StageDesc& d = plan->stages[t0 + j];
+        maxlag = std::max(maxlag, LVL_LAG * (d.weight - 1));
+        R[j][0] = 0;
+        for (int k = 1; k < B; k++) {
+            uint64_t r = rank_at_z(d, k * T) / TILE * TILE;
+            R[j][k] = r < R[j][k - 1] ? R[j][k - 1] : r;
+        }
+        R[j][B] = d.n;
+        for (int k = 0; k < B; k++)
+            if (R[j][k] < R[j][k + 1]) {
+                zs[j][k] = z_of(d, R[j][k]);
+                ze[j][k] = z_of(d, R[j][k + 1] - 1);
+            }
+        tiles_per_stage[j] = n_tiles(d.n);
+    }
+    // claim order: step b runs band b - lag of every sub-stage, lower weights first
+    std::vector<int64_t> first(ns * B, -1), last(ns * B, -1), cnt(ns * B, 0);
+    for (int b = 0; b < B + maxlag; b++)
+        for (int j = 0; j < ns; j++) {
+            const int k = b - LVL_LAG * (plan->stages[t0 + j].weight - 1);
+            if (k < 0 || k >= B || R[j][k] >= R[j][k + 1]) continue;
+            const uint32_t ta = (uint32_t)(R[j][k] / TILE);
+            const uint32_t tb = k + 1 == B ? tiles_per_stage[j] : (uint32_t)(R[j][k + 1] / TILE);
+            for (uint32_t a = ta; a < tb; a += LVL_CHUNK_TILES) {
+                if (first[j * B + k] < 0) first[j * B + k] = (int64_t)L.items.size();
+                last[j * B + k] = (int64_t)L.items.size();
+                cnt[j * B + k]++;
+                L.items.push_back(LvlItem{(uint32_t)(j * B + k), a,
+                                          std::min(tb, a + LVL_CHUNK_TILES), 0u});
+            }
+        }
+    if (L.items.size() > items_cap) return false;
+    L.bands.resize((size_t)ns * B);
+    for (int j = 0; j < ns; j++) {
+        const StageDesc& d = plan->stages[t0 + j];
+        for (int k = 0; k < B; k++) {
+            LvlBand& bd = L.bands[(size_t)j * B + k];
+            bd.stage = (uint32_t)j;
+            bd.counter = (uint32_t)(j * B + k);
+            bd.dep_off = (uint32_t)L.deps.size();
+            bd.dep_cnt = 0;
+            if (R[j][k] >= R[j][k + 1]) continue;
+            const int32_t lo = zs[j][k] - 3 * s, hi = ze[j][k] + 3 * s;
+            for (int jp = 0; jp < ns; jp++) {
+                if (plan->stages[t0 + jp].weight >= d.weight) continue;
+                for (int kp = 0; kp < B; kp++) {
+                    if (R[jp][kp] >= R[jp][kp + 1]) continue;
+                    if (ze[jp][kp] < lo || zs[jp][kp] > hi) continue;
+                    if (last[jp * B + kp] >= first[j * B + k]) return false;
+                    L.deps.push_back(LvlDep{(uint32_t)(jp * B + kp), (uint32_t)cnt[jp * B + kp]});
+                    bd.dep_cnt++;
+                    if (L.deps.size() > LVL_MAX_DEPS) return false;
+                }
+            }
+        }
+    }
+    return true;
+}
+
 }  // namespace
 
 extern "C" {
+
+int latec_set_level_mode(int32_t mode) {
+    if (mode < 0 || mode > 2) return LATEC_ERR_ARG;
+    g_level_mode.store(mode);
+    return LATEC_OK;
+}
 
 const char* latec_version(void) { return "latec_b200 0.1 (sm_100a)"; }
 
@@ -319,16 +479,59 @@ int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
     int rc = launch_count_zeros_all(w.dec, ns, tile0, codes, w.tile_cnt, st);
     if (!rc) rc = launch_tile_offsets_all(w.dec, ns, w.tile_cnt, w.tile_off, err, st);
     if (rc) return rc;
-    for (int t = 0; t < ns; t++) {
-        const StageDesc& d = plan->stages[t];
-        if (!ds[t].items) continue;
-        QParams q;
-        if (!make_q(prm, stage_eb[t], plan->points, q)) return LATEC_ERR_ARG;
-        rc = launch_interp_dequant(d, q, prm->dtype, t == 0, codes + ds[t].codes_off,
-                                   outliers ? (const uint8_t*)outliers + out_off[t] : nullptr,
-                                   w.tile_cnt + ds[t].tile0, w.tile_off + ds[t].tile0, n_out[t],
-                                   recon, err, st);
-        if (rc) return rc;
+    const int mode = g_level_mode.load();
+    int t = 0;
+    while (t < ns) {
+        // a level: consecutive stages of one stride (the anchors stand alone)
+        int t1 = t + 1;
+        if (t > 0)
+            while (t1 < ns && plan->stages[t1].s == plan->stages[t].s) t1++;
+        LevelBuild L;
+        uint32_t tps[LVL_MAX_STAGES];
+        if (build_level(plan, t, t1, C, elem_of(prm->dtype), mode, w.lvl_items_cap, L, tps)) {
+            const int nl = t1 - t;
+            L.st.resize(nl);
+            for (int j = 0; j < nl; j++) {
+                LvlStage& ls = L.st[j];
+                memset(&ls, 0, sizeof(ls));
+                ls.d = plan->stages[t + j];
+                if (!make_q(prm, stage_eb[t + j], plan->points, ls.q)) return LATEC_ERR_ARG;
+                ls.codes = codes + ds[t + j].codes_off;
+                ls.outliers = outliers ? (const uint8_t*)outliers + out_off[t + j] : nullptr;
+                ls.tile_cnt = w.tile_cnt + ds[t + j].tile0;
+                ls.tile_off = w.tile_off + ds[t + j].tile0;
+                ls.n_out = n_out[t + j];
+            }
+            if (cudaMemcpyAsync(w.lvl_stages, L.st.data(), sizeof(LvlStage) * nl,
+                                cudaMemcpyHostToDevice, st) != cudaSuccess ||
+                cudaMemcpyAsync(w.lvl_bands, L.bands.data(), sizeof(LvlBand) * L.bands.size(),
+                                cudaMemcpyHostToDevice, st) != cudaSuccess ||
+                (L.deps.size() &&
+                 cudaMemcpyAsync(w.lvl_deps, L.deps.data(), sizeof(LvlDep) * L.deps.size(),
+                                 cudaMemcpyHostToDevice, st) != cudaSuccess) ||
+                cudaMemcpyAsync(w.lvl_items, L.items.data(), sizeof(LvlItem) * L.items.size(),
+                                cudaMemcpyHostToDevice, st) != cudaSuccess ||
+                cudaMemsetAsync(w.lvl_ctr, 0, sizeof(uint32_t) * (L.bands.size() + 1), st) !=
+                    cudaSuccess)
+                return LATEC_ERR_CUDA;
+            rc = launch_level_dequant(prm->dtype, plan->ndim, prm->order ? 1 : 0, w.lvl_stages,
+                                      w.lvl_bands, w.lvl_deps, w.lvl_items,
+                                      (uint32_t)L.items.size(), w.lvl_ctr, recon, err, st);
+            if (rc) return rc;
+            t = t1;
+            continue;
+        }
+        for (; t < t1; t++) {
+            const StageDesc& d = plan->stages[t];
+            if (!ds[t].items) continue;
+            QParams q;
+            if (!make_q(prm, stage_eb[t], plan->points, q)) return LATEC_ERR_ARG;
+            rc = launch_interp_dequant(d, q, prm->dtype, t == 0, codes + ds[t].codes_off,
+                                       outliers ? (const uint8_t*)outliers + out_off[t] : nullptr,
+                                       w.tile_cnt + ds[t].tile0, w.tile_off + ds[t].tile0,
+                                       n_out[t], recon, err, st);
+            if (rc) return rc;
+        }
     }
     return LATEC_OK;
 }

@@ -131,16 +131,24 @@ struct AxisTaps {
     uint32_t ok;  // bit 0: +s valid, bit 1: -3s valid, bit 2: +3s valid
 };
 
-template <typename T, int CUBIC>
+// Tap load: the read-only cache path, or (COH) L2 only, for taps that other
+// CTAs of the same launch may have written (the level kernels).
+template <typename T, int COH>
+__device__ __forceinline__ T ldtap(const T* p) {
+    if (COH) return __ldcg(p);
+    return __ldg(p);
+}
+
+template <typename T, int CUBIC, int COH = 0>
 __device__ __forceinline__ void load_axis(const T* __restrict__ rc, int64_t flat, int c, int n,
                                           int64_t gs, int s, AxisTaps<T>& t) {
     const int64_t o1 = (int64_t)s * gs;
     const bool vp1 = c + s < n, vm3 = c - 3 * s >= 0, vp3 = c + 3 * s < n;
     const T* b = rc + flat;
-    t.m1 = __ldg(b - o1);
-    t.p1 = __ldg(b + (vp1 ? o1 : -o1));
-    t.m3 = __ldg(b + (vm3 ? -3 * o1 : -o1));
-    t.p3 = CUBIC ? __ldg(b + (vp3 ? 3 * o1 : -o1)) : (T)0;
+    t.m1 = ldtap<T, COH>(b - o1);
+    t.p1 = ldtap<T, COH>(b + (vp1 ? o1 : -o1));
+    t.m3 = ldtap<T, COH>(b + (vm3 ? -3 * o1 : -o1));
+    t.p3 = CUBIC ? ldtap<T, COH>(b + (vp3 ? 3 * o1 : -o1)) : (T)0;
     t.ok = (vp1 ? 1u : 0u) | (vm3 ? 2u : 0u) | (vp3 ? 4u : 0u);
 }
 
@@ -188,7 +196,7 @@ struct PointTaps {
     uint32_t odd;  // center 0, KIND 1: mask of the odd axes
 };
 
-template <typename T, int ND, int KIND, int CUBIC>
+template <typename T, int ND, int KIND, int CUBIC, int COH = 0>
 __device__ __forceinline__ void gather_point(const StageDesc& d, const QParams& q,
                                              const T* __restrict__ rc, int64_t flat,
                                              const int32_t* coord, PointTaps<T, ND, KIND>& pt) {
@@ -205,7 +213,7 @@ __device__ __forceinline__ void gather_point(const StageDesc& d, const QParams& 
                 gs = d.gstride[j];
             }
         }
-        load_axis<T, CUBIC>(rc, flat, ca, na, gs, d.s, pt.ax[0]);
+        load_axis<T, CUBIC, COH>(rc, flat, ca, na, gs, d.s, pt.ax[0]);
         return;
     }
     if (q.center == 0) {
@@ -213,7 +221,7 @@ __device__ __forceinline__ void gather_point(const StageDesc& d, const QParams& 
         for (int j = 0; j < NDV; j++) {
             if ((ND > 0 || j < d.ndim) && (coord[j] & d.s)) {
                 pt.odd |= 1u << j;
-                load_axis<T, CUBIC>(rc, flat, coord[j], d.shape[j], d.gstride[j], d.s,
+                load_axis<T, CUBIC, COH>(rc, flat, coord[j], d.shape[j], d.gstride[j], d.s,
                                     pt.ax[KIND ? j : 0]);
             }
         }
@@ -231,7 +239,7 @@ __device__ __forceinline__ void gather_point(const StageDesc& d, const QParams& 
             found = true;
         }
     }
-    load_axis<T, CUBIC>(rc, flat, ca, na, gs, d.s, pt.ax[0]);
+    load_axis<T, CUBIC, COH>(rc, flat, ca, na, gs, d.s, pt.ax[0]);
 }
 
 template <typename T, int ND, int KIND, int CUBIC>
@@ -473,7 +481,7 @@ __device__ __forceinline__ double locate_predict(const StageDesc& d, const QPara
 }
 
 // Locate one stage point and load its taps (prediction deferred to combine).
-template <typename T, int ND, int KIND, int CUBIC>
+template <typename T, int ND, int KIND, int CUBIC, int COH = 0>
 __device__ __forceinline__ void locate_gather(const StageDesc& d, const QParams& q,
                                               const int is_anchor, uint64_t i,
                                               const T* __restrict__ recon, int64_t& flat,
@@ -487,7 +495,8 @@ __device__ __forceinline__ void locate_gather(const StageDesc& d, const QParams&
     int32_t coord[ND > 0 ? ND : MAXD];
     flat = stage_coords_t<ND, KIND>(d, rank, coord);
     if (!is_anchor)
-        gather_point<T, ND, KIND, CUBIC>(d, q, recon + (uint64_t)c * q.points, flat, coord, pt);
+        gather_point<T, ND, KIND, CUBIC, COH>(d, q, recon + (uint64_t)c * q.points, flat, coord,
+                                              pt);
 }
 
 template <typename T>
@@ -903,6 +912,154 @@ __global__ void __launch_bounds__(THREADS)
     }
 }
 
+// ---------------------------------------------------------------- level decode
+// One 2048-code tile of a stage, as k_interp_dequant, with taps read through
+// L2 (they may have been written by other CTAs of the same launch).
+template <typename T, int ND, int KIND, int CUBIC, int COH>
+__device__ __forceinline__ void dequant_tile_l2(const StageDesc& d, const QParams& q,
+                                                uint32_t tile, const uint16_t* __restrict__ codes,
+                                                const uint8_t* __restrict__ outliers,
+                                                const uint32_t* __restrict__ tile_cnt,
+                                                const uint32_t* __restrict__ tile_off,
+                                                uint32_t n_out, T* __restrict__ recon,
+                                                uint32_t* __restrict__ err) {
+    const uint64_t items = (uint64_t)q.channels * d.n;
+    const uint64_t tile_base = (uint64_t)tile * TILE;
+    const bool any = tile_cnt[tile] != 0;  // uniform across the CTA
+    uint32_t run = any ? tile_off[tile] : 0u;
+    for (int k = 0; k < TILE / THREADS; k += 2) {
+        const uint64_t i0 = tile_base + (uint64_t)k * THREADS + threadIdx.x;
+        const uint64_t i1 = i0 + THREADS;
+        const bool v0 = i0 < items, v1 = i1 < items;
+        const uint32_t q0 = v0 ? codes[i0] : 1u, q1 = v1 ? codes[i1] : 1u;
+        int64_t f0 = 0, f1 = 0;
+        uint32_t c0 = 0, c1 = 0;
+        PointTaps<T, ND, KIND> t0, t1;
+        if (v0 && q0) locate_gather<T, ND, KIND, CUBIC, COH>(d, q, 0, i0, recon, f0, c0, t0);
+        if (v1 && q1) locate_gather<T, ND, KIND, CUBIC, COH>(d, q, 0, i1, recon, f1, c1, t1);
+        uint32_t p0 = 0, p1 = 0;
+        if (any) {  // outlier positions in item order (k, then thread)
+            uint32_t tot;
+            p0 = run + block_excl_flag(v0 && q0 == 0, tot);
+            run += tot;
+            p1 = run + block_excl_flag(v1 && q1 == 0, tot);
+            run += tot;
+        }
+        if (v0) {
+            T v;
+            if (q0) {
+                v = dequant_value<T>(q, combine_point<T, ND, KIND, CUBIC>(q, t0), q0);
+            } else {
+                int32_t coord[ND > 0 ? ND : MAXD];
+                uint32_t c = 0, rank = (uint32_t)i0;
+                if (q.channels > 1) {
+                    c = (uint32_t)(i0 / d.n);
+                    rank = (uint32_t)(i0 - (uint64_t)c * d.n);
+                }
+                f0 = stage_coords_t<ND, KIND>(d, rank, coord);
+                c0 = c;
+                if (p0 < n_out) {
+                    v = load_unaligned<T>(outliers + (uint64_t)p0 * sizeof(T));
+                } else {
+                    v = (T)0;
+                    atomicOr(err, 1u);
+                }
+            }
+            recon[(uint64_t)c0 * q.points + f0] = v;
+        }
+        if (v1) {
+            T v;
+            if (q1) {
+                v = dequant_value<T>(q, combine_point<T, ND, KIND, CUBIC>(q, t1), q1);
+            } else {
+                int32_t coord[ND > 0 ? ND : MAXD];
+                uint32_t c = 0, rank = (uint32_t)i1;
+                if (q.channels > 1) {
+                    c = (uint32_t)(i1 / d.n);
+                    rank = (uint32_t)(i1 - (uint64_t)c * d.n);
+                }
+                f1 = stage_coords_t<ND, KIND>(d, rank, coord);
+                c1 = c;
+                if (p1 < n_out) {
+                    v = load_unaligned<T>(outliers + (uint64_t)p1 * sizeof(T));
+                } else {
+                    v = (T)0;
+                    atomicOr(err, 1u);
+                }
+            }
+            recon[(uint64_t)c1 * q.points + f1] = v;
+        }
+    }
+}
+
+// Bounded wait of thread 0 for an item's dependencies; every later wait is
+// skipped once one has run out (the error bit is set, results are invalid).
+__device__ __forceinline__ void level_wait(const LvlBand& band, const LvlDep* __restrict__ deps,
+                                           uint32_t* __restrict__ ctr, uint32_t* __restrict__ err) {
+    for (uint32_t e = 0; e < band.dep_cnt; e++) {
+        const LvlDep dp = deps[band.dep_off + e];
+        const volatile uint32_t* c = ctr + 1 + dp.counter;
+        uint32_t spins = 0;
+        while (*c < dp.need) {
+            if ((*(volatile uint32_t*)err & ERR_LEVEL_WAIT) || ++spins > LEVEL_WAIT_LIMIT) {
+                atomicOr(err, ERR_LEVEL_WAIT);
+                return;
+            }
+            __nanosleep(100);
+        }
+    }
+    __threadfence();
+}
+
+template <typename T, int ND, int CUBIC>
+__global__ void __launch_bounds__(THREADS, 3)
+    k_level_dequant(const LvlStage* __restrict__ stages, const LvlBand* __restrict__ bands,
+                    const LvlDep* __restrict__ deps, const LvlItem* __restrict__ items,
+                    uint32_t n_items, uint32_t* __restrict__ ctr, T* __restrict__ recon,
+                    uint32_t* __restrict__ err) {
+    __shared__ StageDesc sd;
+    __shared__ QParams sq;
+    __shared__ uint32_t s_item;
+    uint32_t cur = 0xffffffffu;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(&ctr[0], 1u);
+        __syncthreads();
+        const uint32_t it = s_item;
+        if (it >= n_items) break;
+        const LvlItem item = items[it];
+        const LvlBand band = bands[item.band];
+        if (threadIdx.x == 0) level_wait(band, deps, ctr, err);
+        if (band.stage != cur) {  // uniform: every thread saw the same item
+            const uint32_t* src = (const uint32_t*)&stages[band.stage].d;
+            uint32_t* dst = (uint32_t*)&sd;
+            for (uint32_t w = threadIdx.x; w < sizeof(StageDesc) / 4; w += THREADS) dst[w] = src[w];
+            if (threadIdx.x == 0) sq = stages[band.stage].q;
+            cur = band.stage;
+        }
+        __syncthreads();
+        const LvlStage& ls = stages[band.stage];
+        for (uint32_t tile = item.tile0; tile < item.tile1; tile++) {
+            // weight-1 sub-stages read only coarser levels (finished by earlier
+            // launches): their taps may go through L1; the fused sub-stages
+            // read this level's other sub-stages and must read through L2
+            if (sd.kind)
+                dequant_tile_l2<T, ND, 1, CUBIC, 1>(sd, sq, tile, ls.codes, ls.outliers,
+                                                    ls.tile_cnt, ls.tile_off, ls.n_out, recon, err);
+            else if (sd.weight > 1)
+                dequant_tile_l2<T, ND, 0, CUBIC, 1>(sd, sq, tile, ls.codes, ls.outliers,
+                                                    ls.tile_cnt, ls.tile_off, ls.n_out, recon, err);
+            else
+                dequant_tile_l2<T, ND, 0, CUBIC, 0>(sd, sq, tile, ls.codes, ls.outliers,
+                                                    ls.tile_cnt, ls.tile_off, ls.n_out, recon, err);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(&ctr[1 + band.counter], 1u);
+        }
+    }
+}
+
 // ---------------------------------------------------------------- launchers
 static int last_err() {
     count_launches(1);
@@ -1032,6 +1189,33 @@ int launch_dequant_flat(const QParams& q, int dtype, uint64_t items, const void*
         k_dequant_flat<float><<<n_tiles(items), THREADS, 0, st>>>(
             q, items, (const float*)pred, codes, (const uint8_t*)outliers, tile_cnt, tile_off,
             n_out, (float*)recon, err);
+    return last_err();
+}
+
+int launch_level_dequant(int dtype, int nd, int cubic, const LvlStage* stages,
+                         const LvlBand* bands, const LvlDep* deps, const LvlItem* items,
+                         uint32_t n_items, uint32_t* ctr, void* recon, uint32_t* err,
+                         cudaStream_t st) {
+    if (!n_items) return LATEC_OK;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint32_t want = (uint32_t)sms * 3;  // resident CTAs (launch bounds)
+    const uint32_t grid = n_items < want ? n_items : want;
+#define LVL_DQ(TT, NDC, CU)                                                                     \
+    k_level_dequant<TT, NDC, CU><<<grid, THREADS, 0, st>>>(stages, bands, deps, items, n_items, \
+                                                           ctr, (TT*)recon, err)
+#define LVL_DQ_ND(TT)                                                                           \
+    do {                                                                                        \
+        if (nd == 2) { if (cubic) LVL_DQ(TT, 2, 1); else LVL_DQ(TT, 2, 0); }                    \
+        else if (nd == 3) { if (cubic) LVL_DQ(TT, 3, 1); else LVL_DQ(TT, 3, 0); }               \
+        else if (nd == 4) { if (cubic) LVL_DQ(TT, 4, 1); else LVL_DQ(TT, 4, 0); }               \
+        else { if (cubic) LVL_DQ(TT, 0, 1); else LVL_DQ(TT, 0, 0); }                            \
+    } while (0)
+    if (dtype == LATEC_F64) LVL_DQ_ND(double);
+    else LVL_DQ_ND(float);
+#undef LVL_DQ_ND
+#undef LVL_DQ
     return last_err();
 }
 

@@ -48,6 +48,37 @@ struct DecStage {
     uint32_t tile0;      // first global tile of the stage
     uint32_t n_out;      // outliers stored for the stage
 };
+// Level kernels: all sub-stages of one level of the schedule in one launch,
+// as work items (sub-stage, band along axis 0, tile range) claimed in a fixed
+// order; an item waits only for lower-weight items that precede it.
+struct LvlStage {
+    StageDesc d;
+    QParams q;
+    const uint16_t* codes;     // the stage's codes
+    const uint8_t* outliers;   // the stage's outliers (decode)
+    const uint32_t* tile_cnt;  // the stage's outlier counts / offsets per tile
+    const uint32_t* tile_off;
+    uint32_t n_out;
+    uint32_t pad;
+};
+struct LvlBand {
+    uint32_t stage;    // index into the level's LvlStage array
+    uint32_t counter;  // finished items of this band
+    uint32_t dep_off;  // dependencies: LvlDep[dep_off, dep_off + dep_cnt)
+    uint32_t dep_cnt;
+};
+struct LvlDep {
+    uint32_t counter;
+    uint32_t need;     // items of that band
+};
+struct LvlItem {
+    uint32_t band;
+    uint32_t tile0, tile1;  // stage-local tiles
+    uint32_t pad;
+};
+constexpr uint32_t LEVEL_WAIT_LIMIT = 1u << 22;  // polls of one dependency (x ~100 ns)
+constexpr uint32_t ERR_LEVEL_WAIT = 0x200u;
+
 // CTAs of the encode kernels for a stage of `items` points (partials rows).
 uint32_t encode_blocks(uint64_t items);
 inline uint32_t n_blocks(uint64_t items) { return encode_blocks(items); }
@@ -77,6 +108,10 @@ int launch_dequant_flat(const QParams& q, int dtype, uint64_t items, const void*
                         const uint16_t* codes, const void* outliers, const uint32_t* tile_cnt,
                         const uint32_t* tile_off, uint32_t n_out, void* recon, uint32_t* err,
                         cudaStream_t st);
+int launch_level_dequant(int dtype, int nd, int cubic, const LvlStage* stages,
+                         const LvlBand* bands, const LvlDep* deps, const LvlItem* items,
+                         uint32_t n_items, uint32_t* ctr, void* recon, uint32_t* err,
+                         cudaStream_t st);
 int launch_quantize_flat(const QParams& q, int dtype, uint64_t items, const void* x,
                          const void* pred, uint16_t* codes, void* staging, uint32_t* tile_cnt,
                          uint32_t* tile_off, uint32_t* hist_total, uint32_t* hist_seg,
