@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(LT)
 __global__ void __launch_bounds__(LT)
     k_rows_two(const float* __restrict__ E, int64_t N, int K, int d, int ds,
                const float* __restrict__ table, const latec_gnn_geom g, int b,
-               const int32_t* __restrict__ pairs, int64_t np, float* __restrict__ X) {
+               const int32_t* __restrict__ pairs, int64_t np, float* __restrict__ X, int ldx) {
     const int64_t w = ((int64_t)blockIdx.x * LT + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= np * K) return;
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(LT)
     const float* sn = table + (int64_t)g.sidx_n[l * K + k] * ds;
     const float* sp = table + (int64_t)g.sidx_p[l * K + k] * ds;
     const int de = d + ds, width = 2 * de + 2;
-    float* row = X + w * width;
+    float* row = X + w * ldx;
     for (int f = lane; f < width; f += 32) {
         float v;
         if (f < d) v = en[f];
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(LT)
 __global__ void __launch_bounds__(LT)
     k_rows_one(const float* __restrict__ E, int64_t N, int K, int d, int ds,
                const float* __restrict__ table, const latec_gnn_geom g, int b,
-               const int32_t* __restrict__ pairs, int64_t np, float* __restrict__ X) {
+               const int32_t* __restrict__ pairs, int64_t np, float* __restrict__ X, int ldx) {
     const int64_t w = ((int64_t)blockIdx.x * LT + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= np * K) return;
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(LT)
     const float* e = E + (((int64_t)b * N + nb) * K + k) * d;
     const float* s = table + (int64_t)(pos ? g.sidx_p[l * K + k] : g.sidx_n[l * K + k]) * ds;
     const int de = d + ds, width = de + 2;
-    float* row = X + w * width;
+    float* row = X + w * ldx;
     for (int f = lane; f < width; f += 32) {
         float v;
         if (f < d) v = e[f];
@@ -388,7 +388,7 @@ uint64_t latec_gnn_workspace_bytes(int32_t d, int32_t B, int32_t M, int32_t L, i
     const int64_t mt = M < m_tile ? M : m_tile;
     const int64_t h = 2 * d, de = d + (d / 4 > 1 ? d / 4 : 1);
     const int64_t rows = (int64_t)B * mt * L * K;  // live rows of one tile, at most
-    const int64_t embed = rows * (2 * de + 2 + h + d + d + 1 + d) + (int64_t)mt * K * L;
+    const int64_t embed = rows * ((2 * de + 2 + 3) / 4 * 4 + h + d + d + 1 + d) + (int64_t)mt * K * L;
     const int64_t bm = (int64_t)B * M, bmk = bm * K;
     const int64_t head = bmk * (d + 1 + d) + bm * (d + d + 1 + h + 2);
     const int64_t fin = bm * (h + d) + bmk * (2 * d + h + d);
@@ -417,6 +417,7 @@ int latec_gnn_embed(const latec_gnn_model* model, int32_t B, int64_t N, const fl
     const Packed pk = packed_of(model->packed_bf16, P);
     const float scale = 1.0f / sqrtf((float)d);
     const int64_t w2 = 2 * P.de + 2, w1 = P.de + 2;
+    const int64_t l2 = (w2 + 3) / 4 * 4, l1 = (w1 + 3) / 4 * 4;  // 16-byte row strides
     int rc = LATEC_OK;
     for (int t = 0; t < g.n_tiles && !rc; t++) {
         const int m0 = t * g.m_tile;
@@ -426,7 +427,7 @@ int latec_gnn_embed(const latec_gnn_model* model, int32_t B, int64_t N, const fl
         if (n2 < 0 || n1 < 0 || n_live > (int64_t)mt * L) return LATEC_ERR_ARG;
         const int64_t rows = (int64_t)B * n_live * K;
         float* X = (float*)workspace;
-        float* H = X + rows * w2;
+        float* H = X + rows * l2;
         float* MS = H + rows * P.h;
         float* S1 = MS + rows * d;
         float* KEY = S1 + rows * d;
@@ -436,18 +437,20 @@ int latec_gnn_embed(const latec_gnn_model* model, int32_t B, int64_t N, const fl
             float* msb = MS + (int64_t)b * n_live * K * d;
             if (n2) {
                 k_rows_two<<<blocks_for(n2 * K * 32), LT, 0, st>>>(E, N, K, d, P.ds, P.table, g, b,
-                                                                  g.two + g.two_off[t], n2, X);
+                                                                  g.two + g.two_off[t], n2, X,
+                                                                  (int)l2);
                 rc = launched(1);
                 if (!rc)
-                    rc = mlp2(model, X, (int)w2, n2 * K, (int)w2, P.bi0w, P.bi0b, pk.bi1, pk.bi_k1p,
+                    rc = mlp2(model, X, (int)l2, n2 * K, (int)w2, P.bi0w, P.bi0b, pk.bi1, pk.bi_k1p,
                               P.bi2w, P.bi2b, pk.bi2, P.h, d, H, msb, d, st);
             }
             if (n1 && !rc) {
                 k_rows_one<<<blocks_for(n1 * K * 32), LT, 0, st>>>(E, N, K, d, P.ds, P.table, g, b,
-                                                                  g.one + g.one_off[t], n1, X);
+                                                                  g.one + g.one_off[t], n1, X,
+                                                                  (int)l1);
                 rc = launched(1);
                 if (!rc)
-                    rc = mlp2(model, X, (int)w1, n1 * K, (int)w1, P.dir0w, P.dir0b, pk.dir1,
+                    rc = mlp2(model, X, (int)l1, n1 * K, (int)w1, P.dir0w, P.dir0b, pk.dir1,
                               pk.dir_k1p, P.dir2w, P.dir2b, pk.dir2, P.h, d, H, msb + n2 * K * d, d,
                               st);
             }

@@ -2,7 +2,7 @@
 // cores: Y = W2 * gelu(W1 * X + b1) + b2 for rows of X, with BF16 operands in
 // shared memory and FP32 accumulators in tensor memory (tcgen05).
 //
-// One persistent CTA of 4 warps per SM. W1 (N1 x K1) and W2 (N2 x N1) are
+// One persistent CTA of 8 warps per SM. W1 (N1 x K1) and W2 (N2 x N1) are
 // staged once per CTA in shared memory; then for every 128-row tile:
 //   1. the 128 rows of X (float32, any row stride) are rounded to BF16 into
 //      shared memory (zero-padded to K1p, a multiple of 16);
@@ -28,7 +28,7 @@
 namespace latec {
 namespace {
 
-constexpr int TC_THREADS = 128;
+constexpr int TC_THREADS = 256;
 constexpr int TC_M = 128;
 constexpr uint32_t TC_WAIT_LIMIT = 1u << 24;
 
@@ -101,7 +101,18 @@ __device__ __forceinline__ float gelu_tc(float x) {
     return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f));
 }
 
-// N1 = hidden width (128), N2 = output width (64); K1P = padded input width.
+// 16-byte shared store of 8 BF16 values.
+__device__ __forceinline__ void st_bf16x8(__nv_bfloat16* dst, const float* v) {
+    __nv_bfloat162 p[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) p[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+    *(int4*)dst = *(const int4*)p;
+}
+
+// N1 = hidden width (128), N2 = output width (64). 256 threads: thread t
+// converts K chunks of row t % 128 (rows of a warp are 16 bytes apart in the
+// canonical layout: conflict-free stores); warp w reads TMEM lanes
+// 32 (w % 4) .. + 31, warpgroup w / 4 half of the columns.
 template <int N1, int N2>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_mlp2_tc(const float* __restrict__ X, int ldx, int rows, int k1, int k1p,
@@ -113,12 +124,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     __shared__ uint32_t tmem_base;
     __nv_bfloat16* sw1 = (__nv_bfloat16*)smem_raw;             // N1 x k1p
     __nv_bfloat16* sw2 = sw1 + (size_t)N1 * k1p;                // N2 x N1
-    __nv_bfloat16* sa = sw2 + (size_t)N2 * N1;                  // 128 x k1p
+    __nv_bfloat16* sa = sw2 + (size_t)N2 * N1;                  // 128 x k1p (then Y staging)
     __nv_bfloat16* sh = sa + (size_t)TC_M * k1p;                // 128 x N1
+    float* sy = (float*)sa;                                     // 128 x (N2 + 1) float32
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int quarter = warp & 3, half = warp >> 2;
 
-    // stage the packed weights (16-byte copies)
-    {
+    {  // stage the packed weights (16-byte copies)
         const int4* s1 = (const int4*)w1p;
         int4* d1 = (int4*)sw1;
         for (int i = tid; i < N1 * k1p / 8; i += TC_THREADS) d1[i] = s1[i];
@@ -144,19 +156,51 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const uint32_t mb = smem_u32(&mbar);
     uint32_t phase = 0;
     bool ok = true;
-    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-    const int row_in_tile = warp * 32 + lane;  // TMEM lane of this thread
+    const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+    const int trow = quarter * 32 + lane;  // TMEM lane (tile row) of this thread
     const int n_tiles = (rows + TC_M - 1) / TC_M;
+    const int chunks = k1p / 8;
+    // rows start on 16-byte boundaries and ldx >= round_up(k1, 4): a float4
+    // starting below k1 stays inside its row
+    const bool vec4 = (ldx % 4) == 0 && ((uintptr_t)X % 16) == 0 && ldx >= ((k1 + 3) & ~3);
 
     for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
         const int r0 = t * TC_M;
-        // 1. X rows -> BF16 A operand (each warp fills 32 rows, lanes along k)
-        for (int rr = 0; rr < 32; rr++) {
-            const int r = warp * 32 + rr;
+        // 1. rows of X -> BF16 A operand: thread handles row tid % 128,
+        //    K chunks tid / 128, + 2, + 4, ...; four chunks' loads in flight
+        {
+            const int r = tid & (TC_M - 1);
             const int gr = r0 + r;
-            for (int k = lane; k < k1p; k += 32) {
-                const float v = (gr < rows && k < k1) ? X[(int64_t)gr * ldx + k] : 0.0f;
-                sa[canon(r, k, TC_M)] = __float2bfloat16_rn(v);
+            const float* xr = X + (int64_t)gr * ldx;
+            for (int c0 = tid >> 7; c0 < chunks; c0 += 8) {
+                float v[4][8];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int c = c0 + 2 * u;
+                    if (vec4) {  // 16-byte rows: two float4 per chunk, masked past k1
+#pragma unroll
+                        for (int h2 = 0; h2 < 2; h2++) {
+                            const int k = c * 8 + 4 * h2;
+                            float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+                            if (c < chunks && gr < rows && k < k1) f = *(const float4*)(xr + k);
+                            v[u][4 * h2 + 0] = k + 0 < k1 ? f.x : 0.0f;
+                            v[u][4 * h2 + 1] = k + 1 < k1 ? f.y : 0.0f;
+                            v[u][4 * h2 + 2] = k + 2 < k1 ? f.z : 0.0f;
+                            v[u][4 * h2 + 3] = k + 3 < k1 ? f.w : 0.0f;
+                        }
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < 8; e++) {
+                            const int k = c * 8 + e;
+                            v[u][e] = (c < chunks && gr < rows && k < k1) ? xr[k] : 0.0f;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int c = c0 + 2 * u;
+                    if (c < chunks) st_bf16x8(sa + canon(r, c * 8, TC_M), v[u]);
+                }
             }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -164,10 +208,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // 2. layer 1
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sw1);
+            const uint32_t a0 = smem_u32(sa), bb = smem_u32(sw1);
             for (int kk = 0; kk < k1p / 16; kk++) {
                 const uint64_t ad = smem_desc(a0 + kk * 2 * TC_M * 16, TC_M * 16, 128);
-                const uint64_t bd = smem_desc(b0 + kk * 2 * N1 * 16, N1 * 16, 128);
+                const uint64_t bd = smem_desc(bb + kk * 2 * N1 * 16, N1 * 16, 128);
                 mma_bf16(tmem, ad, bd, idesc_bf16(TC_M, N1), kk > 0);
             }
             mma_commit(mb);
@@ -179,14 +223,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
         phase ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;");
-        // 3. epilogue 1: bias + GELU -> BF16 hidden (A operand of layer 2)
-        for (int c = 0; c < N1; c += 16) {
+        // 3. epilogue 1: bias + GELU -> BF16 hidden; each warpgroup half the columns
+        for (int c = half * (N1 / 2); c < (half + 1) * (N1 / 2); c += 16) {
             float v[16];
             tmem_ld16(tmem + lane_base + c, v);
 #pragma unroll
-            for (int i = 0; i < 16; i++)
-                sh[canon(row_in_tile, c + i, TC_M)] =
-                    __float2bfloat16_rn(gelu_tc(__fadd_rn(v[i], b1[c + i])));
+            for (int i = 0; i < 16; i++) v[i] = gelu_tc(__fadd_rn(v[i], b1[c + i]));
+            st_bf16x8(sh + canon(trow, c, TC_M), v);
+            st_bf16x8(sh + canon(trow, c + 8, TC_M), v + 8);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;");
@@ -194,32 +238,35 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // 4. layer 2
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t a0 = smem_u32(sh), b0 = smem_u32(sw2);
+            const uint32_t a0 = smem_u32(sh), bb = smem_u32(sw2);
             for (int kk = 0; kk < N1 / 16; kk++) {
                 const uint64_t ad = smem_desc(a0 + kk * 2 * TC_M * 16, TC_M * 16, 128);
-                const uint64_t bd = smem_desc(b0 + kk * 2 * N2 * 16, N2 * 16, 128);
+                const uint64_t bd = smem_desc(bb + kk * 2 * N2 * 16, N2 * 16, 128);
                 mma_bf16(tmem + N1, ad, bd, idesc_bf16(TC_M, N2), kk > 0);
             }
             mma_commit(mb);
         }
-        ok = __syncthreads_and(mbar_wait(mb, phase)) != 0;  // one decision for the CTA
+        ok = __syncthreads_and(mbar_wait(mb, phase)) != 0;
         if (!ok) {
             if (tid == 0) atomicOr(err, 1u);
             break;
         }
         phase ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;");
-        // 5. epilogue 2: bias -> float32 rows of Y
-        const int gr = r0 + row_in_tile;
-        for (int c = 0; c < N2; c += 16) {
+        // 5. epilogue 2: bias -> float32 tile in shared memory (A is no longer
+        //    read), then coalesced row stores
+        for (int c = half * (N2 / 2); c < (half + 1) * (N2 / 2); c += 16) {
             float v[16];
             tmem_ld16(tmem + lane_base + N1 + c, v);
-            if (gr < rows) {
 #pragma unroll
-                for (int i = 0; i < 16; i++) Y[(int64_t)gr * ldy + c + i] = __fadd_rn(v[i], b2[c + i]);
-            }
+            for (int i = 0; i < 16; i++) sy[trow * (N2 + 1) + c + i] = __fadd_rn(v[i], b2[c + i]);
         }
         asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        for (int e = tid; e < TC_M * N2; e += TC_THREADS) {
+            const int r = e / N2, c = e % N2;
+            if (r0 + r < rows) Y[(int64_t)(r0 + r) * ldy + c] = sy[r * (N2 + 1) + c];
+        }
         __syncthreads();
     }
     if (!ok) {

@@ -47,8 +47,9 @@ def test_pack_layout_on_host():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("pad", [3, None])  # odd row stride (scalar loads) / 16-byte rows
 @pytest.mark.parametrize("rows,k1", [(1000, 162), (128, 82), (300, 128), (1, 162), (0, 82)])
-def test_mlp2_bf16_matches_float64(rows, k1):
+def test_mlp2_bf16_matches_float64(rows, k1, pad):
     import torch
 
     from latec_b200 import _lib
@@ -56,7 +57,8 @@ def test_mlp2_bf16_matches_float64(rows, k1):
     lib = _lib.load()
     rs = np.random.RandomState(rows + k1)
     k1p = -(-k1 // 16) * 16
-    X = rs.randn(max(rows, 1), k1 + 3).astype(np.float32)  # row stride k1 + 3
+    ldx = k1 + 3 if pad else (k1 + 3) // 4 * 4
+    X = rs.randn(max(rows, 1), ldx).astype(np.float32)
     W1 = rs.uniform(-1, 1, (128, k1)).astype(np.float32) / np.sqrt(k1)
     b1 = rs.uniform(-0.1, 0.1, 128).astype(np.float32)
     W2 = rs.uniform(-1, 1, (64, 128)).astype(np.float32) / np.sqrt(128)
@@ -68,7 +70,7 @@ def test_mlp2_bf16_matches_float64(rows, k1):
     b1d, b2d = torch.from_numpy(b1).to(dev), torch.from_numpy(b2).to(dev)
     Y = torch.full((max(rows, 1), 70), 9.0, dtype=torch.float32, device=dev)  # ldy 70
     err = torch.zeros(1, dtype=torch.int32, device=dev)
-    _lib.check(lib.latec_gnn_mlp2_bf16(xd.data_ptr(), k1 + 3, rows, k1, k1p, w1p.data_ptr(),
+    _lib.check(lib.latec_gnn_mlp2_bf16(xd.data_ptr(), ldx, rows, k1, k1p, w1p.data_ptr(),
                                        b1d.data_ptr(), w2p.data_ptr(), b2d.data_ptr(),
                                        Y.data_ptr(), 70, err.data_ptr(),
                                        torch.cuda.current_stream().cuda_stream))
