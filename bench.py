@@ -248,7 +248,24 @@ def batch_shapes(n, seed=0):
     return out
 
 
-def batch_leg(dev, n=BATCH_N):
+def shard(items, rank, world):
+    """Independent units of a replicas-only job: rank r takes r, r + N, ..."""
+    return list(items)[rank::world]
+
+
+def reduce_over_ranks(values, op, world, device):
+    """Sum or max of per-rank floats over all ranks (identity on one rank)."""
+    if world == 1:
+        return list(values)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return [float(v) for v in t.tolist()]
+
+
+def batch_leg(dev, n=BATCH_N, rank=0, world=1):
     """Batched multi-tensor coding through the public API, tensors resident
     on the device: aggregate GB/s and per-tensor latency (compress +
     decompress), absolute eb 1e-3, cubic, levels 4, stride 16."""
@@ -260,7 +277,7 @@ def batch_leg(dev, n=BATCH_N):
     from latec_b200 import fields
 
     tensors = []
-    for shape, f64, ell, seed in batch_shapes(n):
+    for shape, f64, ell, seed in shard(batch_shapes(n), rank, world):
         x = fields.grf_se(shape, ell, seed=seed, device=dev)
         tensors.append(x.double() if f64 else x)
     pred = lambda: lb.InterpPredictor("cubic", 4, 16, 1)  # noqa: E731
@@ -281,6 +298,10 @@ def batch_leg(dev, n=BATCH_N):
         nbytes += x.numel() * x.element_size()
         sbytes += s.numel()
     total = time.perf_counter() - t0
+    # the tensors are sharded over the ranks: bytes add up, the slowest rank
+    # sets the time
+    nbytes, sbytes = reduce_over_ranks([nbytes, sbytes], "sum", world, dev)
+    (total,) = reduce_over_ranks([total], "max", world, dev)
     lat_ms = np.sort(np.asarray(lat)) * 1e3
     return {"workload": f"{n} tensors sampled from the 1000-tensor population (rank 2/3, "
                         "volume log-uniform 64^2..256^3, 20 % float64, SE-GRF l 2..32), "
@@ -288,7 +309,9 @@ def batch_leg(dev, n=BATCH_N):
             "tensors": n, "bytes": nbytes, "gbs": nbytes / total / 1e9,
             "ratio": nbytes / sbytes, "latency_ms_p50": float(np.percentile(lat_ms, 50)),
             "latency_ms_p99": float(np.percentile(lat_ms, 99)),
-            "mode": "serial loop over the public API (no multi-tensor launch)"}
+            "mode": "serial loop over the public API per rank (no multi-tensor launch), "
+                    f"tensors sharded over {world} rank(s)",
+            "latency_scope": "rank 0's tensors"}
 
 
 def run_reference(args, rank):
@@ -512,7 +535,7 @@ def main():
                "sample": f"{SAMPLE[0]}^3 float32 field of the same generator, one compress + "
                          "decompress round trip with the CPU oracle (NumPy + C rANS, compat mode)"}
     gnn_line = None if args.no_gnn else gnn_leg(dev)
-    batch_line = None if args.no_batch else batch_leg(dev)
+    batch_line = None if args.no_batch else batch_leg(dev, rank=rank, world=world)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
