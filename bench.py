@@ -53,9 +53,34 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+_NVML_CHILD = r"""
+import json, select, sys, pynvml
+pynvml.nvmlInit()
+try:
+    h = pynvml.nvmlDeviceGetHandleByPciBusId(sys.argv[1].encode())
+except Exception:
+    h = pynvml.nvmlDeviceGetHandleByIndex(int(sys.argv[2]))
+mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+print("ready", flush=True)
+sys.stdin.readline()
+rows = []
+while True:
+    try:
+        rows.append((pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM), mx,
+                     int(pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(h))))
+    except Exception:
+        pass
+    if select.select([sys.stdin], [], [], 0.002)[0]:
+        break
+print(json.dumps(rows), flush=True)
+"""
+
+
 class ClockSampler:
     """SM clock and clock-event reasons during the timed region, read (never
-    set) through NVML every 5 ms; nvidia-smi at 200 ms when NVML is missing."""
+    set) through NVML every 2 ms by a child process (so the sampling does not
+    wait on this process's interpreter lock); nvidia-smi at 200 ms when NVML
+    is missing."""
 
     # NVML clock-event reason bits
     REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
@@ -65,42 +90,35 @@ class ClockSampler:
         self.idx = gpu_index
         self.rows = []  # (sm_mhz, max_mhz, reasons bitmask)
         self.proc = None
-        self.stop = threading.Event()
+        self.child = None
         self.t = None
         try:  # NVML set-up (slow the first time) happens before the timed region
-            self.nv = self._nvml_handle()
+            self.child = self._start_child()
         except Exception:
-            self.nv = None
+            self.child = None
 
-    def _nvml_handle(self):
-        import pynvml
+    def _start_child(self):
         import torch
 
-        pynvml.nvmlInit()
+        bus = ""
         try:
             p = torch.cuda.get_device_properties(self.idx)
             bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
-            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
         except Exception:
-            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.idx)
-
-    def _nvml_loop(self, nv, h):
-        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
-        while True:  # at least one sample, then every 5 ms until the region ends
-            try:
-                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-                rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
-                self.rows.append((float(sm), float(mx), int(rs)))
-            except Exception:
-                pass
-            if self.stop.wait(0.005):
-                break
+            pass
+        c = subprocess.Popen([sys.executable, "-c", _NVML_CHILD, bus or "none", str(self.idx)],
+                             stdin=subprocess.PIPE, stdout=subprocess.PIPE,
+                             stderr=subprocess.DEVNULL, text=True)
+        if c.stdout.readline().strip() != "ready":
+            c.kill()
+            c.wait()
+            return None
+        return c
 
     def __enter__(self):
-        if self.nv is not None:
-            nv, h = self.nv
-            self.t = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
-            self.t.start()
+        if self.child is not None:
+            self.child.stdin.write("go\n")
+            self.child.stdin.flush()
             return self
         q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -126,7 +144,14 @@ class ClockSampler:
                 continue
 
     def __exit__(self, *a):
-        self.stop.set()
+        if self.child is not None:
+            try:
+                out, _ = self.child.communicate("stop\n", timeout=10)
+                self.rows = [(float(s), float(m), int(b)) for s, m, b in json.loads(out or "[]")]
+            except Exception:
+                self.child.kill()
+                self.child.wait()
+            self.child = None
         if self.proc is not None:
             self.proc.terminate()
             try:

@@ -227,13 +227,16 @@ class _Encoder:
             stages, ns, b.codes.data_ptr(), None, b.stats.data_ptr(), b.outliers.data_ptr(),
             b.elem, payload.data_ptr(), cap, plen.data_ptr(), err.data_ptr(), ws.data_ptr(),
             ws.numel(), stream), "latec_rans_encode")
-        n_bytes = int(plen.item())
+        # one download: payload length, error word and the stage descriptors
+        dsz = ctypes.sizeof(_lib.RansStage) * ns
+        tail = torch.cat([plen.view(torch.uint8), err.view(torch.uint8),
+                          ws[:dsz]]).cpu().numpy()
+        n_bytes = int(tail[:8].view(np.int64)[0])
+        e = int(tail[8:12].view(np.int32)[0])
         t_rans = time.perf_counter()
-        e = int(err.item())
         if e:
             raise RuntimeError(f"entropy coder reported error bits {e:#x}")
-        desc = (_lib.RansStage * ns).from_buffer_copy(
-            ws[:ctypes.sizeof(_lib.RansStage) * ns].cpu().numpy().tobytes())
+        desc = (_lib.RansStage * ns).from_buffer_copy(tail[12:12 + dsz].tobytes())
         rec_bytes = [16 + 4 * int(desc[t].blob_words) + b.elem * int(desc[t].n_out)
                      for t in range(ns)]
         del keep
@@ -463,8 +466,11 @@ def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, rad
     field, spatial, c, src = _prepare(img, dev)
     if len(spatial) > 6:
         raise NotImplementedError("the CUDA codec supports up to 6 spatial axes")
-    mm = torch.aminmax(field) if field.numel() else None
-    vmin, vmax = (float(mm.min.item()), float(mm.max.item())) if mm is not None else (0.0, 0.0)
+    if field.numel():  # one download for both ends of the range
+        mm = torch.aminmax(field)
+        vmin, vmax = (float(v) for v in torch.stack([mm.min, mm.max]).double().cpu().tolist())
+    else:
+        vmin, vmax = 0.0, 0.0
     if not (vmax > vmin):
         if not (np.isnan(vmin) or np.isnan(vmax)):
             vmax = vmin + 1.0
@@ -697,9 +703,12 @@ def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
     _lib.check(lib.latec_parse_records(pay_dev.data_ptr(), n_pay, ns, elem,
                                        int(mode == _lib.RANS_LANES), rec_dev.data_ptr(),
                                        tc_dev.data_ptr(), sp), "latec_parse_records")
-    recs = (_lib.Record * ns).from_buffer_copy(rec_dev.cpu().numpy().tobytes())
-    total_chunks = int(tc_dev.item())
-    if int(err.item()) & 64:
+    # one download: the records, the chunk total and the error word
+    rsz = ns * ctypes.sizeof(_lib.Record)
+    got = torch.cat([rec_dev, tc_dev.view(torch.uint8), err.view(torch.uint8)]).cpu().numpy()
+    recs = (_lib.Record * ns).from_buffer_copy(got[:rsz].tobytes())
+    total_chunks = int(got[rsz:rsz + 8].view(np.int64)[0])
+    if int(got[rsz + 8:rsz + 12].view(np.int32)[0]) & 64:  # err is int32
         raise ValueError("zstd frame is corrupt")
     items = [n * c for n in plan.counts]
     offsets = np.concatenate([[0], np.cumsum(items)]).astype(np.int64)

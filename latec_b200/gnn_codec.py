@@ -356,7 +356,7 @@ class GNNCodec:
             codes = rans.rans_decode(blob, lv64, tables, kexp=f["kexp"], shape=f["shape"],
                                      mode="native")
             codes_d = torch.from_numpy(codes.astype(np.uint16).view(np.int16)).to(dev)
-            outl_d = torch.from_numpy(np.ascontiguousarray(outl, np.float32)).to(dev)
+            outl_d = torch.from_numpy(np.array(outl, np.float32)).to(dev)
             recon = torch.empty(n, dtype=torch.float32, device=dev)
             ws = torch.empty(max(int(lib.latec_dequantize_workspace_bytes(n)), 1),
                              dtype=torch.uint8, device=dev)
