@@ -16,7 +16,9 @@ e2e    : the same through host buffers: a page-locked host field in, the
 roofline: the fused interpolation/quantizer pass (dominant kernel family) --
          algorithmic bytes 10 B/point for float32 (read x, write recon, write
          the 16-bit code) over the pass's CUDA-event time, against the
-         measured HBM copy bandwidth.
+         measured HBM copy bandwidth. Beside it, the opt-in fused finest-level
+         kernels (k_tile_level_enc / _dec, tile mode 1) timed alone by CUDA
+         event pairs the library records on the launching stream.
 cpu_baseline: the CPU oracle (NumPy restatement of the reference algorithm +
          C rANS coder) on a 128^3 sample of the same generator, 1 core.
 
@@ -528,9 +530,40 @@ def main():
         if i:
             times.append(e0.elapsed_time(e1))
     pass_ms = statistics.median(times)
+    # the opt-in fused finest-level kernels alone (tile mode 1): event pairs
+    # around each launch
+    n_level = sum(plan.counts[-5:])
+    n_coarse = sum(plan.counts) - n_level
+    enc_alg = n_level * (4 + 4 + 2) + n_coarse * 4
+    dec_alg = n_level * (2 + 4) + n_coarse * 4
+    kms, kn = ctypes.c_double(), ctypes.c_uint32()
+    _lib.check(lib.latec_set_tile_mode(1))
+    _lib.check(lib.latec_set_kernel_timing(1))
+    for kind in (0, 1):
+        _lib.check(lib.latec_kernel_time(kind, ctypes.byref(kms), ctypes.byref(kn)))
+    for i in range(3):
+        _lib.check(lib.latec_encode_stages(plan.handle, ctypes.byref(prm), eb_arr, x.data_ptr(),
+                                           rc.data_ptr(), b.codes.data_ptr(), b.outliers.data_ptr(),
+                                           b.stats.data_ptr(), b.hist_seg.data_ptr(),
+                                           b.hist_total.data_ptr(), b.ws.data_ptr(), b.ws.numel(),
+                                           s_ptr))
+        out = lb.decompress(stream, out="device")
+    del out
+    torch.cuda.synchronize()
+    _lib.check(lib.latec_kernel_time(0, ctypes.byref(kms), ctypes.byref(kn)))
+    enc_ms = kms.value / max(1, kn.value)
+    _lib.check(lib.latec_kernel_time(1, ctypes.byref(kms), ctypes.byref(kn)))
+    dec_ms = kms.value / max(1, kn.value)
+    _lib.check(lib.latec_set_kernel_timing(0))
+    _lib.check(lib.latec_set_tile_mode(0))
     alg_bytes = sum(plan.counts) * (4 + 4 + 2)
     peak, peak_kind = _peaks()
     achieved = alg_bytes / (pass_ms / 1e3) / 1e9
+    fused = {"mode": "opt-in (latec_set_tile_mode(1)); default off: slower on B200",
+             "encode": {"kernel": "k_tile_level_enc", "alg_bytes": enc_alg, "kernel_ms": enc_ms,
+                        "achieved_gbs": enc_alg / (enc_ms / 1e3) / 1e9 if enc_ms else 0.0},
+             "decode": {"kernel": "k_tile_level_dec", "alg_bytes": dec_alg, "kernel_ms": dec_ms,
+                        "achieved_gbs": dec_alg / (dec_ms / 1e3) / 1e9 if dec_ms else 0.0}}
     del rc, enc
 
     # ---- end to end through host buffers (pinned host input, bytes stream,
@@ -590,7 +623,8 @@ def main():
                      "traffic_source": "ncu dram bytes of the pass at 384^3 scaled by points "
                                        "(profiles/k_interp_quant_turb384.md)",
                      "kernel": "k_interp_quant pass (31 stages incl. scan/compaction)",
-                     "alg_bytes": alg_bytes, "pass_ms": pass_ms, "peak_kind": peak_kind},
+                     "alg_bytes": alg_bytes, "pass_ms": pass_ms, "peak_kind": peak_kind,
+                     "fused_finest_level": fused},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": "GB/s", "h2d_bytes_per_step": nbytes + len(s_e),
                 "d2h_bytes_per_step": nbytes + len(s_e)},

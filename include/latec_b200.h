@@ -157,6 +157,25 @@ int latec_dequantize(const latec_quant_params* prm, double eb, uint64_t items, c
  *      Results are bit-identical in all modes. Process-wide. */
 int latec_set_level_mode(int32_t mode);
 
+/* ---- fused tile levels of 3-D plans (no counterpart in the reference): the
+ *      five sub-stages of a level (weight 1 along axes 0, 1, 2, weight 2,
+ *      weight 3) in one launch over tiles of the level's lattice held in
+ *      shared memory with a 3-point halo, encode and decode alike.
+ *      0 (default) = off (one launch per stage, measured faster on B200),
+ *      1 = the finest level, 2 = every level. Results are bit-identical in
+ *      all modes.
+ *      Process-wide. */
+int latec_set_tile_mode(int32_t mode);
+
+/* ---- kernel timing (a measurement aid, no counterpart in the reference):
+ *      with timing on, a CUDA event pair is recorded on the launching stream
+ *      around every fused tile-level launch. latec_kernel_time sums the
+ *      recorded pairs of one kind (0 = encode, 1 = decode; it waits for their
+ *      end events), returns the milliseconds and the launch count, and clears
+ *      them. Process-wide. */
+int latec_set_kernel_timing(int32_t on);
+int latec_kernel_time(int32_t kind, double* ms, uint32_t* launches);
+
 /* ---- decode: predict + dequantize over every stage
  *      (latec/codec.py:462-510 _decompress_region). codes as produced by
  *      latec_rans_decode; outliers: device byte array holding every stage's

@@ -89,6 +89,10 @@ SIGNATURES = {
     "latec_dequantize": (ctypes.c_int, [ctypes.POINTER(QuantParams), D, U64, P, P, P, U32, P, P,
                                         P, U64, P]),
     "latec_set_level_mode": (ctypes.c_int, [I32]),
+    "latec_set_tile_mode": (ctypes.c_int, [I32]),
+    "latec_set_kernel_timing": (ctypes.c_int, [I32]),
+    "latec_kernel_time": (ctypes.c_int, [I32, ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(ctypes.c_uint32)]),
     "latec_decode_stages": (ctypes.c_int, [P, ctypes.POINTER(QuantParams), P, P, P, P, P, P, P,
                                            P, U64, P]),
     "latec_rans_build_tables": (ctypes.c_int, [P, I32, I32, P, P, P]),

@@ -8,8 +8,10 @@
 #include "interp_kernels.cuh"
 #include "plan.h"
 #include "rans_kernels.cuh"
+#include "tile_kernels.cuh"
 
 #include <atomic>
+#include <mutex>
 
 using namespace latec;
 
@@ -101,7 +103,7 @@ uint64_t stage_ws(uint64_t max_items, uint64_t all_tiles, int n_stages, int elem
     w.tile_cnt = c.take<uint32_t>(tiles);
     w.tile_off = c.take<uint32_t>(tiles);
     w.total = c.take<uint32_t>(4);
-    w.partials = c.take<double>((uint64_t)MAX_BLOCKS * 5 + 5);
+    w.partials = c.take<double>((uint64_t)TILE_STAGES * MAX_BLOCKS * 5 + 5);
     w.dec = c.take<DecStage>(n_stages > 0 ? n_stages : 1);
     w.lvl_items_cap = all_tiles + (uint64_t)LVL_MAX_STAGES * LVL_MAX_BANDS;
     w.lvl_stages = c.take<LvlStage>(LVL_MAX_STAGES);
@@ -113,6 +115,18 @@ uint64_t stage_ws(uint64_t max_items, uint64_t all_tiles, int n_stages, int elem
     return c.off;
 }
 
+// Stages [t, t + 5) form a standard level of a 3-D plan: weight 1 along axes
+// 0, 1 and 2, then the fused weight-2 and weight-3 stages, all of one stride.
+bool tile_level_shape(const latec_plan* plan, int t) {
+    if (plan->ndim != 3 || t < 1 || t + TILE_STAGES > (int)plan->stages.size()) return false;
+    const StageDesc* d = &plan->stages[t];
+    const int s = d[0].s;
+    for (int j = 0; j < 3; j++)
+        if (d[j].kind != 0 || d[j].axis != j || d[j].weight != 1 || d[j].s != s) return false;
+    return d[3].kind == 1 && d[3].weight == 2 && d[3].s == s && d[4].kind == 1 &&
+           d[4].weight == 3 && d[4].s == s;
+}
+
 void plan_sizes(const latec_plan* plan, int C, uint64_t* max_items, uint64_t* all_tiles) {
     uint64_t m = 0, t = 0;
     for (auto& d : plan->stages) {
@@ -120,10 +134,99 @@ void plan_sizes(const latec_plan* plan, int C, uint64_t* max_items, uint64_t* al
         m = items > m ? items : m;
         t += n_tiles(items);
     }
+    // a fused level stages the outliers of its five stages at once
+    for (int k = 1; k < (int)plan->stages.size(); k++) {
+        if (!tile_level_shape(plan, k)) continue;
+        uint64_t sum = 0;
+        for (int j = 0; j < TILE_STAGES; j++) sum += (uint64_t)plan->stages[k + j].n * C;
+        m = sum > m ? sum : m;
+    }
     *max_items = m;
     *all_tiles = t;
 }
 
+// Fused tile levels of 3-D plans: 0 off (per-stage launches, the default:
+// measured faster on B200, the fused kernels being issue-bound on integer
+// work), 1 the finest level (stride 1) only, 2 every level. Results are
+// bit-identical.
+std::atomic<int> g_tile_mode{0};
+
+// Kernel timing (a measurement aid): when on, a CUDA event pair is recorded
+// on the launching stream around every fused-level launch; kind 0 = encode,
+// 1 = decode.
+std::atomic<bool> g_kt_on{false};
+std::mutex g_kt_mu;
+struct KtPair {
+    cudaEvent_t a, b;
+    int kind;
+};
+std::vector<KtPair> g_kt_pairs, g_kt_free;
+
+int kt_start(int kind, cudaStream_t st) {
+    if (!g_kt_on.load()) return -1;
+    std::lock_guard<std::mutex> lk(g_kt_mu);
+    KtPair p;
+    if (!g_kt_free.empty()) {
+        p = g_kt_free.back();
+        g_kt_free.pop_back();
+    } else if (cudaEventCreate(&p.a) != cudaSuccess || cudaEventCreate(&p.b) != cudaSuccess) {
+        return -1;
+    }
+    p.kind = kind;
+    if (cudaEventRecord(p.a, st) != cudaSuccess) {
+        g_kt_free.push_back(p);
+        return -1;
+    }
+    g_kt_pairs.push_back(p);
+    return (int)g_kt_pairs.size() - 1;
+}
+
+void kt_stop(int idx, cudaStream_t st) {
+    if (idx < 0) return;
+    std::lock_guard<std::mutex> lk(g_kt_mu);
+    if (idx < (int)g_kt_pairs.size()) cudaEventRecord(g_kt_pairs[idx].b, st);
+}
+
+bool tile_level_at(const latec_plan* plan, int t, int mode) {
+    if (mode == 0 || !tile_level_shape(plan, t)) return false;
+    if (mode == 1 && plan->stages[t].s != 1) return false;
+    uint64_t n = 0;
+    for (int j = 0; j < TILE_STAGES; j++) n += plan->stages[t + j].n;
+    return n > 0;
+}
+
+int n_sms() {
+    int dev = 0, n = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+}
+
+// The lattice of the level starting at stage t, its work split and the
+// per-stage quantizers and code arrays (codes_off: first code of stage t).
+bool tile_level_init(const latec_plan* plan, const latec_quant_params* prm,
+                     const double* stage_eb, int t, int C, uint16_t* codes, uint64_t codes_off,
+                     TileLevel& L, uint32_t* grid) {
+    std::memset(&L, 0, sizeof(L));
+    const StageDesc& d = plan->stages[t];
+    for (int j = 0; j < 3; j++) {
+        L.N[j] = (int32_t)((d.shape[j] + d.s - 1) / d.s);
+        L.ls[j] = (int64_t)d.s * d.gstride[j];
+    }
+    L.points = plan->points;
+    L.channels = C;
+    tile_level_geometry(L, elem_of(prm->dtype), n_sms(), grid);
+    if (*grid > (uint32_t)MAX_BLOCKS) *grid = MAX_BLOCKS;
+    uint64_t o = codes_off;
+    for (int j = 0; j < TILE_STAGES; j++) {
+        TileStage& S = L.st[j];
+        if (!make_q(prm, stage_eb[t + j], plan->points, S.q)) return false;
+        S.n = plan->stages[t + j].n;
+        S.codes = codes + o;
+        o += (uint64_t)S.n * C;
+    }
+    return true;
+}
 
 // 0 per-stage launches (default: measured faster on B200, see the design
 // notes), 1 level kernels for levels of >= 4 Mi points, 2 every level that
@@ -267,6 +370,42 @@ int latec_set_level_mode(int32_t mode) {
     return LATEC_OK;
 }
 
+int latec_set_tile_mode(int32_t mode) {
+    if (mode < 0 || mode > 2) return LATEC_ERR_ARG;
+    g_tile_mode.store(mode);
+    return LATEC_OK;
+}
+
+int latec_set_kernel_timing(int32_t on) {
+    g_kt_on.store(on != 0);
+    return LATEC_OK;
+}
+
+int latec_kernel_time(int32_t kind, double* ms, uint32_t* launches) {
+    if (!ms || !launches || kind < 0 || kind > 1) return LATEC_ERR_ARG;
+    std::lock_guard<std::mutex> lk(g_kt_mu);
+    double sum = 0.0;
+    uint32_t n = 0;
+    int rc = LATEC_OK;
+    std::vector<KtPair> keep;
+    for (auto& p : g_kt_pairs) {
+        if (p.kind != kind) {
+            keep.push_back(p);
+            continue;
+        }
+        float f = 0.0f;
+        if (cudaEventSynchronize(p.b) != cudaSuccess || cudaEventElapsedTime(&f, p.a, p.b) != cudaSuccess)
+            rc = LATEC_ERR_CUDA;
+        sum += f;
+        n++;
+        g_kt_free.push_back(p);
+    }
+    g_kt_pairs.swap(keep);
+    *ms = sum;
+    *launches = n;
+    return rc;
+}
+
 const char* latec_version(void) { return "latec_b200 0.1 (sm_100a)"; }
 
 uint64_t latec_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
@@ -351,7 +490,53 @@ int latec_encode_stages(const latec_plan* plan, const latec_quant_params* prm,
         cudaMemsetAsync(hist_total, 0, sizeof(uint32_t) * 65536ull * ns, st) != cudaSuccess)
         return LATEC_ERR_CUDA;
     uint64_t off = 0, seg = 0;
+    const int tmode = g_tile_mode.load();
     for (int t = 0; t < ns; t++) {
+        if (tile_level_at(plan, t, tmode)) {
+            // the level's five stages in one fused launch, then per stage the
+            // statistics / tile-offset tail and the outlier compaction
+            TileLevel L;
+            uint32_t grid;
+            if (!tile_level_init(plan, prm, stage_eb, t, C, codes, off, L, &grid))
+                return LATEC_ERR_ARG;
+            L.vec = tile_vec_ok(L, elem, x, recon) ? 1 : 0;
+            TailArgs ta;
+            std::memset(&ta, 0, sizeof(ta));
+            uint64_t stg = 0, o = off, sg = seg;
+            uint32_t tl = 0;
+            for (int j = 0; j < TILE_STAGES; j++) {
+                TileStage& S = L.st[j];
+                const uint64_t items = (uint64_t)S.n * C;
+                S.staging = (uint8_t*)w.staging + stg * elem;
+                S.tile_cnt = w.tile_cnt + tl;
+                S.hist_total = hist_total + 65536ull * (t + j);
+                S.hist_seg = hist_seg + (uint64_t)HBINS * sg;
+                S.partials = w.partials + (uint64_t)j * grid * 5;
+                S.acc = (StageAcc*)(stats + t + j);
+                ta.s[j] = TailStage{S.partials, grid, n_tiles(items), S.tile_cnt, w.tile_off + tl,
+                                    S.acc};
+                stg += items;
+                o += items;
+                sg += n_segments(items);
+                tl += n_tiles(items);
+            }
+            if (tl && cudaMemsetAsync(w.tile_cnt, 0, sizeof(uint32_t) * tl, st) != cudaSuccess)
+                return LATEC_ERR_CUDA;
+            const int ki = kt_start(0, st);
+            int rc = launch_tile_level_encode(L, prm->dtype, prm->order ? 1 : 0, grid, x, recon, st);
+            kt_stop(ki, st);
+            if (!rc) rc = launch_stage_tails(ta, TILE_STAGES, st);
+            for (int j = 0; j < TILE_STAGES && !rc; j++) {
+                const uint64_t items = (uint64_t)L.st[j].n * C;
+                rc = launch_compact(L.st[j].codes, items, L.st[j].staging, elem, ta.s[j].tile_cnt,
+                                    ta.s[j].tile_off, (uint8_t*)outliers + off * elem, st);
+                off += items;
+                seg += n_segments(items);
+            }
+            if (rc) return rc;
+            t += TILE_STAGES - 1;
+            continue;
+        }
         const StageDesc& d = plan->stages[t];
         const uint64_t items = (uint64_t)d.n * C;
         QParams q;
@@ -480,8 +665,45 @@ int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
     if (!rc) rc = launch_tile_offsets_all(w.dec, ns, w.tile_cnt, w.tile_off, err, st);
     if (rc) return rc;
     const int mode = g_level_mode.load();
+    const int tmode = g_tile_mode.load();
     int t = 0;
     while (t < ns) {
+        if (tile_level_at(plan, t, tmode)) {
+            // outliers of the level into the canvas, then the fused decode
+            ScatterArgs sa;
+            std::memset(&sa, 0, sizeof(sa));
+            uint32_t tiles = 0;
+            for (int j = 0; j < TILE_STAGES; j++) {
+                const DecStage& dj = ds[t + j];
+                if (!n_out[t + j] || !dj.items || !outliers) continue;
+                ScatterStage& S = sa.s[sa.n++];
+                S.d = plan->stages[t + j];
+                S.codes = codes + dj.codes_off;
+                S.outliers = (const uint8_t*)outliers + out_off[t + j];
+                S.tile_cnt = w.tile_cnt + dj.tile0;
+                S.tile_off = w.tile_off + dj.tile0;
+                S.items = dj.items;
+                S.n_out = n_out[t + j];
+                S.tile0 = tiles;
+                tiles += n_tiles(dj.items);
+            }
+            sa.channels = C;
+            sa.points = plan->points;
+            rc = launch_scatter_outliers(sa, prm->dtype, tiles, recon, err, st);
+            if (rc) return rc;
+            TileLevel L;
+            uint32_t grid;
+            if (!tile_level_init(plan, prm, stage_eb, t, C, const_cast<uint16_t*>(codes),
+                                 ds[t].codes_off, L, &grid))
+                return LATEC_ERR_ARG;
+            L.vec = tile_vec_ok(L, elem_of(prm->dtype), recon, recon) ? 1 : 0;
+            const int ki = kt_start(1, st);
+            rc = launch_tile_level_decode(L, prm->dtype, prm->order ? 1 : 0, grid, recon, st);
+            kt_stop(ki, st);
+            if (rc) return rc;
+            t += TILE_STAGES;
+            continue;
+        }
         // a level: consecutive stages of one stride (the anchors stand alone)
         int t1 = t + 1;
         if (t > 0)

@@ -42,6 +42,7 @@ def test_level_kernels_match_per_stage_launches(case):
         from latec_b200 import _lib
 
         lib = _lib.load()
+        _lib.check(lib.latec_set_tile_mode(0))  # per-stage launches on the finest level too
         outs, launches = [], []
         for mode in (0, 2):
             _mode(mode)
@@ -60,3 +61,6 @@ def test_level_kernels_match_per_stage_launches(case):
         assert float((d2.double() - x.double()).abs().max().item()) <= eb
     finally:
         _mode(0)
+        from latec_b200 import _lib
+
+        _lib.check(_lib.load().latec_set_tile_mode(0))
