@@ -380,6 +380,68 @@ const char* latec_version(void);
 /* Number of CUDA kernel launches this library has issued in this process. */
 uint64_t latec_launch_count(void);
 
+/* ---- training of the learned predictor (scripts/train_gnn.py): forward
+ *      ops that keep what their backward needs, the backward ops, the
+ *      discretised-Laplace rate loss and the AdamW / EMA updates. float32;
+ *      weights (out, in) row-major as nn.Linear; device pointers; stream may
+ *      be NULL. Gradient buffers accumulate (zero them per step). */
+/* Y = act(X W^T + b), act 1 = GELU; Z (optional) keeps the pre-activation. */
+int latec_tr_linear(const float* X, int64_t ldx, int64_t rows, int32_t in, const float* W,
+                    const float* b, int32_t out, float* Y, int64_t ldy, int32_t act, float* Z,
+                    void* stream);
+/* dX = dZ W (stored, or added when accum_dx; dX may be NULL), dW += dZ^T X,
+ * db += sum dZ, dZ = dY * gelu'(Z) when act. */
+int latec_tr_linear_bwd(const float* X, int64_t ldx, int64_t rows, int32_t in, const float* W,
+                        int32_t out, const float* dY, int64_t ldy, const float* Z, int32_t act,
+                        float* dX, int64_t lddx, int32_t accum_dx, float* dW, float* db,
+                        void* stream);
+/* Message rows of all batches (two-sided when two, else one-sided) for the
+ * pairs of a stage (latec/gnn_predictor.py:618-660 BiDirEmbed / DirEmbed
+ * inputs) and their backward into dE and the direction-state table. */
+int latec_tr_rows(const float* E, int64_t N, int32_t K, int32_t d, int32_t ds, const float* table,
+                  const latec_gnn_geom* geom, const int32_t* pairs, int64_t np, int32_t B,
+                  int32_t two, float* X, int32_t ldx, void* stream);
+int latec_tr_rows_bwd(const float* dX, int32_t ldx, int64_t N, int32_t K, int32_t d, int32_t ds,
+                      const latec_gnn_geom* geom, const int32_t* pairs, int64_t np, int32_t B,
+                      int32_t two, float* dE, float* dtable, void* stream);
+int latec_tr_line_rows(const int32_t* row_of, int32_t M, int32_t L, int32_t K, int32_t B,
+                       int64_t np2, int64_t np1, int32_t* rows, void* stream);
+/* AttnPool (latec/gnn_predictor.py:724-749) keeping the probabilities P
+ * (n_out x (n + 1), null token last), and its backward. */
+int latec_tr_attn(const float* key, const float* V, int32_t d, const int32_t* rows, int32_t n,
+                  int64_t n_out, float scale, const float* null_k, const float* null_v, float* out,
+                  float* P, void* stream);
+int latec_tr_attn_bwd(const float* V, int32_t d, const int32_t* rows, int32_t n, int64_t n_out,
+                      float scale, const float* null_v, const float* P, const float* dout,
+                      float* dkey, float* dV, float* dnull_k, float* dnull_v, void* stream);
+/* PredHead rows / readout with a per-sample log2 eb, and the readout's
+ * backward. */
+int latec_tr_head_rows(const float* pooled, int64_t n, int32_t per_b, int32_t d,
+                       const float* log_eb, float* X, void* stream);
+int latec_tr_head_out(const float* O, int64_t n, int32_t per_b, const float* log_eb, float* mu,
+                      float* log_b, void* stream);
+int latec_tr_head_out_bwd(const float* O, const float* mu, int64_t n, const float* dmu,
+                          const float* dlog_b, float* dO, void* stream);
+/* discretized_laplace_nll (bits) + mse_weight * squared error of n points
+ * (sample = i / per_b, bound eb[sample]); acc[0..2] += bits, squared error,
+ * |error| (double); dmu / dlog_b = scale * d(bits + mse_weight * sq). */
+int latec_tr_loss(const float* mu, const float* log_b, const float* tgt, int64_t n, int32_t per_b,
+                  const float* eb, float mse_weight, float scale, float* dmu, float* dlog_b,
+                  double* acc, void* stream);
+/* MixEmbed rows [ctx | value embedding] and backward; E scatter of the
+ * finalised rows (backward = 1 gathers dE into Y). */
+int latec_tr_mix_rows(const float* ctx, const float* vemb, int64_t bmk, int32_t K, int32_t d,
+                      float* X, void* stream);
+int latec_tr_mix_rows_bwd(const float* dX, int64_t bmk, int32_t K, int32_t d, float* dctx,
+                          float* dvemb, void* stream);
+int latec_tr_scatter_e(float* Y, const int32_t* query, int32_t B, int32_t M, int32_t K, int32_t d,
+                       int64_t N, float* E, int32_t backward, void* stream);
+/* torch.optim.AdamW step (decoupled decay, bias-corrected) and the EMA
+ * shadow update. */
+int latec_tr_adamw(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1,
+                   float b2, float eps, float wd, int64_t step, void* stream);
+int latec_tr_ema(float* shadow, const float* p, int64_t n, float decay, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

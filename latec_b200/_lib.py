@@ -26,6 +26,7 @@ F32, F64 = 1, 2
 RANS_LANES, RANS_COMPAT = 0, 1
 
 U32, U64, I32, P, D = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_double
+I64, F = ctypes.c_int64, ctypes.c_float
 
 
 class QuantParams(ctypes.Structure):
@@ -117,6 +118,25 @@ SIGNATURES = {
                                        ctypes.POINTER(GnnGeom), P, P, U64, P]),
     "latec_gnn_head": (ctypes.c_int, [ctypes.POINTER(GnnModel), I32, I32, I32, P,
                                       ctypes.c_float, P, P, P, U64, P]),
+    "latec_tr_linear": (ctypes.c_int, [P, I64, I64, I32, P, P, I32, P, I64, I32, P, P]),
+    "latec_tr_linear_bwd": (ctypes.c_int, [P, I64, I64, I32, P, I32, P, I64, P, I32, P, I64, I32,
+                                           P, P, P]),
+    "latec_tr_rows": (ctypes.c_int, [P, I64, I32, I32, I32, P, ctypes.POINTER(GnnGeom), P, I64,
+                                     I32, I32, P, I32, P]),
+    "latec_tr_rows_bwd": (ctypes.c_int, [P, I32, I64, I32, I32, I32, ctypes.POINTER(GnnGeom), P,
+                                         I64, I32, I32, P, P, P]),
+    "latec_tr_line_rows": (ctypes.c_int, [P, I32, I32, I32, I32, I64, I64, P, P]),
+    "latec_tr_attn": (ctypes.c_int, [P, P, I32, P, I32, I64, F, P, P, P, P, P]),
+    "latec_tr_attn_bwd": (ctypes.c_int, [P, I32, P, I32, I64, F, P, P, P, P, P, P, P, P]),
+    "latec_tr_head_rows": (ctypes.c_int, [P, I64, I32, I32, P, P, P]),
+    "latec_tr_head_out": (ctypes.c_int, [P, I64, I32, P, P, P, P]),
+    "latec_tr_head_out_bwd": (ctypes.c_int, [P, P, I64, P, P, P, P]),
+    "latec_tr_loss": (ctypes.c_int, [P, P, P, I64, I32, P, F, F, P, P, P, P]),
+    "latec_tr_mix_rows": (ctypes.c_int, [P, P, I64, I32, I32, P, P]),
+    "latec_tr_mix_rows_bwd": (ctypes.c_int, [P, I64, I32, I32, P, P, P]),
+    "latec_tr_scatter_e": (ctypes.c_int, [P, P, I32, I32, I32, I32, I64, P, I32, P]),
+    "latec_tr_adamw": (ctypes.c_int, [P, P, P, P, I64, F, F, F, F, F, I64, P]),
+    "latec_tr_ema": (ctypes.c_int, [P, P, I64, F, P]),
     "latec_gnn_finalize": (ctypes.c_int, [ctypes.POINTER(GnnModel), I32, ctypes.c_int64, I32,
                                           I32, P, P, P, P, P, U64, P]),
     "latec_gnn_pack_bf16": (ctypes.c_int, [P, I32, I32, I32, P]),

@@ -1,0 +1,702 @@
+// Training kernels of the learned predictor (scripts/train_gnn.py): the
+// forward ops of the axial GNN with the activations the backward pass needs,
+// their backward ops, the discretised-Laplace rate loss and the AdamW / EMA
+// updates. float32 throughout; gradient reductions over rows use atomics
+// (training needs no run-to-run bit identity; the codec's inference path is
+// gnn_kernels.cu, whose order is fixed).
+//
+// Layouts: X (rows, ldx) row-major; weights W (out, in) row-major as in the
+// reference's nn.Linear; E (B, N, K, d); contexts (B, M, K, d).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "latec_common.cuh"
+
+namespace latec {
+namespace {
+
+constexpr int TT = 256;
+constexpr int GM = 64, GN = 64, GK = 16;
+
+inline unsigned tblocks(int64_t n) { return (unsigned)((n + TT - 1) / TT); }
+
+__device__ __forceinline__ float gelu_f(float z) {
+    return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
+}
+__device__ __forceinline__ float gelu_d(float z) {
+    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) +
+           z * 0.39894228040143268f * expf(-0.5f * z * z);
+}
+
+// C (M x N, ldc) = sum_k A(m, k) * B(k, n), 64 x 64 tiles, 4 x 4 per thread.
+//   TA = 0: A(m, k) = A[m * lda + k]; TA = 1: A(m, k) = A[k * lda + m]
+//   TB = 0: B(k, n) = B[k * ldb + n]; TB = 1: B(k, n) = B[n * ldb + k]
+//   GA: A is dY and is multiplied by gelu'(Z) on load (Z laid out like A)
+//   split-K over gridDim.z; ACC: add into C with atomics, else store
+//   bias (optional, added once by the z = 0 slice)
+template <int TA, int TB, int GA, int ACC>
+__global__ void __launch_bounds__(TT)
+    k_gemm(int M, int N, int Kd, const float* __restrict__ A, int64_t lda,
+           const float* __restrict__ Bm, int64_t ldb, const float* __restrict__ Z, float* C,
+           int64_t ldc, const float* __restrict__ bias, int act, float* Zout, int64_t ldz) {
+    __shared__ float as[GK][GM + 4];
+    __shared__ float bs[GK][GN + 4];
+    const int m0 = blockIdx.x * GM, n0 = blockIdx.y * GN;
+    const int64_t per = ((int64_t)Kd + gridDim.z - 1) / gridDim.z;
+    const int64_t kb = per * blockIdx.z, ke = kb + per < Kd ? kb + per : Kd;
+    const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
+    float acc[4][4] = {};
+    for (int64_t k0 = kb; k0 < ke; k0 += GK) {
+        for (int e = threadIdx.x; e < GM * GK; e += TT) {
+            int mm, kk;
+            if (TA) { kk = e / GM; mm = e % GM; } else { mm = e / GK; kk = e % GK; }
+            const int m = m0 + mm;
+            const int64_t k = k0 + kk;
+            float v = 0.0f;
+            if (m < M && k < ke) {
+                const int64_t o = TA ? k * lda + m : (int64_t)m * lda + k;
+                v = A[o];
+                if (GA) v *= gelu_d(Z[o]);
+            }
+            as[kk][mm] = v;
+        }
+        for (int e = threadIdx.x; e < GN * GK; e += TT) {
+            int nn, kk;
+            if (TB) { nn = e / GK; kk = e % GK; } else { kk = e / GN; nn = e % GN; }
+            const int n = n0 + nn;
+            const int64_t k = k0 + kk;
+            bs[kk][nn] = (n < N && k < ke) ? Bm[TB ? (int64_t)n * ldb + k : k * ldb + n] : 0.0f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < GK; kk++) {
+            float av[4], bv[4];
+#pragma unroll
+            for (int a = 0; a < 4; a++) av[a] = as[kk][tr * 4 + a];
+#pragma unroll
+            for (int c = 0; c < 4; c++) bv[c] = bs[kk][tc * 4 + c];
+#pragma unroll
+            for (int a = 0; a < 4; a++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc[a][c] += av[a] * bv[c];
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        const int m = m0 + tr * 4 + a;
+        if (m >= M) continue;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const int n = n0 + tc * 4 + c;
+            if (n >= N) continue;
+            float v = acc[a][c];
+            if (ACC) {
+                atomicAdd(&C[(int64_t)m * ldc + n], v);
+            } else {
+                if (bias) v += bias[n];
+                if (Zout) Zout[(int64_t)m * ldz + n] = v;
+                C[(int64_t)m * ldc + n] = act ? gelu_f(v) : v;
+            }
+        }
+    }
+}
+
+// db[j] += sum_r dY[r, j] (* gelu'(Z[r, j])): one warp per column slice.
+__global__ void __launch_bounds__(TT)
+    k_colsum(int64_t rows, int n, const float* __restrict__ dY, int64_t ldy,
+             const float* __restrict__ Z, float* __restrict__ db) {
+    const int j = blockIdx.y;
+    float s = 0.0f;
+    for (int64_t r = (int64_t)blockIdx.x * TT + threadIdx.x; r < rows; r += (int64_t)gridDim.x * TT) {
+        float v = dY[r * ldy + j];
+        if (Z) v *= gelu_d(Z[r * ldy + j]);
+        s += v;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&db[j], s);
+}
+
+// ---- message rows (all batches at once): row w = (b * np + p) * K + k ----
+// two-sided: [E(nbr_n) | table(sidx_n) | E(nbr_p) | table(sidx_p) | logd_n | logd_p]
+// one-sided: [E(side) | table(side) | +-1 | logd_side]
+__global__ void __launch_bounds__(TT)
+    k_tr_rows(const float* __restrict__ E, int64_t N, int K, int d, int ds,
+              const float* __restrict__ table, const latec_gnn_geom g,
+              const int32_t* __restrict__ pairs, int64_t np, int B, int two, float* __restrict__ X,
+              int ldx) {
+    const int64_t w = ((int64_t)blockIdx.x * TT + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= (int64_t)B * np * K) return;
+    const int k = (int)(w % K);
+    const int64_t bp = w / K;
+    const int64_t p = bp % np;
+    const int b = (int)(bp / np);
+    const int pair = pairs[p];
+    const int l = pair / g.M;
+    const int de = d + ds;
+    float* row = X + w * ldx;
+    if (two) {
+        const float* en = E + (((int64_t)b * N + g.nbr_n[pair]) * K + k) * d;
+        const float* ep = E + (((int64_t)b * N + g.nbr_p[pair]) * K + k) * d;
+        const float* sn = table + (int64_t)g.sidx_n[l * K + k] * ds;
+        const float* sp = table + (int64_t)g.sidx_p[l * K + k] * ds;
+        for (int f = lane; f < 2 * de + 2; f += 32) {
+            float v;
+            if (f < d) v = en[f];
+            else if (f < de) v = sn[f - d];
+            else if (f < de + d) v = ep[f - de];
+            else if (f < 2 * de) v = sp[f - de - d];
+            else if (f == 2 * de) v = g.logd_n[pair];
+            else v = g.logd_p[pair];
+            row[f] = v;
+        }
+    } else {
+        const bool pos = g.nbr_p[pair] >= 0;
+        const int64_t nb = pos ? g.nbr_p[pair] : g.nbr_n[pair];
+        const float* e = E + (((int64_t)b * N + nb) * K + k) * d;
+        const float* s = table + (int64_t)(pos ? g.sidx_p[l * K + k] : g.sidx_n[l * K + k]) * ds;
+        for (int f = lane; f < de + 2; f += 32) {
+            float v;
+            if (f < d) v = e[f];
+            else if (f < de) v = s[f - d];
+            else if (f == de) v = pos ? 1.0f : -1.0f;
+            else v = pos ? g.logd_p[pair] : g.logd_n[pair];
+            row[f] = v;
+        }
+    }
+}
+
+// Backward of k_tr_rows: dE and dtable by atomics (the geometry features are
+// constants).
+__global__ void __launch_bounds__(TT)
+    k_tr_rows_bwd(const float* __restrict__ dX, int ldx, int64_t N, int K, int d, int ds,
+                  const latec_gnn_geom g, const int32_t* __restrict__ pairs, int64_t np, int B,
+                  int two, float* __restrict__ dE, float* __restrict__ dtable) {
+    const int64_t w = ((int64_t)blockIdx.x * TT + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= (int64_t)B * np * K) return;
+    const int k = (int)(w % K);
+    const int64_t bp = w / K;
+    const int64_t p = bp % np;
+    const int b = (int)(bp / np);
+    const int pair = pairs[p];
+    const int l = pair / g.M;
+    const int de = d + ds;
+    const float* row = dX + w * ldx;
+    if (two) {
+        float* en = dE + (((int64_t)b * N + g.nbr_n[pair]) * K + k) * d;
+        float* ep = dE + (((int64_t)b * N + g.nbr_p[pair]) * K + k) * d;
+        float* sn = dtable + (int64_t)g.sidx_n[l * K + k] * ds;
+        float* sp = dtable + (int64_t)g.sidx_p[l * K + k] * ds;
+        for (int f = lane; f < 2 * de; f += 32) {
+            const float v = row[f];
+            if (f < d) atomicAdd(en + f, v);
+            else if (f < de) atomicAdd(sn + (f - d), v);
+            else if (f < de + d) atomicAdd(ep + (f - de), v);
+            else atomicAdd(sp + (f - de - d), v);
+        }
+    } else {
+        const bool pos = g.nbr_p[pair] >= 0;
+        const int64_t nb = pos ? g.nbr_p[pair] : g.nbr_n[pair];
+        float* e = dE + (((int64_t)b * N + nb) * K + k) * d;
+        float* s = dtable + (int64_t)(pos ? g.sidx_p[l * K + k] : g.sidx_n[l * K + k]) * ds;
+        for (int f = lane; f < de; f += 32) {
+            const float v = row[f];
+            if (f < d) atomicAdd(e + f, v);
+            else atomicAdd(s + (f - d), v);
+        }
+    }
+}
+
+// Candidate rows of the line pool for every (b, m, k). Message rows are laid
+// out as all two-sided rows ((b * np2 + r) * K + k), then all one-sided rows
+// (B * np2 * K + (b * np1 + r - np2) * K + k); r = row_of[l, m] (two-sided
+// rows first) or -1 (masked).
+__global__ void __launch_bounds__(TT)
+    k_tr_line_rows(const int32_t* __restrict__ row_of, int M, int L, int K, int B, int64_t np2,
+                   int64_t np1, int32_t* __restrict__ rows) {
+    const int64_t t = (int64_t)blockIdx.x * TT + threadIdx.x;
+    if (t >= (int64_t)B * M * K) return;
+    const int k = (int)(t % K);
+    const int64_t bm = t / K;
+    const int m = (int)(bm % M), b = (int)(bm / M);
+    for (int l = 0; l < L; l++) {
+        const int64_t r = row_of[(int64_t)l * M + m];
+        int64_t v = -1;
+        if (r >= 0 && r < np2) v = ((int64_t)b * np2 + r) * K + k;
+        else if (r >= np2) v = (int64_t)B * np2 * K + ((int64_t)b * np1 + (r - np2)) * K + k;
+        rows[t * L + l] = (int32_t)v;
+    }
+}
+
+// AttnPool forward with the probabilities kept: P[o, c] (c < n; 0 when
+// masked) and P[o, n] (null token). One warp per output; d <= 128.
+__global__ void __launch_bounds__(TT)
+    k_tr_attn(const float* __restrict__ key, const float* __restrict__ V, int d,
+              const int32_t* __restrict__ rows, int n, int64_t n_out, float scale,
+              const float* __restrict__ null_k, const float* __restrict__ null_v,
+              float* __restrict__ out, float* __restrict__ P) {
+    const int64_t o = ((int64_t)blockIdx.x * TT + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (o >= n_out) return;
+    const float sn = null_k[0] * scale;
+    float mx = sn;
+    for (int c = 0; c < n; c++) {
+        const int64_t r = rows ? rows[o * n + c] : o * n + c;
+        if (r >= 0) mx = fmaxf(mx, key[r] * scale);
+    }
+    float den = expf(sn - mx);
+    for (int c = 0; c < n; c++) {
+        const int64_t r = rows ? rows[o * n + c] : o * n + c;
+        if (r >= 0) den += expf(key[r] * scale - mx);
+    }
+    const float inv = 1.0f / den;
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int c = 0; c < n; c++) {
+        const int64_t r = rows ? rows[o * n + c] : o * n + c;
+        const float p = r >= 0 ? expf(key[r] * scale - mx) * inv : 0.0f;
+        if (lane == 0) P[o * (n + 1) + c] = p;
+        if (r < 0) continue;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int f = lane + 32 * q;
+            if (f < d) acc[q] += p * V[r * d + f];
+        }
+    }
+    const float pn = expf(sn - mx) * inv;
+    if (lane == 0) P[o * (n + 1) + n] = pn;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int f = lane + 32 * q;
+        if (f < d) out[o * d + f] = acc[q] + pn * null_v[f];
+    }
+}
+
+// AttnPool backward: dkey[r] = p (dot(dout, v) - sum) * scale, dV[r] = p dout
+// (each candidate row belongs to one output), null key / value by atomics.
+__global__ void __launch_bounds__(TT)
+    k_tr_attn_bwd(const float* __restrict__ V, int d, const int32_t* __restrict__ rows, int n,
+                  int64_t n_out, float scale, const float* __restrict__ null_v,
+                  const float* __restrict__ P, const float* __restrict__ dout,
+                  float* __restrict__ dkey, float* __restrict__ dV, float* __restrict__ dnull_k,
+                  float* __restrict__ dnull_v) {
+    const int64_t o = ((int64_t)blockIdx.x * TT + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (o >= n_out) return;
+    float go[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int f = lane + 32 * q;
+        go[q] = f < d ? dout[o * d + f] : 0.0f;
+    }
+    auto dot = [&](const float* v) {
+        float s = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int f = lane + 32 * q;
+            if (f < d) s += go[q] * v[f];
+        }
+#pragma unroll
+        for (int m = 16; m; m >>= 1) s += __shfl_xor_sync(0xffffffffu, s, m);
+        return s;
+    };
+    const float pn = P[o * (n + 1) + n];
+    const float dpn = dot(null_v);
+    float sum = pn * dpn;
+    for (int c = 0; c < n; c++) {
+        const int64_t r = rows ? rows[o * n + c] : o * n + c;
+        if (r < 0) continue;
+        sum += P[o * (n + 1) + c] * dot(V + r * d);
+    }
+    for (int c = 0; c < n; c++) {
+        const int64_t r = rows ? rows[o * n + c] : o * n + c;
+        if (r < 0) continue;
+        const float p = P[o * (n + 1) + c];
+        const float dp = dot(V + r * d);
+        if (lane == 0) dkey[r] = p * (dp - sum) * scale;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int f = lane + 32 * q;
+            if (f < d) dV[r * d + f] = p * go[q];
+        }
+    }
+    if (lane == 0) atomicAdd(dnull_k, pn * (dpn - sum) * scale);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int f = lane + 32 * q;
+        if (f < d) atomicAdd(&dnull_v[f], pn * go[q]);
+    }
+}
+
+// Head rows [pooled | log2 eb_b] (per-sample bound) and the readout
+// mu = sigmoid(o0), log2 b = log2 eb_b + clamp(o1, -4, 12), with its backward.
+__global__ void __launch_bounds__(TT)
+    k_tr_head_rows(const float* __restrict__ pooled, int64_t n, int per_b, int d,
+                   const float* __restrict__ log_eb, float* __restrict__ X) {
+    const int64_t t = (int64_t)blockIdx.x * TT + threadIdx.x;
+    if (t >= n * (d + 1)) return;
+    const int64_t r = t / (d + 1);
+    const int f = (int)(t % (d + 1));
+    X[t] = f < d ? pooled[r * d + f] : log_eb[r / per_b];
+}
+
+__global__ void __launch_bounds__(TT)
+    k_tr_head_out(const float* __restrict__ O, int64_t n, int per_b, const float* __restrict__ log_eb,
+                  float* __restrict__ mu, float* __restrict__ log_b) {
+    const int64_t r = (int64_t)blockIdx.x * TT + threadIdx.x;
+    if (r >= n) return;
+    mu[r] = 1.0f / (1.0f + expf(-O[2 * r]));
+    log_b[r] = log_eb[r / per_b] + fminf(fmaxf(O[2 * r + 1], -4.0f), 12.0f);
+}
+
+__global__ void __launch_bounds__(TT)
+    k_tr_head_out_bwd(const float* __restrict__ O, const float* __restrict__ mu, int64_t n,
+                      const float* __restrict__ dmu, const float* __restrict__ dlog_b,
+                      float* __restrict__ dO) {
+    const int64_t r = (int64_t)blockIdx.x * TT + threadIdx.x;
+    if (r >= n) return;
+    const float m = mu[r], z = O[2 * r + 1];
+    dO[2 * r] = dmu[r] * m * (1.0f - m);
+    dO[2 * r + 1] = (z >= -4.0f && z <= 12.0f) ? dlog_b[r] : 0.0f;
+}
+
+// Discretised-Laplace code length in bits of target under (mu, 2^log_b) with
+// the +-eb cell (train_gnn.py discretized_laplace_nll) plus mse_weight x the
+// squared prediction error; sums into acc[0] (bits), acc[1] (squared error),
+// acc[2] (|error|) and the gradients scaled by `scale` into dmu / dlog_b.
+__global__ void __launch_bounds__(TT)
+    k_tr_loss(const float* __restrict__ mu, const float* __restrict__ log_b,
+              const float* __restrict__ tgt, int64_t n, int per_b, const float* __restrict__ eb,
+              float mse_weight, float scale, float* __restrict__ dmu, float* __restrict__ dlog_b,
+              double* __restrict__ acc) {
+    const int64_t i = (int64_t)blockIdx.x * TT + threadIdx.x;
+    float bits = 0.0f, sq = 0.0f, ab = 0.0f;
+    if (i < n) {
+        const float LN2 = 0.69314718055994531f, LOG2E = 1.4426950408889634f;
+        const float e_b = eb[i / per_b];
+        const float b = fmaxf(exp2f(log_b[i]), 1.17549435e-38f);
+        const float r = tgt[i] - mu[i];
+        const float ar = fabsf(r);
+        const float rho = ar / b, e = e_b / b;
+        float dl_drho, dl_de, logp;
+        if (ar >= e_b) {
+            const float em2 = -2.0f * e;
+            const float eps = 1.1920929e-07f;
+            const bool clamped = em2 > -eps;
+            const float x2 = clamped ? -eps : em2;
+            const float tail = log1pf(-expf(x2));
+            const float dtail = clamped ? 0.0f : 2.0f * expf(x2) / (1.0f - expf(x2));
+            float t = rho - e, dt = 1.0f;
+            const float tmax = 32.0f * LN2;
+            if (t > tmax) {
+                dt = 1.0f / (1.0f + (t - tmax));
+                t = tmax + log1pf(t - tmax);
+            }
+            logp = -LN2 - t + tail;
+            dl_drho = -dt;
+            dl_de = dt + dtail;
+        } else {
+            const float a = expf(-(e - rho)), c = expf(-(e + rho));
+            const float cp = 1.0f - 0.5f * a - 0.5f * c;
+            const float ok = cp > 1e-30f ? 1.0f / cp : 0.0f;
+            logp = logf(fmaxf(cp, 1e-30f));
+            dl_drho = (-0.5f * a + 0.5f * c) * ok;
+            dl_de = (0.5f * a + 0.5f * c) * ok;
+        }
+        bits = -logp * LOG2E;
+        sq = r * r;
+        ab = ar;
+        // d(bits)/d mu: rho depends on |t - mu|; d/d log_b through rho and e
+        const float sgn = r > 0.0f ? 1.0f : (r < 0.0f ? -1.0f : 0.0f);
+        const float dbits_dmu = -LOG2E * dl_drho * (-sgn / b);
+        const float dbits_dlb = -LOG2E * (dl_drho * (-rho * LN2) + dl_de * (-e * LN2));
+        dmu[i] = scale * (dbits_dmu + mse_weight * 2.0f * (mu[i] - tgt[i]));
+        dlog_b[i] = scale * dbits_dlb;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        bits += __shfl_xor_sync(0xffffffffu, bits, o);
+        sq += __shfl_xor_sync(0xffffffffu, sq, o);
+        ab += __shfl_xor_sync(0xffffffffu, ab, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&acc[0], (double)bits);
+        atomicAdd(&acc[1], (double)sq);
+        atomicAdd(&acc[2], (double)ab);
+    }
+}
+
+// MixEmbed rows [ctx(b, m, k) | value_emb(b, m)] and backward (dctx added,
+// dvemb summed over k by atomics).
+__global__ void __launch_bounds__(TT)
+    k_tr_mix_rows(const float* __restrict__ ctx, const float* __restrict__ vemb, int64_t bmk, int K,
+                  int d, float* __restrict__ X) {
+    const int64_t t = (int64_t)blockIdx.x * TT + threadIdx.x;
+    if (t >= bmk * 2 * d) return;
+    const int64_t row = t / (2 * d);
+    const int f = (int)(t % (2 * d));
+    X[t] = f < d ? ctx[row * d + f] : vemb[(row / K) * d + (f - d)];
+}
+
+__global__ void __launch_bounds__(TT)
+    k_tr_mix_rows_bwd(const float* __restrict__ dX, int64_t bmk, int K, int d,
+                      float* __restrict__ dctx, float* __restrict__ dvemb) {
+    const int64_t t = (int64_t)blockIdx.x * TT + threadIdx.x;
+    if (t >= bmk * 2 * d) return;
+    const int64_t row = t / (2 * d);
+    const int f = (int)(t % (2 * d));
+    if (f < d) dctx[row * d + f] += dX[t];
+    else atomicAdd(&dvemb[(row / K) * d + (f - d)], dX[t]);
+}
+
+// E[b, query[m], k, :] = Y[(b M + m) K + k, :] and its backward dY = dE[...].
+__global__ void __launch_bounds__(TT)
+    k_tr_scatter_e(const float* __restrict__ Y, const int32_t* __restrict__ query, int B, int M,
+                   int K, int d, int64_t N, float* __restrict__ E, int backward) {
+    const int64_t t = (int64_t)blockIdx.x * TT + threadIdx.x;
+    if (t >= (int64_t)B * M * K * d) return;
+    const int f = (int)(t % d);
+    const int64_t row = t / d;
+    const int k = (int)(row % K);
+    const int64_t bm = row / K;
+    const int m = (int)(bm % M), b = (int)(bm / M);
+    const int64_t e = (((int64_t)b * N + query[m]) * K + k) * d + f;
+    if (backward) ((float*)Y)[t] = E[e];
+    else E[e] = Y[t];
+}
+
+// AdamW (decoupled weight decay) and the EMA of the weights.
+__global__ void __launch_bounds__(TT)
+    k_adamw(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+            float* __restrict__ v, int64_t n, float lr, float b1, float b2, float eps, float wd,
+            float c1, float c2) {
+    const int64_t i = (int64_t)blockIdx.x * TT + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    float pi = p[i] * (1.0f - lr * wd);
+    pi -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    p[i] = pi;
+}
+
+__global__ void __launch_bounds__(TT)
+    k_ema(float* __restrict__ shadow, const float* __restrict__ p, int64_t n, float decay) {
+    const int64_t i = (int64_t)blockIdx.x * TT + threadIdx.x;
+    if (i < n) shadow[i] = shadow[i] * decay + p[i] * (1.0f - decay);
+}
+
+int done(int n) {
+    count_launches((unsigned)n);
+    return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
+}
+
+}  // namespace
+}  // namespace latec
+
+using namespace latec;
+
+extern "C" {
+
+// Y = act(X W^T + b) (act 1 = GELU); Z (optional) keeps the pre-activation.
+int latec_tr_linear(const float* X, int64_t ldx, int64_t rows, int32_t in, const float* W,
+                    const float* b, int32_t out, float* Y, int64_t ldy, int32_t act, float* Z,
+                    void* stream) {
+    if (rows < 0 || in < 1 || out < 1 || !W || (rows && (!X || !Y)) || rows > 0x7fffffff)
+        return LATEC_ERR_ARG;
+    if (!rows) return LATEC_OK;
+    dim3 grid((unsigned)((rows + GM - 1) / GM), (unsigned)((out + GN - 1) / GN), 1);
+    k_gemm<0, 1, 0, 0><<<grid, TT, 0, (cudaStream_t)stream>>>(
+        (int)rows, out, in, X, ldx, W, in, nullptr, Y, ldy, b, act, Z, ldy);
+    return done(1);
+}
+
+// Backward of latec_tr_linear. dY (rows, ldy); Z = the saved pre-activation
+// when act (same ld as dY). dX (optional) = dZ W is stored, or added when
+// accum_dx; dW (out, in) and db (out) are accumulated.
+int latec_tr_linear_bwd(const float* X, int64_t ldx, int64_t rows, int32_t in, const float* W,
+                        int32_t out, const float* dY, int64_t ldy, const float* Z, int32_t act,
+                        float* dX, int64_t lddx, int32_t accum_dx, float* dW, float* db,
+                        void* stream) {
+    if (rows < 0 || in < 1 || out < 1 || !W || !dW || !db || (act && !Z) ||
+        (rows && (!X || !dY)) || rows > 0x7fffffff)
+        return LATEC_ERR_ARG;
+    if (!rows) return LATEC_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const float* Zg = act ? Z : nullptr;
+    int n = 0;
+    if (dX) {
+        dim3 grid((unsigned)((rows + GM - 1) / GM), (unsigned)((in + GN - 1) / GN), 1);
+        if (act) {
+            if (accum_dx)
+                k_gemm<0, 0, 1, 1><<<grid, TT, 0, st>>>((int)rows, in, out, dY, ldy, W, in, Zg, dX,
+                                                        lddx, nullptr, 0, nullptr, 0);
+            else
+                k_gemm<0, 0, 1, 0><<<grid, TT, 0, st>>>((int)rows, in, out, dY, ldy, W, in, Zg, dX,
+                                                        lddx, nullptr, 0, nullptr, 0);
+        } else {
+            if (accum_dx)
+                k_gemm<0, 0, 0, 1><<<grid, TT, 0, st>>>((int)rows, in, out, dY, ldy, W, in, nullptr,
+                                                        dX, lddx, nullptr, 0, nullptr, 0);
+            else
+                k_gemm<0, 0, 0, 0><<<grid, TT, 0, st>>>((int)rows, in, out, dY, ldy, W, in, nullptr,
+                                                        dX, lddx, nullptr, 0, nullptr, 0);
+        }
+        n++;
+    }
+    // dW[j, i] += sum_r dZ[r, j] X[r, i]: split over rows
+    const unsigned splits = (unsigned)std::min<int64_t>(256, (rows + 4095) / 4096);
+    dim3 gw((unsigned)((out + GM - 1) / GM), (unsigned)((in + GN - 1) / GN), splits ? splits : 1);
+    if (act)
+        k_gemm<1, 0, 1, 1><<<gw, TT, 0, st>>>(out, in, (int)rows, dY, ldy, X, ldx, Zg, dW, in,
+                                              nullptr, 0, nullptr, 0);
+    else
+        k_gemm<1, 0, 0, 1><<<gw, TT, 0, st>>>(out, in, (int)rows, dY, ldy, X, ldx, nullptr, dW, in,
+                                              nullptr, 0, nullptr, 0);
+    dim3 gb((unsigned)std::min<int64_t>(1024, (rows + TT - 1) / TT), (unsigned)out, 1);
+    k_colsum<<<gb, TT, 0, st>>>(rows, out, dY, ldy, Zg, db);
+    return done(n + 2);
+}
+
+int latec_tr_rows(const float* E, int64_t N, int32_t K, int32_t d, int32_t ds, const float* table,
+                  const latec_gnn_geom* geom, const int32_t* pairs, int64_t np, int32_t B,
+                  int32_t two, float* X, int32_t ldx, void* stream) {
+    if (!E || !table || !geom || np < 0 || B < 1 || (np && (!pairs || !X)) || d > 128)
+        return LATEC_ERR_ARG;
+    if (!np) return LATEC_OK;
+    k_tr_rows<<<tblocks((int64_t)B * np * K * 32), TT, 0, (cudaStream_t)stream>>>(
+        E, N, K, d, ds, table, *geom, pairs, np, B, two, X, ldx);
+    return done(1);
+}
+
+int latec_tr_rows_bwd(const float* dX, int32_t ldx, int64_t N, int32_t K, int32_t d, int32_t ds,
+                      const latec_gnn_geom* geom, const int32_t* pairs, int64_t np, int32_t B,
+                      int32_t two, float* dE, float* dtable, void* stream) {
+    if (!geom || np < 0 || B < 1 || (np && (!pairs || !dX || !dE || !dtable)))
+        return LATEC_ERR_ARG;
+    if (!np) return LATEC_OK;
+    k_tr_rows_bwd<<<tblocks((int64_t)B * np * K * 32), TT, 0, (cudaStream_t)stream>>>(
+        dX, ldx, N, K, d, ds, *geom, pairs, np, B, two, dE, dtable);
+    return done(1);
+}
+
+int latec_tr_line_rows(const int32_t* row_of, int32_t M, int32_t L, int32_t K, int32_t B,
+                       int64_t np2, int64_t np1, int32_t* rows, void* stream) {
+    if (!row_of || !rows || M < 0 || L < 1 || K < 1 || B < 1 || np2 < 0 || np1 < 0 ||
+        (int64_t)B * (np2 + np1) * K > 0x7fffffffLL)
+        return LATEC_ERR_ARG;
+    if (!M) return LATEC_OK;
+    k_tr_line_rows<<<tblocks((int64_t)B * M * K), TT, 0, (cudaStream_t)stream>>>(row_of, M, L, K, B,
+                                                                                 np2, np1, rows);
+    return done(1);
+}
+
+int latec_tr_attn(const float* key, const float* V, int32_t d, const int32_t* rows, int32_t n,
+                  int64_t n_out, float scale, const float* null_k, const float* null_v, float* out,
+                  float* P, void* stream) {
+    if (!key || !V || !null_k || !null_v || !out || !P || d < 1 || d > 128 || n < 1 || n_out < 0)
+        return LATEC_ERR_ARG;
+    if (!n_out) return LATEC_OK;
+    k_tr_attn<<<tblocks(n_out * 32), TT, 0, (cudaStream_t)stream>>>(key, V, d, rows, n, n_out, scale,
+                                                                   null_k, null_v, out, P);
+    return done(1);
+}
+
+int latec_tr_attn_bwd(const float* V, int32_t d, const int32_t* rows, int32_t n, int64_t n_out,
+                      float scale, const float* null_v, const float* P, const float* dout,
+                      float* dkey, float* dV, float* dnull_k, float* dnull_v, void* stream) {
+    if (!V || !null_v || !P || !dout || !dkey || !dV || !dnull_k || !dnull_v || d < 1 || d > 128 ||
+        n < 1 || n_out < 0)
+        return LATEC_ERR_ARG;
+    if (!n_out) return LATEC_OK;
+    k_tr_attn_bwd<<<tblocks(n_out * 32), TT, 0, (cudaStream_t)stream>>>(
+        V, d, rows, n, n_out, scale, null_v, P, dout, dkey, dV, dnull_k, dnull_v);
+    return done(1);
+}
+
+int latec_tr_head_rows(const float* pooled, int64_t n, int32_t per_b, int32_t d,
+                       const float* log_eb, float* X, void* stream) {
+    if (!pooled || !log_eb || !X || n < 0 || per_b < 1) return LATEC_ERR_ARG;
+    if (!n) return LATEC_OK;
+    k_tr_head_rows<<<tblocks(n * (d + 1)), TT, 0, (cudaStream_t)stream>>>(pooled, n, per_b, d,
+                                                                         log_eb, X);
+    return done(1);
+}
+
+int latec_tr_head_out(const float* O, int64_t n, int32_t per_b, const float* log_eb, float* mu,
+                      float* log_b, void* stream) {
+    if (!O || !log_eb || !mu || !log_b || n < 0 || per_b < 1) return LATEC_ERR_ARG;
+    if (!n) return LATEC_OK;
+    k_tr_head_out<<<tblocks(n), TT, 0, (cudaStream_t)stream>>>(O, n, per_b, log_eb, mu, log_b);
+    return done(1);
+}
+
+int latec_tr_head_out_bwd(const float* O, const float* mu, int64_t n, const float* dmu,
+                          const float* dlog_b, float* dO, void* stream) {
+    if (!O || !mu || !dmu || !dlog_b || !dO || n < 0) return LATEC_ERR_ARG;
+    if (!n) return LATEC_OK;
+    k_tr_head_out_bwd<<<tblocks(n), TT, 0, (cudaStream_t)stream>>>(O, mu, n, dmu, dlog_b, dO);
+    return done(1);
+}
+
+int latec_tr_loss(const float* mu, const float* log_b, const float* tgt, int64_t n, int32_t per_b,
+                  const float* eb, float mse_weight, float scale, float* dmu, float* dlog_b,
+                  double* acc, void* stream) {
+    if (!mu || !log_b || !tgt || !eb || !dmu || !dlog_b || !acc || n < 0 || per_b < 1)
+        return LATEC_ERR_ARG;
+    if (!n) return LATEC_OK;
+    k_tr_loss<<<tblocks(n), TT, 0, (cudaStream_t)stream>>>(mu, log_b, tgt, n, per_b, eb, mse_weight,
+                                                          scale, dmu, dlog_b, acc);
+    return done(1);
+}
+
+int latec_tr_mix_rows(const float* ctx, const float* vemb, int64_t bmk, int32_t K, int32_t d,
+                      float* X, void* stream) {
+    if (!ctx || !vemb || !X || bmk < 0 || K < 1) return LATEC_ERR_ARG;
+    if (!bmk) return LATEC_OK;
+    k_tr_mix_rows<<<tblocks(bmk * 2 * d), TT, 0, (cudaStream_t)stream>>>(ctx, vemb, bmk, K, d, X);
+    return done(1);
+}
+
+int latec_tr_mix_rows_bwd(const float* dX, int64_t bmk, int32_t K, int32_t d, float* dctx,
+                          float* dvemb, void* stream) {
+    if (!dX || !dctx || !dvemb || bmk < 0 || K < 1) return LATEC_ERR_ARG;
+    if (!bmk) return LATEC_OK;
+    k_tr_mix_rows_bwd<<<tblocks(bmk * 2 * d), TT, 0, (cudaStream_t)stream>>>(dX, bmk, K, d, dctx,
+                                                                            dvemb);
+    return done(1);
+}
+
+// backward = 0: E[query] = Y; backward = 1: Y = dE[query] (Y is then written).
+int latec_tr_scatter_e(float* Y, const int32_t* query, int32_t B, int32_t M, int32_t K, int32_t d,
+                       int64_t N, float* E, int32_t backward, void* stream) {
+    if (!Y || !query || !E || B < 1 || M < 0 || K < 1) return LATEC_ERR_ARG;
+    if (!M) return LATEC_OK;
+    k_tr_scatter_e<<<tblocks((int64_t)B * M * K * d), TT, 0, (cudaStream_t)stream>>>(
+        Y, query, B, M, K, d, N, E, backward);
+    return done(1);
+}
+
+int latec_tr_adamw(float* p, const float* g, float* m, float* v, int64_t n, float lr, float b1,
+                   float b2, float eps, float wd, int64_t step, void* stream) {
+    if (!p || !g || !m || !v || n < 0 || step < 1) return LATEC_ERR_ARG;
+    if (!n) return LATEC_OK;
+    const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+    k_adamw<<<tblocks(n), TT, 0, (cudaStream_t)stream>>>(p, g, m, v, n, lr, b1, b2, eps, wd, c1, c2);
+    return done(1);
+}
+
+int latec_tr_ema(float* shadow, const float* p, int64_t n, float decay, void* stream) {
+    if (!shadow || !p || n < 0) return LATEC_ERR_ARG;
+    if (!n) return LATEC_OK;
+    k_ema<<<tblocks(n), TT, 0, (cudaStream_t)stream>>>(shadow, p, n, decay);
+    return done(1);
+}
+
+}  // extern "C"
