@@ -207,24 +207,26 @@ def cpu_baseline(steps=1):
 TRAFFIC_PER_PASS = 4.155e9
 
 GNN_SHAPE = (32, 32, 32, 32)
+GNN_CKPT = os.path.join(ROOT, "latec_b200", "checkpoints", "gnn_d64_agg1_synthetic.pt")
 GNN_EB, GNN_LEVELS = 1e-3, 4
 
 
 def gnn_leg(dev, steps=2):
     """Learned codec beside the plain one on one 32^4 chunk of the 4-D mixed
     field (0.5 anisotropic GRF + 0.5 turbulence+jumps; the reference's auto
-    chunk of a 128x128x64x64 tensor), absolute eb 1e-3, levels 4, seeded
-    random GNN weights (no trained checkpoint is available on the box).
+    chunk of a 128x128x64x64 tensor), absolute eb 1e-3, levels 4, with the
+    checkpoint trained by latec_b200.train on synthetic fields
+    (latec_b200/checkpoints/gnn_d64_agg1_synthetic.pt).
     Wall time of compress + decompress through the public API with the field
     on the device."""
     import torch
 
     import latec_b200 as lb
-    from latec_b200 import fields, gnn
+    from latec_b200 import fields
 
     x = fields.mixed_4d(GNN_SHAPE, seed=3, device=dev)
     span = float(x.max().item()) - float(x.min().item())
-    codec = lb.GNNCodec(weights=gnn.random_weights(0, 64, 1), d=64, agg_level=1, device=dev)
+    codec = lb.GNNCodec(checkpoint_path=GNN_CKPT, device=dev)
     rel = GNN_EB / span
     s = codec.compress(x, rel, levels=GNN_LEVELS)  # warm-up (geometry, tables)
     codec.uncompress(s)
@@ -247,7 +249,9 @@ def gnn_leg(dev, steps=2):
                         levels=GNN_LEVELS, anchor_stride=16, recon="none")
     nbytes = x.numel() * 4
     return {"workload": "one 32^4 chunk of the 4-D mixed field, abs eb 1e-3, levels 4",
-            "weights": "seeded random initialisation (untrained)",
+            "weights": "trained with latec_b200.train (hand-written forward/backward kernels), "
+                       "797 AdamW steps of 16^4 x 4 + 128^2 x 16 synthetic fields; "
+                       "latec_b200/checkpoints/gnn_d64_agg1_synthetic.pt",
             "ratio_gnn": nbytes / len(s), "ratio_interp": nbytes / len(si),
             "compress_gbs": nbytes * steps / (t1 - t0) / 1e9,
             "decompress_gbs": nbytes * steps / (t2 - t1) / 1e9,
