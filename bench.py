@@ -64,16 +64,20 @@ except Exception:
     h = pynvml.nvmlDeviceGetHandleByIndex(int(sys.argv[2]))
 mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
 print("ready", flush=True)
-sys.stdin.readline()
 rows = []
-while True:
-    try:
-        rows.append((pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM), mx,
-                     int(pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(h))))
-    except Exception:
-        pass
-    if select.select([sys.stdin], [], [], 0.002)[0]:
-        break
+cmd = sys.stdin.readline().strip()
+while cmd == "go":  # sample until "pause" or "stop"; "go" again resumes
+    while True:
+        try:
+            rows.append((pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM), mx,
+                         int(pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(h))))
+        except Exception:
+            pass
+        if select.select([sys.stdin], [], [], 0.002)[0]:
+            cmd = sys.stdin.readline().strip()
+            break
+    if cmd == "pause":
+        cmd = sys.stdin.readline().strip()
 print(json.dumps(rows), flush=True)
 """
 
@@ -119,8 +123,7 @@ class ClockSampler:
 
     def __enter__(self):
         if self.child is not None:
-            self.child.stdin.write("go\n")
-            self.child.stdin.flush()
+            self._send("go")
             return self
         q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -134,6 +137,22 @@ class ClockSampler:
         except Exception:
             self.proc = None
         return self
+
+    def _send(self, cmd):
+        try:
+            self.child.stdin.write(cmd + "\n")
+            self.child.stdin.flush()
+        except Exception:
+            pass
+
+    def pause(self):
+        """Stop sampling between timed regions (NVML child only)."""
+        if self.child is not None:
+            self._send("pause")
+
+    def resume(self):
+        if self.child is not None:
+            self._send("go")
 
     def _smi_read(self):
         bits = [0x8, 0x40, 0x20, 0x4]
@@ -477,23 +496,26 @@ def main():
         dist.barrier()
     l0 = lib.latec_launch_count()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # clocks sampled during both timed regions (device-resident and end to
+    # end), paused in between
     sampler = ClockSampler(local)  # NVML set-up before the timed region
-    with sampler:
-        ev0.record()
-        tc = td = 0.0
-        for _ in range(args.steps):
-            a = time.perf_counter()
-            stream, st = lb.compress(x, eb, pred(), levels=LEVELS, anchor_stride=STRIDE,
-                                     recon="none", stream_out="device")
-            b = time.perf_counter()
-            out = lb.decompress(stream, out="device")
-            torch.cuda.synchronize()
-            c = time.perf_counter()
-            tc += b - a
-            td += c - b
-            del out
-        ev1.record()
+    sampler.__enter__()
+    ev0.record()
+    tc = td = 0.0
+    for _ in range(args.steps):
+        a = time.perf_counter()
+        stream, st = lb.compress(x, eb, pred(), levels=LEVELS, anchor_stride=STRIDE,
+                                 recon="none", stream_out="device")
+        b = time.perf_counter()
+        out = lb.decompress(stream, out="device")
         torch.cuda.synchronize()
+        c = time.perf_counter()
+        tc += b - a
+        td += c - b
+        del out
+    ev1.record()
+    torch.cuda.synchronize()
+    sampler.pause()
     launches = lib.latec_launch_count() - l0
     ms = ev0.elapsed_time(ev1) / args.steps
     if world > 1:
@@ -583,6 +605,7 @@ def main():
         back = lb.decompress(s_e)
     del back
     torch.cuda.synchronize()
+    sampler.resume()
     t0 = time.perf_counter()
     e_steps = max(1, args.steps)
     for _ in range(e_steps):
@@ -591,6 +614,7 @@ def main():
         back = lb.decompress(s_e)
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / e_steps
+    sampler.__exit__(None, None, None)
     if world > 1:
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

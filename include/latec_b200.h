@@ -380,6 +380,22 @@ const char* latec_version(void);
 /* Number of CUDA kernel launches this library has issued in this process. */
 uint64_t latec_launch_count(void);
 
+/* ---- scale-gated interpolation fallback of the learned codec
+ *      (latec/gnn_codec.py:386-462, 776-1000). latec_gate_costs adds, per
+ *      scale bucket (the number of thresholds eb * 2^T, T = 2..13, below the
+ *      model scale b), the rANS-aligned Laplace bits of the GNN residual
+ *      (row 0) and of each candidate ip0..ip2 (cubic, first-axis linear,
+ *      last-axis linear; NULL = skipped) at scale b * 2^-2s, s = 0..3 (row
+ *      1 + 4 k + s), into sums (13 x 13, 2^-20-bit fixed point, zeroed by the
+ *      caller). thr / grid: the 64-level scale grid (63 float32 boundaries,
+ *      64 float64 values). latec_gate_apply replaces mu by ip and b by
+ *      b * 2^-shift where b < eb * 2^T (high = 0) or b >= eb * 2^T (high = 1). */
+int latec_gate_costs(int64_t n, const float* x, const float* mu, const float* ip0,
+                     const float* ip1, const float* ip2, const float* b, double eb, int32_t radius,
+                     const float* thr, const double* grid, uint64_t* sums, void* stream);
+int latec_gate_apply(int64_t n, float* mu, float* b, const float* ip, double eb, int32_t T,
+                     int32_t shift, int32_t high, void* stream);
+
 /* ---- training of the learned predictor (scripts/train_gnn.py): forward
  *      ops that keep what their backward needs, the backward ops, the
  *      discretised-Laplace rate loss and the AdamW / EMA updates. float32;

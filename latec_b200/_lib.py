@@ -118,6 +118,8 @@ SIGNATURES = {
                                        ctypes.POINTER(GnnGeom), P, P, U64, P]),
     "latec_gnn_head": (ctypes.c_int, [ctypes.POINTER(GnnModel), I32, I32, I32, P,
                                       ctypes.c_float, P, P, P, U64, P]),
+    "latec_gate_costs": (ctypes.c_int, [I64, P, P, P, P, P, P, D, I32, P, P, P, P]),
+    "latec_gate_apply": (ctypes.c_int, [I64, P, P, P, D, I32, I32, I32, P]),
     "latec_tr_linear": (ctypes.c_int, [P, I64, I64, I32, P, P, I32, P, I64, I32, P, P]),
     "latec_tr_linear_bwd": (ctypes.c_int, [P, I64, I64, I32, P, I32, P, I64, P, I32, P, I64, I32,
                                            P, P, P]),

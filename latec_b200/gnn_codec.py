@@ -26,7 +26,14 @@ The decoder repeats the same float path and dequantizes on the device.
 Scope of this version:
 
 * The whole tensor is one region: no chunk grid and no halos.
-* There is no interpolation gate: every stage uses the GNN.
+* The scale-gated interpolation fallback (``gate=True``, the default) is
+  chosen per stage: the encoder scores the GNN against the cubic,
+  first-axis-linear and last-axis-linear interpolation of the stage's points
+  with the reference's rANS-aligned Laplace rate, per bucket of the model's
+  scale relative to eb * 2^T (``latec/gnn_codec.py:386-462, 920-1000``), and
+  keeps the GNN only where it codes fewer bits. One gate word per stage, in
+  the reference's bit layout, travels in the header. ``gate_fine`` selects the
+  same per-stage gate (there is no chunk grid to share a word across).
 * Float inputs only.
 * ``fp16=True`` (the default, as in the reference) runs the message and
   finalisation MLPs in BF16 on the tensor cores (tcgen05) with float32
@@ -60,6 +67,15 @@ RANK_LEVELS = {2: 8, 4: 5, 5: 4}
 EB_COARSE_FACTOR = 0.9
 EB_COARSE_SWEEP = (1.0, 0.9, 0.65, 0.41)
 INTERP_KINDS = {"interp-cubic": 1, "interp-linear-first": 2, "interp-linear-last": 3}
+# gate sweep (latec/gnn_codec.py:399-403): thresholds eb * 2^T, scale shifts,
+# and the word layout dir (bit 10) | kind (bits 8-9) | T (bits 4-7) | shift
+GATE_T = tuple(range(2, 14))
+GATE_SHIFTS = (0, 2, 4, 6)
+GATE_DIR_SHIFT = 10
+GATE_END_MODE = 3  # quadratic ends and extrapolation past the line end
+# candidate k: (order, center) of the interpolation predictor
+GATE_KINDS = {1: (1, 0), 2: (0, 1), 3: (0, 2)}
+_GATE_GRIDS: dict = {}
 
 
 def _torch():
@@ -114,6 +130,83 @@ def read_stream(stream: bytes):
 def _qparams(radius):
     return _lib.QuantParams(dtype=_lib.F32, channels=1, radius=int(radius), order=1, center=0,
                             end_mode=1, round_output=0, reserved=0)
+
+
+def gate_scale_grid(eb: float, device):
+    """The gate's 64-level log scale grid for bound eb (``_gate_scale_thresholds``,
+    latec/gnn_codec.py:876-917): float32 level boundaries found by bisection
+    over positive float32 bit patterns, and the float64 grid values."""
+    import numpy as _np
+
+    torch = _torch()
+    key = (str(device), float(eb))
+    hit = _GATE_GRIDS.get(key)
+    if hit is not None:
+        return hit
+    from .rans_model import SCALE_HI_MULT, SCALE_LO_DIV
+
+    lo_f, hi_f = float(eb) / SCALE_LO_DIV, float(eb) * SCALE_HI_MULT
+    log_lo = _np.log(lo_f)
+    log_step = (_np.log(hi_f) - log_lo) / 63.0
+    targets = _np.arange(1, 64)
+    lo = _np.zeros(63, _np.uint32)
+    hi = _np.full(63, _np.asarray(_np.float32(hi_f)).view(_np.uint32), _np.uint32)
+    while _np.any(lo < hi):
+        mid = lo + (hi - lo) // 2
+        v = mid.view(_np.float32).astype(_np.float64)
+        level = _np.rint((_np.log(_np.clip(v, lo_f, hi_f)) - log_lo) / log_step)
+        up = level >= targets
+        hi = _np.where(up, mid, hi).astype(_np.uint32)
+        lo = _np.where(up, lo, mid + 1).astype(_np.uint32)
+    thr = torch.from_numpy(_np.ascontiguousarray(lo.view(_np.float32))).to(device)
+    grid = torch.from_numpy(_np.exp(log_lo + log_step * _np.arange(64))).to(device)
+    _GATE_GRIDS[key] = (thr, grid)
+    return thr, grid
+
+
+def gate_choose(sums) -> tuple[int, int, int, int]:
+    """(kind, dir, T, shift) from the per-bucket rate sums (rows: GNN, then
+    candidate k x shift; columns: scale buckets), the split rule of
+    ``_gate_select_t`` (latec/gnn_codec.py:920-971): a low-side split falls
+    back where b < eb 2^T, a high-side split where b >= eb 2^T; kind 0 = the
+    GNN everywhere (no split codes fewer bits)."""
+    W = np.asarray(sums, np.float64).reshape(1 + 3 * len(GATE_SHIFTS), len(GATE_T) + 1)
+    cums = np.cumsum(W, axis=1)
+    base = cums[0]
+    tot = base[-1]
+    ci = cums[1:]
+    low = tot - base[:-1] + ci[:, :-1]
+    high = base[:-1] + (ci[:, -1:] - ci[:, :-1])
+    costs = np.concatenate([low, high]).reshape(-1)
+    fi = int(np.argmin(costs))
+    if not costs[fi] < tot:
+        return 0, 0, 0, 0
+    ncol, nsh = len(GATE_T), len(GATE_SHIFTS)
+    n_side = 3 * nsh
+    row = fi // ncol
+    side_row = row % n_side
+    return side_row // nsh + 1, int(row >= n_side), GATE_T[fi % ncol], GATE_SHIFTS[side_row % nsh]
+
+
+def gate_word(kind, direction, T, shift) -> int:
+    return (int(direction) << GATE_DIR_SHIFT) | (int(kind) << 8) | (int(T) << 4) | int(shift)
+
+
+def gate_fields(word: int) -> tuple[int, int, int, int]:
+    return (word >> 8) & 3, (word >> GATE_DIR_SHIFT) & 1, (word >> 4) & 15, word & 15
+
+
+def pack_gates(words) -> str:
+    """Gate words as base64 of little-endian uint16 (``_pack_gates``)."""
+    import base64
+
+    return base64.b64encode(np.asarray(words, "<u2").tobytes()).decode("ascii")
+
+
+def unpack_gates(blob: str) -> list:
+    import base64
+
+    return np.frombuffer(base64.b64decode(blob), "<u2").astype(np.int64).tolist()
 
 
 class GNNCodec:
@@ -246,13 +339,14 @@ class GNNCodec:
         reduced = bool(fp16) and self.d == 64
         model = self._model(reduced)
         for ratio in ratios:
-            payload = self._encode(model, xn, shape, lv, eb, ratio, radius)
+            payload, words = self._encode(model, xn, shape, lv, eb, ratio, radius, bool(gate))
             meta = {"shape": list(original_shape), "dtype": np_dtype.str, "error_bound": eb,
                     "levels": lv, "radius": radius, "vmin": vmin, "vmax": vmax,
                     "eb_ratio": ratio, "checkpoint_hash": self.checkpoint_hash.hex(),
                     "chunks": list(edges), "m_tile": 1 << 16, "fp16": reduced, "compiled": False,
                     "predictor": "gnn", "float_path": FLOAT_PATHS[reduced], "d": self.d,
-                    "agg_level": self.agg_level}
+                    "agg_level": self.agg_level, "gate": bool(gate), "gate_fine": bool(gate_fine),
+                    "gates": pack_gates(words)}
             if int(model.tc_err.item()):
                 raise RuntimeError("a tensor-core wait ran out during the GNN forward")
             stream = write_stream(meta, payload, zstd_level)
@@ -260,21 +354,69 @@ class GNNCodec:
                 best = stream
         return best
 
-    def _encode(self, model, xn, shape, levels, eb, ratio, radius):
+    def _plan_stages(self, shape, levels):
+        """The interpolation plan of the schedule and its stage index per
+        non-empty GNN stage."""
+        from .levels import plan_for
+
+        plan = plan_for(shape, levels, 1 << levels, 1)
+        return plan, [t for t, n in enumerate(plan.counts) if n]
+
+    def _gate_candidate(self, plan, stage, kind, recon_all, n, radius):
+        """Interpolation candidate ``kind`` (1 cubic axis-average, 2 first-axis
+        linear, 3 last-axis linear) of a stage from the reconstruction."""
+        import ctypes
+
+        torch = _torch()
+        order, center = GATE_KINDS[kind]
+        out = torch.empty(n, dtype=torch.float32, device=self.device)
+        prm = _lib.QuantParams(dtype=_lib.F32, channels=1, radius=int(radius), order=order,
+                               center=center, end_mode=GATE_END_MODE, round_output=0, reserved=0)
+        _lib.check(_lib.load().latec_interp_predict_stage(plan.handle, stage, ctypes.byref(prm),
+                                                          recon_all.data_ptr(), out.data_ptr(),
+                                                          _lib.stream_ptr()),
+                   "latec_interp_predict_stage")
+        return out
+
+    def _encode(self, model, xn, shape, levels, eb, ratio, radius, gate=True):
         torch = _torch()
         lib = _lib.load()
         geoms = self._geometry(shape, levels)
         ebs = self._stage_ebs(shape, levels, eb, ratio)
+        plan, pstages = self._plan_stages(shape, levels)
         prm = _qparams(radius)
         dev = self.device
         E = torch.zeros((1, xn.numel(), len(shape), self.d), dtype=torch.float32, device=dev)
-        records, prev, ctx, vals = [], None, None, None
-        for g, seb in zip(geoms, ebs):
+        recon_all = torch.zeros(xn.numel(), dtype=torch.float32, device=dev)
+        records, words, prev, ctx, vals = [], [], None, None, None
+        for gi, (g, seb) in enumerate(zip(geoms, ebs)):
             (mu, lb), E, ctx = gnn.stage_forward(model, E, prev, g, vals, finalize_ctx=ctx,
                                                  eb=seb)
             mu = mu.reshape(-1).contiguous()
+            scale = torch.exp2(lb.reshape(-1)).contiguous()
             xs = xn[g.query_idx].contiguous()
             n = g.M
+            word = 0
+            if gate and gi > 0 and n:
+                # the interpolation fallback: score, choose, apply (on the device)
+                ips = [self._gate_candidate(plan, pstages[gi], k, recon_all, n, radius)
+                       for k in (1, 2, 3)]
+                sums = torch.zeros(len(GATE_KINDS) * len(GATE_SHIFTS) * (len(GATE_T) + 1)
+                                   + len(GATE_T) + 1, dtype=torch.int64, device=dev)
+                thr, grid = gate_scale_grid(seb, dev)
+                _lib.check(lib.latec_gate_costs(n, xs.data_ptr(), mu.data_ptr(), ips[0].data_ptr(),
+                                                ips[1].data_ptr(), ips[2].data_ptr(),
+                                                scale.data_ptr(), seb, radius, thr.data_ptr(),
+                                                grid.data_ptr(), sums.data_ptr(),
+                                                _lib.stream_ptr()), "latec_gate_costs")
+                kind, direction, T, shift = gate_choose(sums.cpu().numpy())
+                if kind:
+                    _lib.check(lib.latec_gate_apply(n, mu.data_ptr(), scale.data_ptr(),
+                                                    ips[kind - 1].data_ptr(), seb, T, shift,
+                                                    direction, _lib.stream_ptr()),
+                               "latec_gate_apply")
+                word = gate_word(kind, direction, T, shift)
+            words.append(word)
             codes = torch.empty(n, dtype=torch.int16, device=dev)
             recon = torch.empty(n, dtype=torch.float32, device=dev)
             outl = torch.empty(n, dtype=torch.float32, device=dev)
@@ -290,7 +432,6 @@ class GNNCodec:
                        "latec_quantize")
             st = _lib.StageStats.from_buffer_copy(stats.cpu().numpy().tobytes())
             kexp = max(1, int(st.maxq).bit_length())
-            scale = torch.exp2(lb.reshape(-1))
             lv64 = rans.scale_to_level(scale, seb)
             tables = rans.build_laplace_tables(seb, radius)
             codes_u = codes.view(torch.int16)
@@ -301,8 +442,9 @@ class GNNCodec:
             frame = bitstream.pack_frame(len(blob), kexp, shape_id, 0, 0, False)
             records.append(struct.pack("<IQ", n, frame) + blob + struct.pack("<I", n_out)
                            + outl[:n_out].cpu().numpy().astype("<f4").tobytes())
+            recon_all[g.query_idx] = recon
             prev, vals = g, recon.reshape(1, -1)
-        return b"".join(records)
+        return b"".join(records), words
 
     # ---------------------------------------------------------------- decode
     def uncompress(self, stream):
@@ -332,7 +474,11 @@ class GNNCodec:
         E = torch.zeros((1, N, len(shape), self.d), dtype=torch.float32, device=dev)
         off, prev, ctx, vals = 0, None, None, None
         err = torch.zeros(1, dtype=torch.int32, device=dev)
-        for g, seb in zip(geoms, ebs):
+        words = unpack_gates(meta["gates"]) if meta.get("gates") else [0] * len(geoms)
+        if len(words) != len(geoms):
+            raise ValueError("gate words do not match the stage schedule")
+        plan, pstages = self._plan_stages(shape, levels)
+        for gi, (g, seb) in enumerate(zip(geoms, ebs)):
             (mu, lb), E, ctx = gnn.stage_forward(model, E, prev, g, vals, finalize_ctx=ctx,
                                                  eb=seb)
             mu = mu.reshape(-1).contiguous()
@@ -351,7 +497,16 @@ class GNNCodec:
             outl = np.frombuffer(payload, "<f4", count=n_out, offset=off) if n_out else \
                 np.zeros(1, np.float32)
             off += 4 * n_out
-            lv64 = rans.scale_to_level(torch.exp2(lb.reshape(-1)), seb)
+            scale = torch.exp2(lb.reshape(-1)).contiguous()
+            kind, direction, T, shift = gate_fields(int(words[gi]))
+            if kind:
+                if gi == 0 or kind not in GATE_KINDS:
+                    raise ValueError("invalid gate word")
+                ip = self._gate_candidate(plan, pstages[gi], kind, recon_all, n, radius)
+                _lib.check(lib.latec_gate_apply(n, mu.data_ptr(), scale.data_ptr(), ip.data_ptr(),
+                                                seb, T, shift, direction, _lib.stream_ptr()),
+                           "latec_gate_apply")
+            lv64 = rans.scale_to_level(scale, seb)
             tables = rans.build_laplace_tables(seb, radius)
             codes = rans.rans_decode(blob, lv64, tables, kexp=f["kexp"], shape=f["shape"],
                                      mode="native")

@@ -145,3 +145,27 @@ def test_gnn_codec_float64_and_errors():
         codec.compress(x, 1e-3, levels=3, chunk_size=8)
     with pytest.raises(FileNotFoundError):
         GNNCodec("/nonexistent/checkpoint.pt")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,levels", [((64, 60), 4), ((24, 22, 20), 3), ((12, 12, 10, 10), 2)])
+def test_gate_falls_back_to_interpolation_where_it_codes_fewer_bits(shape, levels):
+    from latec_b200.gnn_codec import gate_fields, read_stream, unpack_gates
+
+    codec = _codec()  # untrained weights: interpolation wins on a smooth field
+    x = _field(shape, 9)
+    gated = codec.compress(x, 1e-3, levels=levels)
+    plain = codec.compress(x, 1e-3, levels=levels, gate=False)
+    meta, _ = read_stream(gated)
+    words = unpack_gates(meta["gates"])
+    assert gate_fields(words[0])[0] == 0  # the anchors have no interpolation
+    assert any(gate_fields(w)[0] for w in words)  # some stage fell back
+    assert all(w == 0 for w in unpack_gates(read_stream(plain)[0]["gates"]))
+    assert len(gated) < len(plain)
+    assert codec.compress(x, 1e-3, levels=levels) == gated  # deterministic
+    out = codec.uncompress(gated).numpy()
+    vmin, vmax = float(np.float32(x.min())), float(np.float32(x.max()))
+    xn = (x.astype(np.float32) - np.float32(vmin)) / np.float32(vmax - vmin)
+    on = (out - np.float32(vmin)) / np.float32(vmax - vmin)
+    assert np.abs(on.astype(np.float64) - xn).max() <= 1e-3 + 4 * np.finfo(np.float32).eps
+    assert np.array_equal(codec.uncompress(gated).numpy(), out)
