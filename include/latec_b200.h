@@ -309,6 +309,11 @@ typedef struct {
      * those MLPs in BF16 on the tensor cores (d = 64 only); NULL = float32 */
     const void* packed_bf16;
     uint32_t* tc_err;  /* device word, bit 1: a tensor-core wait ran out */
+    /* optional, instead of packed_bf16: the same six layers packed by
+     * latec_gnn_pack_fp8 (E4M3) with their per-output-channel scales in the
+     * same order (128, 64, 128, 64, 128, 64 floats); NULL = not used */
+    const void* packed_fp8;
+    const float* fp8_scales;
 } latec_gnn_model;
 
 typedef struct {
@@ -351,6 +356,16 @@ int latec_gnn_finalize(const latec_gnn_model* model, int32_t B, int64_t N, int32
  *      k zero-padded to kp, a multiple of 16; out: n * kp uint16). err bit 1:
  *      a tensor-core completion wait ran out (the output is invalid). */
 int latec_gnn_pack_bf16(const float* w, int32_t n, int32_t k, int32_t kp, uint16_t* out);
+/* FP8 variant: E4M3 operands with one scale per weight output channel
+ * (max |w| / 448) and per row of the activations (input rows and the hidden
+ * layer), FP32 accumulation; kp a multiple of 32; out n * kp bytes, scales n
+ * floats (host). */
+int latec_gnn_pack_fp8(const float* w, int32_t n, int32_t k, int32_t kp, uint8_t* out,
+                       float* scales);
+int latec_gnn_mlp2_fp8(const float* X, int32_t ldx, int64_t rows, int32_t k1, int32_t k1p,
+                       const void* w1p, const float* s1, const float* b1, const void* w2p,
+                       const float* s2, const float* b2, float* Y, int32_t ldy, uint32_t* err,
+                       void* stream);
 int latec_gnn_mlp2_bf16(const float* X, int32_t ldx, int64_t rows, int32_t k1, int32_t k1p,
                         const void* w1p, const float* b1, const void* w2p, const float* b2,
                         float* Y, int32_t ldy, uint32_t* err, void* stream);

@@ -59,7 +59,8 @@ class FitStage(ctypes.Structure):
 
 
 class GnnModel(ctypes.Structure):
-    _fields_ = [("d", I32), ("agg_level", I32), ("params", P), ("packed_bf16", P), ("tc_err", P)]
+    _fields_ = [("d", I32), ("agg_level", I32), ("params", P), ("packed_bf16", P), ("tc_err", P),
+                ("packed_fp8", P), ("fp8_scales", P)]
 
 
 class GnnGeom(ctypes.Structure):
@@ -118,6 +119,8 @@ SIGNATURES = {
                                        ctypes.POINTER(GnnGeom), P, P, U64, P]),
     "latec_gnn_head": (ctypes.c_int, [ctypes.POINTER(GnnModel), I32, I32, I32, P,
                                       ctypes.c_float, P, P, P, U64, P]),
+    "latec_gnn_pack_fp8": (ctypes.c_int, [P, I32, I32, I32, P, P]),
+    "latec_gnn_mlp2_fp8": (ctypes.c_int, [P, I32, I64, I32, I32, P, P, P, P, P, P, P, I32, P, P]),
     "latec_gate_costs": (ctypes.c_int, [I64, P, P, P, P, P, P, D, I32, P, P, P, P]),
     "latec_gate_apply": (ctypes.c_int, [I64, P, P, P, D, I32, I32, I32, P]),
     "latec_tr_linear": (ctypes.c_int, [P, I64, I64, I32, P, P, I32, P, I64, I32, P, P]),

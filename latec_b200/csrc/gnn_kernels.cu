@@ -23,6 +23,9 @@ namespace latec {
 int mlp2_tc(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* w1p,
             const float* b1, const void* w2p, const float* b2, int n1, int n2, float* Y, int ldy,
             uint32_t* err, int n_sm, cudaStream_t st);
+int mlp2_tc8(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* w1p,
+             const float* s1, const float* b1, const void* w2p, const float* s2, const float* b2,
+             int n1, int n2, float* Y, int ldy, uint32_t* err, int n_sm, cudaStream_t st);
 
 namespace {
 
@@ -291,27 +294,55 @@ Params carve(const float* p0, int d, int agg) {
     return q;
 }
 
-// BF16 tensor-core copies of the BiDir / Dir / Mix MLP weights (d = 64):
-// each layer in the layout of latec_gnn_pack_bf16, input width padded to 16.
+// Tensor-core copies of the BiDir / Dir / Mix MLP weights (d = 64): each
+// layer in the layout of latec_gnn_pack_bf16 (input width padded to 16) or of
+// latec_gnn_pack_fp8 (E4M3, padded to 32, one scale per output channel).
+struct TcMlp {
+    const void* w1 = nullptr;
+    const void* w2 = nullptr;
+    const float* s1 = nullptr;
+    const float* s2 = nullptr;
+    int k1p = 0;
+    int fp8 = 0;
+};
 struct Packed {
-    const uint16_t *bi1, *bi2, *dir1, *dir2, *mix1, *mix2;
-    int bi_k1p, dir_k1p, mix_k1p;
+    TcMlp bi, dir, mix;
 };
 
 inline int pad16(int k) { return (k + 15) / 16 * 16; }
+inline int pad32(int k) { return (k + 31) / 32 * 32; }
 
-Packed packed_of(const void* base, const Params& P) {
+Packed packed_of(const latec_gnn_model* m, const Params& P) {
     Packed k;
-    const uint16_t* p = (const uint16_t*)base;
-    k.bi_k1p = pad16(2 * P.de + 2);
-    k.dir_k1p = pad16(P.de + 2);
-    k.mix_k1p = pad16(2 * P.d);
-    k.bi1 = p; p += (size_t)P.h * k.bi_k1p;
-    k.bi2 = p; p += (size_t)P.d * P.h;
-    k.dir1 = p; p += (size_t)P.h * k.dir_k1p;
-    k.dir2 = p; p += (size_t)P.d * P.h;
-    k.mix1 = p; p += (size_t)P.h * k.mix_k1p;
-    k.mix2 = p;
+    const int ins[3] = {2 * P.de + 2, P.de + 2, 2 * P.d};
+    TcMlp* mlps[3] = {&k.bi, &k.dir, &k.mix};
+    if (m->packed_fp8) {
+        const uint8_t* p = (const uint8_t*)m->packed_fp8;
+        const float* sc = m->fp8_scales;
+        for (int i = 0; i < 3; i++) {
+            TcMlp& t = *mlps[i];
+            t.fp8 = 1;
+            t.k1p = pad32(ins[i]);
+            t.w1 = p;
+            p += (size_t)P.h * t.k1p;
+            t.s1 = sc;
+            sc += P.h;
+            t.w2 = p;
+            p += (size_t)P.d * P.h;
+            t.s2 = sc;
+            sc += P.d;
+        }
+    } else if (m->packed_bf16) {
+        const uint16_t* p = (const uint16_t*)m->packed_bf16;
+        for (int i = 0; i < 3; i++) {
+            TcMlp& t = *mlps[i];
+            t.k1p = pad16(ins[i]);
+            t.w1 = p;
+            p += (size_t)P.h * t.k1p;
+            t.w2 = p;
+            p += (size_t)P.d * P.h;
+        }
+    }
     return k;
 }
 
@@ -329,10 +360,10 @@ int n_sms() {
 }
 
 // Two-layer MLP over rows of X: on the tensor cores when the model carries
-// packed BF16 weights, else the float32 path.
+// packed BF16 or E4M3 weights, else the float32 path.
 int mlp2(const latec_gnn_model* m, const float* X, int ldx, int64_t rows, int k1, const float* w1,
-         const float* b1, const uint16_t* w1p, int k1p, const float* w2, const float* b2,
-         const uint16_t* w2p, int h, int d, float* H, float* Y, int ldy, cudaStream_t st);
+         const float* b1, const float* w2, const float* b2, const TcMlp& tc, int h, int d,
+         float* H, float* Y, int ldy, cudaStream_t st);
 
 int linear(const float* X, int ldx, int64_t rows, int in, const float* W, const float* b, int out,
            float* Y, int ldy, int act, cudaStream_t st) {
@@ -346,11 +377,14 @@ int linear(const float* X, int ldx, int64_t rows, int in, const float* W, const 
 }
 
 int mlp2(const latec_gnn_model* m, const float* X, int ldx, int64_t rows, int k1, const float* w1,
-         const float* b1, const uint16_t* w1p, int k1p, const float* w2, const float* b2,
-         const uint16_t* w2p, int h, int d, float* H, float* Y, int ldy, cudaStream_t st) {
-    if (m->packed_bf16)
-        return mlp2_tc(X, ldx, rows, k1, k1p, w1p, b1, w2p, b2, h, d, Y, ldy, m->tc_err, n_sms(),
-                       st);
+         const float* b1, const float* w2, const float* b2, const TcMlp& tc, int h, int d,
+         float* H, float* Y, int ldy, cudaStream_t st) {
+    if (tc.w1 && tc.fp8)
+        return mlp2_tc8(X, ldx, rows, k1, tc.k1p, tc.w1, tc.s1, b1, tc.w2, tc.s2, b2, h, d, Y, ldy,
+                        m->tc_err, n_sms(), st);
+    if (tc.w1)
+        return mlp2_tc(X, ldx, rows, k1, tc.k1p, tc.w1, b1, tc.w2, b2, h, d, Y, ldy, m->tc_err,
+                       n_sms(), st);
     int rc = linear(X, ldx, rows, k1, w1, b1, h, H, h, 1, st);
     if (!rc) rc = linear(H, h, rows, h, w2, b2, d, Y, ldy, 0, st);
     return rc;
@@ -365,7 +399,8 @@ int launched(int n) {
 
 bool valid_model(const latec_gnn_model* m) {
     return m && m->params && m->d >= 4 && m->d <= 128 && m->d % 2 == 0 && m->agg_level >= 1 &&
-           m->agg_level <= 8 && (!m->packed_bf16 || (m->d == 64 && m->tc_err));
+           m->agg_level <= 8 && (!m->packed_bf16 || (m->d == 64 && m->tc_err)) &&
+           (!m->packed_fp8 || (m->d == 64 && m->tc_err && m->fp8_scales));
 }
 
 }  // namespace
@@ -376,7 +411,7 @@ using namespace latec;
 extern "C" {
 
 uint64_t latec_gnn_param_count(int32_t d, int32_t agg_level) {
-    latec_gnn_model m{d, agg_level, (const float*)16, nullptr, nullptr};
+    latec_gnn_model m{d, agg_level, (const float*)16, nullptr, nullptr, nullptr, nullptr};
     if (!valid_model(&m)) return 0;
     return carve(nullptr, d, agg_level).count;
 }
@@ -414,7 +449,7 @@ int latec_gnn_embed(const latec_gnn_model* model, int32_t B, int64_t N, const fl
         return LATEC_ERR_WORKSPACE;
     cudaStream_t st = (cudaStream_t)stream;
     const Params P = carve(model->params, d, model->agg_level);
-    const Packed pk = packed_of(model->packed_bf16, P);
+    const Packed pk = packed_of(model, P);
     const float scale = 1.0f / sqrtf((float)d);
     const int64_t w2 = 2 * P.de + 2, w1 = P.de + 2;
     const int64_t l2 = (w2 + 3) / 4 * 4, l1 = (w1 + 3) / 4 * 4;  // 16-byte row strides
@@ -441,8 +476,8 @@ int latec_gnn_embed(const latec_gnn_model* model, int32_t B, int64_t N, const fl
                                                                   (int)l2);
                 rc = launched(1);
                 if (!rc)
-                    rc = mlp2(model, X, (int)l2, n2 * K, (int)w2, P.bi0w, P.bi0b, pk.bi1, pk.bi_k1p,
-                              P.bi2w, P.bi2b, pk.bi2, P.h, d, H, msb, d, st);
+                    rc = mlp2(model, X, (int)l2, n2 * K, (int)w2, P.bi0w, P.bi0b, P.bi2w, P.bi2b,
+                              pk.bi, P.h, d, H, msb, d, st);
             }
             if (n1 && !rc) {
                 k_rows_one<<<blocks_for(n1 * K * 32), LT, 0, st>>>(E, N, K, d, P.ds, P.table, g, b,
@@ -450,9 +485,8 @@ int latec_gnn_embed(const latec_gnn_model* model, int32_t B, int64_t N, const fl
                                                                   (int)l1);
                 rc = launched(1);
                 if (!rc)
-                    rc = mlp2(model, X, (int)l1, n1 * K, (int)w1, P.dir0w, P.dir0b, pk.dir1,
-                              pk.dir_k1p, P.dir2w, P.dir2b, pk.dir2, P.h, d, H, msb + n2 * K * d, d,
-                              st);
+                    rc = mlp2(model, X, (int)l1, n1 * K, (int)w1, P.dir0w, P.dir0b, P.dir2w,
+                              P.dir2b, pk.dir, P.h, d, H, msb + n2 * K * d, d, st);
             }
         }
         // line pool keys and values of every live row
@@ -532,10 +566,10 @@ int latec_gnn_finalize(const latec_gnn_model* model, int32_t B, int64_t N, int32
     if (rc) return rc;
     k_mix_rows<<<blocks_for(bmk * 2 * d), LT, 0, st>>>(ctx, VE, bmk, K, d, X);
     rc = launched(1);
-    const Packed pk = packed_of(model->packed_bf16, P);
+    const Packed pk = packed_of(model, P);
     if (!rc)
-        rc = mlp2(model, X, 2 * d, bmk, 2 * d, P.mx0w, P.mx0b, pk.mix1, pk.mix_k1p, P.mx2w, P.mx2b,
-                  pk.mix2, P.h, d, H, Y, d, st);
+        rc = mlp2(model, X, 2 * d, bmk, 2 * d, P.mx0w, P.mx0b, P.mx2w, P.mx2b, pk.mix, P.h, d, H,
+                  Y, d, st);
     if (rc) return rc;
     k_scatter_e<<<blocks_for(bmk * d), LT, 0, st>>>(Y, query, B, M, K, d, N, E);
     return launched(1);

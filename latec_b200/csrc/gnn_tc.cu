@@ -19,6 +19,7 @@
 // layout (latec_gnn_pack_bf16). Every mbarrier wait has an iteration limit;
 // on expiry the kernel records an error, stops issuing and frees its TMEM.
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -282,6 +283,254 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
 }
 
+
+// ---------------------------------------------------------------- FP8 variant
+// E4M3 operands, FP32 accumulators. Weights carry one scale per output
+// channel (max |w| / 448, applied in the epilogues); activations one scale per
+// row, for the input rows and again for the hidden layer before layer 2. The
+// canonical layout is the BF16 one in bytes: 8 x 16-byte core matrices of 16
+// elements, one K = 32 MMA spanning two of them.
+constexpr float FP8_MAX = 448.0f;
+
+__host__ __device__ __forceinline__ uint32_t canon8(uint32_t r, uint32_t k, uint32_t R) {
+    return ((k >> 4) * (R >> 3) + (r >> 3)) * 128u + (r & 7u) * 16u + (k & 15u);
+}
+
+// kind::f8f6f4 instruction descriptor: E4M3 A and B (K-major), FP32 D, M x N.
+__host__ __device__ constexpr uint32_t idesc_e4m3(uint32_t M, uint32_t N) {
+    return (1u << 4) | ((N >> 3) << 17) | ((M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_e4m3(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ uint32_t fp8x4(float a, float b, float c, float d) {
+    const uint32_t lo = __nv_cvt_float2_to_fp8x2(make_float2(a, b), __NV_SATFINITE, __NV_E4M3);
+    const uint32_t hi = __nv_cvt_float2_to_fp8x2(make_float2(c, d), __NV_SATFINITE, __NV_E4M3);
+    return lo | (hi << 16);
+}
+
+// 16-byte shared store of 16 E4M3 values (v scaled by inv first).
+__device__ __forceinline__ void st_fp8x16(uint8_t* dst, const float* v, float inv) {
+    uint4 u;
+    u.x = fp8x4(v[0] * inv, v[1] * inv, v[2] * inv, v[3] * inv);
+    u.y = fp8x4(v[4] * inv, v[5] * inv, v[6] * inv, v[7] * inv);
+    u.z = fp8x4(v[8] * inv, v[9] * inv, v[10] * inv, v[11] * inv);
+    u.w = fp8x4(v[12] * inv, v[13] * inv, v[14] * inv, v[15] * inv);
+    *(uint4*)dst = u;
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_mlp2_tc8(const float* __restrict__ X, int ldx, int rows, int k1, int k1p,
+               const uint8_t* __restrict__ w1p, const float* __restrict__ s1,
+               const float* __restrict__ b1, const uint8_t* __restrict__ w2p,
+               const float* __restrict__ s2, const float* __restrict__ b2, float* __restrict__ Y,
+               int ldy, uint32_t* __restrict__ err) {
+    extern __shared__ __align__(128) uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    __shared__ float red[2][TC_M];
+    __shared__ float scale_a[TC_M], scale_h[TC_M];
+    uint8_t* sw1 = smem_raw;                        // N1 x k1p
+    uint8_t* sw2 = sw1 + (size_t)N1 * k1p;          // N2 x N1
+    uint8_t* sa = sw2 + (size_t)N2 * N1;            // 128 x k1p
+    uint8_t* sh = sa + (size_t)TC_M * k1p;          // 128 x N1
+    float* hbuf = (float*)(sh + (size_t)TC_M * N1); // 128 x (N1 + 1) hidden values
+    float* sy = hbuf;                               // 128 x (N2 + 1), after the hidden layer
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int quarter = warp & 3, half = warp >> 2;
+    {
+        const int4* s1p = (const int4*)w1p;
+        int4* d1 = (int4*)sw1;
+        for (int i = tid; i < N1 * k1p / 16; i += TC_THREADS) d1[i] = s1p[i];
+        const int4* s2p = (const int4*)w2p;
+        int4* d2 = (int4*)sw2;
+        for (int i = tid; i < N2 * N1 / 16; i += TC_THREADS) d2[i] = s2p[i];
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    constexpr uint32_t TMEM_COLS = (N1 + N2) <= 128 ? 128 : ((N1 + N2) <= 256 ? 256 : 512);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_base)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base;
+    const uint32_t mb = smem_u32(&mbar);
+    uint32_t phase = 0;
+    bool ok = true;
+    const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+    const int trow = quarter * 32 + lane;
+    const int n_tiles = (rows + TC_M - 1) / TC_M;
+    const int chunks = k1p / 16;
+    const int kh = ((k1 + 1) / 2 + 3) & ~3;  // a multiple of 4: float4 steps
+    // rows start on 16-byte boundaries and ldx >= round_up(k1, 4): a float4
+    // starting below k1 stays inside its row
+    const bool vec4 = (ldx % 4) == 0 && ((uintptr_t)X % 16) == 0 && ldx >= ((k1 + 3) & ~3);
+
+    for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+        const int r0 = t * TC_M;
+        const int r = tid & (TC_M - 1), hf = tid >> 7;
+        const int gr = r0 + r;
+        const float* xr = X + (int64_t)gr * ldx;
+        {  // 1a. per-row scale of X: two threads per row, one half of K each
+            float m = 0.0f;
+            if (gr < rows) {
+                const int ka = hf * kh, kb = min(k1, (hf + 1) * kh);
+                if (vec4) {
+                    for (int k = ka; k < kb; k += 4) {
+                        const float4 f = *(const float4*)(xr + k);
+                        m = fmaxf(m, fmaxf(fmaxf(fabsf(f.x), k + 1 < kb ? fabsf(f.y) : 0.0f),
+                                           fmaxf(k + 2 < kb ? fabsf(f.z) : 0.0f,
+                                                 k + 3 < kb ? fabsf(f.w) : 0.0f)));
+                    }
+                } else {
+                    for (int k = ka; k < kb; k++) m = fmaxf(m, fabsf(xr[k]));
+                }
+            }
+            red[hf][r] = m;
+        }
+        __syncthreads();
+        if (tid < TC_M) {
+            const float m = fmaxf(red[0][tid], red[1][tid]);
+            scale_a[tid] = m > 0.0f ? m / FP8_MAX : 1.0f;
+        }
+        __syncthreads();
+        {  // 1b. rows of X -> E4M3 A operand, 16-element chunks
+            const float inv = 1.0f / scale_a[r];
+            for (int c = hf; c < chunks; c += 2) {
+                float v[16];
+                if (vec4) {
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const int k = c * 16 + 4 * q;
+                        float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (gr < rows && k < k1) f = *(const float4*)(xr + k);
+                        v[4 * q + 0] = k + 0 < k1 ? f.x : 0.0f;
+                        v[4 * q + 1] = k + 1 < k1 ? f.y : 0.0f;
+                        v[4 * q + 2] = k + 2 < k1 ? f.z : 0.0f;
+                        v[4 * q + 3] = k + 3 < k1 ? f.w : 0.0f;
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 16; e++) {
+                        const int k = c * 16 + e;
+                        v[e] = (gr < rows && k < k1) ? xr[k] : 0.0f;
+                    }
+                }
+                st_fp8x16(sa + canon8(r, c * 16, TC_M), v, inv);
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        // 2. layer 1
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t a0 = smem_u32(sa), bb = smem_u32(sw1);
+            for (int kk = 0; kk < k1p / 32; kk++) {
+                const uint64_t ad = smem_desc(a0 + kk * 2 * TC_M * 16, TC_M * 16, 128);
+                const uint64_t bd = smem_desc(bb + kk * 2 * N1 * 16, N1 * 16, 128);
+                mma_e4m3(tmem, ad, bd, idesc_e4m3(TC_M, N1), kk > 0);
+            }
+            mma_commit(mb);
+        }
+        ok = __syncthreads_and(mbar_wait(mb, phase)) != 0;
+        if (!ok) {
+            if (tid == 0) atomicOr(err, 1u);
+            break;
+        }
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        // 3. epilogue 1: bias + GELU, per-row hidden scale, E4M3 hidden operand
+        const float sa_r = scale_a[trow];
+        {  // hidden values into shared memory and their row maximum
+            float m = 0.0f;
+            for (int c = half * (N1 / 2); c < (half + 1) * (N1 / 2); c += 16) {
+                float v[16];
+                tmem_ld16(tmem + lane_base + c, v);
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    const float hv = gelu_tc(__fadd_rn(v[i] * sa_r * s1[c + i], b1[c + i]));
+                    hbuf[trow * (N1 + 1) + c + i] = hv;
+                    m = fmaxf(m, fabsf(hv));
+                }
+            }
+            red[half][trow] = m;
+        }
+        __syncthreads();
+        if (tid < TC_M) {
+            const float m = fmaxf(red[0][tid], red[1][tid]);
+            scale_h[tid] = m > 0.0f ? m / FP8_MAX : 1.0f;
+        }
+        __syncthreads();
+        {
+            const float inv = 1.0f / scale_h[trow];
+            for (int c = half * (N1 / 2); c < (half + 1) * (N1 / 2); c += 16) {
+                float v[16];
+#pragma unroll
+                for (int i = 0; i < 16; i++) v[i] = hbuf[trow * (N1 + 1) + c + i];
+                st_fp8x16(sh + canon8(trow, c, TC_M), v, inv);
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        // 4. layer 2
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t a0 = smem_u32(sh), bb = smem_u32(sw2);
+            for (int kk = 0; kk < N1 / 32; kk++) {
+                const uint64_t ad = smem_desc(a0 + kk * 2 * TC_M * 16, TC_M * 16, 128);
+                const uint64_t bd = smem_desc(bb + kk * 2 * N2 * 16, N2 * 16, 128);
+                mma_e4m3(tmem + N1, ad, bd, idesc_e4m3(TC_M, N2), kk > 0);
+            }
+            mma_commit(mb);
+        }
+        ok = __syncthreads_and(mbar_wait(mb, phase)) != 0;
+        if (!ok) {
+            if (tid == 0) atomicOr(err, 1u);
+            break;
+        }
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        // 5. epilogue 2: scales + bias -> float32 staging, coalesced rows
+        const float sh_r = scale_h[trow];
+        for (int c = half * (N2 / 2); c < (half + 1) * (N2 / 2); c += 16) {
+            float v[16];
+            tmem_ld16(tmem + lane_base + N1 + c, v);
+#pragma unroll
+            for (int i = 0; i < 16; i++)
+                sy[trow * (N2 + 1) + c + i] = __fadd_rn(v[i] * sh_r * s2[c + i], b2[c + i]);
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();
+        for (int e = tid; e < TC_M * N2; e += TC_THREADS) {
+            const int rr = e / N2, c = e % N2;
+            if (r0 + rr < rows) Y[(int64_t)(r0 + rr) * ldy + c] = sy[rr * (N2 + 1) + c];
+        }
+        __syncthreads();
+    }
+    if (!ok) mbar_wait(mb, phase);
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(TMEM_COLS));
+    }
+}
 }  // namespace
 
 // Shared memory of the fused kernel for an input width padded to k1p.
@@ -306,6 +555,33 @@ int mlp2_tc(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* 
     const int grid = (int)(tiles < n_sm ? tiles : n_sm);
     kern<<<grid, TC_THREADS, smem, st>>>(X, ldx, (int)rows, k1, k1p, (const __nv_bfloat16*)w1p, b1,
                                          (const __nv_bfloat16*)w2p, b2, Y, ldy, err);
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
+}
+
+
+uint64_t mlp2_tc8_smem(int k1p, int n1, int n2) {
+    const uint64_t stage = 4ull * TC_M * ((n1 > n2 ? n1 : n2) + 1);  // hidden, then Y
+    return (uint64_t)n1 * k1p + (uint64_t)n2 * n1 + (uint64_t)TC_M * k1p + (uint64_t)TC_M * n1 +
+           stage;
+}
+
+int mlp2_tc8(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* w1p,
+             const float* s1, const float* b1, const void* w2p, const float* s2, const float* b2,
+             int n1, int n2, float* Y, int ldy, uint32_t* err, int n_sm, cudaStream_t st) {
+    if (rows <= 0) return LATEC_OK;
+    if (n1 != 128 || n2 != 64 || k1p % 32 || k1p < k1 || rows > 0x7fffffffLL)
+        return LATEC_ERR_UNSUPPORTED;
+    const uint64_t smem = mlp2_tc8_smem(k1p, n1, n2);
+    if (smem > 200 * 1024) return LATEC_ERR_UNSUPPORTED;
+    auto kern = k_mlp2_tc8<128, 64>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return LATEC_ERR_CUDA;
+    const int64_t tiles = (rows + TC_M - 1) / TC_M;
+    const int grid = (int)(tiles < n_sm ? tiles : n_sm);
+    kern<<<grid, TC_THREADS, smem, st>>>(X, ldx, (int)rows, k1, k1p, (const uint8_t*)w1p, s1, b1,
+                                         (const uint8_t*)w2p, s2, b2, Y, ldy, err);
     count_launches(1);
     return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
 }
@@ -343,6 +619,45 @@ int latec_gnn_mlp2_bf16(const float* X, int32_t ldx, int64_t rows, int32_t k1, i
         cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
     return mlp2_tc(X, ldx, rows, k1, k1p, w1p, b1, w2p, b2, 128, 64, Y, ldy, err, n_sm,
                    (cudaStream_t)stream);
+}
+
+
+// Pack a float32 (n x k) weight matrix into E4M3 with one scale per output
+// row (max |w| / 448, 1 for a zero row), in the canonical no-swizzle
+// K-major layout of the FP8 MLP (k zero-padded to kp, a multiple of 32; n a
+// multiple of 8). Host arrays; out has n * kp bytes, scales n floats.
+int latec_gnn_pack_fp8(const float* w, int32_t n, int32_t k, int32_t kp, uint8_t* out,
+                       float* scales) {
+    if (!w || !out || !scales || n < 8 || n % 8 || k < 1 || kp < k || kp % 32) return LATEC_ERR_ARG;
+    for (int r = 0; r < n; r++) {
+        float m = 0.0f;
+        for (int c = 0; c < k; c++) m = fmaxf(m, fabsf(w[(int64_t)r * k + c]));
+        const float sc = m > 0.0f ? m / FP8_MAX : 1.0f;
+        scales[r] = sc;
+        for (int c = 0; c < kp; c++) {
+            const float v = c < k ? w[(int64_t)r * k + c] / sc : 0.0f;
+            out[canon8((uint32_t)r, (uint32_t)c, (uint32_t)n)] =
+                (uint8_t)__nv_cvt_float_to_fp8(v, __NV_SATFINITE, __NV_E4M3);
+        }
+    }
+    return LATEC_OK;
+}
+
+// Y = W2 * gelu(W1 * X + b1) + b2 with E4M3 operands (hidden 128, output 64):
+// w1p / w2p and s1 / s2 from latec_gnn_pack_fp8 (device). err bit 1: a
+// tensor-core wait ran out (results invalid).
+int latec_gnn_mlp2_fp8(const float* X, int32_t ldx, int64_t rows, int32_t k1, int32_t k1p,
+                       const void* w1p, const float* s1, const float* b1, const void* w2p,
+                       const float* s2, const float* b2, float* Y, int32_t ldy, uint32_t* err,
+                       void* stream) {
+    if ((rows && (!X || !Y)) || !w1p || !s1 || !b1 || !w2p || !s2 || !b2 || !err || ldx < k1 ||
+        ldy < 64)
+        return LATEC_ERR_ARG;
+    int dev = 0, n_sm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    return mlp2_tc8(X, ldx, rows, k1, k1p, w1p, s1, b1, w2p, s2, b2, 128, 64, Y, ldy, err, n_sm,
+                    (cudaStream_t)stream);
 }
 
 }  // extern "C"

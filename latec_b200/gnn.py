@@ -303,18 +303,20 @@ class GNNModel:
 
     def __init__(self, weights: dict, d: int = 64, agg_level: int = 1, device=None,
                  precision: str = "f32"):
-        """``precision``: "f32" (every layer in float32) or "bf16" (the
+        """``precision``: "f32" (every layer in float32), "bf16" (the
         BiDirEmbed, DirEmbed and MixEmbed MLPs in BF16 on the tensor cores with
-        float32 accumulation; pools and readout stay float32; d = 64)."""
+        float32 accumulation; pools and readout stay float32; d = 64) or "fp8"
+        (those MLPs in E4M3 with per-output-channel weight scales and per-row
+        activation scales, float32 accumulation; d = 64)."""
         import ctypes
 
         torch = _torch()
         from . import _lib
 
         lib = _lib.load()
-        if precision not in ("f32", "bf16"):
-            raise ValueError("precision must be 'f32' or 'bf16'")
-        if precision == "bf16" and int(d) != 64:
+        if precision not in ("f32", "bf16", "fp8"):
+            raise ValueError("precision must be 'f32', 'bf16' or 'fp8'")
+        if precision in ("bf16", "fp8") and int(d) != 64:
             raise NotImplementedError("the tensor-core message pass is built for d = 64")
         self.precision = precision
         self.d, self.agg_level = int(d), int(agg_level)
@@ -341,6 +343,24 @@ class GNNModel:
                 parts.append(out)
             self.packed = torch.from_numpy(np.concatenate(parts).view(np.int16)).to(self.device)
             m.packed_bf16 = self.packed.data_ptr()
+            m.tc_err = self.tc_err.data_ptr()
+        elif precision == "fp8":
+            parts, scales = [], []
+            for name in ("bidir.net.0", "bidir.net.2", "dir.net.0", "dir.net.2", "mix.net.0",
+                         "mix.net.2"):
+                w = np.ascontiguousarray(weights[name + ".weight"], np.float32)
+                n, k = w.shape
+                kp = -(-k // 32) * 32
+                out = np.empty(n * kp, np.uint8)
+                sc = np.empty(n, np.float32)
+                _lib.check(lib.latec_gnn_pack_fp8(w.ctypes.data, n, k, kp, out.ctypes.data,
+                                                  sc.ctypes.data), "latec_gnn_pack_fp8")
+                parts.append(out)
+                scales.append(sc)
+            self.packed = torch.from_numpy(np.concatenate(parts)).to(self.device)
+            self.fp8_scales = torch.from_numpy(np.concatenate(scales)).to(self.device)
+            m.packed_fp8 = self.packed.data_ptr()
+            m.fp8_scales = self.fp8_scales.data_ptr()
             m.tc_err = self.tc_err.data_ptr()
         self.struct = m
         self._ws = None

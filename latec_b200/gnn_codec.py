@@ -40,7 +40,9 @@ Scope of this version:
   accumulation; pools and the readout stay float32. ``fp16=False`` is float32
   throughout. ``compile`` is accepted and recorded as not compiled.
 
-Streams carry their ``"float_path"`` (``latec_b200-bf16-1`` or
+``fp8=True`` (an extension) runs those MLPs in FP8 (E4M3) with per-channel
+weight and per-row activation scales instead. Streams carry their
+``"float_path"`` (``latec_b200-bf16-1``, ``latec_b200-fp8-1`` or
 ``latec_b200-f32-1``). As the reference's own encoder/decoder contract
 requires, they decode only with that float path.
 """
@@ -61,7 +63,8 @@ MAGIC = b"LATECGNN"
 VERSION = 14
 PREFIX = "<8sII"
 PREFIX_SIZE = struct.calcsize(PREFIX)
-FLOAT_PATHS = {False: "latec_b200-f32-1", True: "latec_b200-bf16-1"}
+FLOAT_PATHS = {"f32": "latec_b200-f32-1", "bf16": "latec_b200-bf16-1",
+               "fp8": "latec_b200-fp8-1"}
 AUTO_CHUNK_THRESHOLD = 1 << 21
 RANK_LEVELS = {2: 8, 4: 5, 5: 4}
 EB_COARSE_FACTOR = 0.9
@@ -243,15 +246,16 @@ class GNNCodec:
         self._models = {}
         self._geoms = {}
 
-    def _model(self, reduced: bool):
-        """float32 model, or BF16 tensor-core message pass (the counterpart of
-        the reference's fp16 message pass) when ``reduced``."""
-        reduced = bool(reduced) and self.d == 64
-        m = self._models.get(reduced)
+    def _model(self, precision: str):
+        """The model in one float path: "f32", "bf16" (the tensor-core message
+        pass, counterpart of the reference's fp16 one) or "fp8" (E4M3 with
+        per-channel weight and per-row activation scales); d = 64 for the
+        tensor-core paths."""
+        m = self._models.get(precision)
         if m is None:
             m = gnn.GNNModel(self._weights, self.d, self.agg_level, self.device,
-                             precision="bf16" if reduced else "f32")
-            self._models[reduced] = m
+                             precision=precision)
+            self._models[precision] = m
         return m
 
     # ---------------------------------------------------------------- helpers
@@ -278,8 +282,10 @@ class GNNCodec:
     def compress(self, x, error_bound: float = 1e-2, *, levels="auto", radius: int = 1 << 15,
                  zstd_level: int = 9, eb_ratio=None, tune: str = "fast", chunk_size=None,
                  fp16: bool = True, compile="auto", gate: bool = True, gate_fine: bool = False,
-                 predictor: str = "gnn") -> bytes:
-        """Compress a NumPy array or torch tensor (``latec/gnn_codec.py:1576-1775``)."""
+                 predictor: str = "gnn", fp8: bool = False) -> bytes:
+        """Compress a NumPy array or torch tensor (``latec/gnn_codec.py:1576-1775``).
+        ``fp8=True`` (no counterpart in the reference) runs the message-pass
+        MLPs in FP8 instead of BF16; the stream records that float path."""
         torch = _torch()
         if tune not in ("fast", "size"):
             raise ValueError("tune must be 'fast' or 'size'")
@@ -337,14 +343,17 @@ class GNNCodec:
         ratios = sorted({per_step_eb_ratio(c, lv) for c in coarse})
         best = None
         reduced = bool(fp16) and self.d == 64
-        model = self._model(reduced)
+        precision = ("fp8" if fp8 else "bf16") if reduced else "f32"
+        if fp8 and not reduced:
+            raise ValueError("fp8 needs the tensor-core path (fp16=True, d = 64)")
+        model = self._model(precision)
         for ratio in ratios:
             payload, words = self._encode(model, xn, shape, lv, eb, ratio, radius, bool(gate))
             meta = {"shape": list(original_shape), "dtype": np_dtype.str, "error_bound": eb,
                     "levels": lv, "radius": radius, "vmin": vmin, "vmax": vmax,
                     "eb_ratio": ratio, "checkpoint_hash": self.checkpoint_hash.hex(),
                     "chunks": list(edges), "m_tile": 1 << 16, "fp16": reduced, "compiled": False,
-                    "predictor": "gnn", "float_path": FLOAT_PATHS[reduced], "d": self.d,
+                    "predictor": "gnn", "float_path": FLOAT_PATHS[precision], "d": self.d,
                     "agg_level": self.agg_level, "gate": bool(gate), "gate_fine": bool(gate_fine),
                     "gates": pack_gates(words)}
             if int(model.tc_err.item()):
@@ -453,9 +462,10 @@ class GNNCodec:
         torch = _torch()
         lib = _lib.load()
         meta, payload = read_stream(bytes(stream))
-        if meta.get("float_path") not in FLOAT_PATHS.values():
+        paths = {v: k for k, v in FLOAT_PATHS.items()}
+        if meta.get("float_path") not in paths:
             raise ValueError("stream was not written by this codec's float path")
-        model = self._model(meta["float_path"] == FLOAT_PATHS[True])
+        model = self._model(paths[meta["float_path"]])
         if self.strict_checkpoint and meta["checkpoint_hash"] != self.checkpoint_hash.hex():
             raise ValueError("checkpoint hash differs from the stream metadata")
         original_shape = tuple(int(n) for n in meta["shape"])

@@ -122,3 +122,32 @@ def test_bf16_tensor_core_forward_close_to_oracle(name):
     for (m1, l1), (m2, l2) in zip(out, again):  # deterministic
         assert np.array_equal(m1.cpu().numpy().view(np.uint32), m2.cpu().numpy().view(np.uint32))
     assert np.array_equal(E.cpu().numpy(), E2.cpu().numpy())
+
+
+# E4M3 operands (3-bit mantissa) with per-channel weight and per-row
+# activation scales in the message and finalisation MLPs.
+FP8_MU_ATOL = 5e-2
+FP8_LB_ATOL = 5e-1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["g2d", "g3d", "g2d_agg2"])
+def test_fp8_tensor_core_forward_close_to_oracle(name):
+    from latec_b200 import gnn
+    from oracle import gnn as ognn
+
+    c = CASES[name]
+    w = gnn.random_weights(c["seed"], 64, c["agg_level"])
+    model = gnn.GNNModel(w, 64, c["agg_level"], precision="fp8")
+    out, E = gnn.run_stages(model, Z[f"{name}_x"], _geoms(c, None), eb=c["eb"])
+    again, _ = gnn.run_stages(model, Z[f"{name}_x"], _geoms(c, None), eb=c["eb"])
+    ogeoms = ognn.stage_geoms(tuple(c["shape"]), c["levels"], c["stride"], c["block"],
+                              c["max_radius"], c["agg_level"])
+    want, _ = ognn.run_stages(w, Z[f"{name}_x"], ogeoms, c["agg_level"], eb=c["eb"])
+    assert int(model.tc_err.item()) == 0
+    dmu = max(float(np.abs(m.cpu().numpy() - m64).max()) for (m, _), (m64, _) in zip(out, want))
+    dlb = max(float(np.abs(l.cpu().numpy() - l64).max()) for (_, l), (_, l64) in zip(out, want))
+    print(f"{name}: fp8 vs float64 oracle: max |d mu| {dmu:.3g}, max |d log2 b| {dlb:.3g}")
+    assert dmu < FP8_MU_ATOL and dlb < FP8_LB_ATOL
+    for (m1, _), (m2, _) in zip(out, again):  # deterministic
+        assert np.array_equal(m1.cpu().numpy().view(np.uint32), m2.cpu().numpy().view(np.uint32))

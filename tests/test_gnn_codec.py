@@ -169,3 +169,21 @@ def test_gate_falls_back_to_interpolation_where_it_codes_fewer_bits(shape, level
     on = (out - np.float32(vmin)) / np.float32(vmax - vmin)
     assert np.abs(on.astype(np.float64) - xn).max() <= 1e-3 + 4 * np.finfo(np.float32).eps
     assert np.array_equal(codec.uncompress(gated).numpy(), out)
+
+
+@pytest.mark.gpu
+def test_fp8_float_path_round_trip():
+    from latec_b200.gnn_codec import read_stream
+
+    codec = _codec()
+    x = _field((40, 36), 4)
+    s = codec.compress(x, 1e-3, levels=3, fp8=True)
+    assert read_stream(s)[0]["float_path"] == "latec_b200-fp8-1"
+    assert codec.compress(x, 1e-3, levels=3, fp8=True) == s
+    out = codec.uncompress(s).numpy()
+    vmin, vmax = float(np.float32(x.min())), float(np.float32(x.max()))
+    xn = (x.astype(np.float32) - np.float32(vmin)) / np.float32(vmax - vmin)
+    on = (out - np.float32(vmin)) / np.float32(vmax - vmin)
+    assert np.abs(on.astype(np.float64) - xn).max() <= 1e-3 + 4 * np.finfo(np.float32).eps
+    with pytest.raises(ValueError):
+        codec.compress(x, 1e-3, levels=3, fp8=True, fp16=False)
