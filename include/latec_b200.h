@@ -46,8 +46,13 @@ typedef struct latec_quant_params {
     int32_t order;        /* 0 linear, 1 cubic */
     int32_t center;       /* 0 average odd axes, 1 first odd axis, 2 last odd axis */
     int32_t end_mode;     /* bit 0 quadratic ends, bit 1 extrapolation */
-    int32_t round_output; /* verify against the rounded reconstruction (integer sources) */
+    int32_t round_output; /* verify against the rounded reconstruction (integer sources):
+                           * 0 no, 1 rint(recon), 2 the normalised value of the
+                           * nearest raw integer, (rint(recon * round_span +
+                           * round_offset) - round_offset) / round_span */
     int32_t reserved;
+    double round_span;    /* round_output 2: the data range and its minimum */
+    double round_offset;
 } latec_quant_params;
 
 /* Per-stage results written on the device. */

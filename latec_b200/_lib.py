@@ -31,7 +31,8 @@ I64, F = ctypes.c_int64, ctypes.c_float
 
 class QuantParams(ctypes.Structure):
     _fields_ = [("dtype", I32), ("channels", I32), ("radius", I32), ("order", I32),
-                ("center", I32), ("end_mode", I32), ("round_output", I32), ("reserved", I32)]
+                ("center", I32), ("end_mode", I32), ("round_output", I32), ("reserved", I32),
+                ("round_span", D), ("round_offset", D)]
 
 
 class StageStats(ctypes.Structure):

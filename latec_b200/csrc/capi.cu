@@ -48,6 +48,10 @@ bool valid_params(const latec_quant_params* p) {
     if (p->channels < 1 || p->radius < 1 || p->radius > 32768) return false;
     if (p->order < 0 || p->order > 1 || p->center < 0 || p->center > 2) return false;
     if (p->end_mode < 0 || p->end_mode > 3) return false;
+    if (p->round_output < 0 || p->round_output > 2) return false;
+    if (p->round_output == 2 &&
+        !(p->round_span > 0.0 && std::isfinite(p->round_span) && std::isfinite(p->round_offset)))
+        return false;
     return true;
 }
 
@@ -63,6 +67,8 @@ bool make_q(const latec_quant_params* p, double eb, uint64_t points, QParams& q)
     q.center = p->center;
     q.end_mode = p->end_mode;
     q.round_output = p->round_output;
+    q.rspan = p->round_output == 2 ? p->round_span : 1.0;
+    q.roff = p->round_output == 2 ? p->round_offset : 0.0;
     q.channels = p->channels;
     q.points = points;
     return true;

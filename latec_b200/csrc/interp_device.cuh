@@ -165,6 +165,18 @@ __device__ __forceinline__ double quotient_rint(double diff, const QParams& q) {
     return rint(__ddiv_rn(diff, q.w));
 }
 
+// round_output 2 (integer sources coded in normalised units): the value the
+// decoder's caller finally sees is the nearest raw integer, so the bound is
+// checked on it, mapped back: (rint(r * span + offset) - offset) / span.
+__device__ __forceinline__ float round_raw_f(float r, const QParams& q) {
+    const double raw = rint(__dadd_rn(__dmul_rn((double)r, q.rspan), q.roff));
+    return __double2float_rn(__ddiv_rn(__dsub_rn(raw, q.roff), q.rspan));
+}
+__device__ __forceinline__ double round_raw_d(double r, const QParams& q) {
+    const double raw = rint(__dadd_rn(__dmul_rn(r, q.rspan), q.roff));
+    return __ddiv_rn(__dsub_rn(raw, q.roff), q.rspan);
+}
+
 struct QOut {
     uint32_t code;  // 0 = outlier
     int32_t qv;     // bin index when in range
@@ -179,7 +191,8 @@ __device__ __forceinline__ QOut quant_f32(float x, double pd, const QParams& q, 
     if (fabs(qd) < (double)q.radius) {
         const int qi = (int)qd;
         const float rf = __double2float_rn(__dadd_rn(pd, __dmul_rn(q.w, (double)qi)));
-        const float chk = q.round_output ? rintf(rf) : rf;
+        const float chk = q.round_output == 2 ? round_raw_f(rf, q)
+                          : (q.round_output ? rintf(rf) : rf);
         if (fabsf(__fsub_rn(x, chk)) <= q.eb_f) {
             o.code = (uint32_t)(qi + q.radius);
             o.qv = qi;
@@ -197,7 +210,8 @@ __device__ __forceinline__ QOut quant_f64(double x, double pd, const QParams& q,
     if (fabs(qd) < (double)q.radius) {
         const int qi = (int)qd;
         double rd = __dadd_rn(pd, __dmul_rn(q.w, (double)qi));
-        const double chk = q.round_output ? rint(rd) : rd;
+        const double chk = q.round_output == 2 ? round_raw_d(rd, q)
+                           : (q.round_output ? rint(rd) : rd);
         if (fabs(__dsub_rn(x, chk)) <= q.eb) {
             o.code = (uint32_t)(qi + q.radius);
             o.qv = qi;

@@ -22,9 +22,10 @@ struct QParams {
     int order;       // 0 linear, 1 cubic
     int center;      // 0 average, 1 first odd axis, 2 last odd axis
     int end_mode;    // bit 0 quadratic ends, bit 1 extrapolation
-    int round_output;
+    int round_output;  // 0 none, 1 rint, 2 via the raw integer (rspan / roff)
     int channels;
     uint64_t points;  // grid points per channel
+    double rspan, roff;  // round_output 2: the data range and its minimum
 };
 
 // Per-stage device accumulators (one struct per stage).

@@ -99,6 +99,12 @@ int latec_quantize_static(const latec_quant_params* prm, double eb, uint64_t ite
     q.center = prm->center;
     q.end_mode = prm->end_mode;
     q.round_output = prm->round_output;
+    if (q.round_output < 0 || q.round_output > 2 ||
+        (q.round_output == 2 && !(prm->round_span > 0.0 && std::isfinite(prm->round_span) &&
+                                  std::isfinite(prm->round_offset))))
+        return LATEC_ERR_ARG;
+    q.rspan = q.round_output == 2 ? prm->round_span : 1.0;
+    q.roff = q.round_output == 2 ? prm->round_offset : 0.0;
     q.channels = prm->channels;
     q.points = items;
     cudaStream_t st = (cudaStream_t)stream;

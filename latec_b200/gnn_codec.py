@@ -34,7 +34,10 @@ Scope of this version:
   keeps the GNN only where it codes fewer bits. One gate word per stage, in
   the reference's bit layout, travels in the header. ``gate_fine`` selects the
   same per-stage gate (there is no chunk grid to share a word across).
-* Float inputs only.
+* Float, signed and unsigned integer and bool inputs: integers are coded in
+  normalised float32; for signed integers and bools the bound is checked on
+  the nearest raw integer the decoder returns (``round_output`` with the data
+  span and minimum), as in the reference.
 * ``fp16=True`` (the default, as in the reference) runs the message and
   finalisation MLPs in BF16 on the tensor cores (tcgen05) with float32
   accumulation; pools and the readout stay float32. ``fp16=False`` is float32
@@ -130,9 +133,30 @@ def read_stream(stream: bytes):
     return meta, payload
 
 
-def _qparams(radius):
+def _qparams(radius, raw_round=None):
+    """Quantizer parameters; ``raw_round = (span, offset)`` checks the bound
+    on the nearest raw integer of integer sources (``_quantize_t``'s
+    ``round_output`` pair, latec/gnn_codec.py:998-1031)."""
+    if raw_round:
+        return _lib.QuantParams(dtype=_lib.F32, channels=1, radius=int(radius), order=1, center=0,
+                                end_mode=1, round_output=2, reserved=0,
+                                round_span=float(raw_round[0]), round_offset=float(raw_round[1]))
     return _lib.QuantParams(dtype=_lib.F32, channels=1, radius=int(radius), order=1, center=0,
                             end_mode=1, round_output=0, reserved=0)
+
+
+def _restore_dtype(out, dtype):
+    """Decoded float32 values back to the source dtype: integers round to the
+    nearest and clip to the type's range, bools threshold at 0.5
+    (latec/gnn_codec.py:179-185)."""
+    torch = _torch()
+    if dtype.kind in "iu":
+        info = np.iinfo(dtype)
+        r = torch.clamp(torch.round(out.double()), float(info.min), float(info.max))
+        return r.to(getattr(torch, dtype.name))
+    if dtype.kind == "b":
+        return out >= 0.5
+    return out.to(getattr(torch, dtype.name)) if dtype != np.float32 else out
 
 
 def gate_scale_grid(eb: float, device):
@@ -309,8 +333,6 @@ class GNNCodec:
         np_dtype = np.dtype(str(arr.dtype).replace("torch.", "")) if is_t else np.dtype(arr.dtype)
         if np_dtype.kind not in "biuf":
             raise TypeError(f"unsupported dtype {np_dtype}; expected numeric data")
-        if np_dtype.kind != "f":
-            raise NotImplementedError("the GNN codec here codes floating-point tensors")
         eb = float(error_bound)
         if eb <= 0:
             raise ValueError("error_bound must be > 0")
@@ -331,6 +353,8 @@ class GNNCodec:
         edges = tuple(-(-n // stride) * stride for n in shape)
         t = arr if is_t else torch.from_numpy(np.ascontiguousarray(arr))
         t = t.reshape(shape).to(self.device)
+        if np_dtype.kind != "f":  # integer / bool sources are coded in float32
+            t = t.to(torch.float32)
         mm = torch.aminmax(t)
         vmin = float(np.float32(float(mm.min.item())))
         vmax = float(np.float32(float(mm.max.item())))
@@ -338,6 +362,9 @@ class GNNCodec:
             vmax = vmin + 1.0
         span = vmax - vmin
         xn = ((t.to(torch.float32) - np.float32(vmin)) / np.float32(span)).reshape(-1).contiguous()
+        # signed integers and bools are finally rounded to the nearest raw
+        # integer, so the bound is checked on that value
+        raw_round = (span, vmin) if np_dtype.kind in "bi" else None
         coarse = ([float(eb_ratio)] if eb_ratio is not None
                   else (list(EB_COARSE_SWEEP) if tune == "size" else [EB_COARSE_FACTOR]))
         ratios = sorted({per_step_eb_ratio(c, lv) for c in coarse})
@@ -348,7 +375,8 @@ class GNNCodec:
             raise ValueError("fp8 needs the tensor-core path (fp16=True, d = 64)")
         model = self._model(precision)
         for ratio in ratios:
-            payload, words = self._encode(model, xn, shape, lv, eb, ratio, radius, bool(gate))
+            payload, words = self._encode(model, xn, shape, lv, eb, ratio, radius, bool(gate),
+                                          raw_round)
             meta = {"shape": list(original_shape), "dtype": np_dtype.str, "error_bound": eb,
                     "levels": lv, "radius": radius, "vmin": vmin, "vmax": vmax,
                     "eb_ratio": ratio, "checkpoint_hash": self.checkpoint_hash.hex(),
@@ -387,13 +415,13 @@ class GNNCodec:
                    "latec_interp_predict_stage")
         return out
 
-    def _encode(self, model, xn, shape, levels, eb, ratio, radius, gate=True):
+    def _encode(self, model, xn, shape, levels, eb, ratio, radius, gate=True, raw_round=None):
         torch = _torch()
         lib = _lib.load()
         geoms = self._geometry(shape, levels)
         ebs = self._stage_ebs(shape, levels, eb, ratio)
         plan, pstages = self._plan_stages(shape, levels)
-        prm = _qparams(radius)
+        prm = _qparams(radius, raw_round)
         dev = self.device
         E = torch.zeros((1, xn.numel(), len(shape), self.d), dtype=torch.float32, device=dev)
         recon_all = torch.zeros(xn.numel(), dtype=torch.float32, device=dev)
@@ -538,8 +566,7 @@ class GNNCodec:
         if int(model.tc_err.item()):
             raise RuntimeError("a tensor-core wait ran out during the GNN forward")
         out = recon_all * np.float32(vmax - vmin) + np.float32(vmin)
-        out = out.reshape(original_shape).cpu()
-        return out.to(getattr(torch, dtype.name)) if dtype != np.float32 else out
+        return _restore_dtype(out.reshape(original_shape).cpu(), dtype)
 
     decompress = uncompress
 

@@ -140,8 +140,6 @@ def test_gnn_codec_float64_and_errors():
     with pytest.raises(ValueError):
         codec.compress(x, 0.0)
     with pytest.raises(NotImplementedError):
-        codec.compress(x.astype(np.int32), 1e-3)
-    with pytest.raises(NotImplementedError):
         codec.compress(x, 1e-3, levels=3, chunk_size=8)
     with pytest.raises(FileNotFoundError):
         GNNCodec("/nonexistent/checkpoint.pt")
@@ -187,3 +185,81 @@ def test_fp8_float_path_round_trip():
     assert np.abs(on.astype(np.float64) - xn).max() <= 1e-3 + 4 * np.finfo(np.float32).eps
     with pytest.raises(ValueError):
         codec.compress(x, 1e-3, levels=3, fp8=True, fp16=False)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", [np.int16, np.int32, np.uint8, np.bool_])
+def test_integer_sources_round_trip(dtype):
+    import torch
+
+    codec = _codec()
+    f = _field((36, 34), 6)
+    if dtype == np.bool_:
+        x = f > np.median(f)
+    elif dtype == np.uint8:
+        x = np.clip((f - f.min()) / (f.max() - f.min()) * 255, 0, 255).round().astype(np.uint8)
+    else:
+        x = np.round(f * 900).astype(dtype)
+    eb = 2e-3
+    s = codec.compress(x, eb, levels=3)
+    out = codec.uncompress(s)
+    assert out.dtype == getattr(torch, np.dtype(dtype).name) and tuple(out.shape) == x.shape
+    o = out.numpy()
+    if dtype == np.bool_:
+        assert np.array_equal(o, x)  # a bound below 0.5 of the range keeps every bool
+        return
+    span = float(np.float32(x.max())) - float(np.float32(x.min()))
+    err = np.abs(o.astype(np.float64) - x.astype(np.float64)).max()
+    # signed integers: the bound is checked on the returned integer itself;
+    # unsigned ones (as in the reference) only on the float reconstruction
+    limit = eb * span * (1 + 1e-5) + (0.0 if np.dtype(dtype).kind == "i" else 0.5)
+    assert err <= limit, (err, limit)
+
+
+@pytest.mark.gpu
+def test_flat_quantizer_checks_the_raw_integer():
+    """round_output 2 against a NumPy restatement of _quantize_t's (span,
+    offset) check (latec/gnn_codec.py:998-1031)."""
+    import ctypes
+
+    import torch
+
+    from latec_b200 import _lib
+
+    lib = _lib.load()
+    rs = np.random.RandomState(9)
+    n = 200_000
+    span, off = 1234.0, -17.0
+    raw = rs.randint(-17, 1217, n).astype(np.float64)
+    x = ((raw - off) / span).astype(np.float32)
+    pred = (x + rs.randn(n).astype(np.float32) * 3e-3).astype(np.float32)
+    # above half a raw unit (0.5 / 1234 in normalised terms): the nearest raw
+    # integer of a reconstruction can be the wrong one, and the check rejects it
+    eb = 7e-4
+    prm = _lib.QuantParams(dtype=_lib.F32, channels=1, radius=RADIUS, order=1, center=0,
+                           end_mode=1, round_output=2, reserved=0, round_span=span,
+                           round_offset=off)
+    xd, pd = torch.from_numpy(x).cuda(), torch.from_numpy(pred).cuda()
+    codes = torch.empty(n, dtype=torch.int16, device="cuda")
+    recon = torch.empty(n, dtype=torch.float32, device="cuda")
+    outl = torch.empty(n, dtype=torch.float32, device="cuda")
+    stats = torch.zeros(ctypes.sizeof(_lib.StageStats), dtype=torch.uint8, device="cuda")
+    hseg = torch.empty(512, dtype=torch.int32, device="cuda")
+    htot = torch.empty(65536, dtype=torch.int32, device="cuda")
+    ws = torch.empty(int(lib.latec_flat_workspace_bytes(n, _lib.F32)), dtype=torch.uint8,
+                     device="cuda")
+    _lib.check(lib.latec_quantize(ctypes.byref(prm), eb, n, xd.data_ptr(), pd.data_ptr(),
+                                  codes.data_ptr(), recon.data_ptr(), outl.data_ptr(),
+                                  stats.data_ptr(), hseg.data_ptr(), htot.data_ptr(),
+                                  ws.data_ptr(), ws.numel(), torch.cuda.current_stream().cuda_stream))
+    got = codes.cpu().numpy().view(np.uint16).astype(np.int64)
+    w = 2.0 * eb
+    q = np.rint((x.astype(np.float64) - pred.astype(np.float64)) / w).astype(np.int64)
+    inr = np.abs(q) < RADIUS
+    cand = np.where(inr, q + RADIUS, 0)
+    rc = (pred.astype(np.float64) + w * (cand - RADIUS)).astype(np.float32)
+    chk = ((np.rint(rc.astype(np.float64) * span + off) - off) / span).astype(np.float32)
+    ok = inr & (np.abs(x - chk) <= np.float32(eb))
+    want = np.where(ok, cand, 0)
+    assert np.array_equal(got, want)
+    assert 0 < (want == 0).sum() < n  # the check rejects some, keeps most
