@@ -25,7 +25,11 @@ The decoder repeats the same float path and dequantizes on the device.
 
 Scope of this version:
 
-* The whole tensor is one region: no chunk grid and no halos.
+* Tensors above 2^21 points (or with a ``chunk_size``) are cut into a chunk
+  grid (the reference's automatic edges); every chunk is an independent
+  region with its own anchors (no halo context from its neighbours, unlike
+  the reference), and chunks of one shape are coded together as one batch
+  through the GNN, the gate, the quantizer and one rANS blob per stage.
 * The scale-gated interpolation fallback (``gate=True``, the default) is
   chosen per stage: the encoder scores the GNN against the cubic,
   first-axis-linear and last-axis-linear interpolation of the stage's points
@@ -157,6 +161,63 @@ def _restore_dtype(out, dtype):
     if dtype.kind == "b":
         return out >= 0.5
     return out.to(getattr(torch, dtype.name)) if dtype != np.float32 else out
+
+
+def auto_chunk_edges(shape, stride):
+    """Largest near-isotropic chunk under the automatic point budget
+    (``_auto_chunk_edges``, latec/gnn_codec.py:286-314): axes shorter than the
+    budget's edge are taken whole; edges are multiples of the anchor stride."""
+    target = AUTO_CHUNK_THRESHOLD
+    fixed, remaining = 1, len(shape)
+    full = set()
+    for axis in sorted(range(len(shape)), key=lambda a: shape[a]):
+        free_edge = (target / fixed) ** (1.0 / remaining)
+        if shape[axis] > free_edge:
+            break
+        full.add(axis)
+        fixed *= shape[axis]
+        remaining -= 1
+        if not remaining:
+            break
+    free_edge = (target / fixed) ** (1.0 / remaining) if remaining else 0.0
+    return tuple(max(stride, -(-n // stride) * stride) if a in full
+                 else max(stride, int(free_edge) // stride * stride)
+                 for a, n in enumerate(shape))
+
+
+def chunk_edges(shape, stride, chunk_size):
+    """Chunk edges, or None when the tensor is coded as one region: ``None``
+    chunk_size chunks only tensors above the automatic budget
+    (``_chunk_edges``, latec/gnn_codec.py:1549-1574)."""
+    if chunk_size is None:
+        if int(np.prod(shape)) <= AUTO_CHUNK_THRESHOLD:
+            return None
+        edges = auto_chunk_edges(shape, stride)
+    else:
+        edges = ((int(chunk_size),) * len(shape) if np.isscalar(chunk_size)
+                 else tuple(int(e) for e in chunk_size))
+        if len(edges) != len(shape):
+            raise ValueError("chunk_size must be scalar or one entry per axis")
+        for e in edges:
+            if e < stride or e % stride:
+                raise ValueError("chunk_size must be a positive multiple of anchor_stride")
+    return None if all(e >= n for e, n in zip(edges, shape)) else tuple(edges)
+
+
+def chunk_groups(shape, edges):
+    """Chunks of the grid in raster order, grouped by their shape (groups in
+    order of first appearance): [(chunk shape, [origins])]."""
+    grid = [-(-n // e) for n, e in zip(shape, edges)]
+    groups = {}
+    for idx in np.ndindex(*grid):
+        origin = tuple(i * e for i, e in zip(idx, edges))
+        cshape = tuple(min(e, n - o) for e, n, o in zip(edges, shape, origin))
+        groups.setdefault(cshape, []).append(origin)
+    return list(groups.items())
+
+
+def _chunk_slices(origin, cshape):
+    return tuple(slice(o, o + c) for o, c in zip(origin, cshape))
 
 
 def gate_scale_grid(eb: float, device):
@@ -340,17 +401,8 @@ class GNNCodec:
         shape = original_shape if original_shape else (1,)
         lv = auto_levels(shape, self.agg_level) if isinstance(levels, str) else int(levels)
         stride = 1 << lv
-        if chunk_size is not None:
-            edges = ((int(chunk_size),) * len(shape) if np.isscalar(chunk_size)
-                     else tuple(int(e) for e in chunk_size))
-            if len(edges) != len(shape):
-                raise ValueError("chunk_size must be scalar or one entry per axis")
-            for e in edges:
-                if e < stride or e % stride:
-                    raise ValueError("chunk_size must be a positive multiple of anchor_stride")
-            if any(e < n for e, n in zip(edges, shape)):
-                raise NotImplementedError("the GNN codec here codes the tensor as one region")
-        edges = tuple(-(-n // stride) * stride for n in shape)
+        cedges = chunk_edges(shape, stride, chunk_size)
+        edges = cedges or tuple(-(-n // stride) * stride for n in shape)
         t = arr if is_t else torch.from_numpy(np.ascontiguousarray(arr))
         t = t.reshape(shape).to(self.device)
         if np_dtype.kind != "f":  # integer / bool sources are coded in float32
@@ -374,9 +426,23 @@ class GNNCodec:
         if fp8 and not reduced:
             raise ValueError("fp8 needs the tensor-core path (fp16=True, d = 64)")
         model = self._model(precision)
+        cbatch = self._chunk_batch(edges) if cedges else 1
         for ratio in ratios:
-            payload, words = self._encode(model, xn, shape, lv, eb, ratio, radius, bool(gate),
-                                          raw_round)
+            if cedges is None:
+                payload, words = self._encode(model, xn.reshape(1, -1), shape, lv, eb, ratio,
+                                              radius, bool(gate), raw_round)
+            else:  # chunks of one shape coded in batches
+                xg = xn.reshape(shape)
+                parts, words = [], []
+                for cshape, origins in chunk_groups(shape, edges):
+                    for b0 in range(0, len(origins), cbatch):
+                        X = torch.stack([xg[_chunk_slices(o, cshape)].reshape(-1)
+                                         for o in origins[b0:b0 + cbatch]])
+                        part, w = self._encode(model, X, cshape, lv, eb, ratio, radius,
+                                               bool(gate), raw_round)
+                        parts.append(part)
+                        words += w
+                payload = b"".join(parts)
             meta = {"shape": list(original_shape), "dtype": np_dtype.str, "error_bound": eb,
                     "levels": lv, "radius": radius, "vmin": vmin, "vmax": vmax,
                     "eb_ratio": ratio, "checkpoint_hash": self.checkpoint_hash.hex(),
@@ -384,6 +450,8 @@ class GNNCodec:
                     "predictor": "gnn", "float_path": FLOAT_PATHS[precision], "d": self.d,
                     "agg_level": self.agg_level, "gate": bool(gate), "gate_fine": bool(gate_fine),
                     "gates": pack_gates(words)}
+            if cedges is not None:
+                meta["chunk_batch"] = cbatch
             if int(model.tc_err.item()):
                 raise RuntimeError("a tensor-core wait ran out during the GNN forward")
             stream = write_stream(meta, payload, zstd_level)
@@ -399,15 +467,23 @@ class GNNCodec:
         plan = plan_for(shape, levels, 1 << levels, 1)
         return plan, [t for t, n in enumerate(plan.counts) if n]
 
+    def _chunk_batch(self, edges):
+        """Chunks coded together: the embedding field of a batch (chunk points
+        x axes x d float32) and its message-pass workspace stay near 16 GB."""
+        per = int(np.prod(edges)) * len(edges) * self.d * 4 * 3
+        return max(1, min(64, int(16e9 // per)))
+
     def _gate_candidate(self, plan, stage, kind, recon_all, n, radius):
         """Interpolation candidate ``kind`` (1 cubic axis-average, 2 first-axis
-        linear, 3 last-axis linear) of a stage from the reconstruction."""
+        linear, 3 last-axis linear) of a stage from the reconstruction
+        ``recon_all`` (B, N): n = B * stage points, region-major."""
         import ctypes
 
         torch = _torch()
         order, center = GATE_KINDS[kind]
         out = torch.empty(n, dtype=torch.float32, device=self.device)
-        prm = _lib.QuantParams(dtype=_lib.F32, channels=1, radius=int(radius), order=order,
+        prm = _lib.QuantParams(dtype=_lib.F32, channels=int(recon_all.shape[0]),
+                               radius=int(radius), order=order,
                                center=center, end_mode=GATE_END_MODE, round_output=0, reserved=0)
         _lib.check(_lib.load().latec_interp_predict_stage(plan.handle, stage, ctypes.byref(prm),
                                                           recon_all.data_ptr(), out.data_ptr(),
@@ -415,7 +491,10 @@ class GNNCodec:
                    "latec_interp_predict_stage")
         return out
 
-    def _encode(self, model, xn, shape, levels, eb, ratio, radius, gate=True, raw_round=None):
+    def _encode(self, model, X, shape, levels, eb, ratio, radius, gate=True, raw_round=None):
+        """Code B regions of one shape at once: X (B, N) normalised values.
+        Every stage runs the GNN over the batch, and its codes (region-major)
+        form one rANS blob; one gate word per stage serves the batch."""
         torch = _torch()
         lib = _lib.load()
         geoms = self._geometry(shape, levels)
@@ -423,16 +502,17 @@ class GNNCodec:
         plan, pstages = self._plan_stages(shape, levels)
         prm = _qparams(radius, raw_round)
         dev = self.device
-        E = torch.zeros((1, xn.numel(), len(shape), self.d), dtype=torch.float32, device=dev)
-        recon_all = torch.zeros(xn.numel(), dtype=torch.float32, device=dev)
+        B, N = int(X.shape[0]), int(X.shape[1])
+        E = torch.zeros((B, N, len(shape), self.d), dtype=torch.float32, device=dev)
+        recon_all = torch.zeros((B, N), dtype=torch.float32, device=dev)
         records, words, prev, ctx, vals = [], [], None, None, None
         for gi, (g, seb) in enumerate(zip(geoms, ebs)):
             (mu, lb), E, ctx = gnn.stage_forward(model, E, prev, g, vals, finalize_ctx=ctx,
                                                  eb=seb)
             mu = mu.reshape(-1).contiguous()
             scale = torch.exp2(lb.reshape(-1)).contiguous()
-            xs = xn[g.query_idx].contiguous()
-            n = g.M
+            xs = X[:, g.query_idx].reshape(-1).contiguous()
+            n = B * g.M
             word = 0
             if gate and gi > 0 and n:
                 # the interpolation fallback: score, choose, apply (on the device)
@@ -479,8 +559,8 @@ class GNNCodec:
             frame = bitstream.pack_frame(len(blob), kexp, shape_id, 0, 0, False)
             records.append(struct.pack("<IQ", n, frame) + blob + struct.pack("<I", n_out)
                            + outl[:n_out].cpu().numpy().astype("<f4").tobytes())
-            recon_all[g.query_idx] = recon
-            prev, vals = g, recon.reshape(1, -1)
+            recon_all[:, g.query_idx] = recon.reshape(B, -1)
+            prev, vals = g, recon.reshape(B, -1)
         return b"".join(records), words
 
     # ---------------------------------------------------------------- decode
@@ -503,17 +583,53 @@ class GNNCodec:
         if vmax <= vmin:
             vmax = vmin + 1.0
         levels, radius = int(meta["levels"]), int(meta["radius"])
+        eb, ratio = float(meta["error_bound"]), float(meta["eb_ratio"])
+        words = unpack_gates(meta["gates"]) if meta.get("gates") else None
+        err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        if "chunk_batch" in meta:  # chunks of one shape, decoded in the encoder's batches
+            edges = tuple(int(e) for e in meta["chunks"])
+            cbatch = int(meta["chunk_batch"])
+            if len(edges) != len(shape) or cbatch < 1:
+                raise ValueError("malformed chunk grid")
+            out = torch.empty(shape, dtype=torch.float32, device=self.device)
+            off, wi = 0, 0
+            for cshape, origins in chunk_groups(shape, edges):
+                for b0 in range(0, len(origins), cbatch):
+                    sub = origins[b0:b0 + cbatch]
+                    R, off, wi = self._decode(model, payload, off, len(sub), cshape, levels, eb,
+                                              ratio, radius, words, wi, err)
+                    for j, o in enumerate(sub):
+                        out[_chunk_slices(o, cshape)] = R[j].reshape(cshape)
+            recon_all = out.reshape(-1)
+        else:
+            R, off, wi = self._decode(model, payload, 0, 1, shape, levels, eb, ratio, radius,
+                                      words, 0, err)
+            recon_all = R.reshape(-1)
+        if off != len(payload):
+            raise ValueError("trailing data in GNN stage payload")
+        if words is not None and wi != len(words):
+            raise ValueError("gate words do not match the stage schedule")
+        if int(err.item()):
+            raise ValueError("outlier count mismatch")
+        if int(model.tc_err.item()):
+            raise RuntimeError("a tensor-core wait ran out during the GNN forward")
+        out = recon_all * np.float32(vmax - vmin) + np.float32(vmin)
+        return _restore_dtype(out.reshape(original_shape).cpu(), dtype)
+
+    def _decode(self, model, payload, off, B, shape, levels, eb, ratio, radius, words, wi, err):
+        """Decode B regions of one shape from ``payload`` at ``off``; returns
+        (recon (B, N), the offset after them, the next gate word index)."""
+        torch = _torch()
+        lib = _lib.load()
         geoms = self._geometry(shape, levels)
-        ebs = self._stage_ebs(shape, levels, float(meta["error_bound"]), float(meta["eb_ratio"]))
+        ebs = self._stage_ebs(shape, levels, eb, ratio)
         prm = _qparams(radius)
         dev = self.device
         N = int(np.prod(shape))
-        recon_all = torch.zeros(N, dtype=torch.float32, device=dev)
-        E = torch.zeros((1, N, len(shape), self.d), dtype=torch.float32, device=dev)
-        off, prev, ctx, vals = 0, None, None, None
-        err = torch.zeros(1, dtype=torch.int32, device=dev)
-        words = unpack_gates(meta["gates"]) if meta.get("gates") else [0] * len(geoms)
-        if len(words) != len(geoms):
+        recon_all = torch.zeros((B, N), dtype=torch.float32, device=dev)
+        E = torch.zeros((B, N, len(shape), self.d), dtype=torch.float32, device=dev)
+        prev, ctx, vals = None, None, None
+        if words is not None and wi + len(geoms) > len(words):
             raise ValueError("gate words do not match the stage schedule")
         plan, pstages = self._plan_stages(shape, levels)
         for gi, (g, seb) in enumerate(zip(geoms, ebs)):
@@ -524,7 +640,7 @@ class GNNCodec:
                 raise ValueError("truncated GNN stage payload")
             n, frame = struct.unpack_from("<IQ", payload, off)
             f = bitstream.unpack_frame(frame)
-            if n != g.M:
+            if n != B * g.M:
                 raise ValueError("stage size differs from the schedule")
             blob = payload[off + 12:off + 12 + f["hlen"]]
             off += 12 + f["hlen"]
@@ -532,11 +648,13 @@ class GNNCodec:
                 raise ValueError("truncated GNN stage payload")
             (n_out,) = struct.unpack_from("<I", payload, off)
             off += 4
+            if off + 4 * n_out > len(payload):
+                raise ValueError("truncated GNN stage payload")
             outl = np.frombuffer(payload, "<f4", count=n_out, offset=off) if n_out else \
                 np.zeros(1, np.float32)
             off += 4 * n_out
             scale = torch.exp2(lb.reshape(-1)).contiguous()
-            kind, direction, T, shift = gate_fields(int(words[gi]))
+            kind, direction, T, shift = gate_fields(int(words[wi + gi])) if words else (0, 0, 0, 0)
             if kind:
                 if gi == 0 or kind not in GATE_KINDS:
                     raise ValueError("invalid gate word")
@@ -557,16 +675,9 @@ class GNNCodec:
                                             outl_d.data_ptr(), n_out, recon.data_ptr(),
                                             err.data_ptr(), ws.data_ptr(), ws.numel(),
                                             _lib.stream_ptr()), "latec_dequantize")
-            recon_all[g.query_idx] = recon
-            prev, vals = g, recon.reshape(1, -1)
-        if off != len(payload):
-            raise ValueError("trailing data in GNN stage payload")
-        if int(err.item()):
-            raise ValueError("outlier count mismatch")
-        if int(model.tc_err.item()):
-            raise RuntimeError("a tensor-core wait ran out during the GNN forward")
-        out = recon_all * np.float32(vmax - vmin) + np.float32(vmin)
-        return _restore_dtype(out.reshape(original_shape).cpu(), dtype)
+            recon_all[:, g.query_idx] = recon.reshape(B, -1)
+            prev, vals = g, recon.reshape(B, -1)
+        return recon_all, off, wi + len(geoms)
 
     decompress = uncompress
 

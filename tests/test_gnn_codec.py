@@ -139,8 +139,8 @@ def test_gnn_codec_float64_and_errors():
         codec.compress(np.zeros((0, 4), np.float32), 1e-3)
     with pytest.raises(ValueError):
         codec.compress(x, 0.0)
-    with pytest.raises(NotImplementedError):
-        codec.compress(x, 1e-3, levels=3, chunk_size=8)
+    with pytest.raises(ValueError):
+        codec.compress(x, 1e-3, levels=3, chunk_size=12)  # not a multiple of the stride
     with pytest.raises(FileNotFoundError):
         GNNCodec("/nonexistent/checkpoint.pt")
 
@@ -263,3 +263,46 @@ def test_flat_quantizer_checks_the_raw_integer():
     want = np.where(ok, cand, 0)
     assert np.array_equal(got, want)
     assert 0 < (want == 0).sum() < n  # the check rejects some, keeps most
+
+
+def test_chunk_grid_on_host():
+    """The automatic edges of the reference's rule, and a grid that covers every
+    point exactly once, chunks grouped by shape in raster order."""
+    from latec_b200.gnn_codec import (AUTO_CHUNK_THRESHOLD, auto_chunk_edges, chunk_edges,
+                                      chunk_groups)
+
+    assert auto_chunk_edges((128, 128, 64, 64), 32) == (32, 32, 32, 32)
+    assert chunk_edges((128, 128, 64, 64), 32, None) == (32, 32, 32, 32)
+    assert chunk_edges((64, 64), 16, None) is None  # below the budget: one region
+    assert chunk_edges((64, 64), 16, 64) is None
+    assert chunk_edges((64, 64), 16, (32, 16)) == (32, 16)
+    e = auto_chunk_edges((4000, 3), 8)
+    assert e[1] == 8 and e[0] % 8 == 0 and e[0] * 3 <= 2 * AUTO_CHUNK_THRESHOLD
+    for shape, edges in (((70, 66), (16, 16)), ((9, 40, 33), (8, 16, 8))):
+        seen = np.zeros(shape, np.int32)
+        for cshape, origins in chunk_groups(shape, edges):
+            for o in origins:
+                assert tuple(min(e, n - a) for e, n, a in zip(edges, shape, o)) == cshape
+                seen[tuple(slice(a, a + c) for a, c in zip(o, cshape))] += 1
+        assert np.all(seen == 1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,levels,chunk", [((70, 66), 3, 16), ((24, 40, 18), 2, (8, 16, 8))])
+def test_chunked_round_trip_holds_the_bound(shape, levels, chunk):
+    from latec_b200.gnn_codec import read_stream
+
+    codec = _codec()
+    x = _field(shape, 11)
+    s = codec.compress(x, 1e-3, levels=levels, chunk_size=chunk)
+    meta, _ = read_stream(s)
+    assert meta["chunk_batch"] >= 1 and meta["chunks"] == list(
+        (chunk,) * len(shape) if np.isscalar(chunk) else chunk)
+    assert codec.compress(x, 1e-3, levels=levels, chunk_size=chunk) == s  # deterministic
+    out = codec.uncompress(s).numpy()
+    vmin, vmax = float(np.float32(x.min())), float(np.float32(x.max()))
+    xn = (x.astype(np.float32) - np.float32(vmin)) / np.float32(vmax - vmin)
+    on = (out - np.float32(vmin)) / np.float32(vmax - vmin)
+    assert np.abs(on.astype(np.float64) - xn).max() <= 1e-3 + 4 * np.finfo(np.float32).eps
+    one = codec.compress(x, 1e-3, levels=levels)  # the same tensor as one region
+    assert "chunk_batch" not in read_stream(one)[0]
