@@ -592,71 +592,80 @@ __global__ void __launch_bounds__(THREADS, 2)
 }
 
 // ------------------------------------------------------------------ decode
-// Computed points of a unit, in prefetch order: even planes A (HR x TC),
-// B (TR x HC), C (TR x TC); odd planes D (HR x HC), E (HR x TC), F (TR x HC),
-// G (TR x TC).
-template <typename T>
-struct DecList {
-    using B = Box<T>;
-    static constexpr int A = B::HR_N * B::TC_N, Bn = B::TR_N * B::HC_N, C = B::TR_N * B::TC_N;
-    static constexpr int D = B::HR_N * B::HC_N;
-    static constexpr int ODD = D + A + Bn + C;
-    static constexpr int PF = (ODD + THREADS - 1) / THREADS;
-    // f -> box (r, b) and stage; false past the end
-    __device__ static __forceinline__ bool locate(int f, bool even, int& r, int& b, int& stage) {
-        int rows0, nc, b0, st;
-        if (even) {
-            if (f < A) { rows0 = B::HR_R0; nc = B::TC_N; b0 = B::TC_B0; st = 2; }
-            else if ((f -= A) < Bn) { rows0 = B::TR_R0; nc = B::HC_N; b0 = B::HC_B0; st = 1; }
-            else if ((f -= Bn) < C) { rows0 = B::TR_R0; nc = B::TC_N; b0 = B::TC_B0; st = 3; }
-            else return false;
-        } else {
-            if (f < D) { rows0 = B::HR_R0; nc = B::HC_N; b0 = B::HC_B0; st = 0; }
-            else if ((f -= D) < A) { rows0 = B::HR_R0; nc = B::TC_N; b0 = B::TC_B0; st = 3; }
-            else if ((f -= A) < Bn) { rows0 = B::TR_R0; nc = B::HC_N; b0 = B::HC_B0; st = 3; }
-            else if ((f -= Bn) < C) { rows0 = B::TR_R0; nc = B::TC_N; b0 = B::TC_B0; st = 4; }
-            else return false;
-        }
-        const int i = f / nc;
-        r = rows0 + 2 * i;
-        b = b0 + 2 * (f - i * nc);
-        stage = st;
-        return true;
-    }
-};
-
 // Codes of a unit's computed points into registers (issued early; stored to
-// shared memory once the current unit is done).
-template <typename T>
-__device__ __forceinline__ void fetch_codes(const TileLevel& L, const Ranks& rk, const Item& it,
-                                            int z, bool even, uint16_t* pf) {
-    using DL = DecList<T>;
+// shared memory once the current unit is done). One compile-time loop per
+// class region: fixed register slots, constant divisors, the stage known.
+template <typename T, int STAGE, int R0, int NR, int B0, int NC>
+__device__ __forceinline__ void fetch_region(const TileLevel& L, const Ranks& rk, const Item& it,
+                                             int z, uint16_t* pf) {
+    constexpr int K = (NR * NC + THREADS - 1) / THREADS;
+    const uint16_t* codes = L.st[STAGE].codes + (uint64_t)it.c * L.st[STAGE].n;
 #pragma unroll
-    for (int k = 0; k < DL::PF; k++) {
-        pf[k] = 1;
-        int r, b, s;
-        if (z < 0 || z >= L.N[0] || !DL::locate(threadIdx.x + k * THREADS, even, r, b, s)) continue;
-        const int y = it.y0 - 3 + r, x = it.x0 - 4 + b;
-        if (y < 0 || y >= L.N[1] || x < 0 || x >= L.N[2]) continue;
-        uint32_t rr;
-        switch (s) {
-            case 0: rr = rk.of<0>(z, y, x); break;
-            case 1: rr = rk.of<1>(z, y, x); break;
-            case 2: rr = rk.of<2>(z, y, x); break;
-            case 3: rr = rk.of<3>(z, y, x); break;
-            default: rr = rk.of<4>(z, y, x); break;
-        }
-        pf[k] = __ldg(L.st[s].codes + (uint64_t)it.c * L.st[s].n + rr);
+    for (int k = 0; k < K; k++) {
+        const int e = threadIdx.x + k * THREADS;
+        const int i = e / NC;
+        const int y = it.y0 - 3 + R0 + 2 * i, x = it.x0 - 4 + B0 + 2 * (e - i * NC);
+        pf[k] = (e < NR * NC && y >= 0 && y < L.N[1] && x >= 0 && x < L.N[2])
+                    ? __ldg(codes + rk.of<STAGE>(z, y, x))
+                    : (uint16_t)1;
+    }
+}
+
+template <typename T, int R0, int NR, int B0, int NC>
+__device__ __forceinline__ void put_region(const uint16_t* pf, uint16_t* dst) {
+    constexpr int K = (NR * NC + THREADS - 1) / THREADS;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        const int e = threadIdx.x + k * THREADS;
+        const int i = e / NC;
+        if (e < NR * NC) dst[(R0 + 2 * i) * Box<T>::BX + B0 + 2 * (e - i * NC)] = pf[k];
     }
 }
 
 template <typename T>
-__device__ __forceinline__ void put_codes(bool even, const uint16_t* pf, uint16_t* dst) {
-    using DL = DecList<T>;
-#pragma unroll
-    for (int k = 0; k < DL::PF; k++) {
-        int r, b, s;
-        if (DL::locate(threadIdx.x + k * THREADS, even, r, b, s)) dst[r * Box<T>::BX + b] = pf[k];
+struct DecSlots {  // register slots per region: even A, B, C; odd D, E, F, G
+    using B = Box<T>;
+    static constexpr int k(int n) { return (n + THREADS - 1) / THREADS; }
+    static constexpr int A = k(B::HR_N * B::TC_N), Bn = k(B::TR_N * B::HC_N),
+                         C = k(B::TR_N * B::TC_N), D = k(B::HR_N * B::HC_N);
+    static constexpr int EVEN = A + Bn + C, ODD = D + A + Bn + C;
+    static constexpr int PF = EVEN > ODD ? EVEN : ODD;
+};
+
+template <typename T>
+__device__ __forceinline__ void fetch_codes(const TileLevel& L, const Ranks& rk, const Item& it,
+                                            int z, bool even, uint16_t* pf) {
+    using B = Box<T>;
+    using S = DecSlots<T>;
+    if (z < 0 || z >= L.N[0]) return;
+    if (even) {
+        fetch_region<T, 2, B::HR_R0, B::HR_N, B::TC_B0, B::TC_N>(L, rk, it, z, pf);
+        fetch_region<T, 1, B::TR_R0, B::TR_N, B::HC_B0, B::HC_N>(L, rk, it, z, pf + S::A);
+        fetch_region<T, 3, B::TR_R0, B::TR_N, B::TC_B0, B::TC_N>(L, rk, it, z, pf + S::A + S::Bn);
+    } else {
+        fetch_region<T, 0, B::HR_R0, B::HR_N, B::HC_B0, B::HC_N>(L, rk, it, z, pf);
+        fetch_region<T, 3, B::HR_R0, B::HR_N, B::TC_B0, B::TC_N>(L, rk, it, z, pf + S::D);
+        fetch_region<T, 3, B::TR_R0, B::TR_N, B::HC_B0, B::HC_N>(L, rk, it, z, pf + S::D + S::A);
+        fetch_region<T, 4, B::TR_R0, B::TR_N, B::TC_B0, B::TC_N>(L, rk, it, z,
+                                                                  pf + S::D + S::A + S::Bn);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void put_codes(int z, int n0, bool even, const uint16_t* pf,
+                                          uint16_t* dst) {
+    using B = Box<T>;
+    using S = DecSlots<T>;
+    if (z < 0 || z >= n0) return;
+    if (even) {
+        put_region<T, B::HR_R0, B::HR_N, B::TC_B0, B::TC_N>(pf, dst);
+        put_region<T, B::TR_R0, B::TR_N, B::HC_B0, B::HC_N>(pf + S::A, dst);
+        put_region<T, B::TR_R0, B::TR_N, B::TC_B0, B::TC_N>(pf + S::A + S::Bn, dst);
+    } else {
+        put_region<T, B::HR_R0, B::HR_N, B::HC_B0, B::HC_N>(pf, dst);
+        put_region<T, B::HR_R0, B::HR_N, B::TC_B0, B::TC_N>(pf + S::D, dst);
+        put_region<T, B::TR_R0, B::TR_N, B::HC_B0, B::HC_N>(pf + S::D + S::A, dst);
+        put_region<T, B::TR_R0, B::TR_N, B::TC_B0, B::TC_N>(pf + S::D + S::A + S::Bn, dst);
     }
 }
 
@@ -681,14 +690,13 @@ template <typename T, int CUBIC>
 __global__ void __launch_bounds__(THREADS, 2)
     k_tile_level_dec(const TileLevel L, T* __restrict__ recon) {
     using B = Box<T>;
-    using DL = DecList<T>;
     extern __shared__ __align__(16) uint8_t smem[];
     T* planes = (T*)smem;
     uint16_t* csm = (uint16_t*)(planes + B::SLOTS * B::ELEMS);  // 2 x ELEMS codes
     const bool vec = L.vec != 0;
     Ranks rk;
     rk.init(L.N);
-    uint16_t pf[DL::PF];
+    uint16_t pf[DecSlots<T>::PF];
     for (uint32_t w = blockIdx.x; w < L.items; w += gridDim.x) {
         const Item it = item_of<T>(L, w);
         const int n_units = n_units_of(it);
@@ -700,7 +708,7 @@ __global__ void __launch_bounds__(THREADS, 2)
                               recon, vec);
             cp_commit();
             fetch_codes<T>(L, rk, it, z, ev, pf);
-            put_codes<T>(ev, pf, csm);
+            put_codes<T>(z, L.N[0], ev, pf, csm);
         }
         for (int k = 0; k < n_units; k++) {
             bool nev = true;
@@ -741,7 +749,7 @@ __global__ void __launch_bounds__(THREADS, 2)
                 __syncthreads();
                 if (u.owned) store_plane<T>(L, it, z, even, u.P, recon, vec);
             }
-            put_codes<T>(nev, pf, csm + ((k + 1) & 1) * B::ELEMS);
+            put_codes<T>(nz, L.N[0], nev, pf, csm + ((k + 1) & 1) * B::ELEMS);
             __syncthreads();
         }
         cp_wait_all();
