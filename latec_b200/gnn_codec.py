@@ -36,8 +36,10 @@ Scope of this version:
   with the reference's rANS-aligned Laplace rate, per bucket of the model's
   scale relative to eb * 2^T (``latec/gnn_codec.py:386-462, 920-1000``), and
   keeps the GNN only where it codes fewer bits. One gate word per stage, in
-  the reference's bit layout, travels in the header. ``gate_fine`` selects the
-  same per-stage gate (there is no chunk grid to share a word across).
+  the reference's bit layout, travels in the header. With ``gate_fine`` the
+  finest level's sub-stages share one word per region batch, chosen at the
+  first of them (``latec/gnn_codec.py:453-462,1229-1262``); those words travel
+  apart from the per-stage ones, as the reference's ``fine_gates``.
 * Float, signed and unsigned integer and bool inputs: integers are coded in
   normalised float32; for signed integers and bools the bound is checked on
   the nearest raw integer the decoder returns (``round_output`` with the data
@@ -64,7 +66,7 @@ from pathlib import Path
 import numpy as np
 
 from . import _lib, bitstream, gnn, rans
-from .levels import stage_ebs
+from .levels import stage_ebs, stage_strides
 
 MAGIC = b"LATECGNN"
 VERSION = 14
@@ -387,6 +389,8 @@ class GNNCodec:
         radius = int(radius)
         if not 1 <= radius <= 32768:
             raise ValueError("radius must be in [1, 32768]")
+        gate = bool(gate)
+        gate_fine = bool(gate_fine) and gate
         is_t = isinstance(x, torch.Tensor)
         arr = x.detach() if is_t else np.asarray(x)
         if (arr.numel() if is_t else arr.size) == 0:
@@ -429,27 +433,31 @@ class GNNCodec:
         cbatch = self._chunk_batch(edges) if cedges else 1
         for ratio in ratios:
             if cedges is None:
-                payload, words = self._encode(model, xn.reshape(1, -1), shape, lv, eb, ratio,
-                                              radius, bool(gate), raw_round)
+                payload, words, fine_words = self._encode(model, xn.reshape(1, -1), shape, lv,
+                                                          eb, ratio, radius, gate, raw_round,
+                                                          gate_fine)
             else:  # chunks of one shape coded in batches
                 xg = xn.reshape(shape)
-                parts, words = [], []
+                parts, words, fine_words = [], [], []
                 for cshape, origins in chunk_groups(shape, edges):
                     for b0 in range(0, len(origins), cbatch):
                         X = torch.stack([xg[_chunk_slices(o, cshape)].reshape(-1)
                                          for o in origins[b0:b0 + cbatch]])
-                        part, w = self._encode(model, X, cshape, lv, eb, ratio, radius,
-                                               bool(gate), raw_round)
+                        part, w, fw = self._encode(model, X, cshape, lv, eb, ratio, radius,
+                                                   gate, raw_round, gate_fine)
                         parts.append(part)
                         words += w
+                        fine_words += fw
                 payload = b"".join(parts)
             meta = {"shape": list(original_shape), "dtype": np_dtype.str, "error_bound": eb,
                     "levels": lv, "radius": radius, "vmin": vmin, "vmax": vmax,
                     "eb_ratio": ratio, "checkpoint_hash": self.checkpoint_hash.hex(),
                     "chunks": list(edges), "m_tile": 1 << 16, "fp16": reduced, "compiled": False,
                     "predictor": "gnn", "float_path": FLOAT_PATHS[precision], "d": self.d,
-                    "agg_level": self.agg_level, "gate": bool(gate), "gate_fine": bool(gate_fine),
+                    "agg_level": self.agg_level, "gate": gate, "gate_fine": gate_fine,
                     "gates": pack_gates(words)}
+            if gate_fine:
+                meta["fine_gates"] = pack_gates(fine_words)
             if cedges is not None:
                 meta["chunk_batch"] = cbatch
             if int(model.tc_err.item()):
@@ -491,10 +499,13 @@ class GNNCodec:
                    "latec_interp_predict_stage")
         return out
 
-    def _encode(self, model, X, shape, levels, eb, ratio, radius, gate=True, raw_round=None):
+    def _encode(self, model, X, shape, levels, eb, ratio, radius, gate=True, raw_round=None,
+                gate_fine=False):
         """Code B regions of one shape at once: X (B, N) normalised values.
         Every stage runs the GNN over the batch, and its codes (region-major)
-        form one rANS blob; one gate word per stage serves the batch."""
+        form one rANS blob; one gate word per stage serves the batch. With
+        ``gate_fine`` the finest level's sub-stages reuse the gate chosen at
+        the first of them. Returns (payload, per-stage words, finest words)."""
         torch = _torch()
         lib = _lib.load()
         geoms = self._geometry(shape, levels)
@@ -505,7 +516,10 @@ class GNNCodec:
         B, N = int(X.shape[0]), int(X.shape[1])
         E = torch.zeros((B, N, len(shape), self.d), dtype=torch.float32, device=dev)
         recon_all = torch.zeros((B, N), dtype=torch.float32, device=dev)
-        records, words, prev, ctx, vals = [], [], None, None, None
+        strides = stage_strides(len(shape), levels, 1 << levels)
+        finest = [strides[t] == 1 for t in pstages]
+        records, words, fine_words, fine_desc = [], [], [], None
+        prev, ctx, vals = None, None, None
         for gi, (g, seb) in enumerate(zip(geoms, ebs)):
             (mu, lb), E, ctx = gnn.stage_forward(model, E, prev, g, vals, finalize_ctx=ctx,
                                                  eb=seb)
@@ -514,26 +528,38 @@ class GNNCodec:
             xs = X[:, g.query_idx].reshape(-1).contiguous()
             n = B * g.M
             word = 0
+            shared = gate_fine and finest[gi]
             if gate and gi > 0 and n:
                 # the interpolation fallback: score, choose, apply (on the device)
-                ips = [self._gate_candidate(plan, pstages[gi], k, recon_all, n, radius)
-                       for k in (1, 2, 3)]
-                sums = torch.zeros(len(GATE_KINDS) * len(GATE_SHIFTS) * (len(GATE_T) + 1)
-                                   + len(GATE_T) + 1, dtype=torch.int64, device=dev)
-                thr, grid = gate_scale_grid(seb, dev)
-                _lib.check(lib.latec_gate_costs(n, xs.data_ptr(), mu.data_ptr(), ips[0].data_ptr(),
-                                                ips[1].data_ptr(), ips[2].data_ptr(),
-                                                scale.data_ptr(), seb, radius, thr.data_ptr(),
-                                                grid.data_ptr(), sums.data_ptr(),
-                                                _lib.stream_ptr()), "latec_gate_costs")
-                kind, direction, T, shift = gate_choose(sums.cpu().numpy())
+                if shared and fine_desc is not None:
+                    kind, direction, T, shift = fine_desc
+                    ip = (self._gate_candidate(plan, pstages[gi], kind, recon_all, n, radius)
+                          if kind else None)
+                else:
+                    ips = [self._gate_candidate(plan, pstages[gi], k, recon_all, n, radius)
+                           for k in (1, 2, 3)]
+                    sums = torch.zeros(len(GATE_KINDS) * len(GATE_SHIFTS) * (len(GATE_T) + 1)
+                                       + len(GATE_T) + 1, dtype=torch.int64, device=dev)
+                    thr, grid = gate_scale_grid(seb, dev)
+                    _lib.check(lib.latec_gate_costs(n, xs.data_ptr(), mu.data_ptr(),
+                                                    ips[0].data_ptr(), ips[1].data_ptr(),
+                                                    ips[2].data_ptr(), scale.data_ptr(), seb,
+                                                    radius, thr.data_ptr(), grid.data_ptr(),
+                                                    sums.data_ptr(), _lib.stream_ptr()),
+                               "latec_gate_costs")
+                    kind, direction, T, shift = gate_choose(sums.cpu().numpy())
+                    ip = ips[kind - 1] if kind else None
+                    if shared:
+                        fine_desc = (kind, direction, T, shift)
+                        fine_words.append(gate_word(kind, direction, T, shift))
                 if kind:
                     _lib.check(lib.latec_gate_apply(n, mu.data_ptr(), scale.data_ptr(),
-                                                    ips[kind - 1].data_ptr(), seb, T, shift,
-                                                    direction, _lib.stream_ptr()),
+                                                    ip.data_ptr(), seb, T, shift, direction,
+                                                    _lib.stream_ptr()),
                                "latec_gate_apply")
                 word = gate_word(kind, direction, T, shift)
-            words.append(word)
+            if not shared:
+                words.append(word)
             codes = torch.empty(n, dtype=torch.int16, device=dev)
             recon = torch.empty(n, dtype=torch.float32, device=dev)
             outl = torch.empty(n, dtype=torch.float32, device=dev)
@@ -561,7 +587,7 @@ class GNNCodec:
                            + outl[:n_out].cpu().numpy().astype("<f4").tobytes())
             recon_all[:, g.query_idx] = recon.reshape(B, -1)
             prev, vals = g, recon.reshape(B, -1)
-        return b"".join(records), words
+        return b"".join(records), words, fine_words
 
     # ---------------------------------------------------------------- decode
     def uncompress(self, stream):
@@ -585,6 +611,9 @@ class GNNCodec:
         levels, radius = int(meta["levels"]), int(meta["radius"])
         eb, ratio = float(meta["error_bound"]), float(meta["eb_ratio"])
         words = unpack_gates(meta["gates"]) if meta.get("gates") else None
+        fine = unpack_gates(meta.get("fine_gates", "")) if meta.get("gate_fine") else None
+        if fine is not None and words is None:
+            raise ValueError("finest-level gate words without per-stage gate words")
         err = torch.zeros(1, dtype=torch.int32, device=self.device)
         if "chunk_batch" in meta:  # chunks of one shape, decoded in the encoder's batches
             edges = tuple(int(e) for e in meta["chunks"])
@@ -592,22 +621,22 @@ class GNNCodec:
             if len(edges) != len(shape) or cbatch < 1:
                 raise ValueError("malformed chunk grid")
             out = torch.empty(shape, dtype=torch.float32, device=self.device)
-            off, wi = 0, 0
+            off, wi, fi = 0, 0, 0
             for cshape, origins in chunk_groups(shape, edges):
                 for b0 in range(0, len(origins), cbatch):
                     sub = origins[b0:b0 + cbatch]
-                    R, off, wi = self._decode(model, payload, off, len(sub), cshape, levels, eb,
-                                              ratio, radius, words, wi, err)
+                    R, off, wi, fi = self._decode(model, payload, off, len(sub), cshape, levels,
+                                                  eb, ratio, radius, words, wi, fine, fi, err)
                     for j, o in enumerate(sub):
                         out[_chunk_slices(o, cshape)] = R[j].reshape(cshape)
             recon_all = out.reshape(-1)
         else:
-            R, off, wi = self._decode(model, payload, 0, 1, shape, levels, eb, ratio, radius,
-                                      words, 0, err)
+            R, off, wi, fi = self._decode(model, payload, 0, 1, shape, levels, eb, ratio,
+                                          radius, words, 0, fine, 0, err)
             recon_all = R.reshape(-1)
         if off != len(payload):
             raise ValueError("trailing data in GNN stage payload")
-        if words is not None and wi != len(words):
+        if (words is not None and wi != len(words)) or (fine is not None and fi != len(fine)):
             raise ValueError("gate words do not match the stage schedule")
         if int(err.item()):
             raise ValueError("outlier count mismatch")
@@ -616,9 +645,12 @@ class GNNCodec:
         out = recon_all * np.float32(vmax - vmin) + np.float32(vmin)
         return _restore_dtype(out.reshape(original_shape).cpu(), dtype)
 
-    def _decode(self, model, payload, off, B, shape, levels, eb, ratio, radius, words, wi, err):
-        """Decode B regions of one shape from ``payload`` at ``off``; returns
-        (recon (B, N), the offset after them, the next gate word index)."""
+    def _decode(self, model, payload, off, B, shape, levels, eb, ratio, radius, words, wi,
+                fine, fi, err):
+        """Decode B regions of one shape from ``payload`` at ``off``, reading
+        per-stage gate words from ``words[wi:]`` and, when the stream shares
+        one word over the finest level, that word from ``fine[fi]``; returns
+        (recon (B, N), the offset after them, the next wi, the next fi)."""
         torch = _torch()
         lib = _lib.load()
         geoms = self._geometry(shape, levels)
@@ -629,9 +661,14 @@ class GNNCodec:
         recon_all = torch.zeros((B, N), dtype=torch.float32, device=dev)
         E = torch.zeros((B, N, len(shape), self.d), dtype=torch.float32, device=dev)
         prev, ctx, vals = None, None, None
-        if words is not None and wi + len(geoms) > len(words):
-            raise ValueError("gate words do not match the stage schedule")
         plan, pstages = self._plan_stages(shape, levels)
+        strides = stage_strides(len(shape), levels, 1 << levels)
+        shared = [fine is not None and strides[t] == 1 for t in pstages]
+        if words is not None and wi + shared.count(False) > len(words):
+            raise ValueError("gate words do not match the stage schedule")
+        if any(shared) and fi >= len(fine):
+            raise ValueError("gate words do not match the stage schedule")
+        fine_desc = None
         for gi, (g, seb) in enumerate(zip(geoms, ebs)):
             (mu, lb), E, ctx = gnn.stage_forward(model, E, prev, g, vals, finalize_ctx=ctx,
                                                  eb=seb)
@@ -654,7 +691,16 @@ class GNNCodec:
                 np.zeros(1, np.float32)
             off += 4 * n_out
             scale = torch.exp2(lb.reshape(-1)).contiguous()
-            kind, direction, T, shift = gate_fields(int(words[wi + gi])) if words else (0, 0, 0, 0)
+            if shared[gi]:
+                if fine_desc is None:
+                    fine_desc = gate_fields(int(fine[fi]))
+                    fi += 1
+                kind, direction, T, shift = fine_desc
+            elif words is not None:
+                kind, direction, T, shift = gate_fields(int(words[wi]))
+                wi += 1
+            else:
+                kind, direction, T, shift = 0, 0, 0, 0
             if kind:
                 if gi == 0 or kind not in GATE_KINDS:
                     raise ValueError("invalid gate word")
@@ -677,7 +723,7 @@ class GNNCodec:
                                             _lib.stream_ptr()), "latec_dequantize")
             recon_all[:, g.query_idx] = recon.reshape(B, -1)
             prev, vals = g, recon.reshape(B, -1)
-        return recon_all, off, wi + len(geoms)
+        return recon_all, off, wi, fi
 
     decompress = uncompress
 

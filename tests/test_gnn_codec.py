@@ -170,6 +170,53 @@ def test_gate_falls_back_to_interpolation_where_it_codes_fewer_bits(shape, level
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("shape,levels,chunk", [((64, 60), 4, None), ((24, 22, 20), 3, None),
+                                                ((40, 36), 2, 16)])
+def test_gate_fine_shares_one_word_over_the_finest_level(shape, levels, chunk):
+    from latec_b200.gnn_codec import (chunk_edges, chunk_groups, pack_gates, read_stream,
+                                      unpack_gates, write_stream)
+    from latec_b200.levels import stage_counts, stage_strides
+
+    codec = _codec()
+    x = _field(shape, 9)
+    fine = codec.compress(x, 1e-3, levels=levels, gate_fine=True, chunk_size=chunk)
+    per = codec.compress(x, 1e-3, levels=levels, chunk_size=chunk)
+    (mf, payload), mp = read_stream(fine), read_stream(per)[0]
+    assert mf["gate_fine"] and not mp["gate_fine"] and "fine_gates" not in mp
+    # the per-stage stream's words, cut into batches; its finest words give way
+    # to the first of them in the shared-word stream
+    stride = 1 << levels
+    edges = chunk_edges(shape, stride, chunk) or shape
+    cb = mf.get("chunk_batch", 1)
+    wp, want_gates, want_fine = unpack_gates(mp["gates"]), [], []
+    for cshape, origins in chunk_groups(shape, edges):
+        counts = stage_counts(cshape, levels, stride)
+        strides = stage_strides(len(shape), levels, stride)
+        finest = [s == 1 for s, n in zip(strides, counts) if n]
+        for _ in range(0, len(origins), cb):
+            ws, wp = wp[:len(finest)], wp[len(finest):]
+            want_gates += [w for w, f in zip(ws, finest) if not f]
+            want_fine += [w for w, f in zip(ws, finest) if f][:1]
+    assert not wp
+    assert unpack_gates(mf["gates"]) == want_gates
+    assert unpack_gates(mf["fine_gates"]) == want_fine
+    assert codec.compress(x, 1e-3, levels=levels, gate_fine=True, chunk_size=chunk) == fine
+    out = codec.uncompress(fine).numpy()
+    vmin, vmax = float(np.float32(x.min())), float(np.float32(x.max()))
+    xn = (x.astype(np.float32) - np.float32(vmin)) / np.float32(vmax - vmin)
+    on = (out - np.float32(vmin)) / np.float32(vmax - vmin)
+    assert np.abs(on.astype(np.float64) - xn).max() <= 1e-3 + 4 * np.finfo(np.float32).eps
+    # without the gate there is nothing to share
+    off = read_stream(codec.compress(x, 1e-3, levels=levels, gate=False, gate_fine=True,
+                                     chunk_size=chunk))[0]
+    assert not off["gate_fine"] and "fine_gates" not in off
+    # a finest word short is a malformed stream
+    bad = dict(mf, fine_gates=pack_gates(unpack_gates(mf["fine_gates"])[:-1]))
+    with pytest.raises(ValueError):
+        codec.uncompress(write_stream(bad, payload, 3))
+
+
+@pytest.mark.gpu
 def test_fp8_float_path_round_trip():
     from latec_b200.gnn_codec import read_stream
 
