@@ -78,7 +78,9 @@ AUTO_CHUNK_THRESHOLD = 1 << 21
 RANK_LEVELS = {2: 8, 4: 5, 5: 4}
 EB_COARSE_FACTOR = 0.9
 EB_COARSE_SWEEP = (1.0, 0.9, 0.65, 0.41)
-INTERP_KINDS = {"interp-cubic": 1, "interp-linear-first": 2, "interp-linear-last": 3}
+# the predictor ablation (latec/gnn_codec.py:755-774): the model replaced by
+# the gate's interpolation candidate of that kind, coded against a flat scale
+INTERP_KINDS = {"interp-cubic": 1, "interp-linear": 2, "interp-linear-last": 3}
 # gate sweep (latec/gnn_codec.py:399-403): thresholds eb * 2^T, scale shifts,
 # and the word layout dir (bit 10) | kind (bits 8-9) | T (bits 4-7) | shift
 GATE_T = tuple(range(2, 14))
@@ -384,12 +386,11 @@ class GNNCodec:
             raise ValueError("levels must be >= 1")
         if predictor != "gnn" and predictor not in INTERP_KINDS:
             raise ValueError(f"predictor must be 'gnn' or one of {sorted(INTERP_KINDS)}")
-        if predictor != "gnn":
-            raise NotImplementedError("the interpolation ablation of the GNN codec is not built")
+        interp_kind = INTERP_KINDS.get(predictor, 0)
         radius = int(radius)
         if not 1 <= radius <= 32768:
             raise ValueError("radius must be in [1, 32768]")
-        gate = bool(gate)
+        gate = bool(gate) and not interp_kind  # no model prediction to fall back from
         gate_fine = bool(gate_fine) and gate
         is_t = isinstance(x, torch.Tensor)
         arr = x.detach() if is_t else np.asarray(x)
@@ -435,7 +436,7 @@ class GNNCodec:
             if cedges is None:
                 payload, words, fine_words = self._encode(model, xn.reshape(1, -1), shape, lv,
                                                           eb, ratio, radius, gate, raw_round,
-                                                          gate_fine)
+                                                          gate_fine, interp_kind)
             else:  # chunks of one shape coded in batches
                 xg = xn.reshape(shape)
                 parts, words, fine_words = [], [], []
@@ -444,7 +445,7 @@ class GNNCodec:
                         X = torch.stack([xg[_chunk_slices(o, cshape)].reshape(-1)
                                          for o in origins[b0:b0 + cbatch]])
                         part, w, fw = self._encode(model, X, cshape, lv, eb, ratio, radius,
-                                                   gate, raw_round, gate_fine)
+                                                   gate, raw_round, gate_fine, interp_kind)
                         parts.append(part)
                         words += w
                         fine_words += fw
@@ -453,7 +454,7 @@ class GNNCodec:
                     "levels": lv, "radius": radius, "vmin": vmin, "vmax": vmax,
                     "eb_ratio": ratio, "checkpoint_hash": self.checkpoint_hash.hex(),
                     "chunks": list(edges), "m_tile": 1 << 16, "fp16": reduced, "compiled": False,
-                    "predictor": "gnn", "float_path": FLOAT_PATHS[precision], "d": self.d,
+                    "predictor": predictor, "float_path": FLOAT_PATHS[precision], "d": self.d,
                     "agg_level": self.agg_level, "gate": gate, "gate_fine": gate_fine,
                     "gates": pack_gates(words)}
             if gate_fine:
@@ -499,13 +500,26 @@ class GNNCodec:
                    "latec_interp_predict_stage")
         return out
 
+    def _interp_stage(self, plan, stage, gi, kind, recon_all, n, seb, radius):
+        """(prediction, scale) of a stage under the interpolation ablation
+        (``_interp_stage_pred``, latec/gnn_codec.py:763-774): the gate's
+        candidate of ``kind`` (0 for the anchors, as the reference's anchor
+        pass) and a flat scale of the stage's eb."""
+        torch = _torch()
+        mu = (self._gate_candidate(plan, stage, kind, recon_all, n, radius) if gi else
+              torch.zeros(n, dtype=torch.float32, device=self.device))
+        return mu, torch.full((n,), float(seb), dtype=torch.float32, device=self.device)
+
     def _encode(self, model, X, shape, levels, eb, ratio, radius, gate=True, raw_round=None,
-                gate_fine=False):
+                gate_fine=False, interp_kind=0):
         """Code B regions of one shape at once: X (B, N) normalised values.
         Every stage runs the GNN over the batch, and its codes (region-major)
         form one rANS blob; one gate word per stage serves the batch. With
         ``gate_fine`` the finest level's sub-stages reuse the gate chosen at
-        the first of them. Returns (payload, per-stage words, finest words)."""
+        the first of them. ``interp_kind`` codes with that interpolation
+        candidate instead of the model, against a flat scale of the stage's eb
+        (the anchors against 0). Returns (payload, per-stage words, finest
+        words)."""
         torch = _torch()
         lib = _lib.load()
         geoms = self._geometry(shape, levels)
@@ -514,19 +528,24 @@ class GNNCodec:
         prm = _qparams(radius, raw_round)
         dev = self.device
         B, N = int(X.shape[0]), int(X.shape[1])
-        E = torch.zeros((B, N, len(shape), self.d), dtype=torch.float32, device=dev)
+        E = None if interp_kind else torch.zeros((B, N, len(shape), self.d),
+                                                 dtype=torch.float32, device=dev)
         recon_all = torch.zeros((B, N), dtype=torch.float32, device=dev)
         strides = stage_strides(len(shape), levels, 1 << levels)
         finest = [strides[t] == 1 for t in pstages]
         records, words, fine_words, fine_desc = [], [], [], None
         prev, ctx, vals = None, None, None
         for gi, (g, seb) in enumerate(zip(geoms, ebs)):
-            (mu, lb), E, ctx = gnn.stage_forward(model, E, prev, g, vals, finalize_ctx=ctx,
-                                                 eb=seb)
-            mu = mu.reshape(-1).contiguous()
-            scale = torch.exp2(lb.reshape(-1)).contiguous()
-            xs = X[:, g.query_idx].reshape(-1).contiguous()
             n = B * g.M
+            if interp_kind:
+                mu, scale = self._interp_stage(plan, pstages[gi], gi, interp_kind, recon_all, n,
+                                               seb, radius)
+            else:
+                (mu, lb), E, ctx = gnn.stage_forward(model, E, prev, g, vals, finalize_ctx=ctx,
+                                                     eb=seb)
+                mu = mu.reshape(-1).contiguous()
+                scale = torch.exp2(lb.reshape(-1)).contiguous()
+            xs = X[:, g.query_idx].reshape(-1).contiguous()
             word = 0
             shared = gate_fine and finest[gi]
             if gate and gi > 0 and n:
@@ -611,6 +630,10 @@ class GNNCodec:
         levels, radius = int(meta["levels"]), int(meta["radius"])
         eb, ratio = float(meta["error_bound"]), float(meta["eb_ratio"])
         words = unpack_gates(meta["gates"]) if meta.get("gates") else None
+        predictor = meta.get("predictor", "gnn")
+        if predictor != "gnn" and predictor not in INTERP_KINDS:
+            raise ValueError(f"unknown predictor {predictor!r} in stream")
+        interp_kind = INTERP_KINDS.get(predictor, 0)
         fine = unpack_gates(meta.get("fine_gates", "")) if meta.get("gate_fine") else None
         if fine is not None and words is None:
             raise ValueError("finest-level gate words without per-stage gate words")
@@ -626,13 +649,14 @@ class GNNCodec:
                 for b0 in range(0, len(origins), cbatch):
                     sub = origins[b0:b0 + cbatch]
                     R, off, wi, fi = self._decode(model, payload, off, len(sub), cshape, levels,
-                                                  eb, ratio, radius, words, wi, fine, fi, err)
+                                                  eb, ratio, radius, words, wi, fine, fi, err,
+                                                  interp_kind)
                     for j, o in enumerate(sub):
                         out[_chunk_slices(o, cshape)] = R[j].reshape(cshape)
             recon_all = out.reshape(-1)
         else:
             R, off, wi, fi = self._decode(model, payload, 0, 1, shape, levels, eb, ratio,
-                                          radius, words, 0, fine, 0, err)
+                                          radius, words, 0, fine, 0, err, interp_kind)
             recon_all = R.reshape(-1)
         if off != len(payload):
             raise ValueError("trailing data in GNN stage payload")
@@ -646,7 +670,7 @@ class GNNCodec:
         return _restore_dtype(out.reshape(original_shape).cpu(), dtype)
 
     def _decode(self, model, payload, off, B, shape, levels, eb, ratio, radius, words, wi,
-                fine, fi, err):
+                fine, fi, err, interp_kind=0):
         """Decode B regions of one shape from ``payload`` at ``off``, reading
         per-stage gate words from ``words[wi:]`` and, when the stream shares
         one word over the finest level, that word from ``fine[fi]``; returns
@@ -659,7 +683,8 @@ class GNNCodec:
         dev = self.device
         N = int(np.prod(shape))
         recon_all = torch.zeros((B, N), dtype=torch.float32, device=dev)
-        E = torch.zeros((B, N, len(shape), self.d), dtype=torch.float32, device=dev)
+        E = None if interp_kind else torch.zeros((B, N, len(shape), self.d),
+                                                 dtype=torch.float32, device=dev)
         prev, ctx, vals = None, None, None
         plan, pstages = self._plan_stages(shape, levels)
         strides = stage_strides(len(shape), levels, 1 << levels)
@@ -670,9 +695,14 @@ class GNNCodec:
             raise ValueError("gate words do not match the stage schedule")
         fine_desc = None
         for gi, (g, seb) in enumerate(zip(geoms, ebs)):
-            (mu, lb), E, ctx = gnn.stage_forward(model, E, prev, g, vals, finalize_ctx=ctx,
-                                                 eb=seb)
-            mu = mu.reshape(-1).contiguous()
+            if interp_kind:
+                mu, scale = self._interp_stage(plan, pstages[gi], gi, interp_kind, recon_all,
+                                               B * g.M, seb, radius)
+            else:
+                (mu, lb), E, ctx = gnn.stage_forward(model, E, prev, g, vals, finalize_ctx=ctx,
+                                                     eb=seb)
+                mu = mu.reshape(-1).contiguous()
+                scale = torch.exp2(lb.reshape(-1)).contiguous()
             if off + 12 > len(payload):
                 raise ValueError("truncated GNN stage payload")
             n, frame = struct.unpack_from("<IQ", payload, off)
@@ -690,7 +720,6 @@ class GNNCodec:
             outl = np.frombuffer(payload, "<f4", count=n_out, offset=off) if n_out else \
                 np.zeros(1, np.float32)
             off += 4 * n_out
-            scale = torch.exp2(lb.reshape(-1)).contiguous()
             if shared[gi]:
                 if fine_desc is None:
                     fine_desc = gate_fields(int(fine[fi]))

@@ -217,6 +217,60 @@ def test_gate_fine_shares_one_word_over_the_finest_level(shape, levels, chunk):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("predictor,order,center", [("interp-cubic", "cubic", 0),
+                                                    ("interp-linear", "linear", 1),
+                                                    ("interp-linear-last", "linear", 2)])
+@pytest.mark.parametrize("shape,levels", [((40, 36), 3), ((24, 22, 20), 3)])
+def test_interpolation_ablation_reconstructs_as_the_plain_codec(predictor, order, center, shape,
+                                                                levels):
+    """The ablation codes every stage against the gate's interpolation
+    candidate (anchors against 0), so on the normalised field its
+    reconstruction is the plain codec's with that predictor, bit for bit."""
+    import torch
+
+    import latec_b200 as lb
+    from latec_b200.gnn_codec import (EB_COARSE_FACTOR, GATE_END_MODE, per_step_eb_ratio,
+                                      read_stream, unpack_gates)
+
+    codec = _codec()
+    x = _field(shape, 13)
+    s = codec.compress(x, 1e-3, levels=levels, predictor=predictor)
+    meta, _ = read_stream(s)
+    assert meta["predictor"] == predictor and not meta["gate"]
+    assert not any(unpack_gates(meta["gates"]))
+    assert codec.compress(x, 1e-3, levels=levels, predictor=predictor) == s
+    out = codec.uncompress(s)
+    vmin, vmax = float(np.float32(x.min())), float(np.float32(x.max()))
+    span = vmax - vmin
+    xn = ((torch.from_numpy(x).cuda() - np.float32(vmin)) / np.float32(span)).contiguous()
+    stride = 1 << levels
+    pred = lb.InterpPredictor(order, levels, stride, 1, center=center, end_mode=GATE_END_MODE)
+    _, st = lb.compress(xn, 1e-3, pred, levels=levels, anchor_stride=stride,
+                        eb_ratio=per_step_eb_ratio(EB_COARSE_FACTOR, levels), recon="device")
+    want = st["recon"].reshape(shape) * np.float32(span) + np.float32(vmin)
+    assert torch.equal(out.cuda(), want)
+    gnn_s = codec.compress(x, 1e-3, levels=levels)
+    assert read_stream(gnn_s)[0]["predictor"] == "gnn"
+    with pytest.raises(ValueError):
+        codec.compress(x, 1e-3, levels=levels, predictor="interp-quintic")
+
+
+@pytest.mark.gpu
+def test_interpolation_ablation_on_a_chunk_grid():
+    from latec_b200.gnn_codec import read_stream
+
+    codec = _codec()
+    x = _field((70, 66), 14)
+    s = codec.compress(x, 1e-3, levels=3, chunk_size=16, predictor="interp-cubic")
+    assert read_stream(s)[0]["chunk_batch"] >= 1
+    out = codec.uncompress(s).numpy()
+    vmin, vmax = float(np.float32(x.min())), float(np.float32(x.max()))
+    xn = (x.astype(np.float32) - np.float32(vmin)) / np.float32(vmax - vmin)
+    on = (out - np.float32(vmin)) / np.float32(vmax - vmin)
+    assert np.abs(on.astype(np.float64) - xn).max() <= 1e-3 + 4 * np.finfo(np.float32).eps
+
+
+@pytest.mark.gpu
 def test_fp8_float_path_round_trip():
     from latec_b200.gnn_codec import read_stream
 
