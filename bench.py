@@ -601,7 +601,7 @@ def main():
     kms, kn = ctypes.c_double(), ctypes.c_uint32()
     _lib.check(lib.latec_set_tile_mode(1))
     _lib.check(lib.latec_set_kernel_timing(1))
-    for kind in (0, 1):
+    for kind in (0, 1, 2, 3):
         _lib.check(lib.latec_kernel_time(kind, ctypes.byref(kms), ctypes.byref(kn)))
     for i in range(3):
         _lib.check(lib.latec_encode_stages(plan.handle, ctypes.byref(prm), eb_arr, x.data_ptr(),
@@ -616,6 +616,8 @@ def main():
     enc_ms = kms.value / max(1, kn.value)
     _lib.check(lib.latec_kernel_time(1, ctypes.byref(kms), ctypes.byref(kn)))
     dec_ms = kms.value / max(1, kn.value)
+    for kind in (2, 3):  # the lane coder's pairs of these calls: not reported here
+        _lib.check(lib.latec_kernel_time(kind, ctypes.byref(kms), ctypes.byref(kn)))
     _lib.check(lib.latec_set_kernel_timing(0))
     _lib.check(lib.latec_set_tile_mode(0))
     alg_bytes = sum(plan.counts) * (4 + 4 + 2)

@@ -174,10 +174,11 @@ int latec_set_tile_mode(int32_t mode);
 
 /* ---- kernel timing (a measurement aid, no counterpart in the reference):
  *      with timing on, a CUDA event pair is recorded on the launching stream
- *      around every fused tile-level launch. latec_kernel_time sums the
- *      recorded pairs of one kind (0 = encode, 1 = decode; it waits for their
- *      end events), returns the milliseconds and the launch count, and clears
- *      them. Process-wide. */
+ *      around every fused tile-level launch and every native lane-coder
+ *      launch. latec_kernel_time sums the recorded pairs of one kind (0 = tile
+ *      encode, 1 = tile decode, 2 = lane encode, 3 = lane decode; it waits for
+ *      their end events), returns the milliseconds and the launch count, and
+ *      clears them. Process-wide. */
 int latec_set_kernel_timing(int32_t on);
 int latec_kernel_time(int32_t kind, double* ms, uint32_t* launches);
 

@@ -158,8 +158,8 @@ void plan_sizes(const latec_plan* plan, int C, uint64_t* max_items, uint64_t* al
 std::atomic<int> g_tile_mode{0};
 
 // Kernel timing (a measurement aid): when on, a CUDA event pair is recorded
-// on the launching stream around every fused-level launch; kind 0 = encode,
-// 1 = decode.
+// on the launching stream around every fused-level launch (kind 0 = encode,
+// 1 = decode) and every lane-coder launch (2 = encode, 3 = decode).
 std::atomic<bool> g_kt_on{false};
 std::mutex g_kt_mu;
 struct KtPair {
@@ -388,7 +388,7 @@ int latec_set_kernel_timing(int32_t on) {
 }
 
 int latec_kernel_time(int32_t kind, double* ms, uint32_t* launches) {
-    if (!ms || !launches || kind < 0 || kind > 1) return LATEC_ERR_ARG;
+    if (!ms || !launches || kind < 0 || kind > 3) return LATEC_ERR_ARG;
     std::lock_guard<std::mutex> lk(g_kt_mu);
     double sum = 0.0;
     uint32_t n = 0;
@@ -841,7 +841,9 @@ int latec_rans_encode(latec_rans_stage* stages, int32_t n_stages, const uint16_t
         return LATEC_ERR_CUDA;
     bool any_compat = false;
     for (int t = 0; t < n_stages; t++) any_compat |= stages[t].mode == LATEC_RANS_COMPAT;
+    const int ki = kt_start(2, st);
     int rc = launch_lanes_encode(dst, n_stages, tc, codes, levels, scratch, chunk_words, err, st);
+    kt_stop(ki, st);
     if (!rc && any_compat)
         rc = launch_stack_encode(dst, n_stages, codes, levels, scratch, stage_words, err, st);
     if (!rc)
@@ -891,8 +893,10 @@ int latec_rans_decode(latec_rans_stage* stages, int32_t n_stages, uint32_t total
     if (cudaMemcpyAsync(dst, stages, sizeof(RansStageDesc) * n_stages, cudaMemcpyHostToDevice, st) !=
         cudaSuccess)
         return LATEC_ERR_CUDA;
+    const int ki = kt_start(3, st);
     int rc = launch_lanes_decode(dst, n_stages, total_chunks ? blocks : 0, (int)max_alpha, words,
                                  chunk_range, levels, codes, err, st);
+    kt_stop(ki, st);
     if (!rc && any_compat) rc = launch_stack_decode(dst, n_stages, words, levels, codes, err, st);
     return rc;
 }

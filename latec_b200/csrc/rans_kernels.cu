@@ -79,6 +79,13 @@ __device__ __forceinline__ uint32_t widen(uint32_t sym, int radius, int kexp) {
 }
 
 // --------------------------------------------------------------- lanes
+// Steps an encoder warp runs per batch. A step's code, level row and table
+// entry do not depend on the coder state, so a batch loads all of them before
+// its serial state updates, and the next batch's codes are in flight
+// meanwhile: one memory latency per batch instead of one per step (a lane's
+// chain of K steps is the kernel's critical path).
+constexpr int ENC_U = 8;
+
 __global__ void __launch_bounds__(128)
     k_lanes_encode(const RansStageDesc* __restrict__ st, int n_stages, uint32_t total_chunks,
                    const uint16_t* __restrict__ codes, const uint8_t* __restrict__ levels,
@@ -99,32 +106,62 @@ __global__ void __launch_bounds__(128)
     uint64_t x = LANE_L;
     uint32_t tail = 0;
     const unsigned lt = (1u << lane) - 1u;
-    for (int k = (int)K - 1; k >= 0; k--) {
-        const uint64_t i = base + (uint64_t)k * 32u + lane;
-        const bool valid = i < d.n;
-        EncSym e;
-        bool flush = false;
-        if (valid) {
-            const uint32_t sym = narrow(c[i], d.radius, d.kexp);
-            const uint32_t row = lv ? lv[i] : 0u;
-            if (sym >= d.alphabet) {
-                atomicOr(err, 2u);
-                e = enc[row * alpha1];
-            } else {
-                e = enc[row * alpha1 + sym];
+    // steps k0, k0 - 1, ..., k0 - ENC_U + 1 of this lane (the encode order)
+    uint16_t nc[ENC_U];
+    uint8_t nr[ENC_U];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int u = 0; u < ENC_U; u++) {
+            const int kk = k0 - u;
+            const uint64_t i = base + (uint64_t)(kk < 0 ? 0 : kk) * 32u + lane;
+            const bool ok = kk >= 0 && i < d.n;
+            nc[u] = ok ? c[i] : (uint16_t)0;
+            nr[u] = (ok && lv) ? lv[i] : (uint8_t)0;
+        }
+    };
+    fetch((int)K - 1);
+    for (int k = (int)K - 1; k >= 0; k -= ENC_U) {  // k is uniform across the warp
+        uint16_t cc[ENC_U];
+        uint8_t rr[ENC_U];
+#pragma unroll
+        for (int u = 0; u < ENC_U; u++) {
+            cc[u] = nc[u];
+            rr[u] = nr[u];
+        }
+        if (k - ENC_U >= 0) fetch(k - ENC_U);
+        EncSym e[ENC_U];
+#pragma unroll
+        for (int u = 0; u < ENC_U; u++) {
+            const int kk = k - u;
+            const uint64_t i = base + (uint64_t)(kk < 0 ? 0 : kk) * 32u + lane;
+            e[u] = EncSym{0, 0, 0, 0, 0};
+            if (kk >= 0 && i < d.n) {
+                const uint32_t sym = narrow(cc[u], d.radius, d.kexp);
+                if (sym >= d.alphabet) {
+                    atomicOr(err, 2u);
+                    e[u] = enc[rr[u] * alpha1];
+                } else {
+                    e[u] = enc[rr[u] * alpha1 + sym];
+                }
             }
-            flush = x >= ((uint64_t)e.freq << 39);
         }
-        const unsigned bal = __ballot_sync(0xffffffffu, flush);
-        const uint32_t ne = __popc(bal);
-        if (flush) {
-            refill_end[-(int64_t)tail - (int64_t)ne + __popc(bal & lt)] = (uint32_t)x;
-            x >>= 32;
-        }
-        tail += ne;
-        if (valid) {
-            const uint64_t q = __umul64hi(x, e.rcp) >> e.shift;
-            x = x + e.bias + q * e.cmpl;
+#pragma unroll
+        for (int u = 0; u < ENC_U; u++) {
+            const int kk = k - u;
+            if (kk < 0) break;
+            const bool valid = base + (uint64_t)kk * 32u + lane < d.n;
+            const bool flush = valid && x >= ((uint64_t)e[u].freq << 39);
+            const unsigned bal = __ballot_sync(0xffffffffu, flush);
+            const uint32_t ne = __popc(bal);
+            if (flush) {
+                refill_end[-(int64_t)tail - (int64_t)ne + __popc(bal & lt)] = (uint32_t)x;
+                x >>= 32;
+            }
+            tail += ne;
+            if (valid) {
+                const uint64_t q = __umul64hi(x, e[u].rcp) >> e[u].shift;
+                x = x + e[u].bias + q * e[u].cmpl;
+            }
         }
     }
     const bool active = base + lane < d.n;
