@@ -417,10 +417,16 @@ class Trainer:
 def train(steps=3000, *, d=64, agg_level=1, shape4=(16, 16, 16, 16), batch4=4,
           shape2=(128, 128), batch2=16, stride4=8, noise_range=(1e-4, 1e-2), lr=2e-3, warmup=100,
           ema_decay=0.999, mse_weight=1.0, seed=0, device=None, log_every=50, out=None,
-          trainer=None, callback=None):
+          trainer=None, callback=None, synthetic=None):
     """Train on mixed 4-D / 2-D synthetic batches (train_h100.sh: 16^4 x 4
-    plus 128^2 x 16 per step); returns the Trainer."""
-    from .synthetic import sample_synthetic_batch
+    plus 128^2 x 16 per step); returns the Trainer. ``synthetic`` overrides
+    the generator's distribution knobs (``latec_b200.synthetic.DEFAULTS``, the
+    reference's synthetic_dist.yaml)."""
+    from .synthetic import DEFAULTS, sample_synthetic_batch
+
+    knobs = dict(DEFAULTS, **(synthetic or {}))
+    gen = {k: knobs[k] for k in ("turbulence_frac", "max_discontinuities", "discontinuity_frac")}
+    corr = {"synthetic": knobs["correlation_4d"], "field2d": knobs["correlation_2d"]}
 
     tr = trainer or Trainer(d=d, agg_level=agg_level, seed=seed, lr=lr, ema_decay=ema_decay,
                             mse_weight=mse_weight, device=device)
@@ -436,7 +442,7 @@ def train(steps=3000, *, d=64, agg_level=1, shape4=(16, 16, 16, 16), batch4=4,
                                         ("field2d", shape2, batch2, int(rng.choice(strides2)))):
             if not bsz:
                 continue
-            x = sample_synthetic_batch(bsz, shp, rng, device=tr.device)
+            x = sample_synthetic_batch(bsz, shp, corr[kind], rng, device=tr.device, **gen)
             eb = sample_noise(bsz, noise_range, rng, tr.device)
             levels = stride.bit_length() - 1
             w = (n4 if kind == "synthetic" else n2) / max(n4 + n2, 1)
@@ -470,10 +476,22 @@ def main(argv=None):
     ap.add_argument("--noise-range", type=float, nargs=2, default=(1e-4, 1e-2))
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default="gnn_trained.pt")
+    # the generator's knobs (the reference trainer's --synthetic-* flags)
+    ap.add_argument("--synthetic-turbulence-frac", type=float, default=None)
+    ap.add_argument("--synthetic-discontinuities", type=int, default=None)
+    ap.add_argument("--synthetic-discontinuity-frac", type=float, default=None)
+    ap.add_argument("--synthetic-correlation", type=float, nargs=2, default=None)
+    ap.add_argument("--synthetic-2d-correlation", type=float, nargs=2, default=None)
     a = ap.parse_args(argv)
+    given = {"turbulence_frac": a.synthetic_turbulence_frac,
+             "max_discontinuities": a.synthetic_discontinuities,
+             "discontinuity_frac": a.synthetic_discontinuity_frac,
+             "correlation_4d": a.synthetic_correlation,
+             "correlation_2d": a.synthetic_2d_correlation}
     train(a.steps, d=a.d, agg_level=a.agg_level, lr=a.lr, warmup=a.warmup, ema_decay=a.ema_decay,
           mse_weight=a.mse_weight, batch4=a.batch4, batch2=a.batch2,
-          noise_range=tuple(a.noise_range), seed=a.seed, out=a.out)
+          noise_range=tuple(a.noise_range), seed=a.seed, out=a.out,
+          synthetic={k: v for k, v in given.items() if v is not None})
 
 
 if __name__ == "__main__":

@@ -32,7 +32,8 @@ def test_gradient_matches_autograd(shape, levels, stride, batch):
 
     w = gnn.random_weights(3, 64, 1)
     tr = Trainer(d=64, agg_level=1, weights=w, mse_weight=0.5, ema_decay=0)
-    x = synthetic.sample_synthetic_batch(batch, shape, np.random.default_rng(7), device="cuda")
+    x = synthetic.sample_synthetic_batch(batch, shape, (1.0, 8.0), np.random.default_rng(7),
+                                         device="cuda")
     eb = torch.tensor(np.geomspace(1e-3, 2e-2, batch), dtype=torch.float32, device="cuda")
     tr.zero_grad()
     bits, mse, mae, npix = tr.run_stages(x, shape, levels, stride, eb, teacher_noise=False)
