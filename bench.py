@@ -391,10 +391,23 @@ def batch_leg(dev, n=BATCH_N, rank=0, world=1):
         nbytes += x.numel() * x.element_size()
         sbytes += s.numel()
     total = time.perf_counter() - t0
+    # the same tensors through the batch API: one compress_many and one
+    # decompress_many call per rank (warm: the timed serial pass above ran
+    # the same shapes)
+    torch.cuda.synchronize()
+    tb0 = time.perf_counter()
+    bs = lb.compress_many(tensors, 1e-3, pred(), levels=4, anchor_stride=16, stream_out="device")
+    torch.cuda.synchronize()
+    tb1 = time.perf_counter()
+    outs = lb.decompress_many(bs, out="device")
+    torch.cuda.synchronize()
+    tb2 = time.perf_counter()
+    del outs, bs
     # the tensors are sharded over the ranks: bytes add up, the slowest rank
     # sets the time
     nbytes, sbytes = reduce_over_ranks([nbytes, sbytes], "sum", world, dev)
     (total,) = reduce_over_ranks([total], "max", world, dev)
+    tbc, tbd = reduce_over_ranks([tb1 - tb0, tb2 - tb1], "max", world, dev)
     lat_ms = np.sort(np.asarray(lat)) * 1e3
     return {"workload": f"{n} tensors sampled from the 1000-tensor population (rank 2/3, "
                         "volume log-uniform 64^2..256^3, 20 % float64, SE-GRF l 2..32), "
@@ -405,7 +418,11 @@ def batch_leg(dev, n=BATCH_N, rank=0, world=1):
             "latency_ms_p99": float(np.percentile(lat_ms, 99)),
             "mode": "serial loop over the public API per rank (no multi-tensor launch), "
                     f"tensors sharded over {world} rank(s)",
-            "latency_scope": "rank 0's tensors"}
+            "latency_scope": "rank 0's tensors",
+            "batch_api": {"call": "compress_many + decompress_many, one call each per rank",
+                          "gbs": nbytes / (tbc + tbd) / 1e9,
+                          "compress_gbs": nbytes / tbc / 1e9,
+                          "decompress_gbs": nbytes / tbd / 1e9}}
 
 
 def run_reference(args, rank):

@@ -95,9 +95,12 @@ def _prepare(img, device):
 
 
 class _Buffers:
-    """Device buffers of one compress/decompress call, reused across tune candidates."""
+    """Device buffers of one compress/decompress call, reused across tune candidates.
+    ``views`` (kind -> tensor of ``sizes()``'s length and dtype) places the
+    codes, outliers, stage statistics and histograms in buffers shared with
+    other tensors (``latec_b200.batch``)."""
 
-    def __init__(self, plan, c, dtype_id, device):
+    def __init__(self, plan, c, dtype_id, device, views=None):
         torch = _torch()
         self.torch = torch
         self.plan = plan
@@ -110,17 +113,31 @@ class _Buffers:
         self.total = int(self.offsets[-1])
         self.segs = [-(-n // rans_model.SEG) for n in self.items]
         self.seg_off = np.concatenate([[0], np.cumsum(self.segs)]).astype(np.int64)
-        ns = len(plan)
-        self.codes = torch.empty(max(self.total, 1), dtype=torch.int16, device=device)
-        self.outliers = torch.empty(max(self.total, 1) * self.elem, dtype=torch.uint8, device=device)
-        self.stats = torch.empty(ns * ctypes.sizeof(_lib.StageStats), dtype=torch.uint8, device=device)
-        self.hist_seg = torch.empty(max(int(self.seg_off[-1]), 1) * 2 * rans_model.HWIN,
-                                    dtype=torch.int32, device=device)
-        self.hist_total = torch.empty(ns * 65536, dtype=torch.int32, device=device)
+        if views is None:
+            views = {k: torch.empty(n, dtype=dt, device=device)
+                     for k, (n, dt) in buffer_sizes(plan, c, self.elem).items()}
+        self.codes, self.outliers = views["codes"], views["outliers"]
+        self.stats, self.hist_seg = views["stats"], views["hist_seg"]
+        self.hist_total = views["hist_total"]
         lib = _lib.load()
         wsb = lib.latec_stage_workspace_bytes(plan.handle, c, self.ldtype)
         self.ws = torch.empty(max(int(wsb), 1), dtype=torch.uint8, device=device)
         self.err = torch.zeros(2, dtype=torch.int64, device=device)
+
+
+def buffer_sizes(plan, c, elem):
+    """kind -> (elements, dtype) of the per-call buffers a ``_Buffers`` may
+    take as views: codes, outliers, stage statistics, segment and full
+    histograms."""
+    torch = _torch()
+    total = sum(n * c for n in plan.counts)
+    segs = sum(-(-(n * c) // rans_model.SEG) for n in plan.counts)
+    ns = len(plan)
+    return {"codes": (max(total, 1), torch.int16),
+            "outliers": (max(total, 1) * elem, torch.uint8),
+            "stats": (ns * ctypes.sizeof(_lib.StageStats), torch.uint8),
+            "hist_seg": (max(segs, 1) * 2 * rans_model.HWIN, torch.int32),
+            "hist_total": (ns * 65536, torch.int32)}
 
 
 def _qparams(dtype_id, c, radius, order, center, end_mode, round_output):
