@@ -490,6 +490,34 @@ def run_profile(args, dev):
                       "rows": rows}), flush=True)
 
 
+def run_profile_gnn(args, dev):
+    """The learned codec on one 32^4 chunk of the 4-D mixed field: warm-up
+    round trips, then one compress + decompress inside a CUDA profiler range
+    (``ncu --profile-from-start off`` captures only those launches)."""
+    import torch
+
+    import latec_b200 as lb
+    from latec_b200 import fields
+
+    x = fields.mixed_4d(GNN_SHAPE, seed=3, device=dev)
+    rel = GNN_EB / (float(x.max().item()) - float(x.min().item()))
+    codec = lb.GNNCodec(checkpoint_path=GNN_CKPT, device=dev)
+    for _ in range(max(1, args.warmup)):
+        codec.uncompress(codec.compress(x, rel, levels=GNN_LEVELS))
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStart()
+    a = time.perf_counter()
+    s = codec.compress(x, rel, levels=GNN_LEVELS)
+    torch.cuda.synchronize()
+    b = time.perf_counter()
+    codec.uncompress(s)
+    torch.cuda.synchronize()
+    c = time.perf_counter()
+    torch.cuda.cudart().cudaProfilerStop()
+    print(json.dumps({"profile_gnn": list(GNN_SHAPE), "ratio": x.numel() * 4 / len(s),
+                      "compress_ms": (b - a) * 1e3, "decompress_ms": (c - b) * 1e3}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -503,6 +531,9 @@ def main():
                     help="only warm-up + timed device round trips (for ncu launch lists)")
     ap.add_argument("--shape", type=int, nargs="+", default=None,
                     help="field shape for --profile (default 512 512 512)")
+    ap.add_argument("--profile-gnn", action="store_true",
+                    help="only the learned codec's round trip on one 32^4 chunk, inside a CUDA "
+                         "profiler range (for ncu launch lists)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -528,6 +559,8 @@ def main():
     lib = _lib.load()
     if args.profile:
         return run_profile(args, dev)
+    if args.profile_gnn:
+        return run_profile_gnn(args, dev)
     x, eb = make_field(dev)
     nbytes = x.numel() * x.element_size()
 
