@@ -92,6 +92,53 @@ __global__ void __launch_bounds__(LT)
     }
 }
 
+// Y[r, j] = b[j] + sum_i X[r, i] * W[j, i] for OUT <= 2 outputs (the pools'
+// key layers, the head's output layer), which k_linear's 64-wide output tile
+// would compute 32 to 64 times over: one thread per row, the CTA's rows
+// staged through shared memory NK columns at a time. The sum runs over the
+// same zero-padded k range as k_linear (in rounded up to BK) in the same
+// order, with the products and sums rounded separately: the same bits.
+constexpr int NK = 32;
+
+template <int OUT>
+__global__ void __launch_bounds__(LT)
+    k_linear_narrow(const float* __restrict__ X, int ldx, int rows, int in,
+                    const float* __restrict__ W, const float* __restrict__ b,
+                    float* __restrict__ Y, int ldy) {
+    __shared__ float xs[LT][NK + 1];
+    __shared__ float ws[OUT][NK];
+    const int64_t r0 = (int64_t)blockIdx.x * LT;
+    const int inp = (in + BK - 1) / BK * BK;
+    float acc[OUT];
+#pragma unroll
+    for (int j = 0; j < OUT; j++) acc[j] = 0.0f;
+    for (int k0 = 0; k0 < inp; k0 += NK) {
+        for (int e = threadIdx.x; e < LT * NK; e += LT) {  // a warp reads 32 columns of a row
+            const int rr = e / NK, kk = e % NK;
+            const int64_t r = r0 + rr;
+            const int k = k0 + kk;
+            xs[rr][kk] = (r < rows && k < in) ? X[r * ldx + k] : 0.0f;
+        }
+        if (threadIdx.x < OUT * NK) {
+            const int j = threadIdx.x / NK, k = k0 + threadIdx.x % NK;
+            ws[j][threadIdx.x % NK] = k < in ? W[(int64_t)j * in + k] : 0.0f;
+        }
+        __syncthreads();
+        const int kn = inp - k0 < NK ? inp - k0 : NK;
+        for (int kk = 0; kk < kn; kk++) {
+            const float xv = xs[threadIdx.x][kk];
+#pragma unroll
+            for (int j = 0; j < OUT; j++) acc[j] = __fadd_rn(acc[j], __fmul_rn(xv, ws[j][kk]));
+        }
+        __syncthreads();
+    }
+    const int64_t r = r0 + threadIdx.x;
+    if (r < rows) {
+#pragma unroll
+        for (int j = 0; j < OUT; j++) Y[r * ldy + j] = __fadd_rn(acc[j], b[j]);
+    }
+}
+
 // Two-sided message rows [e_neg | state_neg | e_pos | state_pos | logd_neg | logd_pos]
 // (BiDirEmbed input order), one warp per (pair, axis) row.
 __global__ void __launch_bounds__(LT)
@@ -369,6 +416,13 @@ int linear(const float* X, int ldx, int64_t rows, int in, const float* W, const 
            float* Y, int ldy, int act, cudaStream_t st) {
     if (rows <= 0) return LATEC_OK;
     if (rows > 0x7fffffffLL) return LATEC_ERR_UNSUPPORTED;
+    if (!act && out <= 2) {
+        const unsigned g = (unsigned)((rows + LT - 1) / LT);
+        if (out == 1) k_linear_narrow<1><<<g, LT, 0, st>>>(X, ldx, (int)rows, in, W, b, Y, ldy);
+        else k_linear_narrow<2><<<g, LT, 0, st>>>(X, ldx, (int)rows, in, W, b, Y, ldy);
+        count_launches(1);
+        return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
+    }
     const dim3 grid((unsigned)((rows + BM - 1) / BM), (unsigned)((out + BN - 1) / BN));
     if (act) k_linear<1><<<grid, LT, 0, st>>>(X, ldx, (int)rows, in, W, b, out, Y, ldy);
     else k_linear<0><<<grid, LT, 0, st>>>(X, ldx, (int)rows, in, W, b, out, Y, ldy);
