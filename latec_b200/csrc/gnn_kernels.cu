@@ -30,29 +30,33 @@ int mlp2_tc8(const float* X, int ldx, int64_t rows, int k1, int k1p, const void*
 namespace {
 
 constexpr int LT = 256;  // threads of every kernel here
-constexpr int BM = 64, BN = 64, BK = 16;
+constexpr int BN = 64, BK = 16;
 
 __device__ __forceinline__ float gelu(float x) {
     return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f));
 }
 
 // Y[r, j] = act(b[j] + sum_i X[r, i] * W[j, i]); X row stride ldx, Y row
-// stride ldy. 64 x 64 output tile per CTA, 4 x 4 per thread, k ascending.
+// stride ldy. 128 x 64 output tile per CTA, 8 x 4 per thread (operands read
+// as 128-bit shared-memory vectors), k ascending over the zero-padded range
+// [0, in rounded up to BK), each product and sum rounded on its own.
+constexpr int BMR = 128;  // rows of a k_linear tile
+
 template <int ACT>
 __global__ void __launch_bounds__(LT)
     k_linear(const float* __restrict__ X, int ldx, int rows, int in, const float* __restrict__ W,
              const float* __restrict__ b, int out, float* __restrict__ Y, int ldy) {
-    __shared__ float xs[BK][BM + 4];
-    __shared__ float ws[BK][BN + 4];
-    const int r0 = blockIdx.x * BM, j0 = blockIdx.y * BN;
+    __shared__ __align__(16) float xs[BK][BMR + 4];
+    __shared__ __align__(16) float ws[BK][BN + 4];
+    const int r0 = blockIdx.x * BMR, j0 = blockIdx.y * BN;
     const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;
-    float acc[4][4];
+    float acc[8][4];
 #pragma unroll
-    for (int a = 0; a < 4; a++)
+    for (int a = 0; a < 8; a++)
 #pragma unroll
         for (int c = 0; c < 4; c++) acc[a][c] = 0.0f;
     for (int k0 = 0; k0 < in; k0 += BK) {
-        for (int e = threadIdx.x; e < BM * BK; e += LT) {
+        for (int e = threadIdx.x; e < BMR * BK; e += LT) {
             const int rr = e / BK, kk = e % BK;
             const int r = r0 + rr, k = k0 + kk;
             xs[kk][rr] = (r < rows && k < in) ? X[(int64_t)r * ldx + k] : 0.0f;
@@ -65,21 +69,21 @@ __global__ void __launch_bounds__(LT)
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < BK; kk++) {
-            float xv[4], wv[4];
+            const float4 xa = *reinterpret_cast<const float4*>(&xs[kk][tr * 8]);
+            const float4 xb = *reinterpret_cast<const float4*>(&xs[kk][tr * 8 + 4]);
+            const float4 w4 = *reinterpret_cast<const float4*>(&ws[kk][tc * 4]);
+            const float xv[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+            const float wv[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
-            for (int a = 0; a < 4; a++) xv[a] = xs[kk][tr * 4 + a];
-#pragma unroll
-            for (int c = 0; c < 4; c++) wv[c] = ws[kk][tc * 4 + c];
-#pragma unroll
-            for (int a = 0; a < 4; a++)
+            for (int a = 0; a < 8; a++)
 #pragma unroll
                 for (int c = 0; c < 4; c++) acc[a][c] = __fadd_rn(acc[a][c], __fmul_rn(xv[a], wv[c]));
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int a = 0; a < 4; a++) {
-        const int r = r0 + tr * 4 + a;
+    for (int a = 0; a < 8; a++) {
+        const int r = r0 + tr * 8 + a;
         if (r >= rows) continue;
 #pragma unroll
         for (int c = 0; c < 4; c++) {
@@ -423,7 +427,7 @@ int linear(const float* X, int ldx, int64_t rows, int in, const float* W, const 
         count_launches(1);
         return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
     }
-    const dim3 grid((unsigned)((rows + BM - 1) / BM), (unsigned)((out + BN - 1) / BN));
+    const dim3 grid((unsigned)((rows + BMR - 1) / BMR), (unsigned)((out + BN - 1) / BN));
     if (act) k_linear<1><<<grid, LT, 0, st>>>(X, ldx, (int)rows, in, W, b, out, Y, ldy);
     else k_linear<0><<<grid, LT, 0, st>>>(X, ldx, (int)rows, in, W, b, out, Y, ldy);
     count_launches(1);
