@@ -22,7 +22,7 @@ namespace latec {
 
 int mlp2_tc(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* w1p,
             const float* b1, const void* w2p, const float* b2, int n1, int n2, float* Y, int ldy,
-            uint32_t* err, int n_sm, cudaStream_t st);
+            int ny, uint32_t* err, int n_sm, cudaStream_t st);
 int mlp2_tc8(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* w1p,
              const float* s1, const float* b1, const void* w2p, const float* s2, const float* b2,
              int n1, int n2, float* Y, int ldy, uint32_t* err, int n_sm, cudaStream_t st);
@@ -358,9 +358,14 @@ struct TcMlp {
 };
 struct Packed {
     TcMlp bi, dir, mix;
+    // the line pool's key MLP (64 -> 64 -> 1) in BF16, its output layer and
+    // bias zero-padded to 32 rows; null when the model carries none
+    TcMlp key;
+    const float* key_b2 = nullptr;
 };
 
 inline int pad16(int k) { return (k + 15) / 16 * 16; }
+constexpr int KEY_ROWS = 32;  // rows of the padded key output layer
 inline int pad32(int k) { return (k + 31) / 32 * 32; }
 
 Packed packed_of(const latec_gnn_model* m, const Params& P) {
@@ -393,6 +398,13 @@ Packed packed_of(const latec_gnn_model* m, const Params& P) {
             t.w2 = p;
             p += (size_t)P.d * P.h;
         }
+        // then the line pool's key MLP: W1 d x d, W2 32 x d, b2 as 32 floats
+        k.key.k1p = P.d;
+        k.key.w1 = p;
+        p += (size_t)P.d * P.d;
+        k.key.w2 = p;
+        p += (size_t)KEY_ROWS * P.d;
+        k.key_b2 = (const float*)p;
     }
     return k;
 }
@@ -441,7 +453,7 @@ int mlp2(const latec_gnn_model* m, const float* X, int ldx, int64_t rows, int k1
         return mlp2_tc8(X, ldx, rows, k1, tc.k1p, tc.w1, tc.s1, b1, tc.w2, tc.s2, b2, h, d, Y, ldy,
                         m->tc_err, n_sms(), st);
     if (tc.w1)
-        return mlp2_tc(X, ldx, rows, k1, tc.k1p, tc.w1, b1, tc.w2, b2, h, d, Y, ldy, m->tc_err,
+        return mlp2_tc(X, ldx, rows, k1, tc.k1p, tc.w1, b1, tc.w2, b2, h, d, Y, ldy, d, m->tc_err,
                        n_sms(), st);
     int rc = linear(X, ldx, rows, k1, w1, b1, h, H, h, 1, st);
     if (!rc) rc = linear(H, h, rows, h, w2, b2, d, Y, ldy, 0, st);
@@ -547,9 +559,15 @@ int latec_gnn_embed(const latec_gnn_model* model, int32_t B, int64_t N, const fl
                               P.dir2b, pk.dir, P.h, d, H, msb + n2 * K * d, d, st);
             }
         }
-        // line pool keys and values of every live row
-        if (!rc) rc = linear(MS, d, rows, d, P.lp_k0w, P.lp_k0b, d, S1, d, 1, st);
-        if (!rc) rc = linear(S1, d, rows, d, P.lp_k2w, P.lp_k2b, 1, KEY, 1, 0, st);
+        // line pool keys and values of every live row; the key MLP on the
+        // tensor cores when the model carries it in BF16
+        if (!rc && pk.key.w1) {
+            rc = mlp2_tc(MS, d, rows, d, pk.key.k1p, pk.key.w1, P.lp_k0b, pk.key.w2, pk.key_b2, d,
+                         KEY_ROWS, KEY, 1, 1, model->tc_err, n_sms(), st);
+        } else {
+            if (!rc) rc = linear(MS, d, rows, d, P.lp_k0w, P.lp_k0b, d, S1, d, 1, st);
+            if (!rc) rc = linear(S1, d, rows, d, P.lp_k2w, P.lp_k2b, 1, KEY, 1, 0, st);
+        }
         if (!rc) rc = linear(MS, d, rows, d, P.lp_vw, P.lp_vb, d, V, d, 0, st);
         for (int b = 0; b < B && !rc; b++) {
             k_line_rows<<<blocks_for((int64_t)mt * K), LT, 0, st>>>(g.row_of, g.M, L, K, b, m0, mt,

@@ -12,7 +12,11 @@
 //      applies GELU and writes the BF16 hidden row to shared memory: the A
 //      operand of layer 2;
 //   4. N1 / 16 tcgen05.mma into TMEM columns [N1, N1 + N2), commit, wait;
-//   5. the epilogue adds b2 and stores the float32 row of Y.
+//   5. the epilogue adds b2 and stores the first ny columns of the float32
+//      row of Y.
+// Instances: N1 x N2 = 128 x 64 (the message and mix MLPs) and 64 x 32 (the
+// line pool's key MLP, 64 -> 64 -> 1 with the output layer zero-padded to 32
+// rows; ny = 1 stores the key alone).
 // Operands use the no-swizzle K-major canonical layout: 8 x 16-byte core
 // matrices, row groups 128 bytes apart (SBO) and 8-element K chunks R * 16
 // bytes apart (LBO), R the operand's rows. Weights arrive pre-packed in that
@@ -110,7 +114,7 @@ __device__ __forceinline__ void st_bf16x8(__nv_bfloat16* dst, const float* v) {
     *(int4*)dst = *(const int4*)p;
 }
 
-// N1 = hidden width (128), N2 = output width (64). 256 threads: thread t
+// N1 = hidden width, N2 = output width (multiples of 32). 256 threads: thread t
 // converts K chunks of row t % 128 (rows of a warp are 16 bytes apart in the
 // canonical layout: conflict-free stores); warp w reads TMEM lanes
 // 32 (w % 4) .. + 31, warpgroup w / 4 half of the columns.
@@ -119,7 +123,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     k_mlp2_tc(const float* __restrict__ X, int ldx, int rows, int k1, int k1p,
               const __nv_bfloat16* __restrict__ w1p, const float* __restrict__ b1,
               const __nv_bfloat16* __restrict__ w2p, const float* __restrict__ b2,
-              float* __restrict__ Y, int ldy, uint32_t* __restrict__ err) {
+              float* __restrict__ Y, int ldy, int ny, uint32_t* __restrict__ err) {
+    static_assert(N1 % 32 == 0 && N2 % 32 == 0 && N1 + N2 <= 512, "MLP widths");
     extern __shared__ __align__(128) uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_base;
@@ -264,8 +269,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
         asm volatile("tcgen05.fence::before_thread_sync;");
         __syncthreads();
-        for (int e = tid; e < TC_M * N2; e += TC_THREADS) {
-            const int r = e / N2, c = e % N2;
+        for (int e = tid; e < TC_M * ny; e += TC_THREADS) {
+            const int r = e / ny, c = e % ny;
             if (r0 + r < rows) Y[(int64_t)(r0 + r) * ldy + c] = sy[r * (N2 + 1) + c];
         }
         __syncthreads();
@@ -541,20 +546,24 @@ uint64_t mlp2_tc_smem(int k1p, int n1, int n2) {
 
 int mlp2_tc(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* w1p,
             const float* b1, const void* w2p, const float* b2, int n1, int n2, float* Y, int ldy,
-            uint32_t* err, int n_sm, cudaStream_t st) {
+            int ny, uint32_t* err, int n_sm, cudaStream_t st) {
     if (rows <= 0) return LATEC_OK;
-    if (n1 != 128 || n2 != 64 || k1p % 16 || k1p < k1 || rows > 0x7fffffffLL)
+    const bool big = n1 == 128 && n2 == 64, key = n1 == 64 && n2 == 32;
+    if ((!big && !key) || ny < 1 || ny > n2 || ldy < ny || k1p % 16 || k1p < k1 ||
+        rows > 0x7fffffffLL)
         return LATEC_ERR_UNSUPPORTED;
+    // the float32 output tile (128 x (n2 + 1)) is staged over the A and hidden buffers
     const uint64_t smem = mlp2_tc_smem(k1p, n1, n2);
-    if (smem > 220 * 1024) return LATEC_ERR_UNSUPPORTED;
-    auto kern = k_mlp2_tc<128, 64>;
+    if (smem > 220 * 1024 || 4ull * TC_M * (n2 + 1) > 2ull * TC_M * (k1p + n1))
+        return LATEC_ERR_UNSUPPORTED;
+    auto kern = big ? k_mlp2_tc<128, 64> : k_mlp2_tc<64, 32>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return LATEC_ERR_CUDA;
     const int64_t tiles = (rows + TC_M - 1) / TC_M;
     const int grid = (int)(tiles < n_sm ? tiles : n_sm);
     kern<<<grid, TC_THREADS, smem, st>>>(X, ldx, (int)rows, k1, k1p, (const __nv_bfloat16*)w1p, b1,
-                                         (const __nv_bfloat16*)w2p, b2, Y, ldy, err);
+                                         (const __nv_bfloat16*)w2p, b2, Y, ldy, ny, err);
     count_launches(1);
     return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
 }
@@ -617,7 +626,7 @@ int latec_gnn_mlp2_bf16(const float* X, int32_t ldx, int64_t rows, int32_t k1, i
     int dev = 0, n_sm = 148;
     if (cudaGetDevice(&dev) == cudaSuccess)
         cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    return mlp2_tc(X, ldx, rows, k1, k1p, w1p, b1, w2p, b2, 128, 64, Y, ldy, err, n_sm,
+    return mlp2_tc(X, ldx, rows, k1, k1p, w1p, b1, w2p, b2, 128, 64, Y, ldy, 64, err, n_sm,
                    (cudaStream_t)stream);
 }
 

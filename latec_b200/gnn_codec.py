@@ -72,7 +72,7 @@ MAGIC = b"LATECGNN"
 VERSION = 14
 PREFIX = "<8sII"
 PREFIX_SIZE = struct.calcsize(PREFIX)
-FLOAT_PATHS = {"f32": "latec_b200-f32-1", "bf16": "latec_b200-bf16-1",
+FLOAT_PATHS = {"f32": "latec_b200-f32-1", "bf16": "latec_b200-bf16-2",
                "fp8": "latec_b200-fp8-1"}
 AUTO_CHUNK_THRESHOLD = 1 << 21
 RANK_LEVELS = {2: 8, 4: 5, 5: 4}
