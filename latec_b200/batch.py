@@ -43,6 +43,22 @@ _ALIGN = 256  # bytes: every tensor's slice of a shared buffer starts on this bo
 _FIT_ROWS = 32768  # stages per model-fit launch
 
 
+class _View:
+    """A tensor's slice of a shared buffer, as the kernels see it: an address
+    and a length (the buffer itself is kept alive by the caller)."""
+
+    __slots__ = ("ptr", "n")
+
+    def __init__(self, ptr, n):
+        self.ptr, self.n = ptr, n
+
+    def data_ptr(self):
+        return self.ptr
+
+    def numel(self):
+        return self.n
+
+
 def _arenas(sizes, device):
     """Shared buffers for per-tensor size dicts (kind -> (elements, dtype)):
     returns (per-tensor views, kind -> (buffer, per-tensor element offsets)).
@@ -58,13 +74,13 @@ def _arenas(sizes, device):
         esz = torch.empty(0, dtype=dt).element_size()
         unit = {"stats": 1, "hist_total": 1,
                 "hist_seg": 2 * rans_model.HWIN}.get(kind, _ALIGN // esz)
-        offs, at = [], 0
-        for sz in sizes:
-            offs.append(at)
-            at += -(-sz[kind][0] // unit) * unit
-        buf = torch.empty(max(at, 1), dtype=dt, device=device)
-        for j, sz in enumerate(sizes):
-            views[j][kind] = buf[offs[j]:offs[j] + sz[kind][0]]
+        ns = [sz[kind][0] for sz in sizes]
+        padded = [-(-n // unit) * unit for n in ns]
+        offs = np.concatenate([[0], np.cumsum(padded)[:-1]]).astype(np.int64).tolist()
+        buf = torch.empty(max(sum(padded), 1), dtype=dt, device=device)
+        base = buf.data_ptr()
+        for j, n in enumerate(ns):
+            views[j][kind] = _View(base + offs[j] * esz, n)
         bufs[kind] = (buf, offs)
     return views, bufs
 
@@ -179,10 +195,15 @@ def _compress_group(jobs, predictor, dev, lib):
     sp = _lib.stream_ptr()
     views, bufs = _arenas([buffer_sizes(jb.plan, jb.c, jb.elem) for jb in jobs], dev)
     ssz = ctypes.sizeof(_lib.StageStats)
+    # the reconstructions the stage kernels work in: one zeroed buffer
+    esz = jobs[0].field.element_size()
+    rsz = [-(-jb.field.numel() * esz // _ALIGN) * _ALIGN for jb in jobs]
+    recon = torch.zeros(max(sum(rsz), 1), dtype=torch.uint8, device=dev)
+    roff = np.concatenate([[0], np.cumsum(rsz)[:-1]]).astype(np.int64).tolist()
     # ---- stage kernels of every tensor, back to back
-    for jb, v in zip(jobs, views):
+    for jb, v, ro in zip(jobs, views, roff):
         jb.buf = b = _Buffers(jb.plan, jb.c, jb.src, dev, views=v)
-        jb.recon = torch.zeros_like(jb.field)
+        jb.recon = _View(recon.data_ptr() + ro, jb.field.numel())
         prm = _qparams(jb.src, jb.c, jb.radius, predictor.order, jb.center, jb.end_mode,
                        jb.src == 0)
         ns = len(jb.plan)

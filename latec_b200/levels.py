@@ -9,6 +9,7 @@ points from its rank.
 from __future__ import annotations
 
 import ctypes
+from collections import OrderedDict
 
 import numpy as np
 
@@ -101,16 +102,21 @@ class Plan:
             self._h = None
 
 
-_plans: dict = {}
+_plans: "OrderedDict" = OrderedDict()
+_PLAN_CACHE = 1024  # schedules kept (host memory only, a few KB each)
 
 
 def plan_for(shape, levels, anchor_stride, anchor_block=1) -> Plan:
+    """The schedule of a shape, from a least-recently-used cache: a batch of
+    many tensors of different shapes reuses its plans from call to call."""
     key = (tuple(int(n) for n in shape), int(levels), int(anchor_stride), int(anchor_block))
     p = _plans.get(key)
     if p is None:
-        if len(_plans) > 64:
-            _plans.clear()
         p = _plans[key] = Plan(*key)
+        if len(_plans) > _PLAN_CACHE:
+            _plans.popitem(last=False)
+    else:
+        _plans.move_to_end(key)
     return p
 
 
