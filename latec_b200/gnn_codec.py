@@ -65,7 +65,7 @@ from pathlib import Path
 
 import numpy as np
 
-from . import _lib, bitstream, gnn, rans
+from . import _lib, bitstream, gnn, rans, rans_model
 from .levels import stage_ebs, stage_strides
 
 MAGIC = b"LATECGNN"
@@ -533,7 +533,16 @@ class GNNCodec:
         recon_all = torch.zeros((B, N), dtype=torch.float32, device=dev)
         strides = stage_strides(len(shape), levels, 1 << levels)
         finest = [strides[t] == 1 for t in pstages]
-        records, words, fine_words, fine_desc = [], [], [], None
+        # every stage's codes, level rows, outliers and statistics stay on the
+        # device until the entropy step after the stage loop
+        offs = np.concatenate([[0], np.cumsum([B * g.M for g in geoms])]).astype(np.int64)
+        total = max(int(offs[-1]), 1)
+        codes_all = torch.empty(total, dtype=torch.int16, device=dev)
+        lv_all = torch.empty(total, dtype=torch.uint8, device=dev)
+        outl_all = torch.empty(total, dtype=torch.float32, device=dev)
+        ssz = ctypes_sizeof_stats()
+        stats_all = torch.zeros(max(len(geoms), 1) * ssz, dtype=torch.uint8, device=dev)
+        words, fine_words, fine_desc = [], [], None
         prev, ctx, vals = None, None, None
         for gi, (g, seb) in enumerate(zip(geoms, ebs)):
             n = B * g.M
@@ -579,34 +588,85 @@ class GNNCodec:
                 word = gate_word(kind, direction, T, shift)
             if not shared:
                 words.append(word)
-            codes = torch.empty(n, dtype=torch.int16, device=dev)
+            o = int(offs[gi])
             recon = torch.empty(n, dtype=torch.float32, device=dev)
-            outl = torch.empty(n, dtype=torch.float32, device=dev)
-            stats = torch.zeros(ctypes_sizeof_stats(), dtype=torch.uint8, device=dev)
             hseg = torch.empty(max(1, -(-n // (1 << 22))) * 512, dtype=torch.int32, device=dev)
             htot = torch.empty(65536, dtype=torch.int32, device=dev)
             ws = torch.empty(int(lib.latec_flat_workspace_bytes(n, _lib.F32)), dtype=torch.uint8,
                              device=dev)
             _lib.check(lib.latec_quantize(_byref(prm), seb, n, xs.data_ptr(), mu.data_ptr(),
-                                          codes.data_ptr(), recon.data_ptr(), outl.data_ptr(),
-                                          stats.data_ptr(), hseg.data_ptr(), htot.data_ptr(),
-                                          ws.data_ptr(), ws.numel(), _lib.stream_ptr()),
-                       "latec_quantize")
-            st = _lib.StageStats.from_buffer_copy(stats.cpu().numpy().tobytes())
-            kexp = max(1, int(st.maxq).bit_length())
-            lv64 = rans.scale_to_level(scale, seb)
-            tables = rans.build_laplace_tables(seb, radius)
-            codes_u = codes.view(torch.int16)
-            shape_id = rans.choose_shape(_u16_as_i64(codes_u), lv64, tables, kexp) if n else 0
-            blob = rans.rans_encode(_u16_as_i64(codes_u), lv64, tables, kexp=kexp,
-                                    shape=shape_id, mode="native")
-            n_out = int(st.n_out)
-            frame = bitstream.pack_frame(len(blob), kexp, shape_id, 0, 0, False)
-            records.append(struct.pack("<IQ", n, frame) + blob + struct.pack("<I", n_out)
-                           + outl[:n_out].cpu().numpy().astype("<f4").tobytes())
+                                          codes_all.data_ptr() + 2 * o, recon.data_ptr(),
+                                          outl_all.data_ptr() + 4 * o,
+                                          stats_all.data_ptr() + gi * ssz, hseg.data_ptr(),
+                                          htot.data_ptr(), ws.data_ptr(), ws.numel(),
+                                          _lib.stream_ptr()), "latec_quantize")
+            lv_all[o:o + n].copy_(rans.scale_to_level(scale, seb))
             recon_all[:, g.query_idx] = recon.reshape(B, -1)
             prev, vals = g, recon.reshape(B, -1)
-        return b"".join(records), words, fine_words
+        payload = self._entropy(ebs, offs, codes_all, lv_all, outl_all, stats_all, radius)
+        return payload, words, fine_words
+
+    def _entropy(self, ebs, offs, codes_all, lv_all, outl_all, stats_all, radius):
+        """The stage records of one batch (``u32 n | u64 frame | blob | u32
+        n_out | outliers``, the per-point native rANS of ``latec_b200.rans``
+        for every stage): per stage the coder window from the largest code and
+        the table shape of least cost, then every stage through the lane coder
+        and the record assembly in one launch."""
+        torch = _torch()
+        lib = _lib.load()
+        dev = self.device
+        ns = len(ebs)
+        if ns == 0:
+            return b""
+        ssz = ctypes_sizeof_stats()
+        raw = stats_all.cpu().numpy().tobytes()  # one download: every stage's statistics
+        st = (_lib.StageStats * ns).from_buffer_copy(raw[:ns * ssz])
+        kexps = [max(1, int(st[t].maxq).bit_length()) for t in range(ns)]
+        tabs = [rans.build_laplace_tables(seb, radius) for seb in ebs]
+        costs = [rans.shape_costs(codes_all.data_ptr() + 2 * int(offs[t]),
+                                  lv_all.data_ptr() + int(offs[t]), int(offs[t + 1] - offs[t]),
+                                  tabs[t], kexps[t], dev) for t in range(ns)]
+        got = torch.cat([c[1] for c in costs]).cpu().numpy()  # one download: shape costs
+        shapes, at = [], 0
+        for ids, part in costs:
+            shapes.append(rans.pick_shape(ids, got[at:at + part.numel()]))
+            at += part.numel()
+        stages = (_lib.RansStage * ns)()
+        keep = []
+        for t in range(ns):
+            n = int(offs[t + 1] - offs[t])
+            cdf, enc, bucket, alphabet = rans_model.device_tables.get(
+                _lib.RANS_LANES, kexps[t], shapes[t], 0, None, dev)
+            keep.append((cdf, enc, bucket))
+            d = stages[t]
+            d.codes_off = d.out_off = int(offs[t])
+            d.n = n
+            d.kexp, d.radius, d.mode, d.per_point = kexps[t], int(radius), _lib.RANS_LANES, 1
+            d.alphabet = alphabet
+            d.framed_hi = bitstream.pack_frame(0, kexps[t], shapes[t], 0, 0, False)
+            d.cdf, d.enc, d.bucket = cdf.data_ptr(), enc.data_ptr(), bucket.data_ptr()
+            d.K = rans_model.lanes_K(n, 4.0 * n)
+        wsb = lib.latec_rans_encode_workspace_bytes(stages, ns)
+        ws = torch.empty(max(int(wsb), 1), dtype=torch.uint8, device=dev)
+        cap = sum(16 + 4 * (1 + 65 * int(stages[t].n_chunks) + int(stages[t].n) + 2)
+                  + 4 * int(stages[t].n) for t in range(ns))
+        cap = (cap + 15) // 16 * 16
+        payload = torch.empty(cap, dtype=torch.uint8, device=dev)
+        plen = torch.zeros(1, dtype=torch.int64, device=dev)
+        err = torch.zeros(1, dtype=torch.int32, device=dev)
+        _lib.check(lib.latec_rans_encode(stages, ns, codes_all.data_ptr(), lv_all.data_ptr(),
+                                         stats_all.data_ptr(), outl_all.data_ptr(), 4,
+                                         payload.data_ptr(), cap, plen.data_ptr(), err.data_ptr(),
+                                         ws.data_ptr(), ws.numel(), _lib.stream_ptr()),
+                   "latec_rans_encode")
+        tail = torch.cat([plen.view(torch.uint8), err.view(torch.uint8)]).cpu().numpy()
+        if int(tail[8:12].view(np.int32)[0]):
+            raise RuntimeError(f"entropy coder reported error bits "
+                               f"{int(tail[8:12].view(np.int32)[0]):#x}")
+        n_bytes = int(tail[:8].view(np.int64)[0])
+        out = payload[:n_bytes].cpu().numpy().tobytes()
+        del keep
+        return out
 
     # ---------------------------------------------------------------- decode
     def uncompress(self, stream):
@@ -772,6 +832,3 @@ def _byref(prm):
     return ctypes.byref(prm)
 
 
-def _u16_as_i64(codes_i16):
-    """int16 storage of u16 codes -> int64 code values."""
-    return codes_i16.to(_torch().int64) & 0xFFFF

@@ -334,12 +334,21 @@ def choose_shape(codes, levels64, tables: RansTables, kexp: int, *,
     """Dictionary entry minimising the stage's coded length, scored on a
     strided sample against the continuous per-level weights
     (``latec/rans.py:204-243``); costs are float64 sums on the device."""
-    torch = _torch()
-    lib = _lib.load()
     dev = _device(device)
     c, lv, n = _prep_codes_levels(codes, levels64, tables, dev, kexp)
     if n == 0:
         return 0
+    ids, part = shape_costs(c.data_ptr(), lv.data_ptr(), n, tables, kexp, dev, sample)
+    return pick_shape(ids, part.cpu().numpy())
+
+
+def shape_costs(codes_ptr, levels_ptr, n, tables: RansTables, kexp: int, dev,
+                sample: float = _SELECT_SAMPLE):
+    """Launch ``choose_shape``'s cost sums for n int16 codes and uint8 level
+    rows at the given device addresses (n > 0); returns the candidate ids
+    and the device partial sums for ``pick_shape``."""
+    torch = _torch()
+    lib = _lib.load()
     n_levels = tables.cdfs.shape[0]
     step = 1
     if sample < 1.0:
@@ -350,11 +359,17 @@ def choose_shape(codes, levels64, tables: RansTables, kexp: int, *,
     ds = (ctypes.c_int32 * len(ids))(*[SHAPES[i][0] for i in ids])
     ws = (ctypes.c_double * len(ids))(*[SHAPES[i][1] for i in ids])
     part = torch.zeros(len(ids) * _PARTIALS, dtype=torch.float64, device=dev)
-    _lib.check(lib.latec_shape_costs(c.data_ptr(), lv.data_ptr(), n, step, wt.data_ptr(),
+    _lib.check(lib.latec_shape_costs(codes_ptr, levels_ptr, n, step, wt.data_ptr(),
                                      w.shape[1], n_levels, int(tables.radius), int(kexp),
                                      1.0 / tables.total, ds, ws, len(ids), part.data_ptr(),
                                      _PARTIALS, _lib.stream_ptr()), "latec_shape_costs")
-    costs = part.cpu().numpy().reshape(len(ids), _PARTIALS)
+    return ids, part
+
+
+def pick_shape(ids, partials) -> int:
+    """The candidate with the least cost (fsum of its partial sums; the first
+    one on ties)."""
+    costs = np.asarray(partials).reshape(len(ids), _PARTIALS)
     best_id, best = 0, math.inf
     for k, sid in enumerate(ids):
         cost = math.fsum(costs[k].tolist())
