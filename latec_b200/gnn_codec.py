@@ -697,7 +697,10 @@ class GNNCodec:
         fine = unpack_gates(meta.get("fine_gates", "")) if meta.get("gate_fine") else None
         if fine is not None and words is None:
             raise ValueError("finest-level gate words without per-stage gate words")
-        err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        # error words: [0] the dequantizer, [1] the lane decoder; read once at the end
+        err = torch.zeros(2, dtype=torch.int32, device=self.device)
+        pay_dev = torch.from_numpy(np.frombuffer(payload + bytes(8), np.uint8).copy()).to(
+            self.device)  # the whole payload once; stage blobs and outliers are read in place
         if "chunk_batch" in meta:  # chunks of one shape, decoded in the encoder's batches
             edges = tuple(int(e) for e in meta["chunks"])
             cbatch = int(meta["chunk_batch"])
@@ -708,33 +711,42 @@ class GNNCodec:
             for cshape, origins in chunk_groups(shape, edges):
                 for b0 in range(0, len(origins), cbatch):
                     sub = origins[b0:b0 + cbatch]
-                    R, off, wi, fi = self._decode(model, payload, off, len(sub), cshape, levels,
-                                                  eb, ratio, radius, words, wi, fine, fi, err,
-                                                  interp_kind)
+                    R, off, wi, fi = self._decode(model, payload, pay_dev, off, len(sub),
+                                                  cshape, levels, eb, ratio, radius, words, wi,
+                                                  fine, fi, err, interp_kind)
                     for j, o in enumerate(sub):
                         out[_chunk_slices(o, cshape)] = R[j].reshape(cshape)
             recon_all = out.reshape(-1)
         else:
-            R, off, wi, fi = self._decode(model, payload, 0, 1, shape, levels, eb, ratio,
-                                          radius, words, 0, fine, 0, err, interp_kind)
+            R, off, wi, fi = self._decode(model, payload, pay_dev, 0, 1, shape, levels, eb,
+                                          ratio, radius, words, 0, fine, 0, err, interp_kind)
             recon_all = R.reshape(-1)
         if off != len(payload):
             raise ValueError("trailing data in GNN stage payload")
         if (words is not None and wi != len(words)) or (fine is not None and fi != len(fine)):
             raise ValueError("gate words do not match the stage schedule")
-        if int(err.item()):
+        e_dq, e_rans = (int(v) for v in err.cpu().tolist())
+        if e_rans & (4 | 8):
+            raise ValueError("trailing data in rANS payload")
+        if e_rans:
+            raise ValueError(f"malformed rANS payload (error bits {e_rans:#x})")
+        if e_dq:
             raise ValueError("outlier count mismatch")
         if int(model.tc_err.item()):
             raise RuntimeError("a tensor-core wait ran out during the GNN forward")
         out = recon_all * np.float32(vmax - vmin) + np.float32(vmin)
         return _restore_dtype(out.reshape(original_shape).cpu(), dtype)
 
-    def _decode(self, model, payload, off, B, shape, levels, eb, ratio, radius, words, wi,
-                fine, fi, err, interp_kind=0):
-        """Decode B regions of one shape from ``payload`` at ``off``, reading
-        per-stage gate words from ``words[wi:]`` and, when the stream shares
-        one word over the finest level, that word from ``fine[fi]``; returns
-        (recon (B, N), the offset after them, the next wi, the next fi)."""
+    def _decode(self, model, payload, pay_dev, off, B, shape, levels, eb, ratio, radius, words,
+                wi, fine, fi, err, interp_kind=0):
+        """Decode B regions of one shape from ``payload`` (host bytes; its
+        device copy ``pay_dev``) at ``off``, reading per-stage gate words from
+        ``words[wi:]`` and, when the stream shares one word over the finest
+        level, that word from ``fine[fi]``; returns (recon (B, N), the offset
+        after them, the next wi, the next fi). The stage records are parsed on
+        the host first; each stage's codes are then rANS-decoded on the device
+        from the payload copy and dequantized there, and the error words
+        ``err`` are read by the caller."""
         torch = _torch()
         lib = _lib.load()
         geoms = self._geometry(shape, levels)
@@ -753,6 +765,42 @@ class GNNCodec:
             raise ValueError("gate words do not match the stage schedule")
         if any(shared) and fi >= len(fine):
             raise ValueError("gate words do not match the stage schedule")
+        recs = []  # per stage: (n, frame fields, blob byte offset, outliers byte offset, n_out)
+        chunk_ranges = []
+        for g in geoms:
+            if off + 12 > len(payload):
+                raise ValueError("truncated GNN stage payload")
+            n, frame = struct.unpack_from("<IQ", payload, off)
+            f = bitstream.unpack_frame(frame)
+            if n != B * g.M:
+                raise ValueError("stage size differs from the schedule")
+            if f["hlen"] % 4:
+                raise ValueError("rANS payload is not aligned to 32-bit words")
+            bo = off + 12
+            off = bo + f["hlen"]
+            if off + 4 > len(payload):
+                raise ValueError("truncated GNN stage payload")
+            (n_out,) = struct.unpack_from("<I", payload, off)
+            off += 4
+            if n_out > n or off + 4 * n_out > len(payload):
+                raise ValueError("truncated GNN stage payload")
+            # the lane coder's chunk table: K, then each chunk's word count
+            wd = np.frombuffer(payload, "<u4", count=f["hlen"] // 4, offset=bo)
+            if len(wd) < 1 or int(wd[0]) < 1:
+                raise ValueError("malformed rANS payload")
+            K = int(wd[0])
+            nc = -(-n // (32 * K))
+            if len(wd) < 1 + nc:
+                raise ValueError("malformed rANS payload")
+            ends = 1 + nc + np.cumsum(wd[1:1 + nc].astype(np.int64))
+            if int(ends[-1]) != len(wd):
+                raise ValueError("trailing data in rANS payload")
+            starts = ends - wd[1:1 + nc].astype(np.int64)
+            chunk_ranges.append(np.stack([starts, ends], 1).reshape(-1) + bo // 4)
+            recs.append((n, f, bo, off, n_out, K, nc))
+            off += 4 * n_out
+        ranges = torch.from_numpy(np.concatenate(chunk_ranges)).to(dev)  # one upload
+        ch0 = np.concatenate([[0], np.cumsum([r[6] for r in recs])]).astype(np.int64)
         fine_desc = None
         for gi, (g, seb) in enumerate(zip(geoms, ebs)):
             if interp_kind:
@@ -763,23 +811,7 @@ class GNNCodec:
                                                      eb=seb)
                 mu = mu.reshape(-1).contiguous()
                 scale = torch.exp2(lb.reshape(-1)).contiguous()
-            if off + 12 > len(payload):
-                raise ValueError("truncated GNN stage payload")
-            n, frame = struct.unpack_from("<IQ", payload, off)
-            f = bitstream.unpack_frame(frame)
-            if n != B * g.M:
-                raise ValueError("stage size differs from the schedule")
-            blob = payload[off + 12:off + 12 + f["hlen"]]
-            off += 12 + f["hlen"]
-            if off + 4 > len(payload):
-                raise ValueError("truncated GNN stage payload")
-            (n_out,) = struct.unpack_from("<I", payload, off)
-            off += 4
-            if off + 4 * n_out > len(payload):
-                raise ValueError("truncated GNN stage payload")
-            outl = np.frombuffer(payload, "<f4", count=n_out, offset=off) if n_out else \
-                np.zeros(1, np.float32)
-            off += 4 * n_out
+            n, f, bo, oo, n_out, K, nc = recs[gi]
             if shared[gi]:
                 if fine_desc is None:
                     fine_desc = gate_fields(int(fine[fi]))
@@ -797,19 +829,35 @@ class GNNCodec:
                 _lib.check(lib.latec_gate_apply(n, mu.data_ptr(), scale.data_ptr(), ip.data_ptr(),
                                                 seb, T, shift, direction, _lib.stream_ptr()),
                            "latec_gate_apply")
+            # the stage's codes: per-point native rANS (latec_b200.rans.rans_decode),
+            # decoded on the device from the payload copy
             lv64 = rans.scale_to_level(scale, seb)
-            tables = rans.build_laplace_tables(seb, radius)
-            codes = rans.rans_decode(blob, lv64, tables, kexp=f["kexp"], shape=f["shape"],
-                                     mode="native")
-            codes_d = torch.from_numpy(codes.astype(np.uint16).view(np.int16)).to(dev)
-            outl_d = torch.from_numpy(np.array(outl, np.float32)).to(dev)
+            cdf, enc, bucket, alphabet = rans_model.device_tables.get(
+                _lib.RANS_LANES, f["kexp"], f["shape"], 0, None, dev)
+            st = (_lib.RansStage * 1)()
+            d = st[0]
+            d.codes_off, d.n = 0, n
+            d.kexp, d.radius, d.mode, d.per_point = f["kexp"], int(radius), _lib.RANS_LANES, 1
+            d.alphabet = alphabet
+            d.cdf, d.enc, d.bucket = cdf.data_ptr(), enc.data_ptr(), bucket.data_ptr()
+            d.blob_off, d.blob_words = bo // 4, f["hlen"] // 4
+            d.K, d.n_chunks, d.chunk0 = K, nc, 0
+            codes_d = torch.empty(n, dtype=torch.int16, device=dev)
+            rws = torch.empty(int(lib.latec_rans_decode_workspace_bytes(1)), dtype=torch.uint8,
+                              device=dev)
+            _lib.check(lib.latec_rans_decode(st, 1, nc, pay_dev.data_ptr(),
+                                             ranges.data_ptr() + 16 * int(ch0[gi]),
+                                             lv64.data_ptr(), codes_d.data_ptr(),
+                                             err.data_ptr() + 4, rws.data_ptr(), rws.numel(),
+                                             _lib.stream_ptr()), "latec_rans_decode")
             recon = torch.empty(n, dtype=torch.float32, device=dev)
             ws = torch.empty(max(int(lib.latec_dequantize_workspace_bytes(n)), 1),
                              dtype=torch.uint8, device=dev)
             _lib.check(lib.latec_dequantize(_byref(prm), seb, n, mu.data_ptr(), codes_d.data_ptr(),
-                                            outl_d.data_ptr(), n_out, recon.data_ptr(),
+                                            pay_dev.data_ptr() + oo, n_out, recon.data_ptr(),
                                             err.data_ptr(), ws.data_ptr(), ws.numel(),
                                             _lib.stream_ptr()), "latec_dequantize")
+            del cdf, enc, bucket
             recon_all[:, g.query_idx] = recon.reshape(B, -1)
             prev, vals = g, recon.reshape(B, -1)
         return recon_all, off, wi, fi
