@@ -419,6 +419,19 @@ int latec_gate_costs(int64_t n, const float* x, const float* mu, const float* ip
                      const float* thr, const double* grid, uint64_t* sums, void* stream);
 int latec_gate_apply(int64_t n, float* mu, float* b, const float* ip, double eb, int32_t T,
                      int32_t shift, int32_t high, void* stream);
+/* The same choice and application without a host round trip (no counterpart
+ * in the reference): latec_gate_choose_apply reduces the sums to the gate word
+ * on the device (the split rule of _gate_select_t, latec/gnn_codec.py:920-971:
+ * the least-cost low- or high-side split over candidates, shifts and
+ * thresholds, kept only when it codes fewer bits than the GNN), writes it to
+ * *word (layout dir << 10 | kind << 8 | T << 4 | shift; 0 = the GNN
+ * everywhere) and applies it with ip0..ip2; latec_gate_apply_word applies a
+ * word already on the device. */
+int latec_gate_choose_apply(int64_t n, const uint64_t* sums, float* mu, float* b, const float* ip0,
+                            const float* ip1, const float* ip2, double eb, uint32_t* word,
+                            void* stream);
+int latec_gate_apply_word(int64_t n, float* mu, float* b, const float* ip0, const float* ip1,
+                          const float* ip2, double eb, const uint32_t* word, void* stream);
 
 /* ---- training of the learned predictor (scripts/train_gnn.py): forward
  *      ops that keep what their backward needs, the backward ops, the

@@ -124,6 +124,8 @@ SIGNATURES = {
     "latec_gnn_mlp2_fp8": (ctypes.c_int, [P, I32, I64, I32, I32, P, P, P, P, P, P, P, I32, P, P]),
     "latec_gate_costs": (ctypes.c_int, [I64, P, P, P, P, P, P, D, I32, P, P, P, P]),
     "latec_gate_apply": (ctypes.c_int, [I64, P, P, P, D, I32, I32, I32, P]),
+    "latec_gate_choose_apply": (ctypes.c_int, [I64, P, P, P, P, P, P, D, P, P]),
+    "latec_gate_apply_word": (ctypes.c_int, [I64, P, P, P, P, P, D, P, P]),
     "latec_tr_linear": (ctypes.c_int, [P, I64, I64, I32, P, P, I32, P, I64, I32, P, P]),
     "latec_tr_linear_bwd": (ctypes.c_int, [P, I64, I64, I32, P, I32, P, I64, P, I32, P, I64, I32,
                                            P, P, P]),

@@ -119,6 +119,69 @@ __global__ void __launch_bounds__(GT)
     }
 }
 
+// The gate's choice on the device (one thread, the 13 x 13 sums table): per
+// row the cumulative sums over the scale buckets; a low-side split at column
+// c costs tot - gnn[c] + cand[c], a high-side split gnn[c] + cand[last] -
+// cand[c]; the first least cost over (side, row, column) in that order wins
+// when it is below the GNN's total, else the word is 0. Integer arithmetic,
+// the same values as the host rule's exact float64 sums.
+__global__ void k_gate_choose(const unsigned long long* __restrict__ sums,
+                              uint32_t* __restrict__ word) {
+    if (threadIdx.x || blockIdx.x) return;
+    long long cum[GATE_R][GATE_NB];
+    for (int r = 0; r < GATE_R; r++) {
+        long long run = 0;
+        for (int c = 0; c < GATE_NB; c++) {
+            run += (long long)sums[r * GATE_NB + c];
+            cum[r][c] = run;
+        }
+    }
+    const long long tot = cum[0][GATE_NB - 1];
+    const int rows = GATE_NK * GATE_NS;
+    long long best = 0;
+    int fi = -1;
+    for (int side = 0; side < 2; side++)
+        for (int r = 0; r < rows; r++)
+            for (int c = 0; c < GATE_NT; c++) {
+                const long long cost = side == 0
+                                           ? tot - cum[0][c] + cum[1 + r][c]
+                                           : cum[0][c] + (cum[1 + r][GATE_NB - 1] - cum[1 + r][c]);
+                if (fi < 0 || cost < best) {
+                    best = cost;
+                    fi = (side * rows + r) * GATE_NT + c;
+                }
+            }
+    uint32_t w = 0;
+    if (fi >= 0 && best < tot) {
+        const int row = fi / GATE_NT, side_row = row % rows;
+        const uint32_t kind = (uint32_t)(side_row / GATE_NS + 1), high = row >= rows ? 1u : 0u;
+        const uint32_t T = (uint32_t)(2 + fi % GATE_NT), shift = (uint32_t)(2 * (side_row % GATE_NS));
+        w = (high << 10) | (kind << 8) | (T << 4) | shift;
+    }
+    *word = w;
+}
+
+// k_gate_apply with its parameters from a gate word in device memory.
+__global__ void __launch_bounds__(GT)
+    k_gate_apply_word(int64_t n, float* __restrict__ mu, float* __restrict__ b,
+                      const float* __restrict__ ip0, const float* __restrict__ ip1,
+                      const float* __restrict__ ip2, double eb, const uint32_t* __restrict__ word) {
+    const uint32_t w = *word;
+    const uint32_t kind = (w >> 8) & 3u, T = (w >> 4) & 15u, shift = w & 15u;
+    if (!kind || !T) return;
+    const int64_t i = (int64_t)blockIdx.x * GT + threadIdx.x;
+    if (i >= n) return;
+    const float* ip = kind == 1 ? ip0 : (kind == 2 ? ip1 : ip2);
+    const double thr = eb * (double)(1u << T);
+    const float mult = ldexpf(1.0f, -(int)shift);
+    const float bi = b[i];
+    const bool below = (double)bi < thr;
+    if ((w >> 10) & 1u ? !below : below) {
+        mu[i] = ip[i];
+        b[i] = bi * mult;
+    }
+}
+
 }  // namespace
 }  // namespace latec
 
@@ -155,6 +218,37 @@ int latec_gate_apply(int64_t n, float* mu, float* b, const float* ip, double eb,
     if (!mu || !b || !ip || !(eb > 0.0)) return LATEC_ERR_ARG;
     k_gate_apply<<<(unsigned)((n + GT - 1) / GT), GT, 0, (cudaStream_t)stream>>>(
         n, mu, b, ip, eb * (double)(1 << T), exp2f(-(float)shift), high ? 1 : 0);
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
+}
+
+// latec_gate_costs' sums -> the gate word (the host rule of gate_choose in
+// latec_b200/gnn_codec.py) written to *word, then that gate applied; ip0..2
+// the three candidates (cubic, first-axis linear, last-axis linear). Nothing
+// returns to the host: the word stays on the device.
+int latec_gate_choose_apply(int64_t n, const uint64_t* sums, float* mu, float* b, const float* ip0,
+                            const float* ip1, const float* ip2, double eb, uint32_t* word,
+                            void* stream) {
+    if (n < 0 || !sums || !word || !(eb > 0.0) ||
+        (n && (!mu || !b || !ip0 || !ip1 || !ip2)))
+        return LATEC_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    k_gate_choose<<<1, 32, 0, st>>>((const unsigned long long*)sums, word);
+    if (n)
+        k_gate_apply_word<<<(unsigned)((n + GT - 1) / GT), GT, 0, st>>>(n, mu, b, ip0, ip1, ip2,
+                                                                       eb, word);
+    count_launches(n ? 2 : 1);
+    return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
+}
+
+// The gate of a word already on the device (a finest-level word reused).
+int latec_gate_apply_word(int64_t n, float* mu, float* b, const float* ip0, const float* ip1,
+                          const float* ip2, double eb, const uint32_t* word, void* stream) {
+    if (n < 0 || !word || !(eb > 0.0) || (n && (!mu || !b || !ip0 || !ip1 || !ip2)))
+        return LATEC_ERR_ARG;
+    if (!n) return LATEC_OK;
+    k_gate_apply_word<<<(unsigned)((n + GT - 1) / GT), GT, 0, (cudaStream_t)stream>>>(
+        n, mu, b, ip0, ip1, ip2, eb, word);
     count_launches(1);
     return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
 }

@@ -542,7 +542,9 @@ class GNNCodec:
         outl_all = torch.empty(total, dtype=torch.float32, device=dev)
         ssz = ctypes_sizeof_stats()
         stats_all = torch.zeros(max(len(geoms), 1) * ssz, dtype=torch.uint8, device=dev)
-        words, fine_words, fine_desc = [], [], None
+        # gate words, chosen on the device and read once the batch is coded
+        gw = torch.zeros(max(len(geoms), 1), dtype=torch.int32, device=dev)
+        fine_gi = None
         prev, ctx, vals = None, None, None
         for gi, (g, seb) in enumerate(zip(geoms, ebs)):
             n = B * g.M
@@ -555,17 +557,18 @@ class GNNCodec:
                 mu = mu.reshape(-1).contiguous()
                 scale = torch.exp2(lb.reshape(-1)).contiguous()
             xs = X[:, g.query_idx].reshape(-1).contiguous()
-            word = 0
             shared = gate_fine and finest[gi]
             if gate and gi > 0 and n:
-                # the interpolation fallback: score, choose, apply (on the device)
-                if shared and fine_desc is not None:
-                    kind, direction, T, shift = fine_desc
-                    ip = (self._gate_candidate(plan, pstages[gi], kind, recon_all, n, radius)
-                          if kind else None)
+                # the interpolation fallback, scored, chosen (gate_choose's rule)
+                # and applied on the device: no host round trip per stage
+                ips = [self._gate_candidate(plan, pstages[gi], k, recon_all, n, radius)
+                       for k in (1, 2, 3)]
+                if shared and fine_gi is not None:
+                    _lib.check(lib.latec_gate_apply_word(
+                        n, mu.data_ptr(), scale.data_ptr(), ips[0].data_ptr(), ips[1].data_ptr(),
+                        ips[2].data_ptr(), seb, gw.data_ptr() + 4 * fine_gi, _lib.stream_ptr()),
+                        "latec_gate_apply_word")
                 else:
-                    ips = [self._gate_candidate(plan, pstages[gi], k, recon_all, n, radius)
-                           for k in (1, 2, 3)]
                     sums = torch.zeros(len(GATE_KINDS) * len(GATE_SHIFTS) * (len(GATE_T) + 1)
                                        + len(GATE_T) + 1, dtype=torch.int64, device=dev)
                     thr, grid = gate_scale_grid(seb, dev)
@@ -575,19 +578,12 @@ class GNNCodec:
                                                     radius, thr.data_ptr(), grid.data_ptr(),
                                                     sums.data_ptr(), _lib.stream_ptr()),
                                "latec_gate_costs")
-                    kind, direction, T, shift = gate_choose(sums.cpu().numpy())
-                    ip = ips[kind - 1] if kind else None
+                    _lib.check(lib.latec_gate_choose_apply(
+                        n, sums.data_ptr(), mu.data_ptr(), scale.data_ptr(), ips[0].data_ptr(),
+                        ips[1].data_ptr(), ips[2].data_ptr(), seb, gw.data_ptr() + 4 * gi,
+                        _lib.stream_ptr()), "latec_gate_choose_apply")
                     if shared:
-                        fine_desc = (kind, direction, T, shift)
-                        fine_words.append(gate_word(kind, direction, T, shift))
-                if kind:
-                    _lib.check(lib.latec_gate_apply(n, mu.data_ptr(), scale.data_ptr(),
-                                                    ip.data_ptr(), seb, T, shift, direction,
-                                                    _lib.stream_ptr()),
-                               "latec_gate_apply")
-                word = gate_word(kind, direction, T, shift)
-            if not shared:
-                words.append(word)
+                        fine_gi = gi
             o = int(offs[gi])
             recon = torch.empty(n, dtype=torch.float32, device=dev)
             hseg = torch.empty(max(1, -(-n // (1 << 22))) * 512, dtype=torch.int32, device=dev)
@@ -604,6 +600,9 @@ class GNNCodec:
             recon_all[:, g.query_idx] = recon.reshape(B, -1)
             prev, vals = g, recon.reshape(B, -1)
         payload = self._entropy(ebs, offs, codes_all, lv_all, outl_all, stats_all, radius)
+        got = gw.cpu().numpy().astype(np.int64).tolist()
+        words = [got[gi] for gi in range(len(geoms)) if not (gate_fine and finest[gi])]
+        fine_words = [got[fine_gi]] if fine_gi is not None else []
         return payload, words, fine_words
 
     def _entropy(self, ebs, offs, codes_all, lv_all, outl_all, stats_all, radius):

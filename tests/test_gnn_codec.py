@@ -170,6 +170,46 @@ def test_gate_falls_back_to_interpolation_where_it_codes_fewer_bits(shape, level
 
 
 @pytest.mark.gpu
+def test_device_gate_choice_follows_the_host_rule():
+    """latec_gate_choose_apply's word equals gate_word(*gate_choose(sums)) on
+    random rate tables and on ones built to take each branch."""
+    import torch
+
+    from latec_b200 import _lib
+    from latec_b200.gnn_codec import GATE_SHIFTS, GATE_T, gate_choose, gate_fields, gate_word
+
+    lib = _lib.load()
+    R, NB = 1 + 3 * len(GATE_SHIFTS), len(GATE_T) + 1
+    rs = np.random.RandomState(5)
+    cases = [np.zeros((R, NB), np.int64)]
+    low = np.full((R, NB), 1000, np.int64)
+    low[5, :4] = 10  # a candidate cheaper only in the low buckets
+    high = np.full((R, NB), 1000, np.int64)
+    high[9, 8:] = 10  # and one cheaper only in the high buckets
+    cases += [low, high]
+    for _ in range(300):
+        t = rs.randint(0, 1 << 30, size=(R, NB)).astype(np.int64)
+        if rs.rand() < 0.8:
+            r, c = rs.randint(1, R), rs.randint(0, NB)
+            t[r, c:] //= rs.randint(2, 50)
+        cases.append(t)
+    word = torch.zeros(1, dtype=torch.int32, device="cuda")
+    kinds, dirs = set(), set()
+    for sums in cases:
+        dev_sums = torch.from_numpy(sums.reshape(-1)).cuda()
+        _lib.check(lib.latec_gate_choose_apply(0, dev_sums.data_ptr(), None, None, None, None,
+                                               None, 1e-3, word.data_ptr(), _lib.stream_ptr()))
+        want = gate_word(*gate_choose(sums))
+        got = int(word.item())
+        assert got == want, (got, want)
+        kind, direction, _, _ = gate_fields(got)
+        kinds.add(kind)
+        if kind:
+            dirs.add(direction)
+    assert kinds == {0, 1, 2, 3} and dirs == {0, 1}
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("shape,levels,chunk", [((64, 60), 4, None), ((24, 22, 20), 3, None),
                                                 ((40, 36), 2, 16)])
 def test_gate_fine_shares_one_word_over_the_finest_level(shape, levels, chunk):
