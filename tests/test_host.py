@@ -200,3 +200,22 @@ def test_level_thresholds_bracket_the_reference_levels():
         assert np.array_equal(orm.scale_to_level(th, eb), np.arange(1, 64))
         below = np.nextafter(th, np.float32(-np.inf))
         assert np.array_equal(orm.scale_to_level(below, eb), np.arange(0, 63))
+
+
+def test_pick_shape_takes_the_first_least_total():
+    """The shape choice's host half (latec_b200.rans.pick_shape): per
+    candidate the fsum of its partial sums; the first least total wins."""
+    import numpy as np
+
+    from latec_b200 import rans
+
+    P = rans._PARTIALS
+    ids = [4, 7, 9]
+    part = np.zeros((3, P))
+    part[0, 0], part[1, 1], part[2, 2] = 5.0, 3.0, 3.0  # tie between the last two
+    assert rans.pick_shape(ids, part.reshape(-1)) == 7
+    part[2, 3] = -0.5
+    assert rans.pick_shape(ids, part) == 9
+    spread = np.full((3, P), 1.0)
+    spread[1, -1] = 0.5  # the sum over all partials decides, not the first one
+    assert rans.pick_shape(ids, spread) == 7
