@@ -163,6 +163,18 @@ _FIT_DTYPE = np.dtype([("counts_off", np.uint64), ("w_table", np.uint64), ("seg_
                        ("shape_ids", np.uint32, (24,))], align=True)
 
 
+def _stage_flat(plan, t):
+    """Flat grid indices of stage t in the reference's order
+    (np.flatnonzero of the stage mask)."""
+    n = int(plan.counts[t])
+    flat = np.empty(n, np.int64)
+    if n:
+        _lib.check(_lib.load().latec_plan_stage_flat(plan.handle, t, 0, n,
+                                                     flat.ctypes.data_as(ctypes.c_void_p)),
+                   "latec_plan_stage_flat")
+    return flat
+
+
 def _stats_from_device(buf, ns):
     raw = buf.stats.cpu().numpy().tobytes()
     arr = (_lib.StageStats * ns).from_buffer_copy(raw)
@@ -179,8 +191,9 @@ class _Encoder:
     """One compress call's GPU state: the field, the plan and the buffers."""
 
     def __init__(self, field, spatial, c, src, levels_, anchor_stride, anchor_block, radius,
-                 order, entropy, zstd_level, device):
+                 order, entropy, zstd_level, device, predictor=None):
         self.field, self.spatial, self.c, self.src = field, spatial, c, src
+        self.predictor = predictor  # a caller's predictor (None: the fused interpolation)
         self.plan = levels.plan_for(spatial, levels_, anchor_stride, anchor_block)
         self.radius, self.order, self.entropy, self.zstd_level = radius, order, entropy, zstd_level
         self.device = device
@@ -199,10 +212,14 @@ class _Encoder:
         stream = _lib.stream_ptr()
         t0 = time.perf_counter()
         recon.zero_()
-        _lib.check(lib.latec_encode_stages(
-            plan.handle, ctypes.byref(prm), eb_arr, self.field.data_ptr(), recon.data_ptr(),
-            b.codes.data_ptr(), b.outliers.data_ptr(), b.stats.data_ptr(), b.hist_seg.data_ptr(),
-            b.hist_total.data_ptr(), b.ws.data_ptr(), b.ws.numel(), stream), "latec_encode_stages")
+        if self.predictor is None:
+            _lib.check(lib.latec_encode_stages(
+                plan.handle, ctypes.byref(prm), eb_arr, self.field.data_ptr(), recon.data_ptr(),
+                b.codes.data_ptr(), b.outliers.data_ptr(), b.stats.data_ptr(),
+                b.hist_seg.data_ptr(), b.hist_total.data_ptr(), b.ws.data_ptr(), b.ws.numel(),
+                stream), "latec_encode_stages")
+        else:
+            self._caller_stages(ebs, recon, prm, stream)
         st = _stats_from_device(b, ns)
         t1 = time.perf_counter()
         if self.mode == _lib.RANS_LANES:
@@ -273,6 +290,56 @@ class _Encoder:
             stage_fit=fits,
         )
         return payload, n_bytes, stage
+
+    def _caller_stages(self, ebs, recon, prm, stream):
+        """The reference's closed loop (``latec/codec.py:384-459``) around a
+        caller's predictor: per stage its ``predict(recon, known, pos)`` on
+        the host arrays the reference passes (the anchors predicted as 0),
+        then the device quantizer writes the stage's codes, outliers,
+        statistics and histograms where the fused stage kernels would, and
+        its reconstruction returns to ``recon`` and to the host copy."""
+        torch = _torch()
+        lib, b, plan = self.lib, self.buf, self.plan
+        c, spatial = self.c, tuple(self.spatial)
+        dt = np.float64 if self.src == 2 else np.float32
+        recon_np = np.zeros((c,) + spatial, dt)
+        known = np.zeros(spatial, bool)
+        flat_field = self.field.reshape(c, -1)
+        flat_recon = recon.reshape(c, -1)
+        b.stats.zero_()
+        b.hist_seg.zero_()
+        b.hist_total.zero_()
+        ssz = ctypes.sizeof(_lib.StageStats)
+        for t in range(len(plan)):
+            n = int(plan.counts[t])
+            if n == 0:
+                continue
+            flat = _stage_flat(plan, t)
+            pos = np.zeros(int(np.prod(spatial)), bool)
+            pos[flat] = True
+            pos = pos.reshape(spatial)
+            if t == 0:
+                pred = np.zeros((c, n), dt)
+            else:
+                pred = np.asarray(self.predictor.predict(recon_np, known, pos), dt).reshape(c, n)
+            idx = torch.from_numpy(flat).to(self.device)
+            x = flat_field[:, idx].contiguous()
+            p = torch.from_numpy(np.ascontiguousarray(pred)).to(self.device)
+            out = torch.empty_like(x)
+            items = c * n
+            ws = torch.empty(max(int(lib.latec_flat_workspace_bytes(items, b.ldtype)), 1),
+                             dtype=torch.uint8, device=self.device)
+            off = int(b.offsets[t])
+            _lib.check(lib.latec_quantize(
+                ctypes.byref(prm), float(ebs[t]), items, x.data_ptr(), p.data_ptr(),
+                b.codes.data_ptr() + 2 * off, out.data_ptr(), b.outliers.data_ptr() + b.elem * off,
+                b.stats.data_ptr() + t * ssz,
+                b.hist_seg.data_ptr() + 4 * 2 * rans_model.HWIN * int(b.seg_off[t]),
+                b.hist_total.data_ptr() + 4 * 65536 * t, ws.data_ptr(), ws.numel(), stream),
+                "latec_quantize")
+            flat_recon[:, idx] = out
+            recon_np.reshape(c, -1)[:, flat] = out.cpu().numpy()
+            known |= pos
 
     def _fit_native(self, st):
         """Native-mode stage model fit on the device (fit_kernels.cu)."""
@@ -496,16 +563,18 @@ def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, rad
         got = getattr(predictor, name, val)
         if got != val:
             raise ValueError(f"predictor {name}={got} != compress {name}={val}")
-    if not _is_gpu_interp(predictor):
+    # any other predictor is the reference's duck-typed plugin: its predict()
+    # runs per stage on the host, the quantizer and the coder on the device
+    caller = not _is_gpu_interp(predictor)
+    if caller and getattr(predictor, "provides_scale", False):
         raise NotImplementedError(
-            "the CUDA codec runs InterpPredictor stages on the device; use GNNCodec for the "
-            "learned predictor")
+            "per-point scale predictors are coded by GNNCodec (the learned container)")
     from . import levels as _levels
 
     _levels.check_plan(spatial, levels, anchor_stride, anchor_block)
-    order = predictor.order
+    order = "linear" if caller else predictor.order
     enc = _Encoder(field, spatial, c, src, levels, anchor_stride, anchor_block, radius, order,
-                   entropy, zstd_level, dev)
+                   entropy, zstd_level, dev, predictor=predictor if caller else None)
     enc.stream_out = stream_out
     flags = getattr(predictor, "stream_flag", 0)
     if entropy == "native":
@@ -529,9 +598,9 @@ def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, rad
         raise ValueError("tune must be 'fast', 'size', or 'rd'")
     tunable = getattr(predictor, "tunable", False)
     nd = len(spatial)
-    if getattr(predictor, "center", None) is None:
+    if not caller and getattr(predictor, "center", None) is None:
         predictor.center = 1 if nd >= 4 else 0
-    if getattr(predictor, "end_mode", None) is None:
+    if not caller and getattr(predictor, "end_mode", None) is None:
         predictor.end_mode = 1
     if eb_ratio is not None:
         ratio_cands = [eb_ratio]
@@ -540,9 +609,9 @@ def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, rad
     else:
         ratio_cands = [getattr(predictor, "fast_eb_ratio", 1.0)]
     sweep = tunable and tune != "fast" and eb_ratio is None
-    base_center = predictor.center
+    base_center = 0 if caller else predictor.center
     center_cands = [base_center] + ([x for x in (0, 1, 2) if x != base_center] if sweep else [])
-    base_end = predictor.end_mode
+    base_end = 0 if caller else predictor.end_mode
     candidates = []
     seen = set()
 
@@ -580,8 +649,9 @@ def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, rad
     stats["search_predict_s"] = sum(x[7]["predict_s"] for x in candidates)
     stats["search_quantize_s"] = sum(x[7]["quantize_s"] for x in candidates)
     stats["search_entropy_s"] = sum(x[7]["entropy_s"] for x in candidates)
-    predictor.center = center
-    predictor.end_mode = end_mode
+    if not caller:
+        predictor.center = center
+        predictor.end_mode = end_mode
     stats["eb_ratio"] = ratio
     stats["interp_center"] = center
     stats["interp_end_mode"] = end_mode
@@ -601,6 +671,49 @@ def compress(img, eb, predictor, levels=4, anchor_stride=16, anchor_block=1, rad
     stats["original_bytes"] = int(nbytes)
     stats["ratio"] = nbytes / (stream.numel() if _is_tensor(stream) else len(stream))
     return stream, stats
+
+
+def _caller_decode(predictor, plan, ebs, prm, codes, offsets, pay_dev, recs, c, spatial,
+                   src_dtype, recon, err, dev, sp):
+    """The reference's decode loop (``latec/codec.py:462-510``) around a
+    caller's predictor: per stage its ``predict(recon, known, pos)`` on the
+    host, then the device dequantizer against the decoded codes and the
+    stage's outliers (copied out of the payload to an aligned buffer)."""
+    torch = _torch()
+    lib = _lib.load()
+    dt = np.float64 if src_dtype == 2 else np.float32
+    esz = 8 if src_dtype == 2 else 4
+    recon_np = np.zeros((c,) + tuple(spatial), dt)
+    known = np.zeros(tuple(spatial), bool)
+    flat_recon = recon.reshape(c, -1)
+    for t in range(len(plan)):
+        n = int(plan.counts[t])
+        if n == 0:
+            continue
+        flat = _stage_flat(plan, t)
+        pos = np.zeros(int(np.prod(spatial)), bool)
+        pos[flat] = True
+        pos = pos.reshape(tuple(spatial))
+        if t == 0:
+            pred = np.zeros((c, n), dt)
+        else:
+            pred = np.asarray(predictor.predict(recon_np, known, pos), dt).reshape(c, n)
+        p = torch.from_numpy(np.ascontiguousarray(pred)).to(dev)
+        n_o = int(recs[t].n_out)
+        a = int(recs[t].out_at)
+        outl = (pay_dev[a:a + esz * n_o].clone() if n_o
+                else torch.zeros(esz, dtype=torch.uint8, device=dev))
+        items = c * n
+        out = torch.empty((c, n), dtype=recon.dtype, device=dev)
+        ws = torch.empty(max(int(lib.latec_dequantize_workspace_bytes(items)), 1),
+                         dtype=torch.uint8, device=dev)
+        _lib.check(lib.latec_dequantize(ctypes.byref(prm), float(ebs[t]), items, p.data_ptr(),
+                                        codes.data_ptr() + 2 * int(offsets[t]), outl.data_ptr(),
+                                        n_o, out.data_ptr(), err.data_ptr(), ws.data_ptr(),
+                                        ws.numel(), sp), "latec_dequantize")
+        flat_recon[:, torch.from_numpy(flat).to(dev)] = out
+        recon_np.reshape(c, -1)[:, flat] = out.cpu().numpy()
+        known |= pos
 
 
 def _upload_stream(body, dev):
@@ -677,8 +790,9 @@ def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
         predictor.center = header.interp_center
     if hasattr(predictor, "end_mode"):
         predictor.end_mode = (header.flags >> END_MODE_SHIFT) & END_MODE_MAX
-    if not _is_gpu_interp(predictor):
-        raise NotImplementedError("the CUDA codec decodes InterpPredictor streams")
+    caller = not _is_gpu_interp(predictor)  # a caller's predictor: predict() per stage
+    if caller and getattr(predictor, "provides_scale", False):
+        raise NotImplementedError("per-point scale predictors are decoded by GNNCodec")
     if header.src_dtype not in DTYPE_CODES:
         raise KeyError(header.src_dtype)
     _check_radius(header.radius)
@@ -793,8 +907,11 @@ def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
     for t, lc in literal_codes.items():
         codes[int(offsets[t]):int(offsets[t + 1])].copy_(torch.from_numpy(lc.view(np.int16)).to(dev))
     ldt = _lib.F64 if header.src_dtype == 2 else _lib.F32
-    prm = _qparams(header.src_dtype, c, header.radius, predictor.order, predictor.center,
-                   predictor.end_mode, header.src_dtype == 0)
+    if caller:
+        prm = _qparams(header.src_dtype, c, header.radius, "linear", 0, 0, header.src_dtype == 0)
+    else:
+        prm = _qparams(header.src_dtype, c, header.radius, predictor.order, predictor.center,
+                       predictor.end_mode, header.src_dtype == 0)
     ft = torch.float64 if header.src_dtype == 2 else torch.float32
     recon = torch.zeros((c,) + spatial, dtype=ft, device=dev)
     eb_arr = (ctypes.c_double * ns)(*[float(e) for e in ebs])
@@ -802,10 +919,14 @@ def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
     n_out = (ctypes.c_uint32 * ns)(*[recs[t].n_out for t in range(ns)])
     ws2 = torch.empty(max(int(lib.latec_stage_workspace_bytes(plan.handle, c, ldt)), 1),
                       dtype=torch.uint8, device=dev)
-    _lib.check(lib.latec_decode_stages(plan.handle, ctypes.byref(prm), eb_arr, codes.data_ptr(),
-                                       pay_dev.data_ptr(), out_off, n_out, recon.data_ptr(),
-                                       err.data_ptr(), ws2.data_ptr(), ws2.numel(), sp),
-               "latec_decode_stages")
+    if caller:
+        _caller_decode(predictor, plan, ebs, prm, codes, offsets, pay_dev, recs, c, spatial,
+                       header.src_dtype, recon, err, dev, sp)
+    else:
+        _lib.check(lib.latec_decode_stages(plan.handle, ctypes.byref(prm), eb_arr,
+                                           codes.data_ptr(), pay_dev.data_ptr(), out_off, n_out,
+                                           recon.data_ptr(), err.data_ptr(), ws2.data_ptr(),
+                                           ws2.numel(), sp), "latec_decode_stages")
     e = int(err.item())
     del keep
     if e & 1:

@@ -275,3 +275,54 @@ def test_device_stream_roundtrip_equals_host_stream():
     back = lb.decompress(s_dev, out="device")
     assert torch.equal(back, st2["recon"])
     assert np.array_equal(lb.decompress(s_host), st["recon"])
+
+
+class _HostCubic:
+    """A caller's predictor, the reference's duck-typed plugin
+    (``predict(recon, known, pos)``): the oracle's cubic interpolation on the
+    host, finding its stage by the mask it is given."""
+
+    def __init__(self, shape, levels, stride):
+        from oracle import interp, levels as olevels
+
+        self.interp = interp
+        self.plan = list(olevels.iter_plan(shape, levels, stride, 1))
+        self.calls = 0
+
+    def predict(self, recon, known, pos):
+        self.calls += 1
+        for mask, s, axes in self.plan:
+            if np.array_equal(mask, pos):
+                assert not np.any(known & pos)
+                return self.interp.predict(recon, s, axes, np.flatnonzero(pos), "cubic", 0, 1)
+        raise AssertionError("the predictor was given an unknown stage")
+
+
+@pytest.mark.parametrize("shape,entropy", [((40, 36), "native"), ((17, 20, 11), "native"),
+                                           ((40, 36), "compat")])
+def test_caller_predictor_drives_the_closed_loop(shape, entropy):
+    """Any predictor with ``predict(recon, known, pos)`` runs the codec, as in
+    the reference: a host restatement of the cubic interpolation codes the
+    payload InterpPredictor's fused kernels code, and decompress with its
+    factory returns the same field."""
+    from latec_b200 import fields
+    from latec_b200.bitstream import Header
+
+    lb = _lb()
+    x = fields.grf_se(shape, 6.0, seed=4)
+    lv, st = 2, 4
+    host = _HostCubic(shape, lv, st)
+    s_host, st_host = lb.compress(x, 1e-3, host, levels=lv, anchor_stride=st, eb_ratio=0.9,
+                                  entropy=entropy)
+    s_ref, st_ref = lb.compress(x, 1e-3, lb.InterpPredictor("cubic", lv, st, 1), levels=lv,
+                                anchor_stride=st, eb_ratio=0.9, entropy=entropy)
+    assert host.calls > 0
+    hs = Header.unpack(bytes(s_host[:4096])).size
+    assert Header.unpack(bytes(s_ref[:4096])).size == hs
+    assert s_host[hs:] == s_ref[hs:]  # the same frame and stage records
+    assert np.array_equal(st_host["recon"], st_ref["recon"])
+    y = lb.decompress(s_host, predictor_factory=lambda h: _HostCubic(shape, lv, st))
+    assert np.array_equal(y, st_ref["recon"])
+    assert np.abs(y.astype(np.float64) - x).max() <= 1e-3
+    with pytest.raises(ValueError):
+        lb.decompress(s_host)  # the stream names no built-in predictor
