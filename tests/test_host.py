@@ -219,3 +219,22 @@ def test_pick_shape_takes_the_first_least_total():
     spread = np.full((3, P), 1.0)
     spread[1, -1] = 0.5  # the sum over all partials decides, not the first one
     assert rans.pick_shape(ids, spread) == 7
+
+
+def test_plugin_stage_masks_are_the_reference_schedule():
+    """The masks and point order a caller's predictor is given
+    (latec_b200.codec._stage_flat) are the oracle schedule's masks in
+    np.flatnonzero order, stage by stage."""
+    import numpy as np
+
+    from latec_b200 import levels
+    from latec_b200.codec import _stage_flat
+    from oracle import levels as olevels
+
+    for shape, lv, st in [((40, 36), 2, 4), ((17, 20, 11), 2, 4), ((9, 8, 7, 6), 1, 2),
+                          ((5, 130), 3, 8)]:
+        plan = levels.plan_for(shape, lv, st, 1)
+        want = list(olevels.iter_plan(shape, lv, st, 1))
+        assert len(want) == len(plan)
+        for t, (mask, _, _) in enumerate(want):
+            assert np.array_equal(_stage_flat(plan, t), np.flatnonzero(mask))
