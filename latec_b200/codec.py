@@ -169,9 +169,9 @@ def _stage_flat(plan, t):
     n = int(plan.counts[t])
     flat = np.empty(n, np.int64)
     if n:
-        _lib.check(_lib.load().latec_plan_stage_flat(plan.handle, t, 0, n,
-                                                     flat.ctypes.data_as(ctypes.c_void_p)),
-                   "latec_plan_stage_flat")
+        # host-side plan arithmetic: no device needed (as for the plan itself)
+        _lib.check(_lib.load(require_gpu=False).latec_plan_stage_flat(
+            plan.handle, t, 0, n, flat.ctypes.data_as(ctypes.c_void_p)), "latec_plan_stage_flat")
     return flat
 
 
