@@ -390,7 +390,9 @@ int latec_gnn_mlp2_bf16(const float* X, int32_t ldx, int64_t rows, int32_t k1, i
  *      LATEC_ERR_TOO_LARGE). All calls on a device share that array: calls
  *      whose GPU work overlaps race and must not be issued. The first call on
  *      each device looks the array up (cudaGetSymbolAddress); make it before
- *      any stream capture. */
+ *      any stream capture. The lookup is repeated in a new context of the
+ *      device (after cudaDeviceReset, say), so the first call after a reset
+ *      should likewise come before any capture. */
 #define LATEC_ERR_TOO_LARGE (-7)
 #define LATEC_STATIC_MAX_ITEMS (1u << 19)
 int latec_quantize_static(const latec_quant_params* prm, double eb, uint64_t items, const void* x,

@@ -5,6 +5,7 @@
 #include <new>
 #include <vector>
 
+#include "host_util.h"
 #include "interp_kernels.cuh"
 #include "plan.h"
 #include "rans_kernels.cuh"
@@ -41,38 +42,6 @@ struct Carve {
 };
 
 inline int elem_of(int dtype) { return dtype == LATEC_F64 ? 8 : 4; }
-
-bool valid_params(const latec_quant_params* p) {
-    if (!p) return false;
-    if (p->dtype != LATEC_F32 && p->dtype != LATEC_F64) return false;
-    if (p->channels < 1 || p->radius < 1 || p->radius > 32768) return false;
-    if (p->order < 0 || p->order > 1 || p->center < 0 || p->center > 2) return false;
-    if (p->end_mode < 0 || p->end_mode > 3) return false;
-    if (p->round_output < 0 || p->round_output > 2) return false;
-    if (p->round_output == 2 &&
-        !(p->round_span > 0.0 && std::isfinite(p->round_span) && std::isfinite(p->round_offset)))
-        return false;
-    return true;
-}
-
-bool make_q(const latec_quant_params* p, double eb, uint64_t points, QParams& q) {
-    if (!(eb > 0.0)) return false;
-    q.w = 2.0 * eb;
-    const double inv = 1.0 / q.w;
-    q.inv_w = (std::isfinite(inv) && q.w > 0x1p-1000 && std::isfinite(q.w)) ? inv : 0.0;
-    q.eb = eb;
-    q.eb_f = (float)eb;
-    q.radius = p->radius;
-    q.order = p->order;
-    q.center = p->center;
-    q.end_mode = p->end_mode;
-    q.round_output = p->round_output;
-    q.rspan = p->round_output == 2 ? p->round_span : 1.0;
-    q.roff = p->round_output == 2 ? p->round_offset : 0.0;
-    q.channels = p->channels;
-    q.points = points;
-    return true;
-}
 
 // Level-kernel bounds (per level): bands per sub-stage, sub-stages per level.
 constexpr uint32_t LVL_MAX_BANDS = 1024;

@@ -18,11 +18,13 @@
 // threads without ordering) race on the scratch and must not be issued.
 // Set-up: the first call on each device looks the array's device address up
 // with cudaGetSymbolAddress (with that device current); make that first call
-// before any stream capture.
-#include <atomic>
-#include <cmath>
+// before any stream capture. The address is looked up again in a new context
+// of the device (after cudaDeviceReset, for example), so such a call is a
+// set-up call too.
 #include <cuda_runtime.h>
+#include <mutex>
 
+#include "host_util.h"
 #include "interp_kernels.cuh"
 
 namespace latec {
@@ -44,19 +46,35 @@ constexpr uint64_t kBytes = round_up(kPartialsOff + ((uint64_t)MAX_BLOCKS * 5 + 
 static __device__ __align__(256) unsigned char g_quant_scratch[kBytes];
 
 constexpr int kMaxDevices = 64;
-std::atomic<void*> g_scratch_addr[kMaxDevices];
 
-// Device address of g_quant_scratch for the current device, looked up once.
+// Per device: the context the address was looked up in, and the address. A
+// device reset (cudaDeviceReset) or a new primary context reloads the module,
+// which may move the array, so the address is looked up again whenever the
+// current context differs from the one it was found in.
+struct ScratchSlot {
+    std::mutex mu;
+    unsigned long long ctx = 0;
+    void* addr = nullptr;
+};
+ScratchSlot g_scratch[kMaxDevices];
+
+// Device address of g_quant_scratch in the current device's context.
 int scratch_address(void** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return LATEC_ERR_CUDA;
     if (dev < 0 || dev >= kMaxDevices) return LATEC_ERR_UNSUPPORTED;
-    void* p = g_scratch_addr[dev].load(std::memory_order_acquire);
-    if (!p) {
+    const unsigned long long ctx = current_context_id();
+    ScratchSlot& slot = g_scratch[dev];
+    std::lock_guard<std::mutex> lk(slot.mu);
+    // ctx 0: no context was current yet; the lookup below makes the primary
+    // context current, and the next call records its id
+    if (!slot.addr || ctx == 0 || ctx != slot.ctx) {
+        void* p = nullptr;
         if (cudaGetSymbolAddress(&p, g_quant_scratch) != cudaSuccess || !p) return LATEC_ERR_CUDA;
-        g_scratch_addr[dev].store(p, std::memory_order_release);
+        slot.addr = p;
+        slot.ctx = ctx;
     }
-    *out = p;
+    *out = slot.addr;
     return LATEC_OK;
 }
 
@@ -71,14 +89,13 @@ int latec_quantize_static(const latec_quant_params* prm, double eb, uint64_t ite
                           const void* pred, uint16_t* codes, void* recon_out, void* outliers,
                           latec_stage_stats* stats, uint32_t* hist_seg, uint32_t* hist_total,
                           void* stream) {
-    if (!prm || (prm->dtype != LATEC_F32 && prm->dtype != LATEC_F64) || prm->channels < 1 ||
-        prm->radius < 1 || prm->radius > 32768 || prm->order < 0 || prm->order > 1 ||
-        prm->center < 0 || prm->center > 2 || prm->end_mode < 0 || prm->end_mode > 3)
+    // the same parameter checks as latec_quantize, in the same order
+    if (!valid_params(prm) || (items && (!x || !pred || !codes || !recon_out || !outliers)) ||
+        !stats || !hist_seg || !hist_total)
         return LATEC_ERR_ARG;
+    QParams q;
+    if (!make_q(prm, eb, items, q)) return LATEC_ERR_ARG;
     if (items > kItems) return LATEC_ERR_TOO_LARGE;
-    if ((items && (!x || !pred || !codes || !recon_out || !outliers)) || !stats || !hist_seg ||
-        !hist_total)
-        return LATEC_ERR_ARG;
     void* base = nullptr;
     int rc = scratch_address(&base);
     if (rc) return rc;
@@ -87,26 +104,6 @@ int latec_quantize_static(const latec_quant_params* prm, double eb, uint64_t ite
     uint32_t* tile_cnt = (uint32_t*)(s + kTileCntOff);
     uint32_t* tile_off = (uint32_t*)(s + kTileOffOff);
     double* partials = (double*)(s + kPartialsOff);
-    QParams q;
-    if (!(eb > 0.0)) return LATEC_ERR_ARG;
-    q.w = 2.0 * eb;
-    const double inv = 1.0 / q.w;
-    q.inv_w = (std::isfinite(inv) && q.w > 0x1p-1000 && std::isfinite(q.w)) ? inv : 0.0;
-    q.eb = eb;
-    q.eb_f = (float)eb;
-    q.radius = prm->radius;
-    q.order = prm->order;
-    q.center = prm->center;
-    q.end_mode = prm->end_mode;
-    q.round_output = prm->round_output;
-    if (q.round_output < 0 || q.round_output > 2 ||
-        (q.round_output == 2 && !(prm->round_span > 0.0 && std::isfinite(prm->round_span) &&
-                                  std::isfinite(prm->round_offset))))
-        return LATEC_ERR_ARG;
-    q.rspan = q.round_output == 2 ? prm->round_span : 1.0;
-    q.roff = q.round_output == 2 ? prm->round_offset : 0.0;
-    q.channels = prm->channels;
-    q.points = items;
     cudaStream_t st = (cudaStream_t)stream;
     // outputs that accumulate start at zero; tile counts are zeroed by the launcher
     if (cudaMemsetAsync(stats, 0, sizeof(latec_stage_stats), st) != cudaSuccess ||

@@ -9,6 +9,7 @@ points from its rank.
 from __future__ import annotations
 
 import ctypes
+import threading
 from collections import OrderedDict
 
 import numpy as np
@@ -103,20 +104,27 @@ class Plan:
 
 
 _plans: "OrderedDict" = OrderedDict()
+_plans_lock = threading.Lock()
 _PLAN_CACHE = 1024  # schedules kept (host memory only, a few KB each)
 
 
 def plan_for(shape, levels, anchor_stride, anchor_block=1) -> Plan:
     """The schedule of a shape, from a least-recently-used cache: a batch of
-    many tensors of different shapes reuses its plans from call to call."""
+    many tensors of different shapes reuses its plans from call to call.
+    Safe to call from several host threads: the cache is updated under a
+    lock, and a plan built concurrently by two threads is kept once."""
     key = (tuple(int(n) for n in shape), int(levels), int(anchor_stride), int(anchor_block))
-    p = _plans.get(key)
-    if p is None:
-        p = _plans[key] = Plan(*key)
-        if len(_plans) > _PLAN_CACHE:
-            _plans.popitem(last=False)
-    else:
+    with _plans_lock:
+        p = _plans.get(key)
+        if p is not None:
+            _plans.move_to_end(key)
+            return p
+    built = Plan(*key)  # outside the lock: the C++ plan build may take a while
+    with _plans_lock:
+        p = _plans.setdefault(key, built)
         _plans.move_to_end(key)
+        while len(_plans) > _PLAN_CACHE:
+            _plans.popitem(last=False)
     return p
 
 

@@ -18,8 +18,10 @@ train_gnn.py:154-192) are one kernel each. torch only holds device memory and
 draws the random numbers.
 
 Deliberate differences from the reference trainer: float32 (no FP16 autocast
-/ GradScaler), no chunked two-chunk scenes (``run_chunked_scene``), and the
-synthetic generator of ``latec_b200.synthetic`` (no advection warp).
+/ GradScaler) and no chunked two-chunk scenes (``run_chunked_scene``). The
+fields come from ``latec_b200.synthetic``, a restatement of the reference's
+generator (advection warp included) whose seeded fields equal the
+reference's.
 """
 
 from __future__ import annotations

@@ -1,7 +1,7 @@
 """Generate tests/golden/gnn.npz from the reference GNN predictor itself.
 
-Imports the reference package (path given by --ref, default the reference
-checkout) with the test-only zstandard shim, loads seeded weights from
+Imports the reference package (the checkout's root is the required --ref
+argument) with the test-only zstandard shim, loads seeded weights from
 ``latec_b200.gnn.random_weights`` into ``latec.gnn_predictor.build_model``,
 builds the stage geometry with ``build_stage_geoms`` and runs the closed loop
 ``stage_forward`` over every stage (true values revealed after each stage),
@@ -44,7 +44,7 @@ def field(shape, batch, seed):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of the reference LATEC checkout")
     args = ap.parse_args()
     sys.path.insert(0, os.path.join(HERE, "_refshim"))
     sys.path.insert(0, args.ref)

@@ -2,7 +2,7 @@
 
 Run in a container that has the reference checkout (read-only is fine):
 
-    python tests/golden/make_golden.py --reference /root/reference
+    python tests/golden/make_golden.py --reference <reference checkout>
 
 It imports the reference package itself (``latec``) with two test-only
 stand-ins on ``sys.path``: ``_refshim/zstandard.py`` (ctypes over the system
@@ -305,7 +305,7 @@ def make_quantizer_cases(quantizer, out_dir):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of the reference LATEC checkout")
     ap.add_argument("--out", default=HERE)
     args = ap.parse_args()
     sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))

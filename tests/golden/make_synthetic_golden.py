@@ -5,7 +5,7 @@ test-only zstandard shim in ``_refshim``). The cases cover 2-D, 3-D and 4-D
 shapes, smooth and turbulent (advected) rows, every marginal warp and the
 hyperplane jumps, plus the deterministic ``randomize=False`` path.
 
-    python tests/golden/make_synthetic_golden.py [--ref PATH]
+    python tests/golden/make_synthetic_golden.py --ref PATH
 """
 
 import argparse
@@ -29,7 +29,7 @@ CASES = [
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="root of the reference LATEC checkout")
     args = ap.parse_args()
     sys.path.insert(0, os.path.join(HERE, "_refshim"))  # test-only zstandard shim
     sys.path.insert(0, args.ref)
