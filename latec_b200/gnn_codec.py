@@ -334,6 +334,11 @@ class GNNCodec:
         self._weights = weights
         self._models = {}
         self._geoms = {}
+        # a list to receive per-stage device tensors of every encode (model mu
+        # and scale, gate word, codes, scale levels, outliers), or None. A
+        # test and diagnosis aid: parity checks against the reference codec
+        # compare them stage by stage.
+        self.stage_trace = None
 
     def _model(self, precision: str):
         """The model in one float path: "f32", "bf16" (the tensor-core message
@@ -557,6 +562,8 @@ class GNNCodec:
                 mu = mu.reshape(-1).contiguous()
                 scale = torch.exp2(lb.reshape(-1)).contiguous()
             xs = X[:, g.query_idx].reshape(-1).contiguous()
+            if self.stage_trace is not None:
+                tr = {"stage": gi, "eb": seb, "mu": mu.clone(), "scale": scale.clone()}
             shared = gate_fine and finest[gi]
             if gate and gi > 0 and n:
                 # the interpolation fallback, scored, chosen (gate_choose's rule)
@@ -597,6 +604,11 @@ class GNNCodec:
                                           htot.data_ptr(), ws.data_ptr(), ws.numel(),
                                           _lib.stream_ptr()), "latec_quantize")
             lv_all[o:o + n].copy_(rans.scale_to_level(scale, seb))
+            if self.stage_trace is not None:
+                tr.update(codes=codes_all[o:o + n].clone(), levels=lv_all[o:o + n].clone(),
+                          mu_gated=mu.clone(), scale_gated=scale.clone(), word=gw[gi].clone(),
+                          recon=recon.clone(), outliers=outl_all[o:o + n].clone())
+                self.stage_trace.append(tr)
             recon_all[:, g.query_idx] = recon.reshape(B, -1)
             prev, vals = g, recon.reshape(B, -1)
         payload = self._entropy(ebs, offs, codes_all, lv_all, outl_all, stats_all, radius)

@@ -1,0 +1,94 @@
+"""The learned codec against the reference learned codec, stage by stage.
+
+tests/golden/gnn_codec.npz was recorded from the reference's own
+``GNNCodec.compress`` (float32 on the CPU, gate on) with the checkpoint this
+repository ships, by tests/golden/make_gnn_codec_golden.py. Here
+``latec_b200.GNNCodec`` (float32 path, same checkpoint) codes the same fields
+on the GPU, and its per-stage trace is compared with the recording
+(latec/gnn_codec.py:1048-1336 is the loop both follow):
+
+* the model's mu and Laplace scale per stage, within float32 tolerance (the
+  two evaluate the same network in different summation orders);
+* the gate's choice per stage (kind, direction, T, shift);
+* the quantized codes and the scale levels: identical except at the few
+  points whose quotient (x - mu) / 2eb, or whose scale, lies within float32
+  rounding of a bin or level boundary;
+* the final reconstruction and the error bound.
+"""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT
+
+pytestmark = pytest.mark.gpu
+
+CKPT = os.path.join(ROOT, "latec_b200", "checkpoints", "gnn_d64_agg1_synthetic.pt")
+
+
+def _load():
+    z = np.load(os.path.join(GOLDEN, "gnn_codec.npz"))
+    meta = json.loads(bytes(z["meta"]).decode())
+    return z, meta
+
+
+CASES = [m["name"] for m in _load()[1]]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_gnn_codec_matches_reference_per_stage(name):
+    import latec_b200 as lb
+    from latec_b200.gnn_codec import gate_fields
+
+    z, metas = _load()
+    m = next(mm for mm in metas if mm["name"] == name)
+    x = z[f"{name}/x"]
+    codec = lb.GNNCodec(CKPT, device="cuda")
+    codec.stage_trace = []
+    stream = codec.compress(x, m["rel_eb"], levels=m["levels"], fp16=False, gate=True)
+    tr = {t["stage"]: t for t in codec.stage_trace}
+    report = []
+    n_code_diff = n_code = n_lv_diff = 0
+    for k, s in enumerate(m["stages"]):
+        t = tr[s]
+        eb = m["ebs"][k]
+        assert abs(t["eb"] - eb) <= 1e-15 * eb, (s, t["eb"], eb)
+        mu_r, sc_r = z[f"{name}/{k}/mu"], z[f"{name}/{k}/scale"]
+        mu, sc = t["mu"].cpu().numpy(), t["scale"].cpu().numpy()
+        assert mu.shape == mu_r.shape, (s, mu.shape, mu_r.shape)
+        dmu = float(np.abs(mu.astype(np.float64) - mu_r).max())
+        dsc = float(np.abs(np.log2(sc.astype(np.float64) / sc_r)).max())
+        # the gate's choice
+        g_ref = m["gates"][k]
+        g = list(gate_fields(int(t["word"].item())))
+        codes_r, codes = z[f"{name}/{k}/codes"], t["codes"].cpu().numpy().astype(np.int64)
+        lv_r, lv = z[f"{name}/{k}/levels"], t["levels"].cpu().numpy()
+        dc = int((codes != codes_r).sum())
+        dl = int((lv != lv_r).sum())
+        n_code_diff += dc
+        n_lv_diff += dl
+        n_code += len(codes)
+        report.append((s, len(mu), dmu, dsc, g_ref, g, dc, dl))
+        # float32 agreement of the network's outputs (values in [0, 1])
+        assert dmu <= 2e-4, report[-1]
+        assert dsc <= 2e-3, report[-1]
+        if g_ref is not None:
+            assert g == g_ref, ("gate", report[-1])
+    print("\n".join(map(str, report)))
+    # codes and levels: identical up to rounding-boundary points
+    assert n_code_diff <= max(2, n_code // 2000), report
+    assert n_lv_diff <= max(2, n_code // 500), report
+    # the decoded field holds the bound (plus the float32 normalisation slack)
+    back = codec.uncompress(stream).cpu().numpy()
+    vmin, vmax = float(np.float32(x.min())), float(np.float32(x.max()))
+    slack = 2.0 ** -24 * (3.0 * (vmax - vmin) + max(abs(vmin), abs(vmax)))
+    assert float(np.abs(back.astype(np.float64) - x).max()) <= m["eb_abs"] + slack
+    if n_code_diff == 0:
+        # every code equal: the decoded field is the reference's
+        # reconstruction, denormalised as the reference does (float32)
+        recon_r = z[f"{name}/recon"].reshape(x.shape)
+        want = recon_r * np.float32(vmax - vmin) + np.float32(vmin)
+        assert np.array_equal(back.reshape(x.shape), want)
