@@ -162,23 +162,23 @@ int latec_dequantize(const latec_quant_params* prm, double eb, uint64_t items, c
  *      Results are bit-identical in all modes. Process-wide. */
 int latec_set_level_mode(int32_t mode);
 
-/* ---- fused tile levels of 3-D plans (no counterpart in the reference): the
+/* ---- fused levels of 3-D plans (no counterpart in the reference): the
  *      five sub-stages of a level (weight 1 along axes 0, 1, 2, weight 2,
- *      weight 3) in one launch over tiles of the level's lattice held in
- *      shared memory with a 3-point halo, encode and decode alike.
- *      0 (default) = off (one launch per stage, measured faster on B200),
- *      1 = the finest level, 2 = every level. Results are bit-identical in
- *      all modes.
- *      Process-wide. */
+ *      weight 3) in one launch each way, over column tiles of the level's
+ *      lattice whose planes are staged in shared memory (TMA loads) with a
+ *      3-point halo. 0 = off (one launch per stage), 1 = the finest level,
+ *      2 (default) = every level of at least 2^18 points, 3 = every level.
+ *      Results are bit-identical in all modes. Process-wide. */
 int latec_set_tile_mode(int32_t mode);
 
 /* ---- kernel timing (a measurement aid, no counterpart in the reference):
  *      with timing on, a CUDA event pair is recorded on the launching stream
- *      around every fused tile-level launch and every native lane-coder
- *      launch. latec_kernel_time sums the recorded pairs of one kind (0 = tile
- *      encode, 1 = tile decode, 2 = lane encode, 3 = lane decode; it waits for
- *      their end events), returns the milliseconds and the launch count, and
- *      clears them. Process-wide. */
+ *      around every fused level launch and every native lane-coder launch.
+ *      latec_kernel_time sums the recorded pairs of one kind (0 = fused encode
+ *      of a finest level, 1 = its decode, 2 = lane encode, 3 = lane decode,
+ *      4 / 5 = fused encode / decode of a coarser level; it waits for their
+ *      end events), returns the milliseconds and the launch count, and clears
+ *      them. Process-wide. */
 int latec_set_kernel_timing(int32_t on);
 int latec_kernel_time(int32_t kind, double* ms, uint32_t* launches);
 

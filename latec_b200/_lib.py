@@ -36,8 +36,21 @@ class QuantParams(ctypes.Structure):
 
 
 class StageStats(ctypes.Structure):
-    _fields_ = [("n_out", U32), ("maxq", U32), ("pad0", U32), ("pad1", U32),
+    _fields_ = [("n_out", U32), ("maxq", U32), ("done", U32), ("pad1", U32),
                 ("stats", D * 5)]
+
+
+# StageStats.done bit set by a fused level encode whose plane loads did not
+# arrive within the kernel's wait limit (its results are not valid).
+TILE_WAIT_FAILED = 0x80000000
+
+
+def check_stage_stats(stats):
+    """Raise if a fused level kernel reported a failed load wait in the
+    statistics of an encode (``stats``: an array of StageStats)."""
+    if any(int(s.done) & TILE_WAIT_FAILED for s in stats):
+        raise RuntimeError("latec_encode_stages: a fused level kernel timed out waiting for "
+                           "its plane loads; the encode is invalid")
 
 
 class RansStage(ctypes.Structure):

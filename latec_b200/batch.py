@@ -217,6 +217,7 @@ def _compress_group(jobs, predictor, dev, lib):
     for j, jb in enumerate(jobs):
         ns = len(jb.plan)
         jb.st = (_lib.StageStats * ns).from_buffer_copy(raw[stage0[j] * ssz:(stage0[j] + ns) * ssz])
+        _lib.check_stage_stats(jb.st)
     _fit_all(jobs, bufs, stage0, dev, lib)
     payload, starts, lens = _entropy_all(jobs, bufs, dev, lib)
     # ---- frames: the headers uploaded together, one frame launch per stream

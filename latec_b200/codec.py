@@ -178,6 +178,7 @@ def _stage_flat(plan, t):
 def _stats_from_device(buf, ns):
     raw = buf.stats.cpu().numpy().tobytes()
     arr = (_lib.StageStats * ns).from_buffer_copy(raw)
+    _lib.check_stage_stats(arr)
     return arr
 
 

@@ -120,11 +120,14 @@ void plan_sizes(const latec_plan* plan, int C, uint64_t* max_items, uint64_t* al
     *all_tiles = t;
 }
 
-// Fused tile levels of 3-D plans: 0 off (per-stage launches, the default:
-// measured faster on B200, the fused kernels being issue-bound on integer
-// work), 1 the finest level (stride 1) only, 2 every level. Results are
-// bit-identical.
-std::atomic<int> g_tile_mode{0};
+// Fused levels of 3-D plans: 0 off (per-stage launches), 1 the finest level
+// (stride 1) only, 2 every level of at least TILE_MIN_POINTS points (the
+// default), 3 every level whatever its size. Results are bit-identical in
+// every mode.
+std::atomic<int> g_tile_mode{2};
+// Below this many points a level keeps its per-stage launches: a small
+// lattice has too few column tiles to fill the GPU with fused work items.
+constexpr uint64_t TILE_MIN_POINTS = 1ull << 18;
 
 // Kernel timing (a measurement aid): when on, a CUDA event pair is recorded
 // on the launching stream around every fused-level launch (kind 0 = encode,
@@ -167,7 +170,7 @@ bool tile_level_at(const latec_plan* plan, int t, int mode) {
     if (mode == 1 && plan->stages[t].s != 1) return false;
     uint64_t n = 0;
     for (int j = 0; j < TILE_STAGES; j++) n += plan->stages[t + j].n;
-    return n > 0;
+    return mode == 2 ? n >= TILE_MIN_POINTS : n > 0;
 }
 
 int n_sms() {
@@ -346,7 +349,7 @@ int latec_set_level_mode(int32_t mode) {
 }
 
 int latec_set_tile_mode(int32_t mode) {
-    if (mode < 0 || mode > 2) return LATEC_ERR_ARG;
+    if (mode < 0 || mode > 3) return LATEC_ERR_ARG;
     g_tile_mode.store(mode);
     return LATEC_OK;
 }
@@ -357,7 +360,7 @@ int latec_set_kernel_timing(int32_t on) {
 }
 
 int latec_kernel_time(int32_t kind, double* ms, uint32_t* launches) {
-    if (!ms || !launches || kind < 0 || kind > 3) return LATEC_ERR_ARG;
+    if (!ms || !launches || kind < 0 || kind > 5) return LATEC_ERR_ARG;
     std::lock_guard<std::mutex> lk(g_kt_mu);
     double sum = 0.0;
     uint32_t n = 0;
@@ -474,7 +477,7 @@ int latec_encode_stages(const latec_plan* plan, const latec_quant_params* prm,
             uint32_t grid;
             if (!tile_level_init(plan, prm, stage_eb, t, C, codes, off, L, &grid))
                 return LATEC_ERR_ARG;
-            L.vec = tile_vec_ok(L, elem, x, recon) ? 1 : 0;
+            L.tma = tile_tma_ok(L, elem, x, recon) ? 1 : 0;
             TailArgs ta;
             std::memset(&ta, 0, sizeof(ta));
             uint64_t stg = 0, o = off, sg = seg;
@@ -497,7 +500,7 @@ int latec_encode_stages(const latec_plan* plan, const latec_quant_params* prm,
             }
             if (tl && cudaMemsetAsync(w.tile_cnt, 0, sizeof(uint32_t) * tl, st) != cudaSuccess)
                 return LATEC_ERR_CUDA;
-            const int ki = kt_start(0, st);
+            const int ki = kt_start(plan->stages[t].s == 1 ? 0 : 4, st);
             int rc = launch_tile_level_encode(L, prm->dtype, prm->order ? 1 : 0, grid, x, recon, st);
             kt_stop(ki, st);
             if (!rc) rc = launch_stage_tails(ta, TILE_STAGES, st);
@@ -671,9 +674,9 @@ int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
             if (!tile_level_init(plan, prm, stage_eb, t, C, const_cast<uint16_t*>(codes),
                                  ds[t].codes_off, L, &grid))
                 return LATEC_ERR_ARG;
-            L.vec = tile_vec_ok(L, elem_of(prm->dtype), recon, recon) ? 1 : 0;
-            const int ki = kt_start(1, st);
-            rc = launch_tile_level_decode(L, prm->dtype, prm->order ? 1 : 0, grid, recon, st);
+            L.tma = tile_tma_ok(L, elem_of(prm->dtype), recon, recon) ? 1 : 0;
+            const int ki = kt_start(plan->stages[t].s == 1 ? 1 : 5, st);
+            rc = launch_tile_level_decode(L, prm->dtype, prm->order ? 1 : 0, grid, recon, err, st);
             kt_stop(ki, st);
             if (rc) return rc;
             t += TILE_STAGES;

@@ -1,208 +1,385 @@
 // Fused level kernels for 3-D grids: the five sub-stages of one level of the
-// dyadic schedule in one launch, tile by tile in shared memory.
+// dyadic schedule in one launch each way.
 //
 // The level is seen as its lattice (lattice point u <-> grid point s * u).
 // The level's points are the lattice points with an odd coordinate; their
 // predictions read only lattice points one and three steps away along their
-// own odd axes, and a point reached by a step along axis j is even along j,
-// so it never steps along j again. A point therefore depends on nothing more
-// than three lattice steps away on any axis. A CTA owns a TX x TY column of the
-// lattice (axes 2 and 1) over a chunk of axis-0 planes and keeps a box with a
-// 3-point halo (4 along axis 2, so rows start on 16-byte boundaries) of each
-// plane in shared memory:
-//   - a plane with even axis-0 coordinate depends only on itself: its
-//     weight-1 points along axes 2 and 1 come from the coarse points, then its
-//     weight-2 points from those;
-//   - a plane with odd coordinate z needs the even planes z - 3 .. z + 3: its
-//     weight-1 points along axis 0, then the weight-2 points, then weight 3.
-// The CTA walks its chunk as E(zs - 2), E(zs), E(zs + 2), then E(z + 3), O(z)
-// for every odd z of the chunk, with the next plane's box loaded by cp.async
-// (16-byte copies when rows are 16-byte aligned) while the current one is
-// computed (five even planes in a ring, one odd). Only the classes a neighbour
-// needs are computed in the halo, from the same inputs with the same
-// arithmetic, so every CTA that holds a point holds the same reconstruction;
-// only owned points write codes, outliers, statistics and the canvas.
+// own odd axes, and a point reached by a step along axis j is even along j, so
+// no dependency is more than three lattice steps away on any axis. With
+// (z, y, x) the lattice axes 0, 1, 2 and the parities written e/o:
+//   - an even plane z holds the coarse points (e,e,e), weight 1 along y
+//     (e,o,e) and along x (e,e,o), both from the coarse points of the plane,
+//     and weight 2 (e,o,o) from those two;
+//   - an odd plane z holds weight 1 along z (o,e,e) from the coarse points of
+//     the even planes z-3 .. z+3, weight 2 (o,o,e) and (o,e,o) from the even
+//     planes' weight-1 points and the plane's own (o,e,e), and weight 3
+//     (o,o,o) from the even planes' (e,o,o) and the plane's weight-2 points.
 //
+// A CTA owns a column of TY x TX lattice points (axes 1, 2) over a chunk of
+// axis-0 planes and marches along axis 0: E(zs-2), E(zs), E(zs+2), then the
+// pair (E(z+3), O(z)) for every odd z of the chunk. A plane lives in shared
+// memory split by (y, x) parity into four dense sub-arrays (EE, EO, OE, OO),
+// so that every tap read of a warp touches consecutive words: no bank
+// conflicts. The box covers the tile plus the halo the tile's points depend
+// on (3 points along each of y and x); halo points are computed from the same
+// inputs with the same arithmetic as by the CTA that owns them, so every copy
+// of a point holds the same reconstruction, and only owned points write codes,
+// outliers, statistics and the canvas.
+//
+// Planes arrive in a staging buffer in natural layout, by TMA
+// (cp.async.bulk.tensor, no multicast: the tensor maps cover this GPU's own
+// field and canvas) when rows are whole 16-byte groups, else by per-element
+// async copies; the next unit's planes load while the current unit computes.
+// A unit runs in three phases separated by barriers, each a flat list of warp
+// tasks of 32 points of one class:
+//   P1: E.(e,o,e), E.(e,e,o), O.(o,e,e)
+//   P2: E.(e,o,o), O.(o,o,e), O.(o,e,o)
+//   P3: O.(o,o,o)
 // Every prediction and quantization is the per-stage kernels' arithmetic
-// (axis_combine / Quant), so codes, outliers and the reconstruction are
-// bit-identical to the stage-by-stage path. Codes go to each stage's rank
-// order (closed form below), i.e. the reference's per-stage flat order
-// (latec/levels.py:469-574).
+// (axis_combine / Quant / dequant_value), so codes, outliers and the
+// reconstruction are bit-identical to the stage-by-stage path. Codes go to
+// each stage's rank order (closed form below), i.e. the reference's per-stage
+// flat order (latec/levels.py:469-574).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <cstring>
+
+#include "host_util.h"
 #include "interp_device.cuh"
 #include "tile_kernels.cuh"
 
 namespace latec {
 namespace {
 
-template <typename T>
-struct TileShape;
-template <>
-struct TileShape<float> {
-    static constexpr int TX = 64, TY = 32;
-};
-template <>
-struct TileShape<double> {
-    static constexpr int TX = 64, TY = 16;
-};
+constexpr int LT = 256;       // threads per CTA
+constexpr int LW = LT / 32;   // warps per CTA
+constexpr int MAXT = 8;       // warp tasks of one phase at most (decode code prefetch)
+constexpr uint32_t LOAD_WAIT_LIMIT = 1u << 24;  // polls of a plane load before giving up
 
 template <typename T>
-struct Box {
-    static constexpr int TX = TileShape<T>::TX, TY = TileShape<T>::TY;
-    static constexpr int BX = TX + 8;  // lattice columns x0 - 4 .. x0 + TX + 3
-    static constexpr int BY = TY + 6;  // lattice rows y0 - 3 .. y0 + TY + 2
-    static constexpr int ELEMS = BX * BY;
-    static constexpr int SLOTS = 6;  // even planes in a ring of 5, one odd plane
-    static constexpr int VEC = 16 / (int)sizeof(T);  // elements per 16-byte group
-    static constexpr int GROW = BX / VEC;            // 16-byte groups per box row
-    // Class regions (box row r holds lattice row y0 - 3 + r: y is even on odd
-    // r; box column b holds lattice column x0 - 4 + b):
-    static constexpr int HR_R0 = 1, HR_N = TY / 2 + 3;  // even y over the halo
-    static constexpr int TR_R0 = 4, TR_N = TY / 2;      // odd y inside the tile
-    static constexpr int HC_B0 = 2, HC_N = TX / 2 + 3;  // even x over the halo
-    static constexpr int TC_B0 = 5, TC_N = TX / 2;      // odd x inside the tile
+struct G {
+    static constexpr int TX = 64;
+    static constexpr int TY = sizeof(T) == 4 ? 32 : 16;
+    static constexpr int NER = TY / 2 + 3;  // even rows: y0 - 2 .. y0 + TY + 2
+    static constexpr int NOR = TY / 2;      // odd rows: y0 + 1 .. y0 + TY - 1
+    static constexpr int P = TX / 2 + 4;    // row pitch: E-cols x0-4 .. x0+TX+2, O-cols x0-3 ..
+    static constexpr int EE = 0, EO = NER * P, OE = 2 * NER * P, OO = 2 * NER * P + NOR * P;
+    static constexpr int SLOT = 2 * (NER + NOR) * P;  // elements of one plane
+    static constexpr int SLOTS = 6;                   // 4 even planes, 2 odd planes
+    static constexpr int BX = TX + 8;                 // staging columns x0 - 4 .. x0 + TX + 3
+    static constexpr int XR = TY + 5;                 // staging rows y0 - 2 .. y0 + TY + 2
+    static constexpr int RR = TY / 2 + 3;             // coarse staging: even rows only
+    static constexpr int VEC = 16 / (int)sizeof(T);   // elements per 16-byte group
+    static constexpr int GPR = BX / VEC;              // 16-byte groups per staging row
+    static_assert(2 * P == BX, "a staging row maps onto one E row and one O row");
 };
 
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+constexpr uint32_t al128(uint32_t v) { return (v + 127u) & ~127u; }
+
+// Shared-memory layout (byte offsets).
+template <typename T, bool ENC>
+struct Lay {
+    using Gm = G<T>;
+    static constexpr uint32_t SLOTS = 0;
+    static constexpr uint32_t XE = al128(SLOTS + Gm::SLOTS * Gm::SLOT * sizeof(T));
+    static constexpr uint32_t XO = al128(XE + Gm::XR * Gm::BX * sizeof(T));
+    static constexpr uint32_t RS = al128(XO + Gm::XR * Gm::BX * sizeof(T));
+    static constexpr uint32_t HIST = al128(RS + (ENC ? Gm::RR * Gm::BX * sizeof(T) : 0));
+    static constexpr uint32_t WACC =
+        al128(HIST + (ENC ? sizeof(uint32_t) * TILE_STAGES * HBINS : 0));
+    static constexpr uint32_t WMQ = WACC + (ENC ? sizeof(double) * LW * TILE_STAGES * 5 : 0);
+    static constexpr uint32_t WNO = WMQ + (ENC ? sizeof(uint32_t) * LW * TILE_STAGES : 0);
+    // decode: per warp, two buffers of MAXT tasks x 32 lanes of 16-bit codes
+    static constexpr uint32_t CODE_ENTRIES = 2u * LW * MAXT * 32;
+    static constexpr uint32_t CODES =
+        al128(WNO + (ENC ? sizeof(uint32_t) * LW * TILE_STAGES : 0));
+    static constexpr uint32_t MBAR = al128(CODES + (ENC ? 0 : sizeof(uint16_t) * CODE_ENTRIES));
+    static constexpr uint32_t BYTES = MBAR + 16;
+    // two resident CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA)
+    static_assert(2 * (BYTES + 1024) <= 228 * 1024, "fused level CTA exceeds half an SM");
+};
+
+// ------------------------------------------------------------ async copies
+__device__ __forceinline__ uint32_t su32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void* dst, const void* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(smem_addr(dst)), "l"(src),
-                 "n"(BYTES));
+__device__ __forceinline__ void mbar_init(uint32_t bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
-// 16-byte copy; src_bytes 0 writes zeros and reads nothing
-__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_addr(dst)), "l"(src),
-                 "r"(src_bytes));
+__device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, P;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for a phase of the load barrier: false when it did not
+// complete within the limit.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t i = 0; i < LOAD_WAIT_LIMIT; i++)
+        if (mbar_try(bar, parity)) return true;
+    return false;
+}
+// One box of a 4-D tensor map into shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load4(uint32_t dst, const CUtensorMap* map, int c0, int c1,
+                                          int c2, int c3, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+        : "memory");
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_el(void* dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(su32(dst)), "l"(src),
+                 "n"(BYTES), "r"(src_bytes)
+                 : "memory");
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_wait_all() {
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Even / odd lattice counts along axes 1 and 2 and per-plane class counts:
-// the closed-form stage ranks.
-struct Ranks {
-    uint32_t cye, cyo, cxe, cxo;
-    uint32_t a1, a2;  // points of weight 1 / 2 in one axis-0 plane
+// ------------------------------------------------------------ classes
+enum { C_W1Y, C_W1X, C_W2E, C_W1Z, C_W2ZY, C_W2ZX, C_W3, C_NONE };
+
+// A class of level points: its plane (even / odd z), its sub-array, the region
+// it is computed over (rows x columns of the sub-array) and its stage.
+template <typename T, int CL>
+struct Cl {
+    using Gm = G<T>;
+    static constexpr int ZO = CL >= C_W1Z ? 1 : 0;
+    static constexpr int YO = (CL == C_W1Y || CL == C_W2E || CL == C_W2ZY || CL == C_W3) ? 1 : 0;
+    static constexpr int XO = (CL == C_W1X || CL == C_W2E || CL == C_W2ZX || CL == C_W3) ? 1 : 0;
+    static constexpr int SUB = YO ? (XO ? Gm::OO : Gm::OE) : (XO ? Gm::EO : Gm::EE);
+    // odd rows: the tile's; even rows: the tile's plus the 3-point halo
+    static constexpr int NR = YO ? Gm::NOR : Gm::NER;
+    // O-cols: the tile's (2 .. TX/2 + 1); E-cols: plus the halo (1 .. TX/2 + 3)
+    static constexpr int C0 = XO ? 2 : 1;
+    static constexpr int NC = XO ? Gm::TX / 2 : Gm::TX / 2 + 3;
+    static constexpr int STAGE = CL == C_W1Z ? 0 : CL == C_W1Y ? 1 : CL == C_W1X ? 2
+                                 : CL == C_W3 ? 4 : 3;
+    static constexpr int NPTS = NR * NC;
+    static constexpr int NT = (NPTS + 31) / 32;
+};
+
+template <typename T, int CL>
+constexpr int ntasks() {
+    if constexpr (CL == C_NONE) return 0;
+    else return Cl<T, CL>::NT;
+}
+
+// Closed-form stage ranks of lattice point (z, y, x) (per channel): C order
+// over the class lattice for the single-class stages; for the fused weight-2
+// stage, the count of weight-2 points before it in C order.
+struct LvRanks {
+    uint32_t cye, cyo, cxe, cxo, a1, a2;
     __device__ void init(const int32_t* N) {
         cye = (uint32_t)(N[1] + 1) >> 1;
         cyo = (uint32_t)N[1] >> 1;
         cxe = (uint32_t)(N[2] + 1) >> 1;
         cxo = (uint32_t)N[2] >> 1;
-        a1 = cyo * cxe + cye * cxo;
-        a2 = cyo * cxo;
+        a1 = cyo * cxe + cye * cxo;  // weight-2 points of an odd plane
+        a2 = cyo * cxo;              // weight-2 points of an even plane
     }
-    // Rank of lattice point (z, y, x) in its stage: C-order over the class
-    // lattice for the weight-1 stages; for the fused stages, the count of
-    // same-weight points before it in C order.
-    template <int STAGE>
+    template <int CL>
     __device__ __forceinline__ uint32_t of(int z, int y, int x) const {
         const uint32_t zh = (uint32_t)z >> 1, yh = (uint32_t)y >> 1, xh = (uint32_t)x >> 1;
-        if (STAGE == 0) return (zh * cye + yh) * cxe + xh;
-        if (STAGE == 1) return (zh * cyo + yh) * cxe + xh;
-        if (STAGE == 2) return (zh * cye + yh) * cxo + xh;
-        if (STAGE == 4) return (zh * cyo + yh) * cxo + xh;
-        // weight 2
-        if (!(z & 1)) return zh * (a2 + a1) + yh * cxo + xh;
+        if (CL == C_W1Z) return (zh * cye + yh) * cxe + xh;
+        if (CL == C_W1Y) return (zh * cyo + yh) * cxe + xh;
+        if (CL == C_W1X) return (zh * cye + yh) * cxo + xh;
+        if (CL == C_W3) return (zh * cyo + yh) * cxo + xh;
+        if (CL == C_W2E) return zh * (a2 + a1) + yh * cxo + xh;
         return (zh + 1) * a2 + zh * a1 + (((uint32_t)y + 1) >> 1) * cxo + yh * cxe + xh;
     }
 };
 
-// A unit being coded: its plane and its axis-0 neighbours (odd planes only;
-// a neighbour outside the lattice aliases the z - 1 plane and is never used).
+struct Item {
+    int c, x0, y0, zs, ze;  // ze: end of the owned planes (clipped to the lattice)
+    int64_t cbase;          // channel offset in the grid
+};
+
+__device__ __forceinline__ Item item_of(const TileLevel& L, uint32_t w, int tx, int ty) {
+    Item it;
+    const uint32_t ix = w % (uint32_t)L.tiles_x;
+    w /= (uint32_t)L.tiles_x;
+    const uint32_t iy = w % (uint32_t)L.tiles_y;
+    w /= (uint32_t)L.tiles_y;
+    const uint32_t ch = w % (uint32_t)L.chunks;
+    it.c = (int)(w / (uint32_t)L.chunks);
+    it.x0 = (int)ix * tx;
+    it.y0 = (int)iy * ty;
+    it.zs = (int)ch * L.zc;
+    it.ze = min(it.zs + L.zc, L.N[0]);
+    it.cbase = (int64_t)it.c * (int64_t)L.points;
+    return it;
+}
+
+// Units of an item: E(zs-2), E(zs), E(zs+2), then (E(z+3), O(z)) per odd z.
+__device__ __forceinline__ int n_units(const Item& it) { return 3 + (it.ze - it.zs) / 2; }
+__device__ __forceinline__ void unit_planes(const Item& it, int u, int& ez, int& oz) {
+    if (u < 3) {
+        ez = it.zs - 2 + 2 * u;
+        oz = -1;
+    } else {
+        ez = it.zs + 4 + 2 * (u - 3);
+        oz = it.zs + 1 + 2 * (u - 3);
+    }
+}
+
+// Slots: even plane z in slot (z/2) mod 4, odd plane z in 4 + (z/2) mod 2.
+template <typename T>
+__device__ __forceinline__ T* slot_of(T* slots, int z) {
+    const int k = (z & 1) ? 4 + ((z >> 1) & 1) : ((z >> 1) & 3);
+    return slots + k * G<T>::SLOT;
+}
+
 template <typename T>
 struct Unit {
-    T* P;
-    const T* zm3;
-    const T* zm1;
-    const T* zp1;
-    const T* zp3;
-    int z;
-    bool owned;
-};
-
-struct Item {
-    int c, x0, y0, zs, ze;
-    int64_t cbase;  // channel offset in the grid
+    T* E;             // slot of the even plane (valid when ev)
+    T* O;             // slot of the odd plane (valid when ov)
+    const T* zt[4];   // odd plane's axis-0 taps: even planes z-1, z+1, z-3, z+3
+    uint32_t zok;     // bit 0: z+1 valid, bit 1: z-3 valid, bit 2: z+3 valid
+    int ez, oz;
+    bool ev, ov;      // planes inside the lattice (computed)
+    bool eown, oown;  // planes owned by the item
 };
 
 template <typename T>
-__device__ __forceinline__ AxisTaps<T> mk_taps(T m1, T p1, T m3, T p3, int c, int n) {
+__device__ __forceinline__ Unit<T> make_unit(T* slots, const Item& it, int u, int nz) {
+    Unit<T> U;
+    unit_planes(it, u, U.ez, U.oz);
+    U.ev = U.ez >= 0 && U.ez < nz;
+    U.ov = U.oz >= 0 && U.oz < nz;
+    U.eown = U.ev && U.ez >= it.zs && U.ez < it.ze;
+    U.oown = U.ov && U.oz >= it.zs && U.oz < it.ze;
+    U.E = slot_of(slots, U.ez < 0 ? 0 : U.ez);
+    U.O = slot_of(slots, U.oz < 0 ? 1 : U.oz);
+    const int z = U.oz < 0 ? 1 : U.oz;
+    const T* m1 = slot_of(slots, z - 1);
+    U.zt[0] = m1;
+    U.zt[1] = z + 1 < nz ? slot_of(slots, z + 1) : m1;
+    U.zt[2] = z - 3 >= 0 ? slot_of(slots, z - 3) : m1;
+    U.zt[3] = z + 3 < nz ? slot_of(slots, z + 3) : m1;
+    U.zok = (z + 1 < nz ? 1u : 0u) | (z - 3 >= 0 ? 2u : 0u) | (z + 3 < nz ? 4u : 0u);
+    return U;
+}
+
+// Tap validity of an odd lattice coordinate c on an axis of n points.
+__device__ __forceinline__ uint32_t tap_ok(int c, int n) {
+    return (c + 1 < n ? 1u : 0u) | (c >= 3 ? 2u : 0u) | (c + 3 < n ? 4u : 0u);
+}
+
+template <typename T>
+__device__ __forceinline__ AxisTaps<T> taps4(T m1, T p1, T m3, T p3, uint32_t ok) {
     AxisTaps<T> t;
     t.m1 = m1;
     t.p1 = p1;
     t.m3 = m3;
     t.p3 = p3;
-    t.ok = (c + 1 < n ? 1u : 0u) | (c >= 3 ? 2u : 0u) | (c + 3 < n ? 4u : 0u);
+    t.ok = ok;
     return t;
 }
 
-// Prediction of a point whose odd axes are (ZO, YO, XO): predict_point's rule
-// (center 0 averages the odd axes in axis order; 1 / 2 take the first / last).
-template <typename T, int CUBIC, int ZO, int YO, int XO>
-__device__ __forceinline__ double predict_tile(const QParams& q, const Unit<T>& u, int pos, int y,
-                                               int x, const int32_t* N) {
-    using B = Box<T>;
-    constexpr int CNT = ZO + YO + XO;
-    const int em = q.end_mode;
-    auto vz = [&]() {
-        return axis_combine<T, CUBIC>(mk_taps(u.zm1[pos], u.zp1[pos], u.zm3[pos], u.zp3[pos], u.z,
-                                              N[0]),
-                                      em);
-    };
-    auto vy = [&]() {
-        const T* p = u.P + pos;
-        return axis_combine<T, CUBIC>(mk_taps(p[-B::BX], p[B::BX], p[-3 * B::BX], p[3 * B::BX], y,
-                                              N[1]),
-                                      em);
-    };
-    auto vx = [&]() {
-        const T* p = u.P + pos;
-        return axis_combine<T, CUBIC>(mk_taps(p[-1], p[1], p[-3], p[3], x, N[2]), em);
-    };
-    if (CNT == 1) return ZO ? vz() : (YO ? vy() : vx());
-    if (q.center == 1) return ZO ? vz() : vy();
-    if (q.center == 2) return XO ? vx() : vy();
-    if (CNT == 2) {
-        const double a = ZO ? vz() : vy();
-        const double b = XO ? vx() : vy();
-        return __dadd_rn(a, b) * 0.5;
-    }
-    const double t = __dadd_rn(__dadd_rn(vz(), vy()), vx());
-    return __ddiv_rn(t, 3.0);
-}
-
-// Point e of a region (rows R0 + 2i, columns B0 + 2j): box position and
-// lattice coordinates; inactive points (past the region or outside the
-// lattice) take the region's first position, whose taps are in the box.
-template <typename T, int R0, int NR, int B0, int NC>
-struct RegionPoint {
-    int pos, y, x, r, b;
-    bool act;
-    __device__ __forceinline__ RegionPoint(int e, const Item& it, const int32_t* N) {
-        const int i = e / NC, j = e - (e / NC) * NC;
-        r = R0 + 2 * i;
-        b = B0 + 2 * j;
-        y = it.y0 - 3 + r;
-        x = it.x0 - 4 + b;
-        act = e < NR * NC && y >= 0 && y < N[1] && x >= 0 && x < N[2];
-        if (!act) {
-            r = R0;
-            b = B0;
-        }
-        pos = r * Box<T>::BX + b;
-    }
+// A point of a class region: its sub-array position and lattice coordinates.
+// Lanes past the region take its last point and must not store anything.
+struct Pt {
+    int row, col, y, x, idx;
+    bool valid;
 };
 
-// ------------------------------------------------------------------ encode
+template <typename T, int CL>
+__device__ __forceinline__ Pt point_of(int task, const Item& it) {
+    using C = Cl<T, CL>;
+    Pt p;
+    int e = task * 32 + (int)(threadIdx.x & 31);
+    p.valid = e < C::NPTS;
+    if (!p.valid) e = C::NPTS - 1;
+    const int r = e / C::NC;
+    p.row = r;
+    p.col = C::C0 + (e - r * C::NC);
+    p.y = C::YO ? it.y0 + 1 + 2 * p.row : it.y0 - 2 + 2 * p.row;
+    p.x = C::XO ? it.x0 - 3 + 2 * p.col : it.x0 - 4 + 2 * p.col;
+    p.idx = p.row * G<T>::P + p.col;
+    return p;
+}
+
+// Prediction of a point of class CL: predict_point's rule (center 0 averages
+// the odd axes in axis order; 1 / 2 take the first / last odd axis).
+template <typename T, int CUBIC, int CL>
+__device__ __forceinline__ double predict(const QParams& q, const Unit<T>& u, const Pt& p,
+                                          const int32_t* N) {
+    using C = Cl<T, CL>;
+    using Gm = G<T>;
+    constexpr int CNT = C::ZO + C::YO + C::XO;
+    const int em = q.end_mode;
+    const T* plane = C::ZO ? u.O : u.E;
+    auto vz = [&]() {
+        const int o = C::SUB + p.idx;
+        return axis_combine<T, CUBIC>(taps4(u.zt[0][o], u.zt[1][o], u.zt[2][o], u.zt[3][o], u.zok),
+                                      em);
+    };
+    auto vy = [&]() {  // even rows row .. row + 3 are y - 3, y - 1, y + 1, y + 3
+        const T* s = plane + (C::XO ? Gm::EO : Gm::EE) + p.idx;
+        return axis_combine<T, CUBIC>(
+            taps4(s[Gm::P], s[2 * Gm::P], s[0], s[3 * Gm::P], tap_ok(p.y, N[1])), em);
+    };
+    auto vx = [&]() {  // E-cols col - 1 .. col + 2 are x - 3, x - 1, x + 1, x + 3
+        const T* s = plane + (C::YO ? Gm::OE : Gm::EE) + p.idx;
+        return axis_combine<T, CUBIC>(taps4(s[0], s[1], s[-1], s[2], tap_ok(p.x, N[2])), em);
+    };
+    if constexpr (CNT == 1) {
+        if constexpr (C::ZO == 1) return vz();
+        else if constexpr (C::YO == 1) return vy();
+        else return vx();
+    } else {
+        if (q.center == 1) {  // the first odd axis
+            if constexpr (C::ZO == 1) return vz();
+            else return vy();
+        }
+        if (q.center == 2) {  // the last odd axis
+            if constexpr (C::XO == 1) return vx();
+            else return vy();
+        }
+        if constexpr (CNT == 2) {
+            double a, b;
+            if constexpr (C::ZO == 1) a = vz();
+            else a = vy();
+            if constexpr (C::XO == 1) b = vx();
+            else b = vy();
+            return __dadd_rn(a, b) * 0.5;
+        } else {
+            const double t = __dadd_rn(__dadd_rn(vz(), vy()), vx());
+            return __ddiv_rn(t, 3.0);
+        }
+    }
+}
+
+template <typename T, int CL>
+__device__ __forceinline__ bool owned_pos(const Pt& p) {
+    using C = Cl<T, CL>;
+    using Gm = G<T>;
+    return (C::YO || (p.row >= 1 && p.row <= Gm::TY / 2)) &&
+           (C::XO || (p.col >= 2 && p.col <= Gm::TX / 2 + 1));
+}
+
+// ------------------------------------------------------------ encode state
 template <typename T>
 struct TAcc {
     double s[4];  // pred |e|, pred e^2, recon |e|, recon e^2
     T mx;         // recon max |e|
     uint32_t maxq, nout;
+    int stage;    // stage these sums belong to (-1: none)
     __device__ void zero() {
         s[0] = s[1] = s[2] = s[3] = 0.0;
         mx = (T)0;
@@ -217,17 +394,17 @@ struct EncSm {
     uint32_t* wno;   // [warp][stage]
 };
 
-// Warp maximum of a non-negative value (its bit pattern orders like it).
-__device__ __forceinline__ double warp_max_val(float v) {
+__device__ __forceinline__ double wmax_val(float v) {
     return (double)__uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(v)));
 }
-__device__ __forceinline__ double warp_max_val(double v) { return warp_max(v); }
+__device__ __forceinline__ double wmax_val(double v) { return warp_max(v); }
 
-// Warp sums of the four statistics as a reduce-scatter butterfly (12 shuffles
-// instead of 40): lane 8k ends with sum k. The order of the additions is
-// fixed, so the sums are deterministic.
+// Add the warp's sums to its statistics slot of stage a.stage, as a
+// reduce-scatter butterfly (lane 8k ends with sum k). Fixed order of the
+// additions: deterministic.
 template <typename T>
-__device__ __forceinline__ void warp_flush(TAcc<T>& a, const EncSm& sm, int stage) {
+__device__ __forceinline__ void warp_flush(TAcc<T>& a, const EncSm& sm) {
+    if (a.stage < 0) return;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const bool h16 = lane & 16, h8 = lane & 8;
     double k0 = h16 ? a.s[2] : a.s[0], k1 = h16 ? a.s[3] : a.s[1];
@@ -238,350 +415,482 @@ __device__ __forceinline__ void warp_flush(TAcc<T>& a, const EncSm& sm, int stag
     k = __dadd_rn(k, __shfl_xor_sync(0xffffffffu, h8 ? k0 : k1, 8));
 #pragma unroll
     for (int o = 4; o; o >>= 1) k = __dadd_rn(k, __shfl_xor_sync(0xffffffffu, k, o));
-    const double mx = warp_max_val(a.mx);
+    const double mx = wmax_val(a.mx);
     const uint32_t mq = __reduce_max_sync(0xffffffffu, a.maxq);
     const uint32_t no = __reduce_add_sync(0xffffffffu, a.nout);
-    double* slot = sm.wacc + (w * TILE_STAGES + stage) * 5;
+    double* slot = sm.wacc + (w * TILE_STAGES + a.stage) * 5;
     if ((lane & 7) == 0) slot[(h16 ? 2 : 0) + (h8 ? 1 : 0)] += k;
     if (lane == 1) {
         slot[4] = fmax(slot[4], mx);
-        uint32_t& m = sm.wmq[w * TILE_STAGES + stage];
+        uint32_t& m = sm.wmq[w * TILE_STAGES + a.stage];
         m = max(m, mq);
-        sm.wno[w * TILE_STAGES + stage] += no;
+        sm.wno[w * TILE_STAGES + a.stage] += no;
     }
     a.zero();
 }
 
-// One class region of a unit, two points in flight per thread.
-template <typename T, int CUBIC, int ZO, int YO, int XO, int STAGE, int R0, int NR, int B0, int NC>
-__device__ __forceinline__ void enc_region(const TileLevel& L, const Ranks& rk, const Unit<T>& u,
-                                           const Item& it, const EncSm& sm, uint32_t cur_seg,
-                                           TAcc<T>& a) {
-    using B = Box<T>;
-    using RP = RegionPoint<T, R0, NR, B0, NC>;
-    const TileStage& S = L.st[STAGE];
+template <typename T, int CUBIC, int CL>
+__device__ __forceinline__ void enc_task(const TileLevel& L, const LvRanks& rk, const Item& it,
+                                         const Unit<T>& u, int task, const EncSm& sm,
+                                         const uint32_t* cseg, TAcc<T>& a) {
+    using C = Cl<T, CL>;
+    if (a.stage != C::STAGE) {  // uniform across the warp
+        warp_flush(a, sm);
+        a.stage = C::STAGE;
+    }
+    const Pt p = point_of<T, CL>(task, it);
+    T* P = (C::ZO ? u.O : u.E) + C::SUB;
+    const TileStage& S = L.st[C::STAGE];
     const QParams& q = S.q;
-    constexpr int NPTS = NR * NC;
-    const int lane = threadIdx.x & 31;
-    T* staging = (T*)S.staging;
-    for (int e0 = 0; e0 < NPTS; e0 += 2 * THREADS) {
-        const RP p0(e0 + threadIdx.x, it, L.N), p1(e0 + THREADS + threadIdx.x, it, L.N);
-        const T x0 = u.P[p0.pos], x1 = u.P[p1.pos];
-        const double d0 = predict_tile<T, CUBIC, ZO, YO, XO>(q, u, p0.pos, p0.y, p0.x, L.N);
-        const double d1 = predict_tile<T, CUBIC, ZO, YO, XO>(q, u, p1.pos, p1.y, p1.x, L.N);
-        T r0, r1;
-        const QOut o0 = Quant<T>::run(x0, d0, q, r0);
-        const QOut o1 = Quant<T>::run(x1, d1, q, r1);
-        if (p0.act) u.P[p0.pos] = r0;
-        if (p1.act) u.P[p1.pos] = r1;
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const RP& p = h ? p1 : p0;
-            const QOut& o = h ? o1 : o0;
-            const T xv = h ? x1 : x0, rv = h ? r1 : r0;
-            const double pd = h ? d1 : d0;
-            int key = -1;
-            if (u.owned && p.act && p.r >= 3 && p.r < 3 + B::TY && p.b >= 4 && p.b < 4 + B::TX) {
-                const uint64_t gi = (uint64_t)it.c * S.n + rk.of<STAGE>(u.z, p.y, p.x);
-                S.codes[gi] = (uint16_t)o.code;
-                if (!o.code) {
-                    staging[gi] = xv;
-                    atomicAdd(&S.tile_cnt[gi / TILE], 1u);
-                    a.nout++;
-                    key = 0;
-                } else {
-                    const uint32_t aq = (uint32_t)abs(o.qv);
-                    a.maxq = max(a.maxq, aq);
-                    key = aq < HWIN ? o.qv + HWIN : -2;
-                }
-                const uint32_t seg = (uint32_t)(gi >> SEG_SHIFT);
-                if (key >= 0 && seg != cur_seg) {  // another segment: straight to global
-                    atomicAdd(&S.hist_seg[(size_t)seg * HBINS + key], 1u);
-                    key = -1;
-                }
-                const double er = Quant<T>::err(xv, pd);
-                a.s[0] += fabs(er);
-                a.s[1] += er * er;
-                const double re = Quant<T>::rerr(xv, rv);
-                a.s[2] += re;
-                a.s[3] += re * re;
-                a.mx = max(a.mx, (T)re);
-            }
-            if (u.owned) hist_warp(sm.hist + STAGE * HBINS, S.hist_total, key, o.code, lane);
-        }
-    }
-}
-
-__device__ __forceinline__ int even_slot(int z) { return (z >> 1) % 5; }
-
-// Issue the cp.async loads of unit plane z (even planes take their coarse
-// points from the canvas, every other point from src). vec: 16-byte groups
-// (rows 16-byte aligned, unit lattice step along axis 2); even planes then
-// stage the canvas rows of even y in `stage` for even_fixup.
-template <typename T>
-__device__ __forceinline__ void load_plane(const TileLevel& L, const Item& it, int z, bool even,
-                                           T* dst, T* stage, const T* __restrict__ src,
-                                           const T* __restrict__ canvas, bool vec) {
-    using B = Box<T>;
-    const int64_t zoff = it.cbase + (int64_t)z * L.ls[0];
-    if (vec) {
-        for (int e = threadIdx.x; e < B::BY * B::GROW; e += THREADS) {
-            const int r = e / B::GROW, g = e - (e / B::GROW) * B::GROW;
-            const int y = it.y0 - 3 + r, x = it.x0 - 4 + g * B::VEC;
-            const bool in = y >= 0 && y < L.N[1] && x >= 0 && x < L.N[2];
-            const int64_t off = in ? zoff + (int64_t)y * L.ls[1] + x : 0;
-            cp_async16(dst + r * B::BX + g * B::VEC, src + off, in ? 16u : 0u);
-            if (even && !(y & 1))
-                cp_async16(stage + r * B::BX + g * B::VEC, canvas + off, in ? 16u : 0u);
-        }
-        return;
-    }
-    for (int e = threadIdx.x; e < B::ELEMS; e += THREADS) {
-        const int r = e / B::BX, b = e - (e / B::BX) * B::BX;
-        const int y = it.y0 - 3 + r, x = it.x0 - 4 + b;
-        T* d = dst + r * B::BX + b;
-        if (y >= 0 && y < L.N[1] && x >= 0 && x < L.N[2]) {
-            const bool coarse = even && !(y & 1) && !(x & 1);
-            const int64_t g = zoff + (int64_t)y * L.ls[1] + (int64_t)x * L.ls[2];
-            cp_async<sizeof(T)>(d, (coarse ? canvas : src) + g);
+    const T xv = P[p.idx];
+    const double pd = predict<T, CUBIC, CL>(q, u, p, L.N);
+    T rv;
+    const QOut o = Quant<T>::run(xv, pd, q, rv);
+    if (p.valid) P[p.idx] = rv;
+    const bool owned = p.valid && (C::ZO ? u.oown : u.eown) && p.y < L.N[1] && p.x < L.N[2] &&
+                       owned_pos<T, CL>(p);
+    int key = -1;
+    if (owned) {
+        const int z = C::ZO ? u.oz : u.ez;
+        const uint64_t gi = (uint64_t)it.c * S.n + rk.template of<CL>(z, p.y, p.x);
+        S.codes[gi] = (uint16_t)o.code;
+        if (!o.code) {
+            ((T*)S.staging)[gi] = xv;
+            atomicAdd(&S.tile_cnt[gi / TILE], 1u);
+            a.nout++;
+            key = 0;
         } else {
-            *d = (T)0;
+            const uint32_t aq = (uint32_t)abs(o.qv);
+            a.maxq = max(a.maxq, aq);
+            key = aq < HWIN ? o.qv + HWIN : -2;
+        }
+        const uint32_t seg = (uint32_t)(gi >> SEG_SHIFT);
+        if (key >= 0 && seg != cseg[C::STAGE]) {  // another segment: straight to global
+            atomicAdd(&S.hist_seg[(size_t)seg * HBINS + key], 1u);
+            key = -1;
+        }
+        const double er = Quant<T>::err(xv, pd);
+        a.s[0] += fabs(er);
+        a.s[1] = __fma_rn(er, er, a.s[1]);
+        const double re = Quant<T>::rerr(xv, rv);
+        a.s[2] += re;
+        a.s[3] = __fma_rn(re, re, a.s[3]);
+        a.mx = max(a.mx, (T)re);
+    }
+    hist_warp(sm.hist + C::STAGE * HBINS, S.hist_total, key, o.code, threadIdx.x & 31);
+}
+
+// One phase of up to three classes: warp w takes a contiguous range of the
+// phase's tasks (static: the statistics' summation order is fixed).
+template <typename T, int CUBIC, int CA, int CB, int CC>
+__device__ __forceinline__ void enc_phase(const TileLevel& L, const LvRanks& rk, const Item& it,
+                                          const Unit<T>& u, bool ea, bool eb, bool ec,
+                                          const EncSm& sm, const uint32_t* cseg, TAcc<T>& a) {
+    const int na = ea ? ntasks<T, CA>() : 0, nb = eb ? ntasks<T, CB>() : 0;
+    const int nc = ec ? ntasks<T, CC>() : 0;
+    const int tot = na + nb + nc, w = threadIdx.x >> 5;
+    const int tb = w * tot / LW, te = (w + 1) * tot / LW;
+    for (int t = tb; t < te; t++) {
+        if (t < na) {
+            if constexpr (CA != C_NONE) enc_task<T, CUBIC, CA>(L, rk, it, u, t, sm, cseg, a);
+        } else if (t < na + nb) {
+            if constexpr (CB != C_NONE) enc_task<T, CUBIC, CB>(L, rk, it, u, t - na, sm, cseg, a);
+        } else {
+            if constexpr (CC != C_NONE)
+                enc_task<T, CUBIC, CC>(L, rk, it, u, t - na - nb, sm, cseg, a);
         }
     }
 }
 
-// Even plane, 16-byte path: the coarse points (even y, even x) from the staged
-// canvas rows. Even x sits at offsets 0 and 2 of each 16-byte group of floats
-// (offset 0 of doubles).
+// ------------------------------------------------------------ decode tasks
+template <typename T, int CL>
+__device__ __forceinline__ uint32_t code_of(const TileLevel& L, const LvRanks& rk, const Item& it,
+                                            const Unit<T>& u, int task) {
+    using C = Cl<T, CL>;
+    const Pt p = point_of<T, CL>(task, it);
+    if (!p.valid || p.y < 0 || p.x < 0 || p.y >= L.N[1] || p.x >= L.N[2]) return 0u;
+    const TileStage& S = L.st[C::STAGE];
+    const int z = C::ZO ? u.oz : u.ez;
+    return __ldg(S.codes + (uint64_t)it.c * S.n + rk.template of<CL>(z, p.y, p.x));
+}
+
+template <typename T, int CUBIC, int CL>
+__device__ __forceinline__ void dec_task(const TileLevel& L, const Item& it, const Unit<T>& u,
+                                         int task, uint32_t code) {
+    using C = Cl<T, CL>;
+    if (code == 0) return;  // outlier (already in the canvas box) or outside the lattice
+    const Pt p = point_of<T, CL>(task, it);
+    T* P = (C::ZO ? u.O : u.E) + C::SUB;
+    const QParams& q = L.st[C::STAGE].q;
+    const double pd = predict<T, CUBIC, CL>(q, u, p, L.N);
+    P[p.idx] = dequant_value<T>(q, pd, code);
+}
+
+// The task counts of phase ph (0, 1, 2) of a unit, per class.
 template <typename T>
-__device__ __forceinline__ void even_fixup(T* dst, const T* stage) {
-    using B = Box<T>;
-    for (int e = threadIdx.x; e < (B::BY / 2) * B::GROW; e += THREADS) {
-        const int r = 1 + 2 * (e / B::GROW), g = e - (e / B::GROW) * B::GROW;
-        T* d = dst + r * B::BX + g * B::VEC;
-        const T* s = stage + r * B::BX + g * B::VEC;
-        d[0] = s[0];
-        if (B::VEC == 4) d[2] = s[2];
+__device__ __forceinline__ void phase_counts(int ph, bool ev, bool ov, int& na, int& nb, int& nc) {
+    if (ph == 0) {
+        na = ev ? ntasks<T, C_W1Y>() : 0;
+        nb = ev ? ntasks<T, C_W1X>() : 0;
+        nc = ov ? ntasks<T, C_W1Z>() : 0;
+    } else if (ph == 1) {
+        na = ev ? ntasks<T, C_W2E>() : 0;
+        nb = ov ? ntasks<T, C_W2ZY>() : 0;
+        nc = ov ? ntasks<T, C_W2ZX>() : 0;
+    } else {
+        na = ov ? ntasks<T, C_W3>() : 0;
+        nb = nc = 0;
     }
 }
 
-// Write an owned plane's tile to the canvas (16-byte groups on the vec path;
-// the coarse points of even planes are written back unchanged there).
+// Codes of the warp's tasks of phase ph of unit u into registers.
 template <typename T>
-__device__ __forceinline__ void store_plane(const TileLevel& L, const Item& it, int z, bool even,
-                                            const T* P, T* __restrict__ canvas, bool vec) {
-    using B = Box<T>;
-    const int64_t zoff = it.cbase + (int64_t)z * L.ls[0];
-    if (vec) {
-        constexpr int G = B::TX / B::VEC;
-        for (int e = threadIdx.x; e < B::TY * G; e += THREADS) {
-            const int rr = e / G, g = e - (e / G) * G;
-            const int y = it.y0 + rr, x = it.x0 + g * B::VEC;
-            if (y < L.N[1] && x < L.N[2])
-                *(int4*)(canvas + zoff + (int64_t)y * L.ls[1] + x) =
-                    *(const int4*)(P + (rr + 3) * B::BX + 4 + g * B::VEC);
+__device__ __forceinline__ void fetch_phase(const TileLevel& L, const LvRanks& rk, const Item& it,
+                                            const Unit<T>& u, int ph, uint32_t* pf) {
+    int na, nb, nc;
+    phase_counts<T>(ph, u.ev, u.ov, na, nb, nc);
+    const int tot = na + nb + nc, w = threadIdx.x >> 5;
+    const int tb = w * tot / LW, te = (w + 1) * tot / LW;
+#pragma unroll
+    for (int k = 0; k < MAXT; k++) {
+        const int t = tb + k;
+        uint32_t c = 0;
+        if (t < te) {
+            if (ph == 0) {
+                c = t < na ? code_of<T, C_W1Y>(L, rk, it, u, t)
+                    : t < na + nb ? code_of<T, C_W1X>(L, rk, it, u, t - na)
+                                  : code_of<T, C_W1Z>(L, rk, it, u, t - na - nb);
+            } else if (ph == 1) {
+                c = t < na ? code_of<T, C_W2E>(L, rk, it, u, t)
+                    : t < na + nb ? code_of<T, C_W2ZY>(L, rk, it, u, t - na)
+                                  : code_of<T, C_W2ZX>(L, rk, it, u, t - na - nb);
+            } else {
+                c = code_of<T, C_W3>(L, rk, it, u, t);
+            }
+        }
+        pf[k] = c;
+    }
+}
+
+template <typename T, int CUBIC, int CA, int CB, int CC>
+__device__ __forceinline__ void dec_phase(const TileLevel& L, const Item& it, const Unit<T>& u,
+                                          bool ea, bool eb, bool ec, const uint16_t* wcodes) {
+    const int na = ea ? ntasks<T, CA>() : 0, nb = eb ? ntasks<T, CB>() : 0;
+    const int nc = ec ? ntasks<T, CC>() : 0;
+    const int tot = na + nb + nc, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tb = w * tot / LW, te = (w + 1) * tot / LW;
+    for (int t = tb; t < te; t++) {
+        const uint32_t code = wcodes[(t - tb) * 32 + lane];
+        if (t < na) {
+            if constexpr (CA != C_NONE) dec_task<T, CUBIC, CA>(L, it, u, t, code);
+        } else if (t < na + nb) {
+            if constexpr (CB != C_NONE) dec_task<T, CUBIC, CB>(L, it, u, t - na, code);
+        } else {
+            if constexpr (CC != C_NONE) dec_task<T, CUBIC, CC>(L, it, u, t - na - nb, code);
+        }
+    }
+}
+
+// ------------------------------------------------------------ plane movement
+// Issue the loads of a unit's planes into the staging buffers: the even
+// plane's box (x, or the canvas when decoding) and, when encoding, its coarse
+// even rows from the canvas; the odd plane's box. Returns whether anything was
+// issued (uniform).
+template <typename T, bool ENC, int TMA>
+__device__ __forceinline__ bool issue_loads(const CUtensorMap* tmx, const CUtensorMap* tmr,
+                                            const TileLevel& L, const Item& it, const Unit<T>& u,
+                                            T* XE, T* XO, T* RS, uint32_t bar, const T* src,
+                                            const T* canvas) {
+    using Gm = G<T>;
+    if (!u.ev && !u.ov) return false;
+    if (TMA) {
+        if (threadIdx.x == 0) {
+            constexpr uint32_t XB = Gm::XR * Gm::BX * sizeof(T), RB = Gm::RR * Gm::BX * sizeof(T);
+            const uint32_t bytes = (u.ev ? XB + (ENC ? RB : 0u) : 0u) + (u.ov ? XB : 0u);
+            mbar_expect(bar, bytes);
+            const int cx = it.x0 - 4, cy = it.y0 - 2;
+            if (u.ev) {
+                tma_load4(su32(XE), tmx, cx, cy, u.ez, it.c, bar);
+                if (ENC) tma_load4(su32(RS), tmr, cx, it.y0 / 2 - 1, u.ez, it.c, bar);
+            }
+            if (u.ov) tma_load4(su32(XO), tmx, cx, cy, u.oz, it.c, bar);
+        }
+        return true;
+    }
+    auto box = [&](T* dst, const T* base, int z, int ystep, int rows) {
+        const int64_t zo = it.cbase + (int64_t)z * L.ls[0];
+        for (int e = threadIdx.x; e < rows * Gm::BX; e += LT) {
+            const int r = e / Gm::BX, b = e - (e / Gm::BX) * Gm::BX;
+            const int Y = it.y0 - 2 + r * ystep, X = it.x0 - 4 + b;
+            const bool in = Y >= 0 && Y < L.N[1] && X >= 0 && X < L.N[2];
+            const T* s = in ? base + zo + (int64_t)Y * L.ls[1] + (int64_t)X * L.ls[2] : base;
+            cp_el<sizeof(T)>(dst + e, s, in ? (uint32_t)sizeof(T) : 0u);
+        }
+    };
+    if (u.ev) {
+        box(XE, src, u.ez, 1, Gm::XR);
+        if (ENC) box(RS, canvas, u.ez, 2, Gm::RR);
+    }
+    if (u.ov) box(XO, src, u.oz, 1, Gm::XR);
+    cp_commit();
+    return true;
+}
+
+// Staging (natural layout) -> slot (parity-split layout). For an encoded even
+// plane the coarse points (even y, even x) come from the canvas rows in RS.
+template <typename T>
+__device__ __forceinline__ void transpose_plane(T* slot, const T* SX, const T* SR) {
+    using Gm = G<T>;
+    constexpr int ROWS = Gm::NER + Gm::NOR;
+    for (int e = threadIdx.x; e < ROWS * Gm::GPR; e += LT) {
+        const int i = e / Gm::GPR, g = e - (e / Gm::GPR) * Gm::GPR;
+        const bool even = i < Gm::NER;
+        const int ri = even ? i : i - Gm::NER;
+        const int srow = even ? 2 * ri : 3 + 2 * ri;
+        T* Er = slot + (even ? Gm::EE : Gm::OE) + ri * Gm::P;
+        T* Or = slot + (even ? Gm::EO : Gm::OO) + ri * Gm::P;
+        if constexpr (sizeof(T) == 4) {
+            const float4 v = *(const float4*)(SX + srow * Gm::BX + 4 * g);
+            float2 ev = make_float2(v.x, v.z);
+            if (even && SR) {
+                const float4 r = *(const float4*)(SR + ri * Gm::BX + 4 * g);
+                ev = make_float2(r.x, r.z);
+            }
+            *(float2*)(Er + 2 * g) = ev;
+            *(float2*)(Or + 2 * g) = make_float2(v.y, v.w);
+        } else {
+            const double2 v = *(const double2*)(SX + srow * Gm::BX + 2 * g);
+            Er[g] = (even && SR) ? SR[ri * Gm::BX + 2 * g] : v.x;
+            Or[g] = v.y;
+        }
+    }
+}
+
+// Write the tile of an owned plane from its slot to the canvas (16-byte
+// groups on the TMA path, whose rows are whole groups; else element by
+// element, skipping the coarse points of even planes).
+template <typename T, int TMA>
+__device__ __forceinline__ void store_plane(const TileLevel& L, const Item& it, int z,
+                                            const T* slot, T* __restrict__ canvas) {
+    using Gm = G<T>;
+    const int64_t zo = it.cbase + (int64_t)z * L.ls[0];
+    if (TMA) {
+        constexpr int GT = Gm::TX / Gm::VEC;
+        for (int e = threadIdx.x; e < Gm::TY * GT; e += LT) {
+            const int r = e / GT, g = e - (e / GT) * GT;
+            const int y = it.y0 + r, x = it.x0 + g * Gm::VEC;
+            if (y >= L.N[1] || x >= L.N[2]) continue;
+            const bool ey = !(r & 1);
+            const int ri = ey ? r / 2 + 1 : r / 2;
+            const T* E = slot + (ey ? Gm::EE : Gm::OE) + ri * Gm::P;
+            const T* O = slot + (ey ? Gm::EO : Gm::OO) + ri * Gm::P;
+            T* d = canvas + zo + (int64_t)y * L.ls[1] + x;
+            if constexpr (sizeof(T) == 4) {
+                const float2 a = *(const float2*)(E + 2 + 2 * g), b = *(const float2*)(O + 2 + 2 * g);
+                *(float4*)d = make_float4(a.x, b.x, a.y, b.y);
+            } else {
+                *(double2*)d = make_double2(E[2 + g], O[2 + g]);
+            }
         }
         return;
     }
-    for (int e = threadIdx.x; e < B::TX * B::TY; e += THREADS) {
-        const int rr = e / B::TX, bb = e - (e / B::TX) * B::TX;
-        const int y = it.y0 + rr, x = it.x0 + bb;
-        if (y < L.N[1] && x < L.N[2] && !(even && !(y & 1) && !(x & 1)))
-            canvas[zoff + (int64_t)y * L.ls[1] + (int64_t)x * L.ls[2]] =
-                P[(rr + 3) * B::BX + bb + 4];
+    const bool evenz = !(z & 1);
+    for (int e = threadIdx.x; e < Gm::TY * Gm::TX; e += LT) {
+        const int r = e / Gm::TX, b = e - (e / Gm::TX) * Gm::TX;
+        const int y = it.y0 + r, x = it.x0 + b;
+        if (y >= L.N[1] || x >= L.N[2]) continue;
+        const bool ey = !(r & 1), ex = !(b & 1);
+        if (evenz && ey && ex) continue;  // coarse point: unchanged
+        const int ri = ey ? r / 2 + 1 : r / 2;
+        const int sub = ey ? (ex ? Gm::EE : Gm::EO) : (ex ? Gm::OE : Gm::OO);
+        canvas[zo + (int64_t)y * L.ls[1] + (int64_t)x * L.ls[2]] =
+            slot[sub + ri * Gm::P + 2 + b / 2];
     }
 }
 
-// Unit k of a chunk: E(zs - 2), E(zs), E(zs + 2), then E(z + 3), O(z) for
-// z = zs + 1, zs + 3, ...
-__device__ __forceinline__ int unit_z(int k, int zs, bool& even) {
-    if (k < 3) {
-        even = true;
-        return zs - 2 + 2 * k;
+// The histogram segment of stage s's first owned point in unit u (for
+// flushing the shared bins when the segment changes). 0xffffffff: the stage
+// has no owned point in the unit.
+template <typename T>
+__device__ __forceinline__ uint32_t unit_seg(const TileLevel& L, const LvRanks& rk,
+                                             const Item& it, const Unit<T>& u, int s) {
+    uint32_t r;
+    const int y0 = it.y0, x0 = it.x0;
+    // the stage's first point in the tile must lie in the lattice
+    const int fy = y0 + ((s == 1 || s == 4 || (s == 3 && u.eown)) ? 1 : 0);
+    const int fx = x0 + ((s == 2 || s == 3 || s == 4) ? 1 : 0);
+    if (fy >= L.N[1] || fx >= L.N[2]) return 0xffffffffu;
+    switch (s) {
+        case 0:
+            if (!u.oown) return 0xffffffffu;
+            r = rk.of<C_W1Z>(u.oz, y0, x0);
+            break;
+        case 1:
+            if (!u.eown) return 0xffffffffu;
+            r = rk.of<C_W1Y>(u.ez, y0 + 1, x0);
+            break;
+        case 2:
+            if (!u.eown) return 0xffffffffu;
+            r = rk.of<C_W1X>(u.ez, y0, x0 + 1);
+            break;
+        case 3:
+            if (u.eown) r = rk.of<C_W2E>(u.ez, y0 + 1, x0 + 1);
+            else if (u.oown) r = rk.of<C_W2ZX>(u.oz, y0, x0 + 1);
+            else return 0xffffffffu;
+            break;
+        default:
+            if (!u.oown) return 0xffffffffu;
+            r = rk.of<C_W3>(u.oz, y0 + 1, x0 + 1);
+            break;
     }
-    const int j = (k - 3) >> 1;
-    even = ((k - 3) & 1) == 0;
-    return even ? zs + 4 + 2 * j : zs + 1 + 2 * j;
+    return (uint32_t)(((uint64_t)it.c * L.st[s].n + r) >> SEG_SHIFT);
 }
 
-// Work item w: tiles along axis 2 fastest, then axis 1, chunk, channel.
-template <typename T>
-__device__ __forceinline__ Item item_of(const TileLevel& L, uint32_t w) {
-    Item it;
-    const uint32_t tx = w % (uint32_t)L.tiles_x;
-    w /= (uint32_t)L.tiles_x;
-    const uint32_t ty = w % (uint32_t)L.tiles_y;
-    w /= (uint32_t)L.tiles_y;
-    const uint32_t ch = w % (uint32_t)L.chunks;
-    it.c = (int)(w / (uint32_t)L.chunks);
-    it.x0 = (int)tx * Box<T>::TX;
-    it.y0 = (int)ty * Box<T>::TY;
-    it.zs = (int)ch * L.zc;
-    it.ze = min(it.zs + L.zc, L.N[0]);
-    it.cbase = (int64_t)it.c * (int64_t)L.points;
-    return it;
-}
+// ------------------------------------------------------------ kernels
+// The CTA's units, across its items (item blockIdx.x + k gridDim.x).
+struct Cursor {
+    uint32_t item;
+    int u;
+};
 
-template <typename T>
-__device__ __forceinline__ Unit<T> make_unit(T* planes, int z, bool even, const Item& it,
-                                             int n0) {
-    using B = Box<T>;
-    Unit<T> u;
-    u.z = z;
-    u.owned = z >= it.zs && z < it.ze;
-    u.P = planes + (even ? even_slot(z) : 5) * B::ELEMS;
-    const T* m1 = planes + even_slot(z - 1 >= 0 ? z - 1 : 0) * B::ELEMS;
-    u.zm1 = m1;
-    u.zp1 = z + 1 < n0 ? planes + even_slot(z + 1) * B::ELEMS : m1;
-    u.zm3 = z - 3 >= 0 ? planes + even_slot(z - 3) * B::ELEMS : m1;
-    u.zp3 = z + 3 < n0 ? planes + even_slot(z + 3) * B::ELEMS : m1;
-    return u;
-}
-
-// Units of an item: 3 + 2 x (odd planes in [zs, ze)), zs even.
-__device__ __forceinline__ int n_units_of(const Item& it) {
-    return 3 + 2 * (it.ze > it.zs ? (it.ze - it.zs) / 2 : 0);
-}
-
-// Segment of the histogram that a unit's stage starts in (a hint: points in
-// another segment go straight to global memory).
-template <int STAGE>
-__device__ __forceinline__ uint32_t seg_hint(const TileLevel& L, const Ranks& rk, const Item& it,
-                                             int z, int y, int x) {
-    return (uint32_t)(((uint64_t)it.c * L.st[STAGE].n + rk.of<STAGE>(z, y, x)) >> SEG_SHIFT);
-}
-
-template <typename T, int CUBIC>
-__global__ void __launch_bounds__(THREADS, 2)
-    k_tile_level_enc(const TileLevel L, const T* __restrict__ x, T* __restrict__ recon) {
-    using B = Box<T>;
-    extern __shared__ __align__(16) uint8_t smem[];
-    T* planes = (T*)smem;
-    T* stage = planes + B::SLOTS * B::ELEMS;
-    EncSm sm;
-    sm.hist = (uint32_t*)(stage + B::ELEMS);
-    sm.wacc = (double*)(sm.hist + TILE_STAGES * HBINS);
-    sm.wmq = (uint32_t*)(sm.wacc + (THREADS / 32) * TILE_STAGES * 5);
-    sm.wno = sm.wmq + (THREADS / 32) * TILE_STAGES;
-    for (int i = threadIdx.x; i < TILE_STAGES * HBINS; i += THREADS) sm.hist[i] = 0;
-    for (int i = threadIdx.x; i < (THREADS / 32) * TILE_STAGES * 5; i += THREADS) sm.wacc[i] = 0.0;
-    for (int i = threadIdx.x; i < (THREADS / 32) * TILE_STAGES; i += THREADS)
-        sm.wmq[i] = sm.wno[i] = 0u;
-    __syncthreads();
-    const bool vec = L.vec != 0;
-    Ranks rk;
-    rk.init(L.N);
-    uint32_t cur_seg[TILE_STAGES];
-#pragma unroll
-    for (int s = 0; s < TILE_STAGES; s++) cur_seg[s] = 0xffffffffu;
-    TAcc<T> a;
-    a.zero();
-
-    for (uint32_t w = blockIdx.x; w < L.items; w += gridDim.x) {
-        const Item it = item_of<T>(L, w);
-        const int n_units = n_units_of(it);
-        {
-            bool ev;
-            const int z = unit_z(0, it.zs, ev);
-            if (z >= 0 && z < L.N[0])
-                load_plane<T>(L, it, z, ev, planes + even_slot(z) * B::ELEMS, stage, x, recon,
-                              vec);
-            cp_commit();
-        }
-        for (int k = 0; k < n_units; k++) {
-            bool even;
-            const int z = unit_z(k, it.zs, even);
-            const bool live = z >= 0 && z < L.N[0];
+// Phase 0 of a unit: the previous unit's finished planes out to the canvas,
+// then (once its loads landed) this unit's planes from staging into their
+// slots. Within an item the two touch different slots; the first unit of an
+// item may reuse the slot of the previous item's last plane, so those stores
+// finish first.
+template <typename T, int TMA>
+__device__ __forceinline__ void phase0(const TileLevel& L, const Item& prev, int st_e, int st_o,
+                                       const Unit<T>& u, bool first, bool pending, uint32_t bar,
+                                       uint32_t& parity, bool& wait_failed, T* slots, const T* XE,
+                                       const T* XO, const T* RS, T* canvas) {
+    const bool out = st_e >= 0 || st_o >= 0;
+    if (out && first) {
+        if (st_e >= 0) store_plane<T, TMA>(L, prev, st_e, slot_of(slots, st_e), canvas);
+        if (st_o >= 0) store_plane<T, TMA>(L, prev, st_o, slot_of(slots, st_o), canvas);
+        __syncthreads();
+    }
+    if (pending) {
+        if (TMA) {
+            if (!mbar_wait(bar, parity)) wait_failed = true;
+            parity ^= 1u;
+        } else {
             cp_wait_all();
             __syncthreads();
-            if (live && even && vec) {
-                even_fixup<T>(planes + even_slot(z) * B::ELEMS, stage);
-                __syncthreads();
-            }
-            if (k + 1 < n_units) {  // the next unit's plane, while this one is computed
-                bool ev;
-                const int zn = unit_z(k + 1, it.zs, ev);
-                if (zn >= 0 && zn < L.N[0])
-                    load_plane<T>(L, it, zn, ev, planes + (ev ? even_slot(zn) : 5) * B::ELEMS,
-                                  stage, x, recon, vec);
-            }
-            cp_commit();
-            if (!live) continue;
-            const Unit<T> u = make_unit<T>(planes, z, even, it, L.N[0]);
-            if (u.owned) {  // histogram segments of this plane's stages (uniform)
-                uint32_t ns[3];
-                int st[3];
-                if (even) {
-                    st[0] = 1, st[1] = 2, st[2] = 3;
-                    ns[0] = seg_hint<1>(L, rk, it, z, it.y0 + 1, it.x0);
-                    ns[1] = seg_hint<2>(L, rk, it, z, it.y0, it.x0 + 1);
-                    ns[2] = seg_hint<3>(L, rk, it, z, it.y0 + 1, it.x0 + 1);
-                } else {
-                    st[0] = 0, st[1] = 3, st[2] = 4;
-                    ns[0] = seg_hint<0>(L, rk, it, z, it.y0, it.x0);
-                    ns[1] = seg_hint<3>(L, rk, it, z, it.y0, it.x0 + 1);
-                    ns[2] = seg_hint<4>(L, rk, it, z, it.y0 + 1, it.x0 + 1);
-                }
-                bool flushed = false;
-#pragma unroll
-                for (int j = 0; j < 3; j++) {
-                    uint32_t& cs = cur_seg[st[j]];
-                    if (ns[j] != cs) {
-                        if (cs != 0xffffffffu)
-                            flush_hist(sm.hist + st[j] * HBINS, L.st[st[j]].hist_seg, cs);
-                        cs = ns[j];
-                        flushed = true;
-                    }
-                }
-                if (flushed) __syncthreads();
-            }
-            if (even) {
-                // weight 1 along axis 2 (even y over the halo rows, odd x) and
-                // along axis 1 (odd y, even x over the halo columns)
-                enc_region<T, CUBIC, 0, 0, 1, 2, B::HR_R0, B::HR_N, B::TC_B0, B::TC_N>(
-                    L, rk, u, it, sm, cur_seg[2], a);
-                if (u.owned) warp_flush(a, sm, 2);
-                enc_region<T, CUBIC, 0, 1, 0, 1, B::TR_R0, B::TR_N, B::HC_B0, B::HC_N>(
-                    L, rk, u, it, sm, cur_seg[1], a);
-                if (u.owned) warp_flush(a, sm, 1);
-                __syncthreads();
-                enc_region<T, CUBIC, 0, 1, 1, 3, B::TR_R0, B::TR_N, B::TC_B0, B::TC_N>(
-                    L, rk, u, it, sm, cur_seg[3], a);
-                if (u.owned) warp_flush(a, sm, 3);
-            } else {
-                enc_region<T, CUBIC, 1, 0, 0, 0, B::HR_R0, B::HR_N, B::HC_B0, B::HC_N>(
-                    L, rk, u, it, sm, cur_seg[0], a);
-                if (u.owned) warp_flush(a, sm, 0);
-                __syncthreads();
-                enc_region<T, CUBIC, 1, 0, 1, 3, B::HR_R0, B::HR_N, B::TC_B0, B::TC_N>(
-                    L, rk, u, it, sm, cur_seg[3], a);
-                enc_region<T, CUBIC, 1, 1, 0, 3, B::TR_R0, B::TR_N, B::HC_B0, B::HC_N>(
-                    L, rk, u, it, sm, cur_seg[3], a);
-                if (u.owned) warp_flush(a, sm, 3);
-                __syncthreads();
-                enc_region<T, CUBIC, 1, 1, 1, 4, B::TR_R0, B::TR_N, B::TC_B0, B::TC_N>(
-                    L, rk, u, it, sm, cur_seg[4], a);
-                if (u.owned) warp_flush(a, sm, 4);
-            }
-            __syncthreads();
-            if (u.owned) store_plane<T>(L, it, z, even, u.P, recon, vec);
         }
-        cp_wait_all();
+    }
+    if (u.ev) transpose_plane<T>(u.E, XE, RS);
+    if (u.ov) transpose_plane<T>(u.O, XO, nullptr);
+    if (out && !first) {
+        if (st_e >= 0) store_plane<T, TMA>(L, prev, st_e, slot_of(slots, st_e), canvas);
+        if (st_o >= 0) store_plane<T, TMA>(L, prev, st_o, slot_of(slots, st_o), canvas);
+    }
+}
+
+template <typename T, int CUBIC, int TMA>
+__global__ void __launch_bounds__(LT, 2)
+    k_lvl_enc(const __grid_constant__ CUtensorMap tmx, const __grid_constant__ CUtensorMap tmr,
+              const TileLevel L, const T* __restrict__ x, T* __restrict__ recon) {
+    using Gm = G<T>;
+    using Ly = Lay<T, true>;
+    extern __shared__ __align__(128) uint8_t smem[];
+    T* slots = (T*)(smem + Ly::SLOTS);
+    T* XE = (T*)(smem + Ly::XE);
+    T* XO = (T*)(smem + Ly::XO);
+    T* RS = (T*)(smem + Ly::RS);
+    EncSm sm;
+    sm.hist = (uint32_t*)(smem + Ly::HIST);
+    sm.wacc = (double*)(smem + Ly::WACC);
+    sm.wmq = (uint32_t*)(smem + Ly::WMQ);
+    sm.wno = (uint32_t*)(smem + Ly::WNO);
+    const uint32_t bar = su32(smem + Ly::MBAR);
+    for (int i = threadIdx.x; i < TILE_STAGES * HBINS; i += LT) sm.hist[i] = 0;
+    for (int i = threadIdx.x; i < LW * TILE_STAGES * 5; i += LT) sm.wacc[i] = 0.0;
+    for (int i = threadIdx.x; i < LW * TILE_STAGES; i += LT) sm.wmq[i] = sm.wno[i] = 0u;
+    if (threadIdx.x == 0) mbar_init(bar);
+    __syncthreads();
+    LvRanks rk;
+    rk.init(L.N);
+    uint32_t cseg[TILE_STAGES];
+#pragma unroll
+    for (int s = 0; s < TILE_STAGES; s++) cseg[s] = 0xffffffffu;
+    TAcc<T> a;
+    a.zero();
+    a.stage = -1;
+    uint32_t parity = 0;
+    bool wait_failed = false;
+
+    const int nz = L.N[0];
+    Cursor cur{blockIdx.x, 0};
+    Item it{}, prev{};
+    int st_e = -1, st_o = -1;  // planes of the previous unit still to store
+    bool pending = false;
+    if (cur.item < L.items) {
+        it = item_of(L, cur.item, Gm::TX, Gm::TY);
+        pending = issue_loads<T, true, TMA>(&tmx, &tmr, L, it, make_unit(slots, it, 0, nz), XE, XO,
+                                            RS, bar, x, recon);
+    }
+    while (cur.item < L.items) {
+        const Unit<T> u = make_unit(slots, it, cur.u, nz);
+        phase0<T, TMA>(L, prev, st_e, st_o, u, cur.u == 0, pending, bar, parity, wait_failed,
+                       slots, XE, XO, RS, recon);
+        // histogram segments of this unit's stages (uniform decisions)
+#pragma unroll
+        for (int s = 0; s < TILE_STAGES; s++) {
+            const uint32_t ns = unit_seg(L, rk, it, u, s);
+            if (ns != 0xffffffffu && ns != cseg[s]) {
+                if (cseg[s] != 0xffffffffu)
+                    flush_hist(sm.hist + s * HBINS, L.st[s].hist_seg, cseg[s]);
+                cseg[s] = ns;
+            }
+        }
         __syncthreads();
+        // the next unit's loads (the staging buffers are free again)
+        Cursor nxt = cur;
+        if (++nxt.u >= n_units(it)) {
+            nxt.item += gridDim.x;
+            nxt.u = 0;
+        }
+        Item nit = it;
+        pending = false;
+        if (nxt.item < L.items) {
+            if (nxt.item != cur.item) nit = item_of(L, nxt.item, Gm::TX, Gm::TY);
+            pending = issue_loads<T, true, TMA>(&tmx, &tmr, L, nit, make_unit(slots, nit, nxt.u, nz),
+                                                XE, XO, RS, bar, x, recon);
+        }
+        enc_phase<T, CUBIC, C_W1Y, C_W1X, C_W1Z>(L, rk, it, u, u.ev, u.ev, u.ov, sm, cseg, a);
+        __syncthreads();
+        enc_phase<T, CUBIC, C_W2E, C_W2ZY, C_W2ZX>(L, rk, it, u, u.ev, u.ov, u.ov, sm, cseg, a);
+        __syncthreads();
+        if (u.ov)
+            enc_phase<T, CUBIC, C_W3, C_NONE, C_NONE>(L, rk, it, u, true, false, false, sm, cseg,
+                                                      a);
+        __syncthreads();
+        prev = it;
+        st_e = u.eown ? u.ez : -1;
+        st_o = u.oown ? u.oz : -1;
+        cur = nxt;
+        it = nit;
+    }
+    if (st_e >= 0) store_plane<T, TMA>(L, prev, st_e, slot_of(slots, st_e), recon);
+    if (st_o >= 0) store_plane<T, TMA>(L, prev, st_o, slot_of(slots, st_o), recon);
+    warp_flush(a, sm);
+    if (TMA && wait_failed) {  // let a late load land before the CTA exits
+        mbar_wait(bar, parity ^ 1u);
+        if (threadIdx.x == 0) atomicOr(&L.st[0].acc->done, TILE_WAIT_FAILED);
     }
     __syncthreads();
 #pragma unroll
     for (int s = 0; s < TILE_STAGES; s++)
-        if (cur_seg[s] != 0xffffffffu) flush_hist(sm.hist + s * HBINS, L.st[s].hist_seg, cur_seg[s]);
+        if (cseg[s] != 0xffffffffu) flush_hist(sm.hist + s * HBINS, L.st[s].hist_seg, cseg[s]);
     // per stage: the warps' sums in warp order (deterministic), one partial row per CTA
     if (threadIdx.x < TILE_STAGES) {
         const int s = threadIdx.x;
         double t[5] = {0, 0, 0, 0, 0};
         uint32_t mq = 0, no = 0;
-        for (int w = 0; w < THREADS / 32; w++) {
-            const double* slot = sm.wacc + (w * TILE_STAGES + s) * 5;
-            for (int k = 0; k < 4; k++) t[k] += slot[k];
-            t[4] = fmax(t[4], slot[4]);
+        for (int w = 0; w < LW; w++) {
+            const double* sl = sm.wacc + (w * TILE_STAGES + s) * 5;
+            for (int k = 0; k < 4; k++) t[k] += sl[k];
+            t[4] = fmax(t[4], sl[4]);
             mq = max(mq, sm.wmq[w * TILE_STAGES + s]);
             no += sm.wno[w * TILE_STAGES + s];
         }
@@ -591,208 +900,199 @@ __global__ void __launch_bounds__(THREADS, 2)
     }
 }
 
-// ------------------------------------------------------------------ decode
-// Codes of a unit's computed points into registers (issued early; stored to
-// shared memory once the current unit is done). One compile-time loop per
-// class region: fixed register slots, constant divisors, the stage known.
-template <typename T, int STAGE, int R0, int NR, int B0, int NC>
-__device__ __forceinline__ void fetch_region(const TileLevel& L, const Ranks& rk, const Item& it,
-                                             int z, uint16_t* pf) {
-    constexpr int K = (NR * NC + THREADS - 1) / THREADS;
-    const uint16_t* codes = L.st[STAGE].codes + (uint64_t)it.c * L.st[STAGE].n;
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-        const int e = threadIdx.x + k * THREADS;
-        const int i = e / NC;
-        const int y = it.y0 - 3 + R0 + 2 * i, x = it.x0 - 4 + B0 + 2 * (e - i * NC);
-        pf[k] = (e < NR * NC && y >= 0 && y < L.N[1] && x >= 0 && x < L.N[2])
-                    ? __ldg(codes + rk.of<STAGE>(z, y, x))
-                    : (uint16_t)1;
-    }
-}
-
-template <typename T, int R0, int NR, int B0, int NC>
-__device__ __forceinline__ void put_region(const uint16_t* pf, uint16_t* dst) {
-    constexpr int K = (NR * NC + THREADS - 1) / THREADS;
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-        const int e = threadIdx.x + k * THREADS;
-        const int i = e / NC;
-        if (e < NR * NC) dst[(R0 + 2 * i) * Box<T>::BX + B0 + 2 * (e - i * NC)] = pf[k];
-    }
-}
-
-template <typename T>
-struct DecSlots {  // register slots per region: even A, B, C; odd D, E, F, G
-    using B = Box<T>;
-    static constexpr int k(int n) { return (n + THREADS - 1) / THREADS; }
-    static constexpr int A = k(B::HR_N * B::TC_N), Bn = k(B::TR_N * B::HC_N),
-                         C = k(B::TR_N * B::TC_N), D = k(B::HR_N * B::HC_N);
-    static constexpr int EVEN = A + Bn + C, ODD = D + A + Bn + C;
-    static constexpr int PF = EVEN > ODD ? EVEN : ODD;
-};
-
-template <typename T>
-__device__ __forceinline__ void fetch_codes(const TileLevel& L, const Ranks& rk, const Item& it,
-                                            int z, bool even, uint16_t* pf) {
-    using B = Box<T>;
-    using S = DecSlots<T>;
-    if (z < 0 || z >= L.N[0]) return;
-    if (even) {
-        fetch_region<T, 2, B::HR_R0, B::HR_N, B::TC_B0, B::TC_N>(L, rk, it, z, pf);
-        fetch_region<T, 1, B::TR_R0, B::TR_N, B::HC_B0, B::HC_N>(L, rk, it, z, pf + S::A);
-        fetch_region<T, 3, B::TR_R0, B::TR_N, B::TC_B0, B::TC_N>(L, rk, it, z, pf + S::A + S::Bn);
-    } else {
-        fetch_region<T, 0, B::HR_R0, B::HR_N, B::HC_B0, B::HC_N>(L, rk, it, z, pf);
-        fetch_region<T, 3, B::HR_R0, B::HR_N, B::TC_B0, B::TC_N>(L, rk, it, z, pf + S::D);
-        fetch_region<T, 3, B::TR_R0, B::TR_N, B::HC_B0, B::HC_N>(L, rk, it, z, pf + S::D + S::A);
-        fetch_region<T, 4, B::TR_R0, B::TR_N, B::TC_B0, B::TC_N>(L, rk, it, z,
-                                                                  pf + S::D + S::A + S::Bn);
-    }
-}
-
-template <typename T>
-__device__ __forceinline__ void put_codes(int z, int n0, bool even, const uint16_t* pf,
-                                          uint16_t* dst) {
-    using B = Box<T>;
-    using S = DecSlots<T>;
-    if (z < 0 || z >= n0) return;
-    if (even) {
-        put_region<T, B::HR_R0, B::HR_N, B::TC_B0, B::TC_N>(pf, dst);
-        put_region<T, B::TR_R0, B::TR_N, B::HC_B0, B::HC_N>(pf + S::A, dst);
-        put_region<T, B::TR_R0, B::TR_N, B::TC_B0, B::TC_N>(pf + S::A + S::Bn, dst);
-    } else {
-        put_region<T, B::HR_R0, B::HR_N, B::HC_B0, B::HC_N>(pf, dst);
-        put_region<T, B::HR_R0, B::HR_N, B::TC_B0, B::TC_N>(pf + S::D, dst);
-        put_region<T, B::TR_R0, B::TR_N, B::HC_B0, B::HC_N>(pf + S::D + S::A, dst);
-        put_region<T, B::TR_R0, B::TR_N, B::TC_B0, B::TC_N>(pf + S::D + S::A + S::Bn, dst);
-    }
-}
-
-template <typename T, int CUBIC, int ZO, int YO, int XO, int STAGE, int R0, int NR, int B0, int NC>
-__device__ __forceinline__ void dec_region(const TileLevel& L, const Unit<T>& u, const Item& it,
-                                           const uint16_t* codes) {
-    using RP = RegionPoint<T, R0, NR, B0, NC>;
-    const QParams& q = L.st[STAGE].q;
-    constexpr int NPTS = NR * NC;
-    for (int e0 = 0; e0 < NPTS; e0 += 2 * THREADS) {
-        const RP p0(e0 + threadIdx.x, it, L.N), p1(e0 + THREADS + threadIdx.x, it, L.N);
-        const uint32_t c0 = codes[p0.pos], c1 = codes[p1.pos];
-        const double d0 = predict_tile<T, CUBIC, ZO, YO, XO>(q, u, p0.pos, p0.y, p0.x, L.N);
-        const double d1 = predict_tile<T, CUBIC, ZO, YO, XO>(q, u, p1.pos, p1.y, p1.x, L.N);
-        // code 0 (outlier): the canvas value, already in the box
-        if (p0.act && c0) u.P[p0.pos] = dequant_value<T>(q, d0, c0);
-        if (p1.act && c1) u.P[p1.pos] = dequant_value<T>(q, d1, c1);
-    }
-}
-
-template <typename T, int CUBIC>
-__global__ void __launch_bounds__(THREADS, 2)
-    k_tile_level_dec(const TileLevel L, T* __restrict__ recon) {
-    using B = Box<T>;
-    extern __shared__ __align__(16) uint8_t smem[];
-    T* planes = (T*)smem;
-    uint16_t* csm = (uint16_t*)(planes + B::SLOTS * B::ELEMS);  // 2 x ELEMS codes
-    const bool vec = L.vec != 0;
-    Ranks rk;
+template <typename T, int CUBIC, int TMA>
+__global__ void __launch_bounds__(LT, 2)
+    k_lvl_dec(const __grid_constant__ CUtensorMap tmx, const TileLevel L, T* __restrict__ recon,
+              uint32_t* __restrict__ err) {
+    using Gm = G<T>;
+    using Ly = Lay<T, false>;
+    extern __shared__ __align__(128) uint8_t smem[];
+    T* slots = (T*)(smem + Ly::SLOTS);
+    T* XE = (T*)(smem + Ly::XE);
+    T* XO = (T*)(smem + Ly::XO);
+    // this warp's two buffers of MAXT tasks x 32 codes (Ly::CODE_ENTRIES in all)
+    static_assert(Ly::CODE_ENTRIES == LW * 2 * MAXT * 32, "code buffer layout");
+    uint16_t* wc = (uint16_t*)(smem + Ly::CODES) + (threadIdx.x >> 5) * 2 * MAXT * 32;
+    const uint32_t bar = su32(smem + Ly::MBAR);
+    if (threadIdx.x == 0) mbar_init(bar);
+    __syncthreads();
+    LvRanks rk;
     rk.init(L.N);
-    uint16_t pf[DecSlots<T>::PF];
-    for (uint32_t w = blockIdx.x; w < L.items; w += gridDim.x) {
-        const Item it = item_of<T>(L, w);
-        const int n_units = n_units_of(it);
-        {
-            bool ev;
-            const int z = unit_z(0, it.zs, ev);
-            if (z >= 0 && z < L.N[0])
-                load_plane<T>(L, it, z, false, planes + even_slot(z) * B::ELEMS, nullptr, recon,
-                              recon, vec);
-            cp_commit();
-            fetch_codes<T>(L, rk, it, z, ev, pf);
-            put_codes<T>(z, L.N[0], ev, pf, csm);
-        }
-        for (int k = 0; k < n_units; k++) {
-            bool nev = true;
-            int nz = -1;
-            if (k + 1 < n_units) nz = unit_z(k + 1, it.zs, nev);
-            fetch_codes<T>(L, rk, it, nz, nev, pf);
-            cp_wait_all();
-            __syncthreads();
-            if (nz >= 0 && nz < L.N[0])
-                load_plane<T>(L, it, nz, false, planes + (nev ? even_slot(nz) : 5) * B::ELEMS,
-                              nullptr, recon, recon, vec);
-            cp_commit();
-            bool even;
-            const int z = unit_z(k, it.zs, even);
-            const uint16_t* codes = csm + (k & 1) * B::ELEMS;
-            if (z >= 0 && z < L.N[0]) {
-                const Unit<T> u = make_unit<T>(planes, z, even, it, L.N[0]);
-                if (even) {
-                    dec_region<T, CUBIC, 0, 0, 1, 2, B::HR_R0, B::HR_N, B::TC_B0, B::TC_N>(L, u, it,
-                                                                                           codes);
-                    dec_region<T, CUBIC, 0, 1, 0, 1, B::TR_R0, B::TR_N, B::HC_B0, B::HC_N>(L, u, it,
-                                                                                           codes);
-                    __syncthreads();
-                    dec_region<T, CUBIC, 0, 1, 1, 3, B::TR_R0, B::TR_N, B::TC_B0, B::TC_N>(L, u, it,
-                                                                                           codes);
-                } else {
-                    dec_region<T, CUBIC, 1, 0, 0, 0, B::HR_R0, B::HR_N, B::HC_B0, B::HC_N>(L, u, it,
-                                                                                           codes);
-                    __syncthreads();
-                    dec_region<T, CUBIC, 1, 0, 1, 3, B::HR_R0, B::HR_N, B::TC_B0, B::TC_N>(L, u, it,
-                                                                                           codes);
-                    dec_region<T, CUBIC, 1, 1, 0, 3, B::TR_R0, B::TR_N, B::HC_B0, B::HC_N>(L, u, it,
-                                                                                           codes);
-                    __syncthreads();
-                    dec_region<T, CUBIC, 1, 1, 1, 4, B::TR_R0, B::TR_N, B::TC_B0, B::TC_N>(L, u, it,
-                                                                                           codes);
-                }
-                __syncthreads();
-                if (u.owned) store_plane<T>(L, it, z, even, u.P, recon, vec);
-            }
-            put_codes<T>(nz, L.N[0], nev, pf, csm + ((k + 1) & 1) * B::ELEMS);
-            __syncthreads();
-        }
-        cp_wait_all();
-        __syncthreads();
-    }
-}
+    uint32_t parity = 0;
+    bool wait_failed = false;
+    const int nz = L.N[0], lane = threadIdx.x & 31;
 
-template <typename T>
-constexpr uint64_t enc_smem() {
-    using B = Box<T>;
-    return sizeof(T) * (B::SLOTS + 1) * B::ELEMS + 4ull * TILE_STAGES * HBINS +
-           8ull * (THREADS / 32) * TILE_STAGES * 5 + 8ull * (THREADS / 32) * TILE_STAGES;
-}
-template <typename T>
-constexpr uint64_t dec_smem() {
-    using B = Box<T>;
-    return sizeof(T) * B::SLOTS * B::ELEMS + 2ull * 2 * B::ELEMS;
+    Cursor cur{blockIdx.x, 0};
+    Item it{}, prev{};
+    int st_e = -1, st_o = -1;
+    bool pending = false;
+    uint32_t pf[MAXT];
+    int buf = 0;
+    if (cur.item < L.items) {
+        it = item_of(L, cur.item, Gm::TX, Gm::TY);
+        const Unit<T> u0 = make_unit(slots, it, 0, nz);
+        pending = issue_loads<T, false, TMA>(&tmx, &tmx, L, it, u0, XE, XO, nullptr, bar, recon,
+                                             recon);
+        fetch_phase<T>(L, rk, it, u0, 0, pf);
+#pragma unroll
+        for (int k = 0; k < MAXT; k++) wc[k * 32 + lane] = (uint16_t)pf[k];
+        __syncwarp();
+    }
+    while (cur.item < L.items) {
+        const Unit<T> u = make_unit(slots, it, cur.u, nz);
+        phase0<T, TMA>(L, prev, st_e, st_o, u, cur.u == 0, pending, bar, parity, wait_failed,
+                       slots, XE, XO, nullptr, recon);
+        __syncthreads();
+        Cursor nxt = cur;
+        if (++nxt.u >= n_units(it)) {
+            nxt.item += gridDim.x;
+            nxt.u = 0;
+        }
+        Item nit = it;
+        pending = false;
+        const bool more = nxt.item < L.items;
+        if (more) {
+            if (nxt.item != cur.item) nit = item_of(L, nxt.item, Gm::TX, Gm::TY);
+            pending = issue_loads<T, false, TMA>(&tmx, &tmx, L, nit,
+                                                 make_unit(slots, nit, nxt.u, nz), XE, XO, nullptr,
+                                                 bar, recon, recon);
+        }
+        // each phase: fetch the next phase's codes, decode this one, then
+        // store the fetched codes (the loads had the whole phase to land)
+        fetch_phase<T>(L, rk, it, u, 1, pf);
+        dec_phase<T, CUBIC, C_W1Y, C_W1X, C_W1Z>(L, it, u, u.ev, u.ev, u.ov, wc + buf * MAXT * 32);
+        buf ^= 1;
+#pragma unroll
+        for (int k = 0; k < MAXT; k++) wc[buf * MAXT * 32 + k * 32 + lane] = (uint16_t)pf[k];
+        __syncthreads();
+        fetch_phase<T>(L, rk, it, u, 2, pf);
+        dec_phase<T, CUBIC, C_W2E, C_W2ZY, C_W2ZX>(L, it, u, u.ev, u.ov, u.ov,
+                                                   wc + buf * MAXT * 32);
+        buf ^= 1;
+#pragma unroll
+        for (int k = 0; k < MAXT; k++) wc[buf * MAXT * 32 + k * 32 + lane] = (uint16_t)pf[k];
+        __syncthreads();
+        if (more) fetch_phase<T>(L, rk, nit, make_unit(slots, nit, nxt.u, nz), 0, pf);
+        if (u.ov)
+            dec_phase<T, CUBIC, C_W3, C_NONE, C_NONE>(L, it, u, true, false, false,
+                                                      wc + buf * MAXT * 32);
+        buf ^= 1;
+#pragma unroll
+        for (int k = 0; k < MAXT; k++) wc[buf * MAXT * 32 + k * 32 + lane] = (uint16_t)pf[k];
+        __syncthreads();
+        prev = it;
+        st_e = u.eown ? u.ez : -1;
+        st_o = u.oown ? u.oz : -1;
+        cur = nxt;
+        it = nit;
+    }
+    if (st_e >= 0) store_plane<T, TMA>(L, prev, st_e, slot_of(slots, st_e), recon);
+    if (st_o >= 0) store_plane<T, TMA>(L, prev, st_o, slot_of(slots, st_o), recon);
+    if (TMA && wait_failed) {
+        mbar_wait(bar, parity ^ 1u);
+        if (threadIdx.x == 0) atomicOr(err, ERR_TILE_WAIT);
+    }
 }
 
 template <typename K>
-static int set_smem(K kern, uint64_t bytes) {
+static int set_smem(K kern, uint32_t bytes) {
     return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) ==
                    cudaSuccess
                ? LATEC_OK
                : LATEC_ERR_CUDA;
 }
 
+// Tensor map of a 4-D (x, y, z, channel) box over the level's lattice (unit
+// step along x). row_step 2 maps the even rows only.
+template <typename T>
+static bool make_map(CUtensorMap* m, const TileLevel& L, const void* base, int row_step,
+                     uint32_t box_rows) {
+    using Enc = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                             const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                             const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                             CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static Enc enc = driver_fn<Enc>("cuTensorMapEncodeTiled");
+    if (!enc) return false;
+    const uint64_t e = sizeof(T);
+    const cuuint64_t dims[4] = {(cuuint64_t)L.N[2],
+                                (cuuint64_t)((L.N[1] + row_step - 1) / row_step),
+                                (cuuint64_t)L.N[0], (cuuint64_t)L.channels};
+    const cuuint64_t strides[3] = {(cuuint64_t)(L.ls[1] * row_step) * e, (cuuint64_t)L.ls[0] * e,
+                                   (cuuint64_t)L.points * e};
+    const cuuint32_t box[4] = {(cuuint32_t)G<T>::BX, box_rows, 1, 1};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    return enc(m, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+               4, const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <typename T, int CUBIC>
+static int launch_enc(const TileLevel& L, uint32_t grid, const void* x, void* recon,
+                      cudaStream_t st) {
+    CUtensorMap mx, mr;
+    std::memset(&mx, 0, sizeof(mx));
+    std::memset(&mr, 0, sizeof(mr));
+    constexpr uint32_t bytes = Lay<T, true>::BYTES;
+    int rc;
+    if (L.tma) {
+        if (!make_map<T>(&mx, L, x, 1, G<T>::XR) || !make_map<T>(&mr, L, recon, 2, G<T>::RR))
+            return LATEC_ERR_CUDA;
+        if ((rc = set_smem(k_lvl_enc<T, CUBIC, 1>, bytes))) return rc;
+        k_lvl_enc<T, CUBIC, 1><<<grid, LT, bytes, st>>>(mx, mr, L, (const T*)x, (T*)recon);
+    } else {
+        if ((rc = set_smem(k_lvl_enc<T, CUBIC, 0>, bytes))) return rc;
+        k_lvl_enc<T, CUBIC, 0><<<grid, LT, bytes, st>>>(mx, mr, L, (const T*)x, (T*)recon);
+    }
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
+}
+
+template <typename T, int CUBIC>
+static int launch_dec(const TileLevel& L, uint32_t grid, void* recon, uint32_t* err,
+                      cudaStream_t st) {
+    CUtensorMap mx;
+    std::memset(&mx, 0, sizeof(mx));
+    constexpr uint32_t bytes = Lay<T, false>::BYTES;
+    int rc;
+    if (L.tma) {
+        if (!make_map<T>(&mx, L, recon, 1, G<T>::XR)) return LATEC_ERR_CUDA;
+        if ((rc = set_smem(k_lvl_dec<T, CUBIC, 1>, bytes))) return rc;
+        k_lvl_dec<T, CUBIC, 1><<<grid, LT, bytes, st>>>(mx, L, (T*)recon, err);
+    } else {
+        if ((rc = set_smem(k_lvl_dec<T, CUBIC, 0>, bytes))) return rc;
+        k_lvl_dec<T, CUBIC, 0><<<grid, LT, bytes, st>>>(mx, L, (T*)recon, err);
+    }
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
+}
+
 }  // namespace
 
 void tile_level_geometry(TileLevel& L, int elem, int n_sm, uint32_t* grid) {
-    const int tx = 64, ty = elem == 8 ? 16 : 32;
+    const int tx = tile_tx(elem), ty = tile_ty(elem);
     L.tiles_x = (L.N[2] + tx - 1) / tx;
     L.tiles_y = (L.N[1] + ty - 1) / ty;
-    // about 6 items per CTA of one wave (2 per SM) and chunks of >= 16 planes
     const uint64_t cols = (uint64_t)L.tiles_x * L.tiles_y * L.channels;
-    const uint64_t slots = 2ull * (uint64_t)n_sm;
-    uint64_t want = (6 * slots + cols - 1) / cols;
-    if (want < 1) want = 1;
-    int zc = (int)((L.N[0] + want - 1) / want);
-    zc = (zc + 1) & ~1;
-    if (zc < 16) zc = 16;
-    L.zc = zc;
-    L.chunks = (L.N[0] + zc - 1) / zc;
+    const uint64_t slots = 2ull * (uint64_t)n_sm;  // resident CTAs (2 per SM)
+    // chunk length: the cost of a CTA is the items it runs (the busiest CTA
+    // runs ceil(items / slots) of them) times the planes an item computes
+    // (its chunk plus about three halo planes)
+    int best = 16;
+    double best_cost = 1e300;
+    for (int zc = 8; zc <= 128; zc *= 2) {
+        const uint64_t chunks = (uint64_t)(L.N[0] + zc - 1) / zc;
+        const uint64_t items = cols * chunks;
+        const uint64_t per = (items + slots - 1) / slots;
+        const double cost = (double)per * (double)(zc + 3);
+        if (cost < best_cost * 0.999) {
+            best_cost = cost;
+            best = zc;
+        }
+        if ((uint64_t)zc >= (uint64_t)L.N[0]) break;
+    }
+    L.zc = best;
+    L.chunks = (L.N[0] + best - 1) / best;
     const uint64_t items = cols * (uint64_t)L.chunks;
     L.items = (uint32_t)items;
     *grid = (uint32_t)(items < slots ? items : slots);
@@ -801,35 +1101,21 @@ void tile_level_geometry(TileLevel& L, int elem, int n_sm, uint32_t* grid) {
 int launch_tile_level_encode(const TileLevel& L, int dtype, int cubic, uint32_t grid,
                              const void* x, void* recon, cudaStream_t st) {
     if (!grid) return LATEC_OK;
-    int rc;
-    if (dtype == LATEC_F64) {
-        auto k = cubic ? k_tile_level_enc<double, 1> : k_tile_level_enc<double, 0>;
-        if ((rc = set_smem(k, enc_smem<double>()))) return rc;
-        k<<<grid, THREADS, enc_smem<double>(), st>>>(L, (const double*)x, (double*)recon);
-    } else {
-        auto k = cubic ? k_tile_level_enc<float, 1> : k_tile_level_enc<float, 0>;
-        if ((rc = set_smem(k, enc_smem<float>()))) return rc;
-        k<<<grid, THREADS, enc_smem<float>(), st>>>(L, (const float*)x, (float*)recon);
-    }
-    count_launches(1);
-    return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
+    if (dtype == LATEC_F64)
+        return cubic ? launch_enc<double, 1>(L, grid, x, recon, st)
+                     : launch_enc<double, 0>(L, grid, x, recon, st);
+    return cubic ? launch_enc<float, 1>(L, grid, x, recon, st)
+                 : launch_enc<float, 0>(L, grid, x, recon, st);
 }
 
 int launch_tile_level_decode(const TileLevel& L, int dtype, int cubic, uint32_t grid, void* recon,
-                             cudaStream_t st) {
+                             uint32_t* err, cudaStream_t st) {
     if (!grid) return LATEC_OK;
-    int rc;
-    if (dtype == LATEC_F64) {
-        auto k = cubic ? k_tile_level_dec<double, 1> : k_tile_level_dec<double, 0>;
-        if ((rc = set_smem(k, dec_smem<double>()))) return rc;
-        k<<<grid, THREADS, dec_smem<double>(), st>>>(L, (double*)recon);
-    } else {
-        auto k = cubic ? k_tile_level_dec<float, 1> : k_tile_level_dec<float, 0>;
-        if ((rc = set_smem(k, dec_smem<float>()))) return rc;
-        k<<<grid, THREADS, dec_smem<float>(), st>>>(L, (float*)recon);
-    }
-    count_launches(1);
-    return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
+    if (dtype == LATEC_F64)
+        return cubic ? launch_dec<double, 1>(L, grid, recon, err, st)
+                     : launch_dec<double, 0>(L, grid, recon, err, st);
+    return cubic ? launch_dec<float, 1>(L, grid, recon, err, st)
+                 : launch_dec<float, 0>(L, grid, recon, err, st);
 }
 
 }  // namespace latec

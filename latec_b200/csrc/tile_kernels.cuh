@@ -1,6 +1,7 @@
 // Fused level kernels for 3-D grids: all five sub-stages of one level of the
-// dyadic schedule (weight-1 along axes 0, 1, 2, then the fused weight-2 and
-// weight-3 stages) in one launch, tile by tile in shared memory.
+// dyadic schedule (weight 1 along axes 0, 1, 2, then the fused weight-2 and
+// weight-3 stages) in one launch each way, column by column of the level's
+// lattice, with the planes of a column in shared memory.
 #pragma once
 
 #include "interp_kernels.cuh"
@@ -33,34 +34,38 @@ struct TileLevel {
     int64_t ls[3];         // grid element stride of one lattice step per axis
     uint64_t points;       // grid points per channel
     int32_t channels;
-    int32_t tiles_x, tiles_y;  // tiles of the lattice's axes 2 and 1
+    int32_t tiles_x, tiles_y;  // column tiles along the lattice's axes 2 and 1
     int32_t chunks, zc;        // axis-0 chunks of zc planes (zc even)
     uint32_t items;            // channels * chunks * tiles_y * tiles_x work items
-    int32_t vec;               // rows move as 16-byte groups (see tile_vec_ok)
+    int32_t tma;               // planes arrive by TMA (else per-element async copies)
     int32_t pad1;
     TileStage st[TILE_STAGES];
 };
 
-// Tile edge (lattice points) along axis 2 and axis 1 for an element size.
+// Column tile (lattice points) along axis 2 and axis 1 for an element size.
 inline int tile_tx(int) { return 64; }
 inline int tile_ty(int elem) { return elem == 8 ? 16 : 32; }
 
-// 16-byte row copies are valid: unit lattice step along axis 2, every row
-// start and the extent along axis 2 a multiple of 16 bytes, pointers aligned.
-inline bool tile_vec_ok(const TileLevel& L, int elem, const void* a, const void* b) {
+// The TMA path applies: unit lattice step along axis 2, rows of whole 16-byte
+// groups, every 16-byte aligned base pointer.
+inline bool tile_tma_ok(const TileLevel& L, int elem, const void* a, const void* b) {
     const int64_t v = 16 / elem;
     return L.ls[2] == 1 && L.ls[1] % v == 0 && L.ls[0] % v == 0 && (int64_t)L.points % v == 0 &&
-           L.N[2] % v == 0 && ((uintptr_t)a % 16) == 0 && ((uintptr_t)b % 16) == 0;
+           ((uintptr_t)a % 16) == 0 && ((uintptr_t)b % 16) == 0;
 }
 
 // Work decomposition of a level: tiles, axis-0 chunk length, items. grid is
-// the persistent CTA count (one wave).
+// the persistent CTA count (one wave of resident CTAs).
 void tile_level_geometry(TileLevel& L, int elem, int n_sm, uint32_t* grid);
 
+// Fused encode / decode of one level. Encode reports a failed load wait by
+// setting bit 31 of `done` in the stages' statistics; decode through err.
 int launch_tile_level_encode(const TileLevel& L, int dtype, int cubic, uint32_t grid,
                              const void* x, void* recon, cudaStream_t st);
-int launch_tile_level_decode(const TileLevel& L, int dtype, int cubic, uint32_t grid,
-                             void* recon, cudaStream_t st);
+int launch_tile_level_decode(const TileLevel& L, int dtype, int cubic, uint32_t grid, void* recon,
+                             uint32_t* err, cudaStream_t st);
+constexpr uint32_t TILE_WAIT_FAILED = 0x80000000u;  // StageAcc::done bit (encode)
+constexpr uint32_t ERR_TILE_WAIT = 0x400u;          // err bit (decode)
 
 // Stage tails of a fused encode: per stage (one CTA each) the fixed-order
 // reduction of the per-CTA statistics and the exclusive scan of the tile

@@ -1,7 +1,9 @@
-"""The fused tile levels (five sub-stages of a 3-D level in one launch, over
-tiles held in shared memory with a halo) give exactly the per-stage launches'
-results: the same stream bytes, reconstruction and decode. Mode 1 fuses the
-finest level, mode 2 every level (coarser levels run on their lattice)."""
+"""The fused levels (five sub-stages of a 3-D level in one launch, over column
+tiles of the level's lattice staged in shared memory with a halo) give exactly
+the per-stage launches' results: the same stream bytes, reconstruction and
+decode. Mode 1 fuses the finest level, mode 3 every level whatever its size
+(coarser levels run on their lattice), mode 2 (the default) every level of at
+least 2^18 points."""
 
 import numpy as np
 import pytest
@@ -23,6 +25,9 @@ CASES = [
     ((3, 5, 200), 2, 4, np.float32, 0, 1, "cubic", 1 << 15),
     ((2, 2, 2), 1, 2, np.float32, 0, 1, "cubic", 1 << 15),
 ]
+
+
+DEFAULT_MODE = 2
 
 
 def _mode(m):
@@ -47,7 +52,7 @@ def test_tile_levels_match_per_stage_launches(case):
     lib = _lib.load()
     try:
         outs, launches = [], []
-        for mode in (0, 1, 2):
+        for mode in (0, 1, 3, 2):
             _mode(mode)
             pred = lb.InterpPredictor(order, lv, st, 1, center=center, end_mode=em)
             n0 = lib.latec_launch_count()
@@ -74,7 +79,7 @@ def test_tile_levels_match_per_stage_launches(case):
         if min(shape) >= 4:  # a fused level replaced five stage launches each way
             assert launches[1][1] < launches[0][1]
     finally:
-        _mode(0)
+        _mode(DEFAULT_MODE)
 
 
 def test_tile_mode_is_deterministic():
@@ -92,7 +97,7 @@ def test_tile_mode_is_deterministic():
         a, sa = lb.compress(x, eb, pred, levels=4, anchor_stride=16, recon="device")
         b, sb = lb.compress(x, eb, pred, levels=4, anchor_stride=16, recon="device")
     finally:
-        _mode(0)
+        _mode(DEFAULT_MODE)
     assert a == b
     assert sa["stage_recon_sse"] == sb["stage_recon_sse"]
     assert sa["stage_pred_sae"] == sb["stage_pred_sae"]
@@ -102,6 +107,7 @@ def test_tile_mode_rejects_bad_values():
     from latec_b200 import _lib
 
     lib = _lib.load()
-    assert lib.latec_set_tile_mode(3) != 0
+    assert lib.latec_set_tile_mode(4) != 0
     assert lib.latec_set_tile_mode(-1) != 0
     assert lib.latec_set_tile_mode(0) == 0
+    assert lib.latec_set_tile_mode(DEFAULT_MODE) == 0
