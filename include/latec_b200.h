@@ -90,7 +90,9 @@ typedef struct latec_rans_stage {
 
 /* ---- schedule: replaces latec/levels.py:100-147 (iter_stage_plan),
  *      221-282 (stage_counts), 297-326 (stage_strides), 469-574
- *      (stage_layouts). anchor_block must be 1. */
+ *      (stage_layouts). anchor_block in [1, anchor_stride]: blocks of
+ *      anchor_block consecutive lattice points per axis every anchor_stride
+ *      points form the anchor stage (latec/levels.py:100-147). */
 int latec_plan_create(const uint32_t* shape, int32_t ndim, int32_t levels,
                       int32_t anchor_stride, int32_t anchor_block, latec_plan** out);
 int latec_plan_destroy(latec_plan* plan);

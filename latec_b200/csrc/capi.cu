@@ -93,7 +93,10 @@ uint64_t stage_ws(uint64_t max_items, uint64_t all_tiles, int n_stages, int elem
 // Stages [t, t + 5) form a standard level of a 3-D plan: weight 1 along axes
 // 0, 1 and 2, then the fused weight-2 and weight-3 stages, all of one stride.
 bool tile_level_shape(const latec_plan* plan, int t) {
-    if (plan->ndim != 3 || t < 1 || t + TILE_STAGES > (int)plan->stages.size()) return false;
+    // blocked anchors leave holes in the finer stages: per-stage launches only
+    if (plan->ndim != 3 || plan->anchor_block != 1 || t < 1 ||
+        t + TILE_STAGES > (int)plan->stages.size())
+        return false;
     const StageDesc* d = &plan->stages[t];
     const int s = d[0].s;
     for (int j = 0; j < 3; j++)
@@ -245,7 +248,7 @@ struct LevelBuild {
 // slab of slack covers the rounding of band starts down to a tile).
 bool build_level(const latec_plan* plan, int t0, int t1, int C, int elem, int mode,
                  uint64_t items_cap, LevelBuild& L, uint32_t* tiles_per_stage) {
-    if (mode == 0 || C != 1 || plan->ndim < 2 || t0 < 1 || t1 - t0 < 2 ||
+    if (mode == 0 || C != 1 || plan->ndim < 2 || plan->anchor_block != 1 || t0 < 1 || t1 - t0 < 2 ||
         t1 - t0 > (int)LVL_MAX_STAGES)
         return false;
     const int s = plan->stages[t0].s;
@@ -429,7 +432,7 @@ int latec_plan_stage_flat(const latec_plan* plan, int32_t stage, uint64_t first,
     const StageDesc& d = plan->stages[stage];
     if (first + count > d.n) return LATEC_ERR_ARG;
     int32_t coord[MAXD];
-    for (uint64_t i = 0; i < count; i++) out_flat[i] = stage_coords(d, (uint32_t)(first + i), coord);
+    for (uint64_t i = 0; i < count; i++) out_flat[i] = stage_point(d, (uint32_t)(first + i), coord);
     return LATEC_OK;
 }
 

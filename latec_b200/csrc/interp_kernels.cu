@@ -234,7 +234,7 @@ __device__ __forceinline__ double locate_predict(const StageDesc& d, const QPara
         rank = (uint32_t)(i - (uint64_t)c * d.n);
     }
     int32_t coord[ND > 0 ? ND : MAXD];
-    flat = stage_coords_t<ND, KIND>(d, rank, coord);
+    flat = stage_point_t<ND, KIND>(d, rank, coord);
     return is_anchor ? 0.0
                      : predict_point<T, ND, KIND, CUBIC>(d, q, recon + (uint64_t)c * q.points, flat,
                                                          coord);
@@ -253,7 +253,7 @@ __device__ __forceinline__ void locate_gather(const StageDesc& d, const QParams&
         rank = (uint32_t)(i - (uint64_t)c * d.n);
     }
     int32_t coord[ND > 0 ? ND : MAXD];
-    flat = stage_coords_t<ND, KIND>(d, rank, coord);
+    flat = stage_point_t<ND, KIND>(d, rank, coord);
     if (!is_anchor)
         gather_point<T, ND, KIND, CUBIC, COH>(d, q, recon + (uint64_t)c * q.points, flat, coord,
                                               pt);
@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(THREADS)
         rank = (uint32_t)(i - (uint64_t)c * d.n);
     }
     int32_t coord[ND > 0 ? ND : MAXD];
-    const int64_t flat = stage_coords_t<ND, KIND>(d, rank, coord);
+    const int64_t flat = stage_point_t<ND, KIND>(d, rank, coord);
     pred[i] = (T)predict_point<T, ND, KIND, CUBIC>(d, q, recon + (uint64_t)c * q.points, flat,
                                                     coord);
 }
@@ -527,7 +527,7 @@ __device__ __forceinline__ void dequant_point(const StageDesc& d, const QParams&
         rank = (uint32_t)(i - (uint64_t)c * d.n);
     }
     int32_t coord[ND > 0 ? ND : MAXD];
-    const int64_t flat = stage_coords_t<ND, KIND>(d, rank, coord);
+    const int64_t flat = stage_point_t<ND, KIND>(d, rank, coord);
     T* rc = recon + (uint64_t)c * q.points;
     T rv;
     if (code == 0) {
@@ -686,7 +686,7 @@ __global__ void __launch_bounds__(THREADS)
                     rank = (uint32_t)(i - (uint64_t)c * S.d.n);
                 }
                 int32_t coord[MAXD];
-                const int64_t flat = stage_coords(S.d, rank, coord);
+                const int64_t flat = stage_point(S.d, rank, coord);
                 T v = (T)0;
                 if (pos < S.n_out) {
                     v = load_unaligned<T>(S.outliers + (uint64_t)pos * sizeof(T));
@@ -744,7 +744,7 @@ __device__ __forceinline__ void dequant_tile_l2(const StageDesc& d, const QParam
                     c = (uint32_t)(i0 / d.n);
                     rank = (uint32_t)(i0 - (uint64_t)c * d.n);
                 }
-                f0 = stage_coords_t<ND, KIND>(d, rank, coord);
+                f0 = stage_point_t<ND, KIND>(d, rank, coord);
                 c0 = c;
                 if (p0 < n_out) {
                     v = load_unaligned<T>(outliers + (uint64_t)p0 * sizeof(T));
@@ -766,7 +766,7 @@ __device__ __forceinline__ void dequant_tile_l2(const StageDesc& d, const QParam
                     c = (uint32_t)(i1 / d.n);
                     rank = (uint32_t)(i1 - (uint64_t)c * d.n);
                 }
-                f1 = stage_coords_t<ND, KIND>(d, rank, coord);
+                f1 = stage_point_t<ND, KIND>(d, rank, coord);
                 c1 = c;
                 if (p1 < n_out) {
                     v = load_unaligned<T>(outliers + (uint64_t)p1 * sizeof(T));
@@ -830,7 +830,7 @@ __global__ void __launch_bounds__(THREADS, 3)
             // weight-1 sub-stages read only coarser levels (finished by earlier
             // launches): their taps may go through L1; the fused sub-stages
             // read this level's other sub-stages and must read through L2
-            if (sd.kind)
+            if (sd.kind == 1)
                 dequant_tile_l2<T, ND, 1, CUBIC, 1>(sd, sq, tile, ls.codes, ls.outliers,
                                                     ls.tile_cnt, ls.tile_off, ls.n_out, recon, err);
             else if (sd.weight > 1)
@@ -858,7 +858,7 @@ static int last_err() {
 #define LATEC_DISPATCH(KERNEL_CALL)                                                      \
     do {                                                                                 \
         const int nd_ = (d.ndim >= 2 && d.ndim <= 4) ? d.ndim : 0;                      \
-        const int kd_ = d.kind ? 1 : 0, cu_ = q.order ? 1 : 0;                           \
+        const int kd_ = d.kind == 1 ? 1 : 0, cu_ = q.order ? 1 : 0;                      \
         if (dtype == LATEC_F64) {                                                        \
             using T = double;                                                            \
             DISPATCH_ND(KERNEL_CALL);                                                    \

@@ -65,16 +65,34 @@ struct StageDesc {
     int32_t shape[MAXD];
     int64_t gstride[MAXD];
     int32_t start[MAXD];      // kind 0
-    FastDiv size_div[MAXD];   // kind 0: class extent per axis
+    FastDiv size_div[MAXD];   // kind 0 / 2: class extent per axis
     FastDiv g_div[MAXD][MAXD + 1];  // kind 1: G[j][r]
     uint32_t f_even[MAXD][MAXD + 1];  // kind 1: F[j+1][r]
+    // Blocked anchors (anchor_block > 1): the anchor stage is kind 2, every
+    // anchor_block^ndim block of the anchor lattice in C order; a later stage
+    // whose point set meets those blocks skips them ("holes"). Its points are
+    // then the full set above minus the holes, in the same C order.
+    int32_t astride;          // anchor stride (a power of two)
+    int32_t ablock;           // anchor block edge (1: no blocked anchors)
+    int32_t holes;            // the stage's full set contains anchor-block points
+    int32_t lg2s;             // log2(2 s): lattice positions of one parity are 2 s apart
+    uint32_t n_full;          // points of the full set (n + holes)
+    FastDiv blk_div;          // kind 2: divide by ablock
+    // per axis and parity (0: even, 1: odd multiple of s): positions of the
+    // progression parity * s + 2 s m per anchor period (log2), how many of
+    // them start inside a block, and how many of the axis's positions do
+    uint32_t h_lgp[MAXD][2];
+    uint32_t h_k[MAXD][2];
+    uint32_t h_tot[MAXD][2];
+    uint32_t h_c[MAXD + 1][MAXD + 1];  // kind 1: block completions of axes j.., r odd left
+    uint32_t h_suf[MAXD + 1];          // kind 0: product of h_tot over axes j..
 };
 
 // Decode a stage-local rank into grid coordinates; returns the flat grid index.
 __host__ __device__ __forceinline__ int64_t stage_coords(const StageDesc& d, uint32_t rank,
                                                 int32_t* coord) {
     int64_t flat = 0;
-    if (d.kind == 0) {
+    if (d.kind != 1) {
         uint32_t rem = rank;
 #pragma unroll
         for (int j = MAXD - 1; j >= 0; j--) {
@@ -82,7 +100,12 @@ __host__ __device__ __forceinline__ int64_t stage_coords(const StageDesc& d, uin
                 uint32_t q = fdiv(rem, d.size_div[j]);
                 uint32_t m = rem - q * d.size_div[j].d;
                 rem = q;
-                coord[j] = d.start[j] + d.step * (int32_t)m;
+                if (d.kind == 2) {  // block m / ablock, offset m % ablock
+                    const uint32_t b = fdiv(m, d.blk_div);
+                    coord[j] = (int32_t)(b * (uint32_t)d.astride + (m - b * d.blk_div.d));
+                } else {
+                    coord[j] = d.start[j] + d.step * (int32_t)m;
+                }
                 flat += (int64_t)coord[j] * d.gstride[j];
             }
         }
@@ -126,7 +149,12 @@ __host__ __device__ __forceinline__ int64_t stage_coords_t(const StageDesc& d, u
                 const uint32_t q = fdiv(rem, d.size_div[j]);
                 const uint32_t m = rem - q * d.size_div[j].d;
                 rem = q;
-                coord[j] = d.start[j] + d.step * (int32_t)m;
+                if (d.kind == 2) {  // blocked anchors: block m / ablock, offset m % ablock
+                    const uint32_t b = fdiv(m, d.blk_div);
+                    coord[j] = (int32_t)(b * (uint32_t)d.astride + (m - b * d.blk_div.d));
+                } else {
+                    coord[j] = d.start[j] + d.step * (int32_t)m;
+                }
                 flat += (int64_t)coord[j] * d.gstride[j];
             }
         }
@@ -151,6 +179,91 @@ __host__ __device__ __forceinline__ int64_t stage_coords_t(const StageDesc& d, u
         }
     }
     return flat;
+}
+
+// ---- stages with holes (blocked anchors)
+
+// In-block positions among the first m positions of a progression with
+// 2^lgp positions per anchor period, k of them inside a block (the first k).
+__host__ __device__ __forceinline__ uint32_t block_count(uint32_t m, uint32_t lgp, uint32_t k) {
+    const uint32_t r = m & ((1u << lgp) - 1u);
+    return (m >> lgp) * k + (r < k ? r : k);
+}
+
+// The point lies in an anchor block: every coordinate's offset in its anchor
+// period is below the block edge.
+template <int ND>
+__host__ __device__ __forceinline__ bool in_blocks(const StageDesc& d, const int32_t* coord) {
+    constexpr int NDV = ND > 0 ? ND : MAXD;
+    bool in = true;
+#pragma unroll
+    for (int j = 0; j < NDV; j++)
+        if (ND > 0 || j < d.ndim) in = in && (coord[j] & (d.astride - 1)) < d.ablock;
+    return in;
+}
+
+// Holes (anchor-block points of the stage's full set) before the point in C
+// order. A hole precedes the point iff it agrees on axes < j, is smaller on
+// axis j and the agreeing prefix is itself inside the blocks: a sum over j of
+// (in-block positions before coord[j]) x (in-block completions of the later
+// axes), with the stage's parity constraint carried along for the fused kind.
+template <int ND, int KIND>
+__host__ __device__ __forceinline__ uint32_t holes_before(const StageDesc& d,
+                                                          const int32_t* coord) {
+    constexpr int NDV = ND > 0 ? ND : MAXD;
+    uint32_t h = 0;
+    bool in = true;
+    int r = d.weight;
+    const int32_t s = d.s;
+#pragma unroll
+    for (int j = 0; j < NDV; j++) {
+        if (ND > 0 || j < d.ndim) {
+            const uint32_t c = (uint32_t)coord[j];
+            if (KIND == 0) {
+                const uint32_t par = d.start[j] == s ? 1u : 0u;
+                const uint32_t m = (c - (uint32_t)d.start[j]) >> d.lg2s;  // position index
+                if (in) h += block_count(m, d.h_lgp[j][par], d.h_k[j][par]) * d.h_suf[j + 1];
+            } else {
+                // positions of each parity strictly before c
+                const uint32_t m0 = (c + (1u << d.lg2s) - 1u) >> d.lg2s;
+                const uint32_t m1 = (c + (uint32_t)s - 1u) >> d.lg2s;
+                if (in) {
+                    h += block_count(m0, d.h_lgp[j][0], d.h_k[j][0]) * d.h_c[j + 1][r];
+                    if (r > 0) h += block_count(m1, d.h_lgp[j][1], d.h_k[j][1]) * d.h_c[j + 1][r - 1];
+                }
+                r -= (c & (uint32_t)s) ? 1 : 0;
+            }
+            in = in && (c & (uint32_t)(d.astride - 1)) < (uint32_t)d.ablock;
+        }
+    }
+    return h;
+}
+
+// Rank -> grid point of a stage, holes skipped. Without holes this is the
+// closed-form decode; with holes, the rank-r point is the least full-set index
+// i with i - holes_before(i) = r that is not a hole: i = r + holes_before(i)
+// is reached by fixed-point iteration from i = r (the right side never
+// decreases and never passes the least solution), then holes are stepped over.
+template <int ND, int KIND>
+__host__ __device__ __forceinline__ int64_t stage_point_t(const StageDesc& d, uint32_t rank,
+                                                          int32_t* coord) {
+    if (!d.holes) return stage_coords_t<ND, KIND>(d, rank, coord);
+    uint32_t i = rank;
+    int64_t f = stage_coords_t<ND, KIND>(d, i, coord);
+    for (int it = 0; it < 256; it++) {
+        const uint32_t ni = rank + holes_before<ND, KIND>(d, coord);
+        if (ni == i || ni >= d.n_full) break;
+        i = ni;
+        f = stage_coords_t<ND, KIND>(d, i, coord);
+    }
+    while (in_blocks<ND>(d, coord) && i + 1 < d.n_full) f = stage_coords_t<ND, KIND>(d, ++i, coord);
+    return f;
+}
+
+// Runtime-rank form of stage_point_t (host code and rank-generic kernels).
+__host__ __device__ __forceinline__ int64_t stage_point(const StageDesc& d, uint32_t rank,
+                                                        int32_t* coord) {
+    return d.kind == 1 ? stage_point_t<0, 1>(d, rank, coord) : stage_point_t<0, 0>(d, rank, coord);
 }
 
 }  // namespace latec

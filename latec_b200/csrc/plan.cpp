@@ -2,6 +2,7 @@
 // per-stage decode descriptors the kernels use. Follows the reference
 // schedule (latec/levels.py:100-147 iter_stage_plan, 221-282 stage_counts,
 // 469-574 stage_layouts / _fused_classes) without building any mask.
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -23,15 +24,17 @@ int check_plan(const uint32_t* shape, int ndim, int levels, int anchor_stride,
     if (anchor_stride < 2 || (anchor_stride & (anchor_stride - 1))) return LATEC_ERR_ARG;
     if (anchor_block < 1 || anchor_block > anchor_stride) return LATEC_ERR_ARG;
     if ((1ll << levels) < anchor_stride) return LATEC_ERR_ARG;
-    if (anchor_block != 1) return LATEC_ERR_UNSUPPORTED;
     for (int j = 0; j < ndim; j++)
         if (shape[j] == 0 || shape[j] > (1u << 30)) return LATEC_ERR_ARG;
     return LATEC_OK;
 }
 
-static void base_desc(StageDesc& d, const uint32_t* shape, int ndim) {
+static void base_desc(StageDesc& d, const uint32_t* shape, int ndim, int astride, int ablock) {
     std::memset(&d, 0, sizeof(d));
     d.ndim = ndim;
+    d.astride = astride;
+    d.ablock = ablock;
+    d.blk_div = make_fastdiv(1);
     int64_t g = 1;
     for (int j = ndim - 1; j >= 0; j--) {
         d.shape[j] = (int32_t)shape[j];
@@ -42,6 +45,71 @@ static void base_desc(StageDesc& d, const uint32_t* shape, int ndim) {
         d.size_div[j] = make_fastdiv(1);
         for (int r = 0; r <= MAXD; r++) d.g_div[j][r] = make_fastdiv(1);
     }
+}
+
+static int log2u(uint64_t v) {
+    int l = 0;
+    while ((1ull << l) < v) l++;
+    return l;
+}
+
+// Blocked anchors: the anchor stage is every anchor_block^ndim block of the
+// anchor lattice, in C order (latec/levels.py:114-120).
+static int blocked_anchors(StageDesc& d, int astride, int ablock) {
+    uint64_t n = 1;
+    d.kind = 2;
+    d.step = astride;
+    d.blk_div = make_fastdiv((uint32_t)ablock);
+    for (int j = 0; j < d.ndim; j++) {
+        const uint32_t nj = (uint32_t)d.shape[j];
+        const uint32_t c = nj / astride * ablock + std::min<uint32_t>(nj % astride, ablock);
+        d.size_div[j] = make_fastdiv(c ? c : 1);
+        n *= c;
+    }
+    if (n > 0xFFFFFFFFull) return LATEC_ERR_UNSUPPORTED;
+    d.n = d.n_full = (uint32_t)n;
+    return LATEC_OK;
+}
+
+// The holes of a stage at level s (anchor-block points of its full set, which
+// the anchor stage already coded): per axis and parity, the in-block positions
+// of the progression parity * s + 2 s m, then their products over the axes.
+static int stage_holes(StageDesc& d) {
+    const int s = d.s, nd = d.ndim;
+    d.lg2s = log2u(2ull * s);
+    if (d.ablock <= 1 || d.n == 0) return LATEC_OK;
+    const uint32_t per = d.astride / (2 * s) ? (uint32_t)(d.astride / (2 * s)) : 1u;
+    for (int j = 0; j < nd; j++)
+        for (int par = 0; par < 2; par++) {
+            const int64_t first = (int64_t)par * s;
+            uint32_t k = 0;
+            if (d.ablock > first) k = (uint32_t)std::min<int64_t>(per, (d.ablock - first + 2 * s - 1) / (2 * s));
+            d.h_lgp[j][par] = (uint32_t)log2u(per);
+            d.h_k[j][par] = k;
+            const uint64_t m_tot = slice_count(d.shape[j], first, 2 * s);
+            d.h_tot[j][par] = block_count((uint32_t)m_tot, d.h_lgp[j][par], k);
+        }
+    uint64_t holes = 0;
+    if (d.kind == 0) {
+        d.h_suf[nd] = 1;
+        for (int j = nd - 1; j >= 0; j--) {
+            const int par = d.start[j] == s ? 1 : 0;
+            d.h_suf[j] = d.h_suf[j + 1] * d.h_tot[j][par];
+        }
+        holes = d.h_suf[0];
+    } else {
+        for (int r = 0; r <= MAXD; r++) d.h_c[nd][r] = r == 0 ? 1u : 0u;
+        for (int j = nd - 1; j >= 0; j--)
+            for (int r = 0; r <= MAXD; r++)
+                d.h_c[j][r] = d.h_tot[j][0] * d.h_c[j + 1][r] +
+                              (r ? d.h_tot[j][1] * d.h_c[j + 1][r - 1] : 0u);
+        holes = d.h_c[0][d.weight];
+    }
+    if (holes > d.n) return LATEC_ERR_INTERNAL;
+    d.n_full = d.n;
+    d.n = (uint32_t)(d.n - holes);
+    d.holes = holes ? 1 : 0;
+    return LATEC_OK;
 }
 
 static int single_class(StageDesc& d, const int32_t* starts, int step) {
@@ -55,7 +123,7 @@ static int single_class(StageDesc& d, const int32_t* starts, int step) {
         n *= c;
     }
     if (n > 0xFFFFFFFFull) return LATEC_ERR_UNSUPPORTED;
-    d.n = (uint32_t)n;
+    d.n = d.n_full = (uint32_t)n;
     return LATEC_OK;
 }
 
@@ -78,7 +146,7 @@ static int fused(StageDesc& d, int s, int w) {
     if (F[0][w] > 0xFFFFFFFFull) return LATEC_ERR_UNSUPPORTED;
     d.kind = 1;
     d.weight = w;
-    d.n = (uint32_t)F[0][w];
+    d.n = d.n_full = (uint32_t)F[0][w];
     for (int j = 0; j < nd; j++)
         for (int r = 0; r <= w; r++) {
             uint64_t odd = r ? F[j + 1][r - 1] : 0;
@@ -105,10 +173,14 @@ int build_plan(Plan& p, const uint32_t* shape, int ndim, int levels, int anchor_
     p.stages.clear();
     StageDesc d;
     int32_t starts[MAXD] = {0};
-    base_desc(d, shape, ndim);
+    base_desc(d, shape, ndim, anchor_stride, anchor_block);
     d.axis = -1;
     d.s = anchor_stride;
-    if ((rc = single_class(d, starts, anchor_stride))) return rc;
+    if (anchor_block > 1) {
+        if ((rc = blocked_anchors(d, anchor_stride, anchor_block))) return rc;
+    } else if ((rc = single_class(d, starts, anchor_stride))) {
+        return rc;
+    }
     p.stages.push_back(d);
     int prev = -1;
     for (int k = 1; k <= levels; k++) {
@@ -117,21 +189,23 @@ int build_plan(Plan& p, const uint32_t* shape, int ndim, int levels, int anchor_
         bool repeat = s == prev;
         prev = s;
         for (int axis = 0; axis < ndim; axis++) {
-            base_desc(d, shape, ndim);
+            base_desc(d, shape, ndim, anchor_stride, anchor_block);
             d.axis = axis;
             d.weight = 1;
             d.s = s;
             for (int j = 0; j < ndim; j++) starts[j] = j == axis ? s : 0;
             if ((rc = single_class(d, starts, 2 * s))) return rc;
-            if (repeat) d.n = 0;
+            if (repeat) d.n = d.n_full = 0;
+            if ((rc = stage_holes(d))) return rc;
             p.stages.push_back(d);
         }
         for (int w = 2; w <= ndim; w++) {
-            base_desc(d, shape, ndim);
+            base_desc(d, shape, ndim, anchor_stride, anchor_block);
             d.axis = -2;
             d.s = s;
             if ((rc = fused(d, s, w))) return rc;
-            if (repeat) d.n = 0;
+            if (repeat) d.n = d.n_full = 0;
+            if ((rc = stage_holes(d))) return rc;
             p.stages.push_back(d);
         }
     }

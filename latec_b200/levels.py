@@ -61,10 +61,6 @@ class Plan:
 
     def __init__(self, shape, levels, anchor_stride, anchor_block=1):
         self.shape = check_plan(shape, levels, anchor_stride, anchor_block)
-        if anchor_block != 1:
-            raise NotImplementedError(
-                "the CUDA schedule supports anchor_block=1 (the codec's default); "
-                f"got anchor_block={anchor_block}")
         if len(self.shape) > 6:
             raise NotImplementedError("the CUDA schedule supports up to 6 spatial axes")
         self.levels, self.anchor_stride, self.anchor_block = levels, anchor_stride, anchor_block

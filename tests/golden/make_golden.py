@@ -131,6 +131,20 @@ def _cases():
         ("image_3ch", lambda: (np.random.RandomState(14).rand(24, 31, 3) * 100).astype(np.float32),
          0.5, dict(order="cubic", levels=3, anchor_stride=8, anchor_block=1),
          dict(levels=3, anchor_stride=8, anchor_block=1), True),
+        # blocked anchors: anchor_block^ndim blocks on the anchor lattice, the
+        # finer stages skip them (InterpPredictor's own default block is 4)
+        ("block4_2d", lambda: fields.grf_se((45, 38), 5.0, seed=15), 1e-3,
+         dict(order="cubic", levels=4, anchor_stride=8, anchor_block=4),
+         dict(levels=4, anchor_stride=8, anchor_block=4), True),
+        ("block4_3d", lambda: fields.turbulence_jumps((21, 30, 19), seed=16), 5e-3,
+         dict(order="cubic", levels=3, anchor_stride=8, anchor_block=4, center=0, end_mode=3),
+         dict(levels=3, anchor_stride=8, anchor_block=4), True),
+        ("block2_4d", lambda: fields.grf_se((9, 8, 10, 7), 3.0, seed=17), 1e-2,
+         dict(order="cubic", levels=2, anchor_stride=4, anchor_block=2),
+         dict(levels=2, anchor_stride=4, anchor_block=2), True),
+        ("block3_2d_linear", lambda: fields.grf_se((33, 29), 4.0, seed=18), 2e-3,
+         dict(order="linear", levels=3, anchor_stride=8, anchor_block=3, center=0, end_mode=1),
+         dict(levels=3, anchor_stride=8, anchor_block=3), True),
     ]
 
 

@@ -81,6 +81,7 @@ def test_stage_codes_outliers_recon_bit_exact(name):
 
 
 @pytest.mark.parametrize("name", ["grf2d_128", "odd3d_c0_e1", "odd3d_c2_e3", "grf4d_default_center",
+                                  "block4_3d", "block3_2d_linear",
                                   "nan_inf_2d", "small_radius", "image_3ch", "turb3d_64_rel1e-4",
                                   "cfg1_512x512", "thin_17x1x9", "tiny_2x2"])
 @pytest.mark.parametrize("entropy", ["native", "compat"])

@@ -77,8 +77,11 @@ def test_plan_rejects_bad_parameters():
         levels.Plan((64, 64), 2, 16)
     with pytest.raises(ValueError):
         levels.Plan((), 2, 4)
-    with pytest.raises(NotImplementedError):
-        levels.Plan((64, 64), 3, 8, 4)
+    with pytest.raises(ValueError):
+        levels.Plan((64, 64), 3, 8, 9)  # block larger than the anchor stride
+    with pytest.raises(ValueError):
+        levels.Plan((64, 64), 3, 8, 0)
+    assert levels.Plan((64, 64), 3, 8, 4).counts[0] == 8 * 8 * 16  # 8 x 8 blocks of 4 x 4
 
 
 def test_stage_ebs_match_reference_schedule():
@@ -238,3 +241,26 @@ def test_plugin_stage_masks_are_the_reference_schedule():
         assert len(want) == len(plan)
         for t, (mask, _, _) in enumerate(want):
             assert np.array_equal(_stage_flat(plan, t), np.flatnonzero(mask))
+
+
+def test_blocked_anchor_schedule_is_the_reference_schedule():
+    """anchor_block > 1 (the anchors are anchor_block^ndim blocks on the anchor
+    lattice and the finer stages skip those points, latec/levels.py:114-147):
+    the plan's hole-aware rank -> point decode gives every stage's points in
+    the oracle masks' flat order, for power-of-two and other block edges."""
+    import numpy as np
+
+    from latec_b200 import levels
+    from latec_b200.codec import _stage_flat
+    from oracle import levels as olevels
+
+    for shape in [(37,), (19, 23), (9, 17, 20), (7, 9, 11, 6)]:
+        for st, lv in [(4, 2), (8, 3), (8, 4)]:
+            for block in (2, 3, 4, st):
+                plan = levels.plan_for(shape, lv, st, block)
+                masks = olevels.stage_masks(shape, lv, st, block)
+                assert len(masks) == len(plan)
+                for t, mask in enumerate(masks):
+                    assert plan.counts[t] == int(mask.sum())
+                    assert np.array_equal(_stage_flat(plan, t), np.flatnonzero(mask)), \
+                        (shape, st, lv, block, t)
