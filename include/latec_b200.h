@@ -67,7 +67,7 @@ typedef struct latec_stage_stats {
 typedef struct latec_rans_stage {
     uint64_t codes_off;   /* first code of the stage in the codes buffer */
     uint64_t out_off;     /* first outlier of the stage in the outlier buffer */
-    uint64_t enc;         /* device address: encoder symbol table (24 B/entry) */
+    uint64_t enc;         /* device address: encoder symbol table (32 B/entry) */
     uint64_t cdf;         /* device address: CDF rows (alphabet + 1 u32 each) */
     uint64_t bucket;      /* device address: decoder bucket rows (1024 u16 each) */
     uint64_t scratch_off; /* filled by the library */
@@ -197,7 +197,9 @@ int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
 
 /* ---- rANS tables: encoder symbols and decoder buckets for `rows` CDF rows
  *      of alphabet + 1 entries (latec/rans.py:304-329 tables, compiled the
- *      way latec/rans.py:629-657 compiles constriction models). */
+ *      way latec/rans.py:629-657 compiles constriction models). enc: device,
+ *      32 bytes per entry, rows * (alphabet + 1) entries; bucket: device,
+ *      1024 entries per row. Either may be NULL to skip it. */
 int latec_rans_build_tables(const uint32_t* cdf_rows, int32_t alphabet, int32_t rows, void* enc,
                             uint16_t* bucket, void* stream);
 

@@ -23,7 +23,7 @@ void count_launches(unsigned n) { g_launches.fetch_add(n, std::memory_order_rela
 
 static_assert(sizeof(latec_stage_stats) == sizeof(StageAcc), "stats layout");
 static_assert(sizeof(latec_rans_stage) == sizeof(RansStageDesc), "rans stage layout");
-static_assert(sizeof(EncSym) == 24, "encoder symbol layout");
+static_assert(sizeof(EncSym) == 32, "encoder symbol layout");
 
 namespace {
 

@@ -24,7 +24,10 @@ constexpr uint64_t LANE_L = 1ull << 31;
 // --------------------------------------------------------------- tables
 // Encoder symbol: x' = x + bias + mulhi(x, rcp) >> shift * cmpl  (Alverson
 // reciprocal division, exact for x < 2^63; freq == 1 uses rcp = 2^64 - 1,
-// shift 0, bias = start + M - 1).
+// shift 0, bias = start + M - 1). The single-stack coder divides by
+// Granlund-Montgomery (PLDI 1994, fig. 4.1, N = 64): with l = ceil(log2 freq)
+// and m' = floor(2^64 (2^l - freq) / freq) + 1, t = mulhi(m', x) and
+// x / freq = (t + ((x - t) >> min(l, 1))) >> max(l - 1, 0) for every 64-bit x.
 __global__ void k_build_enc(const uint32_t* __restrict__ cdf, int alphabet,
                             EncSym* __restrict__ enc) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -33,18 +36,23 @@ __global__ void k_build_enc(const uint32_t* __restrict__ cdf, int alphabet,
     EncSym e;
     e.freq = freq;
     e.cmpl = (1u << PREC) - freq;
+    e.pad = 0;
+    uint32_t l = 0;
+    while (freq > (1u << l)) l++;
     if (freq < 2) {
         e.rcp = ~0ull;
         e.shift = 0;
         e.bias = start + (1u << PREC) - 1u;
     } else {
-        uint32_t sh = 0;
-        while (freq > (1u << sh)) sh++;
-        const unsigned __int128 num = ((unsigned __int128)1 << (sh + 63)) + (freq - 1);
+        const unsigned __int128 num = ((unsigned __int128)1 << (l + 63)) + (freq - 1);
         e.rcp = (uint64_t)(num / freq);
-        e.shift = sh - 1;
+        e.shift = (uint8_t)(l - 1);
         e.bias = start;
     }
+    const unsigned __int128 gnum = (unsigned __int128)((1ull << l) - (freq ? freq : 1)) << 64;
+    e.gm = (uint64_t)(gnum / (freq ? freq : 1)) + 1ull;
+    e.gsh1 = (uint8_t)(l < 1 ? l : 1);
+    e.gsh2 = (uint8_t)(l > 1 ? l - 1 : 0);
     enc[s] = e;
 }
 
@@ -134,7 +142,7 @@ __global__ void __launch_bounds__(128)
         for (int u = 0; u < ENC_U; u++) {
             const int kk = k - u;
             const uint64_t i = base + (uint64_t)(kk < 0 ? 0 : kk) * 32u + lane;
-            e[u] = EncSym{0, 0, 0, 0, 0};
+            e[u] = EncSym{};
             if (kk >= 0 && i < d.n) {
                 const uint32_t sym = narrow(cc[u], d.radius, d.kexp);
                 if (sym >= d.alphabet) {
@@ -279,34 +287,85 @@ __global__ void __launch_bounds__(32 * DEC_WARPS)
 }
 
 // --------------------------------------------------------------- compat
+// One thread per stage (lane 0 of the stage's own CTA, so that stages never
+// share a warp and diverge against each other) codes the whole stage in
+// reverse. The state chain is serial, so everything off it is fetched ahead:
+// the codes (and scale levels) two groups of SG symbols ahead, the encoder
+// entries one group ahead.
+constexpr int SG = 8;
+
 __global__ void k_stack_encode(const RansStageDesc* __restrict__ st, int n_stages,
                                const uint16_t* __restrict__ codes, const uint8_t* __restrict__ levels,
                                uint32_t* __restrict__ scratch, uint32_t* __restrict__ stage_words,
                                uint32_t* __restrict__ err) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_stages) return;
+    const int t = blockIdx.x;
+    if (t >= n_stages || threadIdx.x != 0) return;
     const RansStageDesc& d = st[t];
     if (d.mode != MODE_COMPAT) return;
-    const uint32_t* cdfs = (const uint32_t*)d.cdf;
+    const EncSym* enc = (const EncSym*)d.enc;
     const uint32_t alpha1 = d.alphabet + 1;
     const uint16_t* c = codes + d.codes_off;
     const uint8_t* lv = d.per_point ? levels + d.codes_off : nullptr;
     uint32_t* out = scratch + d.scratch_off;
+    const int64_t n = d.n;
+    uint16_t nc[SG];
+    uint8_t nr[SG];
+    EncSym ne[SG];
+    bool bad = false;
+    // codes of the group whose highest index is `top`
+    auto fetch_codes = [&](int64_t top) {
+#pragma unroll
+        for (int u = 0; u < SG; u++) {
+            const int64_t j = top - u;
+            nc[u] = j >= 0 ? c[j] : (uint16_t)0;
+            nr[u] = (j >= 0 && lv) ? lv[j] : (uint8_t)0;
+        }
+    };
+    // encoder entries of the codes in nc / nr
+    auto fetch_entries = [&](int64_t top) {
+#pragma unroll
+        for (int u = 0; u < SG; u++) {
+            ne[u] = EncSym{};
+            if (top - u >= 0) {
+                const uint32_t sym = narrow(nc[u], d.radius, d.kexp);
+                bad |= sym >= d.alphabet;
+                ne[u] = enc[(uint64_t)nr[u] * alpha1 + (sym < d.alphabet ? sym : 0u)];
+            }
+        }
+    };
     uint64_t x = 0;
     uint64_t w = 0;
-    for (int64_t i = (int64_t)d.n - 1; i >= 0; i--) {
-        const uint32_t sym = narrow(c[i], d.radius, d.kexp);
-        if (sym >= d.alphabet) {
-            atomicOr(err, 2u);
-            return;
+    if (n > 0) {
+        fetch_codes(n - 1);
+        fetch_entries(n - 1);
+        fetch_codes(n - 1 - SG);
+    }
+    for (int64_t top = n - 1; top >= 0; top -= SG) {
+        EncSym e[SG];
+#pragma unroll
+        for (int u = 0; u < SG; u++) e[u] = ne[u];
+        if (top - SG >= 0) {
+            fetch_entries(top - SG);
+            if (top - 2 * SG >= 0) fetch_codes(top - 2 * SG);
         }
-        const uint32_t* cdf = cdfs + (uint64_t)(lv ? lv[i] : 0u) * alpha1;
-        const uint32_t left = cdf[sym], p = cdf[sym + 1] - left;
-        if ((x >> (64 - PREC)) >= p) {
-            out[w++] = (uint32_t)x;
-            x >>= 32;
+        if (bad) break;
+#pragma unroll
+        for (int u = 0; u < SG; u++) {
+            if (top - u < 0) break;
+            const uint32_t p = e[u].freq;
+            const uint32_t left = p == 1u ? e[u].bias - ((1u << PREC) - 1u) : e[u].bias;
+            if ((x >> (64 - PREC)) >= p) {
+                out[w++] = (uint32_t)x;
+                x >>= 32;
+            }
+            const uint64_t t1 = __umul64hi(x, e[u].gm);
+            const uint64_t q = (t1 + ((x - t1) >> e[u].gsh1)) >> e[u].gsh2;
+            x = (q << PREC) | (uint64_t)((uint32_t)(x - q * p) + left);
         }
-        x = ((x / p) << PREC) | (uint64_t)((uint32_t)(x % p) + left);
+    }
+    if (bad) {
+        atomicOr(err, 2u);
+        return;
     }
     if (x >> 32) {
         out[w++] = (uint32_t)x;
@@ -317,11 +376,14 @@ __global__ void k_stack_encode(const RansStageDesc* __restrict__ st, int n_stage
     stage_words[t] = (uint32_t)w;
 }
 
+// One thread per stage (lane 0 of the stage's own CTA). The next blob word
+// and the scale levels are loaded ahead of their use; the state chain is the
+// bucket and CDF lookups of the slot.
 __global__ void k_stack_decode(const RansStageDesc* __restrict__ st, int n_stages,
                                const uint32_t* __restrict__ words, const uint8_t* __restrict__ levels,
                                uint16_t* __restrict__ codes, uint32_t* __restrict__ err) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n_stages) return;
+    const int t = blockIdx.x;
+    if (t >= n_stages || threadIdx.x != 0) return;
     const RansStageDesc& d = st[t];
     if (d.mode != MODE_COMPAT || d.n == 0) return;
     const uint32_t* cdfs = (const uint32_t*)d.cdf;
@@ -338,17 +400,37 @@ __global__ void k_stack_decode(const RansStageDesc* __restrict__ st, int n_stage
         x = (x << 32) | wd[--top];
         if (x >> 32) break;
     }
+    uint32_t nw = top > 0 ? wd[top - 1] : 0u;  // the next word, loaded ahead
     const uint8_t* lv = d.per_point ? levels + d.codes_off : nullptr;
     uint16_t* out = codes + d.codes_off;
-    for (uint64_t i = 0; i < d.n; i++) {
-        const uint32_t row = lv ? lv[i] : 0u;
-        const uint32_t* cdf = cdfs + (uint64_t)row * alpha1;
-        const uint32_t q = (uint32_t)(x & PMASK);
-        const uint32_t s = lookup_sym(cdf, buckets + (uint64_t)row * NBUCKET, q, d.alphabet);
-        const uint32_t left = cdf[s], p = cdf[s + 1] - left;
-        x = (x >> PREC) * p + (q - left);
-        if (x < (1ull << 32) && top > 0) x = (x << 32) | wd[--top];
-        out[i] = (uint16_t)widen(s, d.radius, d.kexp);
+    const uint64_t n = d.n;
+    uint8_t rows[SG];
+#pragma unroll
+    for (int u = 0; u < SG; u++) rows[u] = (lv && (uint64_t)u < n) ? lv[u] : (uint8_t)0;
+    for (uint64_t i0 = 0; i0 < n; i0 += SG) {
+        uint8_t cur[SG];
+#pragma unroll
+        for (int u = 0; u < SG; u++) {
+            cur[u] = rows[u];
+            rows[u] = (lv && i0 + SG + u < n) ? lv[i0 + SG + u] : (uint8_t)0;
+        }
+#pragma unroll
+        for (int u = 0; u < SG; u++) {
+            const uint64_t i = i0 + u;
+            if (i >= n) break;
+            const uint32_t row = cur[u];
+            const uint32_t* cdf = cdfs + (uint64_t)row * alpha1;
+            const uint32_t q = (uint32_t)(x & PMASK);
+            const uint32_t s = lookup_sym(cdf, buckets + (uint64_t)row * NBUCKET, q, d.alphabet);
+            const uint32_t left = cdf[s], p = cdf[s + 1] - left;
+            x = (x >> PREC) * p + (q - left);
+            if (x < (1ull << 32) && top > 0) {
+                x = (x << 32) | nw;
+                --top;
+                nw = top > 0 ? wd[top - 1] : 0u;
+            }
+            out[i] = (uint16_t)widen(s, d.radius, d.kexp);
+        }
     }
     if (top != 0 || x != 0) atomicOr(err, 16u);
 }
@@ -505,7 +587,7 @@ int launch_stack_encode(const RansStageDesc* st, int n_stages, const uint16_t* c
                         const uint8_t* levels, uint32_t* scratch, uint32_t* stage_words,
                         uint32_t* err, cudaStream_t s) {
     if (!n_stages) return LATEC_OK;
-    k_stack_encode<<<(n_stages + 31) / 32, 32, 0, s>>>(st, n_stages, codes, levels, scratch,
+    k_stack_encode<<<n_stages, 32, 0, s>>>(st, n_stages, codes, levels, scratch,
                                                         stage_words, err);
     return last_err();
 }
@@ -513,7 +595,7 @@ int launch_stack_encode(const RansStageDesc* st, int n_stages, const uint16_t* c
 int launch_stack_decode(const RansStageDesc* st, int n_stages, const uint32_t* words,
                         const uint8_t* levels, uint16_t* codes, uint32_t* err, cudaStream_t s) {
     if (!n_stages) return LATEC_OK;
-    k_stack_decode<<<(n_stages + 31) / 32, 32, 0, s>>>(st, n_stages, words, levels, codes, err);
+    k_stack_decode<<<n_stages, 32, 0, s>>>(st, n_stages, words, levels, codes, err);
     return last_err();
 }
 

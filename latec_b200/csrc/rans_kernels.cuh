@@ -11,12 +11,20 @@ constexpr int NBUCKET = 1 << BUCKET_BITS;
 constexpr int MODE_LANES = 0;
 constexpr int MODE_COMPAT = 1;
 
+// Encoder entry of one symbol (32 bytes). The lane coder divides by the
+// frequency with rcp / shift (exact below 2^63); the single-stack coder, whose
+// state spans all 64 bits, with the Granlund-Montgomery multiplier gm and the
+// shifts gsh1 / gsh2 (exact for every 64-bit state).
 struct EncSym {
     uint64_t rcp;
+    uint64_t gm;
     uint32_t bias;
     uint32_t cmpl;
     uint32_t freq;
-    uint32_t shift;
+    uint8_t shift;
+    uint8_t gsh1;
+    uint8_t gsh2;
+    uint8_t pad;
 };
 
 // One stage of the entropy stage, shared layout with the host (see capi.cu;

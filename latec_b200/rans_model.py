@@ -29,6 +29,7 @@ SEG = 1 << 22          # the reference accumulates its float32 histogram per 2^2
 HWIN = 256             # device histogram window (|q| < HWIN), see interp_kernels.cuh
 LITERAL_MIN = 1 << 12
 NBUCKET = 1 << 10      # decoder bucket table entries per CDF row (rans_kernels.cuh)
+ENC_BYTES = 32          # encoder entry per symbol (EncSym in rans_kernels.cuh)
 LITERAL_SCOUT_SLACK = 0.85
 
 # Native lane coder chunking: keep the 64-bit final lane states under ~1/64 of
@@ -290,7 +291,7 @@ class DeviceTables:
         alphabet = rows.shape[1] - 1
         dev = torch.device(device) if device is not None else torch.device("cuda")
         cdf = torch.from_numpy(np.ascontiguousarray(rows)).to(dev)
-        enc = torch.empty(rows.shape[0] * (alphabet + 1) * 24, dtype=torch.uint8, device=dev)
+        enc = torch.empty(rows.shape[0] * (alphabet + 1) * ENC_BYTES, dtype=torch.uint8, device=dev)
         bucket = torch.empty(rows.shape[0] * NBUCKET, dtype=torch.int16, device=dev)
         lib = _lib.load()
         _lib.check(lib.latec_rans_build_tables(cdf.data_ptr(), alphabet, rows.shape[0],
