@@ -51,8 +51,8 @@ Scope of this version:
 
 ``fp8=True`` (an extension) runs those MLPs in FP8 (E4M3) with per-channel
 weight and per-row activation scales instead. Streams carry their
-``"float_path"`` (``latec_b200-bf16-1``, ``latec_b200-fp8-1`` or
-``latec_b200-f32-1``). As the reference's own encoder/decoder contract
+``"float_path"`` (``latec_b200-bf16-3``, ``latec_b200-fp8-2`` or
+``latec_b200-f32-2``). As the reference's own encoder/decoder contract
 requires, they decode only with that float path.
 """
 
@@ -72,8 +72,8 @@ MAGIC = b"LATECGNN"
 VERSION = 14
 PREFIX = "<8sII"
 PREFIX_SIZE = struct.calcsize(PREFIX)
-FLOAT_PATHS = {"f32": "latec_b200-f32-1", "bf16": "latec_b200-bf16-2",
-               "fp8": "latec_b200-fp8-1"}
+FLOAT_PATHS = {"f32": "latec_b200-f32-2", "bf16": "latec_b200-bf16-3",
+               "fp8": "latec_b200-fp8-2"}
 AUTO_CHUNK_THRESHOLD = 1 << 21
 RANK_LEVELS = {2: 8, 4: 5, 5: 4}
 EB_COARSE_FACTOR = 0.9
@@ -553,7 +553,10 @@ class GNNCodec:
         prev, ctx, vals = None, None, None
         for gi, (g, seb) in enumerate(zip(geoms, ebs)):
             n = B * g.M
-            if interp_kind:
+            if gi == 0 or interp_kind:
+                # the anchor stage is coded against 0 with a flat scale of its
+                # eb, before the model runs (latec/gnn_codec.py:358-373); the
+                # first model stage embeds the anchors from their reconstruction
                 mu, scale = self._interp_stage(plan, pstages[gi], gi, interp_kind, recon_all, n,
                                                seb, radius)
             else:
@@ -814,7 +817,7 @@ class GNNCodec:
         ch0 = np.concatenate([[0], np.cumsum([r[6] for r in recs])]).astype(np.int64)
         fine_desc = None
         for gi, (g, seb) in enumerate(zip(geoms, ebs)):
-            if interp_kind:
+            if gi == 0 or interp_kind:  # the anchors: against 0, as the encoder
                 mu, scale = self._interp_stage(plan, pstages[gi], gi, interp_kind, recon_all,
                                                B * g.M, seb, radius)
             else:

@@ -312,12 +312,12 @@ def test_interpolation_ablation_on_a_chunk_grid():
 
 @pytest.mark.gpu
 def test_fp8_float_path_round_trip():
-    from latec_b200.gnn_codec import read_stream
+    from latec_b200.gnn_codec import FLOAT_PATHS, read_stream
 
     codec = _codec()
     x = _field((40, 36), 4)
     s = codec.compress(x, 1e-3, levels=3, fp8=True)
-    assert read_stream(s)[0]["float_path"] == "latec_b200-fp8-1"
+    assert read_stream(s)[0]["float_path"] == FLOAT_PATHS["fp8"]
     assert codec.compress(x, 1e-3, levels=3, fp8=True) == s
     out = codec.uncompress(s).numpy()
     vmin, vmax = float(np.float32(x.min())), float(np.float32(x.max()))
