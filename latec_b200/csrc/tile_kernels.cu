@@ -52,8 +52,17 @@
 namespace latec {
 namespace {
 
-constexpr int LT = 256;       // threads per CTA
-constexpr int LW = LT / 32;   // warps per CTA
+// Threads per CTA of the encode and decode kernels (two CTAs per SM each):
+// 20 and 24 warps per SM, the most each kernel's registers allow (measured:
+// more resident warps hide more of the per-point dependency chains).
+constexpr int LT_ENC = 320;
+constexpr int LT_DEC = 384;
+template <bool ENC>
+struct Thr {
+    static constexpr int T = ENC ? LT_ENC : LT_DEC;  // threads
+    static constexpr int W = T / 32;                 // warps
+};
+constexpr int LW_ENC = Thr<true>::W, LW_DEC = Thr<false>::W;
 constexpr int MAXT = 8;       // warp tasks of one phase at most (decode code prefetch)
 constexpr uint32_t LOAD_WAIT_LIMIT = 1u << 24;  // polls of a plane load before giving up
 
@@ -88,6 +97,7 @@ struct Lay {
     static constexpr uint32_t HIST = al128(RS + (ENC ? Gm::RR * Gm::BX * sizeof(T) : 0));
     static constexpr uint32_t WACC =
         al128(HIST + (ENC ? sizeof(uint32_t) * TILE_STAGES * HBINS : 0));
+    static constexpr int LW = Thr<ENC>::W;
     static constexpr uint32_t WMQ = WACC + (ENC ? sizeof(double) * LW * TILE_STAGES * 5 : 0);
     static constexpr uint32_t WNO = WMQ + (ENC ? sizeof(uint32_t) * LW * TILE_STAGES : 0);
     // decode: per warp, two buffers of MAXT tasks x 32 lanes of 16-bit codes
@@ -373,6 +383,18 @@ __device__ __forceinline__ bool owned_pos(const Pt& p) {
            (C::XO || (p.col >= 2 && p.col <= Gm::TX / 2 + 1));
 }
 
+// The shared bins of one stage added to its segment's global bins (and
+// cleared), by all threads of an encode CTA.
+__device__ __forceinline__ void lvl_flush_hist(uint32_t* sh_hist, uint32_t* hist_seg, uint32_t seg) {
+    for (int b = threadIdx.x; b < HBINS; b += LT_ENC) {
+        const uint32_t v = sh_hist[b];
+        if (v) {
+            atomicAdd(&hist_seg[(size_t)seg * HBINS + b], v);
+            sh_hist[b] = 0;
+        }
+    }
+}
+
 // ------------------------------------------------------------ encode state
 template <typename T>
 struct TAcc {
@@ -489,7 +511,7 @@ __device__ __forceinline__ void enc_phase(const TileLevel& L, const LvRanks& rk,
     const int na = ea ? ntasks<T, CA>() : 0, nb = eb ? ntasks<T, CB>() : 0;
     const int nc = ec ? ntasks<T, CC>() : 0;
     const int tot = na + nb + nc, w = threadIdx.x >> 5;
-    const int tb = w * tot / LW, te = (w + 1) * tot / LW;
+    const int tb = w * tot / LW_ENC, te = (w + 1) * tot / LW_ENC;
     for (int t = tb; t < te; t++) {
         if (t < na) {
             if constexpr (CA != C_NONE) enc_task<T, CUBIC, CA>(L, rk, it, u, t, sm, cseg, a);
@@ -550,7 +572,7 @@ __device__ __forceinline__ void fetch_phase(const TileLevel& L, const LvRanks& r
     int na, nb, nc;
     phase_counts<T>(ph, u.ev, u.ov, na, nb, nc);
     const int tot = na + nb + nc, w = threadIdx.x >> 5;
-    const int tb = w * tot / LW, te = (w + 1) * tot / LW;
+    const int tb = w * tot / LW_DEC, te = (w + 1) * tot / LW_DEC;
 #pragma unroll
     for (int k = 0; k < MAXT; k++) {
         const int t = tb + k;
@@ -578,7 +600,7 @@ __device__ __forceinline__ void dec_phase(const TileLevel& L, const Item& it, co
     const int na = ea ? ntasks<T, CA>() : 0, nb = eb ? ntasks<T, CB>() : 0;
     const int nc = ec ? ntasks<T, CC>() : 0;
     const int tot = na + nb + nc, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tb = w * tot / LW, te = (w + 1) * tot / LW;
+    const int tb = w * tot / LW_DEC, te = (w + 1) * tot / LW_DEC;
     for (int t = tb; t < te; t++) {
         const uint32_t code = wcodes[(t - tb) * 32 + lane];
         if (t < na) {
@@ -619,7 +641,7 @@ __device__ __forceinline__ bool issue_loads(const CUtensorMap* tmx, const CUtens
     }
     auto box = [&](T* dst, const T* base, int z, int ystep, int rows) {
         const int64_t zo = it.cbase + (int64_t)z * L.ls[0];
-        for (int e = threadIdx.x; e < rows * Gm::BX; e += LT) {
+        for (int e = threadIdx.x; e < rows * Gm::BX; e += Thr<ENC>::T) {
             const int r = e / Gm::BX, b = e - (e / Gm::BX) * Gm::BX;
             const int Y = it.y0 - 2 + r * ystep, X = it.x0 - 4 + b;
             const bool in = Y >= 0 && Y < L.N[1] && X >= 0 && X < L.N[2];
@@ -638,11 +660,11 @@ __device__ __forceinline__ bool issue_loads(const CUtensorMap* tmx, const CUtens
 
 // Staging (natural layout) -> slot (parity-split layout). For an encoded even
 // plane the coarse points (even y, even x) come from the canvas rows in RS.
-template <typename T>
+template <typename T, int NT>
 __device__ __forceinline__ void transpose_plane(T* slot, const T* SX, const T* SR) {
     using Gm = G<T>;
     constexpr int ROWS = Gm::NER + Gm::NOR;
-    for (int e = threadIdx.x; e < ROWS * Gm::GPR; e += LT) {
+    for (int e = threadIdx.x; e < ROWS * Gm::GPR; e += NT) {
         const int i = e / Gm::GPR, g = e - (e / Gm::GPR) * Gm::GPR;
         const bool even = i < Gm::NER;
         const int ri = even ? i : i - Gm::NER;
@@ -669,14 +691,14 @@ __device__ __forceinline__ void transpose_plane(T* slot, const T* SX, const T* S
 // Write the tile of an owned plane from its slot to the canvas (16-byte
 // groups on the TMA path, whose rows are whole groups; else element by
 // element, skipping the coarse points of even planes).
-template <typename T, int TMA>
+template <typename T, int TMA, int NT>
 __device__ __forceinline__ void store_plane(const TileLevel& L, const Item& it, int z,
                                             const T* slot, T* __restrict__ canvas) {
     using Gm = G<T>;
     const int64_t zo = it.cbase + (int64_t)z * L.ls[0];
     if (TMA) {
         constexpr int GT = Gm::TX / Gm::VEC;
-        for (int e = threadIdx.x; e < Gm::TY * GT; e += LT) {
+        for (int e = threadIdx.x; e < Gm::TY * GT; e += NT) {
             const int r = e / GT, g = e - (e / GT) * GT;
             const int y = it.y0 + r, x = it.x0 + g * Gm::VEC;
             if (y >= L.N[1] || x >= L.N[2]) continue;
@@ -695,7 +717,7 @@ __device__ __forceinline__ void store_plane(const TileLevel& L, const Item& it, 
         return;
     }
     const bool evenz = !(z & 1);
-    for (int e = threadIdx.x; e < Gm::TY * Gm::TX; e += LT) {
+    for (int e = threadIdx.x; e < Gm::TY * Gm::TX; e += NT) {
         const int r = e / Gm::TX, b = e - (e / Gm::TX) * Gm::TX;
         const int y = it.y0 + r, x = it.x0 + b;
         if (y >= L.N[1] || x >= L.N[2]) continue;
@@ -758,15 +780,15 @@ struct Cursor {
 // slots. Within an item the two touch different slots; the first unit of an
 // item may reuse the slot of the previous item's last plane, so those stores
 // finish first.
-template <typename T, int TMA>
+template <typename T, int TMA, int NT>
 __device__ __forceinline__ void phase0(const TileLevel& L, const Item& prev, int st_e, int st_o,
                                        const Unit<T>& u, bool first, bool pending, uint32_t bar,
                                        uint32_t& parity, bool& wait_failed, T* slots, const T* XE,
                                        const T* XO, const T* RS, T* canvas) {
     const bool out = st_e >= 0 || st_o >= 0;
     if (out && first) {
-        if (st_e >= 0) store_plane<T, TMA>(L, prev, st_e, slot_of(slots, st_e), canvas);
-        if (st_o >= 0) store_plane<T, TMA>(L, prev, st_o, slot_of(slots, st_o), canvas);
+        if (st_e >= 0) store_plane<T, TMA, NT>(L, prev, st_e, slot_of(slots, st_e), canvas);
+        if (st_o >= 0) store_plane<T, TMA, NT>(L, prev, st_o, slot_of(slots, st_o), canvas);
         __syncthreads();
     }
     if (pending) {
@@ -778,16 +800,16 @@ __device__ __forceinline__ void phase0(const TileLevel& L, const Item& prev, int
             __syncthreads();
         }
     }
-    if (u.ev) transpose_plane<T>(u.E, XE, RS);
-    if (u.ov) transpose_plane<T>(u.O, XO, nullptr);
+    if (u.ev) transpose_plane<T, NT>(u.E, XE, RS);
+    if (u.ov) transpose_plane<T, NT>(u.O, XO, nullptr);
     if (out && !first) {
-        if (st_e >= 0) store_plane<T, TMA>(L, prev, st_e, slot_of(slots, st_e), canvas);
-        if (st_o >= 0) store_plane<T, TMA>(L, prev, st_o, slot_of(slots, st_o), canvas);
+        if (st_e >= 0) store_plane<T, TMA, NT>(L, prev, st_e, slot_of(slots, st_e), canvas);
+        if (st_o >= 0) store_plane<T, TMA, NT>(L, prev, st_o, slot_of(slots, st_o), canvas);
     }
 }
 
 template <typename T, int CUBIC, int TMA>
-__global__ void __launch_bounds__(LT, 2)
+__global__ void __launch_bounds__(LT_ENC, 2)
     k_lvl_enc(const __grid_constant__ CUtensorMap tmx, const __grid_constant__ CUtensorMap tmr,
               const TileLevel L, const T* __restrict__ x, T* __restrict__ recon) {
     using Gm = G<T>;
@@ -803,9 +825,9 @@ __global__ void __launch_bounds__(LT, 2)
     sm.wmq = (uint32_t*)(smem + Ly::WMQ);
     sm.wno = (uint32_t*)(smem + Ly::WNO);
     const uint32_t bar = su32(smem + Ly::MBAR);
-    for (int i = threadIdx.x; i < TILE_STAGES * HBINS; i += LT) sm.hist[i] = 0;
-    for (int i = threadIdx.x; i < LW * TILE_STAGES * 5; i += LT) sm.wacc[i] = 0.0;
-    for (int i = threadIdx.x; i < LW * TILE_STAGES; i += LT) sm.wmq[i] = sm.wno[i] = 0u;
+    for (int i = threadIdx.x; i < TILE_STAGES * HBINS; i += LT_ENC) sm.hist[i] = 0;
+    for (int i = threadIdx.x; i < LW_ENC * TILE_STAGES * 5; i += LT_ENC) sm.wacc[i] = 0.0;
+    for (int i = threadIdx.x; i < LW_ENC * TILE_STAGES; i += LT_ENC) sm.wmq[i] = sm.wno[i] = 0u;
     if (threadIdx.x == 0) mbar_init(bar);
     __syncthreads();
     LvRanks rk;
@@ -831,7 +853,7 @@ __global__ void __launch_bounds__(LT, 2)
     }
     while (cur.item < L.items) {
         const Unit<T> u = make_unit(slots, it, cur.u, nz);
-        phase0<T, TMA>(L, prev, st_e, st_o, u, cur.u == 0, pending, bar, parity, wait_failed,
+        phase0<T, TMA, LT_ENC>(L, prev, st_e, st_o, u, cur.u == 0, pending, bar, parity, wait_failed,
                        slots, XE, XO, RS, recon);
         // histogram segments of this unit's stages (uniform decisions)
 #pragma unroll
@@ -839,7 +861,7 @@ __global__ void __launch_bounds__(LT, 2)
             const uint32_t ns = unit_seg(L, rk, it, u, s);
             if (ns != 0xffffffffu && ns != cseg[s]) {
                 if (cseg[s] != 0xffffffffu)
-                    flush_hist(sm.hist + s * HBINS, L.st[s].hist_seg, cseg[s]);
+                    lvl_flush_hist(sm.hist + s * HBINS, L.st[s].hist_seg, cseg[s]);
                 cseg[s] = ns;
             }
         }
@@ -871,8 +893,8 @@ __global__ void __launch_bounds__(LT, 2)
         cur = nxt;
         it = nit;
     }
-    if (st_e >= 0) store_plane<T, TMA>(L, prev, st_e, slot_of(slots, st_e), recon);
-    if (st_o >= 0) store_plane<T, TMA>(L, prev, st_o, slot_of(slots, st_o), recon);
+    if (st_e >= 0) store_plane<T, TMA, LT_ENC>(L, prev, st_e, slot_of(slots, st_e), recon);
+    if (st_o >= 0) store_plane<T, TMA, LT_ENC>(L, prev, st_o, slot_of(slots, st_o), recon);
     warp_flush(a, sm);
     if (TMA && wait_failed) {  // let a late load land before the CTA exits
         mbar_wait(bar, parity ^ 1u);
@@ -881,13 +903,13 @@ __global__ void __launch_bounds__(LT, 2)
     __syncthreads();
 #pragma unroll
     for (int s = 0; s < TILE_STAGES; s++)
-        if (cseg[s] != 0xffffffffu) flush_hist(sm.hist + s * HBINS, L.st[s].hist_seg, cseg[s]);
+        if (cseg[s] != 0xffffffffu) lvl_flush_hist(sm.hist + s * HBINS, L.st[s].hist_seg, cseg[s]);
     // per stage: the warps' sums in warp order (deterministic), one partial row per CTA
     if (threadIdx.x < TILE_STAGES) {
         const int s = threadIdx.x;
         double t[5] = {0, 0, 0, 0, 0};
         uint32_t mq = 0, no = 0;
-        for (int w = 0; w < LW; w++) {
+        for (int w = 0; w < LW_ENC; w++) {
             const double* sl = sm.wacc + (w * TILE_STAGES + s) * 5;
             for (int k = 0; k < 4; k++) t[k] += sl[k];
             t[4] = fmax(t[4], sl[4]);
@@ -901,7 +923,7 @@ __global__ void __launch_bounds__(LT, 2)
 }
 
 template <typename T, int CUBIC, int TMA>
-__global__ void __launch_bounds__(LT, 2)
+__global__ void __launch_bounds__(LT_DEC, 2)
     k_lvl_dec(const __grid_constant__ CUtensorMap tmx, const TileLevel L, T* __restrict__ recon,
               uint32_t* __restrict__ err) {
     using Gm = G<T>;
@@ -911,7 +933,7 @@ __global__ void __launch_bounds__(LT, 2)
     T* XE = (T*)(smem + Ly::XE);
     T* XO = (T*)(smem + Ly::XO);
     // this warp's two buffers of MAXT tasks x 32 codes (Ly::CODE_ENTRIES in all)
-    static_assert(Ly::CODE_ENTRIES == LW * 2 * MAXT * 32, "code buffer layout");
+    static_assert(Ly::CODE_ENTRIES == LW_DEC * 2 * MAXT * 32, "code buffer layout");
     uint16_t* wc = (uint16_t*)(smem + Ly::CODES) + (threadIdx.x >> 5) * 2 * MAXT * 32;
     const uint32_t bar = su32(smem + Ly::MBAR);
     if (threadIdx.x == 0) mbar_init(bar);
@@ -940,7 +962,7 @@ __global__ void __launch_bounds__(LT, 2)
     }
     while (cur.item < L.items) {
         const Unit<T> u = make_unit(slots, it, cur.u, nz);
-        phase0<T, TMA>(L, prev, st_e, st_o, u, cur.u == 0, pending, bar, parity, wait_failed,
+        phase0<T, TMA, LT_DEC>(L, prev, st_e, st_o, u, cur.u == 0, pending, bar, parity, wait_failed,
                        slots, XE, XO, nullptr, recon);
         __syncthreads();
         Cursor nxt = cur;
@@ -986,8 +1008,8 @@ __global__ void __launch_bounds__(LT, 2)
         cur = nxt;
         it = nit;
     }
-    if (st_e >= 0) store_plane<T, TMA>(L, prev, st_e, slot_of(slots, st_e), recon);
-    if (st_o >= 0) store_plane<T, TMA>(L, prev, st_o, slot_of(slots, st_o), recon);
+    if (st_e >= 0) store_plane<T, TMA, LT_DEC>(L, prev, st_e, slot_of(slots, st_e), recon);
+    if (st_o >= 0) store_plane<T, TMA, LT_DEC>(L, prev, st_o, slot_of(slots, st_o), recon);
     if (TMA && wait_failed) {
         mbar_wait(bar, parity ^ 1u);
         if (threadIdx.x == 0) atomicOr(err, ERR_TILE_WAIT);
@@ -1039,10 +1061,10 @@ static int launch_enc(const TileLevel& L, uint32_t grid, const void* x, void* re
         if (!make_map<T>(&mx, L, x, 1, G<T>::XR) || !make_map<T>(&mr, L, recon, 2, G<T>::RR))
             return LATEC_ERR_CUDA;
         if ((rc = set_smem(k_lvl_enc<T, CUBIC, 1>, bytes))) return rc;
-        k_lvl_enc<T, CUBIC, 1><<<grid, LT, bytes, st>>>(mx, mr, L, (const T*)x, (T*)recon);
+        k_lvl_enc<T, CUBIC, 1><<<grid, LT_ENC, bytes, st>>>(mx, mr, L, (const T*)x, (T*)recon);
     } else {
         if ((rc = set_smem(k_lvl_enc<T, CUBIC, 0>, bytes))) return rc;
-        k_lvl_enc<T, CUBIC, 0><<<grid, LT, bytes, st>>>(mx, mr, L, (const T*)x, (T*)recon);
+        k_lvl_enc<T, CUBIC, 0><<<grid, LT_ENC, bytes, st>>>(mx, mr, L, (const T*)x, (T*)recon);
     }
     count_launches(1);
     return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
@@ -1058,10 +1080,10 @@ static int launch_dec(const TileLevel& L, uint32_t grid, void* recon, uint32_t* 
     if (L.tma) {
         if (!make_map<T>(&mx, L, recon, 1, G<T>::XR)) return LATEC_ERR_CUDA;
         if ((rc = set_smem(k_lvl_dec<T, CUBIC, 1>, bytes))) return rc;
-        k_lvl_dec<T, CUBIC, 1><<<grid, LT, bytes, st>>>(mx, L, (T*)recon, err);
+        k_lvl_dec<T, CUBIC, 1><<<grid, LT_DEC, bytes, st>>>(mx, L, (T*)recon, err);
     } else {
         if ((rc = set_smem(k_lvl_dec<T, CUBIC, 0>, bytes))) return rc;
-        k_lvl_dec<T, CUBIC, 0><<<grid, LT, bytes, st>>>(mx, L, (T*)recon, err);
+        k_lvl_dec<T, CUBIC, 0><<<grid, LT_DEC, bytes, st>>>(mx, L, (T*)recon, err);
     }
     count_launches(1);
     return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;

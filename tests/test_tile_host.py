@@ -32,7 +32,7 @@ W1Y, W1X, W2E, W1Z, W2ZY, W2ZX, W3 = range(7)
 CLS = {W1Y: (0, 1, 0, 1), W1X: (0, 0, 1, 2), W2E: (0, 1, 1, 3), W1Z: (1, 0, 0, 0),
        W2ZY: (1, 1, 0, 3), W2ZX: (1, 0, 1, 3), W3: (1, 1, 1, 4)}
 PHASES = [(W1Y, W1X, W1Z), (W2E, W2ZY, W2ZX), (W3,)]
-LW, MAXT = 8, 8
+LW, MAXT = 12, 8
 
 
 class Geo:
