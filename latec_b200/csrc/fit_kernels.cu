@@ -81,7 +81,13 @@ __global__ void __launch_bounds__(256)
         const uint32_t a0 = warp * span;
         for (uint32_t base = a0; base < a0 + span; base += 32) {
             const uint32_t i = base + lane;
-            double v = (lane < (int)width) ? __dmul_rn((double)W[i], (double)cnt[i]) : 0.0;
+            // every term is >= +0 (weights are -log2 p, counts are counts): a
+            // run of zero counts sums to exactly +0.0, so its weights need no
+            // load (the histogram is narrow; the weight tables are not)
+            const uint32_t c = (lane < (int)width) ? cnt[i] : 0u;
+            double v = 0.0;
+            if (__any_sync(0xffffffffu, c != 0u))
+                v = (lane < (int)width) ? __dmul_rn((double)W[i], (double)c) : 0.0;
             for (uint32_t st = 1; st < width; st <<= 1) {
                 const double o = __shfl_down_sync(0xffffffffu, v, st);
                 if ((lane & (2 * st - 1)) == 0) v = __dadd_rn(v, o);

@@ -39,7 +39,7 @@ __device__ __forceinline__ float gelu(float x) {
 // Y[r, j] = act(b[j] + sum_i X[r, i] * W[j, i]); X row stride ldx, Y row
 // stride ldy. 128 x 64 output tile per CTA, 8 x 4 per thread (operands read
 // as 128-bit shared-memory vectors), k ascending over the zero-padded range
-// [0, in rounded up to BK), each product and sum rounded on its own.
+// [0, in rounded up to BK), accumulated with fused multiply-adds.
 constexpr int BMR = 128;  // rows of a k_linear tile
 
 template <int ACT>

@@ -51,8 +51,8 @@ Scope of this version:
 
 ``fp8=True`` (an extension) runs those MLPs in FP8 (E4M3) with per-channel
 weight and per-row activation scales instead. Streams carry their
-``"float_path"`` (``latec_b200-bf16-3``, ``latec_b200-fp8-2`` or
-``latec_b200-f32-2``). As the reference's own encoder/decoder contract
+``"float_path"`` (``latec_b200-bf16-4``, ``latec_b200-fp8-3`` or
+``latec_b200-f32-3``). As the reference's own encoder/decoder contract
 requires, they decode only with that float path.
 """
 
@@ -72,8 +72,8 @@ MAGIC = b"LATECGNN"
 VERSION = 14
 PREFIX = "<8sII"
 PREFIX_SIZE = struct.calcsize(PREFIX)
-FLOAT_PATHS = {"f32": "latec_b200-f32-2", "bf16": "latec_b200-bf16-3",
-               "fp8": "latec_b200-fp8-2"}
+FLOAT_PATHS = {"f32": "latec_b200-f32-3", "bf16": "latec_b200-bf16-4",
+               "fp8": "latec_b200-fp8-3"}
 AUTO_CHUNK_THRESHOLD = 1 << 21
 RANK_LEVELS = {2: 8, 4: 5, 5: 4}
 EB_COARSE_FACTOR = 0.9
@@ -566,7 +566,8 @@ class GNNCodec:
                 scale = torch.exp2(lb.reshape(-1)).contiguous()
             xs = X[:, g.query_idx].reshape(-1).contiguous()
             if self.stage_trace is not None:
-                tr = {"stage": gi, "eb": seb, "mu": mu.clone(), "scale": scale.clone()}
+                tr = {"stage": gi, "eb": seb, "mu": mu.clone(), "scale": scale.clone(),
+                      "x": xs.clone()}
             shared = gate_fine and finest[gi]
             if gate and gi > 0 and n:
                 # the interpolation fallback, scored, chosen (gate_choose's rule)
