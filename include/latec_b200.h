@@ -316,10 +316,11 @@ typedef struct {
     const float* params;
     /* optional: BiDirEmbed, DirEmbed and MixEmbed weights packed by
      * latec_gnn_pack_bf16 (in that order, first then second layer each), then
-     * the line pool's key MLP: line_pool.wk.0 (64 x 64), line_pool.wk.2
-     * zero-padded to 32 x 64 rows, and its bias as 32 float32 (the first the
-     * real one, the rest 0); runs those MLPs in BF16 on the tensor cores
-     * (d = 64 only); NULL = float32 */
+     * the line pool's key MLP with its value projection: line_pool.wk.0 and
+     * line_pool.wv stacked (128 x 64, packed as one 128-row operand),
+     * line_pool.wk.2 zero-padded to 32 x 64 rows, and its bias as 32 float32
+     * (the first the real one, the rest 0); runs those layers in BF16 on the
+     * tensor cores (d = 64 only); NULL = float32 */
     const void* packed_bf16;
     uint32_t* tc_err;  /* device word, bit 1: a tensor-core wait ran out */
     /* optional, instead of packed_bf16: the same six layers packed by

@@ -23,6 +23,9 @@ namespace latec {
 int mlp2_tc(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* w1p,
             const float* b1, const void* w2p, const float* b2, int n1, int n2, float* Y, int ldy,
             int ny, uint32_t* err, int n_sm, cudaStream_t st);
+int kv_tc(const float* X, int ldx, int64_t rows, const void* w1p, const float* b1,
+          const float* bv, const void* w2p, const float* b2, float* KEY, float* V, int ldv,
+          uint32_t* err, int n_sm, cudaStream_t st);
 int mlp2_tc8(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* w1p,
              const float* s1, const float* b1, const void* w2p, const float* s2, const float* b2,
              int n1, int n2, float* Y, int ldy, uint32_t* err, int n_sm, cudaStream_t st);
@@ -358,8 +361,10 @@ struct TcMlp {
 };
 struct Packed {
     TcMlp bi, dir, mix;
-    // the line pool's key MLP (64 -> 64 -> 1) in BF16, its output layer and
-    // bias zero-padded to 32 rows; null when the model carries none
+    // the line pool's key MLP (64 -> 64 -> 1) in BF16 with the value
+    // projection's weights stacked under its first layer (128 x 64), its
+    // output layer and bias zero-padded to 32 rows; null when the model
+    // carries none
     TcMlp key;
     const float* key_b2 = nullptr;
 };
@@ -398,10 +403,10 @@ Packed packed_of(const latec_gnn_model* m, const Params& P) {
             t.w2 = p;
             p += (size_t)P.d * P.h;
         }
-        // then the line pool's key MLP: W1 d x d, W2 32 x d, b2 as 32 floats
+        // then the line pool's key MLP: [W1; Wv] 2d x d, W2 32 x d, b2 as 32 floats
         k.key.k1p = P.d;
         k.key.w1 = p;
-        p += (size_t)P.d * P.d;
+        p += (size_t)2 * P.d * P.d;
         k.key.w2 = p;
         p += (size_t)KEY_ROWS * P.d;
         k.key_b2 = (const float*)p;
@@ -559,16 +564,16 @@ int latec_gnn_embed(const latec_gnn_model* model, int32_t B, int64_t N, const fl
                               P.dir2b, pk.dir, P.h, d, H, msb + n2 * K * d, d, st);
             }
         }
-        // line pool keys and values of every live row; the key MLP on the
-        // tensor cores when the model carries it in BF16
+        // line pool keys and values of every live row: on the tensor cores
+        // in one pass over MS when the model carries them in BF16
         if (!rc && pk.key.w1) {
-            rc = mlp2_tc(MS, d, rows, d, pk.key.k1p, pk.key.w1, P.lp_k0b, pk.key.w2, pk.key_b2, d,
-                         KEY_ROWS, KEY, 1, 1, model->tc_err, n_sms(), st);
+            rc = kv_tc(MS, d, rows, pk.key.w1, P.lp_k0b, P.lp_vb, pk.key.w2, pk.key_b2, KEY, V, d,
+                       model->tc_err, n_sms(), st);
         } else {
             if (!rc) rc = linear(MS, d, rows, d, P.lp_k0w, P.lp_k0b, d, S1, d, 1, st);
             if (!rc) rc = linear(S1, d, rows, d, P.lp_k2w, P.lp_k2b, 1, KEY, 1, 0, st);
+            if (!rc) rc = linear(MS, d, rows, d, P.lp_vw, P.lp_vb, d, V, d, 0, st);
         }
-        if (!rc) rc = linear(MS, d, rows, d, P.lp_vw, P.lp_vb, d, V, d, 0, st);
         for (int b = 0; b < B && !rc; b++) {
             k_line_rows<<<blocks_for((int64_t)mt * K), LT, 0, st>>>(g.row_of, g.M, L, K, b, m0, mt,
                                                                     n_live, cand);

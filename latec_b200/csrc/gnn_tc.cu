@@ -16,7 +16,10 @@
 //      row of Y.
 // Instances: N1 x N2 = 128 x 64 (the message and mix MLPs) and 64 x 32 (the
 // line pool's key MLP, 64 -> 64 -> 1 with the output layer zero-padded to 32
-// rows; ny = 1 stores the key alone).
+// rows; ny = 1 stores the key alone). With NV > 0 layer 1 carries NV more
+// output columns that skip the activation and layer 2: they are stored, with
+// their bias, as a second float32 output (the line pool's value projection
+// rides on its key MLP's first layer: 64 + 64 columns from one A operand).
 // Operands use the no-swizzle K-major canonical layout: 8 x 16-byte core
 // matrices, row groups 128 bytes apart (SBO) and 8-element K chunks R * 16
 // bytes apart (LBO), R the operand's rows. Weights arrive pre-packed in that
@@ -118,18 +121,21 @@ __device__ __forceinline__ void st_bf16x8(__nv_bfloat16* dst, const float* v) {
 // converts K chunks of row t % 128 (rows of a warp are 16 bytes apart in the
 // canonical layout: conflict-free stores); warp w reads TMEM lanes
 // 32 (w % 4) .. + 31, warpgroup w / 4 half of the columns.
-template <int N1, int N2>
+template <int N1, int N2, int NV>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_mlp2_tc(const float* __restrict__ X, int ldx, int rows, int k1, int k1p,
               const __nv_bfloat16* __restrict__ w1p, const float* __restrict__ b1,
               const __nv_bfloat16* __restrict__ w2p, const float* __restrict__ b2,
-              float* __restrict__ Y, int ldy, int ny, uint32_t* __restrict__ err) {
-    static_assert(N1 % 32 == 0 && N2 % 32 == 0 && N1 + N2 <= 512, "MLP widths");
+              float* __restrict__ Y, int ldy, int ny, const float* __restrict__ bv,
+              float* __restrict__ V, int ldv, uint32_t* __restrict__ err) {
+    constexpr int NL1 = N1 + NV;  // layer 1 outputs: hidden, then the side output
+    static_assert(N1 % 32 == 0 && NV % 32 == 0 && N2 % 32 == 0 && NL1 + N2 <= 512,
+                  "MLP widths");
     extern __shared__ __align__(128) uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t mbar;
     __shared__ uint32_t tmem_base;
-    __nv_bfloat16* sw1 = (__nv_bfloat16*)smem_raw;             // N1 x k1p
-    __nv_bfloat16* sw2 = sw1 + (size_t)N1 * k1p;                // N2 x N1
+    __nv_bfloat16* sw1 = (__nv_bfloat16*)smem_raw;             // NL1 x k1p
+    __nv_bfloat16* sw2 = sw1 + (size_t)NL1 * k1p;               // N2 x N1
     __nv_bfloat16* sa = sw2 + (size_t)N2 * N1;                  // 128 x k1p (then Y staging)
     __nv_bfloat16* sh = sa + (size_t)TC_M * k1p;                // 128 x N1
     float* sy = (float*)sa;                                     // 128 x (N2 + 1) float32
@@ -139,7 +145,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     {  // stage the packed weights (16-byte copies)
         const int4* s1 = (const int4*)w1p;
         int4* d1 = (int4*)sw1;
-        for (int i = tid; i < N1 * k1p / 8; i += TC_THREADS) d1[i] = s1[i];
+        for (int i = tid; i < NL1 * k1p / 8; i += TC_THREADS) d1[i] = s1[i];
         const int4* s2 = (const int4*)w2p;
         int4* d2 = (int4*)sw2;
         for (int i = tid; i < N2 * N1 / 8; i += TC_THREADS) d2[i] = s2[i];
@@ -148,7 +154,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar)), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
-    constexpr uint32_t TMEM_COLS = (N1 + N2) <= 128 ? 128 : ((N1 + N2) <= 256 ? 256 : 512);
+    constexpr uint32_t TMEM_COLS = (NL1 + N2) <= 128 ? 128 : ((NL1 + N2) <= 256 ? 256 : 512);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&tmem_base)),
@@ -217,8 +223,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const uint32_t a0 = smem_u32(sa), bb = smem_u32(sw1);
             for (int kk = 0; kk < k1p / 16; kk++) {
                 const uint64_t ad = smem_desc(a0 + kk * 2 * TC_M * 16, TC_M * 16, 128);
-                const uint64_t bd = smem_desc(bb + kk * 2 * N1 * 16, N1 * 16, 128);
-                mma_bf16(tmem, ad, bd, idesc_bf16(TC_M, N1), kk > 0);
+                const uint64_t bd = smem_desc(bb + kk * 2 * NL1 * 16, NL1 * 16, 128);
+                mma_bf16(tmem, ad, bd, idesc_bf16(TC_M, NL1), kk > 0);
             }
             mma_commit(mb);
         }
@@ -229,14 +235,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
         phase ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;");
-        // 3. epilogue 1: bias + GELU -> BF16 hidden; each warpgroup half the columns
-        for (int c = half * (N1 / 2); c < (half + 1) * (N1 / 2); c += 16) {
+        // 3. epilogue 1: bias + GELU -> BF16 hidden (the side columns: bias,
+        //    then float32 rows of V); each warpgroup half the columns
+        for (int c = half * (NL1 / 2); c < (half + 1) * (NL1 / 2); c += 16) {
             float v[16];
             tmem_ld16(tmem + lane_base + c, v);
+            if (NV == 0 || c < N1) {
 #pragma unroll
-            for (int i = 0; i < 16; i++) v[i] = gelu_tc(__fadd_rn(v[i], b1[c + i]));
-            st_bf16x8(sh + canon(trow, c, TC_M), v);
-            st_bf16x8(sh + canon(trow, c + 8, TC_M), v + 8);
+                for (int i = 0; i < 16; i++) v[i] = gelu_tc(__fadd_rn(v[i], b1[c + i]));
+                st_bf16x8(sh + canon(trow, c, TC_M), v);
+                st_bf16x8(sh + canon(trow, c + 8, TC_M), v + 8);
+            } else if (r0 + trow < rows) {
+                float* vr = V + (int64_t)(r0 + trow) * ldv + (c - N1);
+#pragma unroll
+                for (int i = 0; i < 16; i++) vr[i] = __fadd_rn(v[i], bv[c - N1 + i]);
+            }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;");
@@ -248,7 +261,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             for (int kk = 0; kk < N1 / 16; kk++) {
                 const uint64_t ad = smem_desc(a0 + kk * 2 * TC_M * 16, TC_M * 16, 128);
                 const uint64_t bd = smem_desc(bb + kk * 2 * N2 * 16, N2 * 16, 128);
-                mma_bf16(tmem + N1, ad, bd, idesc_bf16(TC_M, N2), kk > 0);
+                mma_bf16(tmem + NL1, ad, bd, idesc_bf16(TC_M, N2), kk > 0);
             }
             mma_commit(mb);
         }
@@ -263,7 +276,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         //    read), then coalesced row stores
         for (int c = half * (N2 / 2); c < (half + 1) * (N2 / 2); c += 16) {
             float v[16];
-            tmem_ld16(tmem + lane_base + N1 + c, v);
+            tmem_ld16(tmem + lane_base + NL1 + c, v);
 #pragma unroll
             for (int i = 0; i < 16; i++) sy[trow * (N2 + 1) + c + i] = __fadd_rn(v[i], b2[c + i]);
         }
@@ -539,8 +552,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 }  // namespace
 
 // Shared memory of the fused kernel for an input width padded to k1p.
-uint64_t mlp2_tc_smem(int k1p, int n1, int n2) {
-    return 2ull * ((uint64_t)n1 * k1p + (uint64_t)n2 * n1 + (uint64_t)TC_M * k1p +
+uint64_t mlp2_tc_smem(int k1p, int n1, int n2, int nv = 0) {
+    return 2ull * ((uint64_t)(n1 + nv) * k1p + (uint64_t)n2 * n1 + (uint64_t)TC_M * k1p +
                    (uint64_t)TC_M * n1);
 }
 
@@ -556,14 +569,37 @@ int mlp2_tc(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* 
     const uint64_t smem = mlp2_tc_smem(k1p, n1, n2);
     if (smem > 220 * 1024 || 4ull * TC_M * (n2 + 1) > 2ull * TC_M * (k1p + n1))
         return LATEC_ERR_UNSUPPORTED;
-    auto kern = big ? k_mlp2_tc<128, 64> : k_mlp2_tc<64, 32>;
+    auto kern = big ? k_mlp2_tc<128, 64, 0> : k_mlp2_tc<64, 32, 0>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return LATEC_ERR_CUDA;
     const int64_t tiles = (rows + TC_M - 1) / TC_M;
     const int grid = (int)(tiles < n_sm ? tiles : n_sm);
     kern<<<grid, TC_THREADS, smem, st>>>(X, ldx, (int)rows, k1, k1p, (const __nv_bfloat16*)w1p, b1,
-                                         (const __nv_bfloat16*)w2p, b2, Y, ldy, ny, err);
+                                         (const __nv_bfloat16*)w2p, b2, Y, ldy, ny, nullptr,
+                                         nullptr, 0, err);
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
+}
+
+// The line pool's key MLP with its value projection on layer 1's side columns:
+// w1p packs [Wk0; Wv] (128 x 64), KEY gets the key (one float per row), V the
+// 64 values of each row (row stride ldv).
+int kv_tc(const float* X, int ldx, int64_t rows, const void* w1p, const float* b1,
+          const float* bv, const void* w2p, const float* b2, float* KEY, float* V, int ldv,
+          uint32_t* err, int n_sm, cudaStream_t st) {
+    if (rows <= 0) return LATEC_OK;
+    if (rows > 0x7fffffffLL || ldv < 64) return LATEC_ERR_UNSUPPORTED;
+    const uint64_t smem = mlp2_tc_smem(64, 64, 32, 64);
+    auto kern = k_mlp2_tc<64, 32, 64>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return LATEC_ERR_CUDA;
+    const int64_t tiles = (rows + TC_M - 1) / TC_M;
+    const int grid = (int)(tiles < n_sm ? tiles : n_sm);
+    kern<<<grid, TC_THREADS, smem, st>>>(X, ldx, (int)rows, 64, 64, (const __nv_bfloat16*)w1p, b1,
+                                         (const __nv_bfloat16*)w2p, b2, KEY, 1, 1, bv, V, ldv,
+                                         err);
     count_launches(1);
     return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
 }

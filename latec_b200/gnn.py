@@ -304,9 +304,10 @@ class GNNModel:
     def __init__(self, weights: dict, d: int = 64, agg_level: int = 1, device=None,
                  precision: str = "f32"):
         """``precision``: "f32" (every layer in float32), "bf16" (the
-        BiDirEmbed, DirEmbed and MixEmbed MLPs and the line pool's key MLP in
-        BF16 on the tensor cores with float32 accumulation; the pools' values
-        and softmax, the axis pool and the readout stay float32; d = 64) or "fp8"
+        BiDirEmbed, DirEmbed and MixEmbed MLPs, the line pool's key MLP and
+        value projection in BF16 on the tensor cores with float32
+        accumulation; the pools' softmax, the axis pool and the readout stay
+        float32; d = 64) or "fp8"
         (those MLPs in E4M3 with per-output-channel weight scales and per-row
         activation scales, float32 accumulation; d = 64)."""
         import ctypes
@@ -342,9 +343,12 @@ class GNNModel:
                 _lib.check(lib.latec_gnn_pack_bf16(w.ctypes.data, n, k, kp, out.ctypes.data),
                            "latec_gnn_pack_bf16")
                 parts.append(out)
-            # the line pool's key MLP: W1 (d x d), then W2 (1 x d) zero-padded
-            # to 32 rows, then its bias as 32 float32 (the first the real one)
-            w1 = np.ascontiguousarray(weights["line_pool.wk.0.weight"], np.float32)
+            # the line pool's key MLP: W1 (d x d) with the value projection
+            # (d x d) stacked under it, then W2 (1 x d) zero-padded to 32 rows,
+            # then its bias as 32 float32 (the first the real one)
+            w1 = np.ascontiguousarray(np.concatenate(
+                [np.asarray(weights["line_pool.wk.0.weight"], np.float32),
+                 np.asarray(weights["line_pool.wv.weight"], np.float32)]), np.float32)
             w2 = np.zeros((32, self.d), np.float32)
             w2[0] = np.asarray(weights["line_pool.wk.2.weight"], np.float32).reshape(-1)
             b2 = np.zeros(32, np.float32)
