@@ -317,6 +317,58 @@ def compress(img, eb, order="cubic", levels_=4, anchor_stride=16, anchor_block=1
                         end_mode=end_mode, eb_ratio=ratio)
 
 
+END_MODE_MAX = 3
+
+
+def tune_sweep(img, eb, tune="size", order="cubic", levels_=4, anchor_stride=16,
+               anchor_block=1, radius=1 << 15, zstd_level=9, tune_size_slack=1.05,
+               mode="compat"):
+    """The encoder's sequential tune sweep, ``latec/codec.py:171-262``: the base
+    candidate, then every end mode at the first eb ratio, then every (eb ratio,
+    center) at the smallest stream's end mode; ``"size"`` keeps the smallest
+    stream, ``"rd"`` the lowest reconstruction SSE within ``tune_size_slack``
+    of it (ties broken by size, ratio, center, end mode). Returns
+    ``(stream, stats, (ratio, center, end_mode), n_candidates)``."""
+    fimg, spatial, c, src = _normalise(img)
+    nd = len(spatial)
+    base_center, base_end = (1 if nd >= 4 else 0), interp.END_QUAD
+    if tune not in ("fast", "size", "rd"):
+        raise ValueError("tune must be 'fast', 'size', or 'rd'")
+    sweep = tune != "fast"
+    ratio_cands = [1.0, 0.9, 0.8, 0.7] if sweep else [0.9]
+    center_cands = [base_center] + ([x for x in (0, 1, 2) if x != base_center] if sweep else [])
+    field = np.asarray(img)
+    cands, seen = [], set()
+
+    def run_once(ratio, center, end_mode):
+        if (ratio, center, end_mode) in seen:
+            return
+        seen.add((ratio, center, end_mode))
+        stream, st = compress(img, eb, order, levels_, anchor_stride, anchor_block, radius,
+                              zstd_level, eb_ratio=ratio, center=center, end_mode=end_mode,
+                              mode=mode)
+        # reconstruction error: float32 (source-precision) differences, squared in float64
+        d = (np.asarray(field, fimg.dtype) - np.asarray(st["recon"], fimg.dtype))
+        sse = float(np.sum(np.square(d.astype(np.float64))))
+        cands.append((len(stream), sse, ratio, center, end_mode, stream, st))
+
+    run_once(ratio_cands[0], base_center, base_end)
+    chosen_end = base_end
+    if sweep:
+        for em in range(END_MODE_MAX + 1):
+            run_once(ratio_cands[0], base_center, em)
+        chosen_end = min(cands, key=lambda x: (x[0], x[1]))[4]
+    for ratio in ratio_cands:
+        for center in center_cands:
+            run_once(ratio, center, chosen_end)
+    if tune == "rd" and len(cands) > 1:
+        limit = min(x[0] for x in cands) * tune_size_slack
+        best = min((x for x in cands if x[0] <= limit), key=lambda x: (x[1], x[0], x[2], x[3], x[4]))
+    else:
+        best = min(cands, key=lambda x: (x[0], x[1], x[2], x[3], x[4]))
+    return best[5], best[6], (best[2], best[3], best[4]), len(cands)
+
+
 def decompress(stream: bytes):
     """``latec/codec.py:288-322,462-524``."""
     h = unpack_header(stream)

@@ -243,6 +243,28 @@ def test_tune_size_sweep_runs_and_picks_smallest():
     assert np.abs(back.astype(np.float64) - x).max() <= 1e-3
 
 
+@pytest.mark.parametrize("tune", ["size", "rd"])
+@pytest.mark.parametrize("shape", [(72, 60), (24, 20, 28), (12, 10, 8, 6)])
+def test_tune_choice_matches_oracle_sweep(tune, shape):
+    """The encoder's tune sweep (latec/codec.py:171-262) against the oracle's
+    restatement of it: in the reference-readable (compat) mode, where every
+    candidate's stream bytes are the reference's, the same candidates are
+    tried, the same (eb ratio, center, end mode) wins and the chosen stream is
+    byte-identical."""
+    from latec_b200 import fields
+
+    x = fields.turbulence_jumps(shape, seed=11)
+    eb = 2e-3
+    lv, stride = (3, 8)
+    lb = _lb()
+    stream, st = lb.compress(x, eb, lb.InterpPredictor("cubic", lv, stride, 1), levels=lv,
+                             anchor_stride=stride, tune=tune, entropy="compat")
+    ostream, _, choice, n_cand = ocodec.tune_sweep(x, eb, tune, "cubic", lv, stride)
+    assert st["tune_candidates"] == n_cand
+    assert (st["eb_ratio"], st["interp_center"], st["interp_end_mode"]) == choice
+    assert stream == ostream
+
+
 def test_corrupted_streams_raise_not_hang():
     from latec_b200 import fields
 
