@@ -23,6 +23,9 @@ namespace latec {
 int mlp2_tc(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* w1p,
             const float* b1, const void* w2p, const float* b2, int n1, int n2, float* Y, int ldy,
             int ny, uint32_t* err, int n_sm, cudaStream_t st);
+int mlp2_tc_gather(const RowGather& rg, int two_sided, int64_t rows, int k1, int k1p,
+                   const void* w1p, const float* b1, const void* w2p, const float* b2, float* Y,
+                   int ldy, uint32_t* err, int n_sm, cudaStream_t st);
 int kv_tc(const float* X, int ldx, int64_t rows, const void* w1p, const float* b1,
           const float* bv, const void* w2p, const float* b2, float* KEY, float* V, int ldv,
           uint32_t* err, int n_sm, cudaStream_t st);
@@ -543,9 +546,17 @@ int latec_gnn_embed(const latec_gnn_model* model, int32_t B, int64_t N, const fl
         float* KEY = S1 + rows * d;
         float* V = KEY + rows;
         int32_t* cand = (int32_t*)(V + rows * d);
+        // BF16 message MLPs gather their rows in the operand staging
+        const bool gather = pk.bi.w1 && !pk.bi.fp8 && d == 64 && P.ds == 16;
         for (int b = 0; b < B && !rc; b++) {
             float* msb = MS + (int64_t)b * n_live * K * d;
-            if (n2) {
+            RowGather rg{E, N, K, b, g.M, P.table, nullptr, g.nbr_p, g.nbr_n, g.logd_p, g.logd_n,
+                         g.sidx_p, g.sidx_n};
+            if (n2 && gather) {
+                rg.pairs = g.two + g.two_off[t];
+                rc = mlp2_tc_gather(rg, 1, n2 * K, (int)w2, pk.bi.k1p, pk.bi.w1, P.bi0b, pk.bi.w2,
+                                    P.bi2b, msb, d, model->tc_err, n_sms(), st);
+            } else if (n2) {
                 k_rows_two<<<blocks_for(n2 * K * 32), LT, 0, st>>>(E, N, K, d, P.ds, P.table, g, b,
                                                                   g.two + g.two_off[t], n2, X,
                                                                   (int)l2);
@@ -554,7 +565,12 @@ int latec_gnn_embed(const latec_gnn_model* model, int32_t B, int64_t N, const fl
                     rc = mlp2(model, X, (int)l2, n2 * K, (int)w2, P.bi0w, P.bi0b, P.bi2w, P.bi2b,
                               pk.bi, P.h, d, H, msb, d, st);
             }
-            if (n1 && !rc) {
+            if (n1 && !rc && gather) {
+                rg.pairs = g.one + g.one_off[t];
+                rc = mlp2_tc_gather(rg, 0, n1 * K, (int)w1, pk.dir.k1p, pk.dir.w1, P.dir0b,
+                                    pk.dir.w2, P.dir2b, msb + n2 * K * d, d, model->tc_err,
+                                    n_sms(), st);
+            } else if (n1 && !rc) {
                 k_rows_one<<<blocks_for(n1 * K * 32), LT, 0, st>>>(E, N, K, d, P.ds, P.table, g, b,
                                                                   g.one + g.one_off[t], n1, X,
                                                                   (int)l1);

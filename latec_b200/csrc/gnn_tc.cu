@@ -117,17 +117,91 @@ __device__ __forceinline__ void st_bf16x8(__nv_bfloat16* dst, const float* v) {
     *(int4*)dst = *(const int4*)p;
 }
 
+struct GatherRow {
+    const float* e0;  // first embedding row (negative side / the side)
+    const float* s0;  // its state row
+    const float* e1;  // positive side's embedding row (two-sided)
+    const float* s1;
+    float t0, t1;     // the trailing scalars
+    bool live;
+};
+
+template <int GATHER>
+__device__ __forceinline__ void gather_row(const RowGather& rg, int w, GatherRow& g) {
+    g.live = w >= 0;
+    g.e0 = g.s0 = g.e1 = g.s1 = nullptr;
+    g.t0 = g.t1 = 0.0f;
+    if (!g.live) return;
+    const int p = w / rg.K, k = w - (w / rg.K) * rg.K;
+    const int pair = rg.pairs[p];
+    const int l = pair / rg.M;
+    const int64_t rowbase = (int64_t)rg.b * rg.N;
+    if (GATHER == 2) {
+        const int64_t in_ = rg.nbr_n[pair], ip = rg.nbr_p[pair];
+        g.e0 = rg.E + ((rowbase + in_) * rg.K + k) * 64;
+        g.s0 = rg.table + (int64_t)rg.sidx_n[l * rg.K + k] * 16;
+        g.e1 = rg.E + ((rowbase + ip) * rg.K + k) * 64;
+        g.s1 = rg.table + (int64_t)rg.sidx_p[l * rg.K + k] * 16;
+        g.t0 = rg.logd_n[pair];
+        g.t1 = rg.logd_p[pair];
+    } else {
+        const bool pos = rg.nbr_p[pair] >= 0;
+        const int64_t nb = pos ? rg.nbr_p[pair] : rg.nbr_n[pair];
+        g.e0 = rg.E + ((rowbase + nb) * rg.K + k) * 64;
+        g.s0 = rg.table + (int64_t)(pos ? rg.sidx_p[l * rg.K + k] : rg.sidx_n[l * rg.K + k]) * 16;
+        g.t0 = pos ? 1.0f : -1.0f;
+        g.t1 = pos ? rg.logd_p[pair] : rg.logd_n[pair];
+    }
+}
+
+// Features [8c, 8c + 8) of a gathered row (zero past the row or the width).
+// Embedding rows are 256-byte aligned (float4 loads); state rows are read
+// element by element (the table sits at any float offset of the parameters).
+template <int GATHER>
+__device__ __forceinline__ void gather_chunk(const GatherRow& g, int c, int chunks, float* v) {
+#pragma unroll
+    for (int e = 0; e < 8; e++) v[e] = 0.0f;
+    if (!g.live || c >= chunks) return;
+    const float* src = nullptr;
+    bool state = false;
+    if (c < 8) {
+        src = g.e0 + 8 * c;
+    } else if (c < 10) {
+        src = g.s0 + 8 * (c - 8);
+        state = true;
+    } else if (GATHER == 2 && c < 18) {
+        src = g.e1 + 8 * (c - 10);
+    } else if (GATHER == 2 && c < 20) {
+        src = g.s1 + 8 * (c - 18);
+        state = true;
+    } else if (c == (GATHER == 2 ? 20 : 10)) {
+        v[0] = g.t0;
+        v[1] = g.t1;
+        return;
+    } else {
+        return;
+    }
+    if (state) {
+#pragma unroll
+        for (int e = 0; e < 8; e++) v[e] = src[e];
+    } else {
+        const float4 a = *(const float4*)src, b = *(const float4*)(src + 4);
+        v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w;
+        v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+    }
+}
+
 // N1 = hidden width, N2 = output width (multiples of 32). 256 threads: thread t
 // converts K chunks of row t % 128 (rows of a warp are 16 bytes apart in the
 // canonical layout: conflict-free stores); warp w reads TMEM lanes
 // 32 (w % 4) .. + 31, warpgroup w / 4 half of the columns.
-template <int N1, int N2, int NV>
+template <int N1, int N2, int NV, int GATHER>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_mlp2_tc(const float* __restrict__ X, int ldx, int rows, int k1, int k1p,
               const __nv_bfloat16* __restrict__ w1p, const float* __restrict__ b1,
               const __nv_bfloat16* __restrict__ w2p, const float* __restrict__ b2,
               float* __restrict__ Y, int ldy, int ny, const float* __restrict__ bv,
-              float* __restrict__ V, int ldv, uint32_t* __restrict__ err) {
+              float* __restrict__ V, int ldv, const RowGather rg, uint32_t* __restrict__ err) {
     constexpr int NL1 = N1 + NV;  // layer 1 outputs: hidden, then the side output
     static_assert(N1 % 32 == 0 && NV % 32 == 0 && N2 % 32 == 0 && NL1 + N2 <= 512,
                   "MLP widths");
@@ -179,39 +253,59 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
         const int r0 = t * TC_M;
         // 1. rows of X -> BF16 A operand: thread handles row tid % 128,
-        //    K chunks tid / 128, + 2, + 4, ...; four chunks' loads in flight
-        {
+        //    K chunks tid / 128, + 2, + 4, ...; four chunks' loads in flight.
+        //    GATHER: the row is assembled here from the embedding field, the
+        //    direction-state table and the log distances (the message-row
+        //    layout of k_rows_two / k_rows_one), with no X buffer in between.
+        if (GATHER) {
             const int r = tid & (TC_M - 1);
             const int gr = r0 + r;
-            const float* xr = X + (int64_t)gr * ldx;
+            GatherRow row;
+            gather_row<GATHER>(rg, gr < rows ? gr : -1, row);
             for (int c0 = tid >> 7; c0 < chunks; c0 += 8) {
                 float v[4][8];
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const int c = c0 + 2 * u;
-                    if (vec4) {  // 16-byte rows: two float4 per chunk, masked past k1
-#pragma unroll
-                        for (int h2 = 0; h2 < 2; h2++) {
-                            const int k = c * 8 + 4 * h2;
-                            float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
-                            if (c < chunks && gr < rows && k < k1) f = *(const float4*)(xr + k);
-                            v[u][4 * h2 + 0] = k + 0 < k1 ? f.x : 0.0f;
-                            v[u][4 * h2 + 1] = k + 1 < k1 ? f.y : 0.0f;
-                            v[u][4 * h2 + 2] = k + 2 < k1 ? f.z : 0.0f;
-                            v[u][4 * h2 + 3] = k + 3 < k1 ? f.w : 0.0f;
-                        }
-                    } else {
-#pragma unroll
-                        for (int e = 0; e < 8; e++) {
-                            const int k = c * 8 + e;
-                            v[u][e] = (c < chunks && gr < rows && k < k1) ? xr[k] : 0.0f;
-                        }
-                    }
-                }
+                for (int u = 0; u < 4; u++) gather_chunk<GATHER>(row, c0 + 2 * u, chunks, v[u]);
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
                     const int c = c0 + 2 * u;
                     if (c < chunks) st_bf16x8(sa + canon(r, c * 8, TC_M), v[u]);
+                }
+            }
+        } else {
+            {
+                const int r = tid & (TC_M - 1);
+                const int gr = r0 + r;
+                const float* xr = X + (int64_t)gr * ldx;
+                for (int c0 = tid >> 7; c0 < chunks; c0 += 8) {
+                    float v[4][8];
+    #pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int c = c0 + 2 * u;
+                        if (vec4) {  // 16-byte rows: two float4 per chunk, masked past k1
+    #pragma unroll
+                            for (int h2 = 0; h2 < 2; h2++) {
+                                const int k = c * 8 + 4 * h2;
+                                float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+                                if (c < chunks && gr < rows && k < k1) f = *(const float4*)(xr + k);
+                                v[u][4 * h2 + 0] = k + 0 < k1 ? f.x : 0.0f;
+                                v[u][4 * h2 + 1] = k + 1 < k1 ? f.y : 0.0f;
+                                v[u][4 * h2 + 2] = k + 2 < k1 ? f.z : 0.0f;
+                                v[u][4 * h2 + 3] = k + 3 < k1 ? f.w : 0.0f;
+                            }
+                        } else {
+    #pragma unroll
+                            for (int e = 0; e < 8; e++) {
+                                const int k = c * 8 + e;
+                                v[u][e] = (c < chunks && gr < rows && k < k1) ? xr[k] : 0.0f;
+                            }
+                        }
+                    }
+    #pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int c = c0 + 2 * u;
+                        if (c < chunks) st_bf16x8(sa + canon(r, c * 8, TC_M), v[u]);
+                    }
                 }
             }
         }
@@ -569,7 +663,7 @@ int mlp2_tc(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* 
     const uint64_t smem = mlp2_tc_smem(k1p, n1, n2);
     if (smem > 220 * 1024 || 4ull * TC_M * (n2 + 1) > 2ull * TC_M * (k1p + n1))
         return LATEC_ERR_UNSUPPORTED;
-    auto kern = big ? k_mlp2_tc<128, 64, 0> : k_mlp2_tc<64, 32, 0>;
+    auto kern = big ? k_mlp2_tc<128, 64, 0, 0> : k_mlp2_tc<64, 32, 0, 0>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return LATEC_ERR_CUDA;
@@ -577,7 +671,7 @@ int mlp2_tc(const float* X, int ldx, int64_t rows, int k1, int k1p, const void* 
     const int grid = (int)(tiles < n_sm ? tiles : n_sm);
     kern<<<grid, TC_THREADS, smem, st>>>(X, ldx, (int)rows, k1, k1p, (const __nv_bfloat16*)w1p, b1,
                                          (const __nv_bfloat16*)w2p, b2, Y, ldy, ny, nullptr,
-                                         nullptr, 0, err);
+                                         nullptr, 0, RowGather{}, err);
     count_launches(1);
     return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
 }
@@ -591,7 +685,7 @@ int kv_tc(const float* X, int ldx, int64_t rows, const void* w1p, const float* b
     if (rows <= 0) return LATEC_OK;
     if (rows > 0x7fffffffLL || ldv < 64) return LATEC_ERR_UNSUPPORTED;
     const uint64_t smem = mlp2_tc_smem(64, 64, 32, 64);
-    auto kern = k_mlp2_tc<64, 32, 64>;
+    auto kern = k_mlp2_tc<64, 32, 64, 0>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return LATEC_ERR_CUDA;
@@ -599,7 +693,33 @@ int kv_tc(const float* X, int ldx, int64_t rows, const void* w1p, const float* b
     const int grid = (int)(tiles < n_sm ? tiles : n_sm);
     kern<<<grid, TC_THREADS, smem, st>>>(X, ldx, (int)rows, 64, 64, (const __nv_bfloat16*)w1p, b1,
                                          (const __nv_bfloat16*)w2p, b2, KEY, 1, 1, bv, V, ldv,
-                                         err);
+                                         RowGather{}, err);
+    count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
+}
+
+// The message MLP (hidden 128, output 64) over message rows gathered in the
+// operand staging: two_sided 1 = BiDirEmbed rows (k1 162), 0 = DirEmbed rows
+// (k1 82). rows = pairs x K; Y gets 64 floats per row (row stride ldy).
+int mlp2_tc_gather(const RowGather& rg, int two_sided, int64_t rows, int k1, int k1p,
+                   const void* w1p, const float* b1, const void* w2p, const float* b2, float* Y,
+                   int ldy, uint32_t* err, int n_sm, cudaStream_t st) {
+    if (rows <= 0) return LATEC_OK;
+    if (rows > 0x7fffffffLL || k1 != (two_sided ? 162 : 82) || k1p % 16 || k1p < k1 ||
+        ((uintptr_t)rg.E % 16) != 0)
+        return LATEC_ERR_UNSUPPORTED;
+    const uint64_t smem = mlp2_tc_smem(k1p, 128, 64);
+    if (smem > 220 * 1024 || 4ull * TC_M * 65 > 2ull * TC_M * (k1p + 128))
+        return LATEC_ERR_UNSUPPORTED;
+    auto kern = two_sided ? k_mlp2_tc<128, 64, 0, 2> : k_mlp2_tc<128, 64, 0, 1>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return LATEC_ERR_CUDA;
+    const int64_t tiles = (rows + TC_M - 1) / TC_M;
+    const int grid = (int)(tiles < n_sm ? tiles : n_sm);
+    kern<<<grid, TC_THREADS, smem, st>>>(nullptr, 0, (int)rows, k1, k1p, (const __nv_bfloat16*)w1p,
+                                         b1, (const __nv_bfloat16*)w2p, b2, Y, ldy, 64, nullptr,
+                                         nullptr, 0, rg, err);
     count_launches(1);
     return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
 }

@@ -88,11 +88,31 @@ struct StageDesc {
     uint32_t h_suf[MAXD + 1];          // kind 0: product of h_tot over axes j..
 };
 
+// The anchor stage of a blocked plan (kind 2): every anchor_block^ndim block
+// of the anchor lattice in C order; rank -> coordinates, flat grid index.
+__host__ __device__ __forceinline__ int64_t block_anchor_coords(const StageDesc& d, uint32_t rank,
+                                                                int32_t* coord) {
+    int64_t flat = 0;
+    uint32_t rem = rank;
+    for (int j = MAXD - 1; j >= 0; j--) {
+        if (j < d.ndim) {
+            const uint32_t q = fdiv(rem, d.size_div[j]);
+            const uint32_t m = rem - q * d.size_div[j].d;
+            rem = q;
+            const uint32_t b = fdiv(m, d.blk_div);  // block m / ablock, offset m % ablock
+            coord[j] = (int32_t)(b * (uint32_t)d.astride + (m - b * d.blk_div.d));
+            flat += (int64_t)coord[j] * d.gstride[j];
+        }
+    }
+    return flat;
+}
+
 // Decode a stage-local rank into grid coordinates; returns the flat grid index.
 __host__ __device__ __forceinline__ int64_t stage_coords(const StageDesc& d, uint32_t rank,
                                                 int32_t* coord) {
+    if (d.kind == 2) return block_anchor_coords(d, rank, coord);
     int64_t flat = 0;
-    if (d.kind != 1) {
+    if (d.kind == 0) {
         uint32_t rem = rank;
 #pragma unroll
         for (int j = MAXD - 1; j >= 0; j--) {
@@ -100,12 +120,7 @@ __host__ __device__ __forceinline__ int64_t stage_coords(const StageDesc& d, uin
                 uint32_t q = fdiv(rem, d.size_div[j]);
                 uint32_t m = rem - q * d.size_div[j].d;
                 rem = q;
-                if (d.kind == 2) {  // block m / ablock, offset m % ablock
-                    const uint32_t b = fdiv(m, d.blk_div);
-                    coord[j] = (int32_t)(b * (uint32_t)d.astride + (m - b * d.blk_div.d));
-                } else {
-                    coord[j] = d.start[j] + d.step * (int32_t)m;
-                }
+                coord[j] = d.start[j] + d.step * (int32_t)m;
                 flat += (int64_t)coord[j] * d.gstride[j];
             }
         }
@@ -134,8 +149,9 @@ __host__ __device__ __forceinline__ int64_t stage_coords(const StageDesc& d, uin
 }
 
 // Compile-time specialised decode: ND > 0 fixes the rank (loops unroll, the
-// coordinates stay in registers), KIND fixes the stage layout; ND == 0 falls
-// back to the runtime rank.
+// coordinates stay in registers), KIND fixes the stage layout (0 single
+// class, 1 fused); ND == 0 falls back to the runtime rank. Blocked-anchor
+// stages (kind 2) go through stage_point_t.
 template <int ND, int KIND>
 __host__ __device__ __forceinline__ int64_t stage_coords_t(const StageDesc& d, uint32_t rank,
                                                            int32_t* coord) {
@@ -149,12 +165,7 @@ __host__ __device__ __forceinline__ int64_t stage_coords_t(const StageDesc& d, u
                 const uint32_t q = fdiv(rem, d.size_div[j]);
                 const uint32_t m = rem - q * d.size_div[j].d;
                 rem = q;
-                if (d.kind == 2) {  // blocked anchors: block m / ablock, offset m % ablock
-                    const uint32_t b = fdiv(m, d.blk_div);
-                    coord[j] = (int32_t)(b * (uint32_t)d.astride + (m - b * d.blk_div.d));
-                } else {
-                    coord[j] = d.start[j] + d.step * (int32_t)m;
-                }
+                coord[j] = d.start[j] + d.step * (int32_t)m;
                 flat += (int64_t)coord[j] * d.gstride[j];
             }
         }
@@ -247,6 +258,7 @@ __host__ __device__ __forceinline__ uint32_t holes_before(const StageDesc& d,
 template <int ND, int KIND>
 __host__ __device__ __forceinline__ int64_t stage_point_t(const StageDesc& d, uint32_t rank,
                                                           int32_t* coord) {
+    if (KIND == 0 && d.kind == 2) return block_anchor_coords(d, rank, coord);
     if (!d.holes) return stage_coords_t<ND, KIND>(d, rank, coord);
     uint32_t i = rank;
     int64_t f = stage_coords_t<ND, KIND>(d, i, coord);
@@ -265,5 +277,24 @@ __host__ __device__ __forceinline__ int64_t stage_point(const StageDesc& d, uint
                                                         int32_t* coord) {
     return d.kind == 1 ? stage_point_t<0, 1>(d, rank, coord) : stage_point_t<0, 0>(d, rank, coord);
 }
+
+// Message rows of the GNN's embedding pass assembled in the MLP's operand
+// staging (latec/gnn_predictor.py:843-871 message layout, d = 64, ds = 16):
+// two-sided rows [e_neg | state_neg | e_pos | state_pos | logd_neg |
+// logd_pos] (162 features), one-sided [e_side | state_side | sign |
+// logd_side] (82). Row w of the launch is (pair pairs[w / K], axis w % K).
+struct RowGather {
+    const float* E;         // (B, N, K, 64) embedding field
+    int64_t N;
+    int K, b, M;
+    const float* table;     // direction-state rows of 16
+    const int32_t* pairs;   // pair ids l * M + m of the launch's rows
+    const int32_t* nbr_p;   // (L, M) neighbours, -1 = none
+    const int32_t* nbr_n;
+    const float* logd_p;    // (L, M)
+    const float* logd_n;
+    const int32_t* sidx_p;  // (L, K) state rows
+    const int32_t* sidx_n;
+};
 
 }  // namespace latec

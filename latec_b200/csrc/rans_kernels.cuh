@@ -15,9 +15,10 @@ constexpr int MODE_COMPAT = 1;
 // frequency with rcp / shift (exact below 2^63); the single-stack coder, whose
 // state spans all 64 bits, with the Granlund-Montgomery multiplier gm and the
 // shifts gsh1 / gsh2 (exact for every 64-bit state).
+// The lane coder's fields come first (24 bytes, the loads it issues), the
+// stack coder's multiplier last.
 struct EncSym {
     uint64_t rcp;
-    uint64_t gm;
     uint32_t bias;
     uint32_t cmpl;
     uint32_t freq;
@@ -25,6 +26,7 @@ struct EncSym {
     uint8_t gsh1;
     uint8_t gsh2;
     uint8_t pad;
+    uint64_t gm;
 };
 
 // One stage of the entropy stage, shared layout with the host (see capi.cu;
