@@ -857,7 +857,7 @@ static int last_err() {
 // Compile-time dispatch over (dtype, rank 2/3/4 or runtime, layout, order).
 #define LATEC_DISPATCH(KERNEL_CALL)                                                      \
     do {                                                                                 \
-        const int nd_ = (d.ndim >= 2 && d.ndim <= 4) ? d.ndim : 0;                      \
+        const int nd_ = (d.ndim >= 2 && d.ndim <= 4 && !d.holes && d.kind != 2) ? d.ndim : 0; \
         const int kd_ = d.kind == 1 ? 1 : 0, cu_ = q.order ? 1 : 0;                      \
         if (dtype == LATEC_F64) {                                                        \
             using T = double;                                                            \

@@ -256,10 +256,8 @@ __host__ __device__ __forceinline__ uint32_t holes_before(const StageDesc& d,
 // is reached by fixed-point iteration from i = r (the right side never
 // decreases and never passes the least solution), then holes are stepped over.
 template <int ND, int KIND>
-__host__ __device__ __forceinline__ int64_t stage_point_t(const StageDesc& d, uint32_t rank,
-                                                          int32_t* coord) {
-    if (KIND == 0 && d.kind == 2) return block_anchor_coords(d, rank, coord);
-    if (!d.holes) return stage_coords_t<ND, KIND>(d, rank, coord);
+__host__ __device__ __forceinline__ int64_t stage_point_holes(const StageDesc& d, uint32_t rank,
+                                                              int32_t* coord) {
     uint32_t i = rank;
     int64_t f = stage_coords_t<ND, KIND>(d, i, coord);
     for (int it = 0; it < 256; it++) {
@@ -270,6 +268,19 @@ __host__ __device__ __forceinline__ int64_t stage_point_t(const StageDesc& d, ui
     }
     while (in_blocks<ND>(d, coord) && i + 1 < d.n_full) f = stage_coords_t<ND, KIND>(d, ++i, coord);
     return f;
+}
+
+template <int ND, int KIND>
+__host__ __device__ __forceinline__ int64_t stage_point_t(const StageDesc& d, uint32_t rank,
+                                                          int32_t* coord) {
+    // blocked-anchor stages (kind 2, or with holes) run only on the runtime-
+    // rank instances (ND == 0): the rank-specialised ones keep the plain
+    // decode, with no blocked-anchor code beside it
+    if constexpr (ND == 0) {
+        if (KIND == 0 && d.kind == 2) return block_anchor_coords(d, rank, coord);
+        if (d.holes) return stage_point_holes<ND, KIND>(d, rank, coord);
+    }
+    return stage_coords_t<ND, KIND>(d, rank, coord);
 }
 
 // Runtime-rank form of stage_point_t (host code and rank-generic kernels).
