@@ -317,14 +317,17 @@ def cpu_baseline(steps=1):
     return x.nbytes / best / 1e9, x.nbytes / len(stream)
 
 
-# DRAM bytes (read + write) of one launch of the finest-level fused encode on
-# the 512^3 workload: an ncu capture of the same kernel on the 384^3 field
-# of the same generator (308.7 MB read + 277.5 MB written for the 49.5M
-# points of its finest level), scaled by the points of the 512^3 level
-# (117.4M: (512/384)^3), since the kernel's traffic is per point.
-TRAFFIC_FINEST_ENCODE = (308.710144e6 + 277.469696e6) * (512.0 / 384.0) ** 3
-TRAFFIC_SOURCE = ("ncu capture at 384^3 (dram__bytes_read.sum + dram__bytes_write.sum), "
-                  "scaled by the level's points to 512^3")
+# DRAM bytes (read + write) of one encode pass (31 k_interp_quant and their
+# compaction launches, the default per-stage path) on the 512^3 workload: an
+# ncu capture of the pass on the 384^3 field of the same generator (1,752.8 MB
+# for 56.6 M points), scaled by the points to 512^3; the per-stage kernels
+# are unchanged since (same registers, same stack).
+TRAFFIC_ENCODE_PASS = 4.155e9
+TRAFFIC_SOURCE = ("ncu capture of the pass at 384^3 (dram__bytes_read.sum + "
+                  "dram__bytes_write.sum), scaled by points to 512^3")
+# The same for one launch of the opt-in fused finest-level encode (308.7 MB
+# read + 277.5 MB written for the 49.5 M points of the 384^3 finest level).
+TRAFFIC_FINEST_FUSED = (308.710144e6 + 277.469696e6) * (512.0 / 384.0) ** 3
 
 GNN_SHAPE = (32, 32, 32, 32)
 GNN_FULL_SHAPE = (128, 128, 64, 64)
@@ -765,10 +768,13 @@ def main():
         if i:
             times.append(e0.elapsed_time(e1))
     pass_ms = statistics.median(times)
+    # the opt-in fused finest level (tile mode 1) and the lane coders, timed
+    # with events over whole round trips
+    _lib.check(lib.latec_set_tile_mode(1))
     _lib.check(lib.latec_set_kernel_timing(1))
     for kind in range(6):
         kernel_ms(kind)
-    for i in range(3):  # whole round trips: every timed kind runs in each
+    for i in range(3):
         s_k, _ = lb.compress(x, eb, pred(), levels=LEVELS, anchor_stride=STRIDE, recon="none",
                              stream_out="device")
         out = lb.decompress(s_k, out="device")
@@ -776,6 +782,7 @@ def main():
     torch.cuda.synchronize()
     kt = {k: kernel_ms(k) for k in range(6)}
     _lib.check(lib.latec_set_kernel_timing(0))
+    _lib.check(lib.latec_set_tile_mode(0))
     n_fine = sum(plan.counts[-5:])  # the finest level's five sub-stages
     n_coarse = sum(plan.counts) - n_fine
     es = 4  # float32
@@ -784,26 +791,21 @@ def main():
     enc_ms, n_enc = kt[0]
     dec_ms, n_dec = kt[1]
     peak, peak_kind = _peaks()
-    achieved = enc_alg / (enc_ms / 1e3) / 1e9
     alg_bytes = sum(plan.counts) * (es + es + 2)
+    achieved = alg_bytes / (pass_ms / 1e3) / 1e9
     kernels = {
-        "finest_encode": {"kernel": "k_lvl_enc<float,1,1> (TMA planes)", "launches": n_enc,
-                          "alg_bytes": enc_alg, "kernel_ms": enc_ms,
-                          "achieved_gbs": achieved, "frac": achieved / peak},
-        "finest_decode": {"kernel": "k_lvl_dec<float,1,1> (TMA planes)", "launches": n_dec,
-                          "alg_bytes": dec_alg, "kernel_ms": dec_ms,
-                          "achieved_gbs": dec_alg / (dec_ms / 1e3) / 1e9 if dec_ms else 0.0,
-                          "frac": dec_alg / (dec_ms / 1e3) / 1e9 / peak if dec_ms else 0.0},
-        # per round trip (three were timed): the two coarser fused levels
-        # and the lane rANS coder, one launch each way
-        "coarser_fused_encode_ms": kt[4][0] * kt[4][1] / 3,
-        "coarser_fused_decode_ms": kt[5][0] * kt[5][1] / 3,
+        "fused_finest_encode": {"kernel": "k_lvl_enc<float,1,1> (TMA planes; opt-in, tile mode 1)",
+                                "launches": n_enc, "alg_bytes": enc_alg, "kernel_ms": enc_ms,
+                                "achieved_gbs": enc_alg / (enc_ms / 1e3) / 1e9 if enc_ms else 0.0,
+                                "frac": enc_alg / (enc_ms / 1e3) / 1e9 / peak if enc_ms else 0.0,
+                                "traffic": TRAFFIC_FINEST_FUSED},
+        "fused_finest_decode": {"kernel": "k_lvl_dec<float,1,1> (TMA planes; opt-in, tile mode 1)",
+                                "launches": n_dec, "alg_bytes": dec_alg, "kernel_ms": dec_ms,
+                                "achieved_gbs": dec_alg / (dec_ms / 1e3) / 1e9 if dec_ms else 0.0,
+                                "frac": dec_alg / (dec_ms / 1e3) / 1e9 / peak if dec_ms else 0.0},
+        # per round trip (three were timed): the lane rANS coder, one launch
+        # each way
         "lane_encode_ms": kt[2][0] * kt[2][1] / 3, "lane_decode_ms": kt[3][0] * kt[3][1] / 3,
-        "encode_pass": {"ms": pass_ms, "alg_bytes": alg_bytes,
-                        "achieved_gbs": alg_bytes / (pass_ms / 1e3) / 1e9,
-                        "frac": alg_bytes / (pass_ms / 1e3) / 1e9 / peak,
-                        "scope": "latec_encode_stages: all 31 stages (fused levels and the "
-                                 "per-stage launches of the small ones), compaction included"},
     }
     del rc, enc
     # the drop-in (reference-readable) stream on the same field
@@ -869,11 +871,11 @@ def main():
                    "shape": list(SHAPE), "eb": eb, "parallelism": f"replicas x{world}",
                    "l2": "input 512 MiB > 126 MB L2, no flush"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": TRAFFIC_FINEST_ENCODE,
+                     "frac": achieved / peak, "traffic": TRAFFIC_ENCODE_PASS,
                      "traffic_source": TRAFFIC_SOURCE,
-                     "kernel": "k_lvl_enc: fused encode of the finest level (stride 1, five "
-                               "sub-stages, 117.4 M of 134.2 M points)",
-                     "alg_bytes": enc_alg, "kernel_ms": enc_ms, "peak_kind": peak_kind,
+                     "kernel": "encode pass (latec_encode_stages): 31 k_interp_quant launches, "
+                               "one per stage, and their outlier compaction; 134.2 M points",
+                     "alg_bytes": alg_bytes, "pass_ms": pass_ms, "peak_kind": peak_kind,
                      "kernels": kernels},
         "codec_roofline": {"compress_frac": (nbytes + len(stream)) * args.steps / tc / 1e9 / peak,
                            "decompress_frac": (nbytes + len(stream)) * args.steps / td / 1e9 / peak,

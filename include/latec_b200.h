@@ -168,9 +168,9 @@ int latec_set_level_mode(int32_t mode);
  *      five sub-stages of a level (weight 1 along axes 0, 1, 2, weight 2,
  *      weight 3) in one launch each way, over column tiles of the level's
  *      lattice whose planes are staged in shared memory (TMA loads) with a
- *      3-point halo. 0 = off (one launch per stage), 1 = the finest level,
- *      2 (default) = every level of at least 2^18 points, 3 = every level.
- *      Results are bit-identical in all modes. Process-wide. */
+ *      3-point halo. 0 (default) = off (one launch per stage), 1 = the
+ *      finest level, 2 = every level of at least 2^18 points, 3 = every
+ *      level. Results are bit-identical in all modes. Process-wide. */
 int latec_set_tile_mode(int32_t mode);
 
 /* ---- kernel timing (a measurement aid, no counterpart in the reference):

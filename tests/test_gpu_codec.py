@@ -190,22 +190,29 @@ def test_larger_and_high_rank_fields_match_oracle(shape, lv, stride):
     assert np.abs(back.astype(np.float64) - x).max() <= eb
 
 
+@pytest.mark.parametrize("tile_mode", [0, 2])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
-def test_256cube_stream_matches_oracle(dtype):
+def test_256cube_stream_matches_oracle(dtype, tile_mode):
     """256^3 turbulence + jumps at rel eb 1e-4 (cubic, levels 6, stride 64):
     the benchmark's schedule at a size the CPU oracle codes in seconds, so the
-    fused level kernels' stream (native mode) and reconstruction are compared
-    byte for byte with the oracle's; float64 is the FP64 bound path."""
-    from latec_b200 import fields
+    stream (native mode) and reconstruction are compared byte for byte with
+    the oracle's, with per-stage launches (tile mode 0, the default) and with
+    the fused level kernels (mode 2); float64 is the FP64 bound path."""
+    from latec_b200 import _lib, fields
 
     x = fields.turbulence_jumps((256, 256, 256), seed=2).astype(dtype)
     eb = 1e-4 * float(np.float64(x.max()) - np.float64(x.min()))
     lb = _lb()
-    stream, st = lb.compress(x, eb, lb.InterpPredictor("cubic", 6, 64, 1), levels=6,
-                             anchor_stride=64)
+    lib = _lib.load()
+    _lib.check(lib.latec_set_tile_mode(tile_mode))
+    try:
+        stream, st = lb.compress(x, eb, lb.InterpPredictor("cubic", 6, 64, 1), levels=6,
+                                 anchor_stride=64)
+        back = lb.decompress(stream)
+    finally:
+        _lib.check(lib.latec_set_tile_mode(0))
     ostream, ost = ocodec.compress(x, eb, levels_=6, anchor_stride=64, mode="native")
     assert stream == ostream
-    back = lb.decompress(stream)
     assert np.array_equal(back, ost["recon"])
     assert np.abs(back.astype(np.float64) - x.astype(np.float64)).max() <= eb
 

@@ -63,4 +63,4 @@ def test_level_kernels_match_per_stage_launches(case):
         _mode(0)
         from latec_b200 import _lib
 
-        _lib.check(_lib.load().latec_set_tile_mode(2))  # the default
+        _lib.check(_lib.load().latec_set_tile_mode(0))  # the default

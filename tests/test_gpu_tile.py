@@ -27,7 +27,7 @@ CASES = [
 ]
 
 
-DEFAULT_MODE = 2
+DEFAULT_MODE = 0
 
 
 def _mode(m):
