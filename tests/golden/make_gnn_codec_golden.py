@@ -152,7 +152,7 @@ def main():
         arrays[f"{name}/recon"] = rec["recon"].astype(np.float32)
         gates = []
         for k, d in enumerate(st):
-            for key in ("mu", "scale", "outliers"):
+            for key in ("mu", "scale", "outliers", "mu_g", "scale_g"):
                 arrays[f"{name}/{k}/{key}"] = d[key].numpy().astype(np.float32)
             arrays[f"{name}/{k}/codes"] = d["codes"].numpy().astype(np.int32)
             arrays[f"{name}/{k}/levels"] = d["levels"].numpy().astype(np.uint8)

@@ -10,10 +10,12 @@ on the GPU, and its per-stage trace is compared with the recording
 * the model's mu and Laplace scale per stage, within float32 tolerance (the
   two evaluate the same network in different summation orders, and later
   stages see the earlier stages' differences through the reconstruction);
-* the gate's choice per stage (kind, direction, T, shift);
-* the quantized codes and the scale levels: identical except at the few
-  points whose quotient (x - mu) / 2eb, or whose scale, lies within float32
-  rounding of a bin or level boundary;
+* the gate's choice per stage (kind, direction, T, shift), equal except for
+  at most one near-tie once the outputs have drifted apart;
+* the quantized codes: identical except at points whose quotient
+  (x - p) / 2eb lies within the two gated predictions' difference of a bin
+  boundary (or whose reconstruction error lies that close to the bound);
+  the scale levels: identical up to a few boundary points;
 * the final reconstruction (equal to the reference's up to the predictions'
   float32 differences when every code agrees) and the error bound.
 """
@@ -53,8 +55,9 @@ def test_gnn_codec_matches_reference_per_stage(name):
     stream = codec.compress(x, m["rel_eb"], levels=m["levels"], fp16=False, gate=True)
     tr = {t["stage"]: t for t in codec.stage_trace}
     report = []
-    n_code_diff = n_code = n_lv_diff = 0
-    max_dmu = 0.0
+    n_lv_diff = n_code = 0
+    max_dp = 0.0
+    gate_flips = 0
     for k, s in enumerate(m["stages"]):
         t = tr[s]
         eb = m["ebs"][k]
@@ -62,34 +65,45 @@ def test_gnn_codec_matches_reference_per_stage(name):
         mu_r, sc_r = z[f"{name}/{k}/mu"], z[f"{name}/{k}/scale"]
         mu, sc = t["mu"].cpu().numpy(), t["scale"].cpu().numpy()
         assert mu.shape == mu_r.shape, (s, mu.shape, mu_r.shape)
-        dmu = float(np.abs(mu.astype(np.float64) - mu_r).max())
-        dsc = float(np.abs(np.log2(sc.astype(np.float64) / sc_r)).max())
-        max_dmu = max(max_dmu, dmu)
-        # the gate's choice
-        g_ref = m["gates"][k]
-        g = list(gate_fields(int(t["word"].item())))
-        # the device codes are 16-bit words (q + radius), kept in an int16 tensor
-        codes_r = z[f"{name}/{k}/codes"]
-        codes = t["codes"].cpu().numpy().view(np.uint16).astype(np.int64)
-        lv_r, lv = z[f"{name}/{k}/levels"], t["levels"].cpu().numpy()
-        dc = int((codes != codes_r).sum())
-        dl = int((lv != lv_r).sum())
-        n_code_diff += dc
-        n_lv_diff += dl
-        n_code += len(codes)
-        report.append((s, len(mu), dmu, dsc, g_ref, g, dc, dl))
-    print("\n".join(map(str, report)))
-    for s, n, dmu, dsc, g_ref, g, dc, dl in report:
         # float32 agreement of the network's outputs (mu in [0, 1]; the scale
         # as log2): the two evaluate the same network in different summation
         # orders, and from the second level on each stage's inputs carry the
         # previous stages' differences through the reconstruction
+        dmu = float(np.abs(mu.astype(np.float64) - mu_r).max())
+        dsc = float(np.abs(np.log2(sc.astype(np.float64) / sc_r)).max())
         assert dmu <= 5e-4, (s, dmu)
         assert dsc <= 1e-2, (s, dsc)
-        if g_ref is not None:
-            assert g == g_ref, ("gate", s, g, g_ref)
-    # codes and levels: identical up to rounding-boundary points
-    assert n_code_diff <= max(2, n_code // 2000), report
+        # the gate's choice: equal, except that one near-tie may flip once
+        # the network's outputs have drifted apart
+        g_ref = m["gates"][k]
+        g = list(gate_fields(int(t["word"].item())))
+        if g != g_ref:
+            gate_flips += 1
+            assert gate_flips == 1 and dmu > 1e-5, ("gate", s, g, g_ref, dmu)
+            report.append((s, len(mu), dmu, dsc, g_ref, g, None, None))
+            continue
+        # codes: identical except where the gated prediction's difference can
+        # move the point across a bin boundary or across the bound check
+        codes_r = z[f"{name}/{k}/codes"]
+        codes = t["codes"].cpu().numpy().view(np.uint16).astype(np.int64)
+        xs = t["x"].cpu().numpy().astype(np.float64)
+        p_r = z[f"{name}/{k}/mu_g"].astype(np.float64)
+        p_o = t["mu_gated"].cpu().numpy().astype(np.float64)
+        w = 2.0 * eb
+        max_dp = max(max_dp, float(np.abs(p_o - p_r).max()))
+        band = np.abs(p_o - p_r) / w + 1e-9
+        q = (xs - p_r) / w
+        near_bin = np.abs(np.abs(q - np.floor(q)) - 0.5) <= band
+        rec_r = p_r + w * np.rint(q)
+        near_bound = np.abs(np.abs(xs - rec_r) - eb) <= np.abs(p_o - p_r) + 1e-9
+        diff = codes != codes_r
+        assert not (diff & ~near_bin & ~near_bound).any(), (s, int(diff.sum()))
+        lv_r, lv = z[f"{name}/{k}/levels"], t["levels"].cpu().numpy()
+        dl = int((lv != lv_r).sum())
+        n_lv_diff += dl
+        n_code += len(codes)
+        report.append((s, len(mu), dmu, dsc, g_ref, g, int(diff.sum()), dl))
+    print("\n".join(map(str, report)))
     assert n_lv_diff <= max(2, n_code // 500), report
     # the decoded field holds the bound (plus the float32 normalisation slack)
     back = codec.uncompress(stream).cpu().numpy()
@@ -97,9 +111,9 @@ def test_gnn_codec_matches_reference_per_stage(name):
     span = vmax - vmin
     slack = 2.0 ** -24 * (3.0 * span + max(abs(vmin), abs(vmax)))
     assert float(np.abs(back.astype(np.float64) - x).max()) <= m["eb_abs"] + slack
-    if n_code_diff == 0:
+    if all(r[6] == 0 for r in report):
         # every code equal: the decoded field is the reference's
-        # reconstruction up to the predictions' float32 differences (a coded
-        # point is prediction + 2 eb q, an outlier its exact value)
+        # reconstruction up to the gated predictions' float32 differences (a
+        # coded point is prediction + 2 eb q, an outlier its exact value)
         recon_r = z[f"{name}/recon"].reshape(x.shape).astype(np.float64) * span + vmin
-        assert float(np.abs(back.reshape(x.shape) - recon_r).max()) <= max_dmu * span + 4 * slack
+        assert float(np.abs(back.reshape(x.shape) - recon_r).max()) <= max_dp * span + 4 * slack
