@@ -610,7 +610,8 @@ class GNNCodec:
             lv_all[o:o + n].copy_(rans.scale_to_level(scale, seb))
             if self.stage_trace is not None:
                 tr.update(codes=codes_all[o:o + n].clone(), levels=lv_all[o:o + n].clone(),
-                          mu_gated=mu.clone(), scale_gated=scale.clone(), word=gw[gi].clone(),
+                          mu_gated=mu.clone(), scale_gated=scale.clone(),
+                          word=gw[fine_gi if shared and fine_gi is not None else gi].clone(),
                           recon=recon.clone(), outliers=outl_all[o:o + n].clone())
                 self.stage_trace.append(tr)
             recon_all[:, g.query_idx] = recon.reshape(B, -1)

@@ -11,7 +11,9 @@ not installed) is replaced by a recorder, and the per-stage device steps of
 per stage: the model's mu and scale, the gate's choice (kind, direction, T,
 shift), the gated prediction and scale, the codes, the outliers and the scale
 levels; plus the anchor stage's codes and the final normalised
-reconstruction. Single-chunk cases in 2-D, 3-D and 4-D.
+reconstruction. Single-chunk cases in 2-D, 3-D and 4-D, two of them with
+``gate_fine`` (one gate chosen at the first finest sub-stage and reused by the
+others: no choice is recorded for those).
 
     python tests/golden/make_gnn_codec_golden.py --ref PATH
 """
@@ -28,11 +30,14 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 CKPT = os.path.join(ROOT, "latec_b200", "checkpoints", "gnn_d64_agg1_synthetic.pt")
 
 CASES = [
-    # name, shape, levels, absolute eb, field
-    ("c2d", (48, 40), 3, 1e-3, "grf"),
-    ("c3d", (16, 16, 20), 3, 1e-3, "turb"),
-    ("c4d", (8, 8, 10, 8), 2, 1e-3, "mixed"),
-    ("c2d_l4", (40, 36), 4, 3e-4, "mixed2d"),
+    # name, shape, levels, absolute eb, field, gate_fine
+    ("c2d", (48, 40), 3, 1e-3, "grf", False),
+    ("c3d", (16, 16, 20), 3, 1e-3, "turb", False),
+    ("c4d", (8, 8, 10, 8), 2, 1e-3, "mixed", False),
+    ("c2d_l4", (40, 36), 4, 3e-4, "mixed2d", False),
+    # one gate descriptor shared by the finest level's sub-stages
+    ("c3d_fine", (16, 20, 16), 3, 1e-3, "turb", True),
+    ("c2d_fine", (40, 48), 3, 5e-4, "mixed2d", True),
 ]
 
 
@@ -140,12 +145,13 @@ def main():
 
     codec = GNNCodec(CKPT, device="cpu")
     arrays, meta = {}, []
-    for ci, (name, shape, levels, eb_abs, kind) in enumerate(CASES):
+    for ci, (name, shape, levels, eb_abs, kind, fine) in enumerate(CASES):
         x = np.ascontiguousarray(make_field(kind, shape, 100 + ci), np.float32)
         span = float(np.float32(x.max())) - float(np.float32(x.min()))
         rel = eb_abs / span
         rec["stages"], rec["anchor"], rec["recon"] = [], None, None
-        codec.compress(x, rel, levels=levels, fp16=False, gate=True, compile=False)
+        codec.compress(x, rel, levels=levels, fp16=False, gate=True, gate_fine=fine,
+                       compile=False)
         st = rec["stages"]
         arrays[f"{name}/x"] = x
         arrays[f"{name}/anchor_recon"] = rec["anchor"].astype(np.float32)
@@ -158,7 +164,7 @@ def main():
             arrays[f"{name}/{k}/levels"] = d["levels"].numpy().astype(np.uint8)
             gates.append(d.get("gate"))
         meta.append({"name": name, "shape": list(shape), "levels": levels, "rel_eb": rel,
-                     "eb_abs": eb_abs, "stages": [d["s"] for d in st],
+                     "eb_abs": eb_abs, "gate_fine": fine, "stages": [d["s"] for d in st],
                      "ebs": [d["eb"] for d in st], "gates": gates})
         print(name, shape, "stages", len(st), "gates", gates, flush=True)
     arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), np.uint8)

@@ -11,7 +11,9 @@ on the GPU, and its per-stage trace is compared with the recording
   two evaluate the same network in different summation orders, and later
   stages see the earlier stages' differences through the reconstruction);
 * the gate's choice per stage (kind, direction, T, shift), equal except for
-  at most one near-tie once the outputs have drifted apart;
+  at most one near-tie once the outputs have drifted apart; with
+  ``gate_fine`` the finest sub-stages after the first apply the first one's
+  choice (latec/gnn_codec.py:1229-1262);
 * the quantized codes: identical except at points whose quotient
   (x - p) / 2eb lies within the two gated predictions' difference of a bin
   boundary (or whose reconstruction error lies that close to the bound);
@@ -52,12 +54,15 @@ def test_gnn_codec_matches_reference_per_stage(name):
     x = z[f"{name}/x"]
     codec = lb.GNNCodec(CKPT, device="cuda")
     codec.stage_trace = []
-    stream = codec.compress(x, m["rel_eb"], levels=m["levels"], fp16=False, gate=True)
+    fine = bool(m.get("gate_fine", False))
+    stream = codec.compress(x, m["rel_eb"], levels=m["levels"], fp16=False, gate=True,
+                            gate_fine=fine)
     tr = {t["stage"]: t for t in codec.stage_trace}
     report = []
     n_lv_diff = n_code = 0
     max_dp = 0.0
     gate_flips = 0
+    g_last = None
     for k, s in enumerate(m["stages"]):
         t = tr[s]
         eb = m["ebs"][k]
@@ -76,6 +81,11 @@ def test_gnn_codec_matches_reference_per_stage(name):
         # the gate's choice: equal, except that one near-tie may flip once
         # the network's outputs have drifted apart
         g_ref = m["gates"][k]
+        if g_ref is None:
+            # gate_fine: the finest sub-stages after the first reuse its choice
+            assert fine and g_last is not None, (s, "no gate recorded")
+            g_ref = g_last
+        g_last = g_ref
         g = list(gate_fields(int(t["word"].item())))
         if g != g_ref:
             gate_flips += 1
