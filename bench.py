@@ -496,16 +496,28 @@ def batch_leg(dev, n=BATCH_N, rank=0, world=1):
         sbytes += s.numel()
     total = time.perf_counter() - t0
     # the same tensors through the batch API: one compress_many and one
-    # decompress_many call per rank (warm: the timed serial pass above ran
-    # the same shapes)
+    # decompress_many call per rank, after the encode CTA caps are tuned for
+    # the population's classes and one untimed call of each (the first call
+    # puts every plan's stage descriptors on the device)
+    from latec_b200 import _lib as blib
+
+    tuned = lb.autotune_many(tensors, 1e-3, pred(), levels=4, anchor_stride=16)
+    outs = lb.decompress_many(lb.compress_many(tensors, 1e-3, pred(), levels=4,
+                                               anchor_stride=16, stream_out="device"),
+                              out="device")
+    del outs
+    lib = blib.load()
     torch.cuda.synchronize()
+    l0 = lib.latec_launch_count()
     tb0 = time.perf_counter()
     bs = lb.compress_many(tensors, 1e-3, pred(), levels=4, anchor_stride=16, stream_out="device")
     torch.cuda.synchronize()
     tb1 = time.perf_counter()
+    l1 = lib.latec_launch_count()
     outs = lb.decompress_many(bs, out="device")
     torch.cuda.synchronize()
     tb2 = time.perf_counter()
+    l2 = lib.latec_launch_count()
     del outs, bs
     # the tensors are sharded over the ranks: bytes add up, the slowest rank
     # sets the time
@@ -520,13 +532,22 @@ def batch_leg(dev, n=BATCH_N, rank=0, world=1):
             "cold_pass_gbs": nbytes / cold / 1e9,
             "ratio": nbytes / sbytes, "latency_ms_p50": float(np.percentile(lat_ms, 50)),
             "latency_ms_p99": float(np.percentile(lat_ms, 99)),
-            "mode": "serial loop over the public API per rank (no multi-tensor launch), "
-                    f"tensors sharded over {world} rank(s)",
+            "mode": "serial loop over the public API per rank (one compress + decompress "
+                    f"call per tensor), tensors sharded over {world} rank(s)",
             "latency_scope": "rank 0's tensors",
             "batch_api": {"call": "compress_many + decompress_many, one call each per rank",
                           "gbs": nbytes / (tbc + tbd) / 1e9,
                           "compress_gbs": nbytes / tbc / 1e9,
-                          "decompress_gbs": nbytes / tbd / 1e9}}
+                          "decompress_gbs": nbytes / tbd / 1e9,
+                          "launches_compress": int(l1 - l0),
+                          "launches_decompress": int(l2 - l1),
+                          "stage_launches": "one per stage index and kernel class over all "
+                                            "tensors (latec_encode_stages_many / "
+                                            "latec_decode_stages_many)",
+                          "cta_caps": {"/".join(map(str, k)): v[0]
+                                       for k, v in sorted(tuned.items())},
+                          "cta_caps_key": "rank/value bytes/size class (points < 64Ki, "
+                                          "< 512Ki, < 4Mi, larger)"}}
 
 
 def run_reference(args, rank):
@@ -724,12 +745,12 @@ def main():
     value = world * nbytes / (ms / 1e3) / 1e9
     ratio = nbytes / len(stream)
 
-    # ---- roofline. The dominant kernel is the fused encode of the finest
-    # level (k_lvl_enc: the five sub-stages of stride 1, 87.5 % of the
-    # points); it is timed alone by the CUDA event pairs the library records
-    # on the launching stream around each fused launch. Beside it, the whole
-    # encode pass (latec_encode_stages: every stage, fused or not, with its
-    # compaction) timed with events, and the codec-level fractions.
+    # ---- roofline. The dominant work is the encode pass (latec_encode_stages:
+    # one k_interp_quant launch per stage and its outlier compaction, the
+    # default per-stage launches), timed with CUDA events on the launching
+    # stream. Beside it the opt-in fused finest level (k_lvl_enc / k_lvl_dec,
+    # timed by the event pairs the library records around each fused launch),
+    # the lane coders, and the codec-level fractions.
     from latec_b200 import codec as lcodec
     from latec_b200 import levels as llevels
 

@@ -173,6 +173,16 @@ int latec_set_level_mode(int32_t mode);
  *      level. Results are bit-identical in all modes. Process-wide. */
 int latec_set_tile_mode(int32_t mode);
 
+/* ---- row segments (no counterpart in the reference): 1 = the
+ *      per-stage encode and decode of rank 2..4 single-channel plans walk each
+ *      stage in warp segments of 256 consecutive ranks along the grid rows
+ *      (one rank decode and one set of tap offsets per segment, rows of at
+ *      least 128 stage points; decode tiles with outliers keep the per-point
+ *      path); 0 (default) = one rank decode per point. Results are
+ *      bit-identical.
+ *      Process-wide. */
+int latec_set_row_mode(int32_t on);
+
 /* ---- kernel timing (a measurement aid, no counterpart in the reference):
  *      with timing on, a CUDA event pair is recorded on the launching stream
  *      around every fused level launch and every native lane-coder launch.
@@ -194,6 +204,61 @@ int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
                         const double* stage_eb, const uint16_t* codes, const void* outliers,
                         const uint64_t* out_off, const uint32_t* n_out, void* recon,
                         uint32_t* err, void* workspace, uint64_t workspace_bytes, void* stream);
+
+/* ---- many tensors per call (no counterpart in the reference, whose batch
+ *      form is a serial loop of latec/codec.py:45-285 compress and
+ *      :288-381 decompress). One job per tensor holds the arguments
+ *      latec_encode_stages / latec_decode_stages take for it (stage_eb,
+ *      out_off and n_out are host arrays, the rest device memory as there).
+ *      The jobs' stage passes run stage index by stage index: per stage index
+ *      one launch per kernel class (value type, rank, stage layout) covers
+ *      that stage of every tensor that has it, with one zeroing launch and
+ *      (encode) one outlier-compaction launch beside it. Results equal one
+ *      latec_encode_stages / latec_decode_stages call per job, bit for bit
+ *      (codes, outliers, reconstructions, histograms, counts; the float64
+ *      statistic sums may differ in their last bits when max_ctas changes the
+ *      CTA split); the fused levels of latec_set_tile_mode and the level
+ *      scheduling of latec_set_level_mode are not used. max_ctas: the encode
+ *      CTAs of one stage of the job (0 = the single-tensor default).
+ *      table: device scratch of latec_*_many_table_bytes bytes; the call
+ *      uploads its launch tables there (the host copy is taken before the
+ *      call returns). The stage descriptors of each plan are uploaded to the
+ *      device once, on the plan's first many-tensor call. */
+typedef struct latec_encode_job {
+    const latec_plan* plan;
+    latec_quant_params prm;
+    const double* stage_eb;
+    const void* x;
+    void* recon;
+    uint16_t* codes;
+    void* outliers;
+    latec_stage_stats* stats;
+    uint32_t* hist_seg;
+    uint32_t* hist_total;
+    void* workspace;
+    uint64_t workspace_bytes;
+    uint32_t max_ctas;
+    uint32_t reserved;
+} latec_encode_job;
+
+typedef struct latec_decode_job {
+    const latec_plan* plan;
+    latec_quant_params prm;
+    const double* stage_eb;
+    const uint16_t* codes;
+    const void* outliers;
+    const uint64_t* out_off;
+    const uint32_t* n_out;
+    void* recon;
+    uint32_t* err;
+} latec_decode_job;
+
+uint64_t latec_encode_many_table_bytes(const latec_encode_job* jobs, int32_t n_jobs);
+int latec_encode_stages_many(const latec_encode_job* jobs, int32_t n_jobs, void* table,
+                             uint64_t table_bytes, void* stream);
+uint64_t latec_decode_many_table_bytes(const latec_decode_job* jobs, int32_t n_jobs);
+int latec_decode_stages_many(const latec_decode_job* jobs, int32_t n_jobs, void* table,
+                             uint64_t table_bytes, void* stream);
 
 /* ---- rANS tables: encoder symbols and decoder buckets for `rows` CDF rows
  *      of alphabet + 1 entries (latec/rans.py:304-329 tables, compiled the

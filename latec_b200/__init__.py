@@ -7,11 +7,12 @@ tensors. The compute runs in ``liblatec_b200.so`` (sm_100a); there is no CPU
 fallback.
 """
 
-from .batch import compress_many, decompress_many
+from .batch import autotune_many, compress_many, decompress_many
 from .codec import compress, decompress
 from .gnn_codec import GNNCodec, GNNCompressorCodec
 from .predictor import InterpPredictor
 
-__all__ = ["compress", "decompress", "compress_many", "decompress_many", "InterpPredictor",
+__all__ = ["compress", "decompress", "compress_many", "decompress_many", "autotune_many",
+           "InterpPredictor",
            "GNNCodec", "GNNCompressorCodec"]
 __version__ = "0.1.0"

@@ -40,6 +40,20 @@ class StageStats(ctypes.Structure):
                 ("stats", D * 5)]
 
 
+class EncodeJob(ctypes.Structure):
+    """latec_encode_job: one tensor of latec_encode_stages_many."""
+    _fields_ = [("plan", P), ("prm", QuantParams), ("stage_eb", P), ("x", P), ("recon", P),
+                ("codes", P), ("outliers", P), ("stats", P), ("hist_seg", P),
+                ("hist_total", P), ("workspace", P), ("workspace_bytes", U64),
+                ("max_ctas", U32), ("reserved", U32)]
+
+
+class DecodeJob(ctypes.Structure):
+    """latec_decode_job: one tensor of latec_decode_stages_many."""
+    _fields_ = [("plan", P), ("prm", QuantParams), ("stage_eb", P), ("codes", P),
+                ("outliers", P), ("out_off", P), ("n_out", P), ("recon", P), ("err", P)]
+
+
 # StageStats.done bit set by a fused level encode whose plane loads did not
 # arrive within the kernel's wait limit (its results are not valid).
 TILE_WAIT_FAILED = 0x80000000
@@ -96,6 +110,11 @@ SIGNATURES = {
     "latec_plan_stage_flat": (ctypes.c_int, [P, I32, U64, U64, P]),
     "latec_stage_workspace_bytes": (U64, [P, I32, I32]),
     "latec_flat_workspace_bytes": (U64, [U64, I32]),
+    "latec_set_row_mode": (ctypes.c_int, [I32]),
+    "latec_encode_many_table_bytes": (U64, [P, I32]),
+    "latec_encode_stages_many": (ctypes.c_int, [P, I32, P, U64, P]),
+    "latec_decode_many_table_bytes": (U64, [P, I32]),
+    "latec_decode_stages_many": (ctypes.c_int, [P, I32, P, U64, P]),
     "latec_encode_stages": (ctypes.c_int, [P, ctypes.POINTER(QuantParams), P, P, P, P, P, P, P,
                                            P, P, U64, P]),
     "latec_interp_predict_stage": (ctypes.c_int, [P, I32, ctypes.POINTER(QuantParams), P, P, P]),

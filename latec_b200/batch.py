@@ -37,10 +37,32 @@ from .codec import (_FIT_DTYPE, _RANS_DTYPE, _STATUS, END_MODE_MAX, _Buffers, _c
                     _finalize, _is_gpu_interp, _prepare, _qparams, _raw_frame_size, _torch,
                     buffer_sizes, decompress)
 
-__all__ = ["compress_many", "decompress_many"]
+__all__ = ["compress_many", "decompress_many", "autotune_many", "cta_caps"]
 
 _ALIGN = 256  # bytes: every tensor's slice of a shared buffer starts on this boundary
 _FIT_ROWS = 32768  # stages per model-fit launch
+
+# Encode CTAs per stage for the tensors of a class (rank, value bytes, size
+# class), chosen by autotune_many from timed trials; a class without an entry
+# takes the single-tensor grid (0). Any cap gives the same streams.
+_SIZE_BOUNDS = (1 << 16, 1 << 19, 1 << 22)  # points: < 64 Ki, < 512 Ki, < 4 Mi, larger
+_CTA_CANDIDATES = (148, 296, 592, 1184)
+_cta_caps: dict = {}
+
+
+def size_class(points):
+    """The size class of a tensor of ``points`` values (0 .. 3)."""
+    return sum(int(points) >= b for b in _SIZE_BOUNDS)
+
+
+def cta_caps():
+    """The autotuned table: {(rank, value bytes, size class): encode CTAs}."""
+    return dict(_cta_caps)
+
+
+def cta_cap(ndim, elem, points, caps=None):
+    table = _cta_caps if caps is None else caps
+    return int(table.get((int(ndim), int(elem), size_class(points)), 0))
 
 
 class _View:
@@ -177,6 +199,59 @@ def compress_many(tensors, eb, predictor, levels=4, anchor_stride=16, anchor_blo
     return out
 
 
+
+def autotune_many(tensors, eb, predictor, levels=4, anchor_stride=16, anchor_block=1,
+                  radius=1 << 15, eb_ratio=None, *, device=None, per_class=64, repeats=3,
+                  candidates=_CTA_CANDIDATES):
+    """Choose the encode CTAs per stage of each tensor class (rank, value
+    bytes, size class) present in ``tensors`` for ``compress_many``: the
+    stage pass of up to ``per_class`` tensors of the class is timed (CUDA
+    events, best of ``repeats``) at each candidate cap, and the fastest is
+    kept in the table ``compress_many`` reads. Returns {class: (cap, ms)}."""
+    torch = _torch()
+    lib = _lib.load()
+    if not _is_gpu_interp(predictor):
+        raise NotImplementedError("autotune_many times InterpPredictor stages on the device")
+    dev = torch.device(device) if device is not None else torch.device(
+        "cuda", torch.cuda.current_device())
+    groups = {}
+    for x in tensors:
+        jb = _Job(0, x, eb, predictor, levels, anchor_stride, anchor_block, radius, eb_ratio, dev)
+        key = (len(jb.spatial), jb.elem, size_class(jb.field.numel()))
+        if len(groups.setdefault(key, [])) < per_class:
+            groups[key].append(jb)
+    out = {}
+    for key, jobs in sorted(groups.items()):
+        views, _ = _arenas([buffer_sizes(jb.plan, jb.c, jb.elem) for jb in jobs], dev)
+        esz = jobs[0].field.element_size()
+        rsz = [-(-jb.field.numel() * esz // _ALIGN) * _ALIGN for jb in jobs]
+        recon = torch.zeros(max(sum(rsz), 1), dtype=torch.uint8, device=dev)
+        roff = np.concatenate([[0], np.cumsum(rsz)[:-1]]).astype(np.int64).tolist()
+        for jb, v, ro in zip(jobs, views, roff):
+            jb.buf = _Buffers(jb.plan, jb.c, jb.src, dev, views=v)
+            jb.recon = _View(recon.data_ptr() + ro, jb.field.numel())
+        best = None
+        for cap in candidates:
+            caps = {key: int(cap)}
+            _stage_pass(jobs, predictor, dev, lib, caps)  # warm-up
+            ms = []
+            for _ in range(repeats):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record()
+                _stage_pass(jobs, predictor, dev, lib, caps)
+                b.record()
+                b.synchronize()
+                ms.append(a.elapsed_time(b))
+            t = min(ms)
+            if best is None or t < best[1]:
+                best = (int(cap), t)
+        for jb in jobs:
+            del jb.buf, jb.recon
+        _cta_caps[key] = best[0]
+        out[key] = best
+    return out
+
 def _download(views):
     """Device streams -> bytes, through one pinned buffer and one wait."""
     torch = _torch()
@@ -200,18 +275,10 @@ def _compress_group(jobs, predictor, dev, lib):
     rsz = [-(-jb.field.numel() * esz // _ALIGN) * _ALIGN for jb in jobs]
     recon = torch.zeros(max(sum(rsz), 1), dtype=torch.uint8, device=dev)
     roff = np.concatenate([[0], np.cumsum(rsz)[:-1]]).astype(np.int64).tolist()
-    # ---- stage kernels of every tensor, back to back
     for jb, v, ro in zip(jobs, views, roff):
-        jb.buf = b = _Buffers(jb.plan, jb.c, jb.src, dev, views=v)
+        jb.buf = _Buffers(jb.plan, jb.c, jb.src, dev, views=v)
         jb.recon = _View(recon.data_ptr() + ro, jb.field.numel())
-        prm = _qparams(jb.src, jb.c, jb.radius, predictor.order, jb.center, jb.end_mode,
-                       jb.src == 0)
-        ns = len(jb.plan)
-        eb_arr = (ctypes.c_double * ns)(*[float(e) for e in jb.ebs])
-        _lib.check(lib.latec_encode_stages(
-            jb.plan.handle, ctypes.byref(prm), eb_arr, jb.field.data_ptr(), jb.recon.data_ptr(),
-            b.codes.data_ptr(), b.outliers.data_ptr(), b.stats.data_ptr(), b.hist_seg.data_ptr(),
-            b.hist_total.data_ptr(), b.ws.data_ptr(), b.ws.numel(), sp), "latec_encode_stages")
+    _stage_pass(jobs, predictor, dev, lib)
     raw = bufs["stats"][0].cpu().numpy().tobytes()  # one download: every stage's statistics
     stage0 = np.cumsum([0] + [len(jb.plan) for jb in jobs]).tolist()
     for j, jb in enumerate(jobs):
@@ -236,6 +303,38 @@ def _compress_group(jobs, predictor, dev, lib):
         del jb.buf, jb.recon
     return [streams[soff[j]:soff[j + 1]] for j in range(len(jobs))]
 
+
+
+def _stage_pass(jobs, predictor, dev, lib, caps=None):
+    """Every stage of every tensor (buffers set up in ``jb.buf``, ``jb.recon``):
+    stage index by stage index, one launch per kernel class over all tensors
+    (latec_encode_stages_many). ``caps``: encode CTAs per stage by tensor
+    class, default the autotuned table."""
+    torch = _torch()
+    ej = (_lib.EncodeJob * len(jobs))()
+    keep = []
+    for k, jb in enumerate(jobs):
+        b = jb.buf
+        e = ej[k]
+        e.plan = jb.plan.handle
+        e.prm = _qparams(jb.src, jb.c, jb.radius, predictor.order, jb.center, jb.end_mode,
+                         jb.src == 0)
+        eb_arr = (ctypes.c_double * len(jb.plan))(*[float(x) for x in jb.ebs])
+        keep.append(eb_arr)
+        e.stage_eb = ctypes.addressof(eb_arr)
+        e.x, e.recon = jb.field.data_ptr(), jb.recon.data_ptr()
+        e.codes, e.outliers = b.codes.data_ptr(), b.outliers.data_ptr()
+        e.stats, e.hist_seg, e.hist_total = (b.stats.data_ptr(), b.hist_seg.data_ptr(),
+                                             b.hist_total.data_ptr())
+        e.workspace, e.workspace_bytes = b.ws.data_ptr(), b.ws.numel()
+        e.max_ctas = cta_cap(len(jb.spatial), jb.elem, jb.field.numel(), caps)
+    tb = int(lib.latec_encode_many_table_bytes(ej, len(jobs)))
+    if not tb:
+        raise ValueError("latec_encode_many_table_bytes: invalid job")
+    table = torch.empty(tb, dtype=torch.uint8, device=dev)
+    _lib.check(lib.latec_encode_stages_many(ej, len(jobs), table.data_ptr(), tb,
+                                            _lib.stream_ptr()), "latec_encode_stages_many")
+    del keep
 
 def _fit_all(jobs, bufs, stage0, dev, lib):
     """The native stage-model fit (the rule of ``codec._Encoder._fit_native``)
@@ -520,8 +619,11 @@ def decompress_many(streams, *, device=None, out="numpy"):
                                      ranges.data_ptr() if ch0[-1] else None, None,
                                      codes.data_ptr(), errs.data_ptr() + 4 * len(idx),
                                      ws.data_ptr(), ws.numel(), sp), "latec_rans_decode")
-    # ---- each field rebuilt by its stage kernels
+    # ---- every field rebuilt by the stage kernels: stage index by stage
+    # index, one launch per kernel class over all fields
     canv = []
+    dj = (_lib.DecodeJob * len(heads))()
+    hold = []
     for k, h in enumerate(heads):
         c = chans[k]
         pred = InterpPredictor("cubic" if h.flags & FLAG_CUBIC else "linear", h.levels,
@@ -530,7 +632,6 @@ def decompress_many(streams, *, device=None, out="numpy"):
         ebs = _levels.stage_ebs(spatial[k], h.levels, h.anchor_stride, h.anchor_block, h.eb,
                                 h.eb_ratio)
         ns = nss[k]
-        ldt = _lib.F64 if h.src_dtype == 2 else _lib.F32
         prm = _qparams(h.src_dtype, c, h.radius, pred.order, h.interp_center, end_mode,
                        h.src_dtype == 0)
         ft = torch.float64 if h.src_dtype == 2 else torch.float32
@@ -538,15 +639,22 @@ def decompress_many(streams, *, device=None, out="numpy"):
         eb_arr = (ctypes.c_double * ns)(*[float(e) for e in ebs])
         out_at = (ctypes.c_uint64 * ns)(*[recs[st0[k] + t].out_at for t in range(ns)])
         n_out = (ctypes.c_uint32 * ns)(*[recs[st0[k] + t].n_out for t in range(ns)])
-        ws2 = torch.empty(max(int(lib.latec_stage_workspace_bytes(plans[k].handle, c, ldt)), 1),
-                          dtype=torch.uint8, device=dev)
-        _lib.check(lib.latec_decode_stages(plans[k].handle, ctypes.byref(prm), eb_arr,
-                                           codes.data_ptr() + 2 * code_off[k][0],
-                                           pay.data_ptr() + pay_off[k], out_at, n_out,
-                                           recon.data_ptr(), errs.data_ptr() + 4 * k,
-                                           ws2.data_ptr(), ws2.numel(), sp),
-                   "latec_decode_stages")
+        d = dj[k]
+        d.plan, d.prm = plans[k].handle, prm
+        d.stage_eb, d.out_off, d.n_out = (ctypes.addressof(eb_arr), ctypes.addressof(out_at),
+                                          ctypes.addressof(n_out))
+        d.codes = codes.data_ptr() + 2 * code_off[k][0]
+        d.outliers = pay.data_ptr() + pay_off[k]
+        d.recon, d.err = recon.data_ptr(), errs.data_ptr() + 4 * k
+        hold.append((eb_arr, out_at, n_out))
         canv.append(recon)
+    tb = int(lib.latec_decode_many_table_bytes(dj, len(heads)))
+    if not tb:
+        raise ValueError("latec_decode_many_table_bytes: invalid job")
+    table = torch.empty(tb, dtype=torch.uint8, device=dev)
+    _lib.check(lib.latec_decode_stages_many(dj, len(heads), table.data_ptr(), tb, sp),
+               "latec_decode_stages_many")
+    del hold
     e = errs.cpu().numpy()  # one download: every stream's error word
     del keep
     lane = int(e[-1])

@@ -24,6 +24,8 @@ void count_launches(unsigned n) { g_launches.fetch_add(n, std::memory_order_rela
 static_assert(sizeof(latec_stage_stats) == sizeof(StageAcc), "stats layout");
 static_assert(sizeof(latec_rans_stage) == sizeof(RansStageDesc), "rans stage layout");
 static_assert(sizeof(EncSym) == 32, "encoder symbol layout");
+static_assert(sizeof(latec_encode_job) == 144 && sizeof(latec_decode_job) == 112,
+              "many-tensor job layouts (the Python binding mirrors them)");
 
 namespace {
 
@@ -342,6 +344,125 @@ bool build_level(const latec_plan* plan, int t0, int t1, int C, int elem, int mo
     return true;
 }
 
+// ---- many tensors per call
+
+// The plan's stage descriptors on the current device, uploaded on first use.
+const StageDesc* plan_dev_stages(const latec_plan* cp) {
+    latec_plan* p = const_cast<latec_plan*>(cp);  // the device copy is a cache
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lk(p->dev_mu);
+    if (p->dev_stages && p->dev_id == dev) return p->dev_stages;
+    if (p->dev_stages) {
+        cudaFree(p->dev_stages);
+        p->dev_stages = nullptr;
+    }
+    const size_t n = p->stages.size() ? p->stages.size() : 1;
+    StageDesc* d = nullptr;
+    if (cudaMalloc(&d, sizeof(StageDesc) * n) != cudaSuccess) return nullptr;
+    if (!p->stages.empty() &&
+        cudaMemcpy(d, p->stages.data(), sizeof(StageDesc) * p->stages.size(),
+                   cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(d);
+        return nullptr;
+    }
+    p->dev_stages = d;
+    p->dev_id = dev;
+    return d;
+}
+
+// Kernel class of a stage: value type, rank (runtime rank for blocked
+// anchors and ranks outside 2..4), layout, order.
+inline int many_nd(const StageDesc& d) {
+    return (d.ndim >= 2 && d.ndim <= 4 && !d.holes && d.kind != 2) ? d.ndim : 0;
+}
+inline int many_key(int dtype, const StageDesc& d, int order) {
+    return (((dtype == LATEC_F64 ? 1 : 0) * 8 + many_nd(d)) * 2 + (d.kind == 1 ? 1 : 0)) * 2 +
+           (order ? 1 : 0);
+}
+
+// Launch tables of a many-tensor call, built on the host and uploaded in one
+// copy: 16-byte aligned records appended in launch order.
+struct HostTable {
+    std::vector<uint8_t> buf;
+    template <typename T>
+    uint64_t put(const T* p, size_t n) {
+        const uint64_t off = (buf.size() + 15) & ~uint64_t(15);
+        buf.resize(off + sizeof(T) * n);
+        if (n) std::memcpy(buf.data() + off, p, sizeof(T) * n);
+        return off;
+    }
+    uint64_t size() const { return (buf.size() + 15) & ~uint64_t(15); }
+};
+
+struct ManyLaunch {
+    int op;         // 0 zero ranges, 1 quantize, 2 compact, 3 dequantize
+    int key;        // kernel class (op 1)
+    uint64_t recs;  // table offset of the ZeroRange / ManyJob / DecStage records
+    uint64_t first; // table offset of the first-CTA array
+    uint32_t n;     // records
+    uint32_t ctas;  // grid
+};
+
+// Zero ranges in chunks of ZERO_CHUNK words per CTA.
+void add_zero_launch(HostTable& T, std::vector<ManyLaunch>& L, const std::vector<ZeroRange>& r) {
+    std::vector<ZeroRange> keep;
+    std::vector<uint32_t> first;
+    uint64_t ctas = 0;
+    for (const ZeroRange& z : r) {
+        if (!z.words) continue;
+        keep.push_back(z);
+        first.push_back((uint32_t)ctas);
+        ctas += (z.words + ZERO_CHUNK - 1) / ZERO_CHUNK;
+    }
+    if (keep.empty()) return;
+    ManyLaunch l{0, 0, T.put(keep.data(), keep.size()), T.put(first.data(), first.size()),
+                 (uint32_t)keep.size(), (uint32_t)ctas};
+    L.push_back(l);
+}
+
+// One step's jobs laid out by kernel class; a launch per class (op 1
+// quantize, 3 dequantize) and, for the encoder, one compaction launch over
+// all of them (op 2).
+void add_step_launches(HostTable& T, std::vector<ManyLaunch>& L, std::vector<ManyJob>& jobs,
+                       const std::vector<int>& keys, int op, bool compact) {
+    if (jobs.empty()) return;
+    std::vector<size_t> order(jobs.size());
+    for (size_t k = 0; k < order.size(); k++) order[k] = k;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t a, size_t b) { return keys[a] < keys[b]; });
+    std::vector<ManyJob> sorted;
+    sorted.reserve(jobs.size());
+    for (size_t k : order) sorted.push_back(jobs[k]);
+    const uint64_t recs = T.put(sorted.data(), sorted.size());
+    size_t a = 0;
+    while (a < order.size()) {
+        size_t e = a;
+        std::vector<uint32_t> first;
+        uint64_t ctas = 0;
+        while (e < order.size() && keys[order[e]] == keys[order[a]]) {
+            first.push_back((uint32_t)ctas);
+            ctas += sorted[e].blocks;
+            e++;
+        }
+        ManyLaunch l{op, keys[order[a]], recs + sizeof(ManyJob) * a,
+                     T.put(first.data(), first.size()), (uint32_t)(e - a), (uint32_t)ctas};
+        L.push_back(l);
+        a = e;
+    }
+    if (compact) {
+        std::vector<uint32_t> first;
+        uint64_t ctas = 0;
+        for (const ManyJob& j : sorted) {
+            first.push_back((uint32_t)ctas);
+            ctas += j.cblocks;
+        }
+        ManyLaunch l{2, 0, recs, T.put(first.data(), first.size()), (uint32_t)sorted.size(),
+                     (uint32_t)ctas};
+        L.push_back(l);
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -355,6 +476,12 @@ int latec_set_level_mode(int32_t mode) {
 int latec_set_tile_mode(int32_t mode) {
     if (mode < 0 || mode > 3) return LATEC_ERR_ARG;
     g_tile_mode.store(mode);
+    return LATEC_OK;
+}
+
+int latec_set_row_mode(int32_t on) {
+    if (on < 0 || on > 1) return LATEC_ERR_ARG;
+    g_row_mode.store(on);
     return LATEC_OK;
 }
 
@@ -603,12 +730,12 @@ int latec_dequantize(const latec_quant_params* prm, double eb, uint64_t items, c
     const uint32_t tiles = n_tiles(items);
     uint32_t* tile_cnt = c.take<uint32_t>(tiles + 1);
     uint32_t* tile_off = c.take<uint32_t>(tiles + 1);
-    DecStage h{0, items, 0, n_out};
+    DecStage h{codes, err, items, 0, n_out};
     if (cudaMemcpyAsync(ds, &h, sizeof(h), cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemsetAsync(tile_cnt, 0, sizeof(uint32_t) * tiles, st) != cudaSuccess)
         return LATEC_ERR_CUDA;
-    int rc = launch_count_zeros_all(ds, 1, tiles, codes, tile_cnt, st);
-    if (!rc) rc = launch_tile_offsets_all(ds, 1, tile_cnt, tile_off, err, st);
+    int rc = launch_count_zeros_all(ds, 1, tiles, tile_cnt, st);
+    if (!rc) rc = launch_tile_offsets_all(ds, 1, tile_cnt, tile_off, st);
     if (!rc)
         rc = launch_dequant_flat(q, prm->dtype, items, pred, codes, outliers, tile_cnt, tile_off,
                                  n_out, recon_out, err, st);
@@ -632,19 +759,21 @@ int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
     cudaStream_t st = (cudaStream_t)stream;
     // all stages' outlier tiles in two launches
     std::vector<DecStage> ds(ns);
+    std::vector<uint64_t> coff(ns);  // first code of each stage
     uint64_t off = 0;
     uint32_t tile0 = 0;
     for (int t = 0; t < ns; t++) {
         const uint64_t items = (uint64_t)plan->stages[t].n * C;
-        ds[t] = DecStage{off, items, tile0, n_out[t]};
+        ds[t] = DecStage{codes + off, err, items, tile0, n_out[t]};
+        coff[t] = off;
         off += items;
         tile0 += n_tiles(items);
     }
     if (cudaMemcpyAsync(w.dec, ds.data(), sizeof(DecStage) * ns, cudaMemcpyHostToDevice, st) !=
         cudaSuccess)
         return LATEC_ERR_CUDA;
-    int rc = launch_count_zeros_all(w.dec, ns, tile0, codes, w.tile_cnt, st);
-    if (!rc) rc = launch_tile_offsets_all(w.dec, ns, w.tile_cnt, w.tile_off, err, st);
+    int rc = launch_count_zeros_all(w.dec, ns, tile0, w.tile_cnt, st);
+    if (!rc) rc = launch_tile_offsets_all(w.dec, ns, w.tile_cnt, w.tile_off, st);
     if (rc) return rc;
     const int mode = g_level_mode.load();
     const int tmode = g_tile_mode.load();
@@ -660,7 +789,7 @@ int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
                 if (!n_out[t + j] || !dj.items || !outliers) continue;
                 ScatterStage& S = sa.s[sa.n++];
                 S.d = plan->stages[t + j];
-                S.codes = codes + dj.codes_off;
+                S.codes = codes + coff[t + j];
                 S.outliers = (const uint8_t*)outliers + out_off[t + j];
                 S.tile_cnt = w.tile_cnt + dj.tile0;
                 S.tile_off = w.tile_off + dj.tile0;
@@ -676,7 +805,7 @@ int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
             TileLevel L;
             uint32_t grid;
             if (!tile_level_init(plan, prm, stage_eb, t, C, const_cast<uint16_t*>(codes),
-                                 ds[t].codes_off, L, &grid))
+                                 coff[t], L, &grid))
                 return LATEC_ERR_ARG;
             L.tma = tile_tma_ok(L, elem_of(prm->dtype), recon, recon) ? 1 : 0;
             const int ki = kt_start(plan->stages[t].s == 1 ? 1 : 5, st);
@@ -700,7 +829,7 @@ int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
                 memset(&ls, 0, sizeof(ls));
                 ls.d = plan->stages[t + j];
                 if (!make_q(prm, stage_eb[t + j], plan->points, ls.q)) return LATEC_ERR_ARG;
-                ls.codes = codes + ds[t + j].codes_off;
+                ls.codes = codes + coff[t + j];
                 ls.outliers = outliers ? (const uint8_t*)outliers + out_off[t + j] : nullptr;
                 ls.tile_cnt = w.tile_cnt + ds[t + j].tile0;
                 ls.tile_off = w.tile_off + ds[t + j].tile0;
@@ -730,7 +859,7 @@ int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
             if (!ds[t].items) continue;
             QParams q;
             if (!make_q(prm, stage_eb[t], plan->points, q)) return LATEC_ERR_ARG;
-            rc = launch_interp_dequant(d, q, prm->dtype, t == 0, codes + ds[t].codes_off,
+            rc = launch_interp_dequant(d, q, prm->dtype, t == 0, codes + coff[t],
                                        outliers ? (const uint8_t*)outliers + out_off[t] : nullptr,
                                        w.tile_cnt + ds[t].tile0, w.tile_off + ds[t].tile0,
                                        n_out[t], recon, err, st);
@@ -738,6 +867,257 @@ int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
         }
     }
     return LATEC_OK;
+}
+
+// Launch tables of latec_encode_stages_many (see the header).
+static int encode_many_build(const latec_encode_job* jobs, int n, HostTable& T,
+                             std::vector<ManyLaunch>& L) {
+    if (n < 0 || (n && !jobs)) return LATEC_ERR_ARG;
+    std::vector<StageWs> ws(n);
+    std::vector<const StageDesc*> dev(n);
+    std::vector<uint64_t> off(n, 0), seg(n, 0);
+    std::vector<ZeroRange> zr;
+    int max_ns = 0;
+    for (int j = 0; j < n; j++) {
+        const latec_encode_job& J = jobs[j];
+        const latec_plan* plan = J.plan;
+        if (!plan || !valid_params(&J.prm) || !J.stage_eb || !J.x || !J.recon || !J.codes ||
+            !J.outliers || !J.stats || !J.hist_seg || !J.hist_total)
+            return LATEC_ERR_ARG;
+        const int C = J.prm.channels, ns = (int)plan->stages.size();
+        if (!J.workspace ||
+            J.workspace_bytes < latec_stage_workspace_bytes(plan, C, J.prm.dtype))
+            return LATEC_ERR_WORKSPACE;
+        uint64_t m, tiles_all;
+        plan_sizes(plan, C, &m, &tiles_all);
+        stage_ws(m, tiles_all, ns, elem_of(J.prm.dtype), &ws[j], J.workspace);
+        if (!(dev[j] = plan_dev_stages(plan))) return LATEC_ERR_CUDA;
+        uint64_t total_segs = 0;
+        for (auto& d : plan->stages) total_segs += n_segments((uint64_t)d.n * C);
+        zr.push_back(ZeroRange{(uint32_t*)J.stats, sizeof(latec_stage_stats) * ns / 4});
+        zr.push_back(ZeroRange{J.hist_seg, (uint64_t)HBINS * total_segs});
+        zr.push_back(ZeroRange{J.hist_total, 65536ull * ns});
+        max_ns = ns > max_ns ? ns : max_ns;
+    }
+    add_zero_launch(T, L, zr);
+    for (int t = 0; t < max_ns; t++) {
+        std::vector<ManyJob> step;
+        std::vector<int> keys;
+        zr.clear();
+        for (int j = 0; j < n; j++) {
+            const latec_encode_job& J = jobs[j];
+            if (t >= (int)J.plan->stages.size()) continue;
+            const StageDesc& d = J.plan->stages[t];
+            const int elem = elem_of(J.prm.dtype);
+            const uint64_t items = (uint64_t)d.n * J.prm.channels;
+            const uint64_t o = off[j], sg = seg[j];
+            off[j] += items;
+            seg[j] += n_segments(items);
+            if (!items) continue;
+            ManyJob mj;
+            std::memset(&mj, 0, sizeof(mj));
+            if (!make_q(&J.prm, J.stage_eb[t], J.plan->points, mj.q)) return LATEC_ERR_ARG;
+            const uint32_t cap = J.max_ctas && J.max_ctas < (uint32_t)MAX_BLOCKS
+                                     ? J.max_ctas : (uint32_t)MAX_BLOCKS;
+            const StageWs& w = ws[j];
+            mj.d = dev[j] + t;
+            mj.x = J.x;
+            mj.recon = J.recon;
+            mj.codes = J.codes + o;
+            mj.staging = w.staging;
+            mj.tile_cnt = w.tile_cnt;
+            mj.tile_off = w.tile_off;
+            mj.hist_total = J.hist_total + 65536ull * t;
+            mj.hist_seg = J.hist_seg + (uint64_t)HBINS * sg;
+            mj.acc = (StageAcc*)(J.stats + t);
+            mj.partials = w.partials;
+            mj.out = (uint8_t*)J.outliers + o * elem;
+            mj.items = items;
+            mj.gpb = encode_grid(items, cap, &mj.blocks);
+            mj.is_anchor = t == 0 ? 1u : 0u;
+            mj.elem = (uint32_t)elem;
+            const uint32_t tiles = n_tiles(items);
+            mj.cblocks = tiles < 592u ? tiles : 592u;
+            zr.push_back(ZeroRange{w.tile_cnt, tiles});
+            step.push_back(mj);
+            keys.push_back(many_key(J.prm.dtype, d, J.prm.order));
+        }
+        add_zero_launch(T, L, zr);
+        add_step_launches(T, L, step, keys, 1, true);
+    }
+    return LATEC_OK;
+}
+
+static int run_many(const std::vector<ManyLaunch>& L, const HostTable& T, uint64_t upload,
+                    void* table, cudaStream_t st) {
+    if (upload && cudaMemcpyAsync(table, T.buf.data(), upload, cudaMemcpyHostToDevice, st) !=
+                      cudaSuccess)
+        return LATEC_ERR_CUDA;
+    uint8_t* tb = (uint8_t*)table;
+    for (const ManyLaunch& l : L) {
+        const uint32_t* first = (const uint32_t*)(tb + l.first);
+        int rc = LATEC_OK;
+        const int k = l.key, dtype = ((k >> 5) & 1) ? LATEC_F64 : LATEC_F32;
+        const int nd = (k >> 2) & 7, kind = (k >> 1) & 1, cubic = k & 1;
+        switch (l.op) {
+            case 0:
+                rc = launch_zero_many((const ZeroRange*)(tb + l.recs), first, l.n, l.ctas, st);
+                break;
+            case 1:
+                rc = launch_quant_many(dtype, nd, kind, cubic, (const ManyJob*)(tb + l.recs),
+                                       first, l.n, l.ctas, st);
+                break;
+            case 2:
+                rc = launch_compact_many((const ManyJob*)(tb + l.recs), first, l.n, l.ctas, st);
+                break;
+            case 3:
+                rc = launch_dequant_many(dtype, nd, kind, cubic, (const ManyJob*)(tb + l.recs),
+                                         first, l.n, l.ctas, st);
+                break;
+            default:
+                rc = LATEC_ERR_INTERNAL;
+        }
+        if (rc) return rc;
+    }
+    return LATEC_OK;
+}
+
+uint64_t latec_encode_many_table_bytes(const latec_encode_job* jobs, int32_t n_jobs) {
+    HostTable T;
+    std::vector<ManyLaunch> L;
+    if (encode_many_build(jobs, n_jobs, T, L)) return 0;
+    return T.size() ? T.size() : 16;
+}
+
+int latec_encode_stages_many(const latec_encode_job* jobs, int32_t n_jobs, void* table,
+                             uint64_t table_bytes, void* stream) {
+    HostTable T;
+    std::vector<ManyLaunch> L;
+    const int rc = encode_many_build(jobs, n_jobs, T, L);
+    if (rc) return rc;
+    if (T.size() && (!table || table_bytes < T.size())) return LATEC_ERR_WORKSPACE;
+    return run_many(L, T, T.buf.size(), table, (cudaStream_t)stream);
+}
+
+// Launch tables of latec_decode_stages_many: the all-stage outlier tile
+// passes over every stage of every job (records at offset `dec`, the tile
+// counts and offsets after the uploaded part), then the dequantize steps.
+struct DecodeMany {
+    uint64_t dec = 0;         // DecStage records
+    uint32_t n_dec = 0;
+    uint64_t tiles = 0;       // tiles of all stages
+    uint64_t tile_cnt = 0;    // table offsets of the two tile arrays
+    uint64_t tile_off = 0;
+    uint64_t upload = 0;      // bytes uploaded (the records)
+    uint64_t total = 0;       // table bytes
+};
+
+static int decode_many_build(const latec_decode_job* jobs, int n, HostTable& T,
+                             std::vector<ManyLaunch>& L, DecodeMany& D) {
+    if (n < 0 || (n && !jobs)) return LATEC_ERR_ARG;
+    std::vector<DecStage> ds;
+    std::vector<std::vector<uint64_t>> coff(n);
+    std::vector<std::vector<uint32_t>> tile0(n);
+    std::vector<const StageDesc*> dev(n);
+    int max_ns = 0;
+    uint64_t tiles = 0;
+    for (int j = 0; j < n; j++) {
+        const latec_decode_job& J = jobs[j];
+        const latec_plan* plan = J.plan;
+        if (!plan || !valid_params(&J.prm) || !J.stage_eb || !J.codes || !J.out_off ||
+            !J.n_out || !J.recon || !J.err)
+            return LATEC_ERR_ARG;
+        if (!(dev[j] = plan_dev_stages(plan))) return LATEC_ERR_CUDA;
+        const int ns = (int)plan->stages.size();
+        max_ns = ns > max_ns ? ns : max_ns;
+        uint64_t off = 0;
+        for (int t = 0; t < ns; t++) {
+            const uint64_t items = (uint64_t)plan->stages[t].n * J.prm.channels;
+            if (J.n_out[t] && !J.outliers) return LATEC_ERR_ARG;
+            coff[j].push_back(off);
+            tile0[j].push_back((uint32_t)tiles);
+            ds.push_back(DecStage{J.codes + off, J.err, items, (uint32_t)tiles, J.n_out[t]});
+            off += items;
+            tiles += n_tiles(items);
+            if (tiles >= (1ull << 32)) return LATEC_ERR_TOO_LARGE;
+        }
+    }
+    D.dec = T.put(ds.data(), ds.size());
+    D.n_dec = (uint32_t)ds.size();
+    D.tiles = tiles;
+    for (int t = 0; t < max_ns; t++) {
+        std::vector<ManyJob> step;
+        std::vector<int> keys;
+        for (int j = 0; j < n; j++) {
+            const latec_decode_job& J = jobs[j];
+            if (t >= (int)J.plan->stages.size()) continue;
+            const StageDesc& d = J.plan->stages[t];
+            const uint64_t items = (uint64_t)d.n * J.prm.channels;
+            if (!items) continue;
+            ManyJob mj;
+            std::memset(&mj, 0, sizeof(mj));
+            if (!make_q(&J.prm, J.stage_eb[t], J.plan->points, mj.q)) return LATEC_ERR_ARG;
+            mj.d = dev[j] + t;
+            mj.recon = J.recon;
+            mj.codes_in = J.codes + coff[j][t];
+            mj.outliers = J.outliers ? (const uint8_t*)J.outliers + J.out_off[t] : nullptr;
+            mj.err = J.err;
+            mj.items = items;
+            mj.blocks = n_tiles(items);
+            mj.is_anchor = t == 0 ? 1u : 0u;
+            mj.elem = (uint32_t)elem_of(J.prm.dtype);
+            mj.n_out = J.n_out[t];
+            // tile arrays: patched to device addresses once the table is placed
+            mj.tile_cnt = (uint32_t*)(uintptr_t)tile0[j][t];
+            step.push_back(mj);
+            keys.push_back(many_key(J.prm.dtype, d, J.prm.order));
+        }
+        add_step_launches(T, L, step, keys, 3, false);
+    }
+    D.upload = T.buf.size();
+    D.tile_cnt = T.size();
+    D.tile_off = D.tile_cnt + ((tiles + 1) * 4 + 15) / 16 * 16;
+    D.total = D.tile_off + ((tiles + 1) * 4 + 15) / 16 * 16;
+    return LATEC_OK;
+}
+
+uint64_t latec_decode_many_table_bytes(const latec_decode_job* jobs, int32_t n_jobs) {
+    HostTable T;
+    std::vector<ManyLaunch> L;
+    DecodeMany D;
+    if (decode_many_build(jobs, n_jobs, T, L, D)) return 0;
+    return D.total ? D.total : 16;
+}
+
+int latec_decode_stages_many(const latec_decode_job* jobs, int32_t n_jobs, void* table,
+                             uint64_t table_bytes, void* stream) {
+    HostTable T;
+    std::vector<ManyLaunch> L;
+    DecodeMany D;
+    const int rc = decode_many_build(jobs, n_jobs, T, L, D);
+    if (rc) return rc;
+    if (!n_jobs || !D.n_dec) return LATEC_OK;
+    if (!table || table_bytes < D.total) return LATEC_ERR_WORKSPACE;
+    uint8_t* tb = (uint8_t*)table;
+    uint32_t* tile_cnt = (uint32_t*)(tb + D.tile_cnt);
+    uint32_t* tile_off = (uint32_t*)(tb + D.tile_off);
+    // the dequantize records point at their stage's slice of the tile arrays
+    for (const ManyLaunch& l : L) {
+        ManyJob* mj = (ManyJob*)(T.buf.data() + l.recs);
+        for (uint32_t k = 0; k < l.n; k++) {
+            const uint64_t t0 = (uint64_t)(uintptr_t)mj[k].tile_cnt;
+            mj[k].tile_cnt = tile_cnt + t0;
+            mj[k].tile_off = tile_off + t0;
+        }
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemcpyAsync(tb, T.buf.data(), D.upload, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return LATEC_ERR_CUDA;
+    const DecStage* dec = (const DecStage*)(tb + D.dec);
+    int r = launch_count_zeros_all(dec, (int)D.n_dec, (uint32_t)D.tiles, tile_cnt, st);
+    if (!r) r = launch_tile_offsets_all(dec, (int)D.n_dec, tile_cnt, tile_off, st);
+    if (!r) r = run_many(L, T, 0, table, st);
+    return r;
 }
 
 int latec_rans_build_tables(const uint32_t* cdf_rows, int32_t alphabet, int32_t rows, void* enc,

@@ -54,63 +54,110 @@ __global__ void k_fit_counts(const FitStage* __restrict__ fs, const uint32_t* __
     counts[f.counts_off + sym] = v;
 }
 
-// One CTA per (stage, shape, level). The alphabet is split into 8 (or fewer)
-// power-of-two spans of adjacent terms, one per warp; a warp walks its span 32
-// terms at a time (coalesced loads), sums each 32 with a shuffle tree over
-// adjacent lanes and folds the 32-term subtree sums in lane 0 with a
-// binary-counter stack; the warp totals are then paired adjacently. Every
-// partial sum is a node of the perfect binary tree over the alphabet.
+// One warp per (stage, shape, level), eight levels per CTA. Every cost is the
+// sum over the perfect binary tree of the alphabet's terms (its size is a
+// power of two; a term is >= +0: weights are -log2 p, counts are counts):
+// * alphabets of 256 or more: lane l sums its contiguous run of A / 32
+//   terms, visiting only the terms with a nonzero count (a shared bitmap of
+//   the stage's counts): an all-zero subtree sums to +0, which leaves any
+//   partial sum unchanged, so the run's tree is the tree of its nonzero terms
+//   joined at their lowest common ancestors; the 32 run sums are then paired
+//   adjacently by a shuffle tree. Lanes work independently.
+// * smaller alphabets: 32 terms at a time, one per lane, summed by the
+//   shuffle tree, the 32-term sums folded in order by a binary counter (a
+//   subtree completes when its right half does).
+// A zero count contributes +0 without its weight being loaded. The stage's
+// counts sit in shared memory when they fit.
+constexpr uint32_t FIT_SMEM_A = 4096;
+
+__device__ __forceinline__ double fit_term(const float* __restrict__ W,
+                                           const uint32_t* __restrict__ cnt, uint32_t i) {
+    const uint32_t c = cnt[i];
+    return c ? __dmul_rn((double)W[i], (double)c) : 0.0;
+}
+
 __global__ void __launch_bounds__(256)
     k_fit_costs(const FitStage* __restrict__ fs, const uint32_t* __restrict__ counts,
                 double* __restrict__ costs) {
-    const uint32_t level = blockIdx.x, sh = blockIdx.y;
+    const uint32_t sh = blockIdx.y;
     const FitStage& f = fs[blockIdx.z];
     if (sh >= f.n_shapes) return;
     const uint32_t A = f.alphabet;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t span = A >= 256 ? A / 8 : (A >= 32 ? 32 : A);  // terms per warp
-    const uint32_t n_warps = A / span;
-    const uint32_t width = span < 32 ? span : 32;
-    __shared__ double wsum[8];
-    if (warp < (int)n_warps) {
-        const float* W = (const float*)f.w_table + ((uint64_t)sh * 64 + level) * A;
-        const uint32_t* cnt = counts + f.counts_off;
-        double stack[12];
-        int depth[12];
+    __shared__ uint32_t sc[FIT_SMEM_A];
+    const uint32_t* gcnt = counts + f.counts_off;
+    const bool in_smem = A <= FIT_SMEM_A;
+    if (in_smem) {
+        for (uint32_t i = threadIdx.x; i < A; i += 256) sc[i] = gcnt[i];
+        __syncthreads();
+    }
+    const uint32_t* cnt = in_smem ? sc : gcnt;
+    // one bit per term with a nonzero count
+    __shared__ uint32_t nzb[65536 / 32];
+    if (A >= 256) {
+        for (uint32_t wd = threadIdx.x; wd < A / 32; wd += 256) {
+            uint32_t bits = 0;
+            for (int k = 0; k < 32; k++) bits |= (cnt[wd * 32 + k] != 0u ? 1u : 0u) << k;
+            nzb[wd] = bits;
+        }
+        __syncthreads();
+    }
+    const uint32_t level = blockIdx.x * 8 + warp;
+    const float* W = (const float*)f.w_table + ((uint64_t)sh * 64 + level) * A;
+    double stack[12];
+    double v;
+    if (A >= 256) {
+        // lane l: the run [l R, (l + 1) R) of R = A / 32 terms, walked over
+        // its nonzero counts only. A subtree whose terms are all +0 sums to
+        // +0 and x + (+0) = x for every x >= +0, so the tree sum equals the
+        // tree over the nonzero terms with the all-zero subtrees pruned: two
+        // partial sums join at the lowest common ancestor of their positions
+        // (level = bit length of pos_a ^ pos_b), left operand first.
+        const uint32_t R = A / 32, a0 = lane * R;
+        uint32_t spos[12];
         int top = 0;
-        const uint32_t a0 = warp * span;
-        for (uint32_t base = a0; base < a0 + span; base += 32) {
-            const uint32_t i = base + lane;
-            // every term is >= +0 (weights are -log2 p, counts are counts): a
-            // run of zero counts sums to exactly +0.0, so its weights need no
-            // load (the histogram is narrow; the weight tables are not)
-            const uint32_t c = (lane < (int)width) ? cnt[i] : 0u;
-            double v = 0.0;
-            if (__any_sync(0xffffffffu, c != 0u))
-                v = (lane < (int)width) ? __dmul_rn((double)W[i], (double)c) : 0.0;
-            for (uint32_t st = 1; st < width; st <<= 1) {
-                const double o = __shfl_down_sync(0xffffffffu, v, st);
-                if ((lane & (2 * st - 1)) == 0) v = __dadd_rn(v, o);
-            }
-            if (lane == 0) {
-                int dd = 0;
-                while (top > 0 && depth[top - 1] == dd) {
-                    v = __dadd_rn(stack[--top], v);
-                    dd++;
+        for (uint32_t w = a0 / 32; w < (a0 + R + 31) / 32; w++) {
+            uint32_t bits = nzb[w];
+            if (R < 32) bits = (bits >> (a0 & 31)) & ((1u << R) - 1u);
+            while (bits) {
+                const uint32_t p = (R < 32 ? a0 : w * 32) + (uint32_t)(__ffs(bits) - 1);
+                bits &= bits - 1u;
+                const double t = __dmul_rn((double)W[p], (double)cnt[p]);
+                while (top >= 2 &&
+                       (spos[top - 2] ^ spos[top - 1]) < (spos[top - 1] ^ p)) {
+                    stack[top - 2] = __dadd_rn(stack[top - 2], stack[top - 1]);
+                    spos[top - 2] = spos[top - 1];
+                    top--;
                 }
-                stack[top] = v;
-                depth[top] = dd;
+                stack[top] = t;
+                spos[top] = p;
                 top++;
             }
         }
-        if (lane == 0) wsum[warp] = stack[0];
+        while (top >= 2) {
+            stack[top - 2] = __dadd_rn(stack[top - 2], stack[top - 1]);
+            top--;
+        }
+        v = top ? stack[0] : 0.0;
+        for (uint32_t st = 1; st < 32; st <<= 1) {
+            const double o = __shfl_down_sync(0xffffffffu, v, st);
+            if ((lane & (2 * st - 1)) == 0) v = __dadd_rn(v, o);
+        }
+    } else {
+        const uint32_t width = A < 32 ? A : 32, chunks = (A + 31) / 32;
+        for (uint32_t ch = 0; ch < chunks; ch++) {
+            double x = lane < (int)width ? fit_term(W, cnt, ch * 32 + lane) : 0.0;
+            for (uint32_t st = 1; st < width; st <<= 1) {
+                const double o = __shfl_down_sync(0xffffffffu, x, st);
+                if ((lane & (2 * st - 1)) == 0) x = __dadd_rn(x, o);
+            }
+            uint32_t d = 0;
+            for (uint32_t cc = ch; cc & 1u; cc >>= 1) x = __dadd_rn(stack[d++], x);
+            stack[d] = x;
+        }
+        v = stack[31 - __clz(chunks)];
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        for (uint32_t st = 1; st < n_warps; st <<= 1)
-            for (uint32_t w = 0; w + st < n_warps; w += 2 * st) wsum[w] = __dadd_rn(wsum[w], wsum[w + st]);
-        costs[((uint64_t)blockIdx.z * 24 + sh) * 64 + level] = wsum[0];
-    }
+    if (lane == 0) costs[((uint64_t)blockIdx.z * 24 + sh) * 64 + level] = v;
 }
 
 // One warp per stage: first argmin over levels (lower level wins ties), then
@@ -181,7 +228,7 @@ int latec_fit_const(const void* stages_host, int32_t n, const uint32_t* hist_seg
     if (cudaMemcpyAsync(d, h, sizeof(FitStage) * n, cudaMemcpyHostToDevice, st) != cudaSuccess)
         return LATEC_ERR_CUDA;
     k_fit_counts<<<dim3((max_a + 255) / 256, n), 256, 0, st>>>(d, hist_seg, hist_total, counts);
-    k_fit_costs<<<dim3(64, max_s, n), 256, 0, st>>>(d, counts, costs);
+    k_fit_costs<<<dim3(8, max_s, n), 256, 0, st>>>(d, counts, costs);
     k_fit_pick<<<n, 32, 0, st>>>(d, n, costs, out);
     count_launches(3);
     return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;

@@ -9,6 +9,8 @@
 // float64 division (a reciprocal product is used only when it provably rounds
 // to the same integer); the reconstruction is f32(p + 2eb * q) and the bound is
 // verified in float32 exactly as the reference decoder computes it.
+#include <atomic>
+
 #include <cuda_runtime.h>
 
 #include "interp_device.cuh"
@@ -122,7 +124,8 @@ __device__ __forceinline__ double predict_point(const StageDesc& d, const QParam
 }
 
 // Per-block statistics: warp shuffles, then one partial row per CTA.
-__device__ __forceinline__ void block_finish(BlockAcc& a, double* partials, StageAcc* acc) {
+__device__ __forceinline__ void block_finish(BlockAcc& a, double* partials, StageAcc* acc,
+                                             uint32_t bid) {
     __shared__ double sh_red[5][THREADS / 32];
     __shared__ uint32_t sh_mq[THREADS / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -150,7 +153,7 @@ __device__ __forceinline__ void block_finish(BlockAcc& a, double* partials, Stag
             mq = max(mq, sh_mq[w]);
             nt += sh_no[w];
         }
-        for (int k = 0; k < 5; k++) partials[(size_t)blockIdx.x * 5 + k] = s[k];
+        for (int k = 0; k < 5; k++) partials[(size_t)bid * 5 + k] = s[k];
         if (mq) atomicMax(&acc->maxq, mq);
         if (nt) atomicAdd(&acc->nout, nt);
     }
@@ -204,12 +207,12 @@ __device__ void stage_tail(const double* __restrict__ partials, uint32_t blocks,
         for (int k = 0; k < 5; k++) acc->stats[k] = red[k][0];
 }
 
-// Arrival counter: true in the CTA that finishes the stage.
-__device__ __forceinline__ bool last_block(StageAcc* acc) {
+// Arrival counter: true in the CTA that finishes the stage (nblk CTAs).
+__device__ __forceinline__ bool last_block(StageAcc* acc, uint32_t nblk) {
     __shared__ bool is_last;
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) is_last = atomicAdd(&acc->done, 1u) == gridDim.x - 1;
+    if (threadIdx.x == 0) is_last = atomicAdd(&acc->done, 1u) == nblk - 1;
     __syncthreads();
     if (is_last) __threadfence();
     return is_last;
@@ -289,20 +292,26 @@ __device__ __forceinline__ void encode_value(const QParams& q, uint64_t i, T xv,
     a.s[4] = fmax(a.s[4], re);
 }
 
+// One CTA's share of an encode stage pass: CTA bid of nblk takes groups
+// [bid * gpb, (bid + 1) * gpb); the last CTA to finish runs the stage tail.
 template <typename T, int ND, int KIND, int CUBIC>
-__global__ void __launch_bounds__(THREADS, KIND ? 3 : 4)
-    k_interp_quant(const StageDesc d, const QParams q, const int is_anchor, const uint32_t gpb,
-                   const T* __restrict__ x, T* __restrict__ recon, uint16_t* __restrict__ codes,
-                   T* __restrict__ staging, uint32_t* __restrict__ tile_cnt,
-                   uint32_t* __restrict__ tile_off, uint32_t* __restrict__ hist_total,
-                   uint32_t* __restrict__ hist_seg, StageAcc* __restrict__ acc,
-                   double* __restrict__ partials) {
+__device__ __forceinline__ void quant_cta(const StageDesc& d, const QParams& q,
+                                          const int is_anchor, const uint32_t gpb,
+                                          const uint32_t bid, const uint32_t nblk,
+                                          const T* __restrict__ x, T* __restrict__ recon,
+                                          uint16_t* __restrict__ codes, T* __restrict__ staging,
+                                          uint32_t* __restrict__ tile_cnt,
+                                          uint32_t* __restrict__ tile_off,
+                                          uint32_t* __restrict__ hist_total,
+                                          uint32_t* __restrict__ hist_seg,
+                                          StageAcc* __restrict__ acc,
+                                          double* __restrict__ partials) {
     __shared__ uint32_t sh_hist[HBINS];
     for (int b = threadIdx.x; b < HBINS; b += THREADS) sh_hist[b] = 0;
     __syncthreads();
     const uint64_t items = (uint64_t)q.channels * d.n;
     const uint64_t groups = (items + GROUP - 1) / GROUP;
-    const uint64_t g0 = (uint64_t)blockIdx.x * gpb;
+    const uint64_t g0 = (uint64_t)bid * gpb;
     const uint64_t g1 = g0 + gpb < groups ? g0 + gpb : groups;
     const int lane = threadIdx.x & 31;
     BlockAcc a{{0, 0, 0, 0, 0}, 0, 0};
@@ -345,8 +354,253 @@ __global__ void __launch_bounds__(THREADS, KIND ? 3 : 4)
     }
     __syncthreads();
     flush_hist(sh_hist, hist_seg, cur_seg);
-    block_finish(a, partials, acc);
-    if (last_block(acc)) stage_tail(partials, gridDim.x, tile_cnt, n_tiles_of(items), tile_off, acc);
+    block_finish(a, partials, acc, bid);
+    if (last_block(acc, nblk)) stage_tail(partials, nblk, tile_cnt, n_tiles_of(items), tile_off, acc);
+}
+
+// ---------------------------------------------------------------- row segments
+// Consecutive ranks of a stage (single class or fused weight) run along the
+// last axis of one grid row: xstep apart, the other coordinates fixed. A
+// warp takes a segment of ROW_SEG consecutive ranks, decodes its first rank
+// once and places the rest by offset along the row; the tap offsets of the
+// fixed axes (and of the last axis, away from the row's ends) are set once
+// per segment. Points past the row's end fall back to the per-point decode.
+// The prediction, quantizer and bookkeeping are those of the per-point
+// kernels, operation for operation.
+constexpr int ROW_SEG = 256;                   // ranks per warp segment
+constexpr int ROW_GROUP = ROW_SEG * THREADS / 32;  // ranks per CTA iteration
+
+// Tap offsets of one axis from a point (elements): an out-of-line tap reads
+// the -s tap, exactly as load_axis does.
+struct SegTaps {
+    int32_t m1, p1, m3, p3;
+    uint32_t ok;
+};
+
+__device__ __forceinline__ SegTaps seg_taps(int c, int n, int32_t gs, int s) {
+    const int32_t o1 = s * gs;
+    const bool vp1 = c + s < n, vm3 = c - 3 * s >= 0, vp3 = c + 3 * s < n;
+    return SegTaps{-o1, vp1 ? o1 : -o1, vm3 ? -3 * o1 : -o1, vp3 ? 3 * o1 : -o1,
+                   (vp1 ? 1u : 0u) | (vm3 ? 2u : 0u) | (vp3 ? 4u : 0u)};
+}
+
+template <typename T, int CUBIC>
+__device__ __forceinline__ void load_seg(const T* __restrict__ b, const SegTaps& o,
+                                         AxisTaps<T>& t) {
+    t.m1 = __ldg(b + o.m1);
+    t.p1 = __ldg(b + o.p1);
+    t.m3 = __ldg(b + o.m3);
+    t.p3 = CUBIC ? __ldg(b + o.p3) : (T)0;
+    t.ok = o.ok;
+}
+
+// A row segment: the decoded first point, the points left in its row, the
+// axes its points interpolate along (in the order gather_point uses) and the
+// tap offsets of the fixed axes.
+template <int ND, int KIND>
+struct RowSeg {
+    int32_t coord[ND];
+    int64_t flat;
+    uint32_t rem;        // points of the row from the first one on
+    int32_t xstep;
+    uint32_t axes;       // bit j: taps along axis j (KIND 1, center 0: the odd axes)
+    int32_t single;      // the one axis of KIND 0 / centers 1 and 2
+    bool interior;       // last-axis taps of every point in line
+    // taps of the fixed axes: t[0] for the single axis, t[j] for odd axis j
+    // (the last axis's taps are +-s, +-3s when interior, else per point)
+    SegTaps t[KIND ? ND - 1 : 1];
+};
+
+template <int ND, int KIND>
+__device__ __forceinline__ void row_seg(const StageDesc& d, const QParams& q, uint32_t r,
+                                        RowSeg<ND, KIND>& g) {
+    constexpr int X = ND - 1;
+    g.flat = stage_coords_t<ND, KIND>(d, r, g.coord);
+    const int s = d.s, nx = d.shape[X];
+    uint32_t m, len;
+    if (KIND == 0) {
+        g.xstep = d.step;
+        m = (uint32_t)(g.coord[X] - d.start[X]) / (uint32_t)d.step;
+        len = d.size_div[X].d;
+    } else {
+        g.xstep = 2 * s;
+        m = (uint32_t)g.coord[X] >> d.lg2s;
+        len = (g.coord[X] & s) ? (uint32_t)(nx + s - 1) >> d.lg2s
+                               : (uint32_t)(nx + 2 * s - 1) >> d.lg2s;
+    }
+    g.rem = len - m;
+    g.axes = 0;
+    g.single = -1;
+    if (KIND == 0) {
+        g.single = d.axis;
+    } else {
+#pragma unroll
+        for (int j = 0; j < ND; j++)
+            if (g.coord[j] & s) {
+                g.axes |= 1u << j;
+                if (q.center == 2 || (q.center == 1 && g.single < 0)) g.single = j;
+            }
+        if (q.center == 0) g.single = -1;
+    }
+    const int64_t span = (int64_t)(ROW_SEG - 1) * g.xstep;
+    g.interior = g.coord[X] - 3 * s >= 0 && g.coord[X] + span + 3 * s < nx;
+#pragma unroll
+    for (int j = 0; j < X; j++) {
+        const SegTaps tj = seg_taps(g.coord[j], d.shape[j], (int32_t)d.gstride[j], s);
+        if (g.single == j) g.t[0] = tj;
+        if (KIND && g.single < 0 && ((g.axes >> j) & 1u)) g.t[KIND ? j : 0] = tj;
+    }
+}
+
+// Taps of the segment point at offset k along the row (k < rem).
+template <typename T, int ND, int KIND, int CUBIC>
+__device__ __forceinline__ void row_gather(const StageDesc& d, const RowSeg<ND, KIND>& g,
+                                           uint32_t k, const T* __restrict__ rc, int64_t& flat,
+                                           PointTaps<T, ND, KIND>& pt) {
+    constexpr int X = ND - 1;
+    const int32_t off = (int32_t)k * g.xstep;
+    flat = g.flat + off;
+    const T* b = rc + flat;
+    const int x = g.coord[X] + off, s = d.s;
+    const SegTaps tx = g.interior ? SegTaps{-s, s, -3 * s, 3 * s, 7u}
+                                  : seg_taps(x, d.shape[X], 1, s);
+    pt.odd = 0;
+    if (g.single >= 0) {
+        load_seg<T, CUBIC>(b, g.single == X ? tx : g.t[0], pt.ax[0]);
+        return;
+    }
+    pt.odd = g.axes;
+#pragma unroll
+    for (int j = 0; j < ND; j++) {
+        if (!((g.axes >> j) & 1u)) continue;
+        load_seg<T, CUBIC>(b, j == X ? tx : g.t[KIND && j < X ? j : 0], pt.ax[KIND ? j : 0]);
+    }
+}
+
+// One point of a row segment: taps by segment offset when the point lies in
+// the segment's row, else by the per-point decode.
+template <typename T, int ND, int KIND, int CUBIC>
+__device__ __forceinline__ void row_point(const StageDesc& d, const QParams& q,
+                                          const int is_anchor, const RowSeg<ND, KIND>& g,
+                                          uint32_t k,
+                                          uint64_t i, const T* __restrict__ recon, int64_t& flat,
+                                          PointTaps<T, ND, KIND>& pt) {
+    if (k < g.rem) {
+        if (is_anchor) {
+            flat = g.flat + (int64_t)k * g.xstep;
+            pt.odd = 0;
+        } else {
+            row_gather<T, ND, KIND, CUBIC>(d, g, k, recon, flat, pt);
+        }
+    } else {
+        uint32_t c;
+        locate_gather<T, ND, KIND, CUBIC>(d, q, is_anchor, i, recon, flat, c, pt);
+    }
+}
+
+// The encode stage pass over row segments (single channel): CTA bid of nblk
+// takes groups [bid * gpb, (bid + 1) * gpb) of ROW_GROUP ranks; warp w of the
+// CTA the w-th segment of each group; lane l its points l, l + 32, ...
+// (coalesced codes), two in flight.
+template <typename T, int ND, int KIND, int CUBIC>
+__device__ __forceinline__ void quant_rows_cta(const StageDesc& d, const QParams& q,
+                                               const int is_anchor, const uint32_t gpb,
+                                               const uint32_t bid, const uint32_t nblk,
+                                               const T* __restrict__ x, T* __restrict__ recon,
+                                               uint16_t* __restrict__ codes,
+                                               T* __restrict__ staging,
+                                               uint32_t* __restrict__ tile_cnt,
+                                               uint32_t* __restrict__ tile_off,
+                                               uint32_t* __restrict__ hist_total,
+                                               uint32_t* __restrict__ hist_seg,
+                                               StageAcc* __restrict__ acc,
+                                               double* __restrict__ partials) {
+    __shared__ uint32_t sh_hist[HBINS];
+    for (int b = threadIdx.x; b < HBINS; b += THREADS) sh_hist[b] = 0;
+    __syncthreads();
+    const uint64_t items = d.n;
+    const uint64_t groups = (items + ROW_GROUP - 1) / ROW_GROUP;
+    const uint64_t g0 = (uint64_t)bid * gpb;
+    const uint64_t g1 = g0 + gpb < groups ? g0 + gpb : groups;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    BlockAcc a{{0, 0, 0, 0, 0}, 0, 0};
+    uint32_t cur_seg = (uint32_t)((g0 * ROW_GROUP) >> SEG_SHIFT);
+    for (uint64_t g = g0; g < g1; g++) {
+        const uint64_t base = g * ROW_GROUP;
+        const uint32_t seg = (uint32_t)(base >> SEG_SHIFT);
+        if (seg != cur_seg) {  // uniform across the CTA
+            __syncthreads();
+            flush_hist(sh_hist, hist_seg, cur_seg);
+            __syncthreads();
+            cur_seg = seg;
+        }
+        const uint64_t r0 = base + (uint64_t)warp * ROW_SEG;
+        if (r0 >= items) continue;  // uniform across the warp
+        RowSeg<ND, KIND> gs;
+        uint32_t kb = 0;  // segment offset of the decoded point
+        row_seg<ND, KIND>(d, q, (uint32_t)r0, gs);
+#pragma unroll 1
+        for (int j = 0; j < ROW_SEG / 32; j += 2) {
+            if (32u * j - kb >= gs.rem && r0 + 32u * j < items) {  // the next row
+                kb = 32u * j;
+                row_seg<ND, KIND>(d, q, (uint32_t)(r0 + kb), gs);
+            }
+            const uint32_t k0 = 32 * j + lane, k1 = k0 + 32;
+            const uint64_t i0 = r0 + k0, i1 = r0 + k1;
+            const bool v0 = i0 < items, v1 = i1 < items;
+            int64_t f0 = 0, f1 = 0;
+            T x0 = (T)0, x1 = (T)0;
+            PointTaps<T, ND, KIND> t0, t1;
+            if (v0) {
+                row_point<T, ND, KIND, CUBIC>(d, q, is_anchor, gs, k0 - kb, i0, recon, f0, t0);
+                x0 = x[f0];
+            }
+            if (v1) {
+                row_point<T, ND, KIND, CUBIC>(d, q, is_anchor, gs, k1 - kb, i1, recon, f1, t1);
+                x1 = x[f1];
+            }
+            const double p0 = (v0 && !is_anchor) ? combine_point<T, ND, KIND, CUBIC>(q, t0) : 0.0;
+            const double p1 = (v1 && !is_anchor) ? combine_point<T, ND, KIND, CUBIC>(q, t1) : 0.0;
+            int k0h = -1, k1h = -1;
+            uint32_t cd0 = 0, cd1 = 0;
+            if (v0)
+                encode_value<T>(q, i0, x0, p0, recon + f0, staging, tile_cnt, codes, a, k0h, cd0);
+            if (v1)
+                encode_value<T>(q, i1, x1, p1, recon + f1, staging, tile_cnt, codes, a, k1h, cd1);
+            hist_warp(sh_hist, hist_total, k0h, cd0, lane);
+            hist_warp(sh_hist, hist_total, k1h, cd1, lane);
+        }
+    }
+    __syncthreads();
+    flush_hist(sh_hist, hist_seg, cur_seg);
+    block_finish(a, partials, acc, bid);
+    if (last_block(acc, nblk)) stage_tail(partials, nblk, tile_cnt, n_tiles_of(items), tile_off, acc);
+}
+
+template <typename T, int ND, int KIND, int CUBIC>
+__global__ void __launch_bounds__(THREADS, KIND ? 3 : 4)
+    k_interp_quant_rows(const StageDesc d, const QParams q, const int is_anchor,
+                        const uint32_t gpb, const T* __restrict__ x, T* __restrict__ recon,
+                        uint16_t* __restrict__ codes, T* __restrict__ staging,
+                        uint32_t* __restrict__ tile_cnt, uint32_t* __restrict__ tile_off,
+                        uint32_t* __restrict__ hist_total, uint32_t* __restrict__ hist_seg,
+                        StageAcc* __restrict__ acc, double* __restrict__ partials) {
+    quant_rows_cta<T, ND, KIND, CUBIC>(d, q, is_anchor, gpb, blockIdx.x, gridDim.x, x, recon,
+                                       codes, staging, tile_cnt, tile_off, hist_total, hist_seg,
+                                       acc, partials);
+}
+
+template <typename T, int ND, int KIND, int CUBIC>
+__global__ void __launch_bounds__(THREADS, KIND ? 3 : 4)
+    k_interp_quant(const StageDesc d, const QParams q, const int is_anchor, const uint32_t gpb,
+                   const T* __restrict__ x, T* __restrict__ recon, uint16_t* __restrict__ codes,
+                   T* __restrict__ staging, uint32_t* __restrict__ tile_cnt,
+                   uint32_t* __restrict__ tile_off, uint32_t* __restrict__ hist_total,
+                   uint32_t* __restrict__ hist_seg, StageAcc* __restrict__ acc,
+                   double* __restrict__ partials) {
+    quant_cta<T, ND, KIND, CUBIC>(d, q, is_anchor, gpb, blockIdx.x, gridDim.x, x, recon, codes,
+                                  staging, tile_cnt, tile_off, hist_total, hist_seg, acc,
+                                  partials);
 }
 
 // Quantize a compact array against a given prediction (predictor-agnostic
@@ -391,8 +645,9 @@ __global__ void __launch_bounds__(THREADS)
     }
     __syncthreads();
     flush_hist(sh_hist, hist_seg, cur_seg);
-    block_finish(a, partials, acc);
-    if (last_block(acc)) stage_tail(partials, gridDim.x, tile_cnt, n_tiles_of(items), tile_off, acc);
+    block_finish(a, partials, acc, blockIdx.x);
+    if (last_block(acc, gridDim.x))
+        stage_tail(partials, gridDim.x, tile_cnt, n_tiles_of(items), tile_off, acc);
 }
 
 // Prediction only (the predictor plugin's ``predict``): compact output.
@@ -417,7 +672,7 @@ __global__ void __launch_bounds__(THREADS)
 // ---------------------------------------------------------------- scans
 // Decode: zero codes (outliers) per 2048-code tile of every stage in one pass.
 __global__ void __launch_bounds__(THREADS)
-    k_count_zeros_all(const DecStage* __restrict__ ds, int n_stages, const uint16_t* __restrict__ codes,
+    k_count_zeros_all(const DecStage* __restrict__ ds, int n_stages,
                       uint32_t* __restrict__ tile_cnt) {
     const uint32_t gt = blockIdx.x;
     int lo = 0, hi = n_stages;  // last stage with tile0 <= gt
@@ -430,7 +685,7 @@ __global__ void __launch_bounds__(THREADS)
     int cnt = 0;
     for (int k = 0; k < TILE / THREADS; k++) {
         const uint64_t i = base + (uint64_t)k * THREADS + threadIdx.x;
-        cnt += (i < d.items && codes[d.codes_off + i] == 0) ? 1 : 0;
+        cnt += (i < d.items && d.codes[i] == 0) ? 1 : 0;
     }
     __shared__ int sh[THREADS / 32];
     int v = cnt;
@@ -449,7 +704,7 @@ __global__ void __launch_bounds__(THREADS)
 // that the stage's zero codes match its stored outlier count.
 __global__ void __launch_bounds__(THREADS)
     k_tile_offsets_all(const DecStage* __restrict__ ds, const uint32_t* __restrict__ tile_cnt,
-                       uint32_t* __restrict__ tile_off, uint32_t* __restrict__ err) {
+                       uint32_t* __restrict__ tile_off) {
     const DecStage& d = ds[blockIdx.x];
     const uint32_t tiles = n_tiles_of(d.items);
     if (!tiles) return;
@@ -472,7 +727,7 @@ __global__ void __launch_bounds__(THREADS)
         tile_off[d.tile0 + i] = off;
         off += cnt[i];
     }
-    if (threadIdx.x == THREADS - 1 && sc[THREADS - 1] != d.n_out) atomicOr(err, 1u);
+    if (threadIdx.x == THREADS - 1 && sc[THREADS - 1] != d.n_out) atomicOr(d.err, 1u);
 }
 
 // Block-local exclusive scan of a per-thread flag in item order (k-major).
@@ -492,13 +747,17 @@ __device__ __forceinline__ uint32_t block_excl_flag(bool f, uint32_t& block_tota
     return before + __popc(bal & ((1u << lane) - 1u));
 }
 
-__global__ void __launch_bounds__(THREADS)
-    k_compact(const uint16_t* __restrict__ codes, const uint64_t items,
-              const uint8_t* __restrict__ staging, const int elem,
-              const uint32_t* __restrict__ tile_cnt, const uint32_t* __restrict__ tile_off,
-              uint8_t* __restrict__ out) {
+// Outliers of a stage into scan order: tiles bid, bid + nblk, ... of the
+// stage, each only if it counted an outlier.
+__device__ __forceinline__ void compact_cta(const uint16_t* __restrict__ codes,
+                                            const uint64_t items,
+                                            const uint8_t* __restrict__ staging, const int elem,
+                                            const uint32_t* __restrict__ tile_cnt,
+                                            const uint32_t* __restrict__ tile_off,
+                                            uint8_t* __restrict__ out, const uint32_t bid,
+                                            const uint32_t nblk) {
     const uint32_t tiles = n_tiles_of(items);
-    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    for (uint32_t tile = bid; tile < tiles; tile += nblk) {
         if (tile_cnt[tile] == 0) continue;  // uniform across the CTA
         const uint64_t tile_base = (uint64_t)tile * TILE;
         uint32_t run = tile_off[tile];
@@ -512,6 +771,14 @@ __global__ void __launch_bounds__(THREADS)
             run += tot;
         }
     }
+}
+
+__global__ void __launch_bounds__(THREADS)
+    k_compact(const uint16_t* __restrict__ codes, const uint64_t items,
+              const uint8_t* __restrict__ staging, const int elem,
+              const uint32_t* __restrict__ tile_cnt, const uint32_t* __restrict__ tile_off,
+              uint8_t* __restrict__ out) {
+    compact_cta(codes, items, staging, elem, tile_cnt, tile_off, out, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- decode
@@ -553,14 +820,17 @@ __device__ __forceinline__ void dequant_point(const StageDesc& d, const QParams&
 // Tiles without outliers (the common case) take a barrier-free path; others
 // rank their outliers with a block scan in item order.
 template <typename T, int ND, int KIND, int CUBIC>
-__global__ void __launch_bounds__(THREADS, KIND ? 4 : 5)
-    k_interp_dequant(const StageDesc d, const QParams q, const int is_anchor,
-                     const uint16_t* __restrict__ codes, const uint8_t* __restrict__ outliers,
-                     const uint32_t* __restrict__ tile_cnt, const uint32_t* __restrict__ tile_off,
-                     const uint32_t n_out, T* __restrict__ recon, uint32_t* __restrict__ err) {
+__device__ __forceinline__ void dequant_cta(const StageDesc& d, const QParams& q,
+                                            const int is_anchor, const uint32_t tile,
+                                            const uint16_t* __restrict__ codes,
+                                            const uint8_t* __restrict__ outliers,
+                                            const uint32_t* __restrict__ tile_cnt,
+                                            const uint32_t* __restrict__ tile_off,
+                                            const uint32_t n_out, T* __restrict__ recon,
+                                            uint32_t* __restrict__ err) {
     const uint64_t items = (uint64_t)q.channels * d.n;
-    const uint64_t tile_base = (uint64_t)blockIdx.x * TILE;
-    if (tile_cnt[blockIdx.x] == 0) {  // no outliers: two points in flight per thread
+    const uint64_t tile_base = (uint64_t)tile * TILE;
+    if (tile_cnt[tile] == 0) {  // no outliers: two points in flight per thread
         for (int k = 0; k < TILE / THREADS; k += 2) {
             const uint64_t i0 = tile_base + (uint64_t)k * THREADS + threadIdx.x;
             const uint64_t i1 = i0 + THREADS;
@@ -585,7 +855,7 @@ __global__ void __launch_bounds__(THREADS, KIND ? 4 : 5)
         }
         return;
     }
-    uint32_t run = tile_off[blockIdx.x];
+    uint32_t run = tile_off[tile];
     for (int k = 0; k < TILE / THREADS; k++) {
         const uint64_t i = tile_base + (uint64_t)k * THREADS + threadIdx.x;
         const bool valid = i < items;
@@ -596,6 +866,67 @@ __global__ void __launch_bounds__(THREADS, KIND ? 4 : 5)
         if (valid)
             dequant_point<T, ND, KIND, CUBIC>(d, q, is_anchor, i, code, outliers, pos, n_out, recon,
                                               err);
+    }
+}
+
+template <typename T, int ND, int KIND, int CUBIC>
+__global__ void __launch_bounds__(THREADS, KIND ? 4 : 5)
+    k_interp_dequant(const StageDesc d, const QParams q, const int is_anchor,
+                     const uint16_t* __restrict__ codes, const uint8_t* __restrict__ outliers,
+                     const uint32_t* __restrict__ tile_cnt, const uint32_t* __restrict__ tile_off,
+                     const uint32_t n_out, T* __restrict__ recon, uint32_t* __restrict__ err) {
+    dequant_cta<T, ND, KIND, CUBIC>(d, q, is_anchor, blockIdx.x, codes, outliers, tile_cnt,
+                                    tile_off, n_out, recon, err);
+}
+
+// Decode over row segments (single channel): a tile without outliers is
+// eight warp segments of ROW_SEG consecutive ranks, each placed by one rank
+// decode (see quant_rows_cta); a tile with outliers takes dequant_cta's path.
+template <typename T, int ND, int KIND, int CUBIC>
+__global__ void __launch_bounds__(THREADS, KIND ? 4 : 5)
+    k_interp_dequant_rows(const StageDesc d, const QParams q, const int is_anchor,
+                          const uint16_t* __restrict__ codes,
+                          const uint8_t* __restrict__ outliers,
+                          const uint32_t* __restrict__ tile_cnt,
+                          const uint32_t* __restrict__ tile_off, const uint32_t n_out,
+                          T* __restrict__ recon, uint32_t* __restrict__ err) {
+    static_assert(TILE == ROW_SEG * THREADS / 32, "a tile is one segment per warp");
+    if (tile_cnt[blockIdx.x] != 0) {
+        dequant_cta<T, ND, KIND, CUBIC>(d, q, is_anchor, blockIdx.x, codes, outliers, tile_cnt,
+                                        tile_off, n_out, recon, err);
+        return;
+    }
+    const uint64_t items = d.n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t r0 = (uint64_t)blockIdx.x * TILE + (uint64_t)warp * ROW_SEG;
+    if (r0 >= items) return;
+    RowSeg<ND, KIND> gs;
+    uint32_t kb = 0;
+    row_seg<ND, KIND>(d, q, (uint32_t)r0, gs);
+#pragma unroll 1
+    for (int j = 0; j < ROW_SEG / 32; j += 2) {
+        if (32u * j - kb >= gs.rem && r0 + 32u * j < items) {
+            kb = 32u * j;
+            row_seg<ND, KIND>(d, q, (uint32_t)(r0 + kb), gs);
+        }
+        const uint32_t k0 = 32 * j + lane, k1 = k0 + 32;
+        const uint64_t i0 = r0 + k0, i1 = r0 + k1;
+        const bool v0 = i0 < items, v1 = i1 < items;
+        int64_t f0 = 0, f1 = 0;
+        uint32_t c0 = 1, c1 = 1;
+        PointTaps<T, ND, KIND> t0, t1;
+        if (v0) {
+            c0 = codes[i0];
+            row_point<T, ND, KIND, CUBIC>(d, q, is_anchor, gs, k0 - kb, i0, recon, f0, t0);
+        }
+        if (v1) {
+            c1 = codes[i1];
+            row_point<T, ND, KIND, CUBIC>(d, q, is_anchor, gs, k1 - kb, i1, recon, f1, t1);
+        }
+        const double p0 = (v0 && !is_anchor) ? combine_point<T, ND, KIND, CUBIC>(q, t0) : 0.0;
+        const double p1 = (v1 && !is_anchor) ? combine_point<T, ND, KIND, CUBIC>(q, t1) : 0.0;
+        if (v0) recon[f0] = dequant_value<T>(q, p0, c0);
+        if (v1) recon[f1] = dequant_value<T>(q, p1, c1);
     }
 }
 
@@ -633,6 +964,82 @@ __global__ void __launch_bounds__(THREADS)
             recon[i] = dequant_value<T>(q, (double)pred[i], code);
         }
     }
+}
+
+// ---------------------------------------------------------------- many tensors
+// A CTA of a many-tensor launch finds its job (the last one whose first CTA
+// is not after it) and copies the job's stage descriptor into shared memory.
+__device__ __forceinline__ uint32_t find_job(const uint32_t* __restrict__ first, uint32_t n,
+                                             uint32_t b) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (first[mid] <= b) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ uint32_t job_of_block(const uint32_t* __restrict__ first, uint32_t n) {
+    __shared__ uint32_t sj;
+    if (threadIdx.x == 0) sj = find_job(first, n, blockIdx.x);
+    __syncthreads();
+    return sj;
+}
+
+__device__ __forceinline__ void load_desc(StageDesc& sd, const StageDesc* __restrict__ g) {
+    static_assert(sizeof(StageDesc) % 4 == 0, "descriptor copied as words");
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(g);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&sd);
+    for (uint32_t k = threadIdx.x; k < sizeof(StageDesc) / 4; k += THREADS) dst[k] = src[k];
+    __syncthreads();
+}
+
+template <typename T, int ND, int KIND, int CUBIC>
+__global__ void __launch_bounds__(THREADS, KIND ? 3 : 4)
+    k_interp_quant_many(const ManyJob* __restrict__ jobs, const uint32_t* __restrict__ first,
+                        const uint32_t n) {
+    __shared__ __align__(16) StageDesc sd;
+    const uint32_t j = job_of_block(first, n);
+    const ManyJob& J = jobs[j];
+    load_desc(sd, J.d);
+    quant_cta<T, ND, KIND, CUBIC>(sd, J.q, (int)J.is_anchor, J.gpb, blockIdx.x - first[j],
+                                  J.blocks, (const T*)J.x, (T*)J.recon, J.codes, (T*)J.staging,
+                                  J.tile_cnt, J.tile_off, J.hist_total, J.hist_seg, J.acc,
+                                  J.partials);
+}
+
+template <typename T, int ND, int KIND, int CUBIC>
+__global__ void __launch_bounds__(THREADS, KIND ? 4 : 5)
+    k_interp_dequant_many(const ManyJob* __restrict__ jobs, const uint32_t* __restrict__ first,
+                          const uint32_t n) {
+    __shared__ __align__(16) StageDesc sd;
+    const uint32_t j = job_of_block(first, n);
+    const ManyJob& J = jobs[j];
+    load_desc(sd, J.d);
+    dequant_cta<T, ND, KIND, CUBIC>(sd, J.q, (int)J.is_anchor, blockIdx.x - first[j],
+                                    J.codes_in, J.outliers, J.tile_cnt, J.tile_off, J.n_out,
+                                    (T*)J.recon, J.err);
+}
+
+__global__ void __launch_bounds__(THREADS)
+    k_compact_many(const ManyJob* __restrict__ jobs, const uint32_t* __restrict__ first,
+                   const uint32_t n) {
+    const uint32_t j = job_of_block(first, n);
+    const ManyJob& J = jobs[j];
+    compact_cta(J.codes, J.items, (const uint8_t*)J.staging, (int)J.elem, J.tile_cnt,
+                J.tile_off, J.out, blockIdx.x - first[j], J.cblocks);
+}
+
+// Zero word ranges: range r takes CTAs first[r] .. first[r + 1] - 1, each
+// clearing ZERO_CHUNK words of it.
+__global__ void __launch_bounds__(THREADS)
+    k_zero_many(const ZeroRange* __restrict__ r, const uint32_t* __restrict__ first,
+                const uint32_t n) {
+    const uint32_t j = job_of_block(first, n);
+    const uint64_t a = (uint64_t)(blockIdx.x - first[j]) * ZERO_CHUNK;
+    const uint64_t e = a + ZERO_CHUNK < r[j].words ? a + ZERO_CHUNK : r[j].words;
+    uint32_t* p = r[j].p;
+    for (uint64_t i = a + threadIdx.x; i < e; i += THREADS) p[i] = 0u;
 }
 
 // ---------------------------------------------------------------- fused levels
@@ -898,11 +1305,56 @@ static uint32_t groups_per_block(uint64_t items, uint32_t* blocks) {
     return (uint32_t)gpb;
 }
 
+uint32_t encode_grid(uint64_t items, uint32_t cap, uint32_t* blocks) {
+    const uint64_t groups = (items + GROUP - 1) / GROUP;
+    if (groups == 0) {
+        *blocks = 0;
+        return 1;
+    }
+    const uint64_t c = cap ? cap : (uint64_t)MAX_BLOCKS;
+    const uint64_t b = groups < c ? groups : c;
+    const uint64_t gpb = (groups + b - 1) / b;
+    *blocks = (uint32_t)((groups + gpb - 1) / gpb);
+    return (uint32_t)gpb;
+}
+
 uint32_t encode_blocks(uint64_t items) {
     uint32_t b;
     groups_per_block(items, &b);
     return b;
 }
+
+std::atomic<int> g_row_mode{0};
+
+// Row-segment kernels: one channel, rank 2..4 without blocked anchors, 32-bit
+// tap offsets, and rows long enough that a warp segment stays in one row.
+bool rows_ok(const StageDesc& d, const QParams& q) {
+    if (!g_row_mode.load() || q.channels != 1 || d.holes || d.kind == 2 || d.ndim < 2 ||
+        d.ndim > 4 || q.points >= (1ull << 30) || d.gstride[d.ndim - 1] != 1)
+        return false;
+    const int X = d.ndim - 1;
+    const uint32_t len = d.kind == 0 ? d.size_div[X].d
+                                     : (uint32_t)((d.shape[X] + 2 * d.s - 1) / (2 * d.s));
+    return len >= (uint32_t)ROW_SEG / 2;
+}
+
+#define ROWS_DISPATCH(KERNEL_CALL)                                                      \
+    do {                                                                                \
+        const int kd_ = d.kind == 1 ? 1 : 0, cu_ = q.order ? 1 : 0;                     \
+        if (dtype == LATEC_F64) {                                                       \
+            using T = double;                                                           \
+            ROWS_ND(KERNEL_CALL);                                                       \
+        } else {                                                                        \
+            using T = float;                                                            \
+            ROWS_ND(KERNEL_CALL);                                                       \
+        }                                                                               \
+    } while (0)
+#define ROWS_ND(KERNEL_CALL)                                                            \
+    switch (d.ndim) {                                                                   \
+        case 2: DISPATCH_KC(2, KERNEL_CALL); break;                                     \
+        case 3: DISPATCH_KC(3, KERNEL_CALL); break;                                     \
+        default: DISPATCH_KC(4, KERNEL_CALL); break;                                    \
+    }
 
 int launch_interp_quant(const StageDesc& d, const QParams& q, int dtype, int is_anchor,
                         const void* x, void* recon, uint16_t* codes, void* staging,
@@ -910,10 +1362,20 @@ int launch_interp_quant(const StageDesc& d, const QParams& q, int dtype, int is_
                         uint32_t* hist_seg, StageAcc* acc, double* partials, cudaStream_t st) {
     const uint64_t items = (uint64_t)q.channels * d.n;
     if (!items) return LATEC_OK;
-    uint32_t blocks;
-    const uint32_t gpb = groups_per_block(items, &blocks);
     if (cudaMemsetAsync(tile_cnt, 0, sizeof(uint32_t) * n_tiles(items), st) != cudaSuccess)
         return LATEC_ERR_CUDA;
+    if (rows_ok(d, q)) {
+        const uint64_t groups = (items + ROW_GROUP - 1) / ROW_GROUP;
+        const uint64_t b = groups < (uint64_t)MAX_BLOCKS ? groups : (uint64_t)MAX_BLOCKS;
+        const uint32_t gpb = (uint32_t)((groups + b - 1) / b);
+        const uint32_t blocks = (uint32_t)((groups + gpb - 1) / gpb);
+        ROWS_DISPATCH((k_interp_quant_rows<T, ND, KIND, CUBIC><<<blocks, THREADS, 0, st>>>(
+            d, q, is_anchor, gpb, (const T*)x, (T*)recon, codes, (T*)staging, tile_cnt,
+            tile_off, hist_total, hist_seg, acc, partials)));
+        return last_err();
+    }
+    uint32_t blocks;
+    const uint32_t gpb = groups_per_block(items, &blocks);
     LATEC_DISPATCH((k_interp_quant<T, ND, KIND, CUBIC><<<blocks, THREADS, 0, st>>>(
         d, q, is_anchor, gpb, (const T*)x, (T*)recon, codes, (T*)staging, tile_cnt, tile_off,
         hist_total, hist_seg, acc, partials)));
@@ -951,16 +1413,16 @@ int launch_interp_predict(const StageDesc& d, const QParams& q, int dtype, const
 }
 
 int launch_count_zeros_all(const DecStage* ds, int n_stages, uint32_t total_tiles,
-                           const uint16_t* codes, uint32_t* tile_cnt, cudaStream_t st) {
+                           uint32_t* tile_cnt, cudaStream_t st) {
     if (!total_tiles) return LATEC_OK;
-    k_count_zeros_all<<<total_tiles, THREADS, 0, st>>>(ds, n_stages, codes, tile_cnt);
+    k_count_zeros_all<<<total_tiles, THREADS, 0, st>>>(ds, n_stages, tile_cnt);
     return last_err();
 }
 
 int launch_tile_offsets_all(const DecStage* ds, int n_stages, const uint32_t* tile_cnt,
-                            uint32_t* tile_off, uint32_t* err, cudaStream_t st) {
+                            uint32_t* tile_off, cudaStream_t st) {
     if (!n_stages) return LATEC_OK;
-    k_tile_offsets_all<<<n_stages, THREADS, 0, st>>>(ds, tile_cnt, tile_off, err);
+    k_tile_offsets_all<<<n_stages, THREADS, 0, st>>>(ds, tile_cnt, tile_off);
     return last_err();
 }
 
@@ -1023,12 +1485,61 @@ int launch_interp_dequant(const StageDesc& d, const QParams& q, int dtype, int i
                           cudaStream_t st) {
     const uint64_t items = (uint64_t)q.channels * d.n;
     if (!items) return LATEC_OK;
+    if (rows_ok(d, q)) {
+        ROWS_DISPATCH((k_interp_dequant_rows<T, ND, KIND, CUBIC><<<n_tiles(items), THREADS, 0,
+                                                                   st>>>(
+            d, q, is_anchor, codes, (const uint8_t*)outliers, tile_cnt, tile_off, n_out,
+            (T*)recon, err)));
+        return last_err();
+    }
     LATEC_DISPATCH((k_interp_dequant<T, ND, KIND, CUBIC><<<n_tiles(items), THREADS, 0, st>>>(
         d, q, is_anchor, codes, (const uint8_t*)outliers, tile_cnt, tile_off, n_out, (T*)recon,
         err)));
     return last_err();
 }
 
+
+#define MANY_DISPATCH(KERNEL_CALL)                                                      \
+    do {                                                                                \
+        const int nd_ = nd, kd_ = kind, cu_ = cubic;                                    \
+        if (dtype == LATEC_F64) {                                                       \
+            using T = double;                                                           \
+            DISPATCH_ND(KERNEL_CALL);                                                   \
+        } else {                                                                        \
+            using T = float;                                                            \
+            DISPATCH_ND(KERNEL_CALL);                                                   \
+        }                                                                               \
+    } while (0)
+
+int launch_quant_many(int dtype, int nd, int kind, int cubic, const ManyJob* jobs,
+                      const uint32_t* first, uint32_t n_jobs, uint32_t ctas, cudaStream_t st) {
+    if (!n_jobs || !ctas) return LATEC_OK;
+    MANY_DISPATCH((k_interp_quant_many<T, ND, KIND, CUBIC><<<ctas, THREADS, 0, st>>>(
+        jobs, first, n_jobs)));
+    return last_err();
+}
+
+int launch_dequant_many(int dtype, int nd, int kind, int cubic, const ManyJob* jobs,
+                        const uint32_t* first, uint32_t n_jobs, uint32_t ctas, cudaStream_t st) {
+    if (!n_jobs || !ctas) return LATEC_OK;
+    MANY_DISPATCH((k_interp_dequant_many<T, ND, KIND, CUBIC><<<ctas, THREADS, 0, st>>>(
+        jobs, first, n_jobs)));
+    return last_err();
+}
+
+int launch_compact_many(const ManyJob* jobs, const uint32_t* first, uint32_t n_jobs,
+                        uint32_t ctas, cudaStream_t st) {
+    if (!n_jobs || !ctas) return LATEC_OK;
+    k_compact_many<<<ctas, THREADS, 0, st>>>(jobs, first, n_jobs);
+    return last_err();
+}
+
+int launch_zero_many(const ZeroRange* r, const uint32_t* first, uint32_t n, uint32_t ctas,
+                     cudaStream_t st) {
+    if (!n || !ctas) return LATEC_OK;
+    k_zero_many<<<ctas, THREADS, 0, st>>>(r, first, n);
+    return last_err();
+}
 
 int launch_stage_tails(const TailArgs& a, int n, cudaStream_t st) {
     if (n <= 0) return LATEC_OK;

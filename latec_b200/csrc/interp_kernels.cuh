@@ -1,6 +1,8 @@
 // Kernel launch helpers of the fused interpolation / quantizer stage.
 #pragma once
 
+#include <atomic>
+
 #include "latec_common.cuh"
 
 namespace latec {
@@ -42,12 +44,14 @@ __host__ __device__ inline uint32_t n_tiles_of(uint64_t items) {
     return (uint32_t)((items + TILE - 1) / TILE);
 }
 
-// Decode: one stage of the all-stage tile passes.
+// Decode: one stage of the all-stage tile passes (the stages of one tensor,
+// or of many: each stage names its own codes and error word).
 struct DecStage {
-    uint64_t codes_off;  // first code of the stage
-    uint64_t items;      // codes of the stage
-    uint32_t tile0;      // first global tile of the stage
-    uint32_t n_out;      // outliers stored for the stage
+    const uint16_t* codes;  // the stage's codes
+    uint32_t* err;          // bit 1: outlier count mismatch
+    uint64_t items;         // codes of the stage
+    uint32_t tile0;         // first global tile of the stage
+    uint32_t n_out;         // outliers stored for the stage
 };
 // Level kernels: all sub-stages of one level of the schedule in one launch,
 // as work items (sub-stage, band along axis 0, tile range) claimed in a fixed
@@ -80,12 +84,62 @@ struct LvlItem {
 constexpr uint32_t LEVEL_WAIT_LIMIT = 1u << 22;  // polls of one dependency (x ~100 ns)
 constexpr uint32_t ERR_LEVEL_WAIT = 0x200u;
 
+// Many tensors per launch: one stage of one tensor is a job of a launch whose
+// CTAs are dealt to its jobs in order (first[j]: the first CTA of job j).
+struct ManyJob {
+    const StageDesc* d;   // device copy of the stage's descriptor
+    QParams q;
+    const void* x;        // encode: the field
+    void* recon;
+    const uint16_t* codes_in;  // decode: the stage's codes
+    uint16_t* codes;      // encode: the stage's codes
+    void* staging;        // encode: the tensor's outlier staging buffer
+    uint32_t* tile_cnt;   // the stage's per-tile outlier counts / offsets
+    uint32_t* tile_off;
+    uint32_t* hist_total;  // encode: the stage's full-code histogram
+    uint32_t* hist_seg;    // encode: the stage's first histogram segment
+    StageAcc* acc;         // encode: the stage's statistics
+    double* partials;      // encode: per-CTA partial statistics
+    uint8_t* out;          // encode: where the stage's outliers are compacted
+    const uint8_t* outliers;  // decode: the stage's stored outliers
+    uint32_t* err;         // decode: the tensor's error word
+    uint64_t items;
+    uint32_t gpb;          // encode: 512-point groups per CTA
+    uint32_t blocks;       // CTAs of the stage pass (encode) / tiles (decode)
+    uint32_t is_anchor;
+    uint32_t elem;         // bytes per value
+    uint32_t n_out;        // decode: stored outliers
+    uint32_t cblocks;      // encode: compaction CTAs
+};
+struct ZeroRange {
+    uint32_t* p;
+    uint64_t words;
+};
+constexpr uint64_t ZERO_CHUNK = 1u << 16;  // words cleared by one CTA of k_zero_many
+
+// Launch kinds of the many-tensor passes: rank class (2, 3, 4, or 0 for the
+// runtime rank), fused stage layout, interpolation order.
+int launch_quant_many(int dtype, int nd, int kind, int cubic, const ManyJob* jobs,
+                      const uint32_t* first, uint32_t n_jobs, uint32_t ctas, cudaStream_t st);
+int launch_dequant_many(int dtype, int nd, int kind, int cubic, const ManyJob* jobs,
+                        const uint32_t* first, uint32_t n_jobs, uint32_t ctas, cudaStream_t st);
+int launch_compact_many(const ManyJob* jobs, const uint32_t* first, uint32_t n_jobs,
+                        uint32_t ctas, cudaStream_t st);
+int launch_zero_many(const ZeroRange* r, const uint32_t* first, uint32_t n, uint32_t ctas,
+                     cudaStream_t st);
+// The encode grid of a stage of `items` points: CTAs (at most `cap`, 0 = the
+// single-stage cap) and 512-point groups per CTA.
+uint32_t encode_grid(uint64_t items, uint32_t cap, uint32_t* blocks);
+
 // CTAs of the encode kernels for a stage of `items` points (partials rows).
 uint32_t encode_blocks(uint64_t items);
 inline uint32_t n_blocks(uint64_t items) { return encode_blocks(items); }
 inline uint32_t n_segments(uint64_t items) {
     return (uint32_t)((items + (1ull << SEG_SHIFT) - 1) >> SEG_SHIFT);
 }
+
+// Row-segment stage kernels on (1) or off (0, default): process-wide.
+extern std::atomic<int> g_row_mode;
 
 // Launchers (interp_kernels.cu). items = channels * stage points.
 int launch_interp_quant(const StageDesc& d, const QParams& q, int dtype, int is_anchor,
@@ -95,9 +149,9 @@ int launch_interp_quant(const StageDesc& d, const QParams& q, int dtype, int is_
 int launch_interp_predict(const StageDesc& d, const QParams& q, int dtype, const void* recon,
                           void* pred, cudaStream_t st);
 int launch_count_zeros_all(const DecStage* ds, int n_stages, uint32_t total_tiles,
-                           const uint16_t* codes, uint32_t* tile_cnt, cudaStream_t st);
+                           uint32_t* tile_cnt, cudaStream_t st);
 int launch_tile_offsets_all(const DecStage* ds, int n_stages, const uint32_t* tile_cnt,
-                            uint32_t* tile_off, uint32_t* err, cudaStream_t st);
+                            uint32_t* tile_off, cudaStream_t st);
 int launch_compact(const uint16_t* codes, uint64_t items, const void* staging, int elem,
                    const uint32_t* tile_cnt, const uint32_t* tile_off, void* out,
                    cudaStream_t st);

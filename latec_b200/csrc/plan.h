@@ -1,6 +1,7 @@
 // Host-side plan object behind the opaque latec_plan handle.
 #pragma once
 
+#include <mutex>
 #include <vector>
 
 #include "latec_common.cuh"
@@ -13,6 +14,14 @@ struct latec_plan {
     uint32_t shape[LATEC_MAX_NDIM] = {0};
     uint64_t points = 0;
     std::vector<latec::StageDesc> stages;
+    // device copy of `stages` for the many-tensor launches, made on first use
+    // (per device) and freed with the plan
+    std::mutex dev_mu;
+    latec::StageDesc* dev_stages = nullptr;
+    int dev_id = -1;
+    ~latec_plan() {
+        if (dev_stages) cudaFree(dev_stages);
+    }
 };
 
 namespace latec {

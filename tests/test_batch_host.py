@@ -1,6 +1,8 @@
 """Host logic of the batch API (latec_b200.batch) and the schedule cache:
 the shared-buffer layout that lets one model-fit and one lane-coder launch
-address every stage of every tensor, and the least-recently-used plans."""
+address every stage of every tensor, the least-recently-used plans, the
+ctypes job records of the many-tensor stage calls (the C layouts of
+include/latec_b200.h) and the autotuned CTA table's keys."""
 
 import ctypes
 
@@ -63,3 +65,33 @@ def test_plan_cache_keeps_the_recent_schedules():
     finally:
         levels._PLAN_CACHE = old
         levels._plans.clear()
+
+
+def test_job_records_match_the_c_layout():
+    from latec_b200 import _lib
+
+    # latec_quant_params: 8 int32 + 2 double; the job records add pointers
+    assert ctypes.sizeof(_lib.QuantParams) == 48
+    assert ctypes.sizeof(_lib.EncodeJob) == 144
+    assert ctypes.sizeof(_lib.DecodeJob) == 112
+    assert _lib.EncodeJob.max_ctas.offset == 136
+    assert _lib.DecodeJob.err.offset == 104
+
+
+def test_size_classes_and_cap_lookup():
+    from latec_b200 import batch
+
+    assert [batch.size_class(n) for n in (1, 65535, 65536, 524287, 524288, (1 << 22) - 1,
+                                          1 << 22, 1 << 30)] == [0, 0, 1, 1, 2, 2, 3, 3]
+    caps = {(3, 4, 2): 296, (2, 8, 0): 148}
+    assert batch.cta_cap(3, 4, 1 << 21, caps) == 296
+    assert batch.cta_cap(2, 8, 1000, caps) == 148
+    assert batch.cta_cap(3, 8, 1 << 21, caps) == 0  # no entry: the single-tensor grid
+    saved = batch.cta_caps()
+    try:
+        batch._cta_caps.clear()
+        batch._cta_caps[(2, 4, 3)] = 592
+        assert batch.cta_cap(2, 4, 1 << 23) == 592 and batch.cta_caps() == {(2, 4, 3): 592}
+    finally:
+        batch._cta_caps.clear()
+        batch._cta_caps.update(saved)

@@ -101,3 +101,54 @@ def test_bad_streams_raise():
             assert outs[1].shape == tuple(xs[1].shape)
         except (ValueError, KeyError, NotImplementedError):
             pass
+
+
+def test_runtime_rank_and_blocked_anchor_classes():
+    """5-D and 6-D tensors and blocked anchors (runtime-rank launch classes)
+    in one batch: streams equal compress()'s, fields equal decompress()'s."""
+    import latec_b200 as lb
+    from latec_b200 import fields
+    from latec_b200.batch import compress_many, decompress_many
+
+    xs = [fields.grf_se((5, 4, 6, 5, 4, 5), 2.0, seed=11, device="cuda"),
+          fields.grf_se((6, 5, 7, 6, 5), 2.0, seed=12, device="cuda"),
+          fields.grf_se((40, 44), 5.0, seed=13, device="cuda").double(),
+          fields.grf_se((20, 18, 22), 4.0, seed=14, device="cuda")]
+    for block in (1, 2):
+        pred = lambda: lb.InterpPredictor("cubic", 2, 4, block)  # noqa: E731
+        got = compress_many(xs, 2e-3, pred(), levels=2, anchor_stride=4, anchor_block=block)
+        want = [lb.compress(x, 2e-3, pred(), levels=2, anchor_stride=4, anchor_block=block,
+                            recon="none")[0] for x in xs]
+        for j, (g, w) in enumerate(zip(got, want)):
+            assert g == w, (block, j)
+        for j, (s, o) in enumerate(zip(got, decompress_many(got, out="device"))):
+            assert bool((o == lb.decompress(s, out="device")).all()), (block, j)
+
+
+def test_cta_caps_leave_streams_unchanged():
+    """Every encode CTA cap (one CTA per stage up to the single-tensor grid),
+    and the autotuned table, code the same streams."""
+    import latec_b200 as lb
+    from latec_b200 import batch
+
+    xs = _population()[:5]
+    pred = lambda: lb.InterpPredictor("cubic", 3, 8, 1)  # noqa: E731
+    want = [lb.compress(x, 1e-3, pred(), levels=3, anchor_stride=8, recon="none")[0]
+            for x in xs]
+    saved = batch.cta_caps()
+    try:
+        for cap in (1, 3, 148, 5000):
+            batch._cta_caps.clear()
+            for nd in (2, 3, 4):
+                for elem in (4, 8):
+                    for sc in range(4):
+                        batch._cta_caps[(nd, elem, sc)] = cap
+            assert batch.compress_many(xs, 1e-3, pred(), levels=3, anchor_stride=8) == want, cap
+        batch._cta_caps.clear()
+        tuned = batch.autotune_many(xs, 1e-3, pred(), levels=3, anchor_stride=8, repeats=1,
+                                    candidates=(2, 148))
+        assert set(tuned) and all(c in (2, 148) and ms > 0 for c, ms in tuned.values())
+        assert batch.compress_many(xs, 1e-3, pred(), levels=3, anchor_stride=8) == want
+    finally:
+        batch._cta_caps.clear()
+        batch._cta_caps.update(saved)

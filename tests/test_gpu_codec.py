@@ -217,6 +217,44 @@ def test_256cube_stream_matches_oracle(dtype, tile_mode):
     assert np.abs(back.astype(np.float64) - x.astype(np.float64)).max() <= eb
 
 
+@pytest.mark.parametrize("shape,dtype,order,center", [
+    ((256, 256, 256), np.float32, "cubic", 0),
+    ((130, 300, 257), np.float32, "cubic", 0),
+    ((64, 96, 160), np.float64, "cubic", 0),
+    ((200, 1030), np.float32, "cubic", 0),
+    ((24, 40, 20, 300), np.float32, "cubic", 1),
+    ((90, 70, 260), np.float32, "linear", 2),
+])
+def test_row_segments_match_per_point_decode(shape, dtype, order, center):
+    """The row-segment stage kernels (opt-in) and the per-point decode code
+    the same stream and reconstruction, rows of every length and parity: ragged
+    last axes, float64, rank 2 and 4, linear order, both single-axis centers;
+    the stream of the first case is also the oracle's."""
+    from latec_b200 import _lib, fields
+
+    x = fields.turbulence_jumps(shape, seed=3).astype(dtype)
+    eb = 1e-4 * float(np.float64(x.max()) - np.float64(x.min()))
+    lb = _lb()
+    lib = _lib.load()
+    lv = 4 if len(shape) == 4 else 5
+    pred = lambda: lb.InterpPredictor(order, lv, 16, 1, center=center)  # noqa: E731
+    got = {}
+    try:
+        for mode in (1, 0):
+            _lib.check(lib.latec_set_row_mode(mode))
+            got[mode] = lb.compress(x, eb, pred(), levels=lv, anchor_stride=16)
+        _lib.check(lib.latec_set_row_mode(1))
+        back = lb.decompress(got[1][0])  # decoded with row segments too
+    finally:
+        _lib.check(lib.latec_set_row_mode(0))
+    assert got[1][0] == got[0][0]
+    assert np.array_equal(back, got[0][1]["recon"])
+    assert np.array_equal(got[1][1]["recon"], got[0][1]["recon"])
+    if shape == (256, 256, 256):
+        ostream, _ = ocodec.compress(x, eb, levels_=lv, anchor_stride=16, mode="native")
+        assert got[1][0] == ostream
+
+
 def test_full_size_512cube_properties():
     """512^3 float32 turbulence + jumps at rel eb 1e-4 (the benchmark workload):
     bound, encoder recon == decoder output, determinism of two encodes."""
