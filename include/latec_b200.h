@@ -299,12 +299,14 @@ int latec_rans_decode(latec_rans_stage* stages, int32_t n_stages, uint32_t total
                       void* stream);
 
 /* ---- native-mode stage model fit on the device: the reference's
- *      (level, shape) argmin (latec/rans.py:395-430) with float64 pairwise
- *      sums. stages_host: n latec_fit_stage_size()-byte descriptors (see
+ *      (level, shape) argmin (latec/rans.py:395-430) over exact costs, the
+ *      64-bit sum of rint(W * 2^20) * count with W the float32 -log2 p
+ *      weights. stages_host: n latec_fit_stage_size()-byte descriptors (see
  *      fit_kernels.cu); hist_seg / hist_total as written by
  *      latec_encode_stages; counts: device u32 scratch (sum of alphabets);
- *      costs: device f64 scratch (n * 24 * 64); out: device f64 (3 per
- *      stage: cost in bits, level, shape id). */
+ *      costs: device 8-byte scratch (n * 24 * 64; holds the integer sums);
+ *      out: device f64 (3 per stage: cost in bits = sum * 2^-20, level,
+ *      shape id). */
 uint64_t latec_fit_stage_size(void);
 int latec_fit_const(const void* stages_host, int32_t n, const uint32_t* hist_seg,
                     const uint32_t* hist_total, uint32_t* counts, double* costs, double* out,

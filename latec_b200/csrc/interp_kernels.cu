@@ -1329,7 +1329,7 @@ std::atomic<int> g_row_mode{0};
 // Row-segment kernels: one channel, rank 2..4 without blocked anchors, 32-bit
 // tap offsets, and rows long enough that a warp segment stays in one row.
 bool rows_ok(const StageDesc& d, const QParams& q) {
-    if (!g_row_mode.load() || q.channels != 1 || d.holes || d.kind == 2 || d.ndim < 2 ||
+    if (!g_row_mode.load() || q.channels != 1 || d.holes || d.kind != 0 || d.ndim < 2 ||
         d.ndim > 4 || q.points >= (1ull << 30) || d.gstride[d.ndim - 1] != 1)
         return false;
     const int X = d.ndim - 1;

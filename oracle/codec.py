@@ -11,8 +11,8 @@ Two entropy modes, selected by the container flag ``FLAG_LANES``:
   around the payload.
 * ``"native"`` -- the CUDA library's stream: the same stage records, but each
   rANS blob is the 32-lane interleaved coder of ``oracle/ans.c`` with the
-  reference's own 24-bit tables, the stage model fitted with float64 pairwise
-  sums (``rans_model.fit_const_native``), no literal stages, and the payload
+  reference's own 24-bit tables, the stage model fitted with exact fixed-point
+  costs (``rans_model.fit_const_native``), no literal stages, and the payload
   stored in a zstd frame of raw blocks (decodable by any zstd decoder).
 
 float64 input (new; the reference raises on it) uses dtype id 2, keeps the

@@ -264,21 +264,24 @@ def model_bits(codes, levels64, radius, kexp, shape=0):
     return float((-np.log2(probs / (1 << PRECISION))).sum())
 
 
+FIT_FRAC_BITS = 20  # fixed-point fraction bits of the native fit's weights
+
+
 def fit_const_native(counts, n_codes, kexp, n_levels=N_LEVELS, precision=PRECISION):
     """Stage-constant fit of the native entropy mode: the reference's model
-    space and selection rule (``latec/rans.py:421-430``) with every cost a
-    float64 pairwise tree sum of correctly rounded products
-    ``f64(W[level, sym]) * f64(count[sym])`` over the power-of-two alphabet."""
-    counts = np.asarray(counts, np.float64)
+    space and selection rule (``latec/rans.py:421-430``: first minimum over
+    levels, then the first strictly smaller cost over shapes) with every cost
+    an exact integer, sum over the alphabet of ``Wq[level, sym] * count[sym]``
+    where ``Wq = rint(W * 2^20)`` of the float32 weights ``W`` (-log2 p); the
+    returned cost in bits is ``float(sum) * 2^-20``."""
+    counts = np.asarray(counts, np.int64)
     owx = choose_outlier_weight(int(counts[0]), n_codes)
-    best = (np.inf, 0, 0)
+    best = (None, 0, 0)
     for sid in shape_ids(int(kexp)):
-        p = neg_log2_weights(int(kexp), int(sid), n_levels, precision, owx).astype(np.float64)
-        p = p * counts[None, :]
-        while p.shape[1] > 1:
-            p = p[:, 0::2] + p[:, 1::2]
-        cost = p[:, 0]
-        level = int(cost.argmin())
-        if cost[level] < best[0]:
-            best = (float(cost[level]), level, int(sid))
-    return best[1], best[2], owx, best[0]
+        w = neg_log2_weights(int(kexp), int(sid), n_levels, precision, owx)
+        wq = np.rint(w.astype(np.float64) * float(1 << FIT_FRAC_BITS)).astype(np.int64)
+        cost = wq @ counts  # exact: every partial sum stays below 2^56
+        level = int(np.argmin(cost))  # the first minimum
+        if best[0] is None or int(cost[level]) < best[0]:
+            best = (int(cost[level]), level, int(sid))
+    return best[1], best[2], owx, float(best[0]) * 2.0 ** -FIT_FRAC_BITS
