@@ -417,6 +417,47 @@ def gnn_full(dev, codec):
             "roundtrip_slack": 2.0 ** -24 * (3.0 * span + max(abs(vmin), abs(vmax)))}
 
 
+def gnn_eval_1024(dev, ckpt=GNN_CKPT):
+    """The learned codec against plain interpolation on a 1024^3 float32
+    turbulence + jumps field (4 GiB, seed 5) at absolute eb 1e-4, auto levels
+    (the learned codec's chunks of 128^3; interpolation at the same levels and
+    stride): ratios, bound, one timed round trip each. Opt-in
+    (``--gnn-eval-1024``): it holds about 40 GB on the device for a minute."""
+    import torch
+
+    import latec_b200 as lb
+    from latec_b200 import fields
+    from latec_b200.gnn_codec import read_stream
+
+    x = fields.turbulence_jumps((1024, 1024, 1024), seed=5, device=dev)
+    vmin, vmax = float(x.min().item()), float(x.max().item())
+    span = vmax - vmin
+    eb = 1e-4
+    codec = lb.GNNCodec(checkpoint_path=ckpt, device=dev)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s = codec.compress(x, eb / span)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    out = codec.uncompress(s)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    err = float((out.to(dev) - x).abs().max().item())
+    del out
+    meta = read_stream(s)[0]
+    lv = int(meta["levels"])
+    si, _ = lb.compress(x, eb, lb.InterpPredictor("cubic", lv, 1 << lv, 1), levels=lv,
+                        anchor_stride=1 << lv, recon="none")
+    nbytes = x.numel() * 4
+    return {"workload": "1024^3 float32 turbulence + 3 jumps (seed 5), abs eb 1e-4, auto levels",
+            "checkpoint": os.path.relpath(ckpt, ROOT), "levels": lv,
+            "chunks": meta.get("chunks"), "chunk_batch": meta.get("chunk_batch"),
+            "ratio_gnn": nbytes / len(s), "ratio_interp": nbytes / len(si),
+            "compress_gbs": nbytes / (t1 - t0) / 1e9, "decompress_gbs": nbytes / (t2 - t1) / 1e9,
+            "max_abs_err": err, "bound": eb,
+            "roundtrip_slack": 2.0 ** -24 * (3.0 * span + max(abs(vmin), abs(vmax)))}
+
+
 BATCH_N = 1000  # the whole multi-tensor population
 
 
@@ -647,6 +688,39 @@ def run_profile_gnn(args, dev):
                       "compress_ms": (b - a) * 1e3, "decompress_ms": (c - b) * 1e3}), flush=True)
 
 
+def run_profile_batch(args, dev):
+    """The batch API on the first ``--profile-batch`` tensors of the
+    multi-tensor population: warm-up calls, then one compress_many +
+    decompress_many inside a CUDA profiler range (``ncu --profile-from-start
+    off`` captures only those launches)."""
+    import torch
+
+    import latec_b200 as lb
+    from latec_b200 import fields
+
+    tensors = []
+    for shape, f64, ell, seed in batch_shapes(BATCH_N)[:args.profile_batch]:
+        x = fields.grf_se(shape, ell, seed=seed, device=dev)
+        tensors.append(x.double() if f64 else x)
+    pred = lambda: lb.InterpPredictor("cubic", 4, 16, 1)  # noqa: E731
+    for _ in range(max(1, args.warmup)):
+        lb.decompress_many(lb.compress_many(tensors, 1e-3, pred(), levels=4, anchor_stride=16,
+                                            stream_out="device"), out="device")
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStart()
+    a = time.perf_counter()
+    bs = lb.compress_many(tensors, 1e-3, pred(), levels=4, anchor_stride=16, stream_out="device")
+    torch.cuda.synchronize()
+    b = time.perf_counter()
+    lb.decompress_many(bs, out="device")
+    torch.cuda.synchronize()
+    c = time.perf_counter()
+    torch.cuda.cudart().cudaProfilerStop()
+    nbytes = sum(x.numel() * x.element_size() for x in tensors)
+    print(json.dumps({"profile_batch": len(tensors), "bytes": nbytes,
+                      "compress_ms": (b - a) * 1e3, "decompress_ms": (c - b) * 1e3}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -667,6 +741,14 @@ def main():
     ap.add_argument("--profile-gnn", action="store_true",
                     help="only the learned codec's round trip on one 32^4 chunk, inside a CUDA "
                          "profiler range (for ncu launch lists)")
+    ap.add_argument("--profile-batch", type=int, default=0,
+                    help="only the batch API on the first N population tensors, inside a CUDA "
+                         "profiler range (for ncu launch lists)")
+    ap.add_argument("--gnn-eval-1024", action="store_true",
+                    help="only the learned codec against interpolation on a 1024^3 field "
+                         "(one JSON line)")
+    ap.add_argument("--gnn-ckpt", default=None,
+                    help="checkpoint for --gnn-eval-1024 (default: the shipped one)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -694,6 +776,12 @@ def main():
         return run_profile(args, dev)
     if args.profile_gnn:
         return run_profile_gnn(args, dev)
+    if args.profile_batch:
+        return run_profile_batch(args, dev)
+    if args.gnn_eval_1024:
+        print(json.dumps({"gnn_eval_1024": gnn_eval_1024(dev, args.gnn_ckpt or GNN_CKPT)}),
+              flush=True)
+        return 0
     x, eb = make_field(dev)
     nbytes = x.numel() * x.element_size()
 

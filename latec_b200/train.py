@@ -417,18 +417,22 @@ class Trainer:
 
 
 def train(steps=3000, *, d=64, agg_level=1, shape4=(16, 16, 16, 16), batch4=4,
-          shape2=(128, 128), batch2=16, stride4=8, noise_range=(1e-4, 1e-2), lr=2e-3, warmup=100,
+          shape2=(128, 128), batch2=16, stride4=8, shape3=(40, 40, 40), batch3=0, stride3=8,
+          noise_range=(1e-4, 1e-2), lr=2e-3, warmup=100,
           ema_decay=0.999, mse_weight=1.0, seed=0, device=None, log_every=50, out=None,
           trainer=None, callback=None, synthetic=None):
     """Train on mixed 4-D / 2-D synthetic batches (train_h100.sh: 16^4 x 4
-    plus 128^2 x 16 per step); returns the Trainer. ``synthetic`` overrides
+    plus 128^2 x 16 per step); returns the Trainer. ``batch3`` > 0 adds 3-D
+    fields of ``shape3`` (the 4-D correlation knob, ``stride3``) to every step,
+    a mix the reference's script does not train on. ``synthetic`` overrides
     the generator's distribution knobs (``latec_b200.synthetic.DEFAULTS``, the
     reference's synthetic_dist.yaml)."""
     from .synthetic import DEFAULTS, sample_synthetic_batch
 
     knobs = dict(DEFAULTS, **(synthetic or {}))
     gen = {k: knobs[k] for k in ("turbulence_frac", "max_discontinuities", "discontinuity_frac")}
-    corr = {"synthetic": knobs["correlation_4d"], "field2d": knobs["correlation_2d"]}
+    corr = {"synthetic": knobs["correlation_4d"], "field2d": knobs["correlation_2d"],
+            "field3d": knobs["correlation_4d"]}
 
     tr = trainer or Trainer(d=d, agg_level=agg_level, seed=seed, lr=lr, ema_decay=ema_decay,
                             mse_weight=mse_weight, device=device)
@@ -438,16 +442,18 @@ def train(steps=3000, *, d=64, agg_level=1, shape4=(16, 16, 16, 16), batch4=4,
     for step in range(steps):
         tr.zero_grad()
         logs = {}
-        n4 = math.prod(shape4) * batch4 if batch4 else 0
-        n2 = math.prod(shape2) * batch2 if batch2 else 0
-        for kind, shp, bsz, stride in (("synthetic", shape4, batch4, stride4),
-                                        ("field2d", shape2, batch2, int(rng.choice(strides2)))):
+        legs = [("synthetic", shape4, batch4, stride4),
+                ("field2d", shape2, batch2, int(rng.choice(strides2)))]
+        if batch3:
+            legs.append(("field3d", shape3, batch3, stride3))
+        npts = {k: (math.prod(shp) * b if b else 0) for k, shp, b, _ in legs}
+        for kind, shp, bsz, stride in legs:
             if not bsz:
                 continue
             x = sample_synthetic_batch(bsz, shp, corr[kind], rng, device=tr.device, **gen)
             eb = sample_noise(bsz, noise_range, rng, tr.device)
             levels = stride.bit_length() - 1
-            w = (n4 if kind == "synthetic" else n2) / max(n4 + n2, 1)
+            w = npts[kind] / max(sum(npts.values()), 1)
             bits, mse, mae, _ = tr.run_stages(x, shp, levels, stride, eb, weight=w, rng=rng)
             logs[kind] = (bits, mse, mae)
         tr.optimizer_step(tr.lr * lr_factor(step, steps, warmup))
@@ -475,6 +481,8 @@ def main(argv=None):
     ap.add_argument("--mse-weight", type=float, default=1.0)
     ap.add_argument("--batch4", type=int, default=4)
     ap.add_argument("--batch2", type=int, default=16)
+    ap.add_argument("--batch3", type=int, default=0)
+    ap.add_argument("--shape3", type=int, nargs=3, default=(40, 40, 40))
     ap.add_argument("--noise-range", type=float, nargs=2, default=(1e-4, 1e-2))
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default="gnn_trained.pt")
@@ -491,7 +499,8 @@ def main(argv=None):
              "correlation_4d": a.synthetic_correlation,
              "correlation_2d": a.synthetic_2d_correlation}
     train(a.steps, d=a.d, agg_level=a.agg_level, lr=a.lr, warmup=a.warmup, ema_decay=a.ema_decay,
-          mse_weight=a.mse_weight, batch4=a.batch4, batch2=a.batch2,
+          mse_weight=a.mse_weight, batch4=a.batch4, batch2=a.batch2, batch3=a.batch3,
+          shape3=tuple(a.shape3),
           noise_range=tuple(a.noise_range), seed=a.seed, out=a.out,
           synthetic={k: v for k, v in given.items() if v is not None})
 

@@ -2,9 +2,9 @@
 (shape, level) cost the exact 64-bit sum of rint(W * 2^20) * count over the
 power-of-two alphabet, first argmin over levels, first strictly smaller shape)
 against the oracle's restatement (oracle/rans_model.py fit_const_native), bit
-for bit, for
-coder windows from 4 symbols to 16,384: counts in shared memory and in
-global memory, dense, sparse and single-bin histograms, in one launch."""
+for bit, for coder windows from 4 symbols to 16,384: counts in shared memory
+and in global memory, dense, sparse and single-bin histograms, in one
+launch."""
 
 import ctypes
 
