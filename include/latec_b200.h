@@ -115,7 +115,8 @@ uint64_t latec_flat_workspace_bytes(uint64_t items, int32_t dtype);
  *      replaces latec/codec.py:384-459 (_compress_region) with
  *      latec/predictor.py:255-317 (InterpPredictor.predict) and
  *      latec/quantizer.py:28-120 (quantize / dequantize).
- * x, recon: (C, *spatial) device arrays of dtype; recon must be zeroed.
+ * x, recon: (C, *spatial) device arrays of dtype; every point of recon is
+ *   written (the call clears it first when a fused level mode is on).
  * stage_eb: host array, one absolute bound per stage.
  * codes: u16, C*n_t per stage, stage t at offset C*sum(n_<t).
  * outliers: dtype elements, stage t's compacted outliers at the same offset.
@@ -173,13 +174,13 @@ int latec_set_level_mode(int32_t mode);
  *      level. Results are bit-identical in all modes. Process-wide. */
 int latec_set_tile_mode(int32_t mode);
 
-/* ---- row segments (no counterpart in the reference): 1 = the
- *      per-stage encode and decode of rank 2..4 single-channel plans walk each
- *      stage in warp segments of 256 consecutive ranks along the grid rows
- *      (one rank decode and one set of tap offsets per segment, rows of at
- *      least 128 stage points; decode tiles with outliers keep the per-point
- *      path); 0 (default) = one rank decode per point. Results are
- *      bit-identical.
+/* ---- row segments (no counterpart in the reference): 1 (default) = the
+ *      per-stage encode and decode walk each single-class stage (anchors,
+ *      weight-1 sub-stages) of a rank 2..4 single-channel plan in warp
+ *      segments of 256 consecutive ranks along the grid rows (one rank
+ *      decode and one set of tap offsets per segment, rows of at least 128
+ *      stage points; decode tiles with outliers keep the per-point path);
+ *      0 = one rank decode per point everywhere. Results are bit-identical.
  *      Process-wide. */
 int latec_set_row_mode(int32_t on);
 
@@ -199,7 +200,9 @@ int latec_kernel_time(int32_t kind, double* ms, uint32_t* launches);
  *      latec_rans_decode; outliers: device byte array holding every stage's
  *      outliers (dtype elements, no alignment required), stage t starting at
  *      byte out_off[t] with n_out[t] entries (host arrays). err: device word,
- *      bit 1 = outlier count mismatch. recon must be zeroed. */
+ *      bit 1 = outlier count mismatch. Every point of recon is written (the
+ *      call clears it first when a fused level or level-scheduling mode is
+ *      on). */
 int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
                         const double* stage_eb, const uint16_t* codes, const void* outliers,
                         const uint64_t* out_off, const uint32_t* n_out, void* recon,

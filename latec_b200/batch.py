@@ -222,10 +222,12 @@ def autotune_many(tensors, eb, predictor, levels=4, anchor_stride=16, anchor_blo
             groups[key].append(jb)
     out = {}
     for key, jobs in sorted(groups.items()):
-        views, _ = _arenas([buffer_sizes(jb.plan, jb.c, jb.elem) for jb in jobs], dev)
+        # the shared buffers stay referenced (bufs) while the trials run: the
+        # views hold raw addresses only
+        views, bufs = _arenas([buffer_sizes(jb.plan, jb.c, jb.elem) for jb in jobs], dev)
         esz = jobs[0].field.element_size()
         rsz = [-(-jb.field.numel() * esz // _ALIGN) * _ALIGN for jb in jobs]
-        recon = torch.zeros(max(sum(rsz), 1), dtype=torch.uint8, device=dev)
+        recon = torch.empty(max(sum(rsz), 1), dtype=torch.uint8, device=dev)
         roff = np.concatenate([[0], np.cumsum(rsz)[:-1]]).astype(np.int64).tolist()
         for jb, v, ro in zip(jobs, views, roff):
             jb.buf = _Buffers(jb.plan, jb.c, jb.src, dev, views=v)
@@ -246,8 +248,10 @@ def autotune_many(tensors, eb, predictor, levels=4, anchor_stride=16, anchor_blo
             t = min(ms)
             if best is None or t < best[1]:
                 best = (int(cap), t)
+        torch.cuda.synchronize()
         for jb in jobs:
             del jb.buf, jb.recon
+        del bufs, recon
         _cta_caps[key] = best[0]
         out[key] = best
     return out
@@ -270,10 +274,11 @@ def _compress_group(jobs, predictor, dev, lib):
     sp = _lib.stream_ptr()
     views, bufs = _arenas([buffer_sizes(jb.plan, jb.c, jb.elem) for jb in jobs], dev)
     ssz = ctypes.sizeof(_lib.StageStats)
-    # the reconstructions the stage kernels work in: one zeroed buffer
+    # the reconstructions the stage kernels work in: one buffer (every
+    # point is written)
     esz = jobs[0].field.element_size()
     rsz = [-(-jb.field.numel() * esz // _ALIGN) * _ALIGN for jb in jobs]
-    recon = torch.zeros(max(sum(rsz), 1), dtype=torch.uint8, device=dev)
+    recon = torch.empty(max(sum(rsz), 1), dtype=torch.uint8, device=dev)
     roff = np.concatenate([[0], np.cumsum(rsz)[:-1]]).astype(np.int64).tolist()
     for jb, v, ro in zip(jobs, views, roff):
         jb.buf = _Buffers(jb.plan, jb.c, jb.src, dev, views=v)
@@ -635,7 +640,7 @@ def decompress_many(streams, *, device=None, out="numpy"):
         prm = _qparams(h.src_dtype, c, h.radius, pred.order, h.interp_center, end_mode,
                        h.src_dtype == 0)
         ft = torch.float64 if h.src_dtype == 2 else torch.float32
-        recon = torch.zeros((c,) + spatial[k], dtype=ft, device=dev)
+        recon = torch.empty((c,) + spatial[k], dtype=ft, device=dev)  # every point decoded
         eb_arr = (ctypes.c_double * ns)(*[float(e) for e in ebs])
         out_at = (ctypes.c_uint64 * ns)(*[recs[st0[k] + t].out_at for t in range(ns)])
         n_out = (ctypes.c_uint32 * ns)(*[recs[st0[k] + t].n_out for t in range(ns)])

@@ -212,7 +212,8 @@ class _Encoder:
         eb_arr = (ctypes.c_double * ns)(*[float(e) for e in ebs])
         stream = _lib.stream_ptr()
         t0 = time.perf_counter()
-        recon.zero_()
+        if self.predictor is not None:
+            recon.zero_()
         if self.predictor is None:
             _lib.check(lib.latec_encode_stages(
                 plan.handle, ctypes.byref(prm), eb_arr, self.field.data_ptr(), recon.data_ptr(),
@@ -914,7 +915,7 @@ def decompress(stream, predictor_factory=None, *, device=None, out="numpy"):
         prm = _qparams(header.src_dtype, c, header.radius, predictor.order, predictor.center,
                        predictor.end_mode, header.src_dtype == 0)
     ft = torch.float64 if header.src_dtype == 2 else torch.float32
-    recon = torch.zeros((c,) + spatial, dtype=ft, device=dev)
+    recon = torch.empty((c,) + spatial, dtype=ft, device=dev)  # every point is decoded
     eb_arr = (ctypes.c_double * ns)(*[float(e) for e in ebs])
     out_off = (ctypes.c_uint64 * ns)(*[recs[t].out_at for t in range(ns)])
     n_out = (ctypes.c_uint32 * ns)(*[recs[t].n_out for t in range(ns)])

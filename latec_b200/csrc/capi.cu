@@ -600,6 +600,10 @@ int latec_encode_stages(const latec_plan* plan, const latec_quant_params* prm,
         return LATEC_ERR_CUDA;
     uint64_t off = 0, seg = 0;
     const int tmode = g_tile_mode.load();
+    // per-stage launches read only points of earlier stages and write every
+    // point; the fused levels stage whole planes of the canvas
+    if (tmode && cudaMemsetAsync(recon, 0, plan->points * C * elem, st) != cudaSuccess)
+        return LATEC_ERR_CUDA;
     for (int t = 0; t < ns; t++) {
         if (tile_level_at(plan, t, tmode)) {
             // the level's five stages in one fused launch, then per stage the
@@ -777,6 +781,9 @@ int latec_decode_stages(const latec_plan* plan, const latec_quant_params* prm,
     if (rc) return rc;
     const int mode = g_level_mode.load();
     const int tmode = g_tile_mode.load();
+    if ((mode || tmode) &&
+        cudaMemsetAsync(recon, 0, plan->points * C * elem_of(prm->dtype), st) != cudaSuccess)
+        return LATEC_ERR_CUDA;
     int t = 0;
     while (t < ns) {
         if (tile_level_at(plan, t, tmode)) {

@@ -1324,7 +1324,7 @@ uint32_t encode_blocks(uint64_t items) {
     return b;
 }
 
-std::atomic<int> g_row_mode{0};
+std::atomic<int> g_row_mode{1};
 
 // Row-segment kernels: one channel, rank 2..4 without blocked anchors, 32-bit
 // tap offsets, and rows long enough that a warp segment stays in one row.

@@ -138,7 +138,7 @@ inline uint32_t n_segments(uint64_t items) {
     return (uint32_t)((items + (1ull << SEG_SHIFT) - 1) >> SEG_SHIFT);
 }
 
-// Row-segment stage kernels on (1) or off (0, default): process-wide.
+// Row-segment stage kernels on (1, default) or off (0): process-wide.
 extern std::atomic<int> g_row_mode;
 
 // Launchers (interp_kernels.cu). items = channels * stage points.

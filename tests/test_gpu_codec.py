@@ -226,8 +226,8 @@ def test_256cube_stream_matches_oracle(dtype, tile_mode):
     ((90, 70, 260), np.float32, "linear", 2),
 ])
 def test_row_segments_match_per_point_decode(shape, dtype, order, center):
-    """The row-segment stage kernels (opt-in) and the per-point decode code
-    the same stream and reconstruction, rows of every length and parity: ragged
+    """The row-segment stage kernels (the default) and the per-point decode
+    code the same stream and reconstruction, rows of every length and parity: ragged
     last axes, float64, rank 2 and 4, linear order, both single-axis centers;
     the stream of the first case is also the oracle's."""
     from latec_b200 import _lib, fields
@@ -244,9 +244,9 @@ def test_row_segments_match_per_point_decode(shape, dtype, order, center):
             _lib.check(lib.latec_set_row_mode(mode))
             got[mode] = lb.compress(x, eb, pred(), levels=lv, anchor_stride=16)
         _lib.check(lib.latec_set_row_mode(1))
-        back = lb.decompress(got[1][0])  # decoded with row segments too
+        back = lb.decompress(got[1][0])  # decoded with row segments
     finally:
-        _lib.check(lib.latec_set_row_mode(0))
+        _lib.check(lib.latec_set_row_mode(1))
     assert got[1][0] == got[0][0]
     assert np.array_equal(back, got[0][1]["recon"])
     assert np.array_equal(got[1][1]["recon"], got[0][1]["recon"])
