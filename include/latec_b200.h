@@ -525,6 +525,25 @@ int latec_tr_linear_bwd(const float* X, int64_t ldx, int64_t rows, int32_t in, c
                         int32_t out, const float* dY, int64_t ldy, const float* Z, int32_t act,
                         float* dX, int64_t lddx, int32_t accum_dx, float* dW, float* db,
                         void* stream);
+/* The same two ops with BF16 GEMM operands and float32 accumulation: mixed-
+ * precision training with float32 master weights, as the reference's
+ * optional FP16 autocast (scripts/train_gnn.py:147-150, GradScaler at 938);
+ * BF16 keeps float32's exponent range, so no loss scale is needed. Both
+ * operands of each GEMM are rounded to BF16 (nearest even) as they are
+ * staged; tcgen05 tensor cores with tensor-memory accumulators where both
+ * output dimensions are at least 32, SIMT tiles for the narrow layers. Bias,
+ * activation, saved pre-activation and gradients stay float32. */
+int latec_tr_linear_bf16(const float* X, int64_t ldx, int64_t rows, int32_t in, const float* W,
+                         const float* b, int32_t out, float* Y, int64_t ldy, int32_t act, float* Z,
+                         void* stream);
+int latec_tr_linear_bwd_bf16(const float* X, int64_t ldx, int64_t rows, int32_t in,
+                             const float* W, int32_t out, const float* dY, int64_t ldy,
+                             const float* Z, int32_t act, float* dX, int64_t lddx,
+                             int32_t accum_dx, float* dW, float* db, void* stream);
+/* Reads and clears the tensor-core GEMMs' error word; LATEC_ERR_INTERNAL if
+ * an MMA completion wait ran out since the last call (its tile is then not
+ * written). Synchronises the stream. */
+int latec_tr_gemm_status(void* stream);
 /* Message rows of all batches (two-sided when two, else one-sided) for the
  * pairs of a stage (latec/gnn_predictor.py:618-660 BiDirEmbed / DirEmbed
  * inputs) and their backward into dE and the direction-state table. */

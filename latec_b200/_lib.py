@@ -161,6 +161,10 @@ SIGNATURES = {
     "latec_tr_linear": (ctypes.c_int, [P, I64, I64, I32, P, P, I32, P, I64, I32, P, P]),
     "latec_tr_linear_bwd": (ctypes.c_int, [P, I64, I64, I32, P, I32, P, I64, P, I32, P, I64, I32,
                                            P, P, P]),
+    "latec_tr_linear_bf16": (ctypes.c_int, [P, I64, I64, I32, P, P, I32, P, I64, I32, P, P]),
+    "latec_tr_linear_bwd_bf16": (ctypes.c_int, [P, I64, I64, I32, P, I32, P, I64, P, I32, P, I64,
+                                                I32, P, P, P]),
+    "latec_tr_gemm_status": (ctypes.c_int, [P]),
     "latec_tr_rows": (ctypes.c_int, [P, I64, I32, I32, I32, P, ctypes.POINTER(GnnGeom), P, I64,
                                      I32, I32, P, I32, P]),
     "latec_tr_rows_bwd": (ctypes.c_int, [P, I32, I64, I32, I32, I32, ctypes.POINTER(GnnGeom), P,

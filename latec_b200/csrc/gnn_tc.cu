@@ -32,89 +32,16 @@
 #include <cstdint>
 
 #include "latec_common.cuh"
+#include "tc_sm100.cuh"
 
 namespace latec {
 namespace {
 
 constexpr int TC_THREADS = 256;
 constexpr int TC_M = 128;
-constexpr uint32_t TC_WAIT_LIMIT = 1u << 24;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// Canonical K-major element offset of (row r, column k) in an R-row operand.
-__host__ __device__ __forceinline__ uint32_t canon(uint32_t r, uint32_t k, uint32_t R) {
-    return ((k >> 3) * (R >> 3) + (r >> 3)) * 64u + (r & 7u) * 8u + (k & 7u);
-}
-
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);  // version 1, no swizzle
-}
-
-// kind::f16 instruction descriptor: BF16 A and B (K-major), FP32 D, M x N.
-__host__ __device__ constexpr uint32_t idesc_bf16(uint32_t M, uint32_t N) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
-                                         uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-        "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t mbar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-        mbar));
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred P;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, P;\n\t}\n"
-        : "=r"(ok)
-        : "r"(mbar), "r"(parity));
-    return ok != 0;
-}
-
-// Bounded wait: false if the phase did not complete within the limit.
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-    for (uint32_t i = 0; i < TC_WAIT_LIMIT; i++)
-        if (mbar_try_wait(mbar, parity)) return true;
-    return false;
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%"
-        "14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-          "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
-}
 
 __device__ __forceinline__ float gelu_tc(float x) {
     return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f));
-}
-
-// 16-byte shared store of 8 BF16 values.
-__device__ __forceinline__ void st_bf16x8(__nv_bfloat16* dst, const float* v) {
-    __nv_bfloat162 p[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) p[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-    *(int4*)dst = *(const int4*)p;
 }
 
 struct GatherRow {

@@ -1,18 +1,27 @@
 // Training kernels of the learned predictor (scripts/train_gnn.py): the
 // forward ops of the axial GNN with the activations the backward pass needs,
 // their backward ops, the discretised-Laplace rate loss and the AdamW / EMA
-// updates. float32 throughout; gradient reductions over rows use atomics
-// (training needs no run-to-run bit identity; the codec's inference path is
-// gnn_kernels.cu, whose order is fixed).
+// updates. Activations, weights, gradients and optimiser state are float32;
+// gradient reductions over rows use atomics (training needs no run-to-run bit
+// identity; the codec's inference path is gnn_kernels.cu, whose order is
+// fixed). The linear layers' GEMMs run in one of two precisions:
+//   - float32: SIMT tiles (k_gemm);
+//   - BF16 (the reference's mixed-precision training, with float32 master
+//     weights): both operands rounded to BF16 as they are staged, float32
+//     accumulation; tcgen05 tensor-core tiles (k_gemm_tc, accumulators in
+//     tensor memory) where the output tile is at least 32 wide, the SIMT tile
+//     with the same operand rounding for the narrow 1- and 2-wide layers.
 //
 // Layouts: X (rows, ldx) row-major; weights W (out, in) row-major as in the
 // reference's nn.Linear; E (B, N, K, d); contexts (B, M, K, d).
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdint>
 
 #include "latec_common.cuh"
+#include "tc_sm100.cuh"
 
 namespace latec {
 namespace {
@@ -35,12 +44,14 @@ __device__ __forceinline__ float gelu_d(float z) {
 //   TB = 0: B(k, n) = B[k * ldb + n]; TB = 1: B(k, n) = B[n * ldb + k]
 //   GA: A is dY and is multiplied by gelu'(Z) on load (Z laid out like A)
 //   split-K over gridDim.z; ACC: add into C with atomics, else store
-//   bias (optional, added once by the z = 0 slice)
+//   bias (optional; only without split-K)
+//   bf: operands rounded to BF16 (round to nearest even) as they are staged
 template <int TA, int TB, int GA, int ACC>
 __global__ void __launch_bounds__(TT)
     k_gemm(int M, int N, int Kd, const float* __restrict__ A, int64_t lda,
            const float* __restrict__ Bm, int64_t ldb, const float* __restrict__ Z, float* C,
-           int64_t ldc, const float* __restrict__ bias, int act, float* Zout, int64_t ldz) {
+           int64_t ldc, const float* __restrict__ bias, int act, float* Zout, int64_t ldz,
+           int bf) {
     __shared__ float as[GK][GM + 4];
     __shared__ float bs[GK][GN + 4];
     const int m0 = blockIdx.x * GM, n0 = blockIdx.y * GN;
@@ -59,6 +70,7 @@ __global__ void __launch_bounds__(TT)
                 const int64_t o = TA ? k * lda + m : (int64_t)m * lda + k;
                 v = A[o];
                 if (GA) v *= gelu_d(Z[o]);
+                if (bf) v = __bfloat162float(__float2bfloat16_rn(v));
             }
             as[kk][mm] = v;
         }
@@ -67,7 +79,9 @@ __global__ void __launch_bounds__(TT)
             if (TB) { nn = e / GK; kk = e % GK; } else { kk = e / GN; nn = e % GN; }
             const int n = n0 + nn;
             const int64_t k = k0 + kk;
-            bs[kk][nn] = (n < N && k < ke) ? Bm[TB ? (int64_t)n * ldb + k : k * ldb + n] : 0.0f;
+            float v = (n < N && k < ke) ? Bm[TB ? (int64_t)n * ldb + k : k * ldb + n] : 0.0f;
+            if (bf) v = __bfloat162float(__float2bfloat16_rn(v));
+            bs[kk][nn] = v;
         }
         __syncthreads();
 #pragma unroll
@@ -102,6 +116,200 @@ __global__ void __launch_bounds__(TT)
             }
         }
     }
+}
+
+// ------------------------------------------------- BF16 tensor-core GEMM
+// The contract of k_gemm (same TA / TB / GA / ACC meaning, bias, act, Zout,
+// split-K over gridDim.z) on tcgen05: a CTA computes a 128 x NT tile of C
+// with FP32 accumulators in tensor memory (NT columns). K is staged GT_KC
+// elements at a time into a two-buffer ring: all 256 threads load the chunk of
+// A (128 rows) and of B (NT rows of B^T) as float32, apply gelu' to A when GA,
+// round both to BF16 and store them in the no-swizzle K-major canonical
+// layout; one thread then issues GT_KC / 16 MMAs (M 128, N NT, K 16) and
+// commits them to the buffer's mbarrier, which the threads wait on before
+// they refill that buffer two chunks later, so the staging of a chunk
+// overlaps the MMAs of the previous one. The epilogue reads each thread's
+// TMEM lane (one row of the tile) 16 columns at a time. Waits are bounded: on
+// expiry the kernel sets bit 0 of g_gemm_tc_err, waits (bounded) for the MMAs
+// it issued and frees its tensor memory.
+constexpr int GT_THREADS = 256;
+constexpr int GT_M = 128;
+constexpr int GT_KC = 64;
+
+__device__ uint32_t g_gemm_tc_err;
+
+// One GT_KC-wide K chunk of an R-row operand: element (r, k) is
+// src[r * rs + k * ks], zero at r >= r_valid or k >= k_end; times gelu'(Z) at
+// the same offset when GA. Consecutive threads take consecutive rows, so the
+// loads are coalesced when rs == 1 and each thread reads 32 contiguous bytes
+// when ks == 1; the canonical stores of a warp fill 512 contiguous bytes.
+template <int R, int GA>
+__device__ __forceinline__ void stage_chunk(__nv_bfloat16* dst, const float* __restrict__ src,
+                                            const float* __restrict__ Z, int64_t rs, int64_t ks,
+                                            int r_valid, int64_t k0, int64_t k_end, int tid) {
+    constexpr int ITEMS = R * (GT_KC / 8);
+    for (int it = tid; it < ITEMS; it += GT_THREADS) {
+        const int r = it % R, c = it / R;
+        float v[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const int64_t k = k0 + c * 8 + e;
+            float x = 0.0f;
+            if (r < r_valid && k < k_end) {
+                const int64_t o = (int64_t)r * rs + k * ks;
+                x = src[o];
+                if (GA) x *= gelu_d(Z[o]);
+            }
+            v[e] = x;
+        }
+        st_bf16x8(dst + canon((uint32_t)r, (uint32_t)(c * 8), R), v);
+    }
+}
+
+template <int TA, int TB, int GA, int ACC, int NT>
+__global__ void __launch_bounds__(GT_THREADS)
+    k_gemm_tc(int M, int N, int Kd, const float* __restrict__ A, int64_t lda,
+              const float* __restrict__ Bm, int64_t ldb, const float* __restrict__ Z, float* C,
+              int64_t ldc, const float* __restrict__ bias, int act, float* Zout, int64_t ldz) {
+    static_assert(NT == 64 || NT == 128, "tile width");
+    constexpr int A_ELEMS = GT_M * GT_KC, B_ELEMS = NT * GT_KC;
+    constexpr uint32_t TMEM_COLS = NT;
+    extern __shared__ __align__(128) uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_base;
+    __nv_bfloat16* sbuf = (__nv_bfloat16*)smem_raw;  // [A0 | B0 | A1 | B1]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * GT_M, n0 = blockIdx.y * NT;
+    const int64_t per = ((int64_t)Kd + gridDim.z - 1) / gridDim.z;
+    const int64_t kb = per * blockIdx.z;
+    const int64_t ke = kb + per < Kd ? kb + per : Kd;
+    // A(m, k) = TA ? A[k lda + m] : A[m lda + k]; B^T(n, k) = B(k, n)
+    const int64_t a_rs = TA ? 1 : lda, a_ks = TA ? lda : 1;
+    const int64_t a_off = TA ? (int64_t)m0 : (int64_t)m0 * lda;
+    const int64_t b_rs = TB ? ldb : 1, b_ks = TB ? 1 : ldb;
+    const int64_t b_off = TB ? (int64_t)n0 * ldb : (int64_t)n0;
+    const int m_valid = M - m0 < GT_M ? M - m0 : GT_M;
+    const int n_valid = N - n0 < NT ? N - n0 : NT;
+
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar[0])), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar[1])), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_base)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base;
+
+    const int nk = ke > kb ? (int)((ke - kb + GT_KC - 1) / GT_KC) : 0;
+    bool ok = true;
+    int issued = 0;  // chunks whose MMAs were committed
+    for (int i = 0; i < nk; i++) {
+        const int s = i & 1;
+        if (i >= 2) {  // the MMAs of chunk i - 2 have read buffer s
+            ok = __syncthreads_and(mbar_wait(smem_u32(&mbar[s]), (uint32_t)((i - 2) >> 1) & 1u)) != 0;
+            if (!ok) break;
+        }
+        __nv_bfloat16* sa = sbuf + s * (A_ELEMS + B_ELEMS);
+        __nv_bfloat16* sb = sa + A_ELEMS;
+        const int64_t k0 = kb + (int64_t)i * GT_KC;
+        stage_chunk<GT_M, GA>(sa, A + a_off, GA ? Z + a_off : nullptr, a_rs, a_ks, m_valid, k0,
+                              ke, tid);
+        stage_chunk<NT, 0>(sb, Bm + b_off, nullptr, b_rs, b_ks, n_valid, k0, ke, tid);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sb);
+#pragma unroll
+            for (int kk = 0; kk < GT_KC / 16; kk++) {
+                const uint64_t ad = smem_desc(a0 + kk * 2 * GT_M * 16, GT_M * 16, 128);
+                const uint64_t bd = smem_desc(b0 + kk * 2 * NT * 16, NT * 16, 128);
+                mma_bf16(tmem, ad, bd, idesc_bf16(GT_M, NT), (i > 0 || kk > 0) ? 1u : 0u);
+            }
+            mma_commit(smem_u32(&mbar[s]));
+        }
+        issued = i + 1;
+    }
+    if (issued) {  // the last commit covers every MMA issued before it
+        const int l = issued - 1;
+        const bool got = __syncthreads_and(
+                             mbar_wait(smem_u32(&mbar[l & 1]), (uint32_t)(l >> 1) & 1u)) != 0;
+        ok = ok && got;
+    }
+    if (!ok && tid == 0) atomicOr(&g_gemm_tc_err, 1u);
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (ok && issued) {
+        const int quarter = warp & 3, half = warp >> 2;
+        const int m = m0 + quarter * 32 + lane;  // this thread's TMEM lane
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        for (int c = half * (NT / 2); c < (half + 1) * (NT / 2); c += 16) {
+            float v[16];
+            tmem_ld16(tmem + lane_base + c, v);
+            if (m >= M) continue;
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                const int n = n0 + c + i;
+                if (n >= N) continue;
+                float x = v[i];
+                if (ACC) {
+                    atomicAdd(&C[(int64_t)m * ldc + n], x);
+                } else {
+                    if (bias) x += bias[n];
+                    if (Zout) Zout[(int64_t)m * ldz + n] = x;
+                    C[(int64_t)m * ldc + n] = act ? gelu_f(x) : x;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(TMEM_COLS));
+    }
+}
+
+template <int NT>
+constexpr int gemm_tc_smem() {
+    return 2 * (GT_M + NT) * GT_KC * (int)sizeof(__nv_bfloat16);
+}
+
+// C = A B (see k_gemm) in float32 (prec 0) or BF16 operands with float32
+// accumulation (prec 1: tensor cores when M and N are at least 32, the SIMT
+// tile with rounded operands otherwise). Returns the launches.
+template <int TA, int TB, int GA, int ACC>
+int gemm(int prec, int M, int N, int Kd, unsigned splits, const float* A, int64_t lda,
+         const float* Bm, int64_t ldb, const float* Z, float* C, int64_t ldc, const float* bias,
+         int act, float* Zout, int64_t ldz, cudaStream_t st) {
+    if (prec == 1 && M >= 32 && N >= 32) {
+        if (N > 64) {
+            constexpr int NT = 128;
+            cudaFuncSetAttribute(k_gemm_tc<TA, TB, GA, ACC, NT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tc_smem<NT>());
+            dim3 grid((unsigned)((M + GT_M - 1) / GT_M), (unsigned)((N + NT - 1) / NT), splits);
+            k_gemm_tc<TA, TB, GA, ACC, NT><<<grid, GT_THREADS, gemm_tc_smem<NT>(), st>>>(
+                M, N, Kd, A, lda, Bm, ldb, Z, C, ldc, bias, act, Zout, ldz);
+        } else {
+            constexpr int NT = 64;
+            cudaFuncSetAttribute(k_gemm_tc<TA, TB, GA, ACC, NT>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, gemm_tc_smem<NT>());
+            dim3 grid((unsigned)((M + GT_M - 1) / GT_M), (unsigned)((N + NT - 1) / NT), splits);
+            k_gemm_tc<TA, TB, GA, ACC, NT><<<grid, GT_THREADS, gemm_tc_smem<NT>(), st>>>(
+                M, N, Kd, A, lda, Bm, ldb, Z, C, ldc, bias, act, Zout, ldz);
+        }
+        return 1;
+    }
+    dim3 grid((unsigned)((M + GM - 1) / GM), (unsigned)((N + GN - 1) / GN), splits);
+    k_gemm<TA, TB, GA, ACC><<<grid, TT, 0, st>>>(M, N, Kd, A, lda, Bm, ldb, Z, C, ldc, bias, act,
+                                                 Zout, ldz, prec == 1 ? 1 : 0);
+    return 1;
 }
 
 // db[j] += sum_r dY[r, j] (* gelu'(Z[r, j])): one warp per column slice.
@@ -497,6 +705,52 @@ int done(int n) {
     return cudaGetLastError() == cudaSuccess ? LATEC_OK : LATEC_ERR_CUDA;
 }
 
+int linear_fwd(int prec, const float* X, int64_t ldx, int64_t rows, int32_t in, const float* W,
+               const float* b, int32_t out, float* Y, int64_t ldy, int32_t act, float* Z,
+               void* stream) {
+    if (rows < 0 || in < 1 || out < 1 || !W || (rows && (!X || !Y)) || rows > 0x7fffffff)
+        return LATEC_ERR_ARG;
+    if (!rows) return LATEC_OK;
+    return done(gemm<0, 1, 0, 0>(prec, (int)rows, out, in, 1, X, ldx, W, in, nullptr, Y, ldy, b,
+                                 act, Z, ldy, (cudaStream_t)stream));
+}
+
+int linear_bwd(int prec, const float* X, int64_t ldx, int64_t rows, int32_t in, const float* W,
+               int32_t out, const float* dY, int64_t ldy, const float* Z, int32_t act, float* dX,
+               int64_t lddx, int32_t accum_dx, float* dW, float* db, void* stream) {
+    if (rows < 0 || in < 1 || out < 1 || !W || !dW || !db || (act && !Z) ||
+        (rows && (!X || !dY)) || rows > 0x7fffffff)
+        return LATEC_ERR_ARG;
+    if (!rows) return LATEC_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const float* Zg = act ? Z : nullptr;
+    const int r = (int)rows;
+    int n = 0;
+    if (dX) {  // dX (rows, in) = dZ (rows, out) W (out, in)
+        if (act)
+            n += accum_dx ? gemm<0, 0, 1, 1>(prec, r, in, out, 1, dY, ldy, W, in, Zg, dX, lddx,
+                                             nullptr, 0, nullptr, 0, st)
+                          : gemm<0, 0, 1, 0>(prec, r, in, out, 1, dY, ldy, W, in, Zg, dX, lddx,
+                                             nullptr, 0, nullptr, 0, st);
+        else
+            n += accum_dx ? gemm<0, 0, 0, 1>(prec, r, in, out, 1, dY, ldy, W, in, nullptr, dX,
+                                             lddx, nullptr, 0, nullptr, 0, st)
+                          : gemm<0, 0, 0, 0>(prec, r, in, out, 1, dY, ldy, W, in, nullptr, dX,
+                                             lddx, nullptr, 0, nullptr, 0, st);
+    }
+    // dW[j, i] += sum_r dZ[r, j] X[r, i]: split over rows
+    const unsigned splits = (unsigned)std::min<int64_t>(256, (rows + 4095) / 4096);
+    if (act)
+        n += gemm<1, 0, 1, 1>(prec, out, in, r, splits ? splits : 1, dY, ldy, X, ldx, Zg, dW, in,
+                              nullptr, 0, nullptr, 0, st);
+    else
+        n += gemm<1, 0, 0, 1>(prec, out, in, r, splits ? splits : 1, dY, ldy, X, ldx, nullptr, dW,
+                              in, nullptr, 0, nullptr, 0, st);
+    dim3 gb((unsigned)std::min<int64_t>(1024, (rows + TT - 1) / TT), (unsigned)out, 1);
+    k_colsum<<<gb, TT, 0, st>>>(rows, out, dY, ldy, Zg, db);
+    return done(n + 1);
+}
+
 }  // namespace
 }  // namespace latec
 
@@ -508,13 +762,13 @@ extern "C" {
 int latec_tr_linear(const float* X, int64_t ldx, int64_t rows, int32_t in, const float* W,
                     const float* b, int32_t out, float* Y, int64_t ldy, int32_t act, float* Z,
                     void* stream) {
-    if (rows < 0 || in < 1 || out < 1 || !W || (rows && (!X || !Y)) || rows > 0x7fffffff)
-        return LATEC_ERR_ARG;
-    if (!rows) return LATEC_OK;
-    dim3 grid((unsigned)((rows + GM - 1) / GM), (unsigned)((out + GN - 1) / GN), 1);
-    k_gemm<0, 1, 0, 0><<<grid, TT, 0, (cudaStream_t)stream>>>(
-        (int)rows, out, in, X, ldx, W, in, nullptr, Y, ldy, b, act, Z, ldy);
-    return done(1);
+    return linear_fwd(0, X, ldx, rows, in, W, b, out, Y, ldy, act, Z, stream);
+}
+
+int latec_tr_linear_bf16(const float* X, int64_t ldx, int64_t rows, int32_t in, const float* W,
+                         const float* b, int32_t out, float* Y, int64_t ldy, int32_t act, float* Z,
+                         void* stream) {
+    return linear_fwd(1, X, ldx, rows, in, W, b, out, Y, ldy, act, Z, stream);
 }
 
 // Backward of latec_tr_linear. dY (rows, ldy); Z = the saved pre-activation
@@ -524,44 +778,34 @@ int latec_tr_linear_bwd(const float* X, int64_t ldx, int64_t rows, int32_t in, c
                         int32_t out, const float* dY, int64_t ldy, const float* Z, int32_t act,
                         float* dX, int64_t lddx, int32_t accum_dx, float* dW, float* db,
                         void* stream) {
-    if (rows < 0 || in < 1 || out < 1 || !W || !dW || !db || (act && !Z) ||
-        (rows && (!X || !dY)) || rows > 0x7fffffff)
-        return LATEC_ERR_ARG;
-    if (!rows) return LATEC_OK;
+    return linear_bwd(0, X, ldx, rows, in, W, out, dY, ldy, Z, act, dX, lddx, accum_dx, dW, db,
+                      stream);
+}
+
+int latec_tr_linear_bwd_bf16(const float* X, int64_t ldx, int64_t rows, int32_t in,
+                             const float* W, int32_t out, const float* dY, int64_t ldy,
+                             const float* Z, int32_t act, float* dX, int64_t lddx,
+                             int32_t accum_dx, float* dW, float* db, void* stream) {
+    return linear_bwd(1, X, ldx, rows, in, W, out, dY, ldy, Z, act, dX, lddx, accum_dx, dW, db,
+                      stream);
+}
+
+// Reads and clears the tensor-core GEMMs' error word (bit 0: an MMA wait ran
+// out). Synchronises the stream.
+int latec_tr_gemm_status(void* stream) {
+    uint32_t e = 0;
     cudaStream_t st = (cudaStream_t)stream;
-    const float* Zg = act ? Z : nullptr;
-    int n = 0;
-    if (dX) {
-        dim3 grid((unsigned)((rows + GM - 1) / GM), (unsigned)((in + GN - 1) / GN), 1);
-        if (act) {
-            if (accum_dx)
-                k_gemm<0, 0, 1, 1><<<grid, TT, 0, st>>>((int)rows, in, out, dY, ldy, W, in, Zg, dX,
-                                                        lddx, nullptr, 0, nullptr, 0);
-            else
-                k_gemm<0, 0, 1, 0><<<grid, TT, 0, st>>>((int)rows, in, out, dY, ldy, W, in, Zg, dX,
-                                                        lddx, nullptr, 0, nullptr, 0);
-        } else {
-            if (accum_dx)
-                k_gemm<0, 0, 0, 1><<<grid, TT, 0, st>>>((int)rows, in, out, dY, ldy, W, in, nullptr,
-                                                        dX, lddx, nullptr, 0, nullptr, 0);
-            else
-                k_gemm<0, 0, 0, 0><<<grid, TT, 0, st>>>((int)rows, in, out, dY, ldy, W, in, nullptr,
-                                                        dX, lddx, nullptr, 0, nullptr, 0);
-        }
-        n++;
-    }
-    // dW[j, i] += sum_r dZ[r, j] X[r, i]: split over rows
-    const unsigned splits = (unsigned)std::min<int64_t>(256, (rows + 4095) / 4096);
-    dim3 gw((unsigned)((out + GM - 1) / GM), (unsigned)((in + GN - 1) / GN), splits ? splits : 1);
-    if (act)
-        k_gemm<1, 0, 1, 1><<<gw, TT, 0, st>>>(out, in, (int)rows, dY, ldy, X, ldx, Zg, dW, in,
-                                              nullptr, 0, nullptr, 0);
-    else
-        k_gemm<1, 0, 0, 1><<<gw, TT, 0, st>>>(out, in, (int)rows, dY, ldy, X, ldx, nullptr, dW, in,
-                                              nullptr, 0, nullptr, 0);
-    dim3 gb((unsigned)std::min<int64_t>(1024, (rows + TT - 1) / TT), (unsigned)out, 1);
-    k_colsum<<<gb, TT, 0, st>>>(rows, out, dY, ldy, Zg, db);
-    return done(n + 2);
+    if (cudaMemcpyFromSymbolAsync(&e, g_gemm_tc_err, sizeof e, 0, cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return LATEC_ERR_CUDA;
+    if (!e) return LATEC_OK;
+    const uint32_t zero = 0;
+    if (cudaMemcpyToSymbolAsync(g_gemm_tc_err, &zero, sizeof zero, 0, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return LATEC_ERR_CUDA;
+    return LATEC_ERR_INTERNAL;
 }
 
 int latec_tr_rows(const float* E, int64_t N, int32_t K, int32_t d, int32_t ds, const float* table,

@@ -17,8 +17,18 @@ over the last 40 %, train_gnn.py:937-950) and the weight EMA (``ModelEMA``,
 train_gnn.py:154-192) are one kernel each. torch only holds device memory and
 draws the random numbers.
 
-Deliberate differences from the reference trainer: float32 (no FP16 autocast
-/ GradScaler) and no chunked two-chunk scenes (``run_chunked_scene``). The
+Precision: ``precision="fp32"`` runs every linear layer's GEMMs in float32;
+``precision="bf16"`` is the mixed-precision form (the reference trains the
+message pass under optional FP16 autocast with a GradScaler,
+train_gnn.py:147-150,938): the GEMMs' operands are rounded to BF16 and
+accumulated in float32 on the tcgen05 tensor cores (SIMT tiles with the same
+rounding for the 1- and 2-wide layers), while the master weights, gradients,
+AdamW moments and every non-GEMM op stay float32. BF16 has float32's exponent
+range, so no loss scale is kept; a step whose gradient is not finite is
+skipped, as GradScaler skips it.
+
+Deliberate difference from the reference trainer: no chunked two-chunk scenes
+(``run_chunked_scene``). The
 fields come from ``latec_b200.synthetic``, a restatement of the reference's
 generator (advection warp included) whose seeded fields equal the
 reference's.
@@ -85,9 +95,17 @@ class Trainer:
     the kernel-level forward / backward of a teacher-forced stage schedule."""
 
     def __init__(self, d=64, agg_level=1, weights=None, seed=0, lr=2e-3, weight_decay=1e-3,
-                 ema_decay=0.999, mse_weight=1.0, max_radius=64, device=None):
+                 ema_decay=0.999, mse_weight=1.0, max_radius=64, device=None, precision="fp32"):
         torch = _torch()
         self.lib = _lib.load()
+        if precision not in ("fp32", "bf16"):
+            raise ValueError("precision must be 'fp32' or 'bf16'")
+        self.precision = precision
+        bf = precision == "bf16"
+        self._tr_linear = self.lib.latec_tr_linear_bf16 if bf else self.lib.latec_tr_linear
+        self._tr_linear_bwd = (self.lib.latec_tr_linear_bwd_bf16 if bf
+                               else self.lib.latec_tr_linear_bwd)
+        self.skipped_steps = 0
         self.d, self.agg_level = int(d), int(agg_level)
         self.h, self.ds = 2 * self.d, max(1, self.d // 4)
         self.de = self.d + self.ds
@@ -125,14 +143,14 @@ class Trainer:
         """(Y, Z) = act(X W^T + b) with the pre-activation kept when act."""
         Y = self._empty(rows, fout)
         Z = self._empty(rows, fout) if act else None
-        _lib.check(self.lib.latec_tr_linear(X.data_ptr(), fin, rows, fin, self.P.ptr(name + ".weight"),
-                                            self.P.ptr(name + ".bias"), fout, Y.data_ptr(), fout,
-                                            1 if act else 0, Z.data_ptr() if act else None,
-                                            self._s()), "latec_tr_linear")
+        _lib.check(self._tr_linear(X.data_ptr(), fin, rows, fin, self.P.ptr(name + ".weight"),
+                                   self.P.ptr(name + ".bias"), fout, Y.data_ptr(), fout,
+                                   1 if act else 0, Z.data_ptr() if act else None, self._s()),
+                   "latec_tr_linear")
         return Y, Z
 
     def _lin_bwd(self, X, rows, fin, name, fout, dY, Z, dX=None, accum=False):
-        _lib.check(self.lib.latec_tr_linear_bwd(
+        _lib.check(self._tr_linear_bwd(
             X.data_ptr(), fin, rows, fin, self.P.ptr(name + ".weight"), fout, dY.data_ptr(), fout,
             Z.data_ptr() if Z is not None else None, 1 if Z is not None else 0,
             dX.data_ptr() if dX is not None else None, fin, 1 if accum else 0,
@@ -168,11 +186,10 @@ class Trainer:
                                               (t["two"] if two else t["one"]).data_ptr(), npairs, B,
                                               two, X.data_ptr(), w, self._s()), "latec_tr_rows")
             H, Zh = self._lin(X, r, w, name + ".net.0", self.h, True)
-            _lib.check(self.lib.latec_tr_linear(H.data_ptr(), self.h, r, self.h,
-                                                self.P.ptr(name + ".net.2.weight"),
-                                                self.P.ptr(name + ".net.2.bias"), d,
-                                                MS[off:].data_ptr(), d, 0, None, self._s()),
-                       "latec_tr_linear")
+            _lib.check(self._tr_linear(H.data_ptr(), self.h, r, self.h,
+                                       self.P.ptr(name + ".net.2.weight"),
+                                       self.P.ptr(name + ".net.2.bias"), d, MS[off:].data_ptr(), d,
+                                       0, None, self._s()), "latec_tr_linear")
             rec[name] = (X, H, Zh, w, npairs, two)
         S1, Zs = self._lin(MS, rows, d, "line_pool.wk.0", d, True) if rows else (None, None)
         n_out = B * M * K
@@ -384,6 +401,14 @@ class Trainer:
         self.g.zero_()
 
     def optimizer_step(self, lr):
+        """AdamW (+ EMA) on the float32 master weights. In BF16 mode the
+        tensor-core GEMMs' error word is checked first, and a gradient with a
+        non-finite entry skips the step (returns False), as GradScaler does."""
+        if self.precision == "bf16":
+            _lib.check(self.lib.latec_tr_gemm_status(self._s()), "latec_tr_gemm_status")
+            if not bool(_torch().isfinite(self.g).all()):
+                self.skipped_steps += 1
+                return False
         self.step_count += 1
         _lib.check(self.lib.latec_tr_adamw(self.p.data_ptr(), self.g.data_ptr(), self.m.data_ptr(),
                                            self.v.data_ptr(), self.p.numel(), float(lr), 0.9,
@@ -394,6 +419,7 @@ class Trainer:
             decay = min(self.ema_decay, (1.0 + s) / (10.0 + s))
             _lib.check(self.lib.latec_tr_ema(self.ema.data_ptr(), self.p.data_ptr(), self.p.numel(),
                                              float(decay), self._s()), "latec_tr_ema")
+        return True
 
     def weights(self, ema=True):
         """The (EMA) weights as a state_dict of float32 arrays."""
@@ -420,7 +446,7 @@ def train(steps=3000, *, d=64, agg_level=1, shape4=(16, 16, 16, 16), batch4=4,
           shape2=(128, 128), batch2=16, stride4=8, shape3=(40, 40, 40), batch3=0, stride3=8,
           noise_range=(1e-4, 1e-2), lr=2e-3, warmup=100,
           ema_decay=0.999, mse_weight=1.0, seed=0, device=None, log_every=50, out=None,
-          trainer=None, callback=None, synthetic=None):
+          trainer=None, callback=None, synthetic=None, precision="fp32"):
     """Train on mixed 4-D / 2-D synthetic batches (train_h100.sh: 16^4 x 4
     plus 128^2 x 16 per step); returns the Trainer. ``batch3`` > 0 adds 3-D
     fields of ``shape3`` (the 4-D correlation knob, ``stride3``) to every step,
@@ -435,7 +461,7 @@ def train(steps=3000, *, d=64, agg_level=1, shape4=(16, 16, 16, 16), batch4=4,
             "field3d": knobs["correlation_4d"]}
 
     tr = trainer or Trainer(d=d, agg_level=agg_level, seed=seed, lr=lr, ema_decay=ema_decay,
-                            mse_weight=mse_weight, device=device)
+                            mse_weight=mse_weight, device=device, precision=precision)
     rng = np.random.default_rng(seed)
     strides2 = (8, 16, 32)
     hist = []
@@ -486,6 +512,9 @@ def main(argv=None):
     ap.add_argument("--noise-range", type=float, nargs=2, default=(1e-4, 1e-2))
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default="gnn_trained.pt")
+    ap.add_argument("--precision", choices=("fp32", "bf16"), default="fp32",
+                    help="GEMM operands of the linear layers (bf16: tensor cores, float32 "
+                         "accumulation and master weights)")
     # the generator's knobs (the reference trainer's --synthetic-* flags)
     ap.add_argument("--synthetic-turbulence-frac", type=float, default=None)
     ap.add_argument("--synthetic-discontinuities", type=int, default=None)
@@ -501,7 +530,7 @@ def main(argv=None):
     train(a.steps, d=a.d, agg_level=a.agg_level, lr=a.lr, warmup=a.warmup, ema_decay=a.ema_decay,
           mse_weight=a.mse_weight, batch4=a.batch4, batch2=a.batch2, batch3=a.batch3,
           shape3=tuple(a.shape3),
-          noise_range=tuple(a.noise_range), seed=a.seed, out=a.out,
+          noise_range=tuple(a.noise_range), seed=a.seed, out=a.out, precision=a.precision,
           synthetic={k: v for k, v in given.items() if v is not None})
 
 
