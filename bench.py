@@ -291,10 +291,20 @@ def compat_leg(x, eb):
     """The drop-in stream (entropy="compat": the reference's single-stack rANS
     layout and level-9 zstd frame, readable by the reference decoder) on the
     512^3 workload: one timed round trip after a warm-up. The single-stack
-    coder is serial by nature (one thread per stage) and the zstd frame is
-    built on the host."""
+    coder is serial by nature (one state chain per stage) and the zstd frame
+    is built on the host."""
+    import latec_b200 as lb
+
     out = _roundtrip_leg(x, eb, LEVELS, STRIDE, 1, entropy="compat")
     out["workload"] = "512^3 float32 turbulence + 3 jumps, rel eb 1e-4, compat stream"
+    # where one compress spends its time: the device passes and the stage
+    # coder (k_stack_encode) up to the payload download, then the host's
+    # literal-zstd decisions and level-9 frame
+    _s, st = lb.compress(x, eb, lb.InterpPredictor("cubic", LEVELS, STRIDE, 1), levels=LEVELS,
+                         anchor_stride=STRIDE, recon="none", entropy="compat")
+    out["compress_split_s"] = {"stages": st.get("predict_s"), "fit": st.get("fit_s"),
+                               "rans_coder": st.get("rans_s"),
+                               "host_literals_and_zstd_frame": st.get("download_s")}
     return out
 
 

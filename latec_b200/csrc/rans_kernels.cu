@@ -287,83 +287,85 @@ __global__ void __launch_bounds__(32 * DEC_WARPS)
 }
 
 // --------------------------------------------------------------- compat
-// One thread per stage (lane 0 of the stage's own CTA, so that stages never
-// share a warp and diverge against each other) codes the whole stage in
-// reverse. The state chain is serial, so everything off it is fetched ahead:
-// the codes (and scale levels) two groups of SG symbols ahead, the encoder
-// entries one group ahead.
-constexpr int SG = 8;
+// The single-stack coder: one serial state chain per stage, every stage on
+// its own CTA.
+//   Encode (reverse symbol order): a CTA of 256 threads per stage. Thread 0
+//   carries the chain; warps 1-7 turn the next block of SB codes (and scale
+//   levels) into 16-byte records {gm, left, freq | gsh2 << 25 | gsh1 << 30}
+//   in shared memory while thread 0 codes the current block (two buffers, one
+//   __syncthreads per block), so the chain never waits on a global load.
+constexpr int SB = 1024;
+constexpr int ST_THREADS = 256;
+constexpr int SG = 8;  // decoder: scale levels loaded this many symbols ahead
 
-__global__ void k_stack_encode(const RansStageDesc* __restrict__ st, int n_stages,
-                               const uint16_t* __restrict__ codes, const uint8_t* __restrict__ levels,
-                               uint32_t* __restrict__ scratch, uint32_t* __restrict__ stage_words,
-                               uint32_t* __restrict__ err) {
+__global__ void __launch_bounds__(ST_THREADS)
+    k_stack_encode(const RansStageDesc* __restrict__ st, int n_stages,
+                   const uint16_t* __restrict__ codes, const uint8_t* __restrict__ levels,
+                   uint32_t* __restrict__ scratch, uint32_t* __restrict__ stage_words,
+                   uint32_t* __restrict__ err) {
     const int t = blockIdx.x;
-    if (t >= n_stages || threadIdx.x != 0) return;
+    if (t >= n_stages) return;
     const RansStageDesc& d = st[t];
     if (d.mode != MODE_COMPAT) return;
+    __shared__ uint4 ring[2][SB];
+    __shared__ int s_bad;
+    const int tid = threadIdx.x;
     const EncSym* enc = (const EncSym*)d.enc;
     const uint32_t alpha1 = d.alphabet + 1;
     const uint16_t* c = codes + d.codes_off;
     const uint8_t* lv = d.per_point ? levels + d.codes_off : nullptr;
     uint32_t* out = scratch + d.scratch_off;
     const int64_t n = d.n;
-    uint16_t nc[SG];
-    uint8_t nr[SG];
-    EncSym ne[SG];
-    bool bad = false;
-    // codes of the group whose highest index is `top`
-    auto fetch_codes = [&](int64_t top) {
-#pragma unroll
-        for (int u = 0; u < SG; u++) {
-            const int64_t j = top - u;
-            nc[u] = j >= 0 ? c[j] : (uint16_t)0;
-            nr[u] = (j >= 0 && lv) ? lv[j] : (uint8_t)0;
+    const int64_t nb = (n + SB - 1) / SB;
+    if (tid == 0) s_bad = 0;
+    __syncthreads();
+    // block b: slot j holds symbol n - 1 - b SB - j
+    auto fill = [&](int64_t b, int buf, int t0, int nt) {
+        const int64_t top = n - 1 - b * SB;
+        for (int j = t0; j < SB; j += nt) {
+            const int64_t i = top - j;
+            uint4 r = make_uint4(0u, 0u, 0u, 0u);
+            if (i >= 0) {
+                const uint32_t sym = narrow(c[i], d.radius, d.kexp);
+                const uint32_t row = lv ? lv[i] : 0u;
+                if (sym >= d.alphabet) s_bad = 1;
+                const EncSym e = enc[(uint64_t)row * alpha1 + (sym < d.alphabet ? sym : 0u)];
+                const uint32_t left = e.freq == 1u ? e.bias - ((1u << PREC) - 1u) : e.bias;
+                r = make_uint4((uint32_t)e.gm, (uint32_t)(e.gm >> 32), left,
+                               e.freq | ((uint32_t)e.gsh2 << 25) | ((uint32_t)e.gsh1 << 30));
+            }
+            ring[buf][j] = r;
         }
     };
-    // encoder entries of the codes in nc / nr
-    auto fetch_entries = [&](int64_t top) {
-#pragma unroll
-        for (int u = 0; u < SG; u++) {
-            ne[u] = EncSym{};
-            if (top - u >= 0) {
-                const uint32_t sym = narrow(nc[u], d.radius, d.kexp);
-                bad |= sym >= d.alphabet;
-                ne[u] = enc[(uint64_t)nr[u] * alpha1 + (sym < d.alphabet ? sym : 0u)];
+    if (nb > 0) fill(0, 0, tid, ST_THREADS);
+    __syncthreads();
+    uint64_t x = 0, w = 0;
+    for (int64_t b = 0; b < nb; b++) {
+        if (tid >= 32) {
+            if (b + 1 < nb) fill(b + 1, (int)((b + 1) & 1), tid - 32, ST_THREADS - 32);
+        } else if (tid == 0) {
+            const int cnt = (int)(n - b * SB < SB ? n - b * SB : SB);
+            const uint4* rb = ring[b & 1];
+            uint4 nx = rb[0];
+            for (int j = 0; j < cnt; j++) {
+                const uint4 r = nx;
+                if (j + 1 < cnt) nx = rb[j + 1];
+                const uint64_t gm = ((uint64_t)r.y << 32) | r.x;
+                const uint32_t p = r.w & 0x1FFFFFFu;
+                const uint32_t g2 = (r.w >> 25) & 31u, g1 = r.w >> 30;
+                if ((x >> (64 - PREC)) >= p) {
+                    out[w++] = (uint32_t)x;
+                    x >>= 32;
+                }
+                const uint64_t t1 = __umul64hi(x, gm);
+                const uint64_t q = (t1 + ((x - t1) >> g1)) >> g2;
+                x = (q << PREC) | (uint64_t)((uint32_t)(x - q * p) + r.z);
             }
         }
-    };
-    uint64_t x = 0;
-    uint64_t w = 0;
-    if (n > 0) {
-        fetch_codes(n - 1);
-        fetch_entries(n - 1);
-        fetch_codes(n - 1 - SG);
+        __syncthreads();
     }
-    for (int64_t top = n - 1; top >= 0; top -= SG) {
-        EncSym e[SG];
-#pragma unroll
-        for (int u = 0; u < SG; u++) e[u] = ne[u];
-        if (top - SG >= 0) {
-            fetch_entries(top - SG);
-            if (top - 2 * SG >= 0) fetch_codes(top - 2 * SG);
-        }
-        if (bad) break;
-#pragma unroll
-        for (int u = 0; u < SG; u++) {
-            if (top - u < 0) break;
-            const uint32_t p = e[u].freq;
-            const uint32_t left = p == 1u ? e[u].bias - ((1u << PREC) - 1u) : e[u].bias;
-            if ((x >> (64 - PREC)) >= p) {
-                out[w++] = (uint32_t)x;
-                x >>= 32;
-            }
-            const uint64_t t1 = __umul64hi(x, e[u].gm);
-            const uint64_t q = (t1 + ((x - t1) >> e[u].gsh1)) >> e[u].gsh2;
-            x = (q << PREC) | (uint64_t)((uint32_t)(x - q * p) + left);
-        }
-    }
-    if (bad) {
+    if (tid != 0) return;
+    if (s_bad) {
         atomicOr(err, 2u);
         return;
     }
@@ -587,8 +589,8 @@ int launch_stack_encode(const RansStageDesc* st, int n_stages, const uint16_t* c
                         const uint8_t* levels, uint32_t* scratch, uint32_t* stage_words,
                         uint32_t* err, cudaStream_t s) {
     if (!n_stages) return LATEC_OK;
-    k_stack_encode<<<n_stages, 32, 0, s>>>(st, n_stages, codes, levels, scratch,
-                                                        stage_words, err);
+    k_stack_encode<<<n_stages, ST_THREADS, 0, s>>>(st, n_stages, codes, levels, scratch,
+                                                   stage_words, err);
     return last_err();
 }
 

@@ -140,30 +140,80 @@ __device__ uint32_t g_gemm_tc_err;
 
 // One GT_KC-wide K chunk of an R-row operand: element (r, k) is
 // src[r * rs + k * ks], zero at r >= r_valid or k >= k_end; times gelu'(Z) at
-// the same offset when GA. Consecutive threads take consecutive rows, so the
-// loads are coalesced when rs == 1 and each thread reads 32 contiguous bytes
-// when ks == 1; the canonical stores of a warp fill 512 contiguous bytes.
+// the same offset when GA. Each item is 8 consecutive k of one row (one 16-byte
+// canonical store); the canonical stores of 8 consecutive rows fill 128
+// contiguous bytes.
+//   rs == 1 (k strided): consecutive threads take consecutive rows, so each of
+//     the 8 loads of a warp reads 128 contiguous bytes.
+//   ks == 1 (rows contiguous): a warp takes 8 rows x 4 chunks, so the 4
+//     chunks of a row are 128 contiguous bytes, read as float4 (or float2)
+//     when vw says the rows allow it (vw = 4, 2 or 1 elements per load).
 template <int R, int GA>
 __device__ __forceinline__ void stage_chunk(__nv_bfloat16* dst, const float* __restrict__ src,
                                             const float* __restrict__ Z, int64_t rs, int64_t ks,
-                                            int r_valid, int64_t k0, int64_t k_end, int tid) {
+                                            int vw, int r_valid, int64_t k0, int64_t k_end,
+                                            int tid) {
     constexpr int ITEMS = R * (GT_KC / 8);
     for (int it = tid; it < ITEMS; it += GT_THREADS) {
-        const int r = it % R, c = it / R;
+        int r, c;
+        if (ks == 1) {
+            const int g = it >> 5, l = it & 31;
+            r = (g >> 1) * 8 + (l & 7);
+            c = (g & 1) * 4 + (l >> 3);
+        } else {
+            r = it % R;
+            c = it / R;
+        }
         float v[8];
+        const int64_t kc = k0 + c * 8;
+        if (ks == 1 && r < r_valid && kc + 8 <= k_end && vw > 1) {
+            const int64_t o = (int64_t)r * rs + kc;
+            if (vw == 4) {
 #pragma unroll
-        for (int e = 0; e < 8; e++) {
-            const int64_t k = k0 + c * 8 + e;
-            float x = 0.0f;
-            if (r < r_valid && k < k_end) {
-                const int64_t o = (int64_t)r * rs + k * ks;
-                x = src[o];
-                if (GA) x *= gelu_d(Z[o]);
+                for (int h = 0; h < 2; h++) {
+                    const float4 f = *(const float4*)(src + o + 4 * h);
+                    v[4 * h] = f.x, v[4 * h + 1] = f.y, v[4 * h + 2] = f.z, v[4 * h + 3] = f.w;
+                    if (GA) {
+                        const float4 zz = *(const float4*)(Z + o + 4 * h);
+                        v[4 * h] *= gelu_d(zz.x), v[4 * h + 1] *= gelu_d(zz.y);
+                        v[4 * h + 2] *= gelu_d(zz.z), v[4 * h + 3] *= gelu_d(zz.w);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int h = 0; h < 4; h++) {
+                    const float2 f = *(const float2*)(src + o + 2 * h);
+                    v[2 * h] = f.x, v[2 * h + 1] = f.y;
+                    if (GA) {
+                        const float2 zz = *(const float2*)(Z + o + 2 * h);
+                        v[2 * h] *= gelu_d(zz.x), v[2 * h + 1] *= gelu_d(zz.y);
+                    }
+                }
             }
-            v[e] = x;
+        } else {
+#pragma unroll
+            for (int e = 0; e < 8; e++) {
+                const int64_t k = kc + e;
+                float x = 0.0f;
+                if (r < r_valid && k < k_end) {
+                    const int64_t o = (int64_t)r * rs + k * ks;
+                    x = src[o];
+                    if (GA) x *= gelu_d(Z[o]);
+                }
+                v[e] = x;
+            }
         }
         st_bf16x8(dst + canon((uint32_t)r, (uint32_t)(c * 8), R), v);
     }
+}
+
+// Widest vector (4, 2 or 1 floats) that every row start of a row-contiguous
+// operand allows.
+__device__ __forceinline__ int row_vec(const float* p, int64_t rs, const float* z) {
+    const uintptr_t a = (uintptr_t)p | (z ? (uintptr_t)z : 0);
+    if (rs % 4 == 0 && a % 16 == 0) return 4;
+    if (rs % 2 == 0 && a % 8 == 0) return 2;
+    return 1;
 }
 
 template <int TA, int TB, int GA, int ACC, int NT>
@@ -180,7 +230,9 @@ __global__ void __launch_bounds__(GT_THREADS)
     __nv_bfloat16* sbuf = (__nv_bfloat16*)smem_raw;  // [A0 | B0 | A1 | B1]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * GT_M, n0 = blockIdx.y * NT;
-    const int64_t per = ((int64_t)Kd + gridDim.z - 1) / gridDim.z;
+    // split-K slices start on GT_KC boundaries (aligned vector loads)
+    const int64_t per =
+        (((int64_t)Kd + gridDim.z - 1) / gridDim.z + GT_KC - 1) / GT_KC * GT_KC;
     const int64_t kb = per * blockIdx.z;
     const int64_t ke = kb + per < Kd ? kb + per : Kd;
     // A(m, k) = TA ? A[k lda + m] : A[m lda + k]; B^T(n, k) = B(k, n)
@@ -190,6 +242,8 @@ __global__ void __launch_bounds__(GT_THREADS)
     const int64_t b_off = TB ? (int64_t)n0 * ldb : (int64_t)n0;
     const int m_valid = M - m0 < GT_M ? M - m0 : GT_M;
     const int n_valid = N - n0 < NT ? N - n0 : NT;
+    const int a_vw = TA ? 1 : row_vec(A + a_off, a_rs, GA ? Z + a_off : nullptr);
+    const int b_vw = TB ? row_vec(Bm + b_off, b_rs, nullptr) : 1;
 
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&mbar[0])), "r"(1));
@@ -219,9 +273,9 @@ __global__ void __launch_bounds__(GT_THREADS)
         __nv_bfloat16* sa = sbuf + s * (A_ELEMS + B_ELEMS);
         __nv_bfloat16* sb = sa + A_ELEMS;
         const int64_t k0 = kb + (int64_t)i * GT_KC;
-        stage_chunk<GT_M, GA>(sa, A + a_off, GA ? Z + a_off : nullptr, a_rs, a_ks, m_valid, k0,
-                              ke, tid);
-        stage_chunk<NT, 0>(sb, Bm + b_off, nullptr, b_rs, b_ks, n_valid, k0, ke, tid);
+        stage_chunk<GT_M, GA>(sa, A + a_off, GA ? Z + a_off : nullptr, a_rs, a_ks, a_vw, m_valid,
+                              k0, ke, tid);
+        stage_chunk<NT, 0>(sb, Bm + b_off, nullptr, b_rs, b_ks, b_vw, n_valid, k0, ke, tid);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
