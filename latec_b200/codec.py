@@ -482,8 +482,7 @@ class _Encoder:
             kexp, level, shape, owx, bits = fits[t]
             if n >= rans_model.LITERAL_MIN:
                 codes = b.codes[b.offsets[t]:b.offsets[t + 1]].cpu().numpy().view(np.uint16)
-                syms = rans_model.narrow(codes, self.radius, kexp).astype(
-                    rans_model.literal_dtype(kexp)).tobytes()
+                syms = rans_model.narrow_literals(codes, self.radius, kexp).tobytes()
                 z = bitstream.zstd()
                 scout = z.compress(syms, 1)
                 if len(scout) * rans_model.LITERAL_SCOUT_SLACK < bits / 8.0:

@@ -261,6 +261,17 @@ def literal_dtype(kexp):
     return np.dtype(np.uint8 if int(kexp) <= 7 else np.uint16)
 
 
+def narrow_literals(codes, radius, kexp):
+    """``narrow(codes, radius, kexp)`` in ``literal_dtype(kexp)``: the symbol
+    bytes of a literal (zstd) stage. Works in 16-bit modular arithmetic: an
+    in-range code c maps to c - radius + 2^kexp < 2^(kexp + 1) <= 2^16, and an
+    outlier (code 0) to 0."""
+    c = np.asarray(codes, np.uint16)
+    s = c + np.uint16(((1 << int(kexp)) - int(radius)) % (1 << 16))
+    s[c == 0] = 0
+    return s.astype(literal_dtype(kexp), copy=False)
+
+
 # ------------------------------------------------------------------ device tables
 
 class DeviceTables:

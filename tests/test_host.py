@@ -264,3 +264,25 @@ def test_blocked_anchor_schedule_is_the_reference_schedule():
                     assert plan.counts[t] == int(mask.sum())
                     assert np.array_equal(_stage_flat(plan, t), np.flatnonzero(mask)), \
                         (shape, st, lv, block, t)
+
+
+@pytest.mark.parametrize("radius,kexp", [(32768, 1), (32768, 7), (32768, 8), (32768, 15),
+                                         (512, 9), (1, 1), (300, 8), (40000 // 2, 14)])
+def test_literal_narrowing_matches_narrow(radius, kexp):
+    """The literal stages' 16-bit narrowing equals the reference-form narrow()."""
+    from latec_b200 import rans_model
+
+    rng = np.random.default_rng(radius + kexp)
+    span = 1 << kexp
+    q = rng.integers(-(span - 1), span, 100000)
+    codes = np.clip(q + radius, 1, 65535).astype(np.uint16)
+    codes[rng.random(codes.size) < 0.05] = 0
+    lo, hi = max(1, radius - span + 1), min(65535, radius + span - 1)
+    codes[:4] = [0, lo, hi, radius]
+    keep = (codes == 0) | ((codes.astype(np.int64) - radius >= -(span - 1))
+                           & (codes.astype(np.int64) - radius <= span - 1))
+    codes = codes[keep]
+    want = rans_model.narrow(codes, radius, kexp).astype(rans_model.literal_dtype(kexp))
+    got = rans_model.narrow_literals(codes, radius, kexp)
+    assert got.dtype == want.dtype
+    assert np.array_equal(got, want)
