@@ -96,10 +96,10 @@ class Trainer:
 
     def __init__(self, d=64, agg_level=1, weights=None, seed=0, lr=2e-3, weight_decay=1e-3,
                  ema_decay=0.999, mse_weight=1.0, max_radius=64, device=None, precision="fp32"):
-        torch = _torch()
-        self.lib = _lib.load()
         if precision not in ("fp32", "bf16"):
             raise ValueError("precision must be 'fp32' or 'bf16'")
+        torch = _torch()
+        self.lib = _lib.load()
         self.precision = precision
         bf = precision == "bf16"
         self._tr_linear = self.lib.latec_tr_linear_bf16 if bf else self.lib.latec_tr_linear

@@ -286,3 +286,10 @@ def test_literal_narrowing_matches_narrow(radius, kexp):
     got = rans_model.narrow_literals(codes, radius, kexp)
     assert got.dtype == want.dtype
     assert np.array_equal(got, want)
+
+
+def test_trainer_rejects_unknown_precision():
+    from latec_b200.train import Trainer
+
+    with pytest.raises(ValueError):
+        Trainer(precision="fp16")
