@@ -390,7 +390,61 @@ def gnn_leg(dev, steps=2):
             "compress_gbs": nbytes * steps / (t1 - t0) / 1e9,
             "decompress_gbs": nbytes * steps / (t2 - t1) / 1e9,
             "max_abs_err": err, "bound": GNN_EB, "roundtrip_slack": slack, "dtype": "f32",
+            "precision": gnn_precision(codec, x, rel),
             "full_tensor": gnn_full(dev, codec)}
+
+
+def gnn_precision(codec, x, rel):
+    """The same 32^4 chunk coded with the message MLPs in float32, BF16 and
+    FP8 (the codec's fp16=False / fp16=True / fp8=True): stream bytes, and the
+    model's predictions against the float32 run's, as max and RMS differences
+    of mu and log2 b. At the first model stage every run sees the same coded
+    anchors, so that stage isolates the network's precision; over all stages
+    the later inputs also differ by the runs' own reconstructions. Errors are
+    reported in the line instead of ending the bench."""
+    import torch
+
+    try:
+        runs = {}
+        for name, kw in (("f32", {"fp16": False}), ("bf16", {"fp16": True}),
+                         ("fp8", {"fp16": True, "fp8": True})):
+            codec.stage_trace = []
+            try:
+                s = codec.compress(x, rel, levels=GNN_LEVELS, **kw)
+                trace = [(int(t["stage"]), t["mu"].double().reshape(-1),
+                          torch.log2(t["scale"].double()).reshape(-1))
+                         for t in codec.stage_trace]
+            finally:
+                codec.stage_trace = None
+            runs[name] = (len(s), trace)
+
+        def diff(a, b):
+            d = (a - b).abs()
+            return float(d.max().item()), float(d.pow(2).mean().sqrt().item())
+
+        out = {"stream_bytes": {k: v[0] for k, v in runs.items()},
+               "ratio": {k: x.numel() * 4 / v[0] for k, v in runs.items()}}
+        ref = runs["f32"][1]
+        for name in ("bf16", "fp8"):
+            tr = runs[name][1]
+            pairs = [(a, b) for a, b in zip(tr, ref) if a[0] == b[0] and a[1].numel() == b[1].numel()]
+            first = next(((a, b) for a, b in pairs if a[1].numel()), None)
+            if first is None:
+                continue
+            mu_all = diff(torch.cat([a[1] for a, _ in pairs]), torch.cat([b[1] for _, b in pairs]))
+            lb_all = diff(torch.cat([a[2] for a, _ in pairs]), torch.cat([b[2] for _, b in pairs]))
+            out[name + "_vs_f32"] = {
+                "first_model_stage": {"stage": first[0][0], "points": int(first[0][1].numel()),
+                                      "mu_max": diff(first[0][1], first[1][1])[0],
+                                      "mu_rms": diff(first[0][1], first[1][1])[1],
+                                      "log2b_max": diff(first[0][2], first[1][2])[0],
+                                      "log2b_rms": diff(first[0][2], first[1][2])[1]},
+                "all_stages": {"stages": len(pairs), "mu_max": mu_all[0], "mu_rms": mu_all[1],
+                               "log2b_max": lb_all[0], "log2b_rms": lb_all[1]}}
+        out["units"] = "mu on the codec's normalised [0, 1] values; log2 b in bits"
+        return out
+    except Exception as e:  # a diagnostic leg: report, do not end the bench
+        return {"error": f"{type(e).__name__}: {e}"}
 
 
 def gnn_full(dev, codec):
